@@ -1,0 +1,284 @@
+"""Benchmark: FP64 finite-volume residual throughput (M faces/s) on B200.
+
+A step is one full residual evaluation R(W) — first-order ghost update, LSQ
+gradients, limiter (with the global extrema), face fluxes and the atomic-free
+cell gather — on the laminar cylinder workload (O-grid 256x128x1 hex, Roe +
+viscous, Sutherland, Pr 0.72, VK limiter).  Timing: per-step CUDA events on
+the library's stream, L2 flushed (512 MB memset) before every step, max over
+ranks.  ``e2e`` is the same metric through the C ABI with pinned host input
+and output copies inside the timed region.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+    python -m torch.distributed.run --nproc-per-node N bench.py --gpus N ...
+
+Multi-GPU runs are replicas: every rank evaluates its own copy of the mesh
+(weak scaling, no data-path collective).  ``--impl reference`` times the CPU
+restatement of the reference's residual on the host cores instead.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    "cylinder": dict(fn="cylinder_case", kw={}),
+    "wedge": dict(fn="wedge_case", kw={}),
+    "hypersonic": dict(fn="hypersonic_case", kw={}),
+    "plate": dict(fn="plate_case", kw=dict(turbulent=False)),
+    "plate64": dict(fn="plate_case", kw=dict(nk=64, turbulent=False)),
+}
+METRIC = "M faces/s residual + % HBM peak; Newton wall time to 1e-10: mixed+JVP vs plain FP64"
+UNIT = "M faces/s"
+
+
+def make_case(name):
+    from freecfd_b200 import cases
+    w = WORKLOADS[name]
+    return getattr(cases, w["fn"])(**w["kw"])
+
+
+def alg_bytes(m, s=8):
+    """Algorithmic bytes of one residual (FP64): interior state read + residual
+    write + cell geometry + LSQ matrix, ghost state write+read, face geometry and
+    indices, stencil indices and the cell->face list."""
+    return (m.nc * (5 * s + 5 * s + 4 * s + 6 * s) + m.nghost * (10 * s) + m.nf * (8 + 7 * s)
+            + m.n_grad_entries * 4 + m.n_cell_faces * 4)
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampler for the timed region."""
+
+    def __init__(self, index=0):
+        self.index = index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + q,
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                self.samples.append([x.strip() for x in out.stdout.strip().split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if len(s) > 3 + i and "Active" in s[3 + i]
+                          and not s[3 + i].startswith("Not")})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def cpu_baseline(case, seconds=12.0):
+    """Single-core oracle (restatement of the reference's CPU residual)."""
+    import oracle
+    o = oracle.Oracle(case)
+    o.residual(case.state)
+    n, t0 = 0, time.perf_counter()
+    while True:
+        o.residual(case.state)
+        n += 1
+        el = time.perf_counter() - t0
+        if el > seconds or n >= 200:
+            break
+    v = o.nf * n / el / 1e6
+    o.close()
+    return {"value": round(v, 4), "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"{n} full residual evaluations of the same workload ({o.nf} faces) in {el:.1f} s, "
+                      f"single-threaded C++ restatement (-O2, no FMA)"}
+
+
+def _ref_worker(args):
+    name, steps, warmup, q = args
+    import oracle
+    case = make_case(name)
+    o = oracle.Oracle(case)
+    for _ in range(warmup):
+        o.residual(case.state)
+    q.put(("ready", os.getpid()))
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        o.residual(case.state)
+    el = time.perf_counter() - t0
+    q.put(("done", el, o.nf))
+
+
+def run_reference(args):
+    import multiprocessing as mp
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    ctx = mp.get_context("spawn")
+    ncpu = os.cpu_count() or 1
+    workers = max(1, min(ncpu, args.ref_workers))
+    q = ctx.Manager().Queue()
+    steps = args.steps
+    procs = [ctx.Process(target=_ref_worker, args=((args.workload, steps, args.warmup, q),)) for _ in range(workers)]
+    for p in procs:
+        p.start()
+    done = []
+    while len(done) < workers:
+        msg = q.get(timeout=3600)
+        if msg[0] == "done":
+            done.append(msg)
+    for p in procs:
+        p.join()
+    el = max(d[1] for d in done)
+    nf = done[0][2]
+    value = workers * nf * steps / el / 1e6
+    case = make_case(args.workload)
+    line = {"metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": args.gpus, "steps": steps,
+            "warmup": args.warmup, "ms_per_step": round(1e3 * el / steps, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": {"workload": case.workload, "faces": nf, "cells": case.mesh.n_cells},
+            "cpu_baseline": {"value": round(value, 4), "unit": UNIT, "cores": workers, "kind": "port",
+                             "sample": f"{workers} processes x {steps} full residual evaluations each (one mesh copy "
+                                       f"per core, like one MPI rank per core), C++ restatement of the reference"},
+            "e2e": {"value": round(value, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args):
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    dev = local if world > 1 else 0
+    torch.cuda.set_device(dev)
+    import freecfd_b200 as fb
+    case = make_case(args.workload)
+    import tempfile
+    tmp = tempfile.mkdtemp(prefix="fcfd_bench_")
+    cs = fb.Case(case.write_deck(tmp))
+    mesh = fb.Mesh(case.mesh, cs)
+    ns = fb.NavierStokes(mesh, cs, dev)
+    W = np.ascontiguousarray(case.state)
+    ns.residual(W)                               # upload + first evaluation (also checks BC errors)
+    ns.time_residual(max(args.warmup, 1), True)  # warm-up steps
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with Clocks(dev) as clk:
+        t = ns.time_residual(args.steps, True)
+    torch.cuda.synchronize()
+    ms = float(t[0])
+    kern = {"ghost_minmax": t[1], "grad_limiter": t[2], "outlet_density": t[3], "face_flux": t[4], "gather": t[5]}
+    if dist:
+        x = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(x, op=dist.ReduceOp.MAX)
+        ms = float(x.item())
+    value = world * mesh.nf / (ms * 1e-3) / 1e6
+    # end to end through the C ABI with pinned host buffers
+    Wp = torch.empty((mesh.nc, 5), dtype=torch.float64, pin_memory=True)
+    Rp = torch.empty((mesh.nc, 5), dtype=torch.float64, pin_memory=True)
+    Wp.numpy()[:] = W
+    Wn, Rn = Wp.numpy(), Rp.numpy()
+    for _ in range(max(args.warmup, 1)):
+        ns.residual(Wn, Rn)
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        ns.residual(Wn, Rn)
+    e2e_s = (time.perf_counter() - t0) / args.steps
+    if dist:
+        x = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
+        dist.all_reduce(x, op=dist.ReduceOp.MAX)
+        e2e_s = float(x.item())
+    e2e = world * mesh.nf / e2e_s / 1e6
+    peak, kind = peaks()
+    B = alg_bytes(mesh)
+    achieved = B / (ms * 1e-3) / 1e9
+    n_kernels = 4 + (1 if ns_has_outlet(case) else 0)
+    line = {"metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms, 5), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": case.workload, "cells": mesh.nc, "faces": mesh.nf, "ghosts": mesh.nghost,
+                       "stencil_entries": mesh.n_grad_entries, "l2": "flushed (512 MB memset before every step)",
+                       "parallelism": f"replicas x{world}"},
+            "e2e": {"value": round(e2e, 3), "unit": UNIT, "h2d_bytes_per_step": int(W.nbytes),
+                    "d2h_bytes_per_step": int(W.nbytes)},
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "traffic": None, "peak_kind": kind,
+                         "unit_of_work": "one residual evaluation (5 kernels)", "alg_bytes": int(B)},
+            "kernels_ms": {k: round(float(v), 5) for k, v in kern.items()},
+            "gpu_launches": n_kernels * args.steps,
+            "clocks": clk.summary()}
+    if rank == 0 and world == 1 and not args.no_cpu:
+        line["cpu_baseline"] = cpu_baseline(case, args.cpu_seconds)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    del ns
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def ns_has_outlet(case):
+    return "type=outlet" in case.deck
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="cylinder", choices=sorted(WORKLOADS))
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--ref-workers", type=int, default=64)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,107 @@
+"""ctypes binding of libfcfd_b200.so (the C ABI declared in include/fcfd.h).
+
+The shared library is built in-tree by ``freecfd_b200/Makefile`` (nvcc,
+sm_100a).  There is no Python or CPU fallback: if the library is missing,
+importing this module raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_build", "libfcfd_b200.so")
+
+FCFD_OK = 0
+FCFD_DEVICE_PTRS = 1
+STATUS = {0: "OK", 1: "ERR_INPUT", 2: "ERR_MESH", 3: "ERR_DIVERGED", 4: "ERR_NOT_CONVERGED", 5: "ERR_CUDA",
+          6: "ERR_TIMEOUT", 7: "ERR_UNSUPPORTED", 8: "ERR_BC"}
+
+EXPORTED = [
+    "fcfd_last_error", "fcfd_version", "fcfd_case_from_deck", "fcfd_case_destroy", "fcfd_case_summary",
+    "fcfd_mesh_create", "fcfd_mesh_destroy", "fcfd_mesh_sizes", "fcfd_mesh_connectivity", "fcfd_mesh_geometry",
+    "fcfd_mesh_lsq",
+    "fcfd_ctx_create", "fcfd_ctx_destroy", "fcfd_residual", "fcfd_last_stages", "fcfd_local_dt",
+    "fcfd_time_residual", "fcfd_point_flux",
+]
+
+
+class FcfdError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{STATUS.get(code, code)}: {msg}")
+        self.code = code
+
+
+def build(force: bool = False) -> str:
+    """Compile the CUDA library in-tree (nvcc, -gencode arch=compute_100a,code=sm_100a)."""
+    cmd = ["make", "-C", _HERE, "-s"]
+    if force:
+        subprocess.run(["make", "-C", _HERE, "-s", "clean"], check=True)
+    subprocess.run(cmd, check=True)
+    return LIB_PATH
+
+
+class _RawMesh(ctypes.Structure):
+    _fields_ = [("n_nodes", ctypes.c_int32), ("xyz", ctypes.POINTER(ctypes.c_double)),
+                ("n_cells", ctypes.c_int32), ("conn_index", ctypes.POINTER(ctypes.c_int32)),
+                ("conn", ctypes.POINTER(ctypes.c_int32)), ("n_bc", ctypes.c_int32),
+                ("bc_index", ctypes.POINTER(ctypes.c_int32)), ("bc_nodes", ctypes.POINTER(ctypes.c_int32))]
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"libfcfd_b200.so not found at {LIB_PATH}; build it with `make -C {_HERE}`")
+    L = ctypes.CDLL(LIB_PATH)
+    vp, dp, ip, i64p = ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int32), \
+        ctypes.POINTER(ctypes.c_int64)
+    L.fcfd_last_error.restype = ctypes.c_char_p
+    L.fcfd_version.restype = ctypes.c_char_p
+    L.fcfd_case_from_deck.argtypes = [ctypes.c_char_p, ctypes.POINTER(vp)]
+    L.fcfd_case_destroy.argtypes = [vp]
+    L.fcfd_case_destroy.restype = None
+    L.fcfd_case_summary.argtypes = [vp, dp, ip, ctypes.c_int32]
+    L.fcfd_mesh_create.argtypes = [ctypes.POINTER(_RawMesh), vp, ctypes.POINTER(vp)]
+    L.fcfd_mesh_destroy.argtypes = [vp]
+    L.fcfd_mesh_destroy.restype = None
+    L.fcfd_mesh_sizes.argtypes = [vp, i64p]
+    L.fcfd_mesh_connectivity.argtypes = [vp] + [ip] * 10
+    L.fcfd_mesh_geometry.argtypes = [vp] + [dp] * 9
+    L.fcfd_mesh_lsq.argtypes = [vp, dp, dp]
+    L.fcfd_ctx_create.argtypes = [vp, vp, ctypes.c_int, ctypes.POINTER(vp)]
+    L.fcfd_ctx_destroy.argtypes = [vp]
+    L.fcfd_ctx_destroy.restype = None
+    L.fcfd_residual.argtypes = [vp, vp, vp, ctypes.c_int]
+    L.fcfd_last_stages.argtypes = [vp, dp, dp, dp, dp, dp]
+    L.fcfd_local_dt.argtypes = [vp, vp, ctypes.c_double, ctypes.c_int, vp, ctypes.c_int]
+    L.fcfd_time_residual.argtypes = [vp, ctypes.c_int, ctypes.c_int, dp, ctypes.c_int]
+    L.fcfd_point_flux.argtypes = [ctypes.c_int, dp, dp, dp, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                  ctypes.c_double, ctypes.c_double, dp, dp]
+    for name in EXPORTED:
+        getattr(L, name)
+    return L
+
+
+lib = _load()
+
+
+def check(rc: int):
+    if rc != FCFD_OK:
+        raise FcfdError(rc, lib.fcfd_last_error().decode())
+
+
+def _d(a):
+    return None if a is None else a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _i(a):
+    return None if a is None else a.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
+
+
+def _ptr(a):
+    """Host numpy array or CUDA torch tensor -> (void*, flags)."""
+    if isinstance(a, np.ndarray):
+        return ctypes.c_void_p(a.ctypes.data), 0
+    return ctypes.c_void_p(a.data_ptr()), FCFD_DEVICE_PTRS

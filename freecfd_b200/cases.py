@@ -1,0 +1,441 @@
+"""Synthetic benchmark cases: raw CELL-type meshes, input decks and seeded states.
+
+Free CFD reads its meshes through ``Grid::readCGNS`` into a ``GridRawData``
+record (grid/grid.h:61-78): node coordinates, a cell connectivity list in
+CGNS element node order (HEXA_8 / PENTA_6) and, for every boundary-condition
+region, the set of node ids on it.  The benchmark meshes of this project have
+no CGNS file, so they are generated here in memory with exactly that shape:
+
+* cells are listed in generation order (i fastest, then j, then k) and use the
+  CGNS node order, so ``hexaFaces``/``prismFaces`` of
+  grid/grid_create_elements.cc:187-201 give outward normals;
+* boundary region ``b`` of the raw data is ``BC_{b+1}`` of the deck, as in
+  grid/grid_reader_cgns.cc:100-102 (regions are numbered by first appearance);
+* one-cell-thick 2-D meshes carry their front and back planes in a symmetry
+  region, which is what ``set_lengthScales`` (main.cc:456-491) expects.
+
+Every array is plain numpy; the same generated mesh feeds the CUDA library and
+the CPU oracle.
+"""
+from __future__ import annotations
+
+import math
+import os
+from dataclasses import dataclass, field
+
+import numpy as np
+
+R_UNIV = 8314.47215          # material/material.h:26
+R_AIR = 287.0
+MW_AIR = R_UNIV / R_AIR
+
+
+@dataclass
+class RawMesh:
+    """CELL-type raw grid (same meaning as ``GridRawData``, grid/grid.h:61-78)."""
+    nodes: np.ndarray            # (N, 3) float64
+    conn_index: np.ndarray       # (Nc+1,) int32, CSR offsets into conn
+    conn: np.ndarray             # (sum,) int32, node ids in CGNS element order
+    bc_nodes: list               # list of sorted int32 arrays, one per BC region
+    dimension: int = 2
+
+    @property
+    def n_cells(self) -> int:
+        return int(self.conn_index.shape[0] - 1)
+
+    def bc_csr(self):
+        idx = np.zeros(len(self.bc_nodes) + 1, dtype=np.int32)
+        for b, s in enumerate(self.bc_nodes):
+            idx[b + 1] = idx[b] + len(s)
+        flat = (np.concatenate(self.bc_nodes).astype(np.int32)
+                if self.bc_nodes else np.zeros(0, np.int32))
+        return idx, flat
+
+
+@dataclass
+class Case:
+    name: str
+    mesh: RawMesh
+    deck: str                    # input deck text (reference format)
+    materials: dict = field(default_factory=dict)   # name -> .mat text
+    state: np.ndarray = None     # (Nc, 5) float64 seeded primitive state p,u,v,w,T
+    freestream: tuple = ()       # (p, u, v, w, T)
+    workload: str = ""
+
+    def write_deck(self, directory: str) -> str:
+        """Write the deck (and any .mat files) into ``directory``; return deck path."""
+        os.makedirs(directory, exist_ok=True)
+        for mname, text in self.materials.items():
+            with open(os.path.join(directory, mname + ".mat"), "w") as fh:
+                fh.write(text)
+        path = os.path.join(directory, self.name + ".in")
+        with open(path, "w") as fh:
+            fh.write(self.deck)
+        return path
+
+
+# ----------------------------------------------------------------------------
+# mesh builders
+# ----------------------------------------------------------------------------
+
+def _extrude_quads(xy: np.ndarray, quads: np.ndarray, z: np.ndarray):
+    """Stack a 2-D node set over z levels and build HEXA_8 cells.
+
+    ``xy`` is (n2, 2); ``quads`` (nq, 4) counter-clockwise seen from +z.
+    Returns nodes (n2*len(z), 3) and hex connectivity (nq*(len(z)-1), 8).
+    """
+    n2 = xy.shape[0]
+    nz = z.shape[0]
+    nodes = np.empty((n2 * nz, 3), dtype=np.float64)
+    for k in range(nz):
+        nodes[k * n2:(k + 1) * n2, 0] = xy[:, 0]
+        nodes[k * n2:(k + 1) * n2, 1] = xy[:, 1]
+        nodes[k * n2:(k + 1) * n2, 2] = z[k]
+    cells = []
+    for k in range(nz - 1):
+        lo = quads + k * n2
+        hi = quads + (k + 1) * n2
+        cells.append(np.concatenate([lo, hi], axis=1))
+    return nodes, np.concatenate(cells, axis=0).astype(np.int32)
+
+
+def _cells_to_csr(cells: np.ndarray):
+    n, m = cells.shape
+    idx = (np.arange(n + 1, dtype=np.int64) * m).astype(np.int32)
+    return idx, cells.reshape(-1).astype(np.int32)
+
+
+def _structured_quads(ni: int, nj: int, periodic_i: bool = False):
+    """Quads over an (ni+1 or ni) x (nj+1) node lattice, node id = j*nI + i."""
+    nI = ni if periodic_i else ni + 1
+    i = np.arange(ni)
+    j = np.arange(nj)
+    I, J = np.meshgrid(i, j, indexing="xy")          # J rows, I fastest
+    I = I.reshape(-1)
+    J = J.reshape(-1)
+    ip = (I + 1) % nI if periodic_i else I + 1
+    n00 = J * nI + I
+    n10 = J * nI + ip
+    n11 = (J + 1) * nI + ip
+    n01 = (J + 1) * nI + I
+    return nI, n00, n10, n11, n01
+
+
+def wedge_mesh(ni: int = 120, nj: int = 60, length: float = 3.0,
+               height: float = 1.5, ramp_deg: float = 15.0, dz: float = 1.0 / 32.0):
+    """Euler 15-degree wedge/ramp: inlet, outlet (right + top), symmetry, slip wall.
+
+    BC regions (deck order): 1 inlet, 2 outlet, 3 symmetry (front/back), 4 slip wall.
+    """
+    nI, n00, n10, n11, n01 = _structured_quads(ni, nj)
+    x1 = np.linspace(0.0, length, ni + 1)
+    yb = np.maximum(0.0, x1 - length / 3.0) * math.tan(math.radians(ramp_deg))
+    jj = np.arange(nj + 1) / nj
+    X = np.repeat(x1[None, :], nj + 1, axis=0)
+    Y = yb[None, :] + (height - yb[None, :]) * jj[:, None]
+    xy = np.stack([X.reshape(-1), Y.reshape(-1)], axis=1)
+    quads = np.stack([n00, n10, n11, n01], axis=1)     # ccw: +x then +y
+    nodes, cells = _extrude_quads(xy, quads, np.array([0.0, dz]))
+    n2 = xy.shape[0]
+    ii = np.tile(np.arange(nI), nj + 1)
+    jn = np.repeat(np.arange(nj + 1), nI)
+    both = lambda mask: np.sort(np.concatenate([np.nonzero(mask)[0], np.nonzero(mask)[0] + n2])).astype(np.int32)
+    inlet = both(ii == 0)
+    outlet = both((ii == ni) | (jn == nj))
+    sym = np.arange(2 * n2, dtype=np.int32)
+    wall = both(jn == 0)
+    idx, conn = _cells_to_csr(cells)
+    return RawMesh(nodes, idx, conn, [inlet, outlet, sym, wall], dimension=2)
+
+
+def _ogrid_radii(nr: int, r0: float, r1: float, dr0: float):
+    """Geometric radial spacing with first step dr0 between r0 and r1."""
+    span = r1 - r0
+    if abs(dr0 * nr - span) < 1e-14:
+        return r0 + dr0 * np.arange(nr + 1)
+    lo, hi = 1.0 + 1e-12, 2.0
+    f = lambda q: dr0 * (q ** nr - 1.0) / (q - 1.0) - span
+    for _ in range(200):
+        mid = 0.5 * (lo + hi)
+        if f(mid) > 0:
+            hi = mid
+        else:
+            lo = mid
+    q = 0.5 * (lo + hi)
+    steps = dr0 * q ** np.arange(nr)
+    r = r0 + np.concatenate([[0.0], np.cumsum(steps)])
+    r[-1] = r1
+    return r
+
+
+def cylinder_mesh(ntheta: int = 256, nr: int = 128, r0: float = 0.5,
+                  r1: float = 15.0, dr0: float = 1e-3, dz: float = 1.0 / 32.0,
+                  jitter: float = 0.0, seed: int = 4321, prisms: bool = False):
+    """O-grid around a cylinder of diameter 1 (periodic in theta).
+
+    BC regions (deck order): 1 wall (r=r0), 2 inlet (outer ring, x<=0),
+    3 outlet (outer ring, x>=0), 4 symmetry (front/back).
+    ``jitter`` moves interior nodes by U(-jitter, jitter) of the local spacing
+    (seeded); ``prisms`` splits every hex into two PENTA_6 along its n00-n11
+    diagonal.
+    """
+    assert ntheta % 4 == 0
+    r = _ogrid_radii(nr, r0, r1, dr0)
+    th = 2.0 * math.pi * np.arange(ntheta) / ntheta
+    R = np.repeat(r[:, None], ntheta, axis=1)
+    T = np.repeat(th[None, :], nr + 1, axis=0)
+    if jitter > 0.0:
+        rng = np.random.default_rng(seed)
+        dr = np.diff(r)
+        local_dr = np.minimum(np.concatenate([[dr[0]], dr]), np.concatenate([dr, [dr[-1]]]))
+        dth = 2.0 * math.pi / ntheta
+        ur = rng.uniform(-jitter, jitter, size=(nr + 1, ntheta))
+        ut = rng.uniform(-jitter, jitter, size=(nr + 1, ntheta))
+        R[1:nr] += ur[1:nr] * local_dr[1:nr, None]
+        T[1:nr] += ut[1:nr] * dth
+    xy = np.stack([(R * np.cos(T)).reshape(-1), (R * np.sin(T)).reshape(-1)], axis=1)
+    nI, n00, n10, n11, n01 = _structured_quads(ntheta, nr, periodic_i=True)
+    # i runs along +theta, j along +r: (i,j),(i,j+1),(i+1,j+1),(i+1,j) is ccw
+    n2 = xy.shape[0]
+    if not prisms:
+        quads = np.stack([n00, n01, n11, n10], axis=1)
+        nodes, cells = _extrude_quads(xy, quads, np.array([0.0, dz]))
+    else:
+        nodes = np.concatenate([np.c_[xy, np.zeros(n2)], np.c_[xy, np.full(n2, dz)]])
+        a = np.stack([n00, n01, n11], axis=1)
+        b = np.stack([n00, n11, n10], axis=1)
+        tri = np.stack([a, b], axis=1).reshape(-1, 3)     # per quad: A then B
+        cells = np.concatenate([tri, tri + n2], axis=1).astype(np.int32)
+    jn = np.repeat(np.arange(nr + 1), ntheta)
+    it = np.tile(np.arange(ntheta), nr + 1)
+    q1, q3 = ntheta // 4, 3 * ntheta // 4
+    both = lambda mask: np.sort(np.concatenate([np.nonzero(mask)[0], np.nonzero(mask)[0] + n2])).astype(np.int32)
+    wall = both(jn == 0)
+    inlet = both((jn == nr) & (it >= q1) & (it <= q3))
+    outlet = both((jn == nr) & ((it >= q3) | (it <= q1)))
+    sym = np.arange(2 * n2, dtype=np.int32)
+    idx, conn = _cells_to_csr(cells)
+    return RawMesh(nodes, idx, conn, [wall, inlet, outlet, sym], dimension=2)
+
+
+def plate_mesh(ni: int = 384, nj: int = 192, nk: int = 4, plate: float = 2.0,
+               upstream: float = 0.5, height: float = 1.0, y1: float = 1.1e-5,
+               span: float = 0.1):
+    """3-D flat plate: inlet, outlet (right + top), no-slip wall (y=0, x>=0),
+    symmetry (y=0 upstream and the two z planes).
+
+    BC regions (deck order): 1 inlet, 2 outlet, 3 wall, 4 symmetry.
+    """
+    nu = max(2, ni // 6)
+    npl = ni - nu
+    # plate: tanh clustering at the leading edge
+    s = np.linspace(0.0, 1.0, npl + 1)
+    beta = 2.5
+    xp = plate * (1.0 + np.tanh(beta * (s - 1.0)) / math.tanh(beta))
+    xp[0] = 0.0
+    xp[-1] = plate
+    # upstream: mirror of the first plate spacing, geometric toward the inlet
+    d0 = xp[1] - xp[0]
+    xu_r = _ogrid_radii(nu, 0.0, upstream, min(d0, upstream / nu))
+    xu = -xu_r[::-1]
+    x1 = np.concatenate([xu[:-1], xp])
+    y = _ogrid_radii(nj, 0.0, height, min(y1, height / nj))
+    nI = ni + 1
+    X = np.repeat(x1[None, :], nj + 1, axis=0)
+    Y = np.repeat(y[:, None], nI, axis=1)
+    xy = np.stack([X.reshape(-1), Y.reshape(-1)], axis=1)
+    _, n00, n10, n11, n01 = _structured_quads(ni, nj)
+    quads = np.stack([n00, n10, n11, n01], axis=1)
+    z = np.linspace(0.0, span, nk + 1)
+    nodes, cells = _extrude_quads(xy, quads, z)
+    n2 = xy.shape[0]
+    ii = np.tile(np.arange(nI), nj + 1)
+    jn = np.repeat(np.arange(nj + 1), nI)
+    kk = np.repeat(np.arange(nk + 1), n2)
+    i3 = np.tile(ii, nk + 1)
+    j3 = np.tile(jn, nk + 1)
+    xnode = nodes[:, 0]
+    sel = lambda m: np.nonzero(m)[0].astype(np.int32)
+    inlet = sel(i3 == 0)
+    outlet = sel((i3 == ni) | (j3 == nj))
+    wall = sel((j3 == 0) & (xnode >= 0.0))
+    sym = sel(((j3 == 0) & (xnode <= 0.0)) | (kk == 0) | (kk == nk))
+    idx, conn = _cells_to_csr(cells)
+    return RawMesh(nodes, idx, conn, [inlet, outlet, wall, sym], dimension=3)
+
+
+# ----------------------------------------------------------------------------
+# decks
+# ----------------------------------------------------------------------------
+
+def _fmt(v: float) -> str:
+    return repr(float(v))
+
+
+def _vec(v) -> str:
+    return "[" + ",".join(_fmt(x) for x in v) + "]"
+
+
+def _air_mat(mu_ref: float, t_ref: float = 273.15, s: float = 110.4, pr: float = 0.72) -> str:
+    return (
+        f"molar mass={_fmt(MW_AIR)};\n"
+        "gamma=1.4;\n"
+        "equation of state { model=ideal gas; }\n"
+        "viscosity {\n model=sutherlands;\n"
+        f" reference viscosity={_fmt(mu_ref)};\n"
+        f" reference temperature={_fmt(t_ref)};\n"
+        f" sutherland temperature={_fmt(s)};\n}}\n"
+        f"thermal conductivity {{\n model=constant Prandtl;\n Pr={_fmt(pr)};\n}}\n"
+    )
+
+
+def _sutherland_ref(mu_at_t: float, t: float, t_ref: float = 273.15, s: float = 110.4) -> float:
+    return mu_at_t / (((t / t_ref) ** 1.5) * (t_ref + s) / (t + s))
+
+
+def seeded_state(n_cells: int, free: tuple, seed: int, amp: float = 0.01) -> np.ndarray:
+    """Freestream times (1 + amp*U(-1,1)) per component and cell (seeded)."""
+    rng = np.random.default_rng(seed)
+    base = np.asarray(free, dtype=np.float64)[None, :]
+    return base * (1.0 + amp * rng.uniform(-1.0, 1.0, size=(n_cells, 5)))
+
+
+def wedge_case(ni=120, nj=60, seed=1234, flux="Roe", limiter="vk", threshold=1.0,
+               order="second") -> Case:
+    mesh = wedge_mesh(ni, nj)
+    p, T, M = 101325.0, 300.0, 2.5
+    a = math.sqrt(1.4 * R_AIR * T)
+    U = M * a
+    deck = f"""// Euler wedge/ramp {ni}x{nj}x1, M={M}
+reference {{Mach={_fmt(M)}; p=0.; T=0.;}}
+time marching {{ CFLmax=120.; number of steps=500; ramp (initial=5.0; growth=1.1;); }}
+grid_1 {{
+ file=wedge.cgns;
+ dimension=2;
+ equations=navier stokes;
+ material (viscosity=0.; molar mass={_fmt(MW_AIR)}; gamma=1.4;);
+ gradients (hex method=lsqr; prism method=lsqr;);
+ navier stokes (limiter={limiter}; limiter threshold={_fmt(threshold)}; order={order}; convective flux={flux};);
+ write output ( volume variables=[V,p,T]; surface variables=[p]; );
+ IC_1 (p={_fmt(p)}; T={_fmt(T)}; V={_vec((U, 0.0, 0.0))};);
+ BC_1 (type=inlet; p={_fmt(p)}; T={_fmt(T)}; V={_vec((U, 0.0, 0.0))};);
+ BC_2 (type=outlet;);
+ BC_3 (type=symmetry;);
+ BC_4 (type=wall; kind=slip;);
+}}
+"""
+    free = (p, U, 0.0, 0.0, T)
+    st = seeded_state(mesh.n_cells, free, seed)
+    return Case("wedge", mesh, deck, {}, st, free,
+                f"euler_wedge_{ni}x{nj}x1_hex_roe_lsq_vk")
+
+
+def cylinder_case(ntheta=256, nr=128, seed=1234, flux="Roe", limiter="vk",
+                  threshold=1.0, r1=15.0, dr0=1e-3) -> Case:
+    mesh = cylinder_mesh(ntheta, nr, r1=r1, dr0=dr0)
+    p, T, M, Re, D = 101325.0, 300.0, 0.2, 40.0, 1.0
+    a = math.sqrt(1.4 * R_AIR * T)
+    U = M * a
+    rho = p / (R_AIR * T)
+    mu = rho * U * D / Re
+    mat = _air_mat(_sutherland_ref(mu, T))
+    deck = f"""// Laminar cylinder O-grid {ntheta}x{nr}x1, M={M}, Re_D={Re}
+reference {{Mach={_fmt(M)}; p=0.; T=0.;}}
+time marching {{ CFLmax=50.; number of steps=500; }}
+grid_1 {{
+ file=cylinder.cgns;
+ dimension=2;
+ equations=navier stokes;
+ material=air;
+ gradients (hex method=lsqr; prism method=lsqr;);
+ navier stokes (limiter={limiter}; limiter threshold={_fmt(threshold)}; convective flux={flux};);
+ write output ( volume variables=[V,p,T]; surface variables=[p]; load frequency=1; include bcs=[1]; );
+ IC_1 (rho={_fmt(rho)}; V={_vec((U, 0.0, 0.0))}; p={_fmt(p)};);
+ BC_1 (type=wall;);
+ BC_2 (type=inlet; rho={_fmt(rho)}; V={_vec((U, 0.0, 0.0))};);
+ BC_3 (type=outlet; p={_fmt(p)};);
+ BC_4 (type=symmetry;);
+}}
+"""
+    free = (p, U, 0.0, 0.0, T)
+    st = seeded_state(mesh.n_cells, free, seed)
+    return Case("cylinder", mesh, deck, {"air": mat}, st, free,
+                f"laminar_cylinder_{ntheta}x{nr}x1_hex_roe_viscous")
+
+
+def hypersonic_case(ntheta=512, nr=256, seed=1234, flux="AUSM+up", limiter="minmod",
+                    r1=2.5, dr0=2e-3, jitter_seed=4321) -> Case:
+    mesh = cylinder_mesh(ntheta, nr, r1=r1, dr0=dr0 * 256.0 / nr, jitter=0.1,
+                         seed=jitter_seed, prisms=True)
+    p, T, M = 2000.0, 220.0, 8.0
+    a = math.sqrt(1.4 * R_AIR * T)
+    U = M * a
+    deck = f"""// Hypersonic cylinder O-grid {ntheta}x{nr}x1 split into prisms, M={M}
+reference {{Mach={_fmt(M)}; p=0.; T=0.;}}
+time marching {{ CFLmax=1.e3; number of steps=500; ramp (initial=0.1; growth=1.1;); }}
+grid_1 {{
+ file=cylinder.cgns;
+ dimension=2;
+ equations=navier stokes;
+ material (viscosity=0.; molar mass={_fmt(MW_AIR)}; gamma=1.4;);
+ gradients (hex method=lsqr; prism method=lsqr;);
+ navier stokes (limiter={limiter}; convective flux={flux};);
+ write output ( volume variables=[V,p,T]; surface variables=[p]; );
+ IC_1 (p={_fmt(p)}; T={_fmt(T)}; V={_vec((U, 0.0, 0.0))};);
+ BC_1 (type=wall; kind=slip;);
+ BC_2 (type=inlet; p={_fmt(p)}; T={_fmt(T)}; V={_vec((U, 0.0, 0.0))};);
+ BC_3 (type=outlet;);
+ BC_4 (type=symmetry;);
+}}
+"""
+    free = (p, U, 0.0, 0.0, T)
+    st = seeded_state(mesh.n_cells, free, seed)
+    return Case("hypersonic", mesh, deck, {}, st, free,
+                f"hypersonic_cylinder_{ntheta}x{nr}x1_prism_ausm_minmod")
+
+
+def plate_case(ni=384, nj=192, nk=4, seed=1234, flux="Roe", limiter="vk",
+               threshold=1.0, turbulent=True) -> Case:
+    L, ReL = 2.0, 5e6
+    p, T, M = 101325.0, 300.0, 0.2
+    a = math.sqrt(1.4 * R_AIR * T)
+    U = M * a
+    rho = p / (R_AIR * T)
+    mu = rho * U * L / ReL
+    cf = 0.0576 * ReL ** -0.2
+    utau = U * math.sqrt(cf / 2.0)
+    y1 = mu / rho / utau
+    mesh = plate_mesh(ni, nj, nk, plate=L, y1=y1 * 192.0 / nj)
+    mat = _air_mat(_sutherland_ref(mu, T))
+    turb = (" turbulence (model=k-omega;);\n" if turbulent else "")
+    tin = " turbulence intensity=1.e-3; eddy viscosity ratio=1.;" if turbulent else ""
+    deck = f"""// Turbulent flat plate {ni}x{nj}x{nk}, M={M}, Re_L={ReL}
+reference {{Mach={_fmt(M)}; p=0.; T=0.;}}
+time marching {{ CFLmax=50.; number of steps=500; }}
+grid_1 {{
+ file=plate.cgns;
+ dimension=3;
+ equations=navier stokes;
+ material=air;
+ gradients (hex method=lsqr; prism method=lsqr;);
+{turb} navier stokes (limiter={limiter}; limiter threshold={_fmt(threshold)}; convective flux={flux};);
+ write output ( volume variables=[V,p,T]; surface variables=[p]; );
+ IC_1 (rho={_fmt(rho)}; V={_vec((U, 0.0, 0.0))}; p={_fmt(p)};{tin});
+ BC_1 (type=inlet; rho={_fmt(rho)}; V={_vec((U, 0.0, 0.0))};{tin});
+ BC_2 (type=outlet; p={_fmt(p)};);
+ BC_3 (type=wall;);
+ BC_4 (type=symmetry;);
+}}
+"""
+    free = (p, U, 0.0, 0.0, T)
+    st = seeded_state(mesh.n_cells, free, seed)
+    return Case("plate", mesh, deck, {"air": mat}, st, free,
+                f"rans_flat_plate_{ni}x{nj}x{nk}_hex_roe_viscous_komega")
+
+
+CONFIGS = {
+    "wedge": wedge_case,
+    "cylinder": cylinder_case,
+    "hypersonic": hypersonic_case,
+    "plate": plate_case,
+}

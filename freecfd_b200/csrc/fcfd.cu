@@ -1,0 +1,434 @@
+// C ABI, device context and residual pipeline of libfcfd_b200.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "internal.hpp"
+#include "kernels.cuh"
+
+namespace fcfd {
+
+fcfd_case *read_deck(const std::string &path);
+fcfd_mesh *build_mesh(const fcfd_raw_mesh &raw, fcfd_case &cs);
+
+static thread_local std::string g_last_error;
+void set_last_error(const std::string &m) { g_last_error = m; }
+
+#define CK(call)                                                                                        \
+  do {                                                                                                  \
+    cudaError_t e_ = (call);                                                                            \
+    if (e_ != cudaSuccess) throw Error(FCFD_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+template <class T>
+struct DBuf {
+  T *p = nullptr;
+  size_t n = 0;
+  void alloc(size_t count) {
+    free();
+    n = count;
+    if (count) CK(cudaMalloc(&p, count * sizeof(T)));
+  }
+  void upload(const std::vector<T> &v) {
+    alloc(v.size());
+    if (n) CK(cudaMemcpy(p, v.data(), n * sizeof(T), cudaMemcpyHostToDevice));
+  }
+  void free() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  ~DBuf() { free(); }
+};
+
+// [n][k] AoS host array -> [k][n] SoA
+template <class T>
+static std::vector<T> soa(const std::vector<T> &a, size_t n, int k) {
+  std::vector<T> o(a.size());
+  for (size_t i = 0; i < n; ++i)
+    for (int j = 0; j < k; ++j) o[j * n + i] = a[i * k + j];
+  return o;
+}
+
+struct Timing {
+  cudaEvent_t ev[8];
+  Timing() { for (auto &e : ev) cudaEventCreate(&e); }
+  ~Timing() { for (auto &e : ev) cudaEventDestroy(e); }
+};
+
+}  // namespace fcfd
+
+using namespace fcfd;
+
+struct fcfd_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  DevCase cs{};
+  DevMesh dm{};
+  const fcfd_mesh *mesh = nullptr;
+  bool viscous = false;
+  // mesh arrays
+  DBuf<int> f_parent, f_neighbor, f_bc, cf_index, cf_list, st_index, st_keys, bface, outlet;
+  DBuf<double> f_n, f_area, f_x, f_w, c_x, c_len, st_cof, st_self;
+  // state arrays
+  DBuf<double> W, G, Lm, D, stale, R, Win, dt, mdot, wl;
+  DBuf<unsigned long long> ext;
+  DBuf<int> err;
+  DBuf<unsigned char> flush;
+  int n_outlet = 0;
+  cudaGraphExec_t graph = nullptr;
+};
+
+namespace fcfd {
+
+static void launch_residual(fcfd_ctx *x, const double *Wsoa_ready, double *Rout, bool aos_out, bool want_aux) {
+  const DevMesh &m = x->dm;
+  cudaStream_t s = x->stream;
+  (void)Wsoa_ready;
+  const int tb = 256;
+  // extrema slots: even = max (start at key 0), odd = min (start at all ones)
+  CK(cudaMemsetAsync(x->ext.p, 0x00, 8 * sizeof(unsigned long long), s));
+  for (int k = 1; k < 8; k += 2) CK(cudaMemsetAsync(x->ext.p + k, 0xFF, sizeof(unsigned long long), s));
+  int ng = (m.nb + tb - 1) / tb;
+  if (ng < 296) ng = 296;
+  k_ghost_minmax<double><<<ng, tb, 0, s>>>(x->cs, m, x->W.p, x->ext.p, x->err.p);
+  k_grad_limiter<double><<<(m.nc + 127) / 128, 128, 0, s>>>(x->cs, m, x->W.p, x->ext.p, x->G.p, x->Lm.p);
+  if (m.n_outlet > 0)
+    k_outlet_rho<double><<<(m.n_outlet + 127) / 128, 128, 0, s>>>(x->cs, m, x->W.p, x->G.p, x->Lm.p, x->stale.p);
+  double *mo = want_aux ? x->mdot.p : nullptr;
+  double *wo = want_aux ? x->wl.p : nullptr;
+  if (x->viscous)
+    k_face_flux<double, true><<<(m.nf + 127) / 128, 128, 0, s>>>(x->cs, m, x->W.p, x->G.p, x->Lm.p, x->stale.p, nullptr, x->D.p, mo, wo, x->err.p);
+  else
+    k_face_flux<double, false><<<(m.nf + 127) / 128, 128, 0, s>>>(x->cs, m, x->W.p, x->G.p, x->Lm.p, x->stale.p, nullptr, x->D.p, mo, wo, x->err.p);
+  if (aos_out)
+    k_gather<double, true><<<(m.nc + tb - 1) / tb, tb, 0, s>>>(m, x->D.p, Rout);
+  else
+    k_gather<double, false><<<(m.nc + tb - 1) / tb, tb, 0, s>>>(m, x->D.p, Rout);
+  CK(cudaGetLastError());
+}
+
+static int check_err(fcfd_ctx *x) {
+  int h = 0;
+  CK(cudaMemcpyAsync(&h, x->err.p, sizeof(int), cudaMemcpyDeviceToHost, x->stream));
+  CK(cudaStreamSynchronize(x->stream));
+  if (h) {
+    CK(cudaMemsetAsync(x->err.p, 0, sizeof(int), x->stream));
+    if (h & ERR_SUPERSONIC_INLET) throw Error(FCFD_ERR_BC, "an inlet became supersonic; the thermodynamic state must be specified");
+    throw Error(FCFD_ERR_BC, "invalid boundary condition specification");
+  }
+  return 0;
+}
+
+}  // namespace fcfd
+
+#define API_BEGIN try {
+#define API_END                                  \
+  }                                              \
+  catch (const fcfd::Error &e) {                 \
+    fcfd::set_last_error(e.what());              \
+    return e.code;                               \
+  }                                              \
+  catch (const std::exception &e) {              \
+    fcfd::set_last_error(e.what());              \
+    return FCFD_ERR_INPUT;                       \
+  }                                              \
+  return FCFD_OK;
+
+extern "C" {
+
+const char *fcfd_last_error(void) { return g_last_error.c_str(); }
+const char *fcfd_version(void) { return "fcfd_b200 0.1 (sm_100a)"; }
+
+int fcfd_case_from_deck(const char *deck_path, fcfd_case **out) {
+  API_BEGIN
+  if (!deck_path || !out) throw Error(FCFD_ERR_INPUT, "null argument");
+  *out = read_deck(deck_path);
+  API_END
+}
+
+void fcfd_case_destroy(fcfd_case *cs) { delete cs; }
+
+int fcfd_case_summary(const fcfd_case *cs, double *dv, int32_t *iv, int32_t iv_len) {
+  API_BEGIN
+  const Material &m = cs->mat;
+  double d[13] = {m.gamma, m.R, m.Pref, m.Tref, cs->Minf, cs->limiter_threshold, m.mu, m.lambda,
+                  m.sut_mu_ref, m.sut_T_ref, m.sut_S, m.Pr, 0.};
+  std::memcpy(dv, d, sizeof(d));
+  int need = 7 + 4 * (int)cs->bc.size();
+  if (iv_len < need) throw Error(FCFD_ERR_INPUT, "iv too small");
+  iv[0] = cs->flux; iv[1] = cs->limiter; iv[2] = cs->order; iv[3] = m.sutherland; iv[4] = m.prandtl;
+  iv[5] = (int)cs->bc.size(); iv[6] = cs->dimension;
+  for (size_t b = 0; b < cs->bc.size(); ++b) {
+    iv[7 + 4 * b] = cs->bc[b].type; iv[8 + 4 * b] = cs->bc[b].kind;
+    iv[9 + 4 * b] = cs->bc[b].specified; iv[10 + 4 * b] = cs->bc[b].thermal;
+  }
+  API_END
+}
+
+int fcfd_mesh_create(const fcfd_raw_mesh *raw, const fcfd_case *cs, fcfd_mesh **out) {
+  API_BEGIN
+  if (!raw || !cs || !out) throw Error(FCFD_ERR_INPUT, "null argument");
+  fcfd_case copy = *cs;
+  *out = build_mesh(*raw, copy);
+  API_END
+}
+
+void fcfd_mesh_destroy(fcfd_mesh *m) { delete m; }
+
+int fcfd_mesh_sizes(const fcfd_mesh *m, int64_t *out) {
+  API_BEGIN
+  out[0] = m->nc; out[1] = m->nf; out[2] = m->nb; out[3] = m->nc + m->nb; out[4] = m->nnode;
+  out[5] = (int64_t)m->st_keys.size(); out[6] = (int64_t)m->cf_list.size(); out[7] = (int64_t)m->nbr_list.size();
+  API_END
+}
+
+int fcfd_mesh_connectivity(const fcfd_mesh *m, int32_t *face_parent, int32_t *face_neighbor, int32_t *face_bc,
+                           int32_t *face_nodes, int32_t *cell_face_index, int32_t *cell_faces, int32_t *nbr_index,
+                           int32_t *nbrs, int32_t *grad_index, int32_t *grad_keys) {
+  API_BEGIN
+  auto cp = [](int32_t *dst, const std::vector<int32_t> &v) { if (dst && !v.empty()) std::memcpy(dst, v.data(), v.size() * 4); };
+  cp(face_parent, m->f_parent); cp(face_neighbor, m->f_neighbor); cp(face_bc, m->f_bc); cp(face_nodes, m->f_nodes);
+  cp(cell_face_index, m->cf_index); cp(cell_faces, m->cf_list); cp(nbr_index, m->nbr_index); cp(nbrs, m->nbr_list);
+  cp(grad_index, m->st_index); cp(grad_keys, m->st_keys);
+  API_END
+}
+
+int fcfd_mesh_geometry(const fcfd_mesh *m, double *face_normal, double *face_area, double *face_centroid,
+                       double *face_avg, double *cell_centroid, double *cell_volume, double *cell_length,
+                       double *cell_wall_distance, double *length_scale) {
+  API_BEGIN
+  auto cp = [](double *dst, const std::vector<double> &v) { if (dst && !v.empty()) std::memcpy(dst, v.data(), v.size() * 8); };
+  cp(face_normal, m->f_normal); cp(face_area, m->f_area); cp(face_centroid, m->f_centroid); cp(face_avg, m->f_w);
+  cp(cell_centroid, m->c_centroid); cp(cell_volume, m->c_volume); cp(cell_length, m->c_length); cp(cell_wall_distance, m->c_wall);
+  if (length_scale) *length_scale = m->length_scale;
+  API_END
+}
+
+int fcfd_mesh_lsq(const fcfd_mesh *m, double *cofactors, double *self_weight) {
+  API_BEGIN
+  if (cofactors) std::memcpy(cofactors, m->st_cof.data(), m->st_cof.size() * 8);
+  if (self_weight) std::memcpy(self_weight, m->st_self.data(), m->st_self.size() * 8);
+  API_END
+}
+
+int fcfd_ctx_create(const fcfd_mesh *mp, const fcfd_case *csp, int device, fcfd_ctx **out) {
+  API_BEGIN
+  if (!mp || !csp || !out) throw Error(FCFD_ERR_INPUT, "null argument");
+  const fcfd_mesh &m = *mp;
+  const fcfd_case &c = *csp;
+  if ((int)c.bc.size() > kMaxBC) throw Error(FCFD_ERR_UNSUPPORTED, "more than 16 boundary regions");
+  for (const BcRegion &b : c.bc)
+    if (b.type == BC_OUTLET && b.specified == SP_STATE)
+      throw Error(FCFD_ERR_INPUT, "you can't specify complete thermodynamic state at an outlet");
+  std::unique_ptr<fcfd_ctx> x(new fcfd_ctx());
+  x->device = device;
+  CK(cudaSetDevice(device));
+  CK(cudaStreamCreateWithFlags(&x->stream, cudaStreamNonBlocking));
+  x->mesh = mp;
+  DevCase &d = x->cs;
+  const Material &mt = c.mat;
+  d.gamma = mt.gamma; d.R = mt.R; d.Pref = mt.Pref; d.Tref = mt.Tref; d.Minf = c.Minf; d.K = c.limiter_threshold;
+  d.Lref = m.length_scale; d.Cp = mt.Cp(); d.mu = mt.mu; d.lambda = mt.lambda; d.sut_mu_ref = mt.sut_mu_ref;
+  d.sut_T_ref = mt.sut_T_ref; d.sut_S = mt.sut_S; d.Pr = mt.Pr; d.Pr_t = c.Pr_t; d.sutherland = mt.sutherland;
+  d.prandtl = mt.prandtl; d.flux = c.flux; d.limiter = c.limiter; d.order = c.order; d.nbc = (int)c.bc.size();
+  bool fixed_q = false;
+  for (size_t b = 0; b < c.bc.size(); ++b) {
+    const BcRegion &r = c.bc[b];
+    DevBC &o = d.bc[b];
+    o.type = r.type; o.kind = r.kind; o.specified = r.specified; o.thermal = r.thermal;
+    o.p = r.p; o.T = r.T; o.rho = r.rho; o.qdot = r.qdot; o.p_total = r.p_total; o.T_total = r.T_total;
+    o.mdot_per_area = r.mdot / m.bc_total_area[b];
+    for (int k = 0; k < 3; ++k) o.V[k] = r.V[k];
+    if (r.thermal == TH_FIXED_Q && r.type == BC_WALL) fixed_q = true;
+  }
+  x->viscous = mt.sutherland || mt.prandtl || mt.mu != 0. || mt.lambda != 0. || fixed_q;
+  d.viscous = x->viscous;
+  // ---- mesh upload (SoA)
+  const int nc = m.nc, nf = m.nf, nb = m.nb, nt = nc + nb;
+  x->f_parent.upload(m.f_parent); x->f_neighbor.upload(m.f_neighbor); x->f_bc.upload(m.f_bc);
+  x->f_n.upload(soa(m.f_normal, nf, 3)); x->f_area.upload(m.f_area); x->f_x.upload(soa(m.f_centroid, nf, 3));
+  x->f_w.upload(soa(m.f_w, nf, 2)); x->c_x.upload(soa(m.c_centroid, nt, 3));
+  std::vector<double> clen(m.c_length.begin(), m.c_length.begin() + nc);
+  x->c_len.upload(clen);
+  x->cf_index.upload(m.cf_index);
+  std::vector<int32_t> cfl(m.cf_list.size());
+  for (int cc = 0; cc < nc; ++cc)
+    for (int j = m.cf_index[cc]; j < m.cf_index[cc + 1]; ++j) {
+      int f = m.cf_list[j];
+      cfl[j] = (m.f_parent[f] == cc) ? f : ~f;
+    }
+  x->cf_list.upload(cfl);
+  x->st_index.upload(m.st_index); x->st_keys.upload(m.st_keys);
+  x->st_cof.upload(soa(m.st_cof, nc, 7)); x->st_self.upload(soa(m.st_self, nc, 3));
+  std::vector<int32_t> bface(nb), outl;
+  for (int f = 0; f < nf; ++f) {
+    if (m.f_bc[f] >= 0) {
+      bface[m.f_neighbor[f] - nc] = f;
+      if (c.bc[m.f_bc[f]].type == BC_OUTLET) outl.push_back(f);
+    }
+  }
+  x->bface.upload(bface);
+  x->outlet.upload(outl);
+  x->n_outlet = (int)outl.size();
+  // ---- state buffers
+  x->W.alloc(5 * (size_t)nt); x->G.alloc(15 * (size_t)nc); x->Lm.alloc(5 * (size_t)nc); x->D.alloc(5 * (size_t)nf);
+  x->stale.alloc(nb > 0 ? nb : 1); x->R.alloc(5 * (size_t)nc); x->Win.alloc(5 * (size_t)nc); x->dt.alloc(nc);
+  x->mdot.alloc(nf); x->wl.alloc(nf); x->ext.alloc(8); x->err.alloc(1);
+  CK(cudaMemset(x->err.p, 0, sizeof(int)));
+  CK(cudaMemset(x->stale.p, 0, sizeof(double) * (nb > 0 ? nb : 1)));
+  DevMesh &dm = x->dm;
+  dm.nc = nc; dm.nf = nf; dm.nb = nb; dm.nt = nt;
+  dm.f_parent = x->f_parent.p; dm.f_neighbor = x->f_neighbor.p; dm.f_bc = x->f_bc.p;
+  dm.f_n = x->f_n.p; dm.f_area = x->f_area.p; dm.f_x = x->f_x.p; dm.f_w = x->f_w.p; dm.c_x = x->c_x.p;
+  dm.c_len = x->c_len.p; dm.cf_index = x->cf_index.p; dm.cf_list = x->cf_list.p; dm.st_index = x->st_index.p;
+  dm.st_keys = x->st_keys.p; dm.st_cof = x->st_cof.p; dm.st_self = x->st_self.p; dm.bface = x->bface.p;
+  dm.outlet_faces = x->outlet.p; dm.n_outlet = x->n_outlet;
+  CK(cudaDeviceSynchronize());
+  *out = x.release();
+  API_END
+}
+
+void fcfd_ctx_destroy(fcfd_ctx *x) {
+  if (!x) return;
+  cudaSetDevice(x->device);
+  if (x->graph) cudaGraphExecDestroy(x->graph);
+  if (x->stream) cudaStreamDestroy(x->stream);
+  delete x;
+}
+
+int fcfd_residual(fcfd_ctx *x, const double *W, double *R, int flags) {
+  API_BEGIN
+  if (!x || !W || !R) throw Error(FCFD_ERR_INPUT, "null argument");
+  CK(cudaSetDevice(x->device));
+  const DevMesh &m = x->dm;
+  const bool dev = flags & FCFD_DEVICE_PTRS;
+  const double *win = W;
+  if (!dev) {
+    CK(cudaMemcpyAsync(x->Win.p, W, sizeof(double) * 5 * m.nc, cudaMemcpyHostToDevice, x->stream));
+    win = x->Win.p;
+  }
+  k_aos_to_soa<double><<<(m.nc + 255) / 256, 256, 0, x->stream>>>(win, x->W.p, m.nc, m.nt);
+  double *rout = dev ? R : x->R.p;
+  launch_residual(x, x->W.p, rout, true, true);
+  if (!dev) CK(cudaMemcpyAsync(R, x->R.p, sizeof(double) * 5 * m.nc, cudaMemcpyDeviceToHost, x->stream));
+  check_err(x);
+  API_END
+}
+
+int fcfd_last_stages(fcfd_ctx *x, double *grads, double *limiter, double *ghost, double *mdot, double *weightL) {
+  API_BEGIN
+  CK(cudaSetDevice(x->device));
+  CK(cudaStreamSynchronize(x->stream));
+  const DevMesh &m = x->dm;
+  auto get = [&](const double *src, size_t n, int k, double *dst) {
+    if (!dst) return;
+    std::vector<double> h(n * k);
+    CK(cudaMemcpy(h.data(), src, sizeof(double) * n * k, cudaMemcpyDeviceToHost));
+    for (size_t i = 0; i < n; ++i)
+      for (int j = 0; j < k; ++j) dst[i * k + j] = h[j * n + i];
+  };
+  get(x->G.p, m.nc, 15, grads);
+  get(x->Lm.p, m.nc, 5, limiter);
+  if (ghost) {
+    std::vector<double> h(5 * (size_t)m.nt);
+    CK(cudaMemcpy(h.data(), x->W.p, sizeof(double) * 5 * m.nt, cudaMemcpyDeviceToHost));
+    for (int g = 0; g < m.nb; ++g)
+      for (int v = 0; v < 5; ++v) ghost[5 * g + v] = h[(size_t)v * m.nt + m.nc + g];
+  }
+  if (mdot) CK(cudaMemcpy(mdot, x->mdot.p, sizeof(double) * m.nf, cudaMemcpyDeviceToHost));
+  if (weightL) CK(cudaMemcpy(weightL, x->wl.p, sizeof(double) * m.nf, cudaMemcpyDeviceToHost));
+  API_END
+}
+
+int fcfd_local_dt(fcfd_ctx *x, const double *W, double cfl, int mode, double *dt, int flags) {
+  API_BEGIN
+  CK(cudaSetDevice(x->device));
+  const DevMesh &m = x->dm;
+  const bool dev = flags & FCFD_DEVICE_PTRS;
+  const double *win = W;
+  if (!dev) {
+    CK(cudaMemcpyAsync(x->Win.p, W, sizeof(double) * 5 * m.nc, cudaMemcpyHostToDevice, x->stream));
+    win = x->Win.p;
+  }
+  k_aos_to_soa<double><<<(m.nc + 255) / 256, 256, 0, x->stream>>>(win, x->W.p, m.nc, m.nt);
+  double *out = dev ? dt : x->dt.p;
+  if (mode == 1) CK(cudaMemsetAsync(x->ext.p, 0xFF, sizeof(unsigned long long), x->stream));
+  k_local_dt<double><<<(m.nc + 255) / 256, 256, 0, x->stream>>>(x->cs, m, x->W.p, out, cfl, mode == 1 ? x->ext.p : nullptr);
+  if (mode == 1) k_fill_min<double><<<(m.nc + 255) / 256, 256, 0, x->stream>>>(m.nc, out, x->ext.p);
+  CK(cudaGetLastError());
+  if (!dev) CK(cudaMemcpyAsync(dt, x->dt.p, sizeof(double) * m.nc, cudaMemcpyDeviceToHost, x->stream));
+  CK(cudaStreamSynchronize(x->stream));
+  API_END
+}
+
+// out[0] = average ms per residual (whole chain, CUDA-event timed on the
+// context stream); out[1..5] = ghost+minmax, grad+limiter, outlet density,
+// face flux, gather; out[6] = ms per residual from a CUDA-graph replay.
+int fcfd_time_residual(fcfd_ctx *x, int reps, int flush_l2, double *out, int out_len) {
+  API_BEGIN
+  CK(cudaSetDevice(x->device));
+  const DevMesh &m = x->dm;
+  cudaStream_t s = x->stream;
+  if (flush_l2 && x->flush.n == 0) x->flush.alloc((size_t)512 << 20);
+  Timing t;
+  double acc[6] = {0, 0, 0, 0, 0, 0};
+  const int tb = 256;
+  for (int r = 0; r < reps; ++r) {
+    if (flush_l2) CK(cudaMemsetAsync(x->flush.p, r & 0xff, x->flush.n, s));
+    CK(cudaMemsetAsync(x->ext.p, 0x00, 8 * sizeof(unsigned long long), s));
+    for (int k = 1; k < 8; k += 2) CK(cudaMemsetAsync(x->ext.p + k, 0xFF, sizeof(unsigned long long), s));
+    CK(cudaEventRecord(t.ev[0], s));
+    int ng = (m.nb + tb - 1) / tb;
+    if (ng < 296) ng = 296;
+    k_ghost_minmax<double><<<ng, tb, 0, s>>>(x->cs, m, x->W.p, x->ext.p, x->err.p);
+    CK(cudaEventRecord(t.ev[1], s));
+    k_grad_limiter<double><<<(m.nc + 127) / 128, 128, 0, s>>>(x->cs, m, x->W.p, x->ext.p, x->G.p, x->Lm.p);
+    CK(cudaEventRecord(t.ev[2], s));
+    if (m.n_outlet > 0)
+      k_outlet_rho<double><<<(m.n_outlet + 127) / 128, 128, 0, s>>>(x->cs, m, x->W.p, x->G.p, x->Lm.p, x->stale.p);
+    CK(cudaEventRecord(t.ev[3], s));
+    if (x->viscous)
+      k_face_flux<double, true><<<(m.nf + 127) / 128, 128, 0, s>>>(x->cs, m, x->W.p, x->G.p, x->Lm.p, x->stale.p, nullptr, x->D.p, nullptr, nullptr, x->err.p);
+    else
+      k_face_flux<double, false><<<(m.nf + 127) / 128, 128, 0, s>>>(x->cs, m, x->W.p, x->G.p, x->Lm.p, x->stale.p, nullptr, x->D.p, nullptr, nullptr, x->err.p);
+    CK(cudaEventRecord(t.ev[4], s));
+    k_gather<double, false><<<(m.nc + tb - 1) / tb, tb, 0, s>>>(m, x->D.p, x->R.p);
+    CK(cudaEventRecord(t.ev[5], s));
+    CK(cudaGetLastError());
+    CK(cudaEventSynchronize(t.ev[5]));
+    float ms;
+    CK(cudaEventElapsedTime(&ms, t.ev[0], t.ev[5])); acc[0] += ms;
+    for (int k = 0; k < 5; ++k) { CK(cudaEventElapsedTime(&ms, t.ev[k], t.ev[k + 1])); acc[k + 1] += ms; }
+  }
+  for (int k = 0; k < 6 && k < out_len; ++k) out[k] = acc[k] / reps;
+  API_END
+}
+
+int fcfd_point_flux(int flux, const double *L, const double *R, const double *n, double gamma, double gas_R, double Pref,
+                    double Tref, double Minf, double *out, double *weightL) {
+  API_BEGIN
+  DevCase c{};
+  c.gamma = gamma; c.R = gas_R; c.Pref = Pref; c.Tref = Tref; c.Minf = Minf;
+  FState<double> a{}, b{};
+  a.p = L[0]; a.V[0] = L[1]; a.V[1] = L[2]; a.V[2] = L[3]; a.T = L[4];
+  b.p = R[0]; b.V[0] = R[1]; b.V[1] = R[2]; b.V[2] = R[3]; b.T = R[4];
+  a.rho = eos_rho(c, a.p, a.T); b.rho = eos_rho(c, b.p, b.T);
+  finish(c, a, n); finish(c, b, n);
+  double F[5], wl = 0;
+  if (flux == FLUX_ROE) roe(c, a, b, n, F, wl);
+  else if (flux == FLUX_VAN_LEER) vanleer(c, a, b, n, F, wl);
+  else if (flux == FLUX_AUSM_PLUS_UP) ausm(c, a, b, n, F, wl);
+  else throw Error(FCFD_ERR_UNSUPPORTED, "unknown flux");
+  for (int k = 0; k < 5; ++k) out[k] = F[k];
+  if (weightL) *weightL = wl;
+  API_END
+}
+
+}  // extern "C"

@@ -1,0 +1,761 @@
+// Device kernels of the finite-volume residual, templated on the scalar type S.
+//
+// Data layout (all reference-order, structure-of-arrays):
+//   W[5][nt]        primitive state p,u,v,w,T of interior cells [0,nc) and
+//                   boundary ghosts [nc,nt)
+//   G[15][nc]       cell gradients (p,u,v,w,T) x (x,y,z)
+//   L[5][nc]        limiters
+//   D[5][nf]        per-face F_diffusive - F_convective
+//   R               residual, gathered per cell in ascending face order
+// Kernel chain per residual: ghost+minmax -> grad+limiter -> (outlet density)
+// -> face flux -> gather.  The chain mirrors update_boundaries,
+// calc_cell_grads, calc_limiter and the face loop of assemble_linear_system.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace fcfd {
+
+// ------------------------------------------------------------------ scalar ops
+// Parity-critical sums (LSQ gradient, limiter tests) are evaluated with
+// explicitly rounded operations so no multiply-add is contracted and the
+// result is the same double the reference computes.
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double sub_rn(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double div_rn(double a, double b) { return __ddiv_rn(a, b); }
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float sub_rn(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float div_rn(float a, float b) { return __fdiv_rn(a, b); }
+
+// std::max / std::min semantics: max(a,b) = (a<b)?b:a, min(a,b) = (b<a)?b:a
+template <class S> __host__ __device__ __forceinline__ S smax(const S &a, const S &b) { return (a < b) ? b : a; }
+template <class S> __host__ __device__ __forceinline__ S smin(const S &a, const S &b) { return (b < a) ? b : a; }
+
+// ------------------------------------------------------------------ case data
+struct DevBC {
+  int type, kind, specified, thermal;
+  double p, T, rho, qdot, mdot_per_area, p_total, T_total;
+  double V[3];
+};
+constexpr int kMaxBC = 16;
+struct DevCase {
+  double gamma, R, Pref, Tref, Minf, K, Lref, Cp;
+  double mu, lambda, sut_mu_ref, sut_T_ref, sut_S, Pr;
+  double Pr_t;
+  int sutherland, prandtl, flux, limiter, order, viscous, nbc, pad;
+  DevBC bc[kMaxBC];
+};
+
+struct DevMesh {
+  int nc, nf, nb, nt;
+  const int *f_parent, *f_neighbor, *f_bc;
+  const double *f_n, *f_area, *f_x, *f_w;  // f_n/f_x: [3][nf] SoA, f_w: [2][nf]
+  const double *c_x;                       // [3][nt]
+  const double *c_len;                     // [nc]
+  const int *cf_index, *cf_list;           // cf_list: face id, ~face id when the cell is the neighbour
+  const int *st_index, *st_keys;
+  const double *st_cof;                    // [7][nc]
+  const double *st_self;                   // [3][nc]
+  const int *bface;                        // boundary faces in ghost order [nb]
+  const int *outlet_faces;                 // outlet boundary faces [n_outlet]
+  int n_outlet;
+};
+
+enum { T_SYM = 1, T_WALL = 2, T_INLET = 3, T_OUTLET = 4 };
+enum { KN_NONE = -1, KN_NO_REVERSE = 1, KN_DAMP_REVERSE = 2, KN_VELOCITY = 3, KN_MDOT = 4, KN_SLIP = 5, KN_STAGNATION = 6,
+       KN_FORCE_SUPERSONIC = 7 };
+enum { SP_RHO_ = 1, SP_P_ = 2, SP_T_ = 3, SP_STATE_ = 4 };
+enum { TH_FIXED_T_ = 1, TH_FIXED_Q_ = 2 };
+enum { ERR_SUPERSONIC_INLET = 1, ERR_BAD_BC = 2 };
+
+// material (material/material.cc:108-153)
+template <class S> __host__ __device__ __forceinline__ S eos_rho(const DevCase &c, S p, S T) { return (p + c.Pref) / (c.R * (T + c.Tref)); }
+template <class S> __host__ __device__ __forceinline__ S eos_p(const DevCase &c, S rho, S T) { return rho * c.R * (T + c.Tref) - c.Pref; }
+template <class S> __host__ __device__ __forceinline__ S eos_T(const DevCase &c, S p, S rho) { return (p + c.Pref) / (c.R * rho) - c.Tref; }
+template <class S> __host__ __device__ __forceinline__ S sound(const DevCase &c, S p, S T) { return sqrt(c.gamma * (p + c.Pref) / eos_rho(c, p, T)); }
+template <class S> __device__ __forceinline__ S viscosity(const DevCase &c, S T) {
+  if (!c.sutherland) return S(c.mu);
+  return c.sut_mu_ref * pow((T + c.Tref) / c.sut_T_ref, 1.5) * (c.sut_T_ref + c.sut_S) / (T + c.Tref + c.sut_S);
+}
+template <class S> __device__ __forceinline__ S therm_cond(const DevCase &c, S T) {
+  if (!c.prandtl) return S(c.lambda);
+  return c.Cp * viscosity(c, T) / c.Pr;
+}
+
+// face-local state (NS_Cell_State without the rotated frame)
+template <class S>
+struct FState {
+  S p, T, rho, a, H, Vn;
+  S V[3];
+  S pc, Tc;
+  S Vc[3];
+};
+
+template <class S>
+__host__ __device__ __forceinline__ void finish(const DevCase &c, FState<S> &s, const double n[3]) {
+  s.a = sound(c, s.p, s.T);
+  s.H = s.a * s.a / (c.gamma - 1.) + 0.5 * (s.V[0] * s.V[0] + s.V[1] * s.V[1] + s.V[2] * s.V[2]);
+  s.Vn = s.V[0] * n[0] + s.V[1] * n[1] + s.V[2] * n[2];
+}
+
+// Boundary right state (ns_apply_bcs.cc:25-258).  Returns false when the
+// branch leaves R.rho untouched (outlet with everything extrapolated), in which
+// case the caller supplies the density the reference's state cache held.
+template <class S>
+__device__ bool apply_bc(const DevCase &c, const DevBC &b, const FState<S> &L, FState<S> &R, const double n[3], int *err) {
+  const double g = c.gamma;
+  const S uNL = L.V[0] * n[0] + L.V[1] * n[1] + L.V[2] * n[2];
+  bool rho_set = true;
+  if (b.type == T_INLET) {
+    if (b.kind == KN_VELOCITY) {
+      R.V[0] = S(b.V[0]); R.V[1] = S(b.V[1]); R.V[2] = S(b.V[2]);
+      S uNR = R.V[0] * n[0] + R.V[1] * n[1] + R.V[2] * n[2];
+      R.a = L.a + 0.5 * (uNL - uNR) * (g - 1.);
+      S MachL = -uNL / L.a;
+      if (MachL >= 1. && b.specified != SP_STATE_ && err) atomicOr(err, ERR_SUPERSONIC_INLET);
+      if (b.specified == SP_STATE_) { R.p = S(b.p); R.T = S(b.T); R.rho = S(b.rho); }
+      else if (b.specified == SP_P_) { R.p = S(b.p); R.rho = g * (R.p + c.Pref) / (R.a * R.a); R.T = eos_T(c, R.p, R.rho); }
+      else if (b.specified == SP_T_) {
+        R.T = S(b.T);
+        R.rho = L.rho * pow((L.T + c.Tref) / (R.T + c.Tref), 1. / (1. - g));
+        R.p = eos_p(c, R.rho, R.T);
+      } else if (b.specified == SP_RHO_) { R.rho = S(b.rho); R.p = R.a * R.a * R.rho / g - c.Pref; R.T = eos_T(c, R.p, R.rho); }
+      else if (err) atomicOr(err, ERR_BAD_BC);
+      R.pc = R.p; R.Tc = R.T; R.Vc[0] = R.V[0]; R.Vc[1] = R.V[1]; R.Vc[2] = R.V[2];
+    } else if (b.kind == KN_MDOT) {
+      const double mdotNR = -1. * b.mdot_per_area;
+      if (b.specified == SP_STATE_) { R.p = S(b.p); R.T = S(b.T); R.rho = S(b.rho); }
+      else if (b.specified == SP_P_) { R.p = S(b.p); R.T = L.T; R.rho = eos_rho(c, R.p, R.T); }
+      else if (b.specified == SP_T_) { R.T = S(b.T); R.p = L.p; R.rho = eos_rho(c, R.p, R.T); }
+      else if (b.specified == SP_RHO_) {
+        R.rho = S(b.rho);
+        R.a = 0.5 * (g - 1.) * (uNL + 2. * L.a / (g - 1.) - mdotNR / R.rho);
+        R.p = R.a * R.a * R.rho / g - c.Pref;
+        R.T = eos_T(c, R.p, R.rho);
+      } else if (err) atomicOr(err, ERR_BAD_BC);
+      S s = mdotNR / R.rho;
+      R.V[0] = s * n[0]; R.V[1] = s * n[1]; R.V[2] = s * n[2];
+      R.pc = R.p; R.Tc = R.T; R.Vc[0] = R.V[0]; R.Vc[1] = R.V[1]; R.Vc[2] = R.V[2];
+    } else if (b.kind == KN_STAGNATION) {
+      if (uNL > 0.) { R.V[0] = -1. * L.Vc[0]; R.V[1] = -1. * L.Vc[1]; R.V[2] = -1. * L.Vc[2]; }
+      else { R.V[0] = L.Vc[0]; R.V[1] = L.Vc[1]; R.V[2] = L.Vc[2]; }
+      S v2 = R.V[0] * R.V[0] + R.V[1] * R.V[1] + R.V[2] * R.V[2];
+      R.T = b.T_total - 0.5 * (g - 1.) / (g * c.R) * v2;
+      R.p = (b.p_total + c.Pref) / (1. + 0.5 * v2 / (c.R * (R.T + c.Tref))) - c.Pref;
+      R.rho = eos_rho(c, R.p, R.T);
+      R.pc = R.p; R.Tc = R.T; R.Vc[0] = R.V[0]; R.Vc[1] = R.V[1]; R.Vc[2] = R.V[2];
+    } else {
+      rho_set = false;  // inlet without V/mdot/p_total: the reference applies nothing
+    }
+  } else if (b.type == T_OUTLET) {
+    S MachL = uNL / L.a;
+    bool supersonic = (MachL > 1.);
+    const double ig = 1. / g;
+    if (b.specified == SP_P_ && !supersonic) {
+      R.p = S(b.p); R.pc = R.p;
+      R.rho = L.rho * pow((R.p + c.Pref), ig) / pow((L.p + c.Pref), ig);
+      R.a = sqrt(g * (R.p + c.Pref) / R.rho);
+      R.T = eos_T(c, R.p, R.rho);
+      R.V[0] = L.V[0]; R.V[1] = L.V[1]; R.V[2] = L.V[2];
+    } else if (b.specified == SP_T_ && !supersonic) {
+      R.T = S(b.T); R.Tc = R.T;
+      R.a = sqrt(g * c.R * (R.T + c.Tref));
+      R.rho = pow(g * (L.p + c.Pref) / (R.a * R.a * pow(L.rho, g)), 1. - g);
+      R.p = eos_p(c, R.rho, R.T);
+      R.V[0] = L.V[0]; R.V[1] = L.V[1]; R.V[2] = L.V[2];
+    } else if (b.specified == SP_RHO_ && !supersonic) {
+      R.rho = S(b.rho);
+      R.p = (L.p + c.Pref) * pow(R.rho / L.rho, g) - c.Pref;
+      R.T = eos_T(c, R.p, R.rho);
+      R.a = sqrt(g * (R.p + c.Pref) / R.rho);
+      R.V[0] = L.V[0]; R.V[1] = L.V[1]; R.V[2] = L.V[2];
+    } else {
+      R.p = L.p; R.T = L.T; R.V[0] = L.V[0]; R.V[1] = L.V[1]; R.V[2] = L.V[2];
+      rho_set = false;
+    }
+    if (MachL < 0.) {
+      if (b.kind == KN_DAMP_REVERSE) {
+        R.p = R.p - 0.5 * L.rho * uNL * uNL;
+        R.rho = L.rho * pow((R.p + c.Pref), ig) / pow((L.p + c.Pref), ig);
+        R.a = sqrt(g * (R.p + c.Pref) / R.rho);
+        R.T = eos_T(c, R.p, R.rho);
+        rho_set = true;
+      }
+      if (b.kind == KN_NO_REVERSE) { R.V[0] = -1. * L.V[0]; R.V[1] = -1. * L.V[1]; R.V[2] = -1. * L.V[2]; }
+    }
+    if (MachL < 1. && b.kind == KN_FORCE_SUPERSONIC) {
+      S d = L.a - uNL;
+      R.p = R.p - 0.5 * L.rho * (d * d);
+      R.p = smin(S(1.e-8), R.p + c.Pref) - c.Pref;
+      R.rho = L.rho * pow((R.p + c.Pref), ig) / pow((L.p + c.Pref), ig);
+      R.a = sqrt(g * (R.p + c.Pref) / R.rho);
+      R.T = eos_T(c, R.p, R.rho);
+      rho_set = true;
+    }
+  } else if (b.type == T_WALL) {
+    if (b.thermal == TH_FIXED_T_) {
+      R.T = S(b.T); R.Tc = R.T;
+      R.p = L.p;
+      R.rho = eos_rho(c, R.p, R.T);
+    } else {
+      R.p = L.p; R.rho = L.rho; R.T = L.T; R.Tc = L.Tc;
+    }
+    if (b.kind == KN_SLIP) {
+      S s = 2. * uNL;
+      R.V[0] = L.V[0] - s * n[0]; R.V[1] = L.V[1] - s * n[1]; R.V[2] = L.V[2] - s * n[2];
+      S sc = 2. * (L.Vc[0] * n[0] + L.Vc[1] * n[1] + L.Vc[2] * n[2]);
+      R.Vc[0] = L.Vc[0] - sc * n[0]; R.Vc[1] = L.Vc[1] - sc * n[1]; R.Vc[2] = L.Vc[2] - sc * n[2];
+    } else {
+      R.V[0] = -1. * L.V[0]; R.V[1] = -1. * L.V[1]; R.V[2] = -1. * L.V[2];
+      R.Vc[0] = -1. * L.Vc[0]; R.Vc[1] = -1. * L.Vc[1]; R.Vc[2] = -1. * L.Vc[2];
+    }
+    R.pc = L.pc;
+  } else if (b.type == T_SYM) {
+    R.p = L.p;
+    S s = 2. * uNL;
+    R.V[0] = L.V[0] - s * n[0]; R.V[1] = L.V[1] - s * n[1]; R.V[2] = L.V[2] - s * n[2];
+    R.T = L.T;
+    R.rho = L.rho;
+    R.pc = L.pc;
+    R.Tc = L.Tc;
+    S sc = 2. * (L.Vc[0] * n[0] + L.Vc[1] * n[1] + L.Vc[2] * n[2]);
+    R.Vc[0] = L.Vc[0] - sc * n[0]; R.Vc[1] = L.Vc[1] - sc * n[1]; R.Vc[2] = L.Vc[2] - sc * n[2];
+  } else {
+    rho_set = false;
+  }
+  return rho_set;
+}
+
+// Centre state of cell k as a face state (zero gradients).
+template <class S>
+__device__ __forceinline__ void centre_state(const DevCase &c, const S *W, int nt, int k, FState<S> &s, const double n[3]) {
+  s.p = W[k]; s.V[0] = W[nt + k]; s.V[1] = W[2 * nt + k]; s.V[2] = W[3 * nt + k]; s.T = W[4 * nt + k];
+  s.pc = s.p; s.Tc = s.T; s.Vc[0] = s.V[0]; s.Vc[1] = s.V[1]; s.Vc[2] = s.V[2];
+  s.rho = eos_rho(c, s.p, s.T);
+  finish(c, s, n);
+}
+
+// Reconstructed state of cell k at face point xf (left_state_update,
+// ns_assemble_linear_system.cc:269-294).
+template <class S>
+__device__ __forceinline__ void recon_state(const DevCase &c, const DevMesh &m, const S *W, const S *G, const S *Lm, int k,
+                                            const double xf[3], FState<S> &s, const double n[3]) {
+  const int nt = m.nt, nc = m.nc;
+  const double d0 = xf[0] - m.c_x[k], d1 = xf[1] - m.c_x[nt + k], d2 = xf[2] - m.c_x[2 * nt + k];
+  S q[5];
+#pragma unroll
+  for (int v = 0; v < 5; ++v) {
+    S dot = d0 * G[(3 * v) * nc + k] + d1 * G[(3 * v + 1) * nc + k] + d2 * G[(3 * v + 2) * nc + k];
+    q[v] = W[v * nt + k] + Lm[v * nc + k] * dot;
+  }
+  s.pc = W[k]; s.Vc[0] = W[nt + k]; s.Vc[1] = W[2 * nt + k]; s.Vc[2] = W[3 * nt + k]; s.Tc = W[4 * nt + k];
+  s.p = q[0]; s.V[0] = q[1]; s.V[1] = q[2]; s.V[2] = q[3]; s.T = q[4];
+  s.rho = eos_rho(c, s.p, s.T);
+  finish(c, s, n);
+}
+
+// ------------------------------------------------------------------ kernels
+
+// AoS [nc][5] -> SoA W[5][nt]
+template <class S>
+__global__ void k_aos_to_soa(const S *__restrict__ in, S *__restrict__ W, int nc, int nt) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nc) return;
+#pragma unroll
+  for (int v = 0; v < 5; ++v) W[v * nt + c] = in[5 * c + v];
+}
+
+__device__ __forceinline__ unsigned long long okey(double x) {
+  unsigned long long b = __double_as_longlong(x);
+  return (b >> 63) ? ~b : (b | 0x8000000000000000ull);
+}
+__device__ __forceinline__ double okey_inv(unsigned long long k) {
+  unsigned long long b = (k >> 63) ? (k & 0x7fffffffffffffffull) : ~k;
+  return __longlong_as_double(b);
+}
+
+// Ghost update (reconstructed NavierStokes::update_boundaries, first order)
+// over boundary faces, plus the global extrema that find_min_max
+// (ns.cc:400-435) needs: slots 0..7 = max p, min p, max u, min u, max v,
+// min v, max p over cells < nc-1, min p over cells < nc-1 (ordered keys).
+template <class S>
+__global__ void k_ghost_minmax(DevCase cs, DevMesh m, S *__restrict__ W, unsigned long long *__restrict__ ext, int *err) {
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nt = m.nt;
+  if (tid < m.nb) {
+    const int f = m.bface[tid];
+    const int pa = m.f_parent[f];
+    const int b = m.f_bc[f];
+    const double n[3] = {m.f_n[f], m.f_n[m.nf + f], m.f_n[2 * m.nf + f]};
+    FState<S> L, R;
+    centre_state(cs, W, nt, pa, L, n);
+    R.rho = S(0.);
+    apply_bc(cs, cs.bc[b], L, R, n, err);
+    const int g = m.nc + tid;
+    W[g] = R.p; W[nt + g] = R.V[0]; W[2 * nt + g] = R.V[1]; W[3 * nt + g] = R.V[2]; W[4 * nt + g] = R.T;
+  }
+  if (ext) {
+    // grid-stride extrema over interior cells, warp-reduced then one atomic per warp
+    double mx[4] = {-INFINITY, -INFINITY, -INFINITY, -INFINITY}, mn[4] = {INFINITY, INFINITY, INFINITY, INFINITY};
+    for (int c = tid; c < m.nc; c += gridDim.x * blockDim.x) {
+      double p = (double)W[c], u = (double)W[nt + c], v = (double)W[2 * nt + c];
+      mx[0] = fmax(mx[0], p); mn[0] = fmin(mn[0], p);
+      mx[1] = fmax(mx[1], u); mn[1] = fmin(mn[1], u);
+      mx[2] = fmax(mx[2], v); mn[2] = fmin(mn[2], v);
+      if (c < m.nc - 1) { mx[3] = fmax(mx[3], p); mn[3] = fmin(mn[3], p); }
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      for (int o = 16; o > 0; o >>= 1) {
+        mx[i] = fmax(mx[i], __shfl_xor_sync(0xffffffffu, mx[i], o));
+        mn[i] = fmin(mn[i], __shfl_xor_sync(0xffffffffu, mn[i], o));
+      }
+    }
+    if ((threadIdx.x & 31) == 0) {
+      const int slot_max[4] = {0, 2, 4, 6}, slot_min[4] = {1, 3, 5, 7};
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        if (mx[i] != -INFINITY) atomicMax(&ext[slot_max[i]], okey(mx[i]));
+        if (mn[i] != INFINITY) atomicMin(&ext[slot_min[i]], okey(mn[i]));
+      }
+    }
+  }
+}
+
+// LSQ gradient (bit-exact restatement of Variable::cell_gradient over the
+// lsqr_grad_map weights) + limiter, one thread per interior cell.
+template <class S>
+__global__ void __launch_bounds__(128) k_grad_limiter(DevCase cs, DevMesh m, const S *__restrict__ W,
+                                                      const unsigned long long *__restrict__ ext, S *__restrict__ G,
+                                                      S *__restrict__ Lm) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nc = m.nc, nt = m.nt;
+  if (c >= nc) return;
+  const double xc0 = m.c_x[c], xc1 = m.c_x[nt + c], xc2 = m.c_x[2 * nt + c];
+  const double C00 = m.st_cof[c], C01 = m.st_cof[nc + c], C02 = m.st_cof[2 * nc + c];
+  const double C11 = m.st_cof[3 * nc + c], C12 = m.st_cof[4 * nc + c], C22 = m.st_cof[5 * nc + c];
+  const double det = m.st_cof[6 * nc + c];
+  S g[15];
+#pragma unroll
+  for (int i = 0; i < 15; ++i) g[i] = S(0.);
+  const int j0 = m.st_index[c], j1 = m.st_index[c + 1];
+  for (int j = j0; j < j1; ++j) {
+    const int k = m.st_keys[j];
+    double wt0, wt1, wt2;
+    if (k == c) {
+      wt0 = m.st_self[c]; wt1 = m.st_self[nc + c]; wt2 = m.st_self[2 * nc + c];
+    } else {
+      const double d0 = sub_rn(m.c_x[k], xc0), d1 = sub_rn(m.c_x[nt + k], xc1), d2 = sub_rn(m.c_x[2 * nt + k], xc2);
+      const double w = add_rn(add_rn(mul_rn(d0, d0), mul_rn(d1, d1)), mul_rn(d2, d2));
+      wt0 = div_rn(mul_rn(w, add_rn(add_rn(mul_rn(d0, C00), mul_rn(d1, C01)), mul_rn(d2, C02))), det);
+      wt1 = div_rn(mul_rn(w, add_rn(add_rn(mul_rn(d0, C01), mul_rn(d1, C11)), mul_rn(d2, C12))), det);
+      wt2 = div_rn(mul_rn(w, add_rn(add_rn(mul_rn(d0, C02), mul_rn(d1, C12)), mul_rn(d2, C22))), det);
+    }
+#pragma unroll
+    for (int v = 0; v < 5; ++v) {
+      const S phi = W[v * nt + k];
+      g[3 * v] = add_rn(g[3 * v], mul_rn(S(wt0), phi));
+      g[3 * v + 1] = add_rn(g[3 * v + 1], mul_rn(S(wt1), phi));
+      g[3 * v + 2] = add_rn(g[3 * v + 2], mul_rn(S(wt2), phi));
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < 15; ++i) G[i * nc + c] = g[i];
+
+  // ---- limiter (ns_limiters.cc)
+  S phi[5];
+  const S one = S(cs.order == 1 ? 0. : 1.);
+#pragma unroll
+  for (int v = 0; v < 5; ++v) phi[v] = one;
+  if (cs.order != 1 && cs.limiter > 0) {
+    const int f0 = m.cf_index[c], f1 = m.cf_index[c + 1];
+    S u0[5];
+#pragma unroll
+    for (int v = 0; v < 5; ++v) { u0[v] = W[v * nt + c]; phi[v] = S(1.); }
+    if (cs.limiter == 3) {
+      // minmod (ns_limiters.cc:45-92)
+      const double small = 1.e-12;
+      for (int j = f0; j < f1; ++j) {
+        const int e = m.cf_list[j];
+        const int f = e >= 0 ? e : ~e;
+        const int nb = e >= 0 ? m.f_neighbor[f] : m.f_parent[f];
+        const double cf0 = sub_rn(m.f_x[f], xc0), cf1 = sub_rn(m.f_x[m.nf + f], xc1), cf2 = sub_rn(m.f_x[2 * m.nf + f], xc2);
+#pragma unroll
+        for (int v = 0; v < 5; ++v) {
+          S dU = sub_rn(W[v * nt + nb], u0[v]);
+          S dUg = add_rn(add_rn(mul_rn(g[3 * v], S(cf0)), mul_rn(g[3 * v + 1], S(cf1))), mul_rn(g[3 * v + 2], S(cf2)));
+          S mm;
+          if (dU * dUg < 0.) mm = S(0.);
+          else if (dU > 0.) mm = smin(dU, dUg);
+          else mm = smax(dU, dUg);
+          const double sU = (double)((mm > 0.) - (mm < 0.)), sG = (double)((dUg > 0.) - (dUg < 0.));
+          S r = div_rn(add_rn(mm, S(sU * small)), add_rn(dUg, S(sG * small)));
+          phi[v] = smin(phi[v], r);
+        }
+      }
+    } else {
+      // Venkatakrishnan (ns_limiters.cc:161-248) and Barth-Jespersen (94-159)
+      S umax[5], umin[5];
+#pragma unroll
+      for (int v = 0; v < 5; ++v) umax[v] = umin[v] = u0[v];
+      for (int j = f0; j < f1; ++j) {
+        const int e = m.cf_list[j];
+        const int f = e >= 0 ? e : ~e;
+        const int nb = e >= 0 ? m.f_neighbor[f] : m.f_parent[f];
+#pragma unroll
+        for (int v = 0; v < 5; ++v) {
+          const S x = W[v * nt + nb];
+          umax[v] = smax(umax[v], x);
+          umin[v] = smin(umin[v], x);
+        }
+      }
+      double eps2[5] = {0, 0, 0, 0, 0};
+      if (cs.limiter == 1) {
+        // find_min_max with its index quirks: q[3] uses q[4]'s running value,
+        // q[4] tracks p starting from T of cell 0
+        const double pmax = okey_inv(ext[0]), pmin = okey_inv(ext[1]);
+        const double T0 = (double)W[4 * nt + 0], wl = (double)W[3 * nt + nc - 1];
+        double qmax[5], qmin[5];
+        qmax[0] = pmax; qmin[0] = pmin;
+        qmax[1] = okey_inv(ext[2]); qmin[1] = okey_inv(ext[3]);
+        qmax[2] = okey_inv(ext[4]); qmin[2] = okey_inv(ext[5]);
+        double pmax_lt = nc > 1 ? okey_inv(ext[6]) : -INFINITY, pmin_lt = nc > 1 ? okey_inv(ext[7]) : INFINITY;
+        double q4max_prev = T0, q4min_prev = T0;
+        if (nc > 1) { q4max_prev = smax(T0, pmax_lt); q4min_prev = smin(T0, pmin_lt); }
+        qmax[3] = smax(q4max_prev, wl);
+        qmin[3] = smin(q4min_prev, wl);
+        qmax[4] = smax(T0, pmax); qmin[4] = smin(T0, pmin);
+#pragma unroll
+        for (int v = 0; v < 5; ++v) {
+          const double eps = fabs(qmax[v] - qmin[v]) / cs.Lref;
+          const double e = 1.e-6 * cs.K * eps;
+          eps2[v] = e * e;
+        }
+      }
+      for (int j = f0; j < f1; ++j) {
+        const int e = m.cf_list[j];
+        const int f = e >= 0 ? e : ~e;
+        const double cf0 = sub_rn(m.f_x[f], xc0), cf1 = sub_rn(m.f_x[m.nf + f], xc1), cf2 = sub_rn(m.f_x[2 * m.nf + f], xc2);
+#pragma unroll
+        for (int v = 0; v < 5; ++v) {
+          S dM = add_rn(add_rn(mul_rn(g[3 * v], S(cf0)), mul_rn(g[3 * v + 1], S(cf1))), mul_rn(g[3 * v + 2], S(cf2)));
+          S dP = u0[v];
+          if (cs.limiter == 1) {
+            if (dM > 0.) dP = sub_rn(umax[v], dP);
+            else if (dM < 0.) dP = sub_rn(umin[v], dP);
+            const S dP2 = mul_rn(dP, dP), dM2 = mul_rn(dM, dM);
+            const S e2 = S(eps2[v]);
+            if (dM != 0.) {
+              const S num = add_rn(add_rn(dP2, e2), mul_rn(mul_rn(S(2.), dM), dP));
+              const S den = add_rn(add_rn(add_rn(dP2, mul_rn(S(2.), dM2)), mul_rn(dM, dP)), e2);
+              phi[v] = smin(phi[v], div_rn(num, den));
+            }
+          } else {
+            if (dM > 0.) dP = sub_rn(umax[v], dP);
+            else if (dM < 0.) dP = sub_rn(umin[v], dP);
+            else { dP = S(1.); dM = S(1.); }
+            phi[v] = smin(phi[v], div_rn(dP, dM));
+          }
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int v = 0; v < 5; ++v) Lm[v * nc + c] = phi[v];
+}
+
+// Density the reference's `right` state cache holds when face f is reached:
+// the right density of face f-1 (walking back over faces whose BC branch
+// does not set it).  Face 0 starts from the zero-initialised cache.
+template <class S>
+__device__ S cached_right_rho(const DevCase &cs, const DevMesh &m, const S *W, const S *G, const S *Lm, int f) {
+  for (int g = f - 1; g >= 0; --g) {
+    const double n[3] = {m.f_n[g], m.f_n[m.nf + g], m.f_n[2 * m.nf + g]};
+    const double xf[3] = {m.f_x[g], m.f_x[m.nf + g], m.f_x[2 * m.nf + g]};
+    const int b = m.f_bc[g];
+    if (b < 0) {
+      FState<S> R;
+      recon_state(cs, m, W, G, Lm, m.f_neighbor[g], xf, R, n);
+      return R.rho;
+    }
+    FState<S> L, R;
+    recon_state(cs, m, W, G, Lm, m.f_parent[g], xf, L, n);
+    const int gh = m.f_neighbor[g], nt = m.nt;
+    R.pc = W[gh]; R.Vc[0] = W[nt + gh]; R.Vc[1] = W[2 * nt + gh]; R.Vc[2] = W[3 * nt + gh]; R.Tc = W[4 * nt + gh];
+    R.rho = S(0.);
+    if (apply_bc(cs, cs.bc[b], L, R, n, (int *)nullptr)) return R.rho;
+  }
+  return S(0.);
+}
+
+template <class S>
+__global__ void k_outlet_rho(DevCase cs, DevMesh m, const S *__restrict__ W, const S *__restrict__ G,
+                             const S *__restrict__ Lm, S *__restrict__ stale) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m.n_outlet) return;
+  const int f = m.outlet_faces[i];
+  stale[m.f_neighbor[f] - m.nc] = cached_right_rho(cs, m, W, G, Lm, f);
+}
+
+// ---- convective fluxes in xyz (rotated-frame algebra of ns_roe.cc,
+// ns_ausm_plus_up.cc, ns_vanleer.cc, rotated back as in
+// ns_convective_face_flux.cc:51-55, per unit area)
+template <class S>
+__host__ __device__ __forceinline__ void roe(const DevCase &c, const FState<S> &L, const FState<S> &R, const double n[3], S F[5], S &wL) {
+  const double G = c.gamma;
+  S r = sqrt(R.rho / L.rho);
+  const S ir = 1. / (1. + r);
+  S Vr[3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) Vr[i] = (L.V[i] + r * R.V[i]) * ir;
+  const S u = (L.Vn + r * R.Vn) * ir;
+  const S H = (L.H + r * R.H) * ir;
+  const S a = sqrt((G - 1.) * (H - 0.5 * (Vr[0] * Vr[0] + Vr[1] * Vr[1] + Vr[2] * Vr[2])));
+  r = r * L.rho;
+  const S Du = R.Vn - L.Vn, Dp = R.p - L.p;
+  S lambda, dV, Dl, mdot;
+  if (u >= 0.) {
+    dV = 0.5 * (Dp - r * a * Du) / (a * a);
+    lambda = u - a;
+    Dl = 2. * smin(a, smax(S(0.), 2. * (L.a - R.a + Du)));
+    if (lambda <= -0.5 * Dl) {
+    } else if (lambda < 0.5 * Dl) {
+      const S t = lambda - 0.5 * Dl;
+      lambda = -0.5 * t * t / Dl;
+    } else {
+      lambda = S(0.);
+    }
+    mdot = L.rho * L.Vn;
+    const S pr = lambda * dV;
+    F[0] = mdot + pr;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) F[1 + i] = mdot * L.V[i] + L.p * n[i] + pr * (Vr[i] - a * n[i]);
+    F[4] = mdot * L.H + pr * (H - u * a);
+  } else {
+    dV = 0.5 * (Dp + r * a * Du) / (a * a);
+    lambda = u + a;
+    Dl = 2. * smin(a, smax(S(0.), 2. * (R.a - L.a + Du)));
+    if (lambda >= 0.5 * Dl) {
+    } else if (lambda > -0.5 * Dl) {
+      const S t = lambda + 0.5 * Dl;
+      lambda = 0.5 * t * t / Dl;
+    } else {
+      lambda = S(0.);
+    }
+    mdot = R.rho * R.Vn;
+    const S pr = lambda * dV;
+    F[0] = mdot - pr;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) F[1 + i] = mdot * R.V[i] + R.p * n[i] - pr * (Vr[i] + a * n[i]);
+    F[4] = mdot * R.H - pr * (H + u * a);
+  }
+  wL = S(0.5);
+}
+
+template <class S> __host__ __device__ __forceinline__ S m2p(S M) { return 0.25 * (M + 1.) * (M + 1.); }
+template <class S> __host__ __device__ __forceinline__ S m2m(S M) { return -0.25 * (M - 1.) * (M - 1.); }
+
+template <class S>
+__host__ __device__ __forceinline__ void ausm(const DevCase &c, const FState<S> &L, const FState<S> &R, const double n[3], S F[5], S &wL) {
+  const double beta = 0.125, Kp = 0.25, Ku = 0.75, sigma = 1.;
+  const S aLh = L.a * L.a / smax(L.a, L.Vn);
+  const S aRh = R.a * R.a / smax(R.a, -1. * R.Vn);
+  const S a = smin(aLh, aRh);
+  const S rho = 0.5 * (L.rho + R.rho);
+  const S ML = L.Vn / a, MR = R.Vn / a;
+  const S Mbar2 = 0.5 * (ML * ML + MR * MR);
+  S Mref = smax(S(c.Minf), sqrt(Mbar2));
+  Mref = smin(Mref, S(1.));
+  S fa;
+  if (Mbar2 >= 1.) fa = S(1.);
+  else {
+    const S Mo = sqrt(smin(S(1.), smax(Mbar2, Mref * Mref)));
+    fa = Mo * (2. - Mo);
+  }
+  const S m4p = (fabs(ML) >= 1.) ? 0.5 * (ML + fabs(ML)) : m2p(ML) * (1. - 16. * beta * m2m(ML));
+  const S m4m = (fabs(MR) >= 1.) ? 0.5 * (MR - fabs(MR)) : m2m(MR) * (1. + 16. * beta * m2p(MR));
+  const S M = m4p + m4m - Kp / fa * smax(1. - sigma * Mbar2, S(0.)) * (R.p - L.p) / (rho * a * a);
+  const S mdot = (M > 0.) ? a * M * L.rho : a * M * R.rho;
+  const S alpha = 3. / 16. * (-4. + 5. * fa * fa);
+  const S p5p = (fabs(ML) >= 1.) ? 0.5 * (ML + fabs(ML)) / ML : m2p(ML) * ((2. - ML) - 16. * alpha * ML * m2m(ML));
+  const S p5m = (fabs(MR) >= 1.) ? 0.5 * (MR - fabs(MR)) / MR : m2m(MR) * ((-2. - MR) + 16. * alpha * MR * m2p(MR));
+  S p = p5p * (L.p + c.Pref) + p5m * (R.p + c.Pref) - Ku * p5p * p5m * (L.rho + R.rho) * fa * a * (R.Vn - L.Vn);
+  p = p - c.Pref;
+  F[0] = mdot;
+  const FState<S> &U = (mdot > 0.) ? L : R;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) F[1 + i] = mdot * U.V[i] + p * n[i];
+  F[4] = mdot * U.H;
+  wL = (mdot > 0.) ? S(1.) : S(0.);
+}
+
+template <class S>
+__host__ __device__ __forceinline__ void vanleer(const DevCase &c, const FState<S> &L, const FState<S> &R, const double n[3], S F[5], S &wL) {
+  const double G = c.gamma;
+  const S ML = L.Vn / L.a, MR = R.Vn / R.a;
+  const S M = 0.5 * (ML + MR);
+  if (M <= -1.) {
+    const S mdot = R.rho * R.Vn;
+    F[0] = mdot;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) F[1 + i] = mdot * R.V[i] + R.p * n[i];
+    F[4] = mdot * R.H;
+    wL = S(0.);
+  } else if (M >= 1.) {
+    const S mdot = L.rho * L.Vn;
+    F[0] = mdot;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) F[1 + i] = mdot * L.V[i] + L.p * n[i];
+    F[4] = mdot * L.H;
+    wL = S(1.);
+  } else {
+    const S fp = 0.25 * L.rho * L.a * (ML + 1.) * (ML + 1.);
+    const S fm = -0.25 * R.rho * R.a * (1. - MR) * (1. - MR);
+    F[0] = fp + fm;
+    S tL = (2. * L.a / G) * (0.5 * (G - 1.) * ML + 1.);
+    S tR = (2. * R.a / G) * (0.5 * (G - 1.) * MR - 1.);
+    const S fn1 = fp * tL + fm * tR - c.Pref;
+    S VtL[3], VtR[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) { VtL[i] = L.V[i] - L.Vn * n[i]; VtR[i] = R.V[i] - R.Vn * n[i]; }
+#pragma unroll
+    for (int i = 0; i < 3; ++i) F[1 + i] = fn1 * n[i] + fp * VtL[i] + fm * VtR[i];
+    const double k = 0.5 * G * G / (G * G - 1.);
+    tL = k * tL * tL + 0.5 * (VtL[0] * VtL[0] + VtL[1] * VtL[1] + VtL[2] * VtL[2]);
+    tR = k * tR * tR + 0.5 * (VtR[0] * VtR[0] + VtR[1] * VtR[1] + VtR[2] * VtR[2]);
+    F[4] = fp * tL + fm * tR;
+    wL = S(0.5);
+  }
+}
+
+// Face flux: reconstruction, BCs, inviscid + viscous flux; D = Fd - Fc.
+template <class S, bool VISCOUS>
+__global__ void __launch_bounds__(128) k_face_flux(DevCase cs, DevMesh m, const S *__restrict__ W, const S *__restrict__ G,
+                                                   const S *__restrict__ Lm, const S *__restrict__ stale,
+                                                   const S *__restrict__ mu_t, S *__restrict__ D, S *__restrict__ mdot_out,
+                                                   S *__restrict__ wl_out, int *err) {
+  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nf = m.nf, nt = m.nt, nc = m.nc;
+  if (f >= nf) return;
+  const int pa = m.f_parent[f], nb = m.f_neighbor[f], b = m.f_bc[f];
+  const double n[3] = {m.f_n[f], m.f_n[nf + f], m.f_n[2 * nf + f]};
+  const double xf[3] = {m.f_x[f], m.f_x[nf + f], m.f_x[2 * nf + f]};
+  const double A = m.f_area[f];
+  FState<S> L, R;
+  recon_state(cs, m, W, G, Lm, pa, xf, L, n);
+  if (b < 0) {
+    recon_state(cs, m, W, G, Lm, nb, xf, R, n);
+  } else {
+    R.pc = W[nb]; R.Vc[0] = W[nt + nb]; R.Vc[1] = W[2 * nt + nb]; R.Vc[2] = W[3 * nt + nb]; R.Tc = W[4 * nt + nb];
+    R.rho = S(0.);
+    if (!apply_bc(cs, cs.bc[b], L, R, n, err)) R.rho = stale[nb - nc];
+    finish(cs, R, n);
+  }
+  S F[5], wL;
+  if (cs.flux == 1) roe(cs, L, R, n, F, wL);
+  else if (cs.flux == 2) vanleer(cs, L, R, n, F, wL);
+  else ausm(cs, L, R, n, F, wL);
+  S Fd[5] = {S(0.), S(0.), S(0.), S(0.), S(0.)};
+  if (VISCOUS) {
+    // face_state_update (ns_assemble_linear_system.cc:353-415)
+    S gr[12];  // u,v,w,T gradients at the face
+    if (b >= 0) {
+#pragma unroll
+      for (int i = 0; i < 12; ++i) gr[i] = G[(3 + i) * nc + pa];
+    } else {
+      const double wP = m.f_w[f], wN = m.f_w[nf + f];
+#pragma unroll
+      for (int i = 0; i < 12; ++i) gr[i] = wP * G[(3 + i) * nc + pa] + wN * G[(3 + i) * nc + nb];
+    }
+    const double l0 = m.c_x[nb] - m.c_x[pa], l1 = m.c_x[nt + nb] - m.c_x[nt + pa], l2 = m.c_x[2 * nt + nb] - m.c_x[2 * nt + pa];
+    const double lm = sqrt(l0 * l0 + l1 * l1 + l2 * l2);
+    const double e0 = l0 / lm, e1 = l1 / lm, e2 = l2 / lm;
+    const S dc[4] = {R.Vc[0] - L.Vc[0], R.Vc[1] - L.Vc[1], R.Vc[2] - L.Vc[2], R.Tc - L.Tc};
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const S dn = gr[3 * q] * e0 + gr[3 * q + 1] * e1 + gr[3 * q + 2] * e2;
+      const S s = dc[q] / lm - dn;
+      gr[3 * q] = gr[3 * q] + s * e0;
+      gr[3 * q + 1] = gr[3 * q + 1] + s * e1;
+      gr[3 * q + 2] = gr[3 * q + 2] + s * e2;
+    }
+    const S Vf[3] = {0.5 * (L.V[0] + R.V[0]), 0.5 * (L.V[1] + R.V[1]), 0.5 * (L.V[2] + R.V[2])};
+    const S Tf = 0.5 * (L.T + R.T);
+    S mu = viscosity(cs, Tf), lam = therm_cond(cs, Tf);
+    if (mu_t) {
+      const S mt = mu_t[f];
+      mu = mu + mt;
+      lam = lam + cs.Cp * mt / cs.Pr_t;
+    }
+    // ns_diffusive_face_flux.cc:28-64
+    const S *gu = gr, *gv = gr + 3, *gw = gr + 6, *gT = gr + 9;
+    const S tx0 = 2. / 3. * (2. * gu[0] - gv[1] - gw[2]), tx1 = gu[1] + gv[0], tx2 = gu[2] + gw[0];
+    const S ty1 = 2. / 3. * (2. * gv[1] - gu[0] - gw[2]), ty2 = gv[2] + gw[1];
+    const S tz2 = 2. / 3. * (2. * gw[2] - gu[0] - gv[1]);
+    const double an[3] = {n[0] * A, n[1] * A, n[2] * A};
+    Fd[1] = mu * (tx0 * an[0] + tx1 * an[1] + tx2 * an[2]);
+    Fd[2] = mu * (tx1 * an[0] + ty1 * an[1] + ty2 * an[2]);
+    Fd[3] = mu * (tx2 * an[0] + ty2 * an[1] + tz2 * an[2]);
+    Fd[4] = mu * ((tx0 * Vf[0] + tx1 * Vf[1] + tx2 * Vf[2]) * an[0] + (tx1 * Vf[0] + ty1 * Vf[1] + ty2 * Vf[2]) * an[1] +
+                  (tx2 * Vf[0] + ty2 * Vf[1] + tz2 * Vf[2]) * an[2]);
+    S qq = lam * (gT[0] * an[0] + gT[1] * an[1] + gT[2] * an[2]);
+    if (b >= 0 && cs.bc[b].thermal == TH_FIXED_Q_) qq = S(cs.bc[b].qdot * A);
+    Fd[4] = Fd[4] + qq;
+  }
+#pragma unroll
+  for (int v = 0; v < 5; ++v) D[v * nf + f] = Fd[v] - F[v] * A;
+  if (mdot_out) mdot_out[f] = (F[0] * A - Fd[0]) / A;
+  if (wl_out) wl_out[f] = wL;
+}
+
+// Atomic-free gather: R_c = sum over the cell's faces in ascending face order
+// of (+D) for the parent side and (-D) for the neighbour side.
+template <class S, bool AOS>
+__global__ void k_gather(DevMesh m, const S *__restrict__ D, S *__restrict__ R) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= m.nc) return;
+  const int nf = m.nf;
+  S r[5] = {S(0.), S(0.), S(0.), S(0.), S(0.)};
+  for (int j = m.cf_index[c]; j < m.cf_index[c + 1]; ++j) {
+    const int e = m.cf_list[j];
+    if (e >= 0) {
+#pragma unroll
+      for (int v = 0; v < 5; ++v) r[v] = r[v] + (D[v * nf + e] + 0.);
+    } else {
+      const int f = ~e;
+#pragma unroll
+      for (int v = 0; v < 5; ++v) r[v] = r[v] + (-1. * D[v * nf + f] + 0.);
+    }
+  }
+  if (AOS) {
+#pragma unroll
+    for (int v = 0; v < 5; ++v) R[5 * c + v] = r[v];
+  } else {
+#pragma unroll
+    for (int v = 0; v < 5; ++v) R[v * m.nc + c] = r[v];
+  }
+}
+
+// Local time step (time_step.cc:143-224).
+template <class S>
+__global__ void k_local_dt(DevCase cs, DevMesh m, const S *__restrict__ W, S *__restrict__ dt, double cfl,
+                           unsigned long long *__restrict__ minkey) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= m.nc) return;
+  const int nt = m.nt;
+  const S p = W[c], u = W[nt + c], v = W[2 * nt + c], w = W[3 * nt + c], T = W[4 * nt + c];
+  const S a = sound(cs, p, T);
+  const S val = cfl * m.c_len[c] / (sqrt(u * u + v * v + w * w) + a);
+  dt[c] = val;
+  if (minkey) atomicMin(minkey, okey((double)val));
+}
+
+template <class S>
+__global__ void k_fill_min(int n, S *__restrict__ dt, const unsigned long long *__restrict__ minkey) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < n) dt[c] = S(okey_inv(*minkey));
+}
+
+}  // namespace fcfd

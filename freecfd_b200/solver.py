@@ -1,0 +1,163 @@
+"""Host-side mirror of the reference's residual interface.
+
+``Case`` stands for the parsed input deck (read_inputs + MATERIAL::set +
+NavierStokes::set_bcs), ``Mesh`` for ``Grid`` after ``setup``/``set_bcs``/
+``gradient_maps`` and ``NavierStokes`` for the solver object whose residual
+(``assemble_linear_system`` right-hand side), gradients (``calc_cell_grads``),
+limiters (``calc_limiter``) and local time step (``update_time_step``) run on
+the B200 through libfcfd_b200.  Arrays are in the reference's cell / face
+order; states are [n_cells][5] = (p, u, v, w, T).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import tempfile
+
+import numpy as np
+
+from ._lib import _RawMesh, _d, _i, _ptr, check, lib
+
+
+class Case:
+    """Parsed input deck (src/read_inputs.cc schema and defaults)."""
+
+    def __init__(self, deck_path: str):
+        h = ctypes.c_void_p()
+        check(lib.fcfd_case_from_deck(os.fsencode(deck_path), ctypes.byref(h)))
+        self.h = h
+        self.path = deck_path
+
+    @classmethod
+    def from_case(cls, case, workdir: str | None = None):
+        """Write a synthetic ``cases.Case`` deck to ``workdir`` and parse it."""
+        tmp = None
+        if workdir is None:
+            tmp = tempfile.TemporaryDirectory()
+            workdir = tmp.name
+        obj = cls(case.write_deck(workdir))
+        obj._tmp = tmp
+        return obj
+
+    def summary(self):
+        d = np.empty(13)
+        i = np.zeros(7 + 4 * 64, np.int32)
+        check(lib.fcfd_case_summary(self.h, _d(d), _i(i), i.size))
+        return d, i[:7 + 4 * int(i[5])]
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib.fcfd_case_destroy(self.h)
+            self.h = None
+
+
+class Mesh:
+    """Reference-order connectivity, geometry and LSQ stencils (Grid)."""
+
+    def __init__(self, raw, case: Case):
+        self._keep = [np.ascontiguousarray(raw.nodes, np.float64), np.ascontiguousarray(raw.conn_index, np.int32),
+                      np.ascontiguousarray(raw.conn, np.int32)]
+        bidx, bflat = raw.bc_csr()
+        self._keep += [np.ascontiguousarray(bidx, np.int32), np.ascontiguousarray(bflat, np.int32)]
+        nodes, cidx, conn, bidx, bflat = self._keep
+        r = _RawMesh(nodes.shape[0], _d(nodes), raw.n_cells, _i(cidx), _i(conn), len(raw.bc_nodes), _i(bidx), _i(bflat))
+        h = ctypes.c_void_p()
+        check(lib.fcfd_mesh_create(ctypes.byref(r), case.h, ctypes.byref(h)))
+        self.h = h
+        s = (ctypes.c_int64 * 8)()
+        check(lib.fcfd_mesh_sizes(self.h, s))
+        (self.nc, self.nf, self.nghost, self.ntot, self.nnodes, self.n_grad_entries, self.n_cell_faces,
+         self.n_nbrs) = [int(x) for x in s]
+
+    def connectivity(self):
+        nf, nc = self.nf, self.nc
+        out = dict(face_parent=np.empty(nf, np.int32), face_neighbor=np.empty(nf, np.int32),
+                   face_bc=np.empty(nf, np.int32), face_nodes=np.empty((nf, 4), np.int32),
+                   cell_face_index=np.empty(nc + 1, np.int32), cell_faces=np.empty(self.n_cell_faces, np.int32),
+                   nbr_index=np.empty(nc + 1, np.int32), nbrs=np.empty(self.n_nbrs, np.int32),
+                   grad_index=np.empty(nc + 1, np.int32), grad_keys=np.empty(self.n_grad_entries, np.int32))
+        check(lib.fcfd_mesh_connectivity(self.h, *[_i(out[k]) for k in (
+            "face_parent", "face_neighbor", "face_bc", "face_nodes", "cell_face_index", "cell_faces", "nbr_index",
+            "nbrs", "grad_index", "grad_keys")]))
+        return out
+
+    def geometry(self):
+        nf, nt = self.nf, self.ntot
+        out = dict(face_normal=np.empty((nf, 3)), face_area=np.empty(nf), face_centroid=np.empty((nf, 3)),
+                   face_avg=np.empty((nf, 2)), cell_centroid=np.empty((nt, 3)), cell_volume=np.empty(nt),
+                   cell_length=np.empty(nt), cell_wall_distance=np.empty(nt))
+        ls = np.empty(1)
+        check(lib.fcfd_mesh_geometry(self.h, _d(out["face_normal"]), _d(out["face_area"]), _d(out["face_centroid"]),
+                                     _d(out["face_avg"]), _d(out["cell_centroid"]), _d(out["cell_volume"]),
+                                     _d(out["cell_length"]), _d(out["cell_wall_distance"]), _d(ls)))
+        out["length_scale"] = float(ls[0])
+        return out
+
+    def lsq_data(self):
+        cof = np.empty((self.nc, 7)); selfw = np.empty((self.nc, 3))
+        check(lib.fcfd_mesh_lsq(self.h, _d(cof), _d(selfw)))
+        return cof, selfw
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib.fcfd_mesh_destroy(self.h)
+            self.h = None
+
+
+class NavierStokes:
+    """Device residual context (one CUDA stream, device buffers)."""
+
+    def __init__(self, mesh: Mesh, case: Case, device: int = 0):
+        self.mesh, self.case = mesh, case
+        h = ctypes.c_void_p()
+        check(lib.fcfd_ctx_create(mesh.h, case.h, int(device), ctypes.byref(h)))
+        self.h = h
+
+    def residual(self, W, out=None):
+        """R(W) for W [nc][5] (numpy host array or CUDA torch tensor)."""
+        nc = self.mesh.nc
+        if out is None:
+            out = np.empty((nc, 5)) if isinstance(W, np.ndarray) else W.new_empty((nc, 5))
+        if isinstance(W, np.ndarray):
+            W = np.ascontiguousarray(W, dtype=np.float64)
+        pw, fw = _ptr(W)
+        pr, fr = _ptr(out)
+        if fw != fr:
+            raise ValueError("W and R must both be host arrays or both be device tensors")
+        check(lib.fcfd_residual(self.h, pw, pr, fw))
+        return out
+
+    def stages(self):
+        m = self.mesh
+        out = dict(grads=np.empty((m.nc, 15)), limiter=np.empty((m.nc, 5)), ghost=np.empty((m.nghost, 5)),
+                   mdot=np.empty(m.nf), weightL=np.empty(m.nf))
+        check(lib.fcfd_last_stages(self.h, _d(out["grads"]), _d(out["limiter"]), _d(out["ghost"]), _d(out["mdot"]),
+                                   _d(out["weightL"])))
+        return out
+
+    def local_dt(self, W, cfl: float, mode: int = 0):
+        nc = self.mesh.nc
+        W = np.ascontiguousarray(W, dtype=np.float64)
+        dt = np.empty(nc)
+        pw, fw = _ptr(W)
+        check(lib.fcfd_local_dt(self.h, pw, float(cfl), int(mode), ctypes.c_void_p(dt.ctypes.data), fw))
+        return dt
+
+    def time_residual(self, reps: int = 50, flush_l2: bool = True):
+        out = np.zeros(8)
+        check(lib.fcfd_time_residual(self.h, int(reps), int(bool(flush_l2)), _d(out), out.size))
+        return out
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib.fcfd_ctx_destroy(self.h)
+            self.h = None
+
+
+def point_flux(flux: int, L, R, n, gamma=1.4, gas_R=287.0, Pref=0.0, Tref=0.0, Minf=1.0):
+    """Convective flux per unit area through a face with unit normal n."""
+    L = np.ascontiguousarray(L, np.float64); R = np.ascontiguousarray(R, np.float64)
+    n = np.ascontiguousarray(n, np.float64)
+    out = np.empty(5); wl = np.empty(1)
+    check(lib.fcfd_point_flux(int(flux), _d(L), _d(R), _d(n), gamma, gas_R, Pref, Tref, Minf, _d(out), _d(wl)))
+    return out, float(wl[0])

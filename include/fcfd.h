@@ -1,0 +1,141 @@
+/*
+ * fcfd.h — C ABI of the B200 residual / Newton-Krylov library (libfcfd_b200.so).
+ *
+ * Free CFD has no plugin or FFI layer: its residual path is a set of C++
+ * member functions of NavierStokes/RANS reading process-global state
+ * (src/navier_stokes/ns.h:57-64, src/rans/rans.h:40-45).  Each entry point
+ * below names the reference routine(s) it stands in for.  Conventions:
+ *   - every function returns an int status (FCFD_OK = 0) and never exits;
+ *     fcfd_last_error() returns a message for the calling thread;
+ *   - cell arrays are in the reference's cell order (Grid::create_nodes_cells,
+ *     src/grid/grid_create_elements.cc:27-182), AoS [cell][5] = (p,u,v,w,T)
+ *     primitive gauge variables (src/navier_stokes/ns.cc:356-361);
+ *   - face arrays are in the reference's face order (Grid::create_faces,
+ *     src/grid/grid_create_elements.cc:184-412);
+ *   - host pointers unless FCFD_DEVICE_PTRS is passed in `flags`;
+ *   - a context owns its device buffers and one CUDA stream; it is not
+ *     thread-safe; separate contexts may run concurrently.
+ */
+#ifndef FCFD_H
+#define FCFD_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum fcfd_status {
+  FCFD_OK = 0,
+  FCFD_ERR_INPUT = 1,          /* bad deck / argument (reference: cerr + exit(1)) */
+  FCFD_ERR_MESH = 2,           /* mesh could not be built (e.g. unassigned boundary face) */
+  FCFD_ERR_DIVERGED = 3,       /* NaN/Inf in an update (reference: ns.cc:349-355 MPI_Abort) */
+  FCFD_ERR_NOT_CONVERGED = 4,  /* Newton / Krylov iteration cap reached */
+  FCFD_ERR_CUDA = 5,           /* CUDA runtime error */
+  FCFD_ERR_TIMEOUT = 6,        /* a bounded device wait ran out */
+  FCFD_ERR_UNSUPPORTED = 7,    /* option outside the restated path */
+  FCFD_ERR_BC = 8              /* boundary condition failure (e.g. supersonic inlet without state) */
+};
+
+enum fcfd_flags {
+  FCFD_DEVICE_PTRS = 1 /* input/output pointers are device pointers on the context's device */
+};
+
+enum fcfd_precision { FCFD_FP64 = 0, FCFD_FP32 = 1 };
+
+typedef struct fcfd_case fcfd_case;
+typedef struct fcfd_mesh fcfd_mesh;
+typedef struct fcfd_ctx fcfd_ctx;
+
+/* CELL-type raw grid, same meaning as GridRawData (src/grid/grid.h:61-78):
+ * node coordinates, CGNS-ordered element connectivity (4/6/8-node cells),
+ * and per boundary region the node ids on it (region b is BC_{b+1}). */
+typedef struct fcfd_raw_mesh {
+  int32_t n_nodes;
+  const double *xyz;          /* [n_nodes][3] */
+  int32_t n_cells;
+  const int32_t *conn_index;  /* [n_cells+1] */
+  const int32_t *conn;        /* [conn_index[n_cells]] */
+  int32_t n_bc;
+  const int32_t *bc_index;    /* [n_bc+1] */
+  const int32_t *bc_nodes;    /* [bc_index[n_bc]] */
+} fcfd_raw_mesh;
+
+const char *fcfd_last_error(void);
+const char *fcfd_version(void);
+
+/* Parse an input deck (+ <material>.mat beside it).  Replaces read_inputs()
+ * (src/read_inputs.cc:28-218), InputFile (src/inputs/inputs.cc:37-345),
+ * MATERIAL::set (src/material/material.cc:29-106) and NavierStokes::set_bcs
+ * (src/navier_stokes/ns_set_bcs.cc:25-140). */
+int fcfd_case_from_deck(const char *deck_path, fcfd_case **out);
+void fcfd_case_destroy(fcfd_case *cs);
+/* dv[13] = gamma, R, Pref, Tref, Minf, limiter threshold, mu, lambda,
+ *          sutherland mu_ref, T_ref, S, Pr, (unused 0)
+ * iv[7+4*n_bc] = flux, limiter, order, sutherland, prandtl, n_bc, dimension,
+ *                then per BC: type, kind, specified, thermalType           */
+int fcfd_case_summary(const fcfd_case *cs, double *dv, int32_t *iv, int32_t iv_len);
+
+/* Build connectivity, geometry and stencils.  Replaces Grid::setup
+ * (src/grid/grid.cc:55-82), set_bcs (src/set_bcs.cc:35-260),
+ * set_lengthScales (src/main.cc:456-491), face_interpolation_weights
+ * (src/face_interpolation_weights.cc:32-138) and gradient_maps/lsqr_grad_map
+ * (src/gradient_maps.cc:39-78, src/lsqr_grad_map.cc:32-99). */
+int fcfd_mesh_create(const fcfd_raw_mesh *raw, const fcfd_case *cs, fcfd_mesh **out);
+void fcfd_mesh_destroy(fcfd_mesh *m);
+/* out[8] = n_cells, n_faces, n_ghosts, n_total, n_nodes, stencil entries,
+ *          cell-face entries, neighbour entries */
+int fcfd_mesh_sizes(const fcfd_mesh *m, int64_t *out);
+/* Reference-order integer connectivity (for bit-exact parity checks). */
+int fcfd_mesh_connectivity(const fcfd_mesh *m, int32_t *face_parent, int32_t *face_neighbor, int32_t *face_bc,
+                           int32_t *face_nodes /* [nf][4], -1 pad */, int32_t *cell_face_index,
+                           int32_t *cell_faces, int32_t *nbr_index, int32_t *nbrs, int32_t *grad_index,
+                           int32_t *grad_keys);
+/* Geometry in reference order (ghost cells follow interior cells). */
+int fcfd_mesh_geometry(const fcfd_mesh *m, double *face_normal, double *face_area, double *face_centroid,
+                       double *face_avg /* [nf][2] */, double *cell_centroid, double *cell_volume,
+                       double *cell_length, double *cell_wall_distance, double *length_scale);
+
+/* Least-squares gradient data per interior cell: cofactors[nc][7] =
+ * (C00,C01,C02,C11,C12,C22,det) of the weighted normal matrix and
+ * self_weight[nc][3], the weight of the cell's own value
+ * (lsqr_grad_map, src/lsqr_grad_map.cc:74-96). */
+int fcfd_mesh_lsq(const fcfd_mesh *m, double *cofactors, double *self_weight);
+
+/* Create a device context on CUDA device `device`. */
+int fcfd_ctx_create(const fcfd_mesh *m, const fcfd_case *cs, int device, fcfd_ctx **out);
+void fcfd_ctx_destroy(fcfd_ctx *ctx);
+
+/* Spatial residual R(W) = sum over faces of +/-(F_diffusive - F_convective)
+ * for the interior-cell state W[nc][5].  Replaces the residual part of
+ * NavierStokes::assemble_linear_system (src/navier_stokes/ns_assemble_linear_system.cc:34-140)
+ * preceded by update_boundaries (reconstructed, first-order ghost update as at
+ * initialise, ns.cc:93), calc_cell_grads (ns.cc:301-336) and calc_limiter
+ * (ns_limiters.cc:26-248).  R[nc][5]. */
+int fcfd_residual(fcfd_ctx *ctx, const double *W, double *R, int flags);
+/* Per-stage outputs of the last fcfd_residual call (reference order):
+ * grads[nc][15] (p,u,v,w,T gradients), limiter[nc][5], ghost[n_ghosts][5],
+ * mdot[nf] (Variable mdot, ns_assemble_linear_system.cc:123), weightL[nf]. */
+int fcfd_last_stages(fcfd_ctx *ctx, double *grads, double *limiter, double *ghost, double *mdot, double *weightL);
+/* Local time step, update_time_step (src/time_step.cc:143-224):
+ * mode 0 = CFL_LOCAL (dt_c = cfl*l_c/(|V|+a)), mode 1 = CFL_MAX (global min). */
+int fcfd_local_dt(fcfd_ctx *ctx, const double *W, double cfl, int mode, double *dt, int flags);
+
+/* Device timing of the residual: runs `reps` residual evaluations on the
+ * resident state (captured in one CUDA graph) and returns per-kernel average
+ * milliseconds: out[0] total per residual, out[1..] per kernel (see fcfd.cu). */
+int fcfd_time_residual(fcfd_ctx *ctx, int reps, int flush_l2, double *out, int out_len);
+
+/* Point fluxes in the reference's rotated-frame signature
+ * (roe_flux ns_roe.cc:25, AUSMplusUP_flux ns_ausm_plus_up.cc:35,
+ * vanLeer_flux ns_vanleer.cc:25).  L/R = (p,u,v,w,T) face states,
+ * n = unit normal; out[5] = xyz flux per unit area (convective_face_flux
+ * ns_convective_face_flux.cc:32-59 without the area factor).  Material is
+ * given by gamma, R and the gauge offsets Pref/Tref. */
+int fcfd_point_flux(int flux, const double *L, const double *R, const double *n, double gamma, double gas_R,
+                    double Pref, double Tref, double Minf, double *out, double *weightL);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FCFD_H */

@@ -1,0 +1,32 @@
+"""Shared helpers for the parity tests: small instances of every benchmark
+mesh family and the normwise comparison used throughout."""
+import tempfile
+
+import numpy as np
+
+from freecfd_b200 import cases
+
+# Small meshes of each family (the oracle finishes these in well under a second)
+SMALL = {
+    "wedge": lambda **kw: cases.wedge_case(ni=24, nj=12, **kw),
+    "cylinder": lambda **kw: cases.cylinder_case(ntheta=32, nr=16, **kw),
+    "hypersonic": lambda **kw: cases.hypersonic_case(ntheta=32, nr=16, **kw),
+    "plate": lambda **kw: cases.plate_case(ni=24, nj=12, nk=3, turbulent=False, **kw),
+}
+
+
+def build_pair(case, oracle_mod, fb):
+    """Oracle + product objects for the same case (decks in a temp dir)."""
+    d = tempfile.mkdtemp(prefix="fcfd_")
+    o = oracle_mod.Oracle(case, d)
+    cs = fb.Case(case.write_deck(d))
+    m = fb.Mesh(case.mesh, cs)
+    return o, cs, m
+
+
+def rel_err(a, b):
+    """Normwise relative error per equation column: max|a-b| / max|b|."""
+    a = np.asarray(a).reshape(-1, np.asarray(a).shape[-1]) if np.asarray(a).ndim > 1 else np.asarray(a)[:, None]
+    b = np.asarray(b).reshape(a.shape)
+    scale = np.maximum(np.abs(b).max(axis=0), 1e-300)
+    return (np.abs(a - b).max(axis=0) / scale)
