@@ -25,7 +25,7 @@ EXPORTED = [
     "fcfd_mesh_create", "fcfd_mesh_destroy", "fcfd_mesh_sizes", "fcfd_mesh_connectivity", "fcfd_mesh_geometry",
     "fcfd_mesh_lsq",
     "fcfd_ctx_create", "fcfd_ctx_destroy", "fcfd_residual", "fcfd_last_stages", "fcfd_local_dt",
-    "fcfd_time_residual", "fcfd_point_flux",
+    "fcfd_time_residual", "fcfd_point_flux", "fcfd_jvp",
 ]
 
 
@@ -76,6 +76,7 @@ def _load():
     L.fcfd_residual.argtypes = [vp, vp, vp, ctypes.c_int]
     L.fcfd_last_stages.argtypes = [vp, dp, dp, dp, dp, dp]
     L.fcfd_local_dt.argtypes = [vp, vp, ctypes.c_double, ctypes.c_int, vp, ctypes.c_int]
+    L.fcfd_jvp.argtypes = [vp, vp, vp, vp, vp, ctypes.c_int]
     L.fcfd_time_residual.argtypes = [vp, ctypes.c_int, ctypes.c_int, dp, ctypes.c_int]
     L.fcfd_point_flux.argtypes = [ctypes.c_int, dp, dp, dp, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                   ctypes.c_double, ctypes.c_double, dp, dp]

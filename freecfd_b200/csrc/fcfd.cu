@@ -7,12 +7,17 @@
 #include <memory>
 #include <mutex>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "internal.hpp"
 #include "kernels.cuh"
 
 namespace fcfd {
+
+// defined in ghost.cu (compiled with -fmad=false)
+extern template __global__ void k_ghost_minmax<double>(DevCase, DevMesh, double *, unsigned long long *, int *);
+extern template __global__ void k_ghost_minmax<Dual<double>>(DevCase, DevMesh, Dual<double> *, unsigned long long *, int *);
 
 fcfd_case *read_deck(const std::string &path);
 fcfd_mesh *build_mesh(const fcfd_raw_mesh &raw, fcfd_case &cs);
@@ -66,6 +71,23 @@ struct Timing {
 
 using namespace fcfd;
 
+namespace fcfd {
+// Typed working buffers of one residual chain (scalar S = double, or a dual
+// number for tangent runs).
+template <class S>
+struct Pipe {
+  DBuf<S> W, G, Lm, D, stale, R;
+  bool ready = false;
+  void alloc(int nc, int nf, int nb) {
+    const int nt = nc + nb;
+    W.alloc(5 * (size_t)nt); G.alloc(15 * (size_t)nc); Lm.alloc(5 * (size_t)nc); D.alloc(5 * (size_t)nf);
+    stale.alloc(nb > 0 ? nb : 1); R.alloc(5 * (size_t)nc);
+    CK(cudaMemset(stale.p, 0, sizeof(S) * (nb > 0 ? nb : 1)));
+    ready = true;
+  }
+};
+}  // namespace fcfd
+
 struct fcfd_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -77,9 +99,11 @@ struct fcfd_ctx {
   DBuf<int> f_parent, f_neighbor, f_bc, cf_index, cf_list, st_index, st_keys, bface, outlet;
   DBuf<double> f_n, f_area, f_x, f_w, c_x, c_len, st_cof, st_self;
   // state arrays
-  DBuf<double> W, G, Lm, D, stale, R, Win, dt, mdot, wl;
+  Pipe<double> p64;
+  Pipe<Dual<double>> pjv;
+  DBuf<double> Win, Vin, Rtmp, dt, mdot, wl;
   DBuf<unsigned long long> ext;
-  DBuf<int> err;
+  DBuf<int> err, argx;
   DBuf<unsigned char> flush;
   int n_outlet = 0;
   cudaGraphExec_t graph = nullptr;
@@ -87,30 +111,34 @@ struct fcfd_ctx {
 
 namespace fcfd {
 
-static void launch_residual(fcfd_ctx *x, const double *Wsoa_ready, double *Rout, bool aos_out, bool want_aux) {
+template <class S>
+static void launch_chain(fcfd_ctx *x, Pipe<S> &P, S *Rout, bool aos_out, S *mo, S *wo) {
   const DevMesh &m = x->dm;
   cudaStream_t s = x->stream;
-  (void)Wsoa_ready;
   const int tb = 256;
   // extrema slots: even = max (start at key 0), odd = min (start at all ones)
   CK(cudaMemsetAsync(x->ext.p, 0x00, 8 * sizeof(unsigned long long), s));
   for (int k = 1; k < 8; k += 2) CK(cudaMemsetAsync(x->ext.p + k, 0xFF, sizeof(unsigned long long), s));
   int ng = (m.nb + tb - 1) / tb;
   if (ng < 296) ng = 296;
-  k_ghost_minmax<double><<<ng, tb, 0, s>>>(x->cs, m, x->W.p, x->ext.p, x->err.p);
-  k_grad_limiter<double><<<(m.nc + 127) / 128, 128, 0, s>>>(x->cs, m, x->W.p, x->ext.p, x->G.p, x->Lm.p);
+  k_ghost_minmax<S><<<ng, tb, 0, s>>>(x->cs, m, P.W.p, x->ext.p, x->err.p);
+  const int *argx = nullptr;
+  if (!std::is_same<S, double>::value && x->cs.limiter == 1 && x->cs.order != 1) {
+    CK(cudaMemsetAsync(x->argx.p, 0x7F, 8 * sizeof(int), s));
+    k_argext<S><<<(m.nc + tb - 1) / tb, tb, 0, s>>>(m, P.W.p, x->ext.p, x->argx.p);
+    argx = x->argx.p;
+  }
+  k_grad_limiter<S><<<(m.nc + 127) / 128, 128, 0, s>>>(x->cs, m, P.W.p, x->ext.p, argx, P.G.p, P.Lm.p);
   if (m.n_outlet > 0)
-    k_outlet_rho<double><<<(m.n_outlet + 127) / 128, 128, 0, s>>>(x->cs, m, x->W.p, x->G.p, x->Lm.p, x->stale.p);
-  double *mo = want_aux ? x->mdot.p : nullptr;
-  double *wo = want_aux ? x->wl.p : nullptr;
+    k_outlet_rho<S><<<(m.n_outlet + 127) / 128, 128, 0, s>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p);
   if (x->viscous)
-    k_face_flux<double, true><<<(m.nf + 127) / 128, 128, 0, s>>>(x->cs, m, x->W.p, x->G.p, x->Lm.p, x->stale.p, nullptr, x->D.p, mo, wo, x->err.p);
+    k_face_flux<S, true><<<(m.nf + 127) / 128, 128, 0, s>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p, (const S *)nullptr, P.D.p, mo, wo, x->err.p);
   else
-    k_face_flux<double, false><<<(m.nf + 127) / 128, 128, 0, s>>>(x->cs, m, x->W.p, x->G.p, x->Lm.p, x->stale.p, nullptr, x->D.p, mo, wo, x->err.p);
+    k_face_flux<S, false><<<(m.nf + 127) / 128, 128, 0, s>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p, (const S *)nullptr, P.D.p, mo, wo, x->err.p);
   if (aos_out)
-    k_gather<double, true><<<(m.nc + tb - 1) / tb, tb, 0, s>>>(m, x->D.p, Rout);
+    k_gather<S, true><<<(m.nc + tb - 1) / tb, tb, 0, s>>>(m, P.D.p, Rout);
   else
-    k_gather<double, false><<<(m.nc + tb - 1) / tb, tb, 0, s>>>(m, x->D.p, Rout);
+    k_gather<S, false><<<(m.nc + tb - 1) / tb, tb, 0, s>>>(m, P.D.p, Rout);
   CK(cudaGetLastError());
 }
 
@@ -278,11 +306,10 @@ int fcfd_ctx_create(const fcfd_mesh *mp, const fcfd_case *csp, int device, fcfd_
   x->outlet.upload(outl);
   x->n_outlet = (int)outl.size();
   // ---- state buffers
-  x->W.alloc(5 * (size_t)nt); x->G.alloc(15 * (size_t)nc); x->Lm.alloc(5 * (size_t)nc); x->D.alloc(5 * (size_t)nf);
-  x->stale.alloc(nb > 0 ? nb : 1); x->R.alloc(5 * (size_t)nc); x->Win.alloc(5 * (size_t)nc); x->dt.alloc(nc);
-  x->mdot.alloc(nf); x->wl.alloc(nf); x->ext.alloc(8); x->err.alloc(1);
+  x->p64.alloc(nc, nf, nb);
+  x->Win.alloc(5 * (size_t)nc); x->Vin.alloc(5 * (size_t)nc); x->Rtmp.alloc(5 * (size_t)nc); x->dt.alloc(nc);
+  x->mdot.alloc(nf); x->wl.alloc(nf); x->ext.alloc(8); x->err.alloc(1); x->argx.alloc(8);
   CK(cudaMemset(x->err.p, 0, sizeof(int)));
-  CK(cudaMemset(x->stale.p, 0, sizeof(double) * (nb > 0 ? nb : 1)));
   DevMesh &dm = x->dm;
   dm.nc = nc; dm.nf = nf; dm.nb = nb; dm.nt = nt;
   dm.f_parent = x->f_parent.p; dm.f_neighbor = x->f_neighbor.p; dm.f_bc = x->f_bc.p;
@@ -314,10 +341,10 @@ int fcfd_residual(fcfd_ctx *x, const double *W, double *R, int flags) {
     CK(cudaMemcpyAsync(x->Win.p, W, sizeof(double) * 5 * m.nc, cudaMemcpyHostToDevice, x->stream));
     win = x->Win.p;
   }
-  k_aos_to_soa<double><<<(m.nc + 255) / 256, 256, 0, x->stream>>>(win, x->W.p, m.nc, m.nt);
-  double *rout = dev ? R : x->R.p;
-  launch_residual(x, x->W.p, rout, true, true);
-  if (!dev) CK(cudaMemcpyAsync(R, x->R.p, sizeof(double) * 5 * m.nc, cudaMemcpyDeviceToHost, x->stream));
+  k_aos_to_soa<double><<<(m.nc + 255) / 256, 256, 0, x->stream>>>(win, x->p64.W.p, m.nc, m.nt);
+  double *rout = dev ? R : x->Rtmp.p;
+  launch_chain<double>(x, x->p64, rout, true, x->mdot.p, x->wl.p);
+  if (!dev) CK(cudaMemcpyAsync(R, x->Rtmp.p, sizeof(double) * 5 * m.nc, cudaMemcpyDeviceToHost, x->stream));
   check_err(x);
   API_END
 }
@@ -334,11 +361,11 @@ int fcfd_last_stages(fcfd_ctx *x, double *grads, double *limiter, double *ghost,
     for (size_t i = 0; i < n; ++i)
       for (int j = 0; j < k; ++j) dst[i * k + j] = h[j * n + i];
   };
-  get(x->G.p, m.nc, 15, grads);
-  get(x->Lm.p, m.nc, 5, limiter);
+  get(x->p64.G.p, m.nc, 15, grads);
+  get(x->p64.Lm.p, m.nc, 5, limiter);
   if (ghost) {
     std::vector<double> h(5 * (size_t)m.nt);
-    CK(cudaMemcpy(h.data(), x->W.p, sizeof(double) * 5 * m.nt, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(h.data(), x->p64.W.p, sizeof(double) * 5 * m.nt, cudaMemcpyDeviceToHost));
     for (int g = 0; g < m.nb; ++g)
       for (int v = 0; v < 5; ++v) ghost[5 * g + v] = h[(size_t)v * m.nt + m.nc + g];
   }
@@ -357,10 +384,10 @@ int fcfd_local_dt(fcfd_ctx *x, const double *W, double cfl, int mode, double *dt
     CK(cudaMemcpyAsync(x->Win.p, W, sizeof(double) * 5 * m.nc, cudaMemcpyHostToDevice, x->stream));
     win = x->Win.p;
   }
-  k_aos_to_soa<double><<<(m.nc + 255) / 256, 256, 0, x->stream>>>(win, x->W.p, m.nc, m.nt);
+  k_aos_to_soa<double><<<(m.nc + 255) / 256, 256, 0, x->stream>>>(win, x->p64.W.p, m.nc, m.nt);
   double *out = dev ? dt : x->dt.p;
   if (mode == 1) CK(cudaMemsetAsync(x->ext.p, 0xFF, sizeof(unsigned long long), x->stream));
-  k_local_dt<double><<<(m.nc + 255) / 256, 256, 0, x->stream>>>(x->cs, m, x->W.p, out, cfl, mode == 1 ? x->ext.p : nullptr);
+  k_local_dt<double><<<(m.nc + 255) / 256, 256, 0, x->stream>>>(x->cs, m, x->p64.W.p, out, cfl, mode == 1 ? x->ext.p : nullptr);
   if (mode == 1) k_fill_min<double><<<(m.nc + 255) / 256, 256, 0, x->stream>>>(m.nc, out, x->ext.p);
   CK(cudaGetLastError());
   if (!dev) CK(cudaMemcpyAsync(dt, x->dt.p, sizeof(double) * m.nc, cudaMemcpyDeviceToHost, x->stream));
@@ -387,19 +414,20 @@ int fcfd_time_residual(fcfd_ctx *x, int reps, int flush_l2, double *out, int out
     CK(cudaEventRecord(t.ev[0], s));
     int ng = (m.nb + tb - 1) / tb;
     if (ng < 296) ng = 296;
-    k_ghost_minmax<double><<<ng, tb, 0, s>>>(x->cs, m, x->W.p, x->ext.p, x->err.p);
+    Pipe<double> &P = x->p64;
+    k_ghost_minmax<double><<<ng, tb, 0, s>>>(x->cs, m, P.W.p, x->ext.p, x->err.p);
     CK(cudaEventRecord(t.ev[1], s));
-    k_grad_limiter<double><<<(m.nc + 127) / 128, 128, 0, s>>>(x->cs, m, x->W.p, x->ext.p, x->G.p, x->Lm.p);
+    k_grad_limiter<double><<<(m.nc + 127) / 128, 128, 0, s>>>(x->cs, m, P.W.p, x->ext.p, nullptr, P.G.p, P.Lm.p);
     CK(cudaEventRecord(t.ev[2], s));
     if (m.n_outlet > 0)
-      k_outlet_rho<double><<<(m.n_outlet + 127) / 128, 128, 0, s>>>(x->cs, m, x->W.p, x->G.p, x->Lm.p, x->stale.p);
+      k_outlet_rho<double><<<(m.n_outlet + 127) / 128, 128, 0, s>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p);
     CK(cudaEventRecord(t.ev[3], s));
     if (x->viscous)
-      k_face_flux<double, true><<<(m.nf + 127) / 128, 128, 0, s>>>(x->cs, m, x->W.p, x->G.p, x->Lm.p, x->stale.p, nullptr, x->D.p, nullptr, nullptr, x->err.p);
+      k_face_flux<double, true><<<(m.nf + 127) / 128, 128, 0, s>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p, nullptr, P.D.p, nullptr, nullptr, x->err.p);
     else
-      k_face_flux<double, false><<<(m.nf + 127) / 128, 128, 0, s>>>(x->cs, m, x->W.p, x->G.p, x->Lm.p, x->stale.p, nullptr, x->D.p, nullptr, nullptr, x->err.p);
+      k_face_flux<double, false><<<(m.nf + 127) / 128, 128, 0, s>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p, nullptr, P.D.p, nullptr, nullptr, x->err.p);
     CK(cudaEventRecord(t.ev[4], s));
-    k_gather<double, false><<<(m.nc + tb - 1) / tb, tb, 0, s>>>(m, x->D.p, x->R.p);
+    k_gather<double, false><<<(m.nc + tb - 1) / tb, tb, 0, s>>>(m, P.D.p, P.R.p);
     CK(cudaEventRecord(t.ev[5], s));
     CK(cudaGetLastError());
     CK(cudaEventSynchronize(t.ev[5]));
@@ -408,6 +436,34 @@ int fcfd_time_residual(fcfd_ctx *x, int reps, int flush_l2, double *out, int out
     for (int k = 0; k < 5; ++k) { CK(cudaEventElapsedTime(&ms, t.ev[k], t.ev[k + 1])); acc[k + 1] += ms; }
   }
   for (int k = 0; k < 6 && k < out_len; ++k) out[k] = acc[k] / reps;
+  API_END
+}
+
+// Forward tangent: JV = dR/dW . V (and R if requested).
+int fcfd_jvp(fcfd_ctx *x, const double *W, const double *V, double *R, double *JV, int flags) {
+  API_BEGIN
+  if (!x || !W || !V || !JV) throw Error(FCFD_ERR_INPUT, "null argument");
+  CK(cudaSetDevice(x->device));
+  const DevMesh &m = x->dm;
+  if (!x->pjv.ready) x->pjv.alloc(m.nc, m.nf, m.nb);
+  const bool dev = flags & FCFD_DEVICE_PTRS;
+  const double *w = W, *v = V;
+  if (!dev) {
+    CK(cudaMemcpyAsync(x->Win.p, W, sizeof(double) * 5 * m.nc, cudaMemcpyHostToDevice, x->stream));
+    CK(cudaMemcpyAsync(x->Vin.p, V, sizeof(double) * 5 * m.nc, cudaMemcpyHostToDevice, x->stream));
+    w = x->Win.p; v = x->Vin.p;
+  }
+  k_seed_dual<double><<<(m.nc + 255) / 256, 256, 0, x->stream>>>(w, v, x->pjv.W.p, m.nc, m.nt);
+  launch_chain<Dual<double>>(x, x->pjv, x->pjv.R.p, false, nullptr, nullptr);
+  double *rout = R ? (dev ? R : x->Rtmp.p) : nullptr;
+  double *jout = dev ? JV : x->Vin.p;
+  k_split_dual<double><<<(m.nc + 255) / 256, 256, 0, x->stream>>>(x->pjv.R.p, rout, jout, m.nc);
+  CK(cudaGetLastError());
+  if (!dev) {
+    if (R) CK(cudaMemcpyAsync(R, x->Rtmp.p, sizeof(double) * 5 * m.nc, cudaMemcpyDeviceToHost, x->stream));
+    CK(cudaMemcpyAsync(JV, x->Vin.p, sizeof(double) * 5 * m.nc, cudaMemcpyDeviceToHost, x->stream));
+  }
+  check_err(x);
   API_END
 }
 

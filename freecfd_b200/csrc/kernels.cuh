@@ -29,6 +29,82 @@ __device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, 
 __device__ __forceinline__ float sub_rn(float a, float b) { return __fsub_rn(a, b); }
 __device__ __forceinline__ float div_rn(float a, float b) { return __fdiv_rn(a, b); }
 
+
+// ------------------------------------------------------------------ dual numbers
+// Forward tangent arithmetic: value v and directional derivative d.  Branches
+// and comparisons use the value, so a kernel instantiated on Dual computes the
+// residual's directional derivative along the seeded direction exactly
+// (hand-differentiated forward mode of the same code, no finite difference).
+template <class T>
+struct Dual {
+  T v, d;
+  __host__ __device__ Dual() : v(0), d(0) {}
+  __host__ __device__ Dual(double x) : v(T(x)), d(0) {}
+  __host__ __device__ Dual(T x, T y) : v(x), d(y) {}
+};
+template <class T> __host__ __device__ __forceinline__ Dual<T> operator+(const Dual<T> &a, const Dual<T> &b) { return Dual<T>(a.v + b.v, a.d + b.d); }
+template <class T> __host__ __device__ __forceinline__ Dual<T> operator-(const Dual<T> &a, const Dual<T> &b) { return Dual<T>(a.v - b.v, a.d - b.d); }
+template <class T> __host__ __device__ __forceinline__ Dual<T> operator-(const Dual<T> &a) { return Dual<T>(-a.v, -a.d); }
+template <class T> __host__ __device__ __forceinline__ Dual<T> operator*(const Dual<T> &a, const Dual<T> &b) { return Dual<T>(a.v * b.v, a.d * b.v + a.v * b.d); }
+template <class T> __host__ __device__ __forceinline__ Dual<T> operator/(const Dual<T> &a, const Dual<T> &b) {
+  const T q = a.v / b.v;
+  return Dual<T>(q, (a.d - q * b.d) / b.v);
+}
+template <class T> __host__ __device__ __forceinline__ Dual<T> operator+(const Dual<T> &a, double b) { return Dual<T>(a.v + T(b), a.d); }
+template <class T> __host__ __device__ __forceinline__ Dual<T> operator+(double a, const Dual<T> &b) { return Dual<T>(T(a) + b.v, b.d); }
+template <class T> __host__ __device__ __forceinline__ Dual<T> operator-(const Dual<T> &a, double b) { return Dual<T>(a.v - T(b), a.d); }
+template <class T> __host__ __device__ __forceinline__ Dual<T> operator-(double a, const Dual<T> &b) { return Dual<T>(T(a) - b.v, -b.d); }
+template <class T> __host__ __device__ __forceinline__ Dual<T> operator*(const Dual<T> &a, double b) { return Dual<T>(a.v * T(b), a.d * T(b)); }
+template <class T> __host__ __device__ __forceinline__ Dual<T> operator*(double a, const Dual<T> &b) { return Dual<T>(T(a) * b.v, T(a) * b.d); }
+template <class T> __host__ __device__ __forceinline__ Dual<T> operator/(const Dual<T> &a, double b) { return Dual<T>(a.v / T(b), a.d / T(b)); }
+template <class T> __host__ __device__ __forceinline__ Dual<T> operator/(double a, const Dual<T> &b) {
+  const T q = T(a) / b.v;
+  return Dual<T>(q, -q * b.d / b.v);
+}
+#define FCFD_DUAL_CMP(op)                                                                                                  \
+  template <class T> __host__ __device__ __forceinline__ bool operator op(const Dual<T> &a, const Dual<T> &b) { return a.v op b.v; } \
+  template <class T> __host__ __device__ __forceinline__ bool operator op(const Dual<T> &a, double b) { return a.v op T(b); }        \
+  template <class T> __host__ __device__ __forceinline__ bool operator op(double a, const Dual<T> &b) { return T(a) op b.v; }
+FCFD_DUAL_CMP(<)
+FCFD_DUAL_CMP(>)
+FCFD_DUAL_CMP(<=)
+FCFD_DUAL_CMP(>=)
+FCFD_DUAL_CMP(==)
+FCFD_DUAL_CMP(!=)
+#undef FCFD_DUAL_CMP
+template <class T> __host__ __device__ __forceinline__ Dual<T> sqrt(const Dual<T> &a) {
+  const T s = sqrt(a.v);
+  return Dual<T>(s, a.d / (T(2) * s));
+}
+template <class T> __host__ __device__ __forceinline__ Dual<T> fabs(const Dual<T> &a) { return a.v < T(0) ? -a : a; }
+template <class T> __host__ __device__ __forceinline__ Dual<T> pow(const Dual<T> &a, double e) {
+  const T p = pow(a.v, T(e));
+  return Dual<T>(p, a.d == T(0) ? T(0) : T(e) * p / a.v * a.d);
+}
+template <class T> __host__ __device__ __forceinline__ Dual<T> tanh(const Dual<T> &a) {
+  const T t = tanh(a.v);
+  return Dual<T>(t, (T(1) - t * t) * a.d);
+}
+using ::fabs;
+using ::pow;
+using ::sqrt;
+using ::tanh;
+__device__ __forceinline__ Dual<double> mul_rn(Dual<double> a, Dual<double> b) { return Dual<double>(__dmul_rn(a.v, b.v), a.d * b.v + a.v * b.d); }
+__device__ __forceinline__ Dual<double> add_rn(Dual<double> a, Dual<double> b) { return Dual<double>(__dadd_rn(a.v, b.v), a.d + b.d); }
+__device__ __forceinline__ Dual<double> sub_rn(Dual<double> a, Dual<double> b) { return Dual<double>(__dsub_rn(a.v, b.v), a.d - b.d); }
+__device__ __forceinline__ Dual<double> div_rn(Dual<double> a, Dual<double> b) {
+  const double q = __ddiv_rn(a.v, b.v);
+  return Dual<double>(q, (a.d - q * b.d) / b.v);
+}
+__host__ __device__ __forceinline__ double val(double x) { return x; }
+__host__ __device__ __forceinline__ float val(float x) { return x; }
+template <class T> __host__ __device__ __forceinline__ T val(const Dual<T> &x) { return x.v; }
+__host__ __device__ __forceinline__ double tan_of(double) { return 0.; }
+template <class S> struct Mk;
+template <> struct Mk<double> { __host__ __device__ static double of(double v, double) { return v; } };
+template <class T> struct Mk<Dual<T>> { __host__ __device__ static Dual<T> of(double v, double d) { return Dual<T>(T(v), T(d)); } };
+template <class T> __host__ __device__ __forceinline__ T tan_of(const Dual<T> &x) { return x.d; }
+
 // std::max / std::min semantics: max(a,b) = (a<b)?b:a, min(a,b) = (b<a)?b:a
 template <class S> __host__ __device__ __forceinline__ S smax(const S &a, const S &b) { return (a < b) ? b : a; }
 template <class S> __host__ __device__ __forceinline__ S smin(const S &a, const S &b) { return (b < a) ? b : a; }
@@ -300,7 +376,7 @@ __global__ void k_ghost_minmax(DevCase cs, DevMesh m, S *__restrict__ W, unsigne
     // grid-stride extrema over interior cells, warp-reduced then one atomic per warp
     double mx[4] = {-INFINITY, -INFINITY, -INFINITY, -INFINITY}, mn[4] = {INFINITY, INFINITY, INFINITY, INFINITY};
     for (int c = tid; c < m.nc; c += gridDim.x * blockDim.x) {
-      double p = (double)W[c], u = (double)W[nt + c], v = (double)W[2 * nt + c];
+      double p = val(W[c]), u = val(W[nt + c]), v = val(W[2 * nt + c]);
       mx[0] = fmax(mx[0], p); mn[0] = fmin(mn[0], p);
       mx[1] = fmax(mx[1], u); mn[1] = fmin(mn[1], u);
       mx[2] = fmax(mx[2], v); mn[2] = fmin(mn[2], v);
@@ -324,12 +400,53 @@ __global__ void k_ghost_minmax(DevCase cs, DevMesh m, S *__restrict__ W, unsigne
   }
 }
 
+// First cell attaining each extreme (tangent runs): slots as in k_ghost_minmax.
+template <class S>
+__global__ void k_argext(DevMesh m, const S *__restrict__ W, const unsigned long long *__restrict__ ext, int *__restrict__ argx) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= m.nc) return;
+  const int nt = m.nt;
+  const double p = val(W[c]), u = val(W[nt + c]), v = val(W[2 * nt + c]);
+  if (p == okey_inv(ext[0])) atomicMin(&argx[0], c);
+  if (p == okey_inv(ext[1])) atomicMin(&argx[1], c);
+  if (u == okey_inv(ext[2])) atomicMin(&argx[2], c);
+  if (u == okey_inv(ext[3])) atomicMin(&argx[3], c);
+  if (v == okey_inv(ext[4])) atomicMin(&argx[4], c);
+  if (v == okey_inv(ext[5])) atomicMin(&argx[5], c);
+  if (c < m.nc - 1) {
+    if (p == okey_inv(ext[6])) atomicMin(&argx[6], c);
+    if (p == okey_inv(ext[7])) atomicMin(&argx[7], c);
+  }
+}
+
+// Combine a value array and a tangent array (AoS [nc][5]) into SoA duals.
+template <class T>
+__global__ void k_seed_dual(const double *__restrict__ w, const double *__restrict__ dw, Dual<T> *__restrict__ W, int nc, int nt) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nc) return;
+#pragma unroll
+  for (int v = 0; v < 5; ++v) W[v * nt + c] = Dual<T>(T(w[5 * c + v]), T(dw[5 * c + v]));
+}
+
+// Split a dual SoA result into value and tangent AoS arrays.
+template <class T>
+__global__ void k_split_dual(const Dual<T> *__restrict__ R, double *__restrict__ r, double *__restrict__ dr, int nc) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nc) return;
+#pragma unroll
+  for (int v = 0; v < 5; ++v) {
+    const Dual<T> x = R[v * nc + c];
+    if (r) r[5 * c + v] = double(x.v);
+    dr[5 * c + v] = double(x.d);
+  }
+}
+
 // LSQ gradient (bit-exact restatement of Variable::cell_gradient over the
 // lsqr_grad_map weights) + limiter, one thread per interior cell.
 template <class S>
 __global__ void __launch_bounds__(128) k_grad_limiter(DevCase cs, DevMesh m, const S *__restrict__ W,
-                                                      const unsigned long long *__restrict__ ext, S *__restrict__ G,
-                                                      S *__restrict__ Lm) {
+                                                      const unsigned long long *__restrict__ ext, const int *__restrict__ argx,
+                                                      S *__restrict__ G, S *__restrict__ Lm) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   const int nc = m.nc, nt = m.nt;
   if (c >= nc) return;
@@ -411,26 +528,35 @@ __global__ void __launch_bounds__(128) k_grad_limiter(DevCase cs, DevMesh m, con
           umin[v] = smin(umin[v], x);
         }
       }
-      double eps2[5] = {0, 0, 0, 0, 0};
+      S eps2[5] = {S(0.), S(0.), S(0.), S(0.), S(0.)};
       if (cs.limiter == 1) {
         // find_min_max with its index quirks: q[3] uses q[4]'s running value,
-        // q[4] tracks p starting from T of cell 0
+        // q[4] tracks p starting from T of cell 0.  std::max keeps the earlier
+        // operand on ties, so each extreme belongs to a definite cell; `argx`
+        // (tangent runs only) holds the first cell attaining slots 0..7.
         const double pmax = okey_inv(ext[0]), pmin = okey_inv(ext[1]);
-        const double T0 = (double)W[4 * nt + 0], wl = (double)W[3 * nt + nc - 1];
-        double qmax[5], qmin[5];
-        qmax[0] = pmax; qmin[0] = pmin;
-        qmax[1] = okey_inv(ext[2]); qmin[1] = okey_inv(ext[3]);
-        qmax[2] = okey_inv(ext[4]); qmin[2] = okey_inv(ext[5]);
-        double pmax_lt = nc > 1 ? okey_inv(ext[6]) : -INFINITY, pmin_lt = nc > 1 ? okey_inv(ext[7]) : INFINITY;
-        double q4max_prev = T0, q4min_prev = T0;
-        if (nc > 1) { q4max_prev = smax(T0, pmax_lt); q4min_prev = smin(T0, pmin_lt); }
-        qmax[3] = smax(q4max_prev, wl);
-        qmin[3] = smin(q4min_prev, wl);
-        qmax[4] = smax(T0, pmax); qmin[4] = smin(T0, pmin);
+        const double T0 = val(W[4 * nt + 0]), wl = val(W[3 * nt + nc - 1]);
+        const double tT0 = tan_of(W[4 * nt + 0]), twl = tan_of(W[3 * nt + nc - 1]);
+        auto tp = [&](int slot) { return argx ? tan_of(W[argx[slot]]) : 0.; };
+        auto tv = [&](int var, int slot) { return argx ? tan_of(W[var * nt + argx[slot]]) : 0.; };
+        double qmax[5], qmin[5], tmax[5], tmin[5];
+        qmax[0] = pmax; tmax[0] = tp(0); qmin[0] = pmin; tmin[0] = tp(1);
+        qmax[1] = okey_inv(ext[2]); tmax[1] = tv(1, 2); qmin[1] = okey_inv(ext[3]); tmin[1] = tv(1, 3);
+        qmax[2] = okey_inv(ext[4]); tmax[2] = tv(2, 4); qmin[2] = okey_inv(ext[5]); tmin[2] = tv(2, 5);
+        double q4M = T0, t4M = tT0, q4m = T0, t4m = tT0;  // running q[4] before the last cell
+        if (nc > 1) {
+          const double a = okey_inv(ext[6]), b = okey_inv(ext[7]);
+          if (T0 < a) { q4M = a; t4M = tp(6); }
+          if (b < T0) { q4m = b; t4m = tp(7); }
+        }
+        qmax[3] = q4M; tmax[3] = t4M; if (q4M < wl) { qmax[3] = wl; tmax[3] = twl; }
+        qmin[3] = q4m; tmin[3] = t4m; if (wl < q4m) { qmin[3] = wl; tmin[3] = twl; }
+        qmax[4] = T0; tmax[4] = tT0; if (T0 < pmax) { qmax[4] = pmax; tmax[4] = tp(0); }
+        qmin[4] = T0; tmin[4] = tT0; if (pmin < T0) { qmin[4] = pmin; tmin[4] = tp(1); }
 #pragma unroll
         for (int v = 0; v < 5; ++v) {
-          const double eps = fabs(qmax[v] - qmin[v]) / cs.Lref;
-          const double e = 1.e-6 * cs.K * eps;
+          const S eps = fabs(Mk<S>::of(qmax[v], tmax[v]) - Mk<S>::of(qmin[v], tmin[v])) / cs.Lref;
+          const S e = 1.e-6 * cs.K * eps;
           eps2[v] = e * e;
         }
       }
@@ -446,7 +572,7 @@ __global__ void __launch_bounds__(128) k_grad_limiter(DevCase cs, DevMesh m, con
             if (dM > 0.) dP = sub_rn(umax[v], dP);
             else if (dM < 0.) dP = sub_rn(umin[v], dP);
             const S dP2 = mul_rn(dP, dP), dM2 = mul_rn(dM, dM);
-            const S e2 = S(eps2[v]);
+            const S e2 = eps2[v];
             if (dM != 0.) {
               const S num = add_rn(add_rn(dP2, e2), mul_rn(mul_rn(S(2.), dM), dP));
               const S den = add_rn(add_rn(add_rn(dP2, mul_rn(S(2.), dM2)), mul_rn(dM, dP)), e2);
@@ -747,9 +873,9 @@ __global__ void k_local_dt(DevCase cs, DevMesh m, const S *__restrict__ W, S *__
   const int nt = m.nt;
   const S p = W[c], u = W[nt + c], v = W[2 * nt + c], w = W[3 * nt + c], T = W[4 * nt + c];
   const S a = sound(cs, p, T);
-  const S val = cfl * m.c_len[c] / (sqrt(u * u + v * v + w * w) + a);
-  dt[c] = val;
-  if (minkey) atomicMin(minkey, okey((double)val));
+  const S v_dt = cfl * m.c_len[c] / (sqrt(u * u + v * v + w * w) + a);
+  dt[c] = v_dt;
+  if (minkey) atomicMin(minkey, okey(val(v_dt)));
 }
 
 template <class S>

@@ -127,6 +127,25 @@ class NavierStokes:
         check(lib.fcfd_residual(self.h, pw, pr, fw))
         return out
 
+    def jvp(self, W, V, with_residual: bool = False):
+        """Directional derivative (dR/dW).V of the residual (forward tangent)."""
+        nc = self.mesh.nc
+        host = isinstance(W, np.ndarray)
+        if host:
+            W = np.ascontiguousarray(W, dtype=np.float64)
+            V = np.ascontiguousarray(V, dtype=np.float64)
+            JV = np.empty((nc, 5))
+            R = np.empty((nc, 5)) if with_residual else None
+        else:
+            JV = W.new_empty((nc, 5))
+            R = W.new_empty((nc, 5)) if with_residual else None
+        pw, fw = _ptr(W)
+        pv, _ = _ptr(V)
+        pj, _ = _ptr(JV)
+        pr = _ptr(R)[0] if R is not None else None
+        check(lib.fcfd_jvp(self.h, pw, pv, pr, pj, fw))
+        return (R, JV) if with_residual else JV
+
     def stages(self):
         m = self.mesh
         out = dict(grads=np.empty((m.nc, 15)), limiter=np.empty((m.nc, 5)), ghost=np.empty((m.nghost, 5)),

@@ -121,6 +121,14 @@ int fcfd_last_stages(fcfd_ctx *ctx, double *grads, double *limiter, double *ghos
  * mode 0 = CFL_LOCAL (dt_c = cfl*l_c/(|V|+a)), mode 1 = CFL_MAX (global min). */
 int fcfd_local_dt(fcfd_ctx *ctx, const double *W, double cfl, int mode, double *dt, int flags);
 
+/* Forward-tangent (JVP) of the residual: JV = (dR/dW) V for a direction
+ * V[nc][5], evaluated by the same kernels on dual numbers (exact derivative
+ * of the discrete residual, not a finite difference).  Optionally returns
+ * R(W) too (R may be NULL).  Replaces the finite-difference Jacobian columns
+ * of NavierStokes::get_jacobians (ns_assemble_linear_system.cc:197-267) in a
+ * matrix-free Newton-Krylov solve. */
+int fcfd_jvp(fcfd_ctx *ctx, const double *W, const double *V, double *R, double *JV, int flags);
+
 /* Device timing of the residual: runs `reps` residual evaluations on the
  * resident state (captured in one CUDA graph) and returns per-kernel average
  * milliseconds: out[0] total per residual, out[1..] per kernel (see fcfd.cu). */
