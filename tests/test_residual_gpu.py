@@ -16,7 +16,7 @@ import numpy as np
 import pytest
 
 from freecfd_b200 import cases
-from tests.util import SMALL, build_pair, rel_err
+from tests.util import SMALL, build_pair, flux_scale, rel_err
 
 TOL = 1e-12
 BITWISE = {"wedge", "hypersonic"}
@@ -58,7 +58,11 @@ def test_residual_parity(family, flux, limiter, oracle_mod, fb):
     err = rel_err(R, ref["R"])
     assert err.max() <= TOL, err
     assert rel_err(st["mdot"], ref["mdot"]).max() <= TOL
-    assert np.array_equal(st["weightL"], ref["weightL"])
+    # weightL is the upwind side (0 / 0.5 / 1) chosen by the sign of the mass
+    # flux; where that flux is at rounding level (symmetry and slip faces) the
+    # side is a rounding decision and mdot*weightL vanishes either way.
+    big = np.abs(ref["mdot"]) > 1e-9 * np.abs(ref["mdot"]).max()
+    assert np.array_equal(st["weightL"][big], ref["weightL"][big])
 
 
 @pytest.mark.gpu
@@ -68,7 +72,10 @@ def test_uniform_freestream(family, oracle_mod, fb):
     case = SMALL[family]()
     o, cs, m, ns = _ctx(case, oracle_mod, fb)
     W = np.tile(np.asarray(case.freestream), (m.nc, 1))
-    assert rel_err(ns.residual(W), o.residual(W)).max() <= TOL
+    R, ref = ns.residual(W), o.residual(W)
+    # the residual of a uniform state is mostly cancellation noise: bound the
+    # difference by the size of the cancelling face fluxes
+    assert np.abs(R - ref).max() <= TOL * flux_scale(case, m.geometry())
 
 
 @pytest.mark.gpu
@@ -120,5 +127,5 @@ def test_conservation_full_cylinder(oracle_mod, fb):
     R = ns.residual(case.state)
     ref = o.residual(case.state)
     s, sr = R.sum(axis=0), ref.sum(axis=0)
-    scale = np.abs(ref).sum(axis=0)
+    scale = np.maximum(np.abs(ref).sum(axis=0), 1e-6 * np.abs(ref).sum(axis=0).max())
     assert (np.abs(s - sr) / scale).max() < 1e-12

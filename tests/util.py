@@ -24,9 +24,18 @@ def build_pair(case, oracle_mod, fb):
     return o, cs, m
 
 
-def rel_err(a, b):
-    """Normwise relative error per equation column: max|a-b| / max|b|."""
+def rel_err(a, b, floor=1e-300):
+    """Normwise relative error per equation column: max|a-b| / max(max|b|, floor).
+
+    ``floor`` keeps columns that are pure rounding noise (e.g. the z-momentum
+    of a 2-D case) from being divided by ~0."""
     a = np.asarray(a).reshape(-1, np.asarray(a).shape[-1]) if np.asarray(a).ndim > 1 else np.asarray(a)[:, None]
     b = np.asarray(b).reshape(a.shape)
-    scale = np.maximum(np.abs(b).max(axis=0), 1e-300)
+    scale = np.maximum(np.abs(b).max(axis=0), floor)
     return (np.abs(a - b).max(axis=0) / scale)
+
+
+def flux_scale(case, mesh_geometry):
+    """Magnitude of one face's pressure flux, p_inf * max face area: the size of
+    the terms whose cancellation produces a residual."""
+    return abs(case.freestream[0]) * float(np.max(mesh_geometry["face_area"]))
