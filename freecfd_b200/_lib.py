@@ -25,7 +25,7 @@ EXPORTED = [
     "fcfd_mesh_create", "fcfd_mesh_destroy", "fcfd_mesh_sizes", "fcfd_mesh_connectivity", "fcfd_mesh_geometry",
     "fcfd_mesh_lsq",
     "fcfd_ctx_create", "fcfd_ctx_destroy", "fcfd_residual", "fcfd_last_stages", "fcfd_local_dt",
-    "fcfd_time_residual", "fcfd_point_flux", "fcfd_jvp",
+    "fcfd_time_residual", "fcfd_point_flux", "fcfd_jvp", "fcfd_newton_solve",
 ]
 
 
@@ -49,6 +49,20 @@ class _RawMesh(ctypes.Structure):
                 ("n_cells", ctypes.c_int32), ("conn_index", ctypes.POINTER(ctypes.c_int32)),
                 ("conn", ctypes.POINTER(ctypes.c_int32)), ("n_bc", ctypes.c_int32),
                 ("bc_index", ctypes.POINTER(ctypes.c_int32)), ("bc_nodes", ctypes.POINTER(ctypes.c_int32))]
+
+
+class NewtonOpts(ctypes.Structure):
+    _fields_ = [("max_newton", ctypes.c_int32), ("tol", ctypes.c_double), ("krylov_dim", ctypes.c_int32),
+                ("krylov_rtol", ctypes.c_double), ("cfl0", ctypes.c_double), ("cfl_growth", ctypes.c_double),
+                ("cfl_max", ctypes.c_double), ("cfl_mode", ctypes.c_int32), ("ser_exponent", ctypes.c_double),
+                ("jvp_mode", ctypes.c_int32), ("fp32_krylov", ctypes.c_int32), ("max_seconds", ctypes.c_double)]
+
+
+class NewtonReport(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int32), ("newton_iterations", ctypes.c_int32),
+                ("krylov_iterations", ctypes.c_int32), ("pad", ctypes.c_int32), ("res0", ctypes.c_double),
+                ("res_final", ctypes.c_double), ("wall_seconds", ctypes.c_double), ("last_cfl", ctypes.c_double),
+                ("history", ctypes.c_double * 512)]
 
 
 def _load():
@@ -77,6 +91,7 @@ def _load():
     L.fcfd_last_stages.argtypes = [vp, dp, dp, dp, dp, dp]
     L.fcfd_local_dt.argtypes = [vp, vp, ctypes.c_double, ctypes.c_int, vp, ctypes.c_int]
     L.fcfd_jvp.argtypes = [vp, vp, vp, vp, vp, ctypes.c_int]
+    L.fcfd_newton_solve.argtypes = [vp, dp, ctypes.POINTER(NewtonOpts), ctypes.POINTER(NewtonReport)]
     L.fcfd_time_residual.argtypes = [vp, ctypes.c_int, ctypes.c_int, dp, ctypes.c_int]
     L.fcfd_point_flux.argtypes = [ctypes.c_int, dp, dp, dp, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                   ctypes.c_double, ctypes.c_double, dp, dp]

@@ -1,0 +1,106 @@
+// Device context shared by the residual (fcfd.cu) and the Newton-Krylov
+// solver (newton.cu).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+#include <type_traits>
+#include <vector>
+
+#include "internal.hpp"
+#include "kernels.cuh"
+
+namespace fcfd {
+
+#define CK(call)                                                                                        \
+  do {                                                                                                  \
+    cudaError_t e_ = (call);                                                                            \
+    if (e_ != cudaSuccess) throw Error(FCFD_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+template <class T>
+struct DBuf {
+  T *p = nullptr;
+  size_t n = 0;
+  void alloc(size_t count) {
+    free();
+    n = count;
+    if (count) CK(cudaMalloc(&p, count * sizeof(T)));
+  }
+  void upload(const std::vector<T> &v) {
+    alloc(v.size());
+    if (n) CK(cudaMemcpy(p, v.data(), n * sizeof(T), cudaMemcpyHostToDevice));
+  }
+  void free() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  ~DBuf() { free(); }
+};
+
+// [n][k] AoS host array -> [k][n] SoA
+template <class T>
+static std::vector<T> soa(const std::vector<T> &a, size_t n, int k) {
+  std::vector<T> o(a.size());
+  for (size_t i = 0; i < n; ++i)
+    for (int j = 0; j < k; ++j) o[j * n + i] = a[i * k + j];
+  return o;
+}
+
+struct Timing {
+  cudaEvent_t ev[8];
+  Timing() { for (auto &e : ev) cudaEventCreate(&e); }
+  ~Timing() { for (auto &e : ev) cudaEventDestroy(e); }
+};
+
+}  // namespace fcfd
+
+
+namespace fcfd {
+// Typed working buffers of one residual chain (scalar S = double, or a dual
+// number for tangent runs).
+template <class S>
+struct Pipe {
+  DBuf<S> W, G, Lm, D, stale, R;
+  bool ready = false;
+  void alloc(int nc, int nf, int nb) {
+    const int nt = nc + nb;
+    W.alloc(5 * (size_t)nt); G.alloc(15 * (size_t)nc); Lm.alloc(5 * (size_t)nc); D.alloc(5 * (size_t)nf);
+    stale.alloc(nb > 0 ? nb : 1); R.alloc(5 * (size_t)nc);
+    CK(cudaMemset(stale.p, 0, sizeof(S) * (nb > 0 ? nb : 1)));
+    ready = true;
+  }
+};
+}  // namespace fcfd
+
+using namespace fcfd;  // internal header: the context mirrors the device types
+
+struct fcfd_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  DevCase cs{};
+  DevMesh dm{};
+  const fcfd_mesh *mesh = nullptr;
+  bool viscous = false;
+  // mesh arrays
+  DBuf<int> f_parent, f_neighbor, f_bc, cf_index, cf_list, st_index, st_keys, bface, outlet;
+  DBuf<double> f_n, f_area, f_x, f_w, c_x, c_len, st_cof, st_self;
+  // state arrays
+  Pipe<double> p64;
+  Pipe<Dual<double>> pjv;
+  DBuf<double> Win, Vin, Rtmp, dt, mdot, wl;
+  DBuf<unsigned long long> ext;
+  DBuf<int> err, argx;
+  DBuf<unsigned char> flush;
+  int n_outlet = 0;
+  cudaGraphExec_t graph = nullptr;
+};
+
+
+namespace fcfd {
+constexpr int kExtremaBlocks = 296;  // 2 x 148 SMs
+template <class S>
+void launch_chain(fcfd_ctx *x, Pipe<S> &P, S *Rout, bool aos_out, S *mo, S *wo);
+int check_err(fcfd_ctx *x);
+}  // namespace fcfd

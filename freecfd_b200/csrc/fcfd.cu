@@ -10,8 +10,7 @@
 #include <type_traits>
 #include <vector>
 
-#include "internal.hpp"
-#include "kernels.cuh"
+#include "ctx.hpp"
 
 namespace fcfd {
 
@@ -25,103 +24,17 @@ fcfd_mesh *build_mesh(const fcfd_raw_mesh &raw, fcfd_case &cs);
 static thread_local std::string g_last_error;
 void set_last_error(const std::string &m) { g_last_error = m; }
 
-#define CK(call)                                                                                        \
-  do {                                                                                                  \
-    cudaError_t e_ = (call);                                                                            \
-    if (e_ != cudaSuccess) throw Error(FCFD_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
-  } while (0)
-
-template <class T>
-struct DBuf {
-  T *p = nullptr;
-  size_t n = 0;
-  void alloc(size_t count) {
-    free();
-    n = count;
-    if (count) CK(cudaMalloc(&p, count * sizeof(T)));
-  }
-  void upload(const std::vector<T> &v) {
-    alloc(v.size());
-    if (n) CK(cudaMemcpy(p, v.data(), n * sizeof(T), cudaMemcpyHostToDevice));
-  }
-  void free() {
-    if (p) cudaFree(p);
-    p = nullptr;
-    n = 0;
-  }
-  ~DBuf() { free(); }
-};
-
-// [n][k] AoS host array -> [k][n] SoA
-template <class T>
-static std::vector<T> soa(const std::vector<T> &a, size_t n, int k) {
-  std::vector<T> o(a.size());
-  for (size_t i = 0; i < n; ++i)
-    for (int j = 0; j < k; ++j) o[j * n + i] = a[i * k + j];
-  return o;
-}
-
-struct Timing {
-  cudaEvent_t ev[8];
-  Timing() { for (auto &e : ev) cudaEventCreate(&e); }
-  ~Timing() { for (auto &e : ev) cudaEventDestroy(e); }
-};
-
-}  // namespace fcfd
-
-using namespace fcfd;
-
-namespace fcfd {
-// Typed working buffers of one residual chain (scalar S = double, or a dual
-// number for tangent runs).
 template <class S>
-struct Pipe {
-  DBuf<S> W, G, Lm, D, stale, R;
-  bool ready = false;
-  void alloc(int nc, int nf, int nb) {
-    const int nt = nc + nb;
-    W.alloc(5 * (size_t)nt); G.alloc(15 * (size_t)nc); Lm.alloc(5 * (size_t)nc); D.alloc(5 * (size_t)nf);
-    stale.alloc(nb > 0 ? nb : 1); R.alloc(5 * (size_t)nc);
-    CK(cudaMemset(stale.p, 0, sizeof(S) * (nb > 0 ? nb : 1)));
-    ready = true;
-  }
-};
-}  // namespace fcfd
-
-struct fcfd_ctx {
-  int device = 0;
-  cudaStream_t stream = nullptr;
-  DevCase cs{};
-  DevMesh dm{};
-  const fcfd_mesh *mesh = nullptr;
-  bool viscous = false;
-  // mesh arrays
-  DBuf<int> f_parent, f_neighbor, f_bc, cf_index, cf_list, st_index, st_keys, bface, outlet;
-  DBuf<double> f_n, f_area, f_x, f_w, c_x, c_len, st_cof, st_self;
-  // state arrays
-  Pipe<double> p64;
-  Pipe<Dual<double>> pjv;
-  DBuf<double> Win, Vin, Rtmp, dt, mdot, wl;
-  DBuf<unsigned long long> ext;
-  DBuf<int> err, argx;
-  DBuf<unsigned char> flush;
-  int n_outlet = 0;
-  cudaGraphExec_t graph = nullptr;
-};
-
-namespace fcfd {
-
-template <class S>
-static void launch_chain(fcfd_ctx *x, Pipe<S> &P, S *Rout, bool aos_out, S *mo, S *wo) {
+void launch_chain(fcfd_ctx *x, Pipe<S> &P, S *Rout, bool aos_out, S *mo, S *wo) {
   const DevMesh &m = x->dm;
   cudaStream_t s = x->stream;
   const int tb = 256;
   // extrema slots: even = max (start at key 0), odd = min (start at all ones)
   CK(cudaMemsetAsync(x->ext.p, 0x00, 8 * sizeof(unsigned long long), s));
   for (int k = 1; k < 8; k += 2) CK(cudaMemsetAsync(x->ext.p + k, 0xFF, sizeof(unsigned long long), s));
-  int ng = (m.nb + tb - 1) / tb;
-  if (ng < 296) ng = 296;
-  k_ghost_minmax<S><<<ng, tb, 0, s>>>(x->cs, m, P.W.p, x->ext.p, x->err.p);
+  const bool need_ext = x->cs.limiter == 1 && x->cs.order != 1;
+  const int ng = (m.nb + tb - 1) / tb + (need_ext ? kExtremaBlocks : 0);
+  if (ng > 0) k_ghost_minmax<S><<<ng, tb, 0, s>>>(x->cs, m, P.W.p, need_ext ? x->ext.p : nullptr, x->err.p);
   const int *argx = nullptr;
   if (!std::is_same<S, double>::value && x->cs.limiter == 1 && x->cs.order != 1) {
     CK(cudaMemsetAsync(x->argx.p, 0x7F, 8 * sizeof(int), s));
@@ -142,7 +55,7 @@ static void launch_chain(fcfd_ctx *x, Pipe<S> &P, S *Rout, bool aos_out, S *mo, 
   CK(cudaGetLastError());
 }
 
-static int check_err(fcfd_ctx *x) {
+int check_err(fcfd_ctx *x) {
   int h = 0;
   CK(cudaMemcpyAsync(&h, x->err.p, sizeof(int), cudaMemcpyDeviceToHost, x->stream));
   CK(cudaStreamSynchronize(x->stream));
@@ -154,7 +67,12 @@ static int check_err(fcfd_ctx *x) {
   return 0;
 }
 
+template void launch_chain<double>(fcfd_ctx *, Pipe<double> &, double *, bool, double *, double *);
+template void launch_chain<Dual<double>>(fcfd_ctx *, Pipe<Dual<double>> &, Dual<double> *, bool, Dual<double> *, Dual<double> *);
+
 }  // namespace fcfd
+
+using namespace fcfd;
 
 #define API_BEGIN try {
 #define API_END                                  \
@@ -412,10 +330,10 @@ int fcfd_time_residual(fcfd_ctx *x, int reps, int flush_l2, double *out, int out
     CK(cudaMemsetAsync(x->ext.p, 0x00, 8 * sizeof(unsigned long long), s));
     for (int k = 1; k < 8; k += 2) CK(cudaMemsetAsync(x->ext.p + k, 0xFF, sizeof(unsigned long long), s));
     CK(cudaEventRecord(t.ev[0], s));
-    int ng = (m.nb + tb - 1) / tb;
-    if (ng < 296) ng = 296;
+    const bool need_ext = x->cs.limiter == 1 && x->cs.order != 1;
+    const int ng = (m.nb + tb - 1) / tb + (need_ext ? kExtremaBlocks : 0);
     Pipe<double> &P = x->p64;
-    k_ghost_minmax<double><<<ng, tb, 0, s>>>(x->cs, m, P.W.p, x->ext.p, x->err.p);
+    if (ng > 0) k_ghost_minmax<double><<<ng, tb, 0, s>>>(x->cs, m, P.W.p, need_ext ? x->ext.p : nullptr, x->err.p);
     CK(cudaEventRecord(t.ev[1], s));
     k_grad_limiter<double><<<(m.nc + 127) / 128, 128, 0, s>>>(x->cs, m, P.W.p, x->ext.p, nullptr, P.G.p, P.Lm.p);
     CK(cudaEventRecord(t.ev[2], s));

@@ -358,9 +358,11 @@ __device__ __forceinline__ double okey_inv(unsigned long long k) {
 // min v, max p over cells < nc-1, min p over cells < nc-1 (ordered keys).
 template <class S>
 __global__ void k_ghost_minmax(DevCase cs, DevMesh m, S *__restrict__ W, unsigned long long *__restrict__ ext, int *err) {
-  const int tid = blockIdx.x * blockDim.x + threadIdx.x;
   const int nt = m.nt;
-  if (tid < m.nb) {
+  const int ghost_blocks = (m.nb + blockDim.x - 1) / blockDim.x;
+  if ((int)blockIdx.x < ghost_blocks) {
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid >= m.nb) return;
     const int f = m.bface[tid];
     const int pa = m.f_parent[f];
     const int b = m.f_bc[f];
@@ -371,32 +373,38 @@ __global__ void k_ghost_minmax(DevCase cs, DevMesh m, S *__restrict__ W, unsigne
     apply_bc(cs, cs.bc[b], L, R, n, err);
     const int g = m.nc + tid;
     W[g] = R.p; W[nt + g] = R.V[0]; W[2 * nt + g] = R.V[1]; W[3 * nt + g] = R.V[2]; W[4 * nt + g] = R.T;
+    return;
   }
-  if (ext) {
-    // grid-stride extrema over interior cells, warp-reduced then one atomic per warp
-    double mx[4] = {-INFINITY, -INFINITY, -INFINITY, -INFINITY}, mn[4] = {INFINITY, INFINITY, INFINITY, INFINITY};
-    for (int c = tid; c < m.nc; c += gridDim.x * blockDim.x) {
-      double p = val(W[c]), u = val(W[nt + c]), v = val(W[2 * nt + c]);
-      mx[0] = fmax(mx[0], p); mn[0] = fmin(mn[0], p);
-      mx[1] = fmax(mx[1], u); mn[1] = fmin(mn[1], u);
-      mx[2] = fmax(mx[2], v); mn[2] = fmin(mn[2], v);
-      if (c < m.nc - 1) { mx[3] = fmax(mx[3], p); mn[3] = fmin(mn[3], p); }
-    }
+  if (!ext) return;
+  // The remaining blocks reduce the interior extrema: grid-stride, warp
+  // shuffles, a shared-memory block reduction and one atomic per block/slot.
+  const int eb = blockIdx.x - ghost_blocks, neb = gridDim.x - ghost_blocks;
+  double mx[4] = {-INFINITY, -INFINITY, -INFINITY, -INFINITY}, mn[4] = {INFINITY, INFINITY, INFINITY, INFINITY};
+  for (int c = eb * blockDim.x + threadIdx.x; c < m.nc; c += neb * blockDim.x) {
+    const double p = val(W[c]), u = val(W[nt + c]), v = val(W[2 * nt + c]);
+    mx[0] = fmax(mx[0], p); mn[0] = fmin(mn[0], p);
+    mx[1] = fmax(mx[1], u); mn[1] = fmin(mn[1], u);
+    mx[2] = fmax(mx[2], v); mn[2] = fmin(mn[2], v);
+    if (c < m.nc - 1) { mx[3] = fmax(mx[3], p); mn[3] = fmin(mn[3], p); }
+  }
+  __shared__ double smx[4][32], smn[4][32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      for (int o = 16; o > 0; o >>= 1) {
-        mx[i] = fmax(mx[i], __shfl_xor_sync(0xffffffffu, mx[i], o));
-        mn[i] = fmin(mn[i], __shfl_xor_sync(0xffffffffu, mn[i], o));
-      }
+  for (int i = 0; i < 4; ++i) {
+    for (int o = 16; o > 0; o >>= 1) {
+      mx[i] = fmax(mx[i], __shfl_xor_sync(0xffffffffu, mx[i], o));
+      mn[i] = fmin(mn[i], __shfl_xor_sync(0xffffffffu, mn[i], o));
     }
-    if ((threadIdx.x & 31) == 0) {
-      const int slot_max[4] = {0, 2, 4, 6}, slot_min[4] = {1, 3, 5, 7};
-#pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        if (mx[i] != -INFINITY) atomicMax(&ext[slot_max[i]], okey(mx[i]));
-        if (mn[i] != INFINITY) atomicMin(&ext[slot_min[i]], okey(mn[i]));
-      }
-    }
+    if (lane == 0) { smx[i][wid] = mx[i]; smn[i][wid] = mn[i]; }
+  }
+  __syncthreads();
+  if (threadIdx.x < 4) {
+    const int i = threadIdx.x;
+    double a = -INFINITY, b = INFINITY;
+    for (int k = 0; k < nw; ++k) { a = fmax(a, smx[i][k]); b = fmin(b, smn[i][k]); }
+    const int slot_max[4] = {0, 2, 4, 6}, slot_min[4] = {1, 3, 5, 7};
+    if (a != -INFINITY) atomicMax(&ext[slot_max[i]], okey(a));
+    if (b != INFINITY) atomicMin(&ext[slot_min[i]], okey(b));
   }
 }
 
@@ -756,30 +764,17 @@ __host__ __device__ __forceinline__ void vanleer(const DevCase &c, const FState<
   }
 }
 
-// Face flux: reconstruction, BCs, inviscid + viscous flux; D = Fd - Fc.
-template <class S, bool VISCOUS>
-__global__ void __launch_bounds__(128) k_face_flux(DevCase cs, DevMesh m, const S *__restrict__ W, const S *__restrict__ G,
-                                                   const S *__restrict__ Lm, const S *__restrict__ stale,
-                                                   const S *__restrict__ mu_t, S *__restrict__ D, S *__restrict__ mdot_out,
-                                                   S *__restrict__ wl_out, int *err) {
-  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+// Face difference D = F_diffusive - F_convective * A for prepared left/right
+// states (convective_face_flux + diffusive_face_flux,
+// ns_convective_face_flux.cc:32-59, ns_diffusive_face_flux.cc:28-64).  SG is
+// the type of the stored cell gradients (S itself, or double when only the
+// face states carry tangents, as in the face-Jacobian kernel).
+template <class S, class SG, bool VISCOUS>
+__device__ __forceinline__ void face_D(const DevCase &cs, const DevMesh &m, int f, const double n[3], double A, int b,
+                                       int pa, int nb, const FState<S> &L, const FState<S> &R, const SG *__restrict__ G,
+                                       const SG *__restrict__ mu_t, S D[5], S &wL) {
   const int nf = m.nf, nt = m.nt, nc = m.nc;
-  if (f >= nf) return;
-  const int pa = m.f_parent[f], nb = m.f_neighbor[f], b = m.f_bc[f];
-  const double n[3] = {m.f_n[f], m.f_n[nf + f], m.f_n[2 * nf + f]};
-  const double xf[3] = {m.f_x[f], m.f_x[nf + f], m.f_x[2 * nf + f]};
-  const double A = m.f_area[f];
-  FState<S> L, R;
-  recon_state(cs, m, W, G, Lm, pa, xf, L, n);
-  if (b < 0) {
-    recon_state(cs, m, W, G, Lm, nb, xf, R, n);
-  } else {
-    R.pc = W[nb]; R.Vc[0] = W[nt + nb]; R.Vc[1] = W[2 * nt + nb]; R.Vc[2] = W[3 * nt + nb]; R.Tc = W[4 * nt + nb];
-    R.rho = S(0.);
-    if (!apply_bc(cs, cs.bc[b], L, R, n, err)) R.rho = stale[nb - nc];
-    finish(cs, R, n);
-  }
-  S F[5], wL;
+  S F[5];
   if (cs.flux == 1) roe(cs, L, R, n, F, wL);
   else if (cs.flux == 2) vanleer(cs, L, R, n, F, wL);
   else ausm(cs, L, R, n, F, wL);
@@ -789,11 +784,11 @@ __global__ void __launch_bounds__(128) k_face_flux(DevCase cs, DevMesh m, const 
     S gr[12];  // u,v,w,T gradients at the face
     if (b >= 0) {
 #pragma unroll
-      for (int i = 0; i < 12; ++i) gr[i] = G[(3 + i) * nc + pa];
+      for (int i = 0; i < 12; ++i) gr[i] = S(G[(3 + i) * nc + pa]);
     } else {
       const double wP = m.f_w[f], wN = m.f_w[nf + f];
 #pragma unroll
-      for (int i = 0; i < 12; ++i) gr[i] = wP * G[(3 + i) * nc + pa] + wN * G[(3 + i) * nc + nb];
+      for (int i = 0; i < 12; ++i) gr[i] = S(wP * G[(3 + i) * nc + pa] + wN * G[(3 + i) * nc + nb]);
     }
     const double l0 = m.c_x[nb] - m.c_x[pa], l1 = m.c_x[nt + nb] - m.c_x[nt + pa], l2 = m.c_x[2 * nt + nb] - m.c_x[2 * nt + pa];
     const double lm = sqrt(l0 * l0 + l1 * l1 + l2 * l2);
@@ -811,11 +806,10 @@ __global__ void __launch_bounds__(128) k_face_flux(DevCase cs, DevMesh m, const 
     const S Tf = 0.5 * (L.T + R.T);
     S mu = viscosity(cs, Tf), lam = therm_cond(cs, Tf);
     if (mu_t) {
-      const S mt = mu_t[f];
+      const S mt = S(mu_t[f]);
       mu = mu + mt;
       lam = lam + cs.Cp * mt / cs.Pr_t;
     }
-    // ns_diffusive_face_flux.cc:28-64
     const S *gu = gr, *gv = gr + 3, *gw = gr + 6, *gT = gr + 9;
     const S tx0 = 2. / 3. * (2. * gu[0] - gv[1] - gw[2]), tx1 = gu[1] + gv[0], tx2 = gu[2] + gw[0];
     const S ty1 = 2. / 3. * (2. * gv[1] - gu[0] - gw[2]), ty2 = gv[2] + gw[1];
@@ -831,8 +825,47 @@ __global__ void __launch_bounds__(128) k_face_flux(DevCase cs, DevMesh m, const 
     Fd[4] = Fd[4] + qq;
   }
 #pragma unroll
-  for (int v = 0; v < 5; ++v) D[v * nf + f] = Fd[v] - F[v] * A;
-  if (mdot_out) mdot_out[f] = (F[0] * A - Fd[0]) / A;
+  for (int v = 0; v < 5; ++v) D[v] = Fd[v] - F[v] * A;
+}
+
+// Left / right states of face f (reconstruction, or the boundary condition
+// with the cached density where the BC branch leaves it untouched).
+template <class S>
+__device__ __forceinline__ void face_states(const DevCase &cs, const DevMesh &m, int f, const double n[3], int b, int pa,
+                                            int nb, const S *__restrict__ W, const S *__restrict__ G, const S *__restrict__ Lm,
+                                            const S *__restrict__ stale, FState<S> &L, FState<S> &R, int *err) {
+  const int nf = m.nf, nt = m.nt, nc = m.nc;
+  const double xf[3] = {m.f_x[f], m.f_x[nf + f], m.f_x[2 * nf + f]};
+  recon_state(cs, m, W, G, Lm, pa, xf, L, n);
+  if (b < 0) {
+    recon_state(cs, m, W, G, Lm, nb, xf, R, n);
+  } else {
+    R.pc = W[nb]; R.Vc[0] = W[nt + nb]; R.Vc[1] = W[2 * nt + nb]; R.Vc[2] = W[3 * nt + nb]; R.Tc = W[4 * nt + nb];
+    R.rho = S(0.);
+    if (!apply_bc(cs, cs.bc[b], L, R, n, err)) R.rho = stale[nb - nc];
+    finish(cs, R, n);
+  }
+}
+
+// Face flux: reconstruction, BCs, inviscid + viscous flux; D = Fd - Fc.
+template <class S, bool VISCOUS>
+__global__ void __launch_bounds__(128) k_face_flux(DevCase cs, DevMesh m, const S *__restrict__ W, const S *__restrict__ G,
+                                                   const S *__restrict__ Lm, const S *__restrict__ stale,
+                                                   const S *__restrict__ mu_t, S *__restrict__ D, S *__restrict__ mdot_out,
+                                                   S *__restrict__ wl_out, int *err) {
+  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nf = m.nf;
+  if (f >= nf) return;
+  const int pa = m.f_parent[f], nb = m.f_neighbor[f], b = m.f_bc[f];
+  const double n[3] = {m.f_n[f], m.f_n[nf + f], m.f_n[2 * nf + f]};
+  const double A = m.f_area[f];
+  FState<S> L, R;
+  face_states(cs, m, f, n, b, pa, nb, W, G, Lm, stale, L, R, err);
+  S Dv[5], wL;
+  face_D<S, S, VISCOUS>(cs, m, f, n, A, b, pa, nb, L, R, G, mu_t, Dv, wL);
+#pragma unroll
+  for (int v = 0; v < 5; ++v) D[v * nf + f] = Dv[v];
+  if (mdot_out) mdot_out[f] = (-Dv[0]) / A;
   if (wl_out) wl_out[f] = wL;
 }
 

@@ -1,0 +1,587 @@
+// Matrix-free Newton-Krylov solve of R(W) = 0 on the device.
+//
+// Pseudo-transient continuation as in the reference's implicit step
+// (NavierStokes::solve, ns.cc:104-118):  (V P/dt - dR/dW) dW = R(W),
+// W <- W + dW, with P the conservative-to-primitive Jacobian of
+// NavierStokes::cons2prim (ns_time_terms.cc:26-56) and dt the local time step
+// of update_time_step (time_step.cc:143-224).  The reference assembles a
+// finite-difference Jacobian and hands it to PETSc FGMRES; here the Jacobian is
+// never stored:
+//   * Jacobian-vector products come either from a finite difference of the
+//     FP64 residual ("plain") or from the dual-number tangent kernels
+//     (fcfd_jvp's chain; "jvp"), optionally with an FP32 Krylov basis;
+//   * the preconditioner is block Jacobi: per cell the 5x5 block
+//     V P/dt - sum_faces dD_f/dW_c of the first-order face Jacobians (the
+//     reference's get_jacobians perturbs the reconstructed face states the same
+//     way), computed with 5-lane dual numbers and inverted in place;
+//   * GMRES(m) with right preconditioning; Gram-Schmidt (classical, applied
+//     twice) accumulates every dot product in FP64 with a fixed reduction
+//     order, so a solve is bit-reproducible.
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "ctx.hpp"
+
+namespace fcfd {
+
+// ------------------------------------------------------------------ 5-lane duals
+template <int N>
+struct DN {
+  double v, d[N];
+  __host__ __device__ DN() : v(0) { for (int i = 0; i < N; ++i) d[i] = 0; }
+  __host__ __device__ DN(double x) : v(x) { for (int i = 0; i < N; ++i) d[i] = 0; }
+};
+template <int N> __device__ __forceinline__ DN<N> operator+(const DN<N> &a, const DN<N> &b) { DN<N> r; r.v = a.v + b.v; for (int i = 0; i < N; ++i) r.d[i] = a.d[i] + b.d[i]; return r; }
+template <int N> __device__ __forceinline__ DN<N> operator-(const DN<N> &a, const DN<N> &b) { DN<N> r; r.v = a.v - b.v; for (int i = 0; i < N; ++i) r.d[i] = a.d[i] - b.d[i]; return r; }
+template <int N> __device__ __forceinline__ DN<N> operator-(const DN<N> &a) { DN<N> r; r.v = -a.v; for (int i = 0; i < N; ++i) r.d[i] = -a.d[i]; return r; }
+template <int N> __device__ __forceinline__ DN<N> operator*(const DN<N> &a, const DN<N> &b) { DN<N> r; r.v = a.v * b.v; for (int i = 0; i < N; ++i) r.d[i] = a.d[i] * b.v + a.v * b.d[i]; return r; }
+template <int N> __device__ __forceinline__ DN<N> operator/(const DN<N> &a, const DN<N> &b) { DN<N> r; r.v = a.v / b.v; for (int i = 0; i < N; ++i) r.d[i] = (a.d[i] - r.v * b.d[i]) / b.v; return r; }
+template <int N> __device__ __forceinline__ DN<N> operator+(const DN<N> &a, double b) { DN<N> r = a; r.v += b; return r; }
+template <int N> __device__ __forceinline__ DN<N> operator+(double a, const DN<N> &b) { DN<N> r = b; r.v += a; return r; }
+template <int N> __device__ __forceinline__ DN<N> operator-(const DN<N> &a, double b) { DN<N> r = a; r.v -= b; return r; }
+template <int N> __device__ __forceinline__ DN<N> operator-(double a, const DN<N> &b) { DN<N> r = -b; r.v += a; return r; }
+template <int N> __device__ __forceinline__ DN<N> operator*(const DN<N> &a, double b) { DN<N> r; r.v = a.v * b; for (int i = 0; i < N; ++i) r.d[i] = a.d[i] * b; return r; }
+template <int N> __device__ __forceinline__ DN<N> operator*(double a, const DN<N> &b) { return b * a; }
+template <int N> __device__ __forceinline__ DN<N> operator/(const DN<N> &a, double b) { DN<N> r; r.v = a.v / b; for (int i = 0; i < N; ++i) r.d[i] = a.d[i] / b; return r; }
+template <int N> __device__ __forceinline__ DN<N> operator/(double a, const DN<N> &b) { DN<N> r; r.v = a / b.v; for (int i = 0; i < N; ++i) r.d[i] = -r.v * b.d[i] / b.v; return r; }
+#define FCFD_DN_CMP(op)                                                                                                      \
+  template <int N> __device__ __forceinline__ bool operator op(const DN<N> &a, const DN<N> &b) { return a.v op b.v; }      \
+  template <int N> __device__ __forceinline__ bool operator op(const DN<N> &a, double b) { return a.v op b; }              \
+  template <int N> __device__ __forceinline__ bool operator op(double a, const DN<N> &b) { return a op b.v; }
+FCFD_DN_CMP(<)
+FCFD_DN_CMP(>)
+FCFD_DN_CMP(<=)
+FCFD_DN_CMP(>=)
+FCFD_DN_CMP(==)
+FCFD_DN_CMP(!=)
+#undef FCFD_DN_CMP
+template <int N> __device__ __forceinline__ DN<N> sqrt(const DN<N> &a) { DN<N> r; r.v = ::sqrt(a.v); for (int i = 0; i < N; ++i) r.d[i] = a.d[i] / (2. * r.v); return r; }
+template <int N> __device__ __forceinline__ DN<N> fabs(const DN<N> &a) { return a.v < 0. ? -a : a; }
+template <int N> __device__ __forceinline__ DN<N> pow(const DN<N> &a, double e) {
+  DN<N> r; r.v = ::pow(a.v, e);
+  const double s = (a.v == 0.) ? 0. : e * r.v / a.v;
+  for (int i = 0; i < N; ++i) r.d[i] = s * a.d[i];
+  return r;
+}
+
+typedef DN<5> D5;
+
+// ------------------------------------------------------------------ face Jacobians
+__device__ __forceinline__ void seed(const FState<double> &s, FState<D5> &o, const DevCase &cs, const double n[3]) {
+  // perturbations of state_perturb (ns_assemble_linear_system.cc:417-458):
+  // p moves the face pressure only; u,v,w move V and V_center; T moves T and T_center
+  o.p = D5(s.p); o.p.d[0] = 1.;
+  o.pc = D5(s.pc);
+  for (int i = 0; i < 3; ++i) { o.V[i] = D5(s.V[i]); o.V[i].d[1 + i] = 1.; o.Vc[i] = D5(s.Vc[i]); o.Vc[i].d[1 + i] = 1.; }
+  o.T = D5(s.T); o.T.d[4] = 1.;
+  o.Tc = D5(s.Tc); o.Tc.d[4] = 1.;
+  o.rho = eos_rho(cs, o.p, o.T);
+  finish(cs, o, n);
+}
+__device__ __forceinline__ void lift(const FState<double> &s, FState<D5> &o) {
+  o.p = D5(s.p); o.T = D5(s.T); o.rho = D5(s.rho); o.a = D5(s.a); o.H = D5(s.H); o.Vn = D5(s.Vn);
+  o.pc = D5(s.pc); o.Tc = D5(s.Tc);
+  for (int i = 0; i < 3; ++i) { o.V[i] = D5(s.V[i]); o.Vc[i] = D5(s.Vc[i]); }
+}
+
+// Per face: JL = dD/dW_left and (interior faces) JR = dD/dW_right, [25][nf],
+// entry (i,k) = d D_i / d W_k at index (5i+k)*nf + f.
+template <bool VISCOUS>
+__global__ void __launch_bounds__(128) k_face_jac(DevCase cs, DevMesh m, const double *__restrict__ W, const double *__restrict__ G,
+                                                  const double *__restrict__ Lm, const double *__restrict__ stale,
+                                                  double *__restrict__ JL, double *__restrict__ JR) {
+  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nf = m.nf;
+  if (f >= nf) return;
+  const int pa = m.f_parent[f], nb = m.f_neighbor[f], b = m.f_bc[f];
+  const double n[3] = {m.f_n[f], m.f_n[nf + f], m.f_n[2 * nf + f]};
+  const double A = m.f_area[f];
+  FState<double> L, R;
+  face_states(cs, m, f, n, b, pa, nb, W, G, Lm, stale, L, R, (int *)nullptr);
+  FState<D5> Ld, Rd;
+  D5 D[5], wl;
+  seed(L, Ld, cs, n);
+  if (b < 0) {
+    lift(R, Rd);
+  } else {
+    Rd.pc = D5(R.pc); Rd.Tc = D5(R.Tc); Rd.rho = D5(0.);
+    for (int i = 0; i < 3; ++i) Rd.Vc[i] = D5(R.Vc[i]);
+    if (!apply_bc(cs, cs.bc[b], Ld, Rd, n, (int *)nullptr)) Rd.rho = D5(R.rho);
+    finish(cs, Rd, n);
+  }
+  face_D<D5, double, VISCOUS>(cs, m, f, n, A, b, pa, nb, Ld, Rd, G, (const double *)nullptr, D, wl);
+#pragma unroll
+  for (int i = 0; i < 5; ++i)
+#pragma unroll
+    for (int k = 0; k < 5; ++k) JL[(5 * i + k) * nf + f] = D[i].d[k];
+  if (b < 0) {
+    lift(L, Ld);
+    seed(R, Rd, cs, n);
+    face_D<D5, double, VISCOUS>(cs, m, f, n, A, b, pa, nb, Ld, Rd, G, (const double *)nullptr, D, wl);
+#pragma unroll
+    for (int i = 0; i < 5; ++i)
+#pragma unroll
+      for (int k = 0; k < 5; ++k) JR[(5 * i + k) * nf + f] = D[i].d[k];
+  }
+}
+
+// cons2prim (ns_time_terms.cc:26-56): P[i][k] = d(rho, rho u, rho v, rho w, rho E)_i / d(p,u,v,w,T)_k
+__device__ __forceinline__ void cons2prim(const DevCase &cs, double p, double u, double v, double w, double T, double P[25]) {
+  const double pressure = p + cs.Pref, temperature = T + cs.Tref;
+  const double rho = pressure / (cs.R * temperature);
+  const double drho_dT = -1. * rho / temperature, drho_dp = rho / pressure;
+  const double c_p = cs.Cp;
+  const double H = c_p * temperature + 0.5 * (u * u + v * v + w * w);
+  for (int i = 0; i < 25; ++i) P[i] = 0.;
+  P[0] = drho_dp; P[4] = drho_dT;
+  P[5] = drho_dp * u; P[6] = rho; P[9] = drho_dT * u;
+  P[10] = drho_dp * v; P[12] = rho; P[14] = drho_dT * v;
+  P[15] = drho_dp * w; P[18] = rho; P[19] = drho_dT * w;
+  P[20] = drho_dp * H - 1.; P[21] = rho * u; P[22] = rho * v; P[23] = rho * w; P[24] = drho_dT * H + rho * c_p;
+}
+
+// Block assembly + inversion (Gauss-Jordan, partial pivoting): Minv_c = (V P/dt - J_cc)^-1
+__global__ void k_block_jacobi(DevCase cs, DevMesh m, const double *__restrict__ Wn, const double *__restrict__ vol,
+                               const double *__restrict__ dt, const double *__restrict__ JL, const double *__restrict__ JR,
+                               double *__restrict__ Minv, int *__restrict__ err) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nc = m.nc, nf = m.nf;
+  if (c >= nc) return;
+  double B[25];
+  cons2prim(cs, Wn[c], Wn[nc + c], Wn[2 * nc + c], Wn[3 * nc + c], Wn[4 * nc + c], B);
+  const double s = vol[c] / dt[c];
+#pragma unroll
+  for (int i = 0; i < 25; ++i) B[i] *= s;
+  for (int j = m.cf_index[c]; j < m.cf_index[c + 1]; ++j) {
+    const int e = m.cf_list[j];
+    if (e >= 0) {
+#pragma unroll
+      for (int i = 0; i < 25; ++i) B[i] -= JL[i * nf + e];
+    } else {
+      const int f = ~e;
+#pragma unroll
+      for (int i = 0; i < 25; ++i) B[i] += JR[i * nf + f];
+    }
+  }
+  double I[25];
+#pragma unroll
+  for (int i = 0; i < 25; ++i) I[i] = (i % 6 == 0) ? 1. : 0.;
+  for (int col = 0; col < 5; ++col) {
+    int piv = col;
+    double best = ::fabs(B[5 * col + col]);
+    for (int r = col + 1; r < 5; ++r)
+      if (::fabs(B[5 * r + col]) > best) { best = ::fabs(B[5 * r + col]); piv = r; }
+    if (!(best > 0.)) { atomicOr(err, 4); best = 1.; }
+    if (piv != col)
+      for (int k = 0; k < 5; ++k) {
+        double t = B[5 * col + k]; B[5 * col + k] = B[5 * piv + k]; B[5 * piv + k] = t;
+        t = I[5 * col + k]; I[5 * col + k] = I[5 * piv + k]; I[5 * piv + k] = t;
+      }
+    const double inv = 1. / B[5 * col + col];
+    for (int k = 0; k < 5; ++k) { B[5 * col + k] *= inv; I[5 * col + k] *= inv; }
+    for (int r = 0; r < 5; ++r) {
+      if (r == col) continue;
+      const double fct = B[5 * r + col];
+      for (int k = 0; k < 5; ++k) { B[5 * r + k] -= fct * B[5 * col + k]; I[5 * r + k] -= fct * I[5 * col + k]; }
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < 25; ++i) Minv[i * nc + c] = I[i];
+}
+
+// z = Minv x (per-cell 5x5), vectors [5][nc] of type T
+template <class T>
+__global__ void k_precond(int nc, const double *__restrict__ Minv, const T *__restrict__ x, T *__restrict__ z) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nc) return;
+  double xv[5];
+#pragma unroll
+  for (int k = 0; k < 5; ++k) xv[k] = double(x[k * nc + c]);
+#pragma unroll
+  for (int i = 0; i < 5; ++i) {
+    double s = 0.;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) s += Minv[(5 * i + k) * nc + c] * xv[k];
+    z[i * nc + c] = T(s);
+  }
+}
+
+// copy a [5][nc] state into the residual chain's [5][nt] array (+ optional eps*dir)
+template <class T>
+__global__ void k_load_state(int nc, int nt, const double *__restrict__ Wn, const T *__restrict__ dir, double eps,
+                             double *__restrict__ W) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nc) return;
+#pragma unroll
+  for (int v = 0; v < 5; ++v) W[v * nt + c] = Wn[v * nc + c] + (dir ? eps * double(dir[v * nc + c]) : 0.);
+}
+template <class T>
+__global__ void k_load_dual(int nc, int nt, const double *__restrict__ Wn, const T *__restrict__ dir, Dual<double> *__restrict__ W) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nc) return;
+#pragma unroll
+  for (int v = 0; v < 5; ++v) W[v * nt + c] = Dual<double>(Wn[v * nc + c], double(dir[v * nc + c]));
+}
+
+// y = (V P/dt) z - Jz, Jz from a finite difference (R1 - R0)/eps or a tangent run
+template <class T>
+__global__ void k_matvec_finish(DevCase cs, int nc, const double *__restrict__ Wn, const double *__restrict__ vol,
+                                const double *__restrict__ dt, const T *__restrict__ z, const double *__restrict__ R1,
+                                const double *__restrict__ R0, double inv_eps, const Dual<double> *__restrict__ JV,
+                                T *__restrict__ y) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nc) return;
+  double P[25];
+  cons2prim(cs, Wn[c], Wn[nc + c], Wn[2 * nc + c], Wn[3 * nc + c], Wn[4 * nc + c], P);
+  const double s = vol[c] / dt[c];
+  double zv[5];
+#pragma unroll
+  for (int k = 0; k < 5; ++k) zv[k] = double(z[k * nc + c]);
+#pragma unroll
+  for (int i = 0; i < 5; ++i) {
+    double a = 0.;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) a += P[5 * i + k] * zv[k];
+    const double jz = JV ? JV[i * nc + c].d : (R1[i * nc + c] - R0[i * nc + c]) * inv_eps;
+    y[i * nc + c] = T(s * a - jz);
+  }
+}
+
+// ------------------------------------------------------------------ Krylov vector kernels
+constexpr int kRedBlocks = 592;  // 4 x 148
+
+template <class T>
+__global__ void k_dots(int n, int nv, const T *__restrict__ V, size_t ld, const T *__restrict__ w, double *__restrict__ part) {
+  // part[v*gridDim.x + block] = sum over this block's slice of V_v . w
+  const int v = blockIdx.y;
+  const T *a = V + (size_t)v * ld;
+  double s = 0.;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) s += double(a[i]) * double(w[i]);
+  __shared__ double sh[32];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.;
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) t += sh[k];
+    part[v * gridDim.x + blockIdx.x] = t;
+  }
+  (void)nv;
+}
+__global__ void k_sum_parts(int nparts, const double *__restrict__ part, double *__restrict__ out) {
+  const int v = blockIdx.x;
+  double s = 0.;
+  for (int i = threadIdx.x; i < nparts; i += blockDim.x) s += part[v * nparts + i];
+  __shared__ double sh[32];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.;
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) t += sh[k];
+    out[v] = t;
+  }
+}
+// w -= sum_v h[v] V_v
+template <class T>
+__global__ void k_sub_combo(int n, int nv, const T *__restrict__ V, size_t ld, const double *__restrict__ h, T *__restrict__ w) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double s = double(w[i]);
+  for (int v = 0; v < nv; ++v) s -= h[v] * double(V[(size_t)v * ld + i]);
+  w[i] = T(s);
+}
+// out = sum_v y[v] V_v
+template <class T>
+__global__ void k_combo(int n, int nv, const T *__restrict__ V, size_t ld, const double *__restrict__ y, T *__restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double s = 0.;
+  for (int v = 0; v < nv; ++v) s += y[v] * double(V[(size_t)v * ld + i]);
+  out[i] = T(s);
+}
+template <class T>
+__global__ void k_scale_copy(int n, const double *__restrict__ a, double alpha, T *__restrict__ b) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) b[i] = T(alpha * a[i]);
+}
+template <class T>
+__global__ void k_scale(int n, double alpha, T *__restrict__ b) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) b[i] = T(alpha * double(b[i]));
+}
+// W += dW with a NaN/Inf check (update_variables, ns.cc:338-356)
+template <class T>
+__global__ void k_update(int n, double *__restrict__ Wn, const T *__restrict__ dW, int *__restrict__ err) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double d = double(dW[i]);
+  if (!isfinite(d)) atomicOr(err, 8);
+  Wn[i] += d;
+}
+__global__ void k_aos_to_soa_nc(const double *__restrict__ in, double *__restrict__ out, int nc) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nc) return;
+  for (int v = 0; v < 5; ++v) out[v * nc + c] = in[5 * c + v];
+}
+__global__ void k_soa_to_aos_nc(const double *__restrict__ in, double *__restrict__ out, int nc) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nc) return;
+  for (int v = 0; v < 5; ++v) out[5 * c + v] = in[v * nc + c];
+}
+__global__ void k_gather_vol(int nc, const double *__restrict__ v, double *__restrict__ out) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < nc) out[c] = v[c];
+}
+
+// ------------------------------------------------------------------ solver
+template <class T>
+struct Krylov {
+  fcfd_ctx *x;
+  int n, nc, m;
+  DBuf<T> V, Z, w, tmpT;
+  DBuf<double> part, h;
+  std::vector<double> hh;
+  void alloc(fcfd_ctx *ctx, int krylov_dim) {
+    x = ctx; nc = ctx->dm.nc; n = 5 * nc; m = krylov_dim;
+    V.alloc((size_t)(m + 1) * n); w.alloc(n); tmpT.alloc(n);
+    part.alloc((size_t)kRedBlocks * (m + 1)); h.alloc(m + 1);
+    hh.resize(m + 1);
+  }
+  // out[v] = V_v . u for v < nv (deterministic two-pass reduction)
+  void dots(int nv, const T *u, double *out_host) {
+    cudaStream_t s = x->stream;
+    dim3 g(kRedBlocks, nv);
+    k_dots<T><<<g, 256, 0, s>>>(n, nv, V.p, (size_t)n, u, part.p);
+    k_sum_parts<<<nv, 256, 0, s>>>(kRedBlocks, part.p, h.p);
+    CK(cudaMemcpyAsync(out_host, h.p, sizeof(double) * nv, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+  }
+  double norm(const T *u) {
+    cudaStream_t s = x->stream;
+    dim3 g(kRedBlocks, 1);
+    k_dots<T><<<g, 256, 0, s>>>(n, 1, u, (size_t)n, u, part.p);
+    k_sum_parts<<<1, 256, 0, s>>>(kRedBlocks, part.p, h.p);
+    double r;
+    CK(cudaMemcpyAsync(&r, h.p, sizeof(double), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    return std::sqrt(r);
+  }
+};
+
+struct NewtonState {
+  DBuf<double> Wn, R0, R1, dt, vol, JL, JR, Minv;
+  double wscale = 1.;
+};
+
+// residual of the [5][nc] state (+ eps*dir) into R (SoA [5][nc])
+template <class T>
+static void eval_residual(fcfd_ctx *x, const double *Wn, double *R, const T *dir, double eps) {
+  const DevMesh &m = x->dm;
+  k_load_state<T><<<(m.nc + 255) / 256, 256, 0, x->stream>>>(m.nc, m.nt, Wn, dir, eps, x->p64.W.p);
+  launch_chain<double>(x, x->p64, R, false, nullptr, nullptr);
+}
+
+// y = (V P/dt - dR/dW) z
+template <class T>
+static void matvec(fcfd_ctx *x, NewtonState &ns, int mode, const T *z, T *y, double znorm) {
+  const DevMesh &m = x->dm;
+  cudaStream_t s = x->stream;
+  const int tb = 256, gb = (m.nc + tb - 1) / tb;
+  if (mode == 0) {
+    // finite difference of the FP64 residual, eps = sqrt(eps_mach) (1 + |W|) / |z|
+    const double eps = 1.4901161193847656e-08 * (1. + ns.wscale) / (znorm > 0. ? znorm : 1.);
+    eval_residual<T>(x, ns.Wn.p, ns.R1.p, z, eps);
+    k_matvec_finish<T><<<gb, tb, 0, s>>>(x->cs, m.nc, ns.Wn.p, ns.vol.p, ns.dt.p, z, ns.R1.p, ns.R0.p, 1. / eps, nullptr, y);
+  } else {
+    if (!x->pjv.ready) x->pjv.alloc(m.nc, m.nf, m.nb);
+    k_load_dual<T><<<gb, tb, 0, s>>>(m.nc, m.nt, ns.Wn.p, z, x->pjv.W.p);
+    launch_chain<Dual<double>>(x, x->pjv, x->pjv.R.p, false, nullptr, nullptr);
+    k_matvec_finish<T><<<gb, tb, 0, s>>>(x->cs, m.nc, ns.Wn.p, ns.vol.p, ns.dt.p, z, nullptr, nullptr, 0., x->pjv.R.p, y);
+  }
+  CK(cudaGetLastError());
+}
+
+static double dnorm(fcfd_ctx *x, DBuf<double> &part, DBuf<double> &h, const double *u, int n) {
+  cudaStream_t s = x->stream;
+  dim3 g(kRedBlocks, 1);
+  k_dots<double><<<g, 256, 0, s>>>(n, 1, u, (size_t)n, u, part.p);
+  k_sum_parts<<<1, 256, 0, s>>>(kRedBlocks, part.p, h.p);
+  double r;
+  CK(cudaMemcpyAsync(&r, h.p, sizeof(double), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  return std::sqrt(r);
+}
+
+// Right-preconditioned GMRES(m), one cycle (restarts = outer Newton steps).
+template <class T>
+static void gmres(fcfd_ctx *x, NewtonState &ns, Krylov<T> &K, int mode, double rtol, double *dW, int &iters, double &relres) {
+  const int n = K.n, m = K.m, nc = K.nc;
+  cudaStream_t s = x->stream;
+  const int tb = 256, gn = (n + tb - 1) / tb, gc = (nc + tb - 1) / tb;
+  const double beta = dnorm(x, K.part, K.h, ns.R0.p, n);
+  iters = 0;
+  relres = 1.;
+  if (!(beta > 0.)) {
+    CK(cudaMemsetAsync(dW, 0, sizeof(double) * n, s));
+    relres = 0.;
+    return;
+  }
+  k_scale_copy<T><<<gn, tb, 0, s>>>(n, ns.R0.p, 1. / beta, K.V.p);
+  std::vector<double> H((size_t)(m + 1) * m, 0.), cs(m), sn(m), g(m + 1, 0.), h1(m + 1), h2(m + 1);
+  g[0] = beta;
+  int k = 0;
+  for (int j = 0; j < m; ++j) {
+    T *vj = K.V.p + (size_t)j * n;
+    T *w = K.V.p + (size_t)(j + 1) * n;
+    k_precond<T><<<gc, tb, 0, s>>>(nc, ns.Minv.p, vj, K.tmpT.p);
+    const double zn = (mode == 0) ? K.norm(K.tmpT.p) : 0.;
+    matvec<T>(x, ns, mode, K.tmpT.p, w, zn);
+    // classical Gram-Schmidt, twice
+    K.dots(j + 1, w, h1.data());
+    CK(cudaMemcpyAsync(K.h.p, h1.data(), sizeof(double) * (j + 1), cudaMemcpyHostToDevice, s));
+    k_sub_combo<T><<<gn, tb, 0, s>>>(n, j + 1, K.V.p, (size_t)n, K.h.p, w);
+    K.dots(j + 1, w, h2.data());
+    CK(cudaMemcpyAsync(K.h.p, h2.data(), sizeof(double) * (j + 1), cudaMemcpyHostToDevice, s));
+    k_sub_combo<T><<<gn, tb, 0, s>>>(n, j + 1, K.V.p, (size_t)n, K.h.p, w);
+    const double hn = K.norm(w);
+    for (int i = 0; i <= j; ++i) H[(size_t)i * m + j] = h1[i] + h2[i];
+    H[(size_t)(j + 1) * m + j] = hn;
+    if (hn > 0.) k_scale<T><<<gn, tb, 0, s>>>(n, 1. / hn, w);
+    // Givens rotations
+    for (int i = 0; i < j; ++i) {
+      const double a = H[(size_t)i * m + j], b = H[(size_t)(i + 1) * m + j];
+      H[(size_t)i * m + j] = cs[i] * a + sn[i] * b;
+      H[(size_t)(i + 1) * m + j] = -sn[i] * a + cs[i] * b;
+    }
+    const double a = H[(size_t)j * m + j], b = H[(size_t)(j + 1) * m + j];
+    const double r = std::hypot(a, b);
+    cs[j] = (r > 0.) ? a / r : 1.;
+    sn[j] = (r > 0.) ? b / r : 0.;
+    H[(size_t)j * m + j] = r;
+    H[(size_t)(j + 1) * m + j] = 0.;
+    g[j + 1] = -sn[j] * g[j];
+    g[j] = cs[j] * g[j];
+    k = j + 1;
+    relres = std::fabs(g[j + 1]) / beta;
+    if (relres <= rtol || !(hn > 0.)) break;
+  }
+  // back substitution H(0:k,0:k) y = g
+  std::vector<double> y(k, 0.);
+  for (int i = k - 1; i >= 0; --i) {
+    double t = g[i];
+    for (int l = i + 1; l < k; ++l) t -= H[(size_t)i * m + l] * y[l];
+    y[i] = t / H[(size_t)i * m + i];
+  }
+  CK(cudaMemcpyAsync(K.h.p, y.data(), sizeof(double) * k, cudaMemcpyHostToDevice, s));
+  k_combo<T><<<gn, tb, 0, s>>>(n, k, K.V.p, (size_t)n, K.h.p, K.w.p);
+  k_precond<T><<<gc, tb, 0, s>>>(nc, ns.Minv.p, K.w.p, K.tmpT.p);
+  CK(cudaMemsetAsync(dW, 0, sizeof(double) * n, s));
+  k_update<T><<<gn, tb, 0, s>>>(n, dW, K.tmpT.p, x->err.p);
+  iters = k;
+  CK(cudaGetLastError());
+}
+
+}  // namespace fcfd
+
+using namespace fcfd;
+
+extern "C" {
+
+int fcfd_newton_solve(fcfd_ctx *x, double *W, const fcfd_newton_opts *o, fcfd_newton_report *rep) {
+  try {
+    if (!x || !W || !o || !rep) throw Error(FCFD_ERR_INPUT, "null argument");
+    CK(cudaSetDevice(x->device));
+    const DevMesh &m = x->dm;
+    const int nc = m.nc, n = 5 * nc;
+    cudaStream_t s = x->stream;
+    const int tb = 256, gc = (nc + tb - 1) / tb, gn = (n + tb - 1) / tb;
+    std::memset(rep, 0, sizeof(*rep));
+    NewtonState ns;
+    ns.Wn.alloc(n); ns.R0.alloc(n); ns.R1.alloc(n); ns.dt.alloc(nc); ns.vol.alloc(nc);
+    ns.JL.alloc(25 * (size_t)m.nf); ns.JR.alloc(25 * (size_t)m.nf); ns.Minv.alloc(25 * (size_t)nc);
+    CK(cudaMemsetAsync(ns.JR.p, 0, sizeof(double) * 25 * (size_t)m.nf, s));
+    std::vector<double> vol(x->mesh->c_volume.begin(), x->mesh->c_volume.begin() + nc);
+    CK(cudaMemcpyAsync(ns.vol.p, vol.data(), sizeof(double) * nc, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(x->Win.p, W, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+    k_aos_to_soa_nc<<<gc, tb, 0, s>>>(x->Win.p, ns.Wn.p, nc);
+    const int mdim = o->krylov_dim > 0 ? o->krylov_dim : 30;
+    Krylov<double> K64;
+    Krylov<float> K32;
+    const bool f32 = o->fp32_krylov != 0;
+    if (f32) K32.alloc(x, mdim); else K64.alloc(x, mdim);
+    DBuf<double> part, hh;
+    part.alloc(kRedBlocks); hh.alloc(1);
+    CK(cudaStreamSynchronize(s));
+    auto t0 = std::chrono::steady_clock::now();
+    eval_residual<double>(x, ns.Wn.p, ns.R0.p, nullptr, 0.);
+    check_err(x);
+    const double r0 = dnorm(x, part, hh, ns.R0.p, nc);  // mass (continuity) row
+    double rm = r0;
+    rep->res0 = r0;
+    double cfl = o->cfl0 > 0 ? o->cfl0 : 1.;
+    int status = FCFD_ERR_NOT_CONVERGED;
+    const int maxit = o->max_newton > 0 ? o->max_newton : 200;
+    const int hist = (int)(sizeof(rep->history) / sizeof(rep->history[0]));
+    for (int it = 0; it < maxit; ++it) {
+      if (it < hist) rep->history[it] = rm / r0;
+      if (rm <= o->tol * r0) { status = FCFD_OK; break; }
+      if (o->max_seconds > 0 &&
+          std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() > o->max_seconds) break;
+      if (it > 0) {
+        if (o->cfl_mode == 1) cfl = std::min(o->cfl_max, (o->cfl0 > 0 ? o->cfl0 : 1.) * std::pow(r0 / rm, o->ser_exponent > 0 ? o->ser_exponent : 1.));
+        else cfl = std::min(cfl * (o->cfl_growth > 0 ? o->cfl_growth : 1.2), o->cfl_max);
+      }
+      // local time step on the current state (loaded by the last residual)
+      k_local_dt<double><<<gc, tb, 0, s>>>(x->cs, m, x->p64.W.p, ns.dt.p, cfl, nullptr);
+      // block-Jacobi preconditioner from the first-order face Jacobians
+      if (x->viscous)
+        k_face_jac<true><<<(m.nf + 127) / 128, 128, 0, s>>>(x->cs, m, x->p64.W.p, x->p64.G.p, x->p64.Lm.p, x->p64.stale.p, ns.JL.p, ns.JR.p);
+      else
+        k_face_jac<false><<<(m.nf + 127) / 128, 128, 0, s>>>(x->cs, m, x->p64.W.p, x->p64.G.p, x->p64.Lm.p, x->p64.stale.p, ns.JL.p, ns.JR.p);
+      k_block_jacobi<<<gc, tb, 0, s>>>(x->cs, m, ns.Wn.p, ns.vol.p, ns.dt.p, ns.JL.p, ns.JR.p, ns.Minv.p, x->err.p);
+      CK(cudaGetLastError());
+      // |W| for the finite-difference step
+      ns.wscale = dnorm(x, part, hh, ns.Wn.p, n);
+      int kit = 0;
+      double rr = 0.;
+      const double krtol = o->krylov_rtol > 0 ? o->krylov_rtol : 1e-2;
+      if (f32) gmres<float>(x, ns, K32, o->jvp_mode, krtol, ns.R1.p, kit, rr);
+      else gmres<double>(x, ns, K64, o->jvp_mode, krtol, ns.R1.p, kit, rr);
+      rep->krylov_iterations += kit;
+      k_update<double><<<gn, tb, 0, s>>>(n, ns.Wn.p, ns.R1.p, x->err.p);
+      int h = 0;
+      CK(cudaMemcpyAsync(&h, x->err.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+      CK(cudaStreamSynchronize(s));
+      if (h & 8) { CK(cudaMemsetAsync(x->err.p, 0, sizeof(int), s)); status = FCFD_ERR_DIVERGED; rep->newton_iterations = it + 1; break; }
+      eval_residual<double>(x, ns.Wn.p, ns.R0.p, nullptr, 0.);
+      rm = dnorm(x, part, hh, ns.R0.p, nc);
+      rep->newton_iterations = it + 1;
+      rep->last_cfl = cfl;
+      if (!std::isfinite(rm)) { status = FCFD_ERR_DIVERGED; break; }
+    }
+    CK(cudaStreamSynchronize(s));
+    rep->wall_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    rep->res_final = rm;
+    rep->status = status;
+    if (rep->newton_iterations < hist) rep->history[rep->newton_iterations] = rm / r0;
+    k_soa_to_aos_nc<<<gc, tb, 0, s>>>(ns.Wn.p, x->Win.p, nc);
+    CK(cudaMemcpyAsync(W, x->Win.p, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (status != FCFD_OK) {
+      set_last_error(status == FCFD_ERR_DIVERGED ? "Newton iteration diverged (NaN/Inf update)" : "Newton iteration did not reach the tolerance");
+      return status;
+    }
+  } catch (const Error &e) {
+    set_last_error(e.what());
+    return e.code;
+  } catch (const std::exception &e) {
+    set_last_error(e.what());
+    return FCFD_ERR_INPUT;
+  }
+  return FCFD_OK;
+}
+
+}  // extern "C"

@@ -16,7 +16,7 @@ import tempfile
 
 import numpy as np
 
-from ._lib import _RawMesh, _d, _i, _ptr, check, lib
+from ._lib import NewtonOpts, NewtonReport, _RawMesh, _d, _i, _ptr, check, lib, FcfdError
 
 
 class Case:
@@ -145,6 +145,24 @@ class NavierStokes:
         pr = _ptr(R)[0] if R is not None else None
         check(lib.fcfd_jvp(self.h, pw, pv, pr, pj, fw))
         return (R, JV) if with_residual else JV
+
+    def newton_solve(self, W, tol=1e-10, max_newton=200, krylov_dim=30, krylov_rtol=1e-2, cfl0=1.0,
+                     cfl_growth=1.2, cfl_max=1e6, cfl_mode=1, ser_exponent=1.0, jvp=True, fp32_krylov=False,
+                     max_seconds=0.0, raise_on_fail=True):
+        """Steady solve R(W) = 0 (pseudo-transient Newton-Krylov on the device).
+        Returns (W_converged, report dict)."""
+        W = np.array(W, dtype=np.float64, order="C", copy=True)
+        o = NewtonOpts(int(max_newton), float(tol), int(krylov_dim), float(krylov_rtol), float(cfl0), float(cfl_growth),
+                       float(cfl_max), int(cfl_mode), float(ser_exponent), int(bool(jvp)), int(bool(fp32_krylov)),
+                       float(max_seconds))
+        r = NewtonReport()
+        rc = lib.fcfd_newton_solve(self.h, _d(W), ctypes.byref(o), ctypes.byref(r))
+        rep = dict(status=r.status, newton_iterations=r.newton_iterations, krylov_iterations=r.krylov_iterations,
+                   res0=r.res0, res_final=r.res_final, wall_seconds=r.wall_seconds, last_cfl=r.last_cfl,
+                   history=np.array(r.history[:r.newton_iterations + 1]))
+        if rc != 0 and raise_on_fail:
+            raise FcfdError(rc, lib.fcfd_last_error().decode() + f" after {r.newton_iterations} steps")
+        return W, rep
 
     def stages(self):
         m = self.mesh

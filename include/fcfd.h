@@ -129,6 +129,38 @@ int fcfd_local_dt(fcfd_ctx *ctx, const double *W, double cfl, int mode, double *
  * matrix-free Newton-Krylov solve. */
 int fcfd_jvp(fcfd_ctx *ctx, const double *W, const double *V, double *R, double *JV, int flags);
 
+/* Options of the device Newton-Krylov solve. */
+typedef struct fcfd_newton_opts {
+  int32_t max_newton;     /* Newton (pseudo-time) steps, default 200 */
+  double tol;             /* stop when |R_mass|_2 <= tol * |R_mass(W0)|_2 */
+  int32_t krylov_dim;     /* GMRES basis size m (one cycle per Newton step), default 30 */
+  double krylov_rtol;     /* GMRES relative tolerance, default 1e-2 */
+  double cfl0;            /* initial CFL (time marching ramp initial) */
+  double cfl_growth;      /* ramp growth per step (cfl_mode 0) */
+  double cfl_max;         /* CFL cap */
+  int32_t cfl_mode;       /* 0: reference ramp (time_step.cc:146-156); 1: CFL0 * (|R0|/|R|)^ser_exponent */
+  double ser_exponent;
+  int32_t jvp_mode;       /* 0: finite-difference J.v of the FP64 residual; 1: tangent (dual-number) kernels */
+  int32_t fp32_krylov;    /* 1: Krylov basis and preconditioned vectors in FP32 (dot products in FP64) */
+  double max_seconds;     /* wall-clock cap (0: none) */
+} fcfd_newton_opts;
+
+typedef struct fcfd_newton_report {
+  int32_t status, newton_iterations, krylov_iterations, pad;
+  double res0, res_final, wall_seconds, last_cfl;
+  double history[512];    /* |R_mass| / |R_mass(W0)| per Newton step */
+} fcfd_newton_report;
+
+/* Steady solve R(W) = 0 by pseudo-transient matrix-free Newton-Krylov on the
+ * device: (V P/dt - dR/dW) dW = R(W), W += dW, with P = cons2prim
+ * (ns_time_terms.cc:26-56), local dt (time_step.cc:143-224), block-Jacobi
+ * preconditioner from first-order face Jacobians (get_jacobians,
+ * ns_assemble_linear_system.cc:197-267) and GMRES(m) with FP64
+ * Gram-Schmidt.  Replaces NavierStokes::solve's assemble + PETSc FGMRES
+ * (ns.cc:104-118, ns_petsc_functions.cc:85-110).  W[nc][5] host, in/out.
+ * Returns FCFD_ERR_NOT_CONVERGED / FCFD_ERR_DIVERGED with the report filled. */
+int fcfd_newton_solve(fcfd_ctx *ctx, double *W, const fcfd_newton_opts *opts, fcfd_newton_report *report);
+
 /* Device timing of the residual: runs `reps` residual evaluations on the
  * resident state (captured in one CUDA graph) and returns per-kernel average
  * milliseconds: out[0] total per residual, out[1..] per kernel (see fcfd.cu). */

@@ -35,7 +35,14 @@ def rel_err(a, b, floor=1e-300):
     return (np.abs(a - b).max(axis=0) / scale)
 
 
-def flux_scale(case, mesh_geometry):
-    """Magnitude of one face's pressure flux, p_inf * max face area: the size of
-    the terms whose cancellation produces a residual."""
-    return abs(case.freestream[0]) * float(np.max(mesh_geometry["face_area"]))
+def flux_scale(case, mesh_geometry, gamma=1.4, R=287.0):
+    """Per-equation magnitude of one face's freestream flux (mass, momentum,
+    energy) times the largest face area: the size of the terms whose
+    cancellation produces a residual."""
+    p, u, v, w, T = case.freestream
+    rho = p / (R * T)
+    U = float(np.sqrt(u * u + v * v + w * w))
+    H = gamma / (gamma - 1.0) * R * T + 0.5 * U * U
+    A = float(np.max(mesh_geometry["face_area"]))
+    mom = (rho * U * U + p) * A
+    return np.array([rho * U * A, mom, mom, mom, rho * U * H * A])
