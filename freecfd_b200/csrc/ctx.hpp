@@ -95,12 +95,13 @@ struct fcfd_ctx {
   DBuf<unsigned char> flush;
   int n_outlet = 0;
   cudaGraphExec_t graph = nullptr;
+  bool newton_frozen = false;
 };
 
 
 namespace fcfd {
 constexpr int kExtremaBlocks = 296;  // 2 x 148 SMs
 template <class S>
-void launch_chain(fcfd_ctx *x, Pipe<S> &P, S *Rout, bool aos_out, S *mo, S *wo);
+void launch_chain(fcfd_ctx *x, Pipe<S> &P, S *Rout, bool aos_out, S *mo, S *wo, bool frozen_limiter = false);
 int check_err(fcfd_ctx *x);
 }  // namespace fcfd

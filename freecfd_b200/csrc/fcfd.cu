@@ -25,8 +25,10 @@ static thread_local std::string g_last_error;
 void set_last_error(const std::string &m) { g_last_error = m; }
 
 template <class S>
-void launch_chain(fcfd_ctx *x, Pipe<S> &P, S *Rout, bool aos_out, S *mo, S *wo) {
+void launch_chain(fcfd_ctx *x, Pipe<S> &P, S *Rout, bool aos_out, S *mo, S *wo, bool frozen_limiter) {
   const DevMesh &m = x->dm;
+  DevCase csl = x->cs;
+  csl.frozen_limiter = frozen_limiter ? 1 : 0;
   cudaStream_t s = x->stream;
   const int tb = 256;
   // extrema slots: even = max (start at key 0), odd = min (start at all ones)
@@ -41,7 +43,7 @@ void launch_chain(fcfd_ctx *x, Pipe<S> &P, S *Rout, bool aos_out, S *mo, S *wo) 
     k_argext<S><<<(m.nc + tb - 1) / tb, tb, 0, s>>>(m, P.W.p, x->ext.p, x->argx.p);
     argx = x->argx.p;
   }
-  k_grad_limiter<S><<<(m.nc + 127) / 128, 128, 0, s>>>(x->cs, m, P.W.p, x->ext.p, argx, P.G.p, P.Lm.p);
+  k_grad_limiter<S><<<(m.nc + 127) / 128, 128, 0, s>>>(csl, m, P.W.p, x->ext.p, argx, P.G.p, P.Lm.p);
   if (m.n_outlet > 0)
     k_outlet_rho<S><<<(m.n_outlet + 127) / 128, 128, 0, s>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p);
   if (x->viscous)
@@ -67,8 +69,8 @@ int check_err(fcfd_ctx *x) {
   return 0;
 }
 
-template void launch_chain<double>(fcfd_ctx *, Pipe<double> &, double *, bool, double *, double *);
-template void launch_chain<Dual<double>>(fcfd_ctx *, Pipe<Dual<double>> &, Dual<double> *, bool, Dual<double> *, Dual<double> *);
+template void launch_chain<double>(fcfd_ctx *, Pipe<double> &, double *, bool, double *, double *, bool);
+template void launch_chain<Dual<double>>(fcfd_ctx *, Pipe<Dual<double>> &, Dual<double> *, bool, Dual<double> *, Dual<double> *, bool);
 
 }  // namespace fcfd
 

@@ -120,7 +120,7 @@ struct DevCase {
   double gamma, R, Pref, Tref, Minf, K, Lref, Cp;
   double mu, lambda, sut_mu_ref, sut_T_ref, sut_S, Pr;
   double Pr_t;
-  int sutherland, prandtl, flux, limiter, order, viscous, nbc, pad;
+  int sutherland, prandtl, flux, limiter, order, viscous, nbc, frozen_limiter;
   DevBC bc[kMaxBC];
 };
 
@@ -595,6 +595,11 @@ __global__ void __launch_bounds__(128) k_grad_limiter(DevCase cs, DevMesh m, con
         }
       }
     }
+  }
+  if (cs.frozen_limiter) {
+    // tangent runs for Newton-Krylov: treat the limiter as a constant
+#pragma unroll
+    for (int v = 0; v < 5; ++v) phi[v] = Mk<S>::of(val(phi[v]), 0.);
   }
 #pragma unroll
   for (int v = 0; v < 5; ++v) Lm[v * nc + c] = phi[v];

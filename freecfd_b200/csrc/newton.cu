@@ -398,7 +398,7 @@ static void matvec(fcfd_ctx *x, NewtonState &ns, int mode, const T *z, T *y, dou
   } else {
     if (!x->pjv.ready) x->pjv.alloc(m.nc, m.nf, m.nb);
     k_load_dual<T><<<gb, tb, 0, s>>>(m.nc, m.nt, ns.Wn.p, z, x->pjv.W.p);
-    launch_chain<Dual<double>>(x, x->pjv, x->pjv.R.p, false, nullptr, nullptr);
+    launch_chain<Dual<double>>(x, x->pjv, x->pjv.R.p, false, nullptr, nullptr, x->newton_frozen);
     k_matvec_finish<T><<<gb, tb, 0, s>>>(x->cs, m.nc, ns.Wn.p, ns.vol.p, ns.dt.p, z, nullptr, nullptr, 0., x->pjv.R.p, y);
   }
   CK(cudaGetLastError());
@@ -511,6 +511,7 @@ int fcfd_newton_solve(fcfd_ctx *x, double *W, const fcfd_newton_opts *o, fcfd_ne
     Krylov<double> K64;
     Krylov<float> K32;
     const bool f32 = o->fp32_krylov != 0;
+    x->newton_frozen = o->jvp_mode == 1;
     if (f32) K32.alloc(x, mdim); else K64.alloc(x, mdim);
     DBuf<double> part, hh;
     part.alloc(kRedBlocks); hh.alloc(1);

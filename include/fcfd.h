@@ -140,7 +140,8 @@ typedef struct fcfd_newton_opts {
   double cfl_max;         /* CFL cap */
   int32_t cfl_mode;       /* 0: reference ramp (time_step.cc:146-156); 1: CFL0 * (|R0|/|R|)^ser_exponent */
   double ser_exponent;
-  int32_t jvp_mode;       /* 0: finite-difference J.v of the FP64 residual; 1: tangent (dual-number) kernels */
+  int32_t jvp_mode;       /* 0: finite-difference J.v of the FP64 residual; 1: tangent (dual-number)
+                             kernels with the limiter held fixed (frozen-limiter Jacobian) */
   int32_t fp32_krylov;    /* 1: Krylov basis and preconditioned vectors in FP32 (dot products in FP64) */
   double max_seconds;     /* wall-clock cap (0: none) */
 } fcfd_newton_opts;
