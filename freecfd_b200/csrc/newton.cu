@@ -192,13 +192,17 @@ __global__ void k_block_jacobi(DevCase cs, DevMesh m, const double *__restrict__
 }
 
 // z = Minv x (per-cell 5x5), vectors [5][nc] of type T
+struct RowScale {
+  double s[5];  // per-equation weight of the GMRES norm
+};
+// z = Minv (D^-1 x): right preconditioner of the row-scaled system D A
 template <class T>
-__global__ void k_precond(int nc, const double *__restrict__ Minv, const T *__restrict__ x, T *__restrict__ z) {
+__global__ void k_precond(int nc, const double *__restrict__ Minv, const T *__restrict__ x, T *__restrict__ z, RowScale rs) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= nc) return;
   double xv[5];
 #pragma unroll
-  for (int k = 0; k < 5; ++k) xv[k] = double(x[k * nc + c]);
+  for (int k = 0; k < 5; ++k) xv[k] = double(x[k * nc + c]) / rs.s[k];
 #pragma unroll
   for (int i = 0; i < 5; ++i) {
     double s = 0.;
@@ -230,7 +234,7 @@ template <class T>
 __global__ void k_matvec_finish(DevCase cs, int nc, const double *__restrict__ Wn, const double *__restrict__ vol,
                                 const double *__restrict__ dt, const T *__restrict__ z, const double *__restrict__ R1,
                                 const double *__restrict__ R0, double inv_eps, const Dual<double> *__restrict__ JV,
-                                T *__restrict__ y) {
+                                T *__restrict__ y, RowScale rs) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= nc) return;
   double P[25];
@@ -245,7 +249,7 @@ __global__ void k_matvec_finish(DevCase cs, int nc, const double *__restrict__ W
 #pragma unroll
     for (int k = 0; k < 5; ++k) a += P[5 * i + k] * zv[k];
     const double jz = JV ? JV[i * nc + c].d : (R1[i * nc + c] - R0[i * nc + c]) * inv_eps;
-    y[i * nc + c] = T(s * a - jz);
+    y[i * nc + c] = T(rs.s[i] * (s * a - jz));
   }
 }
 
@@ -312,14 +316,34 @@ __global__ void k_scale(int n, double alpha, T *__restrict__ b) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) b[i] = T(alpha * double(b[i]));
 }
-// W += dW with a NaN/Inf check (update_variables, ns.cc:338-356)
+// W += alpha dW with a NaN/Inf check (update_variables, ns.cc:338-356)
 template <class T>
-__global__ void k_update(int n, double *__restrict__ Wn, const T *__restrict__ dW, int *__restrict__ err) {
+__global__ void k_update(int n, double *__restrict__ Wn, const T *__restrict__ dW, double alpha, int *__restrict__ err) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const double d = double(dW[i]);
   if (!isfinite(d)) atomicOr(err, 8);
-  Wn[i] += d;
+  Wn[i] += alpha * d;
+}
+// scaled copy b = alpha a (same type)
+__global__ void k_rowscale_copy(int nc, const double *__restrict__ a, RowScale rs, double alpha, double *__restrict__ b) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nc) return;
+  for (int v = 0; v < 5; ++v) b[v * nc + c] = alpha * rs.s[v] * a[v * nc + c];
+}
+// largest relative change of the absolute pressure and temperature, as an ordered key
+__global__ void k_max_rel_change(DevCase cs, int nc, const double *__restrict__ Wn, const double *__restrict__ dW,
+                                 unsigned long long *__restrict__ key) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  double r = 0.;
+  if (c < nc) {
+    const double pa = Wn[c] + cs.Pref, Ta = Wn[4 * nc + c] + cs.Tref;
+    const double rp = ::fabs(dW[c]) / ::fabs(pa), rT = ::fabs(dW[4 * nc + c]) / ::fabs(Ta);
+    r = rp > rT ? rp : rT;
+    if (!isfinite(r)) r = 1e300;
+  }
+  for (int o = 16; o > 0; o >>= 1) r = fmax(r, __shfl_xor_sync(0xffffffffu, r, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(key, okey(r));
 }
 __global__ void k_aos_to_soa_nc(const double *__restrict__ in, double *__restrict__ out, int nc) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
@@ -386,7 +410,7 @@ static void eval_residual(fcfd_ctx *x, const double *Wn, double *R, const T *dir
 
 // y = (V P/dt - dR/dW) z
 template <class T>
-static void matvec(fcfd_ctx *x, NewtonState &ns, int mode, const T *z, T *y, double znorm) {
+static void matvec(fcfd_ctx *x, NewtonState &ns, int mode, const T *z, T *y, double znorm, const RowScale &rs) {
   const DevMesh &m = x->dm;
   cudaStream_t s = x->stream;
   const int tb = 256, gb = (m.nc + tb - 1) / tb;
@@ -394,12 +418,12 @@ static void matvec(fcfd_ctx *x, NewtonState &ns, int mode, const T *z, T *y, dou
     // finite difference of the FP64 residual, eps = sqrt(eps_mach) (1 + |W|) / |z|
     const double eps = 1.4901161193847656e-08 * (1. + ns.wscale) / (znorm > 0. ? znorm : 1.);
     eval_residual<T>(x, ns.Wn.p, ns.R1.p, z, eps);
-    k_matvec_finish<T><<<gb, tb, 0, s>>>(x->cs, m.nc, ns.Wn.p, ns.vol.p, ns.dt.p, z, ns.R1.p, ns.R0.p, 1. / eps, nullptr, y);
+    k_matvec_finish<T><<<gb, tb, 0, s>>>(x->cs, m.nc, ns.Wn.p, ns.vol.p, ns.dt.p, z, ns.R1.p, ns.R0.p, 1. / eps, nullptr, y, rs);
   } else {
     if (!x->pjv.ready) x->pjv.alloc(m.nc, m.nf, m.nb);
     k_load_dual<T><<<gb, tb, 0, s>>>(m.nc, m.nt, ns.Wn.p, z, x->pjv.W.p);
     launch_chain<Dual<double>>(x, x->pjv, x->pjv.R.p, false, nullptr, nullptr, x->newton_frozen);
-    k_matvec_finish<T><<<gb, tb, 0, s>>>(x->cs, m.nc, ns.Wn.p, ns.vol.p, ns.dt.p, z, nullptr, nullptr, 0., x->pjv.R.p, y);
+    k_matvec_finish<T><<<gb, tb, 0, s>>>(x->cs, m.nc, ns.Wn.p, ns.vol.p, ns.dt.p, z, nullptr, nullptr, 0., x->pjv.R.p, y, rs);
   }
   CK(cudaGetLastError());
 }
@@ -417,11 +441,14 @@ static double dnorm(fcfd_ctx *x, DBuf<double> &part, DBuf<double> &h, const doub
 
 // Right-preconditioned GMRES(m), one cycle (restarts = outer Newton steps).
 template <class T>
-static void gmres(fcfd_ctx *x, NewtonState &ns, Krylov<T> &K, int mode, double rtol, double *dW, int &iters, double &relres) {
+static void gmres(fcfd_ctx *x, NewtonState &ns, Krylov<T> &K, int mode, double rtol, double *dW, int &iters, double &relres,
+                  const RowScale &rs) {
   const int n = K.n, m = K.m, nc = K.nc;
   cudaStream_t s = x->stream;
   const int tb = 256, gn = (n + tb - 1) / tb, gc = (nc + tb - 1) / tb;
-  const double beta = dnorm(x, K.part, K.h, ns.R0.p, n);
+  // row-scaled right-hand side D R0 (kept in ns.R1 until the matvecs reuse it)
+  k_rowscale_copy<<<gc, tb, 0, s>>>(nc, ns.R0.p, rs, 1., dW);
+  const double beta = dnorm(x, K.part, K.h, dW, n);
   iters = 0;
   relres = 1.;
   if (!(beta > 0.)) {
@@ -429,16 +456,16 @@ static void gmres(fcfd_ctx *x, NewtonState &ns, Krylov<T> &K, int mode, double r
     relres = 0.;
     return;
   }
-  k_scale_copy<T><<<gn, tb, 0, s>>>(n, ns.R0.p, 1. / beta, K.V.p);
+  k_scale_copy<T><<<gn, tb, 0, s>>>(n, dW, 1. / beta, K.V.p);
   std::vector<double> H((size_t)(m + 1) * m, 0.), cs(m), sn(m), g(m + 1, 0.), h1(m + 1), h2(m + 1);
   g[0] = beta;
   int k = 0;
   for (int j = 0; j < m; ++j) {
     T *vj = K.V.p + (size_t)j * n;
     T *w = K.V.p + (size_t)(j + 1) * n;
-    k_precond<T><<<gc, tb, 0, s>>>(nc, ns.Minv.p, vj, K.tmpT.p);
+    k_precond<T><<<gc, tb, 0, s>>>(nc, ns.Minv.p, vj, K.tmpT.p, rs);
     const double zn = (mode == 0) ? K.norm(K.tmpT.p) : 0.;
-    matvec<T>(x, ns, mode, K.tmpT.p, w, zn);
+    matvec<T>(x, ns, mode, K.tmpT.p, w, zn, rs);
     // classical Gram-Schmidt, twice
     K.dots(j + 1, w, h1.data());
     CK(cudaMemcpyAsync(K.h.p, h1.data(), sizeof(double) * (j + 1), cudaMemcpyHostToDevice, s));
@@ -477,9 +504,9 @@ static void gmres(fcfd_ctx *x, NewtonState &ns, Krylov<T> &K, int mode, double r
   }
   CK(cudaMemcpyAsync(K.h.p, y.data(), sizeof(double) * k, cudaMemcpyHostToDevice, s));
   k_combo<T><<<gn, tb, 0, s>>>(n, k, K.V.p, (size_t)n, K.h.p, K.w.p);
-  k_precond<T><<<gc, tb, 0, s>>>(nc, ns.Minv.p, K.w.p, K.tmpT.p);
+  k_precond<T><<<gc, tb, 0, s>>>(nc, ns.Minv.p, K.w.p, K.tmpT.p, rs);
   CK(cudaMemsetAsync(dW, 0, sizeof(double) * n, s));
-  k_update<T><<<gn, tb, 0, s>>>(n, dW, K.tmpT.p, x->err.p);
+  k_update<T><<<gn, tb, 0, s>>>(n, dW, K.tmpT.p, 1., x->err.p);
   iters = k;
   CK(cudaGetLastError());
 }
@@ -515,26 +542,40 @@ int fcfd_newton_solve(fcfd_ctx *x, double *W, const fcfd_newton_opts *o, fcfd_ne
     if (f32) K32.alloc(x, mdim); else K64.alloc(x, mdim);
     DBuf<double> part, hh;
     part.alloc(kRedBlocks); hh.alloc(1);
+    DBuf<double> Wsave;
+    Wsave.alloc(n);
+    DBuf<unsigned long long> key;
+    key.alloc(1);
     CK(cudaStreamSynchronize(s));
     auto t0 = std::chrono::steady_clock::now();
-    eval_residual<double>(x, ns.Wn.p, ns.R0.p, nullptr, 0.);
+    eval_residual<double>(x, ns.Wn.p, ns.R0.p, (const double *)nullptr, 0.);
     check_err(x);
-    const double r0 = dnorm(x, part, hh, ns.R0.p, nc);  // mass (continuity) row
+    auto row_norms = [&](double out[5]) {
+      for (int v = 0; v < 5; ++v) out[v] = dnorm(x, part, hh, ns.R0.p + (size_t)v * nc, nc);
+    };
+    double rows[5];
+    row_norms(rows);
+    const double r0 = rows[0];  // mass (continuity) row
     double rm = r0;
     rep->res0 = r0;
-    double cfl = o->cfl0 > 0 ? o->cfl0 : 1.;
+    const double cfl0 = o->cfl0 > 0 ? o->cfl0 : 1.;
+    const double growth = o->cfl_growth > 0 ? o->cfl_growth : 1.2;
+    const double cflmax = o->cfl_max > 0 ? o->cfl_max : 1e6;
+    double cfl = cfl0, cfl_prev = cfl0;
     int status = FCFD_ERR_NOT_CONVERGED;
     const int maxit = o->max_newton > 0 ? o->max_newton : 200;
     const int hist = (int)(sizeof(rep->history) / sizeof(rep->history[0]));
+    int rejects = 0;
     for (int it = 0; it < maxit; ++it) {
       if (it < hist) rep->history[it] = rm / r0;
       if (rm <= o->tol * r0) { status = FCFD_OK; break; }
       if (o->max_seconds > 0 &&
           std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() > o->max_seconds) break;
-      if (it > 0) {
-        if (o->cfl_mode == 1) cfl = std::min(o->cfl_max, (o->cfl0 > 0 ? o->cfl0 : 1.) * std::pow(r0 / rm, o->ser_exponent > 0 ? o->ser_exponent : 1.));
-        else cfl = std::min(cfl * (o->cfl_growth > 0 ? o->cfl_growth : 1.2), o->cfl_max);
-      }
+      // GMRES norm weights: each equation's residual counts equally
+      double rmax = 0.;
+      for (int v = 0; v < 5; ++v) rmax = std::max(rmax, rows[v]);
+      RowScale rs;
+      for (int v = 0; v < 5; ++v) rs.s[v] = 1. / std::max(rows[v], 1e-10 * rmax);
       // local time step on the current state (loaded by the last residual)
       k_local_dt<double><<<gc, tb, 0, s>>>(x->cs, m, x->p64.W.p, ns.dt.p, cfl, nullptr);
       // block-Jacobi preconditioner from the first-order face Jacobians
@@ -544,24 +585,60 @@ int fcfd_newton_solve(fcfd_ctx *x, double *W, const fcfd_newton_opts *o, fcfd_ne
         k_face_jac<false><<<(m.nf + 127) / 128, 128, 0, s>>>(x->cs, m, x->p64.W.p, x->p64.G.p, x->p64.Lm.p, x->p64.stale.p, ns.JL.p, ns.JR.p);
       k_block_jacobi<<<gc, tb, 0, s>>>(x->cs, m, ns.Wn.p, ns.vol.p, ns.dt.p, ns.JL.p, ns.JR.p, ns.Minv.p, x->err.p);
       CK(cudaGetLastError());
-      // |W| for the finite-difference step
       ns.wscale = dnorm(x, part, hh, ns.Wn.p, n);
       int kit = 0;
       double rr = 0.;
       const double krtol = o->krylov_rtol > 0 ? o->krylov_rtol : 1e-2;
-      if (f32) gmres<float>(x, ns, K32, o->jvp_mode, krtol, ns.R1.p, kit, rr);
-      else gmres<double>(x, ns, K64, o->jvp_mode, krtol, ns.R1.p, kit, rr);
+      if (f32) gmres<float>(x, ns, K32, o->jvp_mode, krtol, ns.R1.p, kit, rr, rs);
+      else gmres<double>(x, ns, K64, o->jvp_mode, krtol, ns.R1.p, kit, rr, rs);
       rep->krylov_iterations += kit;
-      k_update<double><<<gn, tb, 0, s>>>(n, ns.Wn.p, ns.R1.p, x->err.p);
+      // relax the update so that p and T change by at most 20 % per step
+      CK(cudaMemsetAsync(key.p, 0, sizeof(unsigned long long), s));
+      k_max_rel_change<<<gc, tb, 0, s>>>(x->cs, nc, ns.Wn.p, ns.R1.p, key.p);
+      unsigned long long kh = 0;
+      CK(cudaMemcpyAsync(&kh, key.p, sizeof(kh), cudaMemcpyDeviceToHost, s));
+      CK(cudaStreamSynchronize(s));
+      double dmax = 0.;
+      {
+        unsigned long long b = (kh >> 63) ? (kh & 0x7fffffffffffffffull) : ~kh;
+        std::memcpy(&dmax, &b, sizeof(dmax));
+      }
+      const double alpha = (dmax > 0.2) ? 0.2 / dmax : 1.;
+      CK(cudaMemcpyAsync(Wsave.p, ns.Wn.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+      k_update<double><<<gn, tb, 0, s>>>(n, ns.Wn.p, ns.R1.p, alpha, x->err.p);
       int h = 0;
       CK(cudaMemcpyAsync(&h, x->err.p, sizeof(int), cudaMemcpyDeviceToHost, s));
       CK(cudaStreamSynchronize(s));
-      if (h & 8) { CK(cudaMemsetAsync(x->err.p, 0, sizeof(int), s)); status = FCFD_ERR_DIVERGED; rep->newton_iterations = it + 1; break; }
-      eval_residual<double>(x, ns.Wn.p, ns.R0.p, nullptr, 0.);
-      rm = dnorm(x, part, hh, ns.R0.p, nc);
+      double rnew = NAN;
+      if (!(h & 8)) {
+        eval_residual<double>(x, ns.Wn.p, ns.R0.p, (const double *)nullptr, 0.);
+        CK(cudaMemcpyAsync(&h, x->err.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        row_norms(rows);
+        rnew = rows[0];
+      }
+      if (h) CK(cudaMemsetAsync(x->err.p, 0, sizeof(int), s));
       rep->newton_iterations = it + 1;
+      if (!std::isfinite(rnew) || (h & 8)) {
+        // reject the step: restore the state, cut the CFL, re-evaluate
+        if (++rejects > 12) { status = FCFD_ERR_DIVERGED; break; }
+        CK(cudaMemcpyAsync(ns.Wn.p, Wsave.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+        eval_residual<double>(x, ns.Wn.p, ns.R0.p, (const double *)nullptr, 0.);
+        row_norms(rows);
+        cfl = std::max(cfl * 0.25, 1e-3);
+        cfl_prev = cfl;
+        continue;
+      }
+      rejects = 0;
+      rm = rnew;
       rep->last_cfl = cfl;
-      if (!std::isfinite(rm)) { status = FCFD_ERR_DIVERGED; break; }
+      // next CFL: reference ramp, or switched evolution/relaxation on |R_mass|
+      double next;
+      if (o->cfl_mode == 1) next = cfl0 * std::pow(r0 / rm, o->ser_exponent > 0 ? o->ser_exponent : 1.);
+      else next = cfl * growth;
+      next = std::min(next, cfl_prev * 2.);
+      cfl_prev = cfl;
+      cfl = std::min(std::max(next, 1e-3), cflmax);
     }
     CK(cudaStreamSynchronize(s));
     rep->wall_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
