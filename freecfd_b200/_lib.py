@@ -55,7 +55,8 @@ class NewtonOpts(ctypes.Structure):
     _fields_ = [("max_newton", ctypes.c_int32), ("tol", ctypes.c_double), ("krylov_dim", ctypes.c_int32),
                 ("krylov_rtol", ctypes.c_double), ("cfl0", ctypes.c_double), ("cfl_growth", ctypes.c_double),
                 ("cfl_max", ctypes.c_double), ("cfl_mode", ctypes.c_int32), ("ser_exponent", ctypes.c_double),
-                ("jvp_mode", ctypes.c_int32), ("fp32_krylov", ctypes.c_int32), ("max_seconds", ctypes.c_double)]
+                ("jvp_mode", ctypes.c_int32), ("fp32_krylov", ctypes.c_int32), ("max_seconds", ctypes.c_double),
+                ("precond_sweeps", ctypes.c_int32), ("krylov_cycles", ctypes.c_int32)]
 
 
 class NewtonReport(ctypes.Structure):

@@ -212,6 +212,45 @@ __global__ void k_precond(int nc, const double *__restrict__ Minv, const T *__re
   }
 }
 
+// One block-Jacobi sweep on the first-order operator A1 = B + O:
+// y_out = Binv (r - O y_in), with (O y)_c = -sum_{f: c parent} JR_f y_nb + sum_{f: c neighbour} JL_f y_parent.
+template <class T>
+__global__ void k_jacobi_sweep(DevMesh m, const double *__restrict__ Minv, const double *__restrict__ JL,
+                               const double *__restrict__ JR, const double *__restrict__ r, const double *__restrict__ yin,
+                               double *__restrict__ yout) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nc = m.nc, nf = m.nf;
+  if (c >= nc) return;
+  double t[5];
+#pragma unroll
+  for (int i = 0; i < 5; ++i) t[i] = r[i * nc + c];
+  for (int j = m.cf_index[c]; j < m.cf_index[c + 1]; ++j) {
+    const int e = m.cf_list[j];
+    const int f = e >= 0 ? e : ~e;
+    if (m.f_bc[f] >= 0) continue;  // boundary faces have no off-diagonal block
+    const int o = e >= 0 ? m.f_neighbor[f] : m.f_parent[f];
+    const double *J = e >= 0 ? JR : JL;
+    const double sg = e >= 0 ? 1. : -1.;  // r - O y
+    double yo[5];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) yo[k] = yin[k * nc + o];
+#pragma unroll
+    for (int i = 0; i < 5; ++i) {
+      double a = 0.;
+#pragma unroll
+      for (int k = 0; k < 5; ++k) a += J[(5 * i + k) * nf + f] * yo[k];
+      t[i] += sg * a;
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < 5; ++i) {
+    double s = 0.;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) s += Minv[(5 * i + k) * nc + c] * t[k];
+    yout[i * nc + c] = s;
+  }
+}
+
 // copy a [5][nc] state into the residual chain's [5][nt] array (+ optional eps*dir)
 template <class T>
 __global__ void k_load_state(int nc, int nt, const double *__restrict__ Wn, const T *__restrict__ dir, double eps,
@@ -396,9 +435,26 @@ struct Krylov {
 };
 
 struct NewtonState {
-  DBuf<double> Wn, R0, R1, dt, vol, JL, JR, Minv;
+  DBuf<double> Wn, R0, R1, dt, vol, JL, JR, Minv, Pr, Py0, Py1, Xs;
   double wscale = 1.;
+  int sweeps = 0, cycles = 1;
 };
+template <class T>
+__global__ void k_unscale(int nc, const T *__restrict__ v, RowScale rs, double *__restrict__ out) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nc) return;
+  for (int k = 0; k < 5; ++k) out[k * nc + c] = double(v[k * nc + c]) / rs.s[k];
+}
+template <class T>
+__global__ void k_axpy_to(int n, const double *__restrict__ b, const T *__restrict__ w, T *__restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = T(b[i] - double(w[i]));
+}
+template <class T>
+__global__ void k_cast(int n, const double *__restrict__ a, T *__restrict__ b) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) b[i] = T(a[i]);
+}
 
 // residual of the [5][nc] state (+ eps*dir) into R (SoA [5][nc])
 template <class T>
@@ -439,75 +495,112 @@ static double dnorm(fcfd_ctx *x, DBuf<double> &part, DBuf<double> &h, const doub
   return std::sqrt(r);
 }
 
-// Right-preconditioned GMRES(m), one cycle (restarts = outer Newton steps).
+// Preconditioner: z = M^-1 D^-1 v with M^-1 = `sweeps` block-Jacobi sweeps on
+// the first-order operator (0 sweeps: the block diagonal alone).
+template <class T>
+static void apply_prec(fcfd_ctx *x, NewtonState &ns, const T *v, T *z, const RowScale &rs, int sweeps) {
+  const int nc = x->dm.nc, tb = 256, gc = (nc + tb - 1) / tb;
+  cudaStream_t s = x->stream;
+  if (sweeps <= 0) {
+    k_precond<T><<<gc, tb, 0, s>>>(nc, ns.Minv.p, v, z, rs);
+    return;
+  }
+  // r = D^-1 v (double), y0 = Binv r
+  k_unscale<T><<<gc, tb, 0, s>>>(nc, v, rs, ns.Pr.p);
+  RowScale one;
+  for (int i = 0; i < 5; ++i) one.s[i] = 1.;
+  k_precond<double><<<gc, tb, 0, s>>>(nc, ns.Minv.p, ns.Pr.p, ns.Py0.p, one);
+  double *a = ns.Py0.p, *b = ns.Py1.p;
+  for (int k = 0; k < sweeps; ++k) {
+    k_jacobi_sweep<double><<<gc, tb, 0, s>>>(x->dm, ns.Minv.p, ns.JL.p, ns.JR.p, ns.Pr.p, a, b);
+    std::swap(a, b);
+  }
+  k_cast<T><<<(5 * nc + tb - 1) / tb, tb, 0, s>>>(5 * nc, a, z);
+}
+
+// Right-preconditioned GMRES(m) with up to `cycles` restarts.
 template <class T>
 static void gmres(fcfd_ctx *x, NewtonState &ns, Krylov<T> &K, int mode, double rtol, double *dW, int &iters, double &relres,
                   const RowScale &rs) {
   const int n = K.n, m = K.m, nc = K.nc;
   cudaStream_t s = x->stream;
   const int tb = 256, gn = (n + tb - 1) / tb, gc = (nc + tb - 1) / tb;
-  // row-scaled right-hand side D R0 (kept in ns.R1 until the matvecs reuse it)
-  k_rowscale_copy<<<gc, tb, 0, s>>>(nc, ns.R0.p, rs, 1., dW);
-  const double beta = dnorm(x, K.part, K.h, dW, n);
   iters = 0;
   relres = 1.;
-  if (!(beta > 0.)) {
-    CK(cudaMemsetAsync(dW, 0, sizeof(double) * n, s));
-    relres = 0.;
-    return;
-  }
-  k_scale_copy<T><<<gn, tb, 0, s>>>(n, dW, 1. / beta, K.V.p);
+  // scaled right-hand side b = D R0; x0 = 0
+  k_rowscale_copy<<<gc, tb, 0, s>>>(nc, ns.R0.p, rs, 1., dW);
+  const double bnorm = dnorm(x, K.part, K.h, dW, n);
+  CK(cudaMemsetAsync(ns.Xs.p, 0, sizeof(double) * n, s));
+  if (!(bnorm > 0.)) { CK(cudaMemsetAsync(dW, 0, sizeof(double) * n, s)); relres = 0.; return; }
   std::vector<double> H((size_t)(m + 1) * m, 0.), cs(m), sn(m), g(m + 1, 0.), h1(m + 1), h2(m + 1);
-  g[0] = beta;
-  int k = 0;
-  for (int j = 0; j < m; ++j) {
-    T *vj = K.V.p + (size_t)j * n;
-    T *w = K.V.p + (size_t)(j + 1) * n;
-    k_precond<T><<<gc, tb, 0, s>>>(nc, ns.Minv.p, vj, K.tmpT.p, rs);
-    const double zn = (mode == 0) ? K.norm(K.tmpT.p) : 0.;
-    matvec<T>(x, ns, mode, K.tmpT.p, w, zn, rs);
-    // classical Gram-Schmidt, twice
-    K.dots(j + 1, w, h1.data());
-    CK(cudaMemcpyAsync(K.h.p, h1.data(), sizeof(double) * (j + 1), cudaMemcpyHostToDevice, s));
-    k_sub_combo<T><<<gn, tb, 0, s>>>(n, j + 1, K.V.p, (size_t)n, K.h.p, w);
-    K.dots(j + 1, w, h2.data());
-    CK(cudaMemcpyAsync(K.h.p, h2.data(), sizeof(double) * (j + 1), cudaMemcpyHostToDevice, s));
-    k_sub_combo<T><<<gn, tb, 0, s>>>(n, j + 1, K.V.p, (size_t)n, K.h.p, w);
-    const double hn = K.norm(w);
-    for (int i = 0; i <= j; ++i) H[(size_t)i * m + j] = h1[i] + h2[i];
-    H[(size_t)(j + 1) * m + j] = hn;
-    if (hn > 0.) k_scale<T><<<gn, tb, 0, s>>>(n, 1. / hn, w);
-    // Givens rotations
-    for (int i = 0; i < j; ++i) {
-      const double a = H[(size_t)i * m + j], b = H[(size_t)(i + 1) * m + j];
-      H[(size_t)i * m + j] = cs[i] * a + sn[i] * b;
-      H[(size_t)(i + 1) * m + j] = -sn[i] * a + cs[i] * b;
+  for (int cyc = 0; cyc < ns.cycles; ++cyc) {
+    double beta;
+    if (cyc == 0) {
+      beta = bnorm;
+      k_scale_copy<T><<<gn, tb, 0, s>>>(n, dW, 1. / beta, K.V.p);
+    } else {
+      // r = b - (D A M^-1 D^-1 ...) applied to the current solution: recompute through one matvec of
+      // z = M^-1 D^-1 (sum) already folded into Xs (physical units): r = D (R0 - A Xs)
+      k_cast<T><<<gn, tb, 0, s>>>(n, ns.Xs.p, K.tmpT.p);
+      const double zn = (mode == 0) ? K.norm(K.tmpT.p) : 0.;
+      matvec<T>(x, ns, mode, K.tmpT.p, K.w.p, zn, rs);
+      k_rowscale_copy<<<gc, tb, 0, s>>>(nc, ns.R0.p, rs, 1., dW);
+      k_axpy_to<T><<<gn, tb, 0, s>>>(n, dW, K.w.p, K.V.p);  // V0 = b - A x (unnormalised)
+      beta = K.norm(K.V.p);
+      if (!(beta > 0.)) break;
+      k_scale<T><<<gn, tb, 0, s>>>(n, 1. / beta, K.V.p);
     }
-    const double a = H[(size_t)j * m + j], b = H[(size_t)(j + 1) * m + j];
-    const double r = std::hypot(a, b);
-    cs[j] = (r > 0.) ? a / r : 1.;
-    sn[j] = (r > 0.) ? b / r : 0.;
-    H[(size_t)j * m + j] = r;
-    H[(size_t)(j + 1) * m + j] = 0.;
-    g[j + 1] = -sn[j] * g[j];
-    g[j] = cs[j] * g[j];
-    k = j + 1;
-    relres = std::fabs(g[j + 1]) / beta;
-    if (relres <= rtol || !(hn > 0.)) break;
+    std::fill(g.begin(), g.end(), 0.);
+    g[0] = beta;
+    int k = 0;
+    bool done = false;
+    for (int j = 0; j < m; ++j) {
+      T *vj = K.V.p + (size_t)j * n;
+      T *w = K.V.p + (size_t)(j + 1) * n;
+      apply_prec<T>(x, ns, vj, K.tmpT.p, rs, ns.sweeps);
+      const double zn = (mode == 0) ? K.norm(K.tmpT.p) : 0.;
+      matvec<T>(x, ns, mode, K.tmpT.p, w, zn, rs);
+      K.dots(j + 1, w, h1.data());
+      CK(cudaMemcpyAsync(K.h.p, h1.data(), sizeof(double) * (j + 1), cudaMemcpyHostToDevice, s));
+      k_sub_combo<T><<<gn, tb, 0, s>>>(n, j + 1, K.V.p, (size_t)n, K.h.p, w);
+      K.dots(j + 1, w, h2.data());
+      CK(cudaMemcpyAsync(K.h.p, h2.data(), sizeof(double) * (j + 1), cudaMemcpyHostToDevice, s));
+      k_sub_combo<T><<<gn, tb, 0, s>>>(n, j + 1, K.V.p, (size_t)n, K.h.p, w);
+      const double hn = K.norm(w);
+      for (int i = 0; i <= j; ++i) H[(size_t)i * m + j] = h1[i] + h2[i];
+      H[(size_t)(j + 1) * m + j] = hn;
+      if (hn > 0.) k_scale<T><<<gn, tb, 0, s>>>(n, 1. / hn, w);
+      for (int i = 0; i < j; ++i) {
+        const double a = H[(size_t)i * m + j], b = H[(size_t)(i + 1) * m + j];
+        H[(size_t)i * m + j] = cs[i] * a + sn[i] * b;
+        H[(size_t)(i + 1) * m + j] = -sn[i] * a + cs[i] * b;
+      }
+      const double a = H[(size_t)j * m + j], b = H[(size_t)(j + 1) * m + j];
+      const double r = std::hypot(a, b);
+      cs[j] = (r > 0.) ? a / r : 1.;
+      sn[j] = (r > 0.) ? b / r : 0.;
+      H[(size_t)j * m + j] = r;
+      H[(size_t)(j + 1) * m + j] = 0.;
+      g[j + 1] = -sn[j] * g[j];
+      g[j] = cs[j] * g[j];
+      k = j + 1;
+      ++iters;
+      relres = std::fabs(g[j + 1]) / bnorm;
+      if (relres <= rtol || !(hn > 0.)) { done = true; break; }
+    }
+    std::vector<double> y(k, 0.);
+    for (int i = k - 1; i >= 0; --i) {
+      double t = g[i];
+      for (int l = i + 1; l < k; ++l) t -= H[(size_t)i * m + l] * y[l];
+      y[i] = t / H[(size_t)i * m + i];
+    }
+    CK(cudaMemcpyAsync(K.h.p, y.data(), sizeof(double) * k, cudaMemcpyHostToDevice, s));
+    k_combo<T><<<gn, tb, 0, s>>>(n, k, K.V.p, (size_t)n, K.h.p, K.w.p);
+    apply_prec<T>(x, ns, K.w.p, K.tmpT.p, rs, ns.sweeps);
+    k_update<T><<<gn, tb, 0, s>>>(n, ns.Xs.p, K.tmpT.p, 1., x->err.p);
+    if (done) break;
   }
-  // back substitution H(0:k,0:k) y = g
-  std::vector<double> y(k, 0.);
-  for (int i = k - 1; i >= 0; --i) {
-    double t = g[i];
-    for (int l = i + 1; l < k; ++l) t -= H[(size_t)i * m + l] * y[l];
-    y[i] = t / H[(size_t)i * m + i];
-  }
-  CK(cudaMemcpyAsync(K.h.p, y.data(), sizeof(double) * k, cudaMemcpyHostToDevice, s));
-  k_combo<T><<<gn, tb, 0, s>>>(n, k, K.V.p, (size_t)n, K.h.p, K.w.p);
-  k_precond<T><<<gc, tb, 0, s>>>(nc, ns.Minv.p, K.w.p, K.tmpT.p, rs);
-  CK(cudaMemsetAsync(dW, 0, sizeof(double) * n, s));
-  k_update<T><<<gn, tb, 0, s>>>(n, dW, K.tmpT.p, 1., x->err.p);
-  iters = k;
+  CK(cudaMemcpyAsync(dW, ns.Xs.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
   CK(cudaGetLastError());
 }
 
@@ -529,6 +622,8 @@ int fcfd_newton_solve(fcfd_ctx *x, double *W, const fcfd_newton_opts *o, fcfd_ne
     NewtonState ns;
     ns.Wn.alloc(n); ns.R0.alloc(n); ns.R1.alloc(n); ns.dt.alloc(nc); ns.vol.alloc(nc);
     ns.JL.alloc(25 * (size_t)m.nf); ns.JR.alloc(25 * (size_t)m.nf); ns.Minv.alloc(25 * (size_t)nc);
+    ns.Pr.alloc(n); ns.Py0.alloc(n); ns.Py1.alloc(n); ns.Xs.alloc(n);
+    ns.sweeps = o->precond_sweeps; ns.cycles = o->krylov_cycles > 0 ? o->krylov_cycles : 1;
     CK(cudaMemsetAsync(ns.JR.p, 0, sizeof(double) * 25 * (size_t)m.nf, s));
     std::vector<double> vol(x->mesh->c_volume.begin(), x->mesh->c_volume.begin() + nc);
     CK(cudaMemcpyAsync(ns.vol.p, vol.data(), sizeof(double) * nc, cudaMemcpyHostToDevice, s));
@@ -539,6 +634,7 @@ int fcfd_newton_solve(fcfd_ctx *x, double *W, const fcfd_newton_opts *o, fcfd_ne
     Krylov<float> K32;
     const bool f32 = o->fp32_krylov != 0;
     x->newton_frozen = o->jvp_mode == 1;
+    const int jmode = o->jvp_mode == 0 ? 0 : 1;
     if (f32) K32.alloc(x, mdim); else K64.alloc(x, mdim);
     DBuf<double> part, hh;
     part.alloc(kRedBlocks); hh.alloc(1);
@@ -589,8 +685,8 @@ int fcfd_newton_solve(fcfd_ctx *x, double *W, const fcfd_newton_opts *o, fcfd_ne
       int kit = 0;
       double rr = 0.;
       const double krtol = o->krylov_rtol > 0 ? o->krylov_rtol : 1e-2;
-      if (f32) gmres<float>(x, ns, K32, o->jvp_mode, krtol, ns.R1.p, kit, rr, rs);
-      else gmres<double>(x, ns, K64, o->jvp_mode, krtol, ns.R1.p, kit, rr, rs);
+      if (f32) gmres<float>(x, ns, K32, jmode, krtol, ns.R1.p, kit, rr, rs);
+      else gmres<double>(x, ns, K64, jmode, krtol, ns.R1.p, kit, rr, rs);
       rep->krylov_iterations += kit;
       // relax the update so that p and T change by at most 20 % per step
       CK(cudaMemsetAsync(key.p, 0, sizeof(unsigned long long), s));

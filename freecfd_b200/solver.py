@@ -148,13 +148,13 @@ class NavierStokes:
 
     def newton_solve(self, W, tol=1e-10, max_newton=200, krylov_dim=30, krylov_rtol=1e-2, cfl0=1.0,
                      cfl_growth=1.2, cfl_max=1e6, cfl_mode=1, ser_exponent=1.0, jvp=True, fp32_krylov=False,
-                     max_seconds=0.0, raise_on_fail=True):
+                     max_seconds=0.0, raise_on_fail=True, precond_sweeps=0, krylov_cycles=1, exact_jvp=False):
         """Steady solve R(W) = 0 (pseudo-transient Newton-Krylov on the device).
         Returns (W_converged, report dict)."""
         W = np.array(W, dtype=np.float64, order="C", copy=True)
         o = NewtonOpts(int(max_newton), float(tol), int(krylov_dim), float(krylov_rtol), float(cfl0), float(cfl_growth),
-                       float(cfl_max), int(cfl_mode), float(ser_exponent), int(bool(jvp)), int(bool(fp32_krylov)),
-                       float(max_seconds))
+                       float(cfl_max), int(cfl_mode), float(ser_exponent), (2 if exact_jvp else 1) if jvp else 0,
+                       int(bool(fp32_krylov)), float(max_seconds), int(precond_sweeps), int(krylov_cycles))
         r = NewtonReport()
         rc = lib.fcfd_newton_solve(self.h, _d(W), ctypes.byref(o), ctypes.byref(r))
         rep = dict(status=r.status, newton_iterations=r.newton_iterations, krylov_iterations=r.krylov_iterations,

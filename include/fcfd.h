@@ -141,9 +141,12 @@ typedef struct fcfd_newton_opts {
   int32_t cfl_mode;       /* 0: reference ramp (time_step.cc:146-156); 1: CFL0 * (|R0|/|R|)^ser_exponent */
   double ser_exponent;
   int32_t jvp_mode;       /* 0: finite-difference J.v of the FP64 residual; 1: tangent (dual-number)
-                             kernels with the limiter held fixed (frozen-limiter Jacobian) */
+                             kernels with the limiter held fixed (frozen-limiter Jacobian);
+                             2: tangent kernels, exact (limiter differentiated too) */
   int32_t fp32_krylov;    /* 1: Krylov basis and preconditioned vectors in FP32 (dot products in FP64) */
   double max_seconds;     /* wall-clock cap (0: none) */
+  int32_t precond_sweeps; /* block-Jacobi sweeps on the first-order operator (0: block diagonal only) */
+  int32_t krylov_cycles;  /* GMRES(m) restarts per Newton step (default 1) */
 } fcfd_newton_opts;
 
 typedef struct fcfd_newton_report {
