@@ -84,7 +84,8 @@ struct fcfd_ctx {
   const fcfd_mesh *mesh = nullptr;
   bool viscous = false;
   // mesh arrays
-  DBuf<int> f_parent, f_neighbor, f_bc, cf_index, cf_list, st_index, st_keys, bface, outlet;
+  DBuf<int> f_parent, f_neighbor, f_bc, cf_index, cf_list, st_index, st_keys, bface, outlet, color_cells;
+  std::vector<int> color_index;
   DBuf<double> f_n, f_area, f_x, f_w, c_x, c_len, st_cof, st_self;
   // state arrays
   Pipe<double> p64;

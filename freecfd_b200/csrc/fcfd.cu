@@ -223,6 +223,8 @@ int fcfd_ctx_create(const fcfd_mesh *mp, const fcfd_case *csp, int device, fcfd_
     }
   }
   x->bface.upload(bface);
+  x->color_cells.upload(m.color_cells);
+  x->color_index = m.color_index;
   x->outlet.upload(outl);
   x->n_outlet = (int)outl.size();
   // ---- state buffers

@@ -88,6 +88,7 @@ struct fcfd_mesh {
   std::vector<double> st_cof;                                // [nc][7]: C00 C01 C02 C11 C12 C22 det
   std::vector<double> st_self;                               // [nc][3]: self weight
   std::vector<uint8_t> has_lsq;                              // 1 if gradMap non-empty
+  std::vector<int32_t> color_index, color_cells;             // face-neighbour colouring
   std::vector<double> nodes;                                 // [nnode][3]
   double length_scale = 0, total_volume = 0;
   std::vector<double> bc_total_area;

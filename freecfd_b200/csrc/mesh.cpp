@@ -428,6 +428,32 @@ fcfd_mesh *build_mesh(const fcfd_raw_mesh &raw, fcfd_case &cs) {
     } else {
       throw Error(FCFD_ERR_UNSUPPORTED, "IDW face interpolation is not supported on the B200 path");
     }
+    // ---------------- greedy colouring of the face-neighbour graph (cells of one
+    // colour share no face), used by the multicolour Gauss-Seidel preconditioner
+    {
+      std::vector<int32_t> col(nc, -1);
+      int ncol = 0;
+      std::vector<char> used;
+      for (int c = 0; c < nc; ++c) {
+        used.assign(ncol + 1, 0);
+        for (int j = m.cf_index[c]; j < m.cf_index[c + 1]; ++j) {
+          int f = m.cf_list[j];
+          if (m.f_bc[f] >= 0) continue;
+          int o = (m.f_parent[f] == c) ? m.f_neighbor[f] : m.f_parent[f];
+          if (col[o] >= 0) used[col[o]] = 1;
+        }
+        int k = 0;
+        while (k < ncol && used[k]) ++k;
+        col[c] = k;
+        if (k == ncol) ++ncol;
+      }
+      m.color_index.assign(ncol + 1, 0);
+      for (int c = 0; c < nc; ++c) m.color_index[col[c] + 1]++;
+      for (int k = 0; k < ncol; ++k) m.color_index[k + 1] += m.color_index[k];
+      m.color_cells.resize(nc);
+      std::vector<int32_t> fill(m.color_index.begin(), m.color_index.end() - 1);
+      for (int c = 0; c < nc; ++c) m.color_cells[fill[col[c]]++] = c;
+    }
     // ---------------- least-squares gradient data (lsqr_grad_map.cc:32-99)
     m.st_index.assign(nc + 1, 0);
     m.st_cof.assign(7 * (size_t)nc, 0.);

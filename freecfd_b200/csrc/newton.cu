@@ -251,6 +251,45 @@ __global__ void k_jacobi_sweep(DevMesh m, const double *__restrict__ Minv, const
   }
 }
 
+// Block Gauss-Seidel update of the cells of one colour, in place:
+// y_c = Binv (r - O y)_c (no two cells of a colour share a face).
+__global__ void k_gs_color(DevMesh m, const int *__restrict__ cells, int ncells, const double *__restrict__ Minv,
+                           const double *__restrict__ JL, const double *__restrict__ JR, const double *__restrict__ r,
+                           double *__restrict__ y) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= ncells) return;
+  const int c = cells[i];
+  const int nc = m.nc, nf = m.nf;
+  double t[5];
+#pragma unroll
+  for (int q = 0; q < 5; ++q) t[q] = r[q * nc + c];
+  for (int j = m.cf_index[c]; j < m.cf_index[c + 1]; ++j) {
+    const int e = m.cf_list[j];
+    const int f = e >= 0 ? e : ~e;
+    if (m.f_bc[f] >= 0) continue;
+    const int o = e >= 0 ? m.f_neighbor[f] : m.f_parent[f];
+    const double *J = e >= 0 ? JR : JL;
+    const double sg = e >= 0 ? 1. : -1.;
+    double yo[5];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) yo[k] = y[k * nc + o];
+#pragma unroll
+    for (int q = 0; q < 5; ++q) {
+      double a = 0.;
+#pragma unroll
+      for (int k = 0; k < 5; ++k) a += J[(5 * q + k) * nf + f] * yo[k];
+      t[q] += sg * a;
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < 5; ++q) {
+    double s = 0.;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) s += Minv[(5 * q + k) * nc + c] * t[k];
+    y[q * nc + c] = s;
+  }
+}
+
 // copy a [5][nc] state into the residual chain's [5][nt] array (+ optional eps*dir)
 template <class T>
 __global__ void k_load_state(int nc, int nt, const double *__restrict__ Wn, const T *__restrict__ dir, double eps,
@@ -495,8 +534,8 @@ static double dnorm(fcfd_ctx *x, DBuf<double> &part, DBuf<double> &h, const doub
   return std::sqrt(r);
 }
 
-// Preconditioner: z = M^-1 D^-1 v with M^-1 = `sweeps` block-Jacobi sweeps on
-// the first-order operator (0 sweeps: the block diagonal alone).
+// Preconditioner: z = M^-1 D^-1 v with M^-1 = `sweeps` symmetric multicolour
+// block Gauss-Seidel sweeps on the first-order operator (0: block diagonal alone).
 template <class T>
 static void apply_prec(fcfd_ctx *x, NewtonState &ns, const T *v, T *z, const RowScale &rs, int sweeps) {
   const int nc = x->dm.nc, tb = 256, gc = (nc + tb - 1) / tb;
@@ -510,10 +549,18 @@ static void apply_prec(fcfd_ctx *x, NewtonState &ns, const T *v, T *z, const Row
   RowScale one;
   for (int i = 0; i < 5; ++i) one.s[i] = 1.;
   k_precond<double><<<gc, tb, 0, s>>>(nc, ns.Minv.p, ns.Pr.p, ns.Py0.p, one);
-  double *a = ns.Py0.p, *b = ns.Py1.p;
+  double *a = ns.Py0.p;
+  // symmetric multicolour block Gauss-Seidel: colours forward, then backward
+  const std::vector<int> &ci = x->color_index;
+  const int ncol = (int)ci.size() - 1;
   for (int k = 0; k < sweeps; ++k) {
-    k_jacobi_sweep<double><<<gc, tb, 0, s>>>(x->dm, ns.Minv.p, ns.JL.p, ns.JR.p, ns.Pr.p, a, b);
-    std::swap(a, b);
+    for (int pass = 0; pass < 2; ++pass)
+      for (int q = 0; q < ncol; ++q) {
+        const int col = pass == 0 ? q : ncol - 1 - q;
+        const int cnt = ci[col + 1] - ci[col];
+        if (cnt > 0)
+          k_gs_color<<<(cnt + tb - 1) / tb, tb, 0, s>>>(x->dm, x->color_cells.p + ci[col], cnt, ns.Minv.p, ns.JL.p, ns.JR.p, ns.Pr.p, a);
+      }
   }
   k_cast<T><<<(5 * nc + tb - 1) / tb, tb, 0, s>>>(5 * nc, a, z);
 }

@@ -145,7 +145,8 @@ typedef struct fcfd_newton_opts {
                              2: tangent kernels, exact (limiter differentiated too) */
   int32_t fp32_krylov;    /* 1: Krylov basis and preconditioned vectors in FP32 (dot products in FP64) */
   double max_seconds;     /* wall-clock cap (0: none) */
-  int32_t precond_sweeps; /* block-Jacobi sweeps on the first-order operator (0: block diagonal only) */
+  int32_t precond_sweeps; /* symmetric multicolour block Gauss-Seidel sweeps on the first-order
+                             operator (0: block-Jacobi, the block diagonal only) */
   int32_t krylov_cycles;  /* GMRES(m) restarts per Newton step (default 1) */
 } fcfd_newton_opts;
 
