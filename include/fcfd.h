@@ -171,6 +171,21 @@ int fcfd_newton_solve(fcfd_ctx *ctx, double *W, const fcfd_newton_opts *opts, fc
  * milliseconds: out[0] total per residual, out[1..] per kernel (see fcfd.cu). */
 int fcfd_time_residual(fcfd_ctx *ctx, int reps, int flush_l2, double *out, int out_len);
 
+/* Allocation-free CFL_MAX local time step, for callers that cannot call
+ * cudaMalloc (host applications that own all device memory through their own
+ * pool, code that must not allocate once set up).  No counterpart in the
+ * reference.  Same result as fcfd_local_dt(mode 1) but with no context: all
+ * pointers are device pointers, W[n_cells][5] = (p,u,v,w,T), length[n_cells]
+ * = cell length scales, dt[n_cells] output; gas_R, Pref, Tref as in the deck;
+ * stream may be NULL (legacy default stream).  The scratch for the global
+ * minimum is a file-scope __device__ array of 4096+32 doubles, so n_cells is
+ * limited to 1,048,576 (larger sizes return FCFD_ERR_INPUT).  The first call
+ * on a device looks up the array's device address (cudaGetSymbolAddress);
+ * make that first call before any stream capture.  Every call shares the one
+ * array: calls that overlap on the GPU race and must be serialised. */
+int fcfd_local_dt_cflmax_noalloc(const double *W, const double *length, int32_t n_cells, double gamma, double gas_R,
+                                 double Pref, double Tref, double cfl, double *dt, void *stream);
+
 /* Point fluxes in the reference's rotated-frame signature
  * (roe_flux ns_roe.cc:25, AUSMplusUP_flux ns_ausm_plus_up.cc:35,
  * vanLeer_flux ns_vanleer.cc:25).  L/R = (p,u,v,w,T) face states,
