@@ -68,6 +68,10 @@ template <int N> __device__ __forceinline__ DN<N> pow(const DN<N> &a, double e) 
 
 typedef DN<5> D5;
 
+struct RowScale {
+  double s[5];  // per-equation weight of the GMRES norm
+};
+
 // ------------------------------------------------------------------ face Jacobians
 __device__ __forceinline__ void seed(const FState<double> &s, FState<D5> &o, const DevCase &cs, const double n[3]) {
   // perturbations of state_perturb (ns_assemble_linear_system.cc:417-458):
@@ -145,7 +149,8 @@ __device__ __forceinline__ void cons2prim(const DevCase &cs, double p, double u,
 // Block assembly + inversion (Gauss-Jordan, partial pivoting): Minv_c = (V P/dt - J_cc)^-1
 __global__ void k_block_jacobi(DevCase cs, DevMesh m, const double *__restrict__ Wn, const double *__restrict__ vol,
                                const double *__restrict__ dt, const double *__restrict__ JL, const double *__restrict__ JR,
-                               double *__restrict__ Minv, int *__restrict__ err) {
+                               double *__restrict__ Minv, int *__restrict__ err, RowScale wref,
+                               double *__restrict__ rowmag) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   const int nc = m.nc, nf = m.nf;
   if (c >= nc) return;
@@ -164,6 +169,14 @@ __global__ void k_block_jacobi(DevCase cs, DevMesh m, const double *__restrict__
 #pragma unroll
       for (int i = 0; i < 25; ++i) B[i] += JR[i * nf + f];
     }
+  }
+  // magnitude of each equation's row for reference state changes: sum_k |B_ik| Wref_k
+#pragma unroll
+  for (int i = 0; i < 5; ++i) {
+    double s = 0.;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) s += ::fabs(B[5 * i + k]) * wref.s[k];
+    rowmag[i * nc + c] = s;
   }
   double I[25];
 #pragma unroll
@@ -192,9 +205,6 @@ __global__ void k_block_jacobi(DevCase cs, DevMesh m, const double *__restrict__
 }
 
 // z = Minv x (per-cell 5x5), vectors [5][nc] of type T
-struct RowScale {
-  double s[5];  // per-equation weight of the GMRES norm
-};
 // z = Minv (D^-1 x): right preconditioner of the row-scaled system D A
 template <class T>
 __global__ void k_precond(int nc, const double *__restrict__ Minv, const T *__restrict__ x, T *__restrict__ z, RowScale rs) {
@@ -474,7 +484,7 @@ struct Krylov {
 };
 
 struct NewtonState {
-  DBuf<double> Wn, R0, R1, dt, vol, JL, JR, Minv, Pr, Py0, Py1, Xs;
+  DBuf<double> Wn, R0, R1, dt, vol, JL, JR, Minv, Pr, Py0, Py1, Xs, rowmag;
   double wscale = 1.;
   int sweeps = 0, cycles = 1;
 };
@@ -669,7 +679,7 @@ int fcfd_newton_solve(fcfd_ctx *x, double *W, const fcfd_newton_opts *o, fcfd_ne
     NewtonState ns;
     ns.Wn.alloc(n); ns.R0.alloc(n); ns.R1.alloc(n); ns.dt.alloc(nc); ns.vol.alloc(nc);
     ns.JL.alloc(25 * (size_t)m.nf); ns.JR.alloc(25 * (size_t)m.nf); ns.Minv.alloc(25 * (size_t)nc);
-    ns.Pr.alloc(n); ns.Py0.alloc(n); ns.Py1.alloc(n); ns.Xs.alloc(n);
+    ns.Pr.alloc(n); ns.Py0.alloc(n); ns.Py1.alloc(n); ns.Xs.alloc(n); ns.rowmag.alloc(n);
     ns.sweeps = o->precond_sweeps; ns.cycles = o->krylov_cycles > 0 ? o->krylov_cycles : 1;
     CK(cudaMemsetAsync(ns.JR.p, 0, sizeof(double) * 25 * (size_t)m.nf, s));
     std::vector<double> vol(x->mesh->c_volume.begin(), x->mesh->c_volume.begin() + nc);
@@ -714,20 +724,35 @@ int fcfd_newton_solve(fcfd_ctx *x, double *W, const fcfd_newton_opts *o, fcfd_ne
       if (rm <= o->tol * r0) { status = FCFD_OK; break; }
       if (o->max_seconds > 0 &&
           std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() > o->max_seconds) break;
-      // GMRES norm weights: each equation's residual counts equally
-      double rmax = 0.;
-      for (int v = 0; v < 5; ++v) rmax = std::max(rmax, rows[v]);
-      RowScale rs;
-      for (int v = 0; v < 5; ++v) rs.s[v] = 1. / std::max(rows[v], 1e-10 * rmax);
       // local time step on the current state (loaded by the last residual)
       k_local_dt<double><<<gc, tb, 0, s>>>(x->cs, m, x->p64.W.p, ns.dt.p, cfl, nullptr);
+      // reference state magnitudes: RMS of |p+Pref|, |V|, |T+Tref|
+      RowScale wref;
+      {
+        double rp = dnorm(x, part, hh, ns.Wn.p, nc), ru = dnorm(x, part, hh, ns.Wn.p + nc, nc);
+        double rv = dnorm(x, part, hh, ns.Wn.p + 2 * (size_t)nc, nc), rw = dnorm(x, part, hh, ns.Wn.p + 3 * (size_t)nc, nc);
+        double rT = dnorm(x, part, hh, ns.Wn.p + 4 * (size_t)nc, nc);
+        const double sq = std::sqrt((double)nc);
+        double U = std::sqrt(ru * ru + rv * rv + rw * rw) / sq;
+        wref.s[0] = rp / sq + std::fabs(x->cs.Pref);
+        wref.s[4] = rT / sq + std::fabs(x->cs.Tref);
+        if (!(U > 0.)) U = std::sqrt(x->cs.gamma * x->cs.R * wref.s[4]);
+        wref.s[1] = wref.s[2] = wref.s[3] = U;
+      }
       // block-Jacobi preconditioner from the first-order face Jacobians
       if (x->viscous)
         k_face_jac<true><<<(m.nf + 127) / 128, 128, 0, s>>>(x->cs, m, x->p64.W.p, x->p64.G.p, x->p64.Lm.p, x->p64.stale.p, ns.JL.p, ns.JR.p);
       else
         k_face_jac<false><<<(m.nf + 127) / 128, 128, 0, s>>>(x->cs, m, x->p64.W.p, x->p64.G.p, x->p64.Lm.p, x->p64.stale.p, ns.JL.p, ns.JR.p);
-      k_block_jacobi<<<gc, tb, 0, s>>>(x->cs, m, ns.Wn.p, ns.vol.p, ns.dt.p, ns.JL.p, ns.JR.p, ns.Minv.p, x->err.p);
+      k_block_jacobi<<<gc, tb, 0, s>>>(x->cs, m, ns.Wn.p, ns.vol.p, ns.dt.p, ns.JL.p, ns.JR.p, ns.Minv.p, x->err.p, wref, ns.rowmag.p);
       CK(cudaGetLastError());
+      // GMRES norm weights: 1 / RMS row magnitude, so every equation is measured
+      // in units of a relative state change (consistent across equations)
+      RowScale rs;
+      for (int v = 0; v < 5; ++v) {
+        const double r = dnorm(x, part, hh, ns.rowmag.p + (size_t)v * nc, nc) / std::sqrt((double)nc);
+        rs.s[v] = (r > 0.) ? 1. / r : 1.;
+      }
       ns.wscale = dnorm(x, part, hh, ns.Wn.p, n);
       int kit = 0;
       double rr = 0.;
