@@ -62,17 +62,13 @@ namespace fcfd {
 // number for tangent runs).
 template <class S>
 struct Pipe {
-  DBuf<S> X, D, stale, R;  // X: per-cell records [nt][REC]
+  DBuf<S> W, G, Lm, D, stale, R;
   bool ready = false;
-  void alloc(int nc, int nf, int nb, const double *c_x) {
+  void alloc(int nc, int nf, int nb) {
     const int nt = nc + nb;
-    X.alloc((size_t)REC * nt); D.alloc(5 * (size_t)nf);
+    W.alloc(5 * (size_t)nt); G.alloc(15 * (size_t)nc); Lm.alloc(5 * (size_t)nc); D.alloc(5 * (size_t)nf);
     stale.alloc(nb > 0 ? nb : 1); R.alloc(5 * (size_t)nc);
-    CK(cudaMemset(X.p, 0, sizeof(S) * (size_t)REC * nt));
     CK(cudaMemset(stale.p, 0, sizeof(S) * (nb > 0 ? nb : 1)));
-    k_init_centroids<S><<<(nt + 255) / 256, 256>>>(c_x, X.p, nt);
-    CK(cudaGetLastError());
-    CK(cudaDeviceSynchronize());
     ready = true;
   }
 };

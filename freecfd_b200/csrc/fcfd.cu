@@ -36,20 +36,20 @@ void launch_chain(fcfd_ctx *x, Pipe<S> &P, S *Rout, bool aos_out, S *mo, S *wo, 
   for (int k = 1; k < 8; k += 2) CK(cudaMemsetAsync(x->ext.p + k, 0xFF, sizeof(unsigned long long), s));
   const bool need_ext = x->cs.limiter == 1 && x->cs.order != 1;
   const int ng = (m.nb + tb - 1) / tb + (need_ext ? kExtremaBlocks : 0);
-  if (ng > 0) k_ghost_minmax<S><<<ng, tb, 0, s>>>(x->cs, m, P.X.p, need_ext ? x->ext.p : nullptr, x->err.p);
+  if (ng > 0) k_ghost_minmax<S><<<ng, tb, 0, s>>>(x->cs, m, P.W.p, need_ext ? x->ext.p : nullptr, x->err.p);
   const int *argx = nullptr;
   if (!std::is_same<S, double>::value && x->cs.limiter == 1 && x->cs.order != 1) {
     CK(cudaMemsetAsync(x->argx.p, 0x7F, 8 * sizeof(int), s));
-    k_argext<S><<<(m.nc + tb - 1) / tb, tb, 0, s>>>(m, P.X.p, x->ext.p, x->argx.p);
+    k_argext<S><<<(m.nc + tb - 1) / tb, tb, 0, s>>>(m, P.W.p, x->ext.p, x->argx.p);
     argx = x->argx.p;
   }
-  k_grad_limiter<S><<<(4 * m.nc + 127) / 128, 128, 0, s>>>(csl, m, P.X.p, x->ext.p, argx);
+  k_grad_limiter<S><<<(m.nc + 127) / 128, 128, 0, s>>>(csl, m, P.W.p, x->ext.p, argx, P.G.p, P.Lm.p);
   if (m.n_outlet > 0)
-    k_outlet_rho<S><<<(m.n_outlet + 127) / 128, 128, 0, s>>>(x->cs, m, P.X.p, P.stale.p);
+    k_outlet_rho<S><<<(m.n_outlet + 127) / 128, 128, 0, s>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p);
   if (x->viscous)
-    k_face_flux<S, true><<<(m.nf + 127) / 128, 128, 0, s>>>(x->cs, m, P.X.p, P.stale.p, (const S *)nullptr, P.D.p, mo, wo, x->err.p);
+    k_face_flux<S, true><<<(m.nf + 127) / 128, 128, 0, s>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p, (const S *)nullptr, P.D.p, mo, wo, x->err.p);
   else
-    k_face_flux<S, false><<<(m.nf + 127) / 128, 128, 0, s>>>(x->cs, m, P.X.p, P.stale.p, (const S *)nullptr, P.D.p, mo, wo, x->err.p);
+    k_face_flux<S, false><<<(m.nf + 127) / 128, 128, 0, s>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p, (const S *)nullptr, P.D.p, mo, wo, x->err.p);
   if (aos_out)
     k_gather<S, true><<<(m.nc + tb - 1) / tb, tb, 0, s>>>(m, P.D.p, Rout);
   else
@@ -228,7 +228,7 @@ int fcfd_ctx_create(const fcfd_mesh *mp, const fcfd_case *csp, int device, fcfd_
   x->outlet.upload(outl);
   x->n_outlet = (int)outl.size();
   // ---- state buffers
-  x->p64.alloc(nc, nf, nb, x->c_x.p);
+  x->p64.alloc(nc, nf, nb);
   x->Win.alloc(5 * (size_t)nc); x->Vin.alloc(5 * (size_t)nc); x->Rtmp.alloc(5 * (size_t)nc); x->dt.alloc(nc);
   x->mdot.alloc(nf); x->wl.alloc(nf); x->ext.alloc(8); x->err.alloc(1); x->argx.alloc(8);
   CK(cudaMemset(x->err.p, 0, sizeof(int)));
@@ -263,7 +263,7 @@ int fcfd_residual(fcfd_ctx *x, const double *W, double *R, int flags) {
     CK(cudaMemcpyAsync(x->Win.p, W, sizeof(double) * 5 * m.nc, cudaMemcpyHostToDevice, x->stream));
     win = x->Win.p;
   }
-  k_load_rec<double><<<(m.nc + 255) / 256, 256, 0, x->stream>>>(win, x->p64.X.p, m.nc);
+  k_aos_to_soa<double><<<(m.nc + 255) / 256, 256, 0, x->stream>>>(win, x->p64.W.p, m.nc, m.nt);
   double *rout = dev ? R : x->Rtmp.p;
   launch_chain<double>(x, x->p64, rout, true, x->mdot.p, x->wl.p);
   if (!dev) CK(cudaMemcpyAsync(R, x->Rtmp.p, sizeof(double) * 5 * m.nc, cudaMemcpyDeviceToHost, x->stream));
@@ -276,17 +276,21 @@ int fcfd_last_stages(fcfd_ctx *x, double *grads, double *limiter, double *ghost,
   CK(cudaSetDevice(x->device));
   CK(cudaStreamSynchronize(x->stream));
   const DevMesh &m = x->dm;
-  std::vector<double> h((size_t)REC * m.nt);
-  CK(cudaMemcpy(h.data(), x->p64.X.p, sizeof(double) * h.size(), cudaMemcpyDeviceToHost));
-  if (grads)
-    for (int c = 0; c < m.nc; ++c)
-      for (int i = 0; i < 15; ++i) grads[15 * (size_t)c + i] = h[(size_t)REC * c + RG + i];
-  if (limiter)
-    for (int c = 0; c < m.nc; ++c)
-      for (int v = 0; v < 5; ++v) limiter[5 * (size_t)c + v] = h[(size_t)REC * c + RL + v];
-  if (ghost)
+  auto get = [&](const double *src, size_t n, int k, double *dst) {
+    if (!dst) return;
+    std::vector<double> h(n * k);
+    CK(cudaMemcpy(h.data(), src, sizeof(double) * n * k, cudaMemcpyDeviceToHost));
+    for (size_t i = 0; i < n; ++i)
+      for (int j = 0; j < k; ++j) dst[i * k + j] = h[j * n + i];
+  };
+  get(x->p64.G.p, m.nc, 15, grads);
+  get(x->p64.Lm.p, m.nc, 5, limiter);
+  if (ghost) {
+    std::vector<double> h(5 * (size_t)m.nt);
+    CK(cudaMemcpy(h.data(), x->p64.W.p, sizeof(double) * 5 * m.nt, cudaMemcpyDeviceToHost));
     for (int g = 0; g < m.nb; ++g)
-      for (int v = 0; v < 5; ++v) ghost[5 * (size_t)g + v] = h[(size_t)REC * (m.nc + g) + v];
+      for (int v = 0; v < 5; ++v) ghost[5 * g + v] = h[(size_t)v * m.nt + m.nc + g];
+  }
   if (mdot) CK(cudaMemcpy(mdot, x->mdot.p, sizeof(double) * m.nf, cudaMemcpyDeviceToHost));
   if (weightL) CK(cudaMemcpy(weightL, x->wl.p, sizeof(double) * m.nf, cudaMemcpyDeviceToHost));
   API_END
@@ -302,10 +306,10 @@ int fcfd_local_dt(fcfd_ctx *x, const double *W, double cfl, int mode, double *dt
     CK(cudaMemcpyAsync(x->Win.p, W, sizeof(double) * 5 * m.nc, cudaMemcpyHostToDevice, x->stream));
     win = x->Win.p;
   }
-  k_load_rec<double><<<(m.nc + 255) / 256, 256, 0, x->stream>>>(win, x->p64.X.p, m.nc);
+  k_aos_to_soa<double><<<(m.nc + 255) / 256, 256, 0, x->stream>>>(win, x->p64.W.p, m.nc, m.nt);
   double *out = dev ? dt : x->dt.p;
   if (mode == 1) CK(cudaMemsetAsync(x->ext.p, 0xFF, sizeof(unsigned long long), x->stream));
-  k_local_dt<double><<<(m.nc + 255) / 256, 256, 0, x->stream>>>(x->cs, m, x->p64.X.p, out, cfl, mode == 1 ? x->ext.p : nullptr);
+  k_local_dt<double><<<(m.nc + 255) / 256, 256, 0, x->stream>>>(x->cs, m, x->p64.W.p, out, cfl, mode == 1 ? x->ext.p : nullptr);
   if (mode == 1) k_fill_min<double><<<(m.nc + 255) / 256, 256, 0, x->stream>>>(m.nc, out, x->ext.p);
   CK(cudaGetLastError());
   if (!dev) CK(cudaMemcpyAsync(dt, x->dt.p, sizeof(double) * m.nc, cudaMemcpyDeviceToHost, x->stream));
@@ -333,17 +337,17 @@ int fcfd_time_residual(fcfd_ctx *x, int reps, int flush_l2, double *out, int out
     const bool need_ext = x->cs.limiter == 1 && x->cs.order != 1;
     const int ng = (m.nb + tb - 1) / tb + (need_ext ? kExtremaBlocks : 0);
     Pipe<double> &P = x->p64;
-    if (ng > 0) k_ghost_minmax<double><<<ng, tb, 0, s>>>(x->cs, m, P.X.p, need_ext ? x->ext.p : nullptr, x->err.p);
+    if (ng > 0) k_ghost_minmax<double><<<ng, tb, 0, s>>>(x->cs, m, P.W.p, need_ext ? x->ext.p : nullptr, x->err.p);
     CK(cudaEventRecord(t.ev[1], s));
-    k_grad_limiter<double><<<(4 * m.nc + 127) / 128, 128, 0, s>>>(x->cs, m, P.X.p, x->ext.p, nullptr);
+    k_grad_limiter<double><<<(m.nc + 127) / 128, 128, 0, s>>>(x->cs, m, P.W.p, x->ext.p, nullptr, P.G.p, P.Lm.p);
     CK(cudaEventRecord(t.ev[2], s));
     if (m.n_outlet > 0)
-      k_outlet_rho<double><<<(m.n_outlet + 127) / 128, 128, 0, s>>>(x->cs, m, P.X.p, P.stale.p);
+      k_outlet_rho<double><<<(m.n_outlet + 127) / 128, 128, 0, s>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p);
     CK(cudaEventRecord(t.ev[3], s));
     if (x->viscous)
-      k_face_flux<double, true><<<(m.nf + 127) / 128, 128, 0, s>>>(x->cs, m, P.X.p, P.stale.p, nullptr, P.D.p, nullptr, nullptr, x->err.p);
+      k_face_flux<double, true><<<(m.nf + 127) / 128, 128, 0, s>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p, nullptr, P.D.p, nullptr, nullptr, x->err.p);
     else
-      k_face_flux<double, false><<<(m.nf + 127) / 128, 128, 0, s>>>(x->cs, m, P.X.p, P.stale.p, nullptr, P.D.p, nullptr, nullptr, x->err.p);
+      k_face_flux<double, false><<<(m.nf + 127) / 128, 128, 0, s>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p, nullptr, P.D.p, nullptr, nullptr, x->err.p);
     CK(cudaEventRecord(t.ev[4], s));
     k_gather<double, false><<<(m.nc + tb - 1) / tb, tb, 0, s>>>(m, P.D.p, P.R.p);
     CK(cudaEventRecord(t.ev[5], s));
@@ -363,7 +367,7 @@ int fcfd_jvp(fcfd_ctx *x, const double *W, const double *V, double *R, double *J
   if (!x || !W || !V || !JV) throw Error(FCFD_ERR_INPUT, "null argument");
   CK(cudaSetDevice(x->device));
   const DevMesh &m = x->dm;
-  if (!x->pjv.ready) x->pjv.alloc(m.nc, m.nf, m.nb, x->c_x.p);
+  if (!x->pjv.ready) x->pjv.alloc(m.nc, m.nf, m.nb);
   const bool dev = flags & FCFD_DEVICE_PTRS;
   const double *w = W, *v = V;
   if (!dev) {
@@ -371,7 +375,7 @@ int fcfd_jvp(fcfd_ctx *x, const double *W, const double *V, double *R, double *J
     CK(cudaMemcpyAsync(x->Vin.p, V, sizeof(double) * 5 * m.nc, cudaMemcpyHostToDevice, x->stream));
     w = x->Win.p; v = x->Vin.p;
   }
-  k_seed_dual<double><<<(m.nc + 255) / 256, 256, 0, x->stream>>>(w, v, x->pjv.X.p, m.nc);
+  k_seed_dual<double><<<(m.nc + 255) / 256, 256, 0, x->stream>>>(w, v, x->pjv.W.p, m.nc, m.nt);
   launch_chain<Dual<double>>(x, x->pjv, x->pjv.R.p, false, nullptr, nullptr);
   double *rout = R ? (dev ? R : x->Rtmp.p) : nullptr;
   double *jout = dev ? JV : x->Vin.p;

@@ -1,12 +1,11 @@
 // Device kernels of the finite-volume residual, templated on the scalar type S.
 //
-// Data layout (reference order):
-//   X[nt][32]       one 256-byte record per cell (interior [0,nc), boundary
-//                   ghosts [nc,nt)): p,u,v,w,T (0-4), centroid (5-7),
-//                   gradients of p,u,v,w,T x (x,y,z) (8-22), limiters (23-27).
-//                   A neighbour access touches one or two contiguous sectors
-//                   instead of one per field.
-//   D[5][nf]        per-face F_diffusive - F_convective (structure of arrays)
+// Data layout (all reference-order, structure-of-arrays):
+//   W[5][nt]        primitive state p,u,v,w,T of interior cells [0,nc) and
+//                   boundary ghosts [nc,nt)
+//   G[15][nc]       cell gradients (p,u,v,w,T) x (x,y,z)
+//   L[5][nc]        limiters
+//   D[5][nf]        per-face F_diffusive - F_convective
 //   R               residual, gathered per cell in ascending face order
 // Kernel chain per residual: ghost+minmax -> grad+limiter -> (outlet density)
 // -> face flux -> gather.  The chain mirrors update_boundaries,
@@ -139,10 +138,6 @@ struct DevMesh {
   const int *outlet_faces;                 // outlet boundary faces [n_outlet]
   int n_outlet;
 };
-
-// per-cell record layout
-constexpr int REC = 32, RW = 0, RX = 5, RG = 8, RL = 23;
-__host__ __device__ __forceinline__ size_t rec(int k) { return (size_t)REC * (size_t)k; }
 
 enum { T_SYM = 1, T_WALL = 2, T_INLET = 3, T_OUTLET = 4 };
 enum { KN_NONE = -1, KN_NO_REVERSE = 1, KN_DAMP_REVERSE = 2, KN_VELOCITY = 3, KN_MDOT = 4, KN_SLIP = 5, KN_STAGNATION = 6,
@@ -311,9 +306,8 @@ __device__ bool apply_bc(const DevCase &c, const DevBC &b, const FState<S> &L, F
 
 // Centre state of cell k as a face state (zero gradients).
 template <class S>
-__device__ __forceinline__ void centre_state(const DevCase &c, const S *X, int k, FState<S> &s, const double n[3]) {
-  const S *r = X + rec(k);
-  s.p = r[0]; s.V[0] = r[1]; s.V[1] = r[2]; s.V[2] = r[3]; s.T = r[4];
+__device__ __forceinline__ void centre_state(const DevCase &c, const S *W, int nt, int k, FState<S> &s, const double n[3]) {
+  s.p = W[k]; s.V[0] = W[nt + k]; s.V[1] = W[2 * nt + k]; s.V[2] = W[3 * nt + k]; s.T = W[4 * nt + k];
   s.pc = s.p; s.Tc = s.T; s.Vc[0] = s.V[0]; s.Vc[1] = s.V[1]; s.Vc[2] = s.V[2];
   s.rho = eos_rho(c, s.p, s.T);
   finish(c, s, n);
@@ -322,18 +316,17 @@ __device__ __forceinline__ void centre_state(const DevCase &c, const S *X, int k
 // Reconstructed state of cell k at face point xf (left_state_update,
 // ns_assemble_linear_system.cc:269-294).
 template <class S>
-__device__ __forceinline__ void recon_state(const DevCase &c, const DevMesh &m, const S *X, int k, const double xf[3],
-                                            FState<S> &s, const double n[3]) {
-  const int nt = m.nt;
-  const S *r = X + rec(k);
+__device__ __forceinline__ void recon_state(const DevCase &c, const DevMesh &m, const S *W, const S *G, const S *Lm, int k,
+                                            const double xf[3], FState<S> &s, const double n[3]) {
+  const int nt = m.nt, nc = m.nc;
   const double d0 = xf[0] - m.c_x[k], d1 = xf[1] - m.c_x[nt + k], d2 = xf[2] - m.c_x[2 * nt + k];
   S q[5];
 #pragma unroll
   for (int v = 0; v < 5; ++v) {
-    S dot = d0 * r[RG + 3 * v] + d1 * r[RG + 3 * v + 1] + d2 * r[RG + 3 * v + 2];
-    q[v] = r[v] + r[RL + v] * dot;
+    S dot = d0 * G[(3 * v) * nc + k] + d1 * G[(3 * v + 1) * nc + k] + d2 * G[(3 * v + 2) * nc + k];
+    q[v] = W[v * nt + k] + Lm[v * nc + k] * dot;
   }
-  s.pc = r[0]; s.Vc[0] = r[1]; s.Vc[1] = r[2]; s.Vc[2] = r[3]; s.Tc = r[4];
+  s.pc = W[k]; s.Vc[0] = W[nt + k]; s.Vc[1] = W[2 * nt + k]; s.Vc[2] = W[3 * nt + k]; s.Tc = W[4 * nt + k];
   s.p = q[0]; s.V[0] = q[1]; s.V[1] = q[2]; s.V[2] = q[3]; s.T = q[4];
   s.rho = eos_rho(c, s.p, s.T);
   finish(c, s, n);
@@ -341,22 +334,13 @@ __device__ __forceinline__ void recon_state(const DevCase &c, const DevMesh &m, 
 
 // ------------------------------------------------------------------ kernels
 
-// AoS [nc][5] state -> the state fields of the interior records
+// AoS [nc][5] -> SoA W[5][nt]
 template <class S>
-__global__ void k_load_rec(const S *__restrict__ in, S *__restrict__ X, int nc) {
+__global__ void k_aos_to_soa(const S *__restrict__ in, S *__restrict__ W, int nc, int nt) {
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= nc) return;
 #pragma unroll
-  for (int v = 0; v < 5; ++v) X[rec(c) + v] = in[5 * c + v];
-}
-
-// centroids into the records (once per context)
-template <class S>
-__global__ void k_init_centroids(const double *__restrict__ c_x, S *__restrict__ X, int nt) {
-  int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= nt) return;
-#pragma unroll
-  for (int i = 0; i < 3; ++i) X[rec(c) + RX + i] = S(c_x[(size_t)i * nt + c]);
+  for (int v = 0; v < 5; ++v) W[v * nt + c] = in[5 * c + v];
 }
 
 __device__ __forceinline__ unsigned long long okey(double x) {
@@ -373,7 +357,8 @@ __device__ __forceinline__ double okey_inv(unsigned long long k) {
 // (ns.cc:400-435) needs: slots 0..7 = max p, min p, max u, min u, max v,
 // min v, max p over cells < nc-1, min p over cells < nc-1 (ordered keys).
 template <class S>
-__global__ void k_ghost_minmax(DevCase cs, DevMesh m, S *__restrict__ X, unsigned long long *__restrict__ ext, int *err) {
+__global__ void k_ghost_minmax(DevCase cs, DevMesh m, S *__restrict__ W, unsigned long long *__restrict__ ext, int *err) {
+  const int nt = m.nt;
   const int ghost_blocks = (m.nb + blockDim.x - 1) / blockDim.x;
   if ((int)blockIdx.x < ghost_blocks) {
     const int tid = blockIdx.x * blockDim.x + threadIdx.x;
@@ -383,11 +368,11 @@ __global__ void k_ghost_minmax(DevCase cs, DevMesh m, S *__restrict__ X, unsigne
     const int b = m.f_bc[f];
     const double n[3] = {m.f_n[f], m.f_n[m.nf + f], m.f_n[2 * m.nf + f]};
     FState<S> L, R;
-    centre_state(cs, X, pa, L, n);
+    centre_state(cs, W, nt, pa, L, n);
     R.rho = S(0.);
     apply_bc(cs, cs.bc[b], L, R, n, err);
-    S *r = X + rec(m.nc + tid);
-    r[0] = R.p; r[1] = R.V[0]; r[2] = R.V[1]; r[3] = R.V[2]; r[4] = R.T;
+    const int g = m.nc + tid;
+    W[g] = R.p; W[nt + g] = R.V[0]; W[2 * nt + g] = R.V[1]; W[3 * nt + g] = R.V[2]; W[4 * nt + g] = R.T;
     return;
   }
   if (!ext) return;
@@ -396,8 +381,7 @@ __global__ void k_ghost_minmax(DevCase cs, DevMesh m, S *__restrict__ X, unsigne
   const int eb = blockIdx.x - ghost_blocks, neb = gridDim.x - ghost_blocks;
   double mx[4] = {-INFINITY, -INFINITY, -INFINITY, -INFINITY}, mn[4] = {INFINITY, INFINITY, INFINITY, INFINITY};
   for (int c = eb * blockDim.x + threadIdx.x; c < m.nc; c += neb * blockDim.x) {
-    const S *r = X + rec(c);
-    const double p = val(r[0]), u = val(r[1]), v = val(r[2]);
+    const double p = val(W[c]), u = val(W[nt + c]), v = val(W[2 * nt + c]);
     mx[0] = fmax(mx[0], p); mn[0] = fmin(mn[0], p);
     mx[1] = fmax(mx[1], u); mn[1] = fmin(mn[1], u);
     mx[2] = fmax(mx[2], v); mn[2] = fmin(mn[2], v);
@@ -426,11 +410,11 @@ __global__ void k_ghost_minmax(DevCase cs, DevMesh m, S *__restrict__ X, unsigne
 
 // First cell attaining each extreme (tangent runs): slots as in k_ghost_minmax.
 template <class S>
-__global__ void k_argext(DevMesh m, const S *__restrict__ X, const unsigned long long *__restrict__ ext, int *__restrict__ argx) {
+__global__ void k_argext(DevMesh m, const S *__restrict__ W, const unsigned long long *__restrict__ ext, int *__restrict__ argx) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= m.nc) return;
-  const S *r = X + rec(c);
-  const double p = val(r[0]), u = val(r[1]), v = val(r[2]);
+  const int nt = m.nt;
+  const double p = val(W[c]), u = val(W[nt + c]), v = val(W[2 * nt + c]);
   if (p == okey_inv(ext[0])) atomicMin(&argx[0], c);
   if (p == okey_inv(ext[1])) atomicMin(&argx[1], c);
   if (u == okey_inv(ext[2])) atomicMin(&argx[2], c);
@@ -445,11 +429,11 @@ __global__ void k_argext(DevMesh m, const S *__restrict__ X, const unsigned long
 
 // Combine a value array and a tangent array (AoS [nc][5]) into SoA duals.
 template <class T>
-__global__ void k_seed_dual(const double *__restrict__ w, const double *__restrict__ dw, Dual<T> *__restrict__ X, int nc) {
+__global__ void k_seed_dual(const double *__restrict__ w, const double *__restrict__ dw, Dual<T> *__restrict__ W, int nc, int nt) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= nc) return;
 #pragma unroll
-  for (int v = 0; v < 5; ++v) X[rec(c) + v] = Dual<T>(T(w[5 * c + v]), T(dw[5 * c + v]));
+  for (int v = 0; v < 5; ++v) W[v * nt + c] = Dual<T>(T(w[5 * c + v]), T(dw[5 * c + v]));
 }
 
 // Split a dual SoA result into value and tangent AoS arrays.
@@ -465,87 +449,56 @@ __global__ void k_split_dual(const Dual<T> *__restrict__ R, double *__restrict__
   }
 }
 
-// Shuffle of a double or a dual number.
-__device__ __forceinline__ double shfl(double x, int src) { return __shfl_sync(0xffffffffu, x, src); }
-template <class T>
-__device__ __forceinline__ Dual<T> shfl(const Dual<T> &x, int src) {
-  return Dual<T>(__shfl_sync(0xffffffffu, x.v, src), __shfl_sync(0xffffffffu, x.d, src));
-}
-
 // LSQ gradient (bit-exact restatement of Variable::cell_gradient over the
-// lsqr_grad_map weights, variable.h:193-216, lsqr_grad_map.cc:32-99) and the
-// limiter (ns_limiters.cc), four lanes per interior cell.  Lane i < 3 owns the
-// i-th gradient component: it rebuilds the i-th weight of every stencil entry
-// (one IEEE division) and accumulates the five variables in std::map key
-// order with explicitly rounded operations, so each component is the
-// reference's double.  The 15 components are then shared by shuffles and the
-// limiter is split over the lanes by variable (lane 0: p and T).
+// lsqr_grad_map weights) + limiter, one thread per interior cell.
 template <class S>
-__global__ void __launch_bounds__(128) k_grad_limiter(DevCase cs, DevMesh m, S *__restrict__ X,
-                                                      const unsigned long long *__restrict__ ext,
-                                                      const int *__restrict__ argx) {
+__global__ void __launch_bounds__(128) k_grad_limiter(DevCase cs, DevMesh m, const S *__restrict__ W,
+                                                      const unsigned long long *__restrict__ ext, const int *__restrict__ argx,
+                                                      S *__restrict__ G, S *__restrict__ Lm) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
   const int nc = m.nc, nt = m.nt;
-  const int q = threadIdx.x & 3;
-  const int c0 = (blockIdx.x * blockDim.x + threadIdx.x) >> 2;
-  const bool active = c0 < nc;
-  const int c = active ? c0 : nc - 1;  // inactive lanes shadow the last cell (no stores)
-  const int base = (threadIdx.x & 31) & ~3;
+  if (c >= nc) return;
   const double xc0 = m.c_x[c], xc1 = m.c_x[nt + c], xc2 = m.c_x[2 * nt + c];
-  // cofactor column of this lane's component: (C0i, C1i, C2i)
-  const int iq = q < 3 ? q : 0;
-  const int ci0 = iq == 0 ? 0 : (iq == 1 ? 1 : 2), ci1 = iq == 0 ? 1 : (iq == 1 ? 3 : 4), ci2 = iq == 0 ? 2 : (iq == 1 ? 4 : 5);
-  const double Ca = m.st_cof[(size_t)ci0 * nc + c], Cb = m.st_cof[(size_t)ci1 * nc + c], Cc = m.st_cof[(size_t)ci2 * nc + c];
-  const double det = m.st_cof[6 * (size_t)nc + c];
-  const double selfw = m.st_self[(size_t)iq * nc + c];
-  S acc[5] = {S(0.), S(0.), S(0.), S(0.), S(0.)};
-  const int j0 = m.st_index[c], j1 = m.st_index[c + 1];
-  if (q < 3) {
-    for (int j = j0; j < j1; ++j) {
-      const int kk = m.st_keys[j];
-      const S *r = X + rec(kk);
-      double wt;
-      if (kk == c) {
-        wt = selfw;
-      } else {
-        const double d0 = sub_rn(val(r[RX]), xc0), d1 = sub_rn(val(r[RX + 1]), xc1), d2 = sub_rn(val(r[RX + 2]), xc2);
-        const double w = add_rn(add_rn(mul_rn(d0, d0), mul_rn(d1, d1)), mul_rn(d2, d2));
-        wt = div_rn(mul_rn(w, add_rn(add_rn(mul_rn(d0, Ca), mul_rn(d1, Cb)), mul_rn(d2, Cc))), det);
-      }
-#pragma unroll
-      for (int v = 0; v < 5; ++v) acc[v] = add_rn(acc[v], mul_rn(S(wt), r[v]));
-    }
-  }
-  // share the 15 components
+  const double C00 = m.st_cof[c], C01 = m.st_cof[nc + c], C02 = m.st_cof[2 * nc + c];
+  const double C11 = m.st_cof[3 * nc + c], C12 = m.st_cof[4 * nc + c], C22 = m.st_cof[5 * nc + c];
+  const double det = m.st_cof[6 * nc + c];
   S g[15];
 #pragma unroll
-  for (int v = 0; v < 5; ++v)
+  for (int i = 0; i < 15; ++i) g[i] = S(0.);
+  const int j0 = m.st_index[c], j1 = m.st_index[c + 1];
+  for (int j = j0; j < j1; ++j) {
+    const int k = m.st_keys[j];
+    double wt0, wt1, wt2;
+    if (k == c) {
+      wt0 = m.st_self[c]; wt1 = m.st_self[nc + c]; wt2 = m.st_self[2 * nc + c];
+    } else {
+      const double d0 = sub_rn(m.c_x[k], xc0), d1 = sub_rn(m.c_x[nt + k], xc1), d2 = sub_rn(m.c_x[2 * nt + k], xc2);
+      const double w = add_rn(add_rn(mul_rn(d0, d0), mul_rn(d1, d1)), mul_rn(d2, d2));
+      wt0 = div_rn(mul_rn(w, add_rn(add_rn(mul_rn(d0, C00), mul_rn(d1, C01)), mul_rn(d2, C02))), det);
+      wt1 = div_rn(mul_rn(w, add_rn(add_rn(mul_rn(d0, C01), mul_rn(d1, C11)), mul_rn(d2, C12))), det);
+      wt2 = div_rn(mul_rn(w, add_rn(add_rn(mul_rn(d0, C02), mul_rn(d1, C12)), mul_rn(d2, C22))), det);
+    }
 #pragma unroll
-    for (int i = 0; i < 3; ++i) g[3 * v + i] = shfl(acc[v], base + i);
-  S *own = X + rec(c);
-  if (active && q < 3) {
-#pragma unroll
-    for (int v = 0; v < 5; ++v) own[RG + 3 * v + q] = acc[v];
+    for (int v = 0; v < 5; ++v) {
+      const S phi = W[v * nt + k];
+      g[3 * v] = add_rn(g[3 * v], mul_rn(S(wt0), phi));
+      g[3 * v + 1] = add_rn(g[3 * v + 1], mul_rn(S(wt1), phi));
+      g[3 * v + 2] = add_rn(g[3 * v + 2], mul_rn(S(wt2), phi));
+    }
   }
+#pragma unroll
+  for (int i = 0; i < 15; ++i) G[i * nc + c] = g[i];
 
-  // ---- limiter: lane 0 handles p and T, lanes 1..3 handle u, v, w
-  const int nvar = (q == 0) ? 2 : 1;
-  const int vars[2] = {q == 0 ? 0 : q, 4};
-  if (cs.order == 1) {
-    if (active)
-      for (int a = 0; a < nvar; ++a) own[RL + vars[a]] = S(0.);
-    return;
-  }
-  if (cs.limiter <= 0) {
-    if (active)
-      for (int a = 0; a < nvar; ++a) own[RL + vars[a]] = S(1.);
-    return;
-  }
-  const int f0 = m.cf_index[c], f1 = m.cf_index[c + 1];
-  for (int a = 0; a < nvar; ++a) {
-    const int v = vars[a];
-    const S gx = g[3 * v], gy = g[3 * v + 1], gz = g[3 * v + 2];
-    const S u0 = own[v];
-    S phi = S(1.);
+  // ---- limiter (ns_limiters.cc)
+  S phi[5];
+  const S one = S(cs.order == 1 ? 0. : 1.);
+#pragma unroll
+  for (int v = 0; v < 5; ++v) phi[v] = one;
+  if (cs.order != 1 && cs.limiter > 0) {
+    const int f0 = m.cf_index[c], f1 = m.cf_index[c + 1];
+    S u0[5];
+#pragma unroll
+    for (int v = 0; v < 5; ++v) { u0[v] = W[v * nt + c]; phi[v] = S(1.); }
     if (cs.limiter == 3) {
       // minmod (ns_limiters.cc:45-92)
       const double small = 1.e-12;
@@ -554,107 +507,122 @@ __global__ void __launch_bounds__(128) k_grad_limiter(DevCase cs, DevMesh m, S *
         const int f = e >= 0 ? e : ~e;
         const int nb = e >= 0 ? m.f_neighbor[f] : m.f_parent[f];
         const double cf0 = sub_rn(m.f_x[f], xc0), cf1 = sub_rn(m.f_x[m.nf + f], xc1), cf2 = sub_rn(m.f_x[2 * m.nf + f], xc2);
-        S dU = sub_rn(X[rec(nb) + v], u0);
-        S dUg = add_rn(add_rn(mul_rn(gx, S(cf0)), mul_rn(gy, S(cf1))), mul_rn(gz, S(cf2)));
-        S mm;
-        if (dU * dUg < 0.) mm = S(0.);
-        else if (dU > 0.) mm = smin(dU, dUg);
-        else mm = smax(dU, dUg);
-        const double sU = (double)((mm > 0.) - (mm < 0.)), sG = (double)((dUg > 0.) - (dUg < 0.));
-        S rr = div_rn(add_rn(mm, S(sU * small)), add_rn(dUg, S(sG * small)));
-        phi = smin(phi, rr);
+#pragma unroll
+        for (int v = 0; v < 5; ++v) {
+          S dU = sub_rn(W[v * nt + nb], u0[v]);
+          S dUg = add_rn(add_rn(mul_rn(g[3 * v], S(cf0)), mul_rn(g[3 * v + 1], S(cf1))), mul_rn(g[3 * v + 2], S(cf2)));
+          S mm;
+          if (dU * dUg < 0.) mm = S(0.);
+          else if (dU > 0.) mm = smin(dU, dUg);
+          else mm = smax(dU, dUg);
+          const double sU = (double)((mm > 0.) - (mm < 0.)), sG = (double)((dUg > 0.) - (dUg < 0.));
+          S r = div_rn(add_rn(mm, S(sU * small)), add_rn(dUg, S(sG * small)));
+          phi[v] = smin(phi[v], r);
+        }
       }
     } else {
       // Venkatakrishnan (ns_limiters.cc:161-248) and Barth-Jespersen (94-159)
-      S umax = u0, umin = u0;
+      S umax[5], umin[5];
+#pragma unroll
+      for (int v = 0; v < 5; ++v) umax[v] = umin[v] = u0[v];
       for (int j = f0; j < f1; ++j) {
         const int e = m.cf_list[j];
         const int f = e >= 0 ? e : ~e;
         const int nb = e >= 0 ? m.f_neighbor[f] : m.f_parent[f];
-        const S xv = X[rec(nb) + v];
-        umax = smax(umax, xv);
-        umin = smin(umin, xv);
-      }
-      S eps2 = S(0.);
-      if (cs.limiter == 1) {
-        // find_min_max with its index quirks (ns.cc:400-435): q[3] uses q[4]'s
-        // running value, q[4] tracks p starting from T of cell 0.  std::max keeps
-        // the earlier operand on ties, so each extreme belongs to a definite
-        // cell; `argx` (tangent runs only) holds the first cell per slot.
-        const S *r0 = X + rec(0), *rl = X + rec(nc - 1);
-        const double pmax = okey_inv(ext[0]), pmin = okey_inv(ext[1]);
-        const double T0 = val(r0[4]), wl = val(rl[3]);
-        const double tT0 = tan_of(r0[4]), twl = tan_of(rl[3]);
-        auto tp = [&](int slot) { return argx ? tan_of(X[rec(argx[slot])]) : 0.; };
-        auto tv = [&](int var, int slot) { return argx ? tan_of(X[rec(argx[slot]) + var]) : 0.; };
-        double qM, qm, tM, tm;
-        if (v == 0) { qM = pmax; tM = tp(0); qm = pmin; tm = tp(1); }
-        else if (v == 1) { qM = okey_inv(ext[2]); tM = tv(1, 2); qm = okey_inv(ext[3]); tm = tv(1, 3); }
-        else if (v == 2) { qM = okey_inv(ext[4]); tM = tv(2, 4); qm = okey_inv(ext[5]); tm = tv(2, 5); }
-        else if (v == 3) {
-          double q4M = T0, t4M = tT0, q4m = T0, t4m = tT0;  // running q[4] before the last cell
-          if (nc > 1) {
-            const double a2 = okey_inv(ext[6]), b2 = okey_inv(ext[7]);
-            if (T0 < a2) { q4M = a2; t4M = tp(6); }
-            if (b2 < T0) { q4m = b2; t4m = tp(7); }
-          }
-          qM = q4M; tM = t4M; if (q4M < wl) { qM = wl; tM = twl; }
-          qm = q4m; tm = t4m; if (wl < q4m) { qm = wl; tm = twl; }
-        } else {
-          qM = T0; tM = tT0; if (T0 < pmax) { qM = pmax; tM = tp(0); }
-          qm = T0; tm = tT0; if (pmin < T0) { qm = pmin; tm = tp(1); }
+#pragma unroll
+        for (int v = 0; v < 5; ++v) {
+          const S x = W[v * nt + nb];
+          umax[v] = smax(umax[v], x);
+          umin[v] = smin(umin[v], x);
         }
-        const S eps = fabs(Mk<S>::of(qM, tM) - Mk<S>::of(qm, tm)) / cs.Lref;
-        const S e = 1.e-6 * cs.K * eps;
-        eps2 = e * e;
+      }
+      S eps2[5] = {S(0.), S(0.), S(0.), S(0.), S(0.)};
+      if (cs.limiter == 1) {
+        // find_min_max with its index quirks: q[3] uses q[4]'s running value,
+        // q[4] tracks p starting from T of cell 0.  std::max keeps the earlier
+        // operand on ties, so each extreme belongs to a definite cell; `argx`
+        // (tangent runs only) holds the first cell attaining slots 0..7.
+        const double pmax = okey_inv(ext[0]), pmin = okey_inv(ext[1]);
+        const double T0 = val(W[4 * nt + 0]), wl = val(W[3 * nt + nc - 1]);
+        const double tT0 = tan_of(W[4 * nt + 0]), twl = tan_of(W[3 * nt + nc - 1]);
+        auto tp = [&](int slot) { return argx ? tan_of(W[argx[slot]]) : 0.; };
+        auto tv = [&](int var, int slot) { return argx ? tan_of(W[var * nt + argx[slot]]) : 0.; };
+        double qmax[5], qmin[5], tmax[5], tmin[5];
+        qmax[0] = pmax; tmax[0] = tp(0); qmin[0] = pmin; tmin[0] = tp(1);
+        qmax[1] = okey_inv(ext[2]); tmax[1] = tv(1, 2); qmin[1] = okey_inv(ext[3]); tmin[1] = tv(1, 3);
+        qmax[2] = okey_inv(ext[4]); tmax[2] = tv(2, 4); qmin[2] = okey_inv(ext[5]); tmin[2] = tv(2, 5);
+        double q4M = T0, t4M = tT0, q4m = T0, t4m = tT0;  // running q[4] before the last cell
+        if (nc > 1) {
+          const double a = okey_inv(ext[6]), b = okey_inv(ext[7]);
+          if (T0 < a) { q4M = a; t4M = tp(6); }
+          if (b < T0) { q4m = b; t4m = tp(7); }
+        }
+        qmax[3] = q4M; tmax[3] = t4M; if (q4M < wl) { qmax[3] = wl; tmax[3] = twl; }
+        qmin[3] = q4m; tmin[3] = t4m; if (wl < q4m) { qmin[3] = wl; tmin[3] = twl; }
+        qmax[4] = T0; tmax[4] = tT0; if (T0 < pmax) { qmax[4] = pmax; tmax[4] = tp(0); }
+        qmin[4] = T0; tmin[4] = tT0; if (pmin < T0) { qmin[4] = pmin; tmin[4] = tp(1); }
+#pragma unroll
+        for (int v = 0; v < 5; ++v) {
+          const S eps = fabs(Mk<S>::of(qmax[v], tmax[v]) - Mk<S>::of(qmin[v], tmin[v])) / cs.Lref;
+          const S e = 1.e-6 * cs.K * eps;
+          eps2[v] = e * e;
+        }
       }
       for (int j = f0; j < f1; ++j) {
         const int e = m.cf_list[j];
         const int f = e >= 0 ? e : ~e;
         const double cf0 = sub_rn(m.f_x[f], xc0), cf1 = sub_rn(m.f_x[m.nf + f], xc1), cf2 = sub_rn(m.f_x[2 * m.nf + f], xc2);
-        S dM = add_rn(add_rn(mul_rn(gx, S(cf0)), mul_rn(gy, S(cf1))), mul_rn(gz, S(cf2)));
-        S dP = u0;
-        if (cs.limiter == 1) {
-          if (dM > 0.) dP = sub_rn(umax, dP);
-          else if (dM < 0.) dP = sub_rn(umin, dP);
-          const S dP2 = mul_rn(dP, dP), dM2 = mul_rn(dM, dM);
-          if (dM != 0.) {
-            const S num = add_rn(add_rn(dP2, eps2), mul_rn(mul_rn(S(2.), dM), dP));
-            const S den = add_rn(add_rn(add_rn(dP2, mul_rn(S(2.), dM2)), mul_rn(dM, dP)), eps2);
-            phi = smin(phi, div_rn(num, den));
+#pragma unroll
+        for (int v = 0; v < 5; ++v) {
+          S dM = add_rn(add_rn(mul_rn(g[3 * v], S(cf0)), mul_rn(g[3 * v + 1], S(cf1))), mul_rn(g[3 * v + 2], S(cf2)));
+          S dP = u0[v];
+          if (cs.limiter == 1) {
+            if (dM > 0.) dP = sub_rn(umax[v], dP);
+            else if (dM < 0.) dP = sub_rn(umin[v], dP);
+            const S dP2 = mul_rn(dP, dP), dM2 = mul_rn(dM, dM);
+            const S e2 = eps2[v];
+            if (dM != 0.) {
+              const S num = add_rn(add_rn(dP2, e2), mul_rn(mul_rn(S(2.), dM), dP));
+              const S den = add_rn(add_rn(add_rn(dP2, mul_rn(S(2.), dM2)), mul_rn(dM, dP)), e2);
+              phi[v] = smin(phi[v], div_rn(num, den));
+            }
+          } else {
+            if (dM > 0.) dP = sub_rn(umax[v], dP);
+            else if (dM < 0.) dP = sub_rn(umin[v], dP);
+            else { dP = S(1.); dM = S(1.); }
+            phi[v] = smin(phi[v], div_rn(dP, dM));
           }
-        } else {
-          if (dM > 0.) dP = sub_rn(umax, dP);
-          else if (dM < 0.) dP = sub_rn(umin, dP);
-          else { dP = S(1.); dM = S(1.); }
-          phi = smin(phi, div_rn(dP, dM));
         }
       }
     }
-    // tangent runs for Newton-Krylov may treat the limiter as a constant
-    if (cs.frozen_limiter) phi = Mk<S>::of(val(phi), 0.);
-    if (active) own[RL + v] = phi;
   }
+  if (cs.frozen_limiter) {
+    // tangent runs for Newton-Krylov: treat the limiter as a constant
+#pragma unroll
+    for (int v = 0; v < 5; ++v) phi[v] = Mk<S>::of(val(phi[v]), 0.);
+  }
+#pragma unroll
+  for (int v = 0; v < 5; ++v) Lm[v * nc + c] = phi[v];
 }
 
 // Density the reference's `right` state cache holds when face f is reached:
 // the right density of face f-1 (walking back over faces whose BC branch
 // does not set it).  Face 0 starts from the zero-initialised cache.
 template <class S>
-__device__ S cached_right_rho(const DevCase &cs, const DevMesh &m, const S *X, int f) {
+__device__ S cached_right_rho(const DevCase &cs, const DevMesh &m, const S *W, const S *G, const S *Lm, int f) {
   for (int g = f - 1; g >= 0; --g) {
     const double n[3] = {m.f_n[g], m.f_n[m.nf + g], m.f_n[2 * m.nf + g]};
     const double xf[3] = {m.f_x[g], m.f_x[m.nf + g], m.f_x[2 * m.nf + g]};
     const int b = m.f_bc[g];
     if (b < 0) {
       FState<S> R;
-      recon_state(cs, m, X, m.f_neighbor[g], xf, R, n);
+      recon_state(cs, m, W, G, Lm, m.f_neighbor[g], xf, R, n);
       return R.rho;
     }
     FState<S> L, R;
-    recon_state(cs, m, X, m.f_parent[g], xf, L, n);
-    const S *rg = X + rec(m.f_neighbor[g]);
-    R.pc = rg[0]; R.Vc[0] = rg[1]; R.Vc[1] = rg[2]; R.Vc[2] = rg[3]; R.Tc = rg[4];
+    recon_state(cs, m, W, G, Lm, m.f_parent[g], xf, L, n);
+    const int gh = m.f_neighbor[g], nt = m.nt;
+    R.pc = W[gh]; R.Vc[0] = W[nt + gh]; R.Vc[1] = W[2 * nt + gh]; R.Vc[2] = W[3 * nt + gh]; R.Tc = W[4 * nt + gh];
     R.rho = S(0.);
     if (apply_bc(cs, cs.bc[b], L, R, n, (int *)nullptr)) return R.rho;
   }
@@ -662,11 +630,12 @@ __device__ S cached_right_rho(const DevCase &cs, const DevMesh &m, const S *X, i
 }
 
 template <class S>
-__global__ void k_outlet_rho(DevCase cs, DevMesh m, const S *__restrict__ X, S *__restrict__ stale) {
+__global__ void k_outlet_rho(DevCase cs, DevMesh m, const S *__restrict__ W, const S *__restrict__ G,
+                             const S *__restrict__ Lm, S *__restrict__ stale) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= m.n_outlet) return;
   const int f = m.outlet_faces[i];
-  stale[m.f_neighbor[f] - m.nc] = cached_right_rho(cs, m, X, f);
+  stale[m.f_neighbor[f] - m.nc] = cached_right_rho(cs, m, W, G, Lm, f);
 }
 
 // ---- convective fluxes in xyz (rotated-frame algebra of ns_roe.cc,
@@ -807,9 +776,9 @@ __host__ __device__ __forceinline__ void vanleer(const DevCase &c, const FState<
 // face states carry tangents, as in the face-Jacobian kernel).
 template <class S, class SG, bool VISCOUS>
 __device__ __forceinline__ void face_D(const DevCase &cs, const DevMesh &m, int f, const double n[3], double A, int b,
-                                       int pa, int nb, const FState<S> &L, const FState<S> &R, const SG *__restrict__ X,
+                                       int pa, int nb, const FState<S> &L, const FState<S> &R, const SG *__restrict__ G,
                                        const SG *__restrict__ mu_t, S D[5], S &wL) {
-  const int nf = m.nf, nt = m.nt;
+  const int nf = m.nf, nt = m.nt, nc = m.nc;
   S F[5];
   if (cs.flux == 1) roe(cs, L, R, n, F, wL);
   else if (cs.flux == 2) vanleer(cs, L, R, n, F, wL);
@@ -818,15 +787,13 @@ __device__ __forceinline__ void face_D(const DevCase &cs, const DevMesh &m, int 
   if (VISCOUS) {
     // face_state_update (ns_assemble_linear_system.cc:353-415)
     S gr[12];  // u,v,w,T gradients at the face
-    const SG *rP = X + rec(pa);
     if (b >= 0) {
 #pragma unroll
-      for (int i = 0; i < 12; ++i) gr[i] = S(rP[RG + 3 + i]);
+      for (int i = 0; i < 12; ++i) gr[i] = S(G[(3 + i) * nc + pa]);
     } else {
-      const SG *rN = X + rec(nb);
       const double wP = m.f_w[f], wN = m.f_w[nf + f];
 #pragma unroll
-      for (int i = 0; i < 12; ++i) gr[i] = S(wP * rP[RG + 3 + i] + wN * rN[RG + 3 + i]);
+      for (int i = 0; i < 12; ++i) gr[i] = S(wP * G[(3 + i) * nc + pa] + wN * G[(3 + i) * nc + nb]);
     }
     const double l0 = m.c_x[nb] - m.c_x[pa], l1 = m.c_x[nt + nb] - m.c_x[nt + pa], l2 = m.c_x[2 * nt + nb] - m.c_x[2 * nt + pa];
     const double lm = sqrt(l0 * l0 + l1 * l1 + l2 * l2);
@@ -870,16 +837,15 @@ __device__ __forceinline__ void face_D(const DevCase &cs, const DevMesh &m, int 
 // with the cached density where the BC branch leaves it untouched).
 template <class S>
 __device__ __forceinline__ void face_states(const DevCase &cs, const DevMesh &m, int f, const double n[3], int b, int pa,
-                                            int nb, const S *__restrict__ X, const S *__restrict__ stale, FState<S> &L,
-                                            FState<S> &R, int *err) {
-  const int nf = m.nf, nc = m.nc;
+                                            int nb, const S *__restrict__ W, const S *__restrict__ G, const S *__restrict__ Lm,
+                                            const S *__restrict__ stale, FState<S> &L, FState<S> &R, int *err) {
+  const int nf = m.nf, nt = m.nt, nc = m.nc;
   const double xf[3] = {m.f_x[f], m.f_x[nf + f], m.f_x[2 * nf + f]};
-  recon_state(cs, m, X, pa, xf, L, n);
+  recon_state(cs, m, W, G, Lm, pa, xf, L, n);
   if (b < 0) {
-    recon_state(cs, m, X, nb, xf, R, n);
+    recon_state(cs, m, W, G, Lm, nb, xf, R, n);
   } else {
-    const S *rg = X + rec(nb);
-    R.pc = rg[0]; R.Vc[0] = rg[1]; R.Vc[1] = rg[2]; R.Vc[2] = rg[3]; R.Tc = rg[4];
+    R.pc = W[nb]; R.Vc[0] = W[nt + nb]; R.Vc[1] = W[2 * nt + nb]; R.Vc[2] = W[3 * nt + nb]; R.Tc = W[4 * nt + nb];
     R.rho = S(0.);
     if (!apply_bc(cs, cs.bc[b], L, R, n, err)) R.rho = stale[nb - nc];
     finish(cs, R, n);
@@ -888,10 +854,10 @@ __device__ __forceinline__ void face_states(const DevCase &cs, const DevMesh &m,
 
 // Face flux: reconstruction, BCs, inviscid + viscous flux; D = Fd - Fc.
 template <class S, bool VISCOUS>
-__global__ void __launch_bounds__(128) k_face_flux(DevCase cs, DevMesh m, const S *__restrict__ X,
-                                                   const S *__restrict__ stale, const S *__restrict__ mu_t,
-                                                   S *__restrict__ D, S *__restrict__ mdot_out, S *__restrict__ wl_out,
-                                                   int *err) {
+__global__ void __launch_bounds__(128) k_face_flux(DevCase cs, DevMesh m, const S *__restrict__ W, const S *__restrict__ G,
+                                                   const S *__restrict__ Lm, const S *__restrict__ stale,
+                                                   const S *__restrict__ mu_t, S *__restrict__ D, S *__restrict__ mdot_out,
+                                                   S *__restrict__ wl_out, int *err) {
   const int f = blockIdx.x * blockDim.x + threadIdx.x;
   const int nf = m.nf;
   if (f >= nf) return;
@@ -899,9 +865,9 @@ __global__ void __launch_bounds__(128) k_face_flux(DevCase cs, DevMesh m, const 
   const double n[3] = {m.f_n[f], m.f_n[nf + f], m.f_n[2 * nf + f]};
   const double A = m.f_area[f];
   FState<S> L, R;
-  face_states(cs, m, f, n, b, pa, nb, X, stale, L, R, err);
+  face_states(cs, m, f, n, b, pa, nb, W, G, Lm, stale, L, R, err);
   S Dv[5], wL;
-  face_D<S, S, VISCOUS>(cs, m, f, n, A, b, pa, nb, L, R, X, mu_t, Dv, wL);
+  face_D<S, S, VISCOUS>(cs, m, f, n, A, b, pa, nb, L, R, G, mu_t, Dv, wL);
 #pragma unroll
   for (int v = 0; v < 5; ++v) D[v * nf + f] = Dv[v];
   if (mdot_out) mdot_out[f] = (-Dv[0]) / A;
@@ -938,12 +904,12 @@ __global__ void k_gather(DevMesh m, const S *__restrict__ D, S *__restrict__ R) 
 
 // Local time step (time_step.cc:143-224).
 template <class S>
-__global__ void k_local_dt(DevCase cs, DevMesh m, const S *__restrict__ X, S *__restrict__ dt, double cfl,
+__global__ void k_local_dt(DevCase cs, DevMesh m, const S *__restrict__ W, S *__restrict__ dt, double cfl,
                            unsigned long long *__restrict__ minkey) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= m.nc) return;
-  const S *r = X + rec(c);
-  const S p = r[0], u = r[1], v = r[2], w = r[3], T = r[4];
+  const int nt = m.nt;
+  const S p = W[c], u = W[nt + c], v = W[2 * nt + c], w = W[3 * nt + c], T = W[4 * nt + c];
   const S a = sound(cs, p, T);
   const S v_dt = cfl * m.c_len[c] / (sqrt(u * u + v * v + w * w) + a);
   dt[c] = v_dt;

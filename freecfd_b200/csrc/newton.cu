@@ -93,9 +93,9 @@ __device__ __forceinline__ void lift(const FState<double> &s, FState<D5> &o) {
 // Per face: JL = dD/dW_left and (interior faces) JR = dD/dW_right, [25][nf],
 // entry (i,k) = d D_i / d W_k at index (5i+k)*nf + f.
 template <bool VISCOUS>
-__global__ void __launch_bounds__(128) k_face_jac(DevCase cs, DevMesh m, const double *__restrict__ X,
-                                                  const double *__restrict__ stale, double *__restrict__ JL,
-                                                  double *__restrict__ JR) {
+__global__ void __launch_bounds__(128) k_face_jac(DevCase cs, DevMesh m, const double *__restrict__ W, const double *__restrict__ G,
+                                                  const double *__restrict__ Lm, const double *__restrict__ stale,
+                                                  double *__restrict__ JL, double *__restrict__ JR) {
   const int f = blockIdx.x * blockDim.x + threadIdx.x;
   const int nf = m.nf;
   if (f >= nf) return;
@@ -103,7 +103,7 @@ __global__ void __launch_bounds__(128) k_face_jac(DevCase cs, DevMesh m, const d
   const double n[3] = {m.f_n[f], m.f_n[nf + f], m.f_n[2 * nf + f]};
   const double A = m.f_area[f];
   FState<double> L, R;
-  face_states(cs, m, f, n, b, pa, nb, X, stale, L, R, (int *)nullptr);
+  face_states(cs, m, f, n, b, pa, nb, W, G, Lm, stale, L, R, (int *)nullptr);
   FState<D5> Ld, Rd;
   D5 D[5], wl;
   seed(L, Ld, cs, n);
@@ -115,7 +115,7 @@ __global__ void __launch_bounds__(128) k_face_jac(DevCase cs, DevMesh m, const d
     if (!apply_bc(cs, cs.bc[b], Ld, Rd, n, (int *)nullptr)) Rd.rho = D5(R.rho);
     finish(cs, Rd, n);
   }
-  face_D<D5, double, VISCOUS>(cs, m, f, n, A, b, pa, nb, Ld, Rd, X, (const double *)nullptr, D, wl);
+  face_D<D5, double, VISCOUS>(cs, m, f, n, A, b, pa, nb, Ld, Rd, G, (const double *)nullptr, D, wl);
 #pragma unroll
   for (int i = 0; i < 5; ++i)
 #pragma unroll
@@ -123,7 +123,7 @@ __global__ void __launch_bounds__(128) k_face_jac(DevCase cs, DevMesh m, const d
   if (b < 0) {
     lift(L, Ld);
     seed(R, Rd, cs, n);
-    face_D<D5, double, VISCOUS>(cs, m, f, n, A, b, pa, nb, Ld, Rd, X, (const double *)nullptr, D, wl);
+    face_D<D5, double, VISCOUS>(cs, m, f, n, A, b, pa, nb, Ld, Rd, G, (const double *)nullptr, D, wl);
 #pragma unroll
     for (int i = 0; i < 5; ++i)
 #pragma unroll
@@ -302,19 +302,19 @@ __global__ void k_gs_color(DevMesh m, const int *__restrict__ cells, int ncells,
 
 // copy a [5][nc] state into the residual chain's [5][nt] array (+ optional eps*dir)
 template <class T>
-__global__ void k_load_state(int nc, const double *__restrict__ Wn, const T *__restrict__ dir, double eps,
-                             double *__restrict__ X) {
+__global__ void k_load_state(int nc, int nt, const double *__restrict__ Wn, const T *__restrict__ dir, double eps,
+                             double *__restrict__ W) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= nc) return;
 #pragma unroll
-  for (int v = 0; v < 5; ++v) X[rec(c) + v] = Wn[v * nc + c] + (dir ? eps * double(dir[v * nc + c]) : 0.);
+  for (int v = 0; v < 5; ++v) W[v * nt + c] = Wn[v * nc + c] + (dir ? eps * double(dir[v * nc + c]) : 0.);
 }
 template <class T>
-__global__ void k_load_dual(int nc, const double *__restrict__ Wn, const T *__restrict__ dir, Dual<double> *__restrict__ X) {
+__global__ void k_load_dual(int nc, int nt, const double *__restrict__ Wn, const T *__restrict__ dir, Dual<double> *__restrict__ W) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= nc) return;
 #pragma unroll
-  for (int v = 0; v < 5; ++v) X[rec(c) + v] = Dual<double>(Wn[v * nc + c], double(dir[v * nc + c]));
+  for (int v = 0; v < 5; ++v) W[v * nt + c] = Dual<double>(Wn[v * nc + c], double(dir[v * nc + c]));
 }
 
 // y = (V P/dt) z - Jz, Jz from a finite difference (R1 - R0)/eps or a tangent run
@@ -509,7 +509,7 @@ __global__ void k_cast(int n, const double *__restrict__ a, T *__restrict__ b) {
 template <class T>
 static void eval_residual(fcfd_ctx *x, const double *Wn, double *R, const T *dir, double eps) {
   const DevMesh &m = x->dm;
-  k_load_state<T><<<(m.nc + 255) / 256, 256, 0, x->stream>>>(m.nc, Wn, dir, eps, x->p64.X.p);
+  k_load_state<T><<<(m.nc + 255) / 256, 256, 0, x->stream>>>(m.nc, m.nt, Wn, dir, eps, x->p64.W.p);
   launch_chain<double>(x, x->p64, R, false, nullptr, nullptr);
 }
 
@@ -525,8 +525,8 @@ static void matvec(fcfd_ctx *x, NewtonState &ns, int mode, const T *z, T *y, dou
     eval_residual<T>(x, ns.Wn.p, ns.R1.p, z, eps);
     k_matvec_finish<T><<<gb, tb, 0, s>>>(x->cs, m.nc, ns.Wn.p, ns.vol.p, ns.dt.p, z, ns.R1.p, ns.R0.p, 1. / eps, nullptr, y, rs);
   } else {
-    if (!x->pjv.ready) x->pjv.alloc(m.nc, m.nf, m.nb, x->c_x.p);
-    k_load_dual<T><<<gb, tb, 0, s>>>(m.nc, ns.Wn.p, z, x->pjv.X.p);
+    if (!x->pjv.ready) x->pjv.alloc(m.nc, m.nf, m.nb);
+    k_load_dual<T><<<gb, tb, 0, s>>>(m.nc, m.nt, ns.Wn.p, z, x->pjv.W.p);
     launch_chain<Dual<double>>(x, x->pjv, x->pjv.R.p, false, nullptr, nullptr, x->newton_frozen);
     k_matvec_finish<T><<<gb, tb, 0, s>>>(x->cs, m.nc, ns.Wn.p, ns.vol.p, ns.dt.p, z, nullptr, nullptr, 0., x->pjv.R.p, y, rs);
   }
@@ -725,7 +725,7 @@ int fcfd_newton_solve(fcfd_ctx *x, double *W, const fcfd_newton_opts *o, fcfd_ne
       if (o->max_seconds > 0 &&
           std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() > o->max_seconds) break;
       // local time step on the current state (loaded by the last residual)
-      k_local_dt<double><<<gc, tb, 0, s>>>(x->cs, m, x->p64.X.p, ns.dt.p, cfl, nullptr);
+      k_local_dt<double><<<gc, tb, 0, s>>>(x->cs, m, x->p64.W.p, ns.dt.p, cfl, nullptr);
       // reference state magnitudes: RMS of |p+Pref|, |V|, |T+Tref|
       RowScale wref;
       {
@@ -741,9 +741,9 @@ int fcfd_newton_solve(fcfd_ctx *x, double *W, const fcfd_newton_opts *o, fcfd_ne
       }
       // block-Jacobi preconditioner from the first-order face Jacobians
       if (x->viscous)
-        k_face_jac<true><<<(m.nf + 127) / 128, 128, 0, s>>>(x->cs, m, x->p64.X.p, x->p64.stale.p, ns.JL.p, ns.JR.p);
+        k_face_jac<true><<<(m.nf + 127) / 128, 128, 0, s>>>(x->cs, m, x->p64.W.p, x->p64.G.p, x->p64.Lm.p, x->p64.stale.p, ns.JL.p, ns.JR.p);
       else
-        k_face_jac<false><<<(m.nf + 127) / 128, 128, 0, s>>>(x->cs, m, x->p64.X.p, x->p64.stale.p, ns.JL.p, ns.JR.p);
+        k_face_jac<false><<<(m.nf + 127) / 128, 128, 0, s>>>(x->cs, m, x->p64.W.p, x->p64.G.p, x->p64.Lm.p, x->p64.stale.p, ns.JL.p, ns.JR.p);
       k_block_jacobi<<<gc, tb, 0, s>>>(x->cs, m, ns.Wn.p, ns.vol.p, ns.dt.p, ns.JL.p, ns.JR.p, ns.Minv.p, x->err.p, wref, ns.rowmag.p);
       CK(cudaGetLastError());
       // GMRES norm weights: 1 / RMS row magnitude, so every equation is measured
