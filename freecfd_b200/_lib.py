@@ -24,7 +24,7 @@ EXPORTED = [
     "fcfd_last_error", "fcfd_version", "fcfd_case_from_deck", "fcfd_case_destroy", "fcfd_case_summary",
     "fcfd_mesh_create", "fcfd_mesh_destroy", "fcfd_mesh_sizes", "fcfd_mesh_connectivity", "fcfd_mesh_geometry",
     "fcfd_mesh_lsq",
-    "fcfd_ctx_create", "fcfd_ctx_destroy", "fcfd_residual", "fcfd_last_stages", "fcfd_local_dt",
+    "fcfd_ctx_create", "fcfd_ctx_destroy", "fcfd_ctx_set_exact_gradients", "fcfd_residual", "fcfd_last_stages", "fcfd_local_dt",
     "fcfd_time_residual", "fcfd_point_flux", "fcfd_jvp", "fcfd_newton_solve", "fcfd_local_dt_cflmax_noalloc",
 ]
 
@@ -88,6 +88,7 @@ def _load():
     L.fcfd_ctx_create.argtypes = [vp, vp, ctypes.c_int, ctypes.POINTER(vp)]
     L.fcfd_ctx_destroy.argtypes = [vp]
     L.fcfd_ctx_destroy.restype = None
+    L.fcfd_ctx_set_exact_gradients.argtypes = [vp, ctypes.c_int]
     L.fcfd_residual.argtypes = [vp, vp, vp, ctypes.c_int]
     L.fcfd_last_stages.argtypes = [vp, dp, dp, dp, dp, dp]
     L.fcfd_local_dt.argtypes = [vp, vp, ctypes.c_double, ctypes.c_int, vp, ctypes.c_int]

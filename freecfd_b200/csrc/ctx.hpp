@@ -82,11 +82,12 @@ struct fcfd_ctx {
   DevCase cs{};
   DevMesh dm{};
   const fcfd_mesh *mesh = nullptr;
+  const fcfd_case *case_ptr = nullptr;
   bool viscous = false;
   // mesh arrays
   DBuf<int> f_parent, f_neighbor, f_bc, cf_index, cf_list, st_index, st_keys, bface, outlet, color_cells;
   std::vector<int> color_index;
-  DBuf<double> f_n, f_area, f_x, f_w, c_x, c_len, st_cof, st_self;
+  DBuf<double> f_n, f_area, f_x, f_w, c_x, c_len, st_cof, st_self, st_recip, st_mirror;
   // state arrays
   Pipe<double> p64;
   Pipe<Dual<double>> pjv;

@@ -180,6 +180,7 @@ int fcfd_ctx_create(const fcfd_mesh *mp, const fcfd_case *csp, int device, fcfd_
   CK(cudaSetDevice(device));
   CK(cudaStreamCreateWithFlags(&x->stream, cudaStreamNonBlocking));
   x->mesh = mp;
+  x->case_ptr = csp;
   DevCase &d = x->cs;
   const Material &mt = c.mat;
   d.gamma = mt.gamma; d.R = mt.R; d.Pref = mt.Pref; d.Tref = mt.Tref; d.Minf = c.Minf; d.K = c.limiter_threshold;
@@ -198,6 +199,10 @@ int fcfd_ctx_create(const fcfd_mesh *mp, const fcfd_case *csp, int device, fcfd_
   }
   x->viscous = mt.sutherland || mt.prandtl || mt.mu != 0. || mt.lambda != 0. || fixed_q;
   d.viscous = x->viscous;
+  // Limiters that are continuous in the gradient take the fused (non bit-exact)
+  // gradient; minmod, Barth-Jespersen and VK with K = 0 decide on the sign of
+  // rounding noise and take the bit-exact one.
+  d.fast_grad = (c.order == ORDER_FIRST || c.limiter == LIM_NONE || (c.limiter == LIM_VK && c.limiter_threshold > 0.)) ? 1 : 0;
   // ---- mesh upload (SoA)
   const int nc = m.nc, nf = m.nf, nb = m.nb, nt = nc + nb;
   x->f_parent.upload(m.f_parent); x->f_neighbor.upload(m.f_neighbor); x->f_bc.upload(m.f_bc);
@@ -215,6 +220,7 @@ int fcfd_ctx_create(const fcfd_mesh *mp, const fcfd_case *csp, int device, fcfd_
   x->cf_list.upload(cfl);
   x->st_index.upload(m.st_index); x->st_keys.upload(m.st_keys);
   x->st_cof.upload(soa(m.st_cof, nc, 7)); x->st_self.upload(soa(m.st_self, nc, 3));
+  x->st_recip.upload(m.st_recip); x->st_mirror.upload(soa(m.st_mirror, nc, 3));
   std::vector<int32_t> bface(nb), outl;
   for (int f = 0; f < nf; ++f) {
     if (m.f_bc[f] >= 0) {
@@ -238,6 +244,7 @@ int fcfd_ctx_create(const fcfd_mesh *mp, const fcfd_case *csp, int device, fcfd_
   dm.f_n = x->f_n.p; dm.f_area = x->f_area.p; dm.f_x = x->f_x.p; dm.f_w = x->f_w.p; dm.c_x = x->c_x.p;
   dm.c_len = x->c_len.p; dm.cf_index = x->cf_index.p; dm.cf_list = x->cf_list.p; dm.st_index = x->st_index.p;
   dm.st_keys = x->st_keys.p; dm.st_cof = x->st_cof.p; dm.st_self = x->st_self.p; dm.bface = x->bface.p;
+  dm.st_recip = x->st_recip.p; dm.st_mirror = x->st_mirror.p;
   dm.outlet_faces = x->outlet.p; dm.n_outlet = x->n_outlet;
   CK(cudaDeviceSynchronize());
   *out = x.release();
@@ -358,6 +365,17 @@ int fcfd_time_residual(fcfd_ctx *x, int reps, int flush_l2, double *out, int out
     for (int k = 0; k < 5; ++k) { CK(cudaEventElapsedTime(&ms, t.ev[k], t.ev[k + 1])); acc[k + 1] += ms; }
   }
   for (int k = 0; k < 6 && k < out_len; ++k) out[k] = acc[k] / reps;
+  API_END
+}
+
+int fcfd_ctx_set_exact_gradients(fcfd_ctx *x, int exact) {
+  API_BEGIN
+  if (!x) throw Error(FCFD_ERR_INPUT, "null context");
+  if (exact) x->cs.fast_grad = 0;
+  else {
+    const fcfd_case *c = x->case_ptr;
+    x->cs.fast_grad = (c->order == ORDER_FIRST || c->limiter == LIM_NONE || (c->limiter == LIM_VK && c->limiter_threshold > 0.)) ? 1 : 0;
+  }
   API_END
 }
 

@@ -87,6 +87,8 @@ struct fcfd_mesh {
   std::vector<int32_t> st_index, st_keys;
   std::vector<double> st_cof;                                // [nc][7]: C00 C01 C02 C11 C12 C22 det
   std::vector<double> st_self;                               // [nc][3]: self weight
+  std::vector<double> st_recip;                              // [nc]: 1/det where the reciprocal division is exact, else 0
+  std::vector<double> st_mirror;                             // [nc][3]: sum of the symmetry-mirror weights
   std::vector<uint8_t> has_lsq;                              // 1 if gradMap non-empty
   std::vector<int32_t> color_index, color_cells;             // face-neighbour colouring
   std::vector<double> nodes;                                 // [nnode][3]

@@ -121,6 +121,7 @@ struct DevCase {
   double mu, lambda, sut_mu_ref, sut_T_ref, sut_S, Pr;
   double Pr_t;
   int sutherland, prandtl, flux, limiter, order, viscous, nbc, frozen_limiter;
+  int fast_grad, pad_;
   DevBC bc[kMaxBC];
 };
 
@@ -134,6 +135,8 @@ struct DevMesh {
   const int *st_index, *st_keys;
   const double *st_cof;                    // [7][nc]
   const double *st_self;                   // [3][nc]
+  const double *st_recip;                  // [nc] 1/det where the reciprocal division is exact, else 0
+  const double *st_mirror;                 // [3][nc] summed symmetry-mirror weights
   const int *bface;                        // boundary faces in ghost order [nb]
   const int *outlet_faces;                 // outlet boundary faces [n_outlet]
   int n_outlet;
@@ -466,24 +469,71 @@ __global__ void __launch_bounds__(128) k_grad_limiter(DevCase cs, DevMesh m, con
 #pragma unroll
   for (int i = 0; i < 15; ++i) g[i] = S(0.);
   const int j0 = m.st_index[c], j1 = m.st_index[c + 1];
-  for (int j = j0; j < j1; ++j) {
-    const int k = m.st_keys[j];
-    double wt0, wt1, wt2;
-    if (k == c) {
-      wt0 = m.st_self[c]; wt1 = m.st_self[nc + c]; wt2 = m.st_self[2 * nc + c];
-    } else {
-      const double d0 = sub_rn(m.c_x[k], xc0), d1 = sub_rn(m.c_x[nt + k], xc1), d2 = sub_rn(m.c_x[2 * nt + k], xc2);
-      const double w = add_rn(add_rn(mul_rn(d0, d0), mul_rn(d1, d1)), mul_rn(d2, d2));
-      wt0 = div_rn(mul_rn(w, add_rn(add_rn(mul_rn(d0, C00), mul_rn(d1, C01)), mul_rn(d2, C02))), det);
-      wt1 = div_rn(mul_rn(w, add_rn(add_rn(mul_rn(d0, C01), mul_rn(d1, C11)), mul_rn(d2, C12))), det);
-      wt2 = div_rn(mul_rn(w, add_rn(add_rn(mul_rn(d0, C02), mul_rn(d1, C12)), mul_rn(d2, C22))), det);
+  if (cs.fast_grad) {
+    // Continuous limiters only (VK with K > 0, none, first order): the same
+    // weighted least-squares gradient in the compact form
+    //   grad = C . sum_k w_k d_k (phi_k - phi_c) / det - mirror * phi_c
+    // with fused multiply-adds (equal to the reference's sum up to rounding).
+    S u0[5];
+#pragma unroll
+    for (int v = 0; v < 5; ++v) u0[v] = W[v * nt + c];
+    S acc[15];
+#pragma unroll
+    for (int i = 0; i < 15; ++i) acc[i] = S(0.);
+    for (int j = j0; j < j1; ++j) {
+      const int k = m.st_keys[j];
+      if (k == c) continue;
+      const double d0 = m.c_x[k] - xc0, d1 = m.c_x[nt + k] - xc1, d2 = m.c_x[2 * nt + k] - xc2;
+      const double w = d0 * d0 + d1 * d1 + d2 * d2;
+#pragma unroll
+      for (int v = 0; v < 5; ++v) {
+        const S a = w * (W[v * nt + k] - u0[v]);
+        acc[3 * v] = acc[3 * v] + a * d0;
+        acc[3 * v + 1] = acc[3 * v + 1] + a * d1;
+        acc[3 * v + 2] = acc[3 * v + 2] + a * d2;
+      }
     }
+    const double id = 1. / det;
+    const double M0 = m.st_mirror[c], M1 = m.st_mirror[nc + c], M2 = m.st_mirror[2 * nc + c];
 #pragma unroll
     for (int v = 0; v < 5; ++v) {
-      const S phi = W[v * nt + k];
-      g[3 * v] = add_rn(g[3 * v], mul_rn(S(wt0), phi));
-      g[3 * v + 1] = add_rn(g[3 * v + 1], mul_rn(S(wt1), phi));
-      g[3 * v + 2] = add_rn(g[3 * v + 2], mul_rn(S(wt2), phi));
+      const S s0 = acc[3 * v], s1 = acc[3 * v + 1], s2 = acc[3 * v + 2];
+      g[3 * v] = (C00 * s0 + C01 * s1 + C02 * s2) * id - M0 * u0[v];
+      g[3 * v + 1] = (C01 * s0 + C11 * s1 + C12 * s2) * id - M1 * u0[v];
+      g[3 * v + 2] = (C02 * s0 + C12 * s1 + C22 * s2) * id - M2 * u0[v];
+    }
+  } else {
+    // Bit-exact: every weight rebuilt with the reference's rounded operations.
+    // The division by det uses the reciprocal with one fused correction where
+    // the mesh builder verified it returns the IEEE quotient for every weight.
+    const double rc = m.st_recip[c];
+    auto qdiv = [&](double x) -> double {
+      if (rc != 0.) {
+        const double q0 = __dmul_rn(x, rc);
+        const double rem = __fma_rn(-q0, det, x);
+        return __fma_rn(rem, rc, q0);
+      }
+      return __ddiv_rn(x, det);
+    };
+    for (int j = j0; j < j1; ++j) {
+      const int k = m.st_keys[j];
+      double wt0, wt1, wt2;
+      if (k == c) {
+        wt0 = m.st_self[c]; wt1 = m.st_self[nc + c]; wt2 = m.st_self[2 * nc + c];
+      } else {
+        const double d0 = sub_rn(m.c_x[k], xc0), d1 = sub_rn(m.c_x[nt + k], xc1), d2 = sub_rn(m.c_x[2 * nt + k], xc2);
+        const double w = add_rn(add_rn(mul_rn(d0, d0), mul_rn(d1, d1)), mul_rn(d2, d2));
+        wt0 = qdiv(mul_rn(w, add_rn(add_rn(mul_rn(d0, C00), mul_rn(d1, C01)), mul_rn(d2, C02))));
+        wt1 = qdiv(mul_rn(w, add_rn(add_rn(mul_rn(d0, C01), mul_rn(d1, C11)), mul_rn(d2, C12))));
+        wt2 = qdiv(mul_rn(w, add_rn(add_rn(mul_rn(d0, C02), mul_rn(d1, C12)), mul_rn(d2, C22))));
+      }
+#pragma unroll
+      for (int v = 0; v < 5; ++v) {
+        const S phi = W[v * nt + k];
+        g[3 * v] = add_rn(g[3 * v], mul_rn(S(wt0), phi));
+        g[3 * v + 1] = add_rn(g[3 * v + 1], mul_rn(S(wt1), phi));
+        g[3 * v + 2] = add_rn(g[3 * v + 2], mul_rn(S(wt2), phi));
+      }
     }
   }
 #pragma unroll

@@ -458,6 +458,8 @@ fcfd_mesh *build_mesh(const fcfd_raw_mesh &raw, fcfd_case &cs) {
     m.st_index.assign(nc + 1, 0);
     m.st_cof.assign(7 * (size_t)nc, 0.);
     m.st_self.assign(3 * (size_t)nc, 0.);
+    m.st_recip.assign(nc, 0.);
+    m.st_mirror.assign(3 * (size_t)nc, 0.);
     m.has_lsq.assign(nc, 0);
     {
       std::vector<int32_t> st;
@@ -499,15 +501,35 @@ fcfd_mesh *build_mesh(const fcfd_raw_mesh &raw, fcfd_case &cs) {
         cof[0] = C00; cof[1] = C01; cof[2] = C02; cof[3] = C11; cof[4] = C12; cof[5] = C22; cof[6] = det;
         // self weight: first entry inserts -w, later entries subtract (std::map semantics)
         double s0 = 0., s1 = 0., s2 = 0.;
+        // Division by det through a reciprocal and one fused correction
+        // (Markstein's method) is used on the device only if it reproduces the
+        // IEEE quotient for every weight of this cell (checked here).
+        const double recip = 1. / det;
+        bool exact = std::isfinite(recip);
+        double mir0 = 0., mir1 = 0., mir2 = 0.;
         for (size_t k = 0; k < st.size(); ++k) {
           const P3 &dk = dist[k];
           double w0 = w[k] * (dk.x * C00 + dk.y * C01 + dk.z * C02);
           double w1 = w[k] * (dk.x * C01 + dk.y * C11 + dk.z * C12);
           double w2 = w[k] * (dk.x * C02 + dk.y * C12 + dk.z * C22);
+          for (double num : {w0, w1, w2}) {
+            const double q0 = num * recip;
+            const double rem = std::fma(-q0, det, num);
+            const double q1 = std::fma(rem, recip, q0);
+            const double qd = num / det;
+            if (std::memcmp(&q1, &qd, sizeof(double)) != 0) exact = false;
+          }
           w0 /= det; w1 /= det; w2 /= det;
-          if (k == 0) { s0 = -1. * w0; s1 = -1. * w1; s2 = -1. * w2; }
+          if (k == 0 && st[0] == c) {
+            // a mirror first (no real neighbour): its insert lands and the
+            // subtraction cancels it (lsqr_grad_map.cc:92-94)
+            s0 = w0 - w0; s1 = w1 - w1; s2 = w2 - w2;
+          } else if (k == 0) { s0 = -1. * w0; s1 = -1. * w1; s2 = -1. * w2; }
           else { s0 -= w0; s1 -= w1; s2 -= w2; }
+          if (st[k] == c && k > 0) { mir0 += w0; mir1 += w1; mir2 += w2; }
         }
+        m.st_recip[c] = exact ? recip : 0.;
+        m.st_mirror[3 * c] = mir0; m.st_mirror[3 * c + 1] = mir1; m.st_mirror[3 * c + 2] = mir2;
         m.st_self[3 * c] = s0; m.st_self[3 * c + 1] = s1; m.st_self[3 * c + 2] = s2;
         // keys in ascending order (std::map iteration order), self included once
         std::vector<int32_t> keys(st.begin(), st.end());

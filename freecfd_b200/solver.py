@@ -107,11 +107,13 @@ class Mesh:
 class NavierStokes:
     """Device residual context (one CUDA stream, device buffers)."""
 
-    def __init__(self, mesh: Mesh, case: Case, device: int = 0):
+    def __init__(self, mesh: Mesh, case: Case, device: int = 0, exact_gradients: bool = False):
         self.mesh, self.case = mesh, case
         h = ctypes.c_void_p()
         check(lib.fcfd_ctx_create(mesh.h, case.h, int(device), ctypes.byref(h)))
         self.h = h
+        if exact_gradients:
+            check(lib.fcfd_ctx_set_exact_gradients(self.h, 1))
 
     def residual(self, W, out=None):
         """R(W) for W [nc][5] (numpy host array or CUDA torch tensor)."""

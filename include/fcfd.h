@@ -106,6 +106,13 @@ int fcfd_mesh_lsq(const fcfd_mesh *m, double *cofactors, double *self_weight);
 int fcfd_ctx_create(const fcfd_mesh *m, const fcfd_case *cs, int device, fcfd_ctx **out);
 void fcfd_ctx_destroy(fcfd_ctx *ctx);
 
+/* Gradient arithmetic.  By default the LSQ gradient is evaluated bit-exactly
+ * (the reference's rounded sums, src/lsqr_grad_map.cc:86-94, src/variable/variable.h:194-202)
+ * when the limiter decides on the sign of rounding noise (minmod,
+ * Barth-Jespersen, VK with threshold 0) and in a fused form equal to it up to
+ * rounding otherwise.  exact=1 forces the bit-exact form for every limiter. */
+int fcfd_ctx_set_exact_gradients(fcfd_ctx *ctx, int exact);
+
 /* Spatial residual R(W) = sum over faces of +/-(F_diffusive - F_convective)
  * for the interior-cell state W[nc][5].  Replaces the residual part of
  * NavierStokes::assemble_linear_system (src/navier_stokes/ns_assemble_linear_system.cc:34-140)

@@ -1,31 +1,60 @@
 """Residual parity of the CUDA path (through the C ABI) against the CPU oracle.
 
-Bar: integer/index work bit-exact (tests/test_mesh_parity.py).  Ghost states,
-gradients and limiters bit-exact wherever the boundary conditions involved do
-not call pow() (the ghost kernel is built without multiply-add contraction and
-the gradient/limiter kernels use explicitly rounded operations, so they produce
-the reference's doubles; CUDA's pow and libm's pow may differ in the last
-bit).  That covers the wedge and hypersonic families, whose minmod limiter is
-decided by the sign of rounding noise and so needs the exact doubles; the
-cylinder and plate (subsonic outlets, pow in the BC) are held to 1e-13.  The
-residual, mdot and weightL within 1e-12 normwise relative per equation (FP64;
-the flux arithmetic may contract multiply-adds and avoids the rotated frame,
-so it differs from the reference at rounding level).
+Bar: integer/index work bit-exact (tests/test_mesh_parity.py).  Ghost states
+bit-exact wherever the boundary conditions involved do not call pow() (the
+ghost kernel is built without multiply-add contraction; CUDA's pow and libm's
+pow may differ in the last bit).  Gradients and limiters bit-exact where the
+limiter decides on the sign of rounding noise (minmod, Barth-Jespersen: the
+gradient kernel then rebuilds the reference's rounded sums) and on request
+(exact_gradients=True); with a continuous limiter the fused gradient is held
+to 1e-12 of each variable's largest gradient.  The wedge and hypersonic
+families have no pow in their BCs, so they are the bit-exact cases; the
+cylinder and plate (subsonic outlets) are held to 1e-13.  The residual, mdot
+and weightL within 1e-12 normwise relative per equation (FP64; the flux
+arithmetic may contract multiply-adds and avoids the rotated frame, so it
+differs from the reference at rounding level).
 """
 import numpy as np
 import pytest
 
 from freecfd_b200 import cases
-from tests.util import SMALL, build_pair, flux_scale, rel_err
+from tests.util import SMALL, build_pair, flux_scale, rel_err, res_err
 
 TOL = 1e-12
 BITWISE = {"wedge", "hypersonic"}
 
 
-def _ctx(case, oracle_mod, fb):
+def _ctx(case, oracle_mod, fb, exact=False):
     o, cs, m = build_pair(case, oracle_mod, fb)
-    ns = fb.NavierStokes(m, cs, 0)
+    ns = fb.NavierStokes(m, cs, 0, exact_gradients=exact)
     return o, cs, m, ns
+
+
+def grad_err(g, ref, nc):
+    """Per-variable error of [nc][15] gradients relative to that variable's
+    largest gradient component (one-layer meshes have a z column of pure
+    rounding noise that a per-column norm would divide by ~0)."""
+    g = np.asarray(g).reshape(nc, 5, 3)
+    r = np.asarray(ref)[:nc].reshape(nc, 5, 3)
+    scale = np.maximum(np.abs(r).max(axis=(0, 2)), 1e-300)
+    return np.abs(g - r).max(axis=(0, 2)) / scale
+
+
+def _check_stages(family, limiter, exact, st, ref, m):
+    noise_limiter = limiter in ("minmod", "bj")
+    if family in BITWISE:
+        assert np.array_equal(st["ghost"], ref["ghost"]), "ghost states"
+    else:
+        assert rel_err(st["ghost"], ref["ghost"]).max() <= 1e-14
+    if family in BITWISE and (noise_limiter or exact):
+        assert np.array_equal(st["grads"], ref["grads"][: m.nc]), "gradients"
+        assert np.array_equal(st["limiter"], ref["limiter"]), "limiters"
+    elif noise_limiter or exact:
+        assert grad_err(st["grads"], ref["grads"], m.nc).max() <= 1e-13
+        assert rel_err(st["limiter"], ref["limiter"]).max() <= 1e-12
+    else:
+        assert grad_err(st["grads"], ref["grads"], m.nc).max() <= 1e-12
+        assert rel_err(st["limiter"], ref["limiter"]).max() <= 1e-11
 
 
 def _variants():
@@ -47,15 +76,8 @@ def test_residual_parity(family, flux, limiter, oracle_mod, fb):
     ref = o.residual(case.state, full=True)
     R = ns.residual(case.state)
     st = ns.stages()
-    if family in BITWISE:
-        assert np.array_equal(st["ghost"], ref["ghost"]), "ghost states"
-        assert np.array_equal(st["grads"], ref["grads"][: m.nc]), "gradients"
-        assert np.array_equal(st["limiter"], ref["limiter"]), "limiters"
-    else:
-        assert rel_err(st["ghost"], ref["ghost"]).max() <= 1e-14
-        assert rel_err(st["grads"], ref["grads"][: m.nc]).max() <= 1e-13
-        assert rel_err(st["limiter"], ref["limiter"]).max() <= 1e-12
-    err = rel_err(R, ref["R"])
+    _check_stages(family, limiter, False, st, ref, m)
+    err = res_err(R, ref["R"])
     assert err.max() <= TOL, err
     assert rel_err(st["mdot"], ref["mdot"]).max() <= TOL
     # weightL is the upwind side (0 / 0.5 / 1) chosen by the sign of the mass
@@ -63,6 +85,24 @@ def test_residual_parity(family, flux, limiter, oracle_mod, fb):
     # side is a rounding decision and mdot*weightL vanishes either way.
     big = np.abs(ref["mdot"]) > 1e-9 * np.abs(ref["mdot"]).max()
     assert np.array_equal(st["weightL"][big], ref["weightL"][big])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("family,flux,limiter", [("wedge", "Roe", "vk"), ("hypersonic", "AUSM+up", "vk"),
+                                                 ("wedge", "vanLeer", "none"), ("cylinder", "Roe", "vk"),
+                                                 ("plate", "AUSM+up", "vk")])
+def test_exact_gradients_on_request(family, flux, limiter, oracle_mod, fb):
+    """exact_gradients=True rebuilds the reference's rounded gradient sums for
+    a continuous limiter too (bit-exact on the wedge and hypersonic families),
+    and the fused default agrees with it to rounding."""
+    case = SMALL[family](flux=flux, limiter=limiter)
+    o, cs, m, ns = _ctx(case, oracle_mod, fb, exact=True)
+    ref = o.residual(case.state, full=True)
+    R = ns.residual(case.state)
+    _check_stages(family, limiter, True, ns.stages(), ref, m)
+    assert res_err(R, ref["R"]).max() <= TOL
+    fast = fb.NavierStokes(m, cs, 0)
+    assert res_err(fast.residual(case.state), R).max() <= TOL
 
 
 @pytest.mark.gpu
@@ -113,8 +153,9 @@ def test_full_size_parity(family, oracle_mod, fb):
     ref = o.residual(case.state, full=True)
     R = ns.residual(case.state)
     st = ns.stages()
-    assert np.array_equal(st["limiter"], ref["limiter"])
-    assert rel_err(R, ref["R"]).max() <= TOL
+    limiter = "minmod" if family == "hypersonic" else "vk"
+    _check_stages(family, limiter, False, st, ref, m)
+    assert res_err(R, ref["R"]).max() <= TOL
 
 
 @pytest.mark.gpu

@@ -35,6 +35,17 @@ def rel_err(a, b, floor=1e-300):
     return (np.abs(a - b).max(axis=0) / scale)
 
 
+def res_err(a, b):
+    """Normwise relative error of [n][5] residual-like arrays: per equation,
+    with the three momentum components sharing one scale (on one-layer
+    meshes the z-momentum column is rounding noise)."""
+    a = np.asarray(a).reshape(-1, 5)
+    b = np.asarray(b).reshape(a.shape)
+    scale = np.abs(b).max(axis=0)
+    scale[1:4] = scale[1:4].max()
+    return np.abs(a - b).max(axis=0) / np.maximum(scale, 1e-300)
+
+
 def flux_scale(case, mesh_geometry, gamma=1.4, R=287.0):
     """Per-equation magnitude of one face's freestream flux (mass, momentum,
     energy) times the largest face area: the size of the terms whose
