@@ -56,6 +56,33 @@ def alg_bytes(m, s=8):
             + m.n_grad_entries * 4 + m.n_cell_faces * 4)
 
 
+def kernel_bytes(m, name, viscous=True, exact_grad=False, s=8):
+    """Algorithmic bytes of one launch of a residual kernel: every array it
+    must read once and every array it writes (cell/face/stencil counts from
+    the mesh).  Gradients and limiters are counted where a kernel reads or
+    writes them."""
+    nc, nf, nb, nt = m.nc, m.nf, m.nghost, m.nc + m.nghost
+    E, ncf = m.n_grad_entries, m.n_cell_faces
+    if name == "grad_limiter":
+        b = nt * (5 * s + 3 * s)                    # states, centroids (stencils reach the ghosts)
+        b += nc * (7 * s + 4 + 4) + E * 4 + ncf * 4  # cofactors + det, stencil and cell->face CSR
+        b += nc * (4 * s if exact_grad else 3 * s)   # self weights + reciprocal, or mirror weights
+        b += nf * (8 + 3 * s)                        # face parent/neighbour, face centroids
+        b += nc * (15 * s + 5 * s)                   # gradient and limiter writes
+        return b
+    if name == "face_flux":
+        b = nf * (12 + 3 * s + s + 3 * s + (2 * s if viscous else 0))  # indices, normal, area, centroid, weights
+        b += nt * (5 * s + 3 * s)                    # states, centroids
+        b += nc * (15 * s + 5 * s)                   # gradients, limiters
+        b += nf * 5 * s                              # face differences written
+        return b
+    if name == "gather":
+        return nc * (4 + 5 * s) + ncf * 4 + ncf * 5 * s
+    if name == "ghost_minmax":
+        return nb * (8 + 5 * s + 5 * s) + nc * 3 * s
+    return 0
+
+
 def peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
@@ -235,6 +262,13 @@ def run_ours(args):
     B = alg_bytes(mesh)
     achieved = B / (ms * 1e-3) / 1e9
     n_kernels = 4 + (1 if ns_has_outlet(case) else 0)
+    # dominant kernel: its own algorithmic bytes over its event-timed duration
+    viscous = args.workload in ("cylinder", "plate", "plate64")          # laminar / viscous materials
+    exact_grad = "limiter=minmod" in case.deck or "limiter=bj" in case.deck
+    top = max(("grad_limiter", "face_flux", "gather", "ghost_minmax"), key=lambda k: kern[k])
+    kb = kernel_bytes(mesh, top, viscous, exact_grad)
+    k_ach = kb / (float(kern[top]) * 1e-3) / 1e9
+    traffic = NCU_TRAFFIC.get((args.workload, top))
     line = {"metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms, 5), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
@@ -243,12 +277,16 @@ def run_ours(args):
                        "parallelism": f"replicas x{world}"},
             "e2e": {"value": round(e2e, 3), "unit": UNIT, "h2d_bytes_per_step": int(W.nbytes),
                     "d2h_bytes_per_step": int(W.nbytes)},
-            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                         "frac": round(achieved / peak, 4), "traffic": None, "peak_kind": kind,
-                         "unit_of_work": "one residual evaluation (5 kernels)", "alg_bytes": int(B)},
+            "roofline": {"bound": "hbm", "achieved": round(k_ach, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(k_ach / peak, 4), "traffic": traffic, "peak_kind": kind, "kernel": top,
+                         "alg_bytes_per_launch": int(kb), "ms_per_launch": round(float(kern[top]), 5)},
+            "step_roofline": {"achieved": round(achieved, 1), "frac": round(achieved / peak, 4), "alg_bytes": int(B),
+                              "unit_of_work": "one residual evaluation (all kernels)"},
             "kernels_ms": {k: round(float(v), 5) for k, v in kern.items()},
             "gpu_launches": n_kernels * args.steps,
             "clocks": clk.summary()}
+    if not args.no_newton:
+        line["newton"] = run_newton(fb, cs, mesh, case, dev, dist)
     if rank == 0 and world == 1 and not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline(case, args.cpu_seconds)
     if rank == 0:
@@ -257,6 +295,53 @@ def run_ours(args):
     if dist:
         dist.barrier()
         dist.destroy_process_group()
+
+
+NEWTON_KW = dict(tol=1e-10, max_newton=400, cfl0=2.0, cfl_max=1e6, krylov_rtol=1e-3, precond_sweeps=4,
+                 krylov_cycles=3)
+
+
+def run_newton(fb, cs, mesh, case, dev, dist):
+    """Steady solve from the seeded state until |R_mass|/|R_mass0| <= 1e-10:
+    plain FP64 (finite-difference J.v, FP64 Krylov) against mixed (tangent
+    J.v kernels, FP32 Krylov basis and preconditioner application, FP64 outer
+    residual).  Wall time of the whole call (host state in, host state out);
+    replicas under torchrun, max over ranks."""
+    import torch
+    out = {}
+    states = {}
+    variants = (("plain_fp64_fd", dict(jvp=False)),
+                ("mixed_jvp_fp32", dict(jvp=True, exact_jvp=True, fp32_krylov=True)))
+    for label, opts in variants:
+        ns = fb.NavierStokes(mesh, cs, dev)
+        ns.newton_solve(case.state, **dict(NEWTON_KW, max_newton=2), raise_on_fail=False, **opts)  # warm-up
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        t0 = time.perf_counter()
+        W, rep = ns.newton_solve(case.state, **NEWTON_KW, raise_on_fail=False, **opts)
+        el = time.perf_counter() - t0
+        if dist:
+            x = torch.tensor([el], device="cuda", dtype=torch.float64)
+            dist.all_reduce(x, op=dist.ReduceOp.MAX)
+            el = float(x.item())
+        states[label] = W
+        out[label] = {"seconds": round(el, 4), "converged": rep["status"] == 0,
+                      "newton_iterations": rep["newton_iterations"], "krylov_iterations": rep["krylov_iterations"],
+                      "mass_residual_drop": float(rep["res_final"] / rep["res0"])}
+        del ns
+    a, b = states["plain_fp64_fd"], states["mixed_jvp_fp32"]
+    scale = np.abs(a).max(axis=0)
+    scale[1:4] = np.abs(a[:, 1:4]).max()
+    out["speedup_mixed_vs_plain"] = round(out["plain_fp64_fd"]["seconds"] / out["mixed_jvp_fp32"]["seconds"], 3)
+    out["state_rel_diff_mixed_vs_plain"] = float((np.abs(a - b).max(axis=0) / scale).max())
+    out["settings"] = dict(NEWTON_KW)
+    return out
+
+
+# DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) from
+# ncu captures of the same kernels; the capture commands are in profiles/.
+NCU_TRAFFIC = {}
 
 
 def ns_has_outlet(case):
@@ -273,6 +358,7 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--ref-workers", type=int, default=64)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-newton", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

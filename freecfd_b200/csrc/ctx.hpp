@@ -92,7 +92,8 @@ struct fcfd_ctx {
   Pipe<double> p64;
   Pipe<Dual<double>> pjv;
   DBuf<double> Win, Vin, Rtmp, dt, mdot, wl;
-  DBuf<unsigned long long> ext;
+  DBuf<unsigned long long> ext;    // global extrema slots of the VK limiter (armed between chains)
+  DBuf<unsigned long long> dtmin;  // CFL_MAX minimum of the local time step
   DBuf<int> err, argx;
   DBuf<unsigned char> flush;
   int n_outlet = 0;

@@ -31,15 +31,13 @@ void launch_chain(fcfd_ctx *x, Pipe<S> &P, S *Rout, bool aos_out, S *mo, S *wo, 
   csl.frozen_limiter = frozen_limiter ? 1 : 0;
   cudaStream_t s = x->stream;
   const int tb = 256;
-  // extrema slots: even = max (start at key 0), odd = min (start at all ones)
-  CK(cudaMemsetAsync(x->ext.p, 0x00, 8 * sizeof(unsigned long long), s));
-  for (int k = 1; k < 8; k += 2) CK(cudaMemsetAsync(x->ext.p + k, 0xFF, sizeof(unsigned long long), s));
+  // the extrema and argx slots arrive armed (context set-up, then the
+  // previous chain's gather)
   const bool need_ext = x->cs.limiter == 1 && x->cs.order != 1;
   const int ng = (m.nb + tb - 1) / tb + (need_ext ? kExtremaBlocks : 0);
   if (ng > 0) k_ghost_minmax<S><<<ng, tb, 0, s>>>(x->cs, m, P.W.p, need_ext ? x->ext.p : nullptr, x->err.p);
   const int *argx = nullptr;
   if (!std::is_same<S, double>::value && x->cs.limiter == 1 && x->cs.order != 1) {
-    CK(cudaMemsetAsync(x->argx.p, 0x7F, 8 * sizeof(int), s));
     k_argext<S><<<(m.nc + tb - 1) / tb, tb, 0, s>>>(m, P.W.p, x->ext.p, x->argx.p);
     argx = x->argx.p;
   }
@@ -51,9 +49,9 @@ void launch_chain(fcfd_ctx *x, Pipe<S> &P, S *Rout, bool aos_out, S *mo, S *wo, 
   else
     k_face_flux<S, false><<<(m.nf + 127) / 128, 128, 0, s>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p, (const S *)nullptr, P.D.p, mo, wo, x->err.p);
   if (aos_out)
-    k_gather<S, true><<<(m.nc + tb - 1) / tb, tb, 0, s>>>(m, P.D.p, Rout);
+    k_gather<S, true><<<(m.nc + tb - 1) / tb, tb, 0, s>>>(m, P.D.p, Rout, x->ext.p, x->argx.p);
   else
-    k_gather<S, false><<<(m.nc + tb - 1) / tb, tb, 0, s>>>(m, P.D.p, Rout);
+    k_gather<S, false><<<(m.nc + tb - 1) / tb, tb, 0, s>>>(m, P.D.p, Rout, x->ext.p, x->argx.p);
   CK(cudaGetLastError());
 }
 
@@ -236,8 +234,18 @@ int fcfd_ctx_create(const fcfd_mesh *mp, const fcfd_case *csp, int device, fcfd_
   // ---- state buffers
   x->p64.alloc(nc, nf, nb);
   x->Win.alloc(5 * (size_t)nc); x->Vin.alloc(5 * (size_t)nc); x->Rtmp.alloc(5 * (size_t)nc); x->dt.alloc(nc);
-  x->mdot.alloc(nf); x->wl.alloc(nf); x->ext.alloc(8); x->err.alloc(1); x->argx.alloc(8);
+  x->mdot.alloc(nf); x->wl.alloc(nf); x->ext.alloc(8); x->err.alloc(1); x->argx.alloc(8); x->dtmin.alloc(1);
   CK(cudaMemset(x->err.p, 0, sizeof(int)));
+  {
+    // arm the extrema slots (max slots start at key 0, min slots at all
+    // ones) and the first-attaining-cell slots; every residual chain's gather
+    // re-arms them for the next chain
+    unsigned long long e0[8];
+    int a0[8];
+    for (int k = 0; k < 8; ++k) { e0[k] = (k & 1) ? ~0ull : 0ull; a0[k] = 0x7F7F7F7F; }
+    CK(cudaMemcpy(x->ext.p, e0, sizeof(e0), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(x->argx.p, a0, sizeof(a0), cudaMemcpyHostToDevice));
+  }
   DevMesh &dm = x->dm;
   dm.nc = nc; dm.nf = nf; dm.nb = nb; dm.nt = nt;
   dm.f_parent = x->f_parent.p; dm.f_neighbor = x->f_neighbor.p; dm.f_bc = x->f_bc.p;
@@ -315,9 +323,9 @@ int fcfd_local_dt(fcfd_ctx *x, const double *W, double cfl, int mode, double *dt
   }
   k_aos_to_soa<double><<<(m.nc + 255) / 256, 256, 0, x->stream>>>(win, x->p64.W.p, m.nc, m.nt);
   double *out = dev ? dt : x->dt.p;
-  if (mode == 1) CK(cudaMemsetAsync(x->ext.p, 0xFF, sizeof(unsigned long long), x->stream));
-  k_local_dt<double><<<(m.nc + 255) / 256, 256, 0, x->stream>>>(x->cs, m, x->p64.W.p, out, cfl, mode == 1 ? x->ext.p : nullptr);
-  if (mode == 1) k_fill_min<double><<<(m.nc + 255) / 256, 256, 0, x->stream>>>(m.nc, out, x->ext.p);
+  if (mode == 1) CK(cudaMemsetAsync(x->dtmin.p, 0xFF, sizeof(unsigned long long), x->stream));
+  k_local_dt<double><<<(m.nc + 255) / 256, 256, 0, x->stream>>>(x->cs, m, x->p64.W.p, out, cfl, mode == 1 ? x->dtmin.p : nullptr);
+  if (mode == 1) k_fill_min<double><<<(m.nc + 255) / 256, 256, 0, x->stream>>>(m.nc, out, x->dtmin.p);
   CK(cudaGetLastError());
   if (!dev) CK(cudaMemcpyAsync(dt, x->dt.p, sizeof(double) * m.nc, cudaMemcpyDeviceToHost, x->stream));
   CK(cudaStreamSynchronize(x->stream));
@@ -338,8 +346,6 @@ int fcfd_time_residual(fcfd_ctx *x, int reps, int flush_l2, double *out, int out
   const int tb = 256;
   for (int r = 0; r < reps; ++r) {
     if (flush_l2) CK(cudaMemsetAsync(x->flush.p, r & 0xff, x->flush.n, s));
-    CK(cudaMemsetAsync(x->ext.p, 0x00, 8 * sizeof(unsigned long long), s));
-    for (int k = 1; k < 8; k += 2) CK(cudaMemsetAsync(x->ext.p + k, 0xFF, sizeof(unsigned long long), s));
     CK(cudaEventRecord(t.ev[0], s));
     const bool need_ext = x->cs.limiter == 1 && x->cs.order != 1;
     const int ng = (m.nb + tb - 1) / tb + (need_ext ? kExtremaBlocks : 0);
@@ -356,7 +362,7 @@ int fcfd_time_residual(fcfd_ctx *x, int reps, int flush_l2, double *out, int out
     else
       k_face_flux<double, false><<<(m.nf + 127) / 128, 128, 0, s>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p, nullptr, P.D.p, nullptr, nullptr, x->err.p);
     CK(cudaEventRecord(t.ev[4], s));
-    k_gather<double, false><<<(m.nc + tb - 1) / tb, tb, 0, s>>>(m, P.D.p, P.R.p);
+    k_gather<double, false><<<(m.nc + tb - 1) / tb, tb, 0, s>>>(m, P.D.p, P.R.p, x->ext.p, x->argx.p);
     CK(cudaEventRecord(t.ev[5], s));
     CK(cudaGetLastError());
     CK(cudaEventSynchronize(t.ev[5]));

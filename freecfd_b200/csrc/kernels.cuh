@@ -924,10 +924,23 @@ __global__ void __launch_bounds__(128) k_face_flux(DevCase cs, DevMesh m, const 
   if (wl_out) wl_out[f] = wL;
 }
 
+// Initial values of the extrema slots (even: max, starts at key 0; odd: min,
+// starts at all ones) and of the first-attaining-cell slots.
+__device__ __forceinline__ void reset_extrema(unsigned long long *ext, int *argx) {
+  const int t = threadIdx.x;
+  if (blockIdx.x == 0 && t < 8) {
+    if (ext) ext[t] = (t & 1) ? ~0ull : 0ull;
+    if (argx) argx[t] = 0x7F7F7F7F;
+  }
+}
+
 // Atomic-free gather: R_c = sum over the cell's faces in ascending face order
-// of (+D) for the parent side and (-D) for the neighbour side.
+// of (+D) for the parent side and (-D) for the neighbour side.  The last
+// kernel of a residual chain, so it also re-arms the extrema slots for the
+// next chain (every reader of them has finished by now on this stream).
 template <class S, bool AOS>
-__global__ void k_gather(DevMesh m, const S *__restrict__ D, S *__restrict__ R) {
+__global__ void k_gather(DevMesh m, const S *__restrict__ D, S *__restrict__ R, unsigned long long *ext, int *argx) {
+  reset_extrema(ext, argx);
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= m.nc) return;
   const int nf = m.nf;

@@ -301,11 +301,19 @@ __global__ void k_gs_color(DevMesh m, const int *__restrict__ cells, int ncells,
 }
 
 // copy a [5][nc] state into the residual chain's [5][nt] array (+ optional eps*dir)
+// Finite-difference step eps = eps_num / |z| with |z|^2 read from the device
+// (eps_num alone where zz is null or |z| = 0).
+__device__ __forceinline__ double fd_eps(double eps_num, const double *zz) {
+  if (!zz) return eps_num;
+  const double q = *zz;
+  return q > 0. ? eps_num / sqrt(q) : eps_num;
+}
 template <class T>
-__global__ void k_load_state(int nc, int nt, const double *__restrict__ Wn, const T *__restrict__ dir, double eps,
-                             double *__restrict__ W) {
+__global__ void k_load_state(int nc, int nt, const double *__restrict__ Wn, const T *__restrict__ dir, double eps_num,
+                             const double *__restrict__ zz, double *__restrict__ W) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= nc) return;
+  const double eps = fd_eps(eps_num, zz);
 #pragma unroll
   for (int v = 0; v < 5; ++v) W[v * nt + c] = Wn[v * nc + c] + (dir ? eps * double(dir[v * nc + c]) : 0.);
 }
@@ -321,10 +329,11 @@ __global__ void k_load_dual(int nc, int nt, const double *__restrict__ Wn, const
 template <class T>
 __global__ void k_matvec_finish(DevCase cs, int nc, const double *__restrict__ Wn, const double *__restrict__ vol,
                                 const double *__restrict__ dt, const T *__restrict__ z, const double *__restrict__ R1,
-                                const double *__restrict__ R0, double inv_eps, const Dual<double> *__restrict__ JV,
-                                T *__restrict__ y, RowScale rs) {
+                                const double *__restrict__ R0, double eps_num, const double *__restrict__ zz,
+                                const Dual<double> *__restrict__ JV, T *__restrict__ y, RowScale rs) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= nc) return;
+  const double inv_eps = JV ? 0. : 1. / fd_eps(eps_num, zz);
   double P[25];
   cons2prim(cs, Wn[c], Wn[nc + c], Wn[2 * nc + c], Wn[3 * nc + c], Wn[4 * nc + c], P);
   const double s = vol[c] / dt[c];
@@ -449,43 +458,92 @@ __global__ void k_gather_vol(int nc, const double *__restrict__ v, double *__res
 }
 
 // ------------------------------------------------------------------ solver
+// part[block] = sum over this block's slice of (z_i / wref_v)^2, v = i / nc
+template <class T>
+__global__ void k_wdot(int n, int nc, const T *__restrict__ z, RowScale winv, double *__restrict__ part) {
+  double s = 0.;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double q = double(z[i]) * winv.s[i / nc];
+    s += q * q;
+  }
+  __shared__ double sh[32];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.;
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) t += sh[k];
+    part[blockIdx.x] = t;
+  }
+}
+
+template <class T>
+__global__ void k_scale_rsqrt(int n, const double *__restrict__ ss, T *__restrict__ b) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const double q = *ss;
+  if (i < n && q > 0.) b[i] = T(double(b[i]) / sqrt(q));
+}
+
 template <class T>
 struct Krylov {
-  fcfd_ctx *x;
-  int n, nc, m;
-  DBuf<T> V, Z, w, tmpT;
-  DBuf<double> part, h;
-  std::vector<double> hh;
+  fcfd_ctx *x = nullptr;
+  int n = 0, nc = 0, m = 0, nparts = 1;
+  DBuf<T> V, w, tmpT;
+  DBuf<double> part, hd;  // hd: [0,m+1) first CGS pass, [m+1,2m+2) second, [2m+2] |w|^2, [2m+3] |z|^2
+  double *hp = nullptr;   // pinned host mirror of hd
+  Krylov() = default;
+  Krylov(const Krylov &) = delete;
+  Krylov &operator=(const Krylov &) = delete;
+  ~Krylov() {
+    if (hp) cudaFreeHost(hp);
+  }
   void alloc(fcfd_ctx *ctx, int krylov_dim) {
     x = ctx; nc = ctx->dm.nc; n = 5 * nc; m = krylov_dim;
+    nparts = std::min(kRedBlocks, std::max(1, (n + 1023) / 1024));
     V.alloc((size_t)(m + 1) * n); w.alloc(n); tmpT.alloc(n);
-    part.alloc((size_t)kRedBlocks * (m + 1)); h.alloc(m + 1);
-    hh.resize(m + 1);
+    part.alloc((size_t)nparts * (m + 1)); hd.alloc(2 * (size_t)m + 4);
+    CK(cudaMallocHost((void **)&hp, sizeof(double) * (2 * (size_t)m + 4)));
   }
-  // out[v] = V_v . u for v < nv (deterministic two-pass reduction)
-  void dots(int nv, const T *u, double *out_host) {
+  double *h1() { return hd.p; }
+  double *h2() { return hd.p + m + 1; }
+  double *ww() { return hd.p + 2 * m + 2; }
+  double *zz() { return hd.p + 2 * m + 3; }
+  // out[v] = Vb_v . u for v < nv, left on the device (deterministic two-pass reduction)
+  void dots_dev(int nv, const T *Vb, const T *u, double *out) {
     cudaStream_t s = x->stream;
-    dim3 g(kRedBlocks, nv);
-    k_dots<T><<<g, 256, 0, s>>>(n, nv, V.p, (size_t)n, u, part.p);
-    k_sum_parts<<<nv, 256, 0, s>>>(kRedBlocks, part.p, h.p);
-    CK(cudaMemcpyAsync(out_host, h.p, sizeof(double) * nv, cudaMemcpyDeviceToHost, s));
-    CK(cudaStreamSynchronize(s));
+    dim3 g(nparts, nv);
+    k_dots<T><<<g, 256, 0, s>>>(n, nv, Vb, (size_t)n, u, part.p);
+    k_sum_parts<<<nv, 256, 0, s>>>(nparts, part.p, out);
+  }
+  // bring hd back to the host (the one synchronisation of a GMRES iteration)
+  void fetch() {
+    CK(cudaMemcpyAsync(hp, hd.p, sizeof(double) * (2 * (size_t)m + 4), cudaMemcpyDeviceToHost, x->stream));
+    CK(cudaStreamSynchronize(x->stream));
   }
   double norm(const T *u) {
+    dots_dev(1, u, u, ww());
+    fetch();
+    return std::sqrt(hp[2 * m + 2]);
+  }
+  // |S^-1 u|^2 on the device (S = per-variable reference magnitudes)
+  void wnorm2_dev(const T *u, const RowScale &winv, double *out) {
     cudaStream_t s = x->stream;
-    dim3 g(kRedBlocks, 1);
-    k_dots<T><<<g, 256, 0, s>>>(n, 1, u, (size_t)n, u, part.p);
-    k_sum_parts<<<1, 256, 0, s>>>(kRedBlocks, part.p, h.p);
-    double r;
-    CK(cudaMemcpyAsync(&r, h.p, sizeof(double), cudaMemcpyDeviceToHost, s));
-    CK(cudaStreamSynchronize(s));
-    return std::sqrt(r);
+    k_wdot<T><<<nparts, 256, 0, s>>>(n, nc, u, winv, part.p);
+    k_sum_parts<<<1, 256, 0, s>>>(nparts, part.p, out);
+  }
+  double norm64(const double *u) {
+    cudaStream_t s = x->stream;
+    k_dots<double><<<dim3(nparts, 1), 256, 0, s>>>(n, 1, u, (size_t)n, u, part.p);
+    k_sum_parts<<<1, 256, 0, s>>>(nparts, part.p, ww());
+    fetch();
+    return std::sqrt(hp[2 * m + 2]);
   }
 };
 
 struct NewtonState {
   DBuf<double> Wn, R0, R1, dt, vol, JL, JR, Minv, Pr, Py0, Py1, Xs, rowmag;
-  double wscale = 1.;
+  double wscale = 1.;  // |S^-1 W| (finite-difference step scale)
+  RowScale winv;       // 1 / per-variable reference magnitudes
   int sweeps = 0, cycles = 1;
 };
 template <class T>
@@ -507,28 +565,30 @@ __global__ void k_cast(int n, const double *__restrict__ a, T *__restrict__ b) {
 
 // residual of the [5][nc] state (+ eps*dir) into R (SoA [5][nc])
 template <class T>
-static void eval_residual(fcfd_ctx *x, const double *Wn, double *R, const T *dir, double eps) {
+static void eval_residual(fcfd_ctx *x, const double *Wn, double *R, const T *dir, double eps,
+                          const double *zz = nullptr) {
   const DevMesh &m = x->dm;
-  k_load_state<T><<<(m.nc + 255) / 256, 256, 0, x->stream>>>(m.nc, m.nt, Wn, dir, eps, x->p64.W.p);
+  k_load_state<T><<<(m.nc + 255) / 256, 256, 0, x->stream>>>(m.nc, m.nt, Wn, dir, eps, zz, x->p64.W.p);
   launch_chain<double>(x, x->p64, R, false, nullptr, nullptr);
 }
 
-// y = (V P/dt - dR/dW) z
+// y = (V P/dt - dR/dW) z; zz: device |z|^2 (finite-difference mode only)
 template <class T>
-static void matvec(fcfd_ctx *x, NewtonState &ns, int mode, const T *z, T *y, double znorm, const RowScale &rs) {
+static void matvec(fcfd_ctx *x, NewtonState &ns, int mode, const T *z, T *y, const double *zz, const RowScale &rs) {
   const DevMesh &m = x->dm;
   cudaStream_t s = x->stream;
   const int tb = 256, gb = (m.nc + tb - 1) / tb;
   if (mode == 0) {
-    // finite difference of the FP64 residual, eps = sqrt(eps_mach) (1 + |W|) / |z|
-    const double eps = 1.4901161193847656e-08 * (1. + ns.wscale) / (znorm > 0. ? znorm : 1.);
-    eval_residual<T>(x, ns.Wn.p, ns.R1.p, z, eps);
-    k_matvec_finish<T><<<gb, tb, 0, s>>>(x->cs, m.nc, ns.Wn.p, ns.vol.p, ns.dt.p, z, ns.R1.p, ns.R0.p, 1. / eps, nullptr, y, rs);
+    // finite difference of the FP64 residual in variables scaled by their
+    // reference magnitudes: eps = sqrt(eps_mach) (1 + |S^-1 W|) / |S^-1 z|
+    const double eps_num = 1.4901161193847656e-08 * (1. + ns.wscale);
+    eval_residual<T>(x, ns.Wn.p, ns.R1.p, z, eps_num, zz);
+    k_matvec_finish<T><<<gb, tb, 0, s>>>(x->cs, m.nc, ns.Wn.p, ns.vol.p, ns.dt.p, z, ns.R1.p, ns.R0.p, eps_num, zz, nullptr, y, rs);
   } else {
     if (!x->pjv.ready) x->pjv.alloc(m.nc, m.nf, m.nb);
     k_load_dual<T><<<gb, tb, 0, s>>>(m.nc, m.nt, ns.Wn.p, z, x->pjv.W.p);
     launch_chain<Dual<double>>(x, x->pjv, x->pjv.R.p, false, nullptr, nullptr, x->newton_frozen);
-    k_matvec_finish<T><<<gb, tb, 0, s>>>(x->cs, m.nc, ns.Wn.p, ns.vol.p, ns.dt.p, z, nullptr, nullptr, 0., x->pjv.R.p, y, rs);
+    k_matvec_finish<T><<<gb, tb, 0, s>>>(x->cs, m.nc, ns.Wn.p, ns.vol.p, ns.dt.p, z, nullptr, nullptr, 0., nullptr, x->pjv.R.p, y, rs);
   }
   CK(cudaGetLastError());
 }
@@ -586,10 +646,10 @@ static void gmres(fcfd_ctx *x, NewtonState &ns, Krylov<T> &K, int mode, double r
   relres = 1.;
   // scaled right-hand side b = D R0; x0 = 0
   k_rowscale_copy<<<gc, tb, 0, s>>>(nc, ns.R0.p, rs, 1., dW);
-  const double bnorm = dnorm(x, K.part, K.h, dW, n);
+  const double bnorm = K.norm64(dW);
   CK(cudaMemsetAsync(ns.Xs.p, 0, sizeof(double) * n, s));
   if (!(bnorm > 0.)) { CK(cudaMemsetAsync(dW, 0, sizeof(double) * n, s)); relres = 0.; return; }
-  std::vector<double> H((size_t)(m + 1) * m, 0.), cs(m), sn(m), g(m + 1, 0.), h1(m + 1), h2(m + 1);
+  std::vector<double> H((size_t)(m + 1) * m, 0.), cs(m), sn(m), g(m + 1, 0.);
   for (int cyc = 0; cyc < ns.cycles; ++cyc) {
     double beta;
     if (cyc == 0) {
@@ -599,8 +659,8 @@ static void gmres(fcfd_ctx *x, NewtonState &ns, Krylov<T> &K, int mode, double r
       // r = b - (D A M^-1 D^-1 ...) applied to the current solution: recompute through one matvec of
       // z = M^-1 D^-1 (sum) already folded into Xs (physical units): r = D (R0 - A Xs)
       k_cast<T><<<gn, tb, 0, s>>>(n, ns.Xs.p, K.tmpT.p);
-      const double zn = (mode == 0) ? K.norm(K.tmpT.p) : 0.;
-      matvec<T>(x, ns, mode, K.tmpT.p, K.w.p, zn, rs);
+      if (mode == 0) K.wnorm2_dev(K.tmpT.p, ns.winv, K.zz());
+      matvec<T>(x, ns, mode, K.tmpT.p, K.w.p, K.zz(), rs);
       k_rowscale_copy<<<gc, tb, 0, s>>>(nc, ns.R0.p, rs, 1., dW);
       k_axpy_to<T><<<gn, tb, 0, s>>>(n, dW, K.w.p, K.V.p);  // V0 = b - A x (unnormalised)
       beta = K.norm(K.V.p);
@@ -615,18 +675,19 @@ static void gmres(fcfd_ctx *x, NewtonState &ns, Krylov<T> &K, int mode, double r
       T *vj = K.V.p + (size_t)j * n;
       T *w = K.V.p + (size_t)(j + 1) * n;
       apply_prec<T>(x, ns, vj, K.tmpT.p, rs, ns.sweeps);
-      const double zn = (mode == 0) ? K.norm(K.tmpT.p) : 0.;
-      matvec<T>(x, ns, mode, K.tmpT.p, w, zn, rs);
-      K.dots(j + 1, w, h1.data());
-      CK(cudaMemcpyAsync(K.h.p, h1.data(), sizeof(double) * (j + 1), cudaMemcpyHostToDevice, s));
-      k_sub_combo<T><<<gn, tb, 0, s>>>(n, j + 1, K.V.p, (size_t)n, K.h.p, w);
-      K.dots(j + 1, w, h2.data());
-      CK(cudaMemcpyAsync(K.h.p, h2.data(), sizeof(double) * (j + 1), cudaMemcpyHostToDevice, s));
-      k_sub_combo<T><<<gn, tb, 0, s>>>(n, j + 1, K.V.p, (size_t)n, K.h.p, w);
-      const double hn = K.norm(w);
-      for (int i = 0; i <= j; ++i) H[(size_t)i * m + j] = h1[i] + h2[i];
+      if (mode == 0) K.wnorm2_dev(K.tmpT.p, ns.winv, K.zz());
+      matvec<T>(x, ns, mode, K.tmpT.p, w, K.zz(), rs);
+      // classical Gram-Schmidt twice, coefficients kept on the device
+      K.dots_dev(j + 1, K.V.p, w, K.h1());
+      k_sub_combo<T><<<gn, tb, 0, s>>>(n, j + 1, K.V.p, (size_t)n, K.h1(), w);
+      K.dots_dev(j + 1, K.V.p, w, K.h2());
+      k_sub_combo<T><<<gn, tb, 0, s>>>(n, j + 1, K.V.p, (size_t)n, K.h2(), w);
+      K.dots_dev(1, w, w, K.ww());
+      k_scale_rsqrt<T><<<gn, tb, 0, s>>>(n, K.ww(), w);
+      K.fetch();
+      const double hn = std::sqrt(K.hp[2 * m + 2]);
+      for (int i = 0; i <= j; ++i) H[(size_t)i * m + j] = K.hp[i] + K.hp[m + 1 + i];
       H[(size_t)(j + 1) * m + j] = hn;
-      if (hn > 0.) k_scale<T><<<gn, tb, 0, s>>>(n, 1. / hn, w);
       for (int i = 0; i < j; ++i) {
         const double a = H[(size_t)i * m + j], b = H[(size_t)(i + 1) * m + j];
         H[(size_t)i * m + j] = cs[i] * a + sn[i] * b;
@@ -651,8 +712,9 @@ static void gmres(fcfd_ctx *x, NewtonState &ns, Krylov<T> &K, int mode, double r
       for (int l = i + 1; l < k; ++l) t -= H[(size_t)i * m + l] * y[l];
       y[i] = t / H[(size_t)i * m + i];
     }
-    CK(cudaMemcpyAsync(K.h.p, y.data(), sizeof(double) * k, cudaMemcpyHostToDevice, s));
-    k_combo<T><<<gn, tb, 0, s>>>(n, k, K.V.p, (size_t)n, K.h.p, K.w.p);
+    std::copy(y.begin(), y.end(), K.hp);
+    CK(cudaMemcpyAsync(K.hd.p, K.hp, sizeof(double) * k, cudaMemcpyHostToDevice, s));
+    k_combo<T><<<gn, tb, 0, s>>>(n, k, K.V.p, (size_t)n, K.hd.p, K.w.p);
     apply_prec<T>(x, ns, K.w.p, K.tmpT.p, rs, ns.sweeps);
     k_update<T><<<gn, tb, 0, s>>>(n, ns.Xs.p, K.tmpT.p, 1., x->err.p);
     if (done) break;
@@ -728,10 +790,12 @@ int fcfd_newton_solve(fcfd_ctx *x, double *W, const fcfd_newton_opts *o, fcfd_ne
       k_local_dt<double><<<gc, tb, 0, s>>>(x->cs, m, x->p64.W.p, ns.dt.p, cfl, nullptr);
       // reference state magnitudes: RMS of |p+Pref|, |V|, |T+Tref|
       RowScale wref;
+      double wn[5];
       {
         double rp = dnorm(x, part, hh, ns.Wn.p, nc), ru = dnorm(x, part, hh, ns.Wn.p + nc, nc);
         double rv = dnorm(x, part, hh, ns.Wn.p + 2 * (size_t)nc, nc), rw = dnorm(x, part, hh, ns.Wn.p + 3 * (size_t)nc, nc);
         double rT = dnorm(x, part, hh, ns.Wn.p + 4 * (size_t)nc, nc);
+        wn[0] = rp; wn[1] = ru; wn[2] = rv; wn[3] = rw; wn[4] = rT;
         const double sq = std::sqrt((double)nc);
         double U = std::sqrt(ru * ru + rv * rv + rw * rw) / sq;
         wref.s[0] = rp / sq + std::fabs(x->cs.Pref);
@@ -753,7 +817,13 @@ int fcfd_newton_solve(fcfd_ctx *x, double *W, const fcfd_newton_opts *o, fcfd_ne
         const double r = dnorm(x, part, hh, ns.rowmag.p + (size_t)v * nc, nc) / std::sqrt((double)nc);
         rs.s[v] = (r > 0.) ? 1. / r : 1.;
       }
-      ns.wscale = dnorm(x, part, hh, ns.Wn.p, n);
+      for (int v = 0; v < 5; ++v) ns.winv.s[v] = 1. / wref.s[v];
+      {
+        // |S^-1 W| from the per-variable norms
+        double q = 0.;
+        for (int v = 0; v < 5; ++v) q += wn[v] * wn[v] * ns.winv.s[v] * ns.winv.s[v];
+        ns.wscale = std::sqrt(q);
+      }
       int kit = 0;
       double rr = 0.;
       const double krtol = o->krylov_rtol > 0 ? o->krylov_rtol : 1e-2;
