@@ -341,7 +341,10 @@ def run_newton(fb, cs, mesh, case, dev, dist):
 
 # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) from
 # ncu captures of the same kernels; the capture commands are in profiles/.
-NCU_TRAFFIC = {}
+NCU_TRAFFIC = {
+    ("cylinder", "grad_limiter"): 17762816, ("cylinder", "face_flux"): 22143744,
+    ("hypersonic", "grad_limiter"): 176979200, ("hypersonic", "face_flux"): 141528064,
+}
 
 
 def ns_has_outlet(case):

@@ -87,6 +87,10 @@ struct fcfd_ctx {
   // mesh arrays
   DBuf<int> f_parent, f_neighbor, f_bc, cf_index, cf_list, st_index, st_keys, bface, outlet, color_cells;
   std::vector<int> color_index;
+  // Gauss-Seidel couplings packed per colour, slot-major [gs_deg][cells of the
+  // colour]: the neighbour across each interior face and the signed face
+  DBuf<int> gs_nbr, gs_src;
+  int gs_deg = 0;
   DBuf<double> f_n, f_area, f_x, f_w, c_x, c_len, st_cof, st_self, st_recip, st_mirror;
   // state arrays
   Pipe<double> p64;

@@ -229,6 +229,40 @@ int fcfd_ctx_create(const fcfd_mesh *mp, const fcfd_case *csp, int device, fcfd_
   x->bface.upload(bface);
   x->color_cells.upload(m.color_cells);
   x->color_index = m.color_index;
+  {
+    // packed Gauss-Seidel couplings (colour by colour, slot-major)
+    const std::vector<int> &ci = m.color_index;
+    const std::vector<int> &cc = m.color_cells;
+    int deg = 0;
+    for (int c = 0; c < nc; ++c) {
+      int d = 0;
+      for (int j = m.cf_index[c]; j < m.cf_index[c + 1]; ++j) {
+        if (m.f_bc[m.cf_list[j]] < 0) ++d;
+      }
+      deg = std::max(deg, d);
+    }
+    std::vector<int> nbr((size_t)nc * deg, -1), src((size_t)nc * deg, 0);
+    for (size_t col = 0; col + 1 < ci.size(); ++col) {
+      const int base = ci[col], cnt = ci[col + 1] - ci[col];
+      for (int i = 0; i < cnt; ++i) {
+        const int c = cc[base + i];
+        int slot = 0;
+        for (int j = m.cf_index[c]; j < m.cf_index[c + 1]; ++j) {
+          // host cf_list holds plain face indices; src is signed like the
+          // device list (~f where this cell is the face's neighbour)
+          const int f = m.cf_list[j];
+          if (m.f_bc[f] >= 0) continue;
+          const bool parent = m.f_parent[f] == c;
+          const size_t at = (size_t)base * deg + (size_t)slot * cnt + i;
+          nbr[at] = parent ? m.f_neighbor[f] : m.f_parent[f];
+          src[at] = parent ? f : ~f;
+          ++slot;
+        }
+      }
+    }
+    x->gs_deg = deg;
+    if (deg > 0) { x->gs_nbr.upload(nbr); x->gs_src.upload(src); }
+  }
   x->outlet.upload(outl);
   x->n_outlet = (int)outl.size();
   // ---- state buffers

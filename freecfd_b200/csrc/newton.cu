@@ -261,42 +261,87 @@ __global__ void k_jacobi_sweep(DevMesh m, const double *__restrict__ Minv, const
   }
 }
 
-// Block Gauss-Seidel update of the cells of one colour, in place:
-// y_c = Binv (r - O y)_c (no two cells of a colour share a face).
-__global__ void k_gs_color(DevMesh m, const int *__restrict__ cells, int ncells, const double *__restrict__ Minv,
-                           const double *__restrict__ JL, const double *__restrict__ JR, const double *__restrict__ r,
-                           double *__restrict__ y) {
+// Pack one colour's couplings for the Gauss-Seidel kernel: the signed
+// off-diagonal blocks (slot-major [deg][25][cnt]) and the inverse diagonal
+// blocks ([25][cnt]), so that consecutive threads read consecutive words.
+__global__ void k_pack_gs(int nc, int nf, int deg, int cnt, const int *__restrict__ cells, const int *__restrict__ nbr,
+                          const int *__restrict__ src, const double *__restrict__ JL, const double *__restrict__ JR,
+                          const double *__restrict__ Minv, double *__restrict__ OB, double *__restrict__ MinvP) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= ncells) return;
+  if (i >= cnt) return;
   const int c = cells[i];
-  const int nc = m.nc, nf = m.nf;
-  double t[5];
 #pragma unroll
-  for (int q = 0; q < 5; ++q) t[q] = r[q * nc + c];
-  for (int j = m.cf_index[c]; j < m.cf_index[c + 1]; ++j) {
-    const int e = m.cf_list[j];
+  for (int q = 0; q < 25; ++q) MinvP[(size_t)q * cnt + i] = Minv[(size_t)q * nc + c];
+  for (int sl = 0; sl < deg; ++sl) {
+    const int o = nbr[(size_t)sl * cnt + i], e = src[(size_t)sl * cnt + i];
     const int f = e >= 0 ? e : ~e;
-    if (m.f_bc[f] >= 0) continue;
-    const int o = e >= 0 ? m.f_neighbor[f] : m.f_parent[f];
     const double *J = e >= 0 ? JR : JL;
     const double sg = e >= 0 ? 1. : -1.;
-    double yo[5];
 #pragma unroll
-    for (int k = 0; k < 5; ++k) yo[k] = y[k * nc + o];
+    for (int q = 0; q < 25; ++q) OB[((size_t)sl * 25 + q) * cnt + i] = o >= 0 ? sg * J[(size_t)q * nf + f] : 0.;
+  }
+}
+
+// Block Gauss-Seidel update of the cells of one colour, in place, from the
+// packed couplings: y_c = Binv (r - O y)_c (no two cells of a colour share a
+// face, so the cells update independently).  Eight lanes per cell, lane q < 5
+// owning row q, so that a colour of a few thousand cells still fills the SMs;
+// the rows meet through warp shuffles for the diagonal solve.
+constexpr int kGsLanes = 8;
+constexpr int kGsMaxDeg = 6;  // interior faces per cell of hexes, prisms, tetrahedra
+__global__ void k_gs_packed(int nc, int deg, int cnt, const int *__restrict__ cells, const int *__restrict__ nbr,
+                            const double *__restrict__ OB, const double *__restrict__ MinvP, const double *__restrict__ r,
+                            double *__restrict__ y) {
+  const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = gt / kGsLanes, q = gt % kGsLanes;
+  const bool act = i < cnt && q < 5;
+  double t = 0.;
+  int c = 0;
+  if (act) {
+    c = cells[i];
+    t = r[q * nc + c];
+    if (deg <= kGsMaxDeg) {
+      // all neighbour indices, then all neighbour states, then the products:
+      // independent loads in flight together instead of one slot at a time
+      int o[kGsMaxDeg];
 #pragma unroll
-    for (int q = 0; q < 5; ++q) {
-      double a = 0.;
+      for (int sl = 0; sl < kGsMaxDeg; ++sl) o[sl] = sl < deg ? nbr[(size_t)sl * cnt + i] : -1;
+      double yv[kGsMaxDeg][5];
 #pragma unroll
-      for (int k = 0; k < 5; ++k) a += J[(5 * q + k) * nf + f] * yo[k];
-      t[q] += sg * a;
+      for (int sl = 0; sl < kGsMaxDeg; ++sl)
+#pragma unroll
+        for (int k = 0; k < 5; ++k) yv[sl][k] = o[sl] >= 0 ? y[k * nc + o[sl]] : 0.;
+#pragma unroll
+      for (int sl = 0; sl < kGsMaxDeg; ++sl) {
+        if (o[sl] < 0) continue;
+        const double *B = OB + ((size_t)sl * 25 + 5 * q) * cnt + i;
+        double a = 0.;
+#pragma unroll
+        for (int k = 0; k < 5; ++k) a += B[(size_t)k * cnt] * yv[sl][k];
+        t += a;
+      }
+    } else {
+      for (int sl = 0; sl < deg; ++sl) {
+        const int o = nbr[(size_t)sl * cnt + i];
+        if (o < 0) continue;
+        const double *B = OB + ((size_t)sl * 25 + 5 * q) * cnt + i;
+        double a = 0.;
+#pragma unroll
+        for (int k = 0; k < 5; ++k) a += B[(size_t)k * cnt] * y[k * nc + o];
+        t += a;
+      }
     }
   }
+  // every lane takes part in the shuffles (blockDim is a multiple of 32)
+  const int lane0 = (threadIdx.x & 31) & ~(kGsLanes - 1);
+  double tk[5];
 #pragma unroll
-  for (int q = 0; q < 5; ++q) {
-    double s = 0.;
+  for (int k = 0; k < 5; ++k) tk[k] = __shfl_sync(0xffffffffu, t, lane0 + k);
+  if (act) {
+    double v = 0.;
 #pragma unroll
-    for (int k = 0; k < 5; ++k) s += Minv[(5 * q + k) * nc + c] * t[k];
-    y[q * nc + c] = s;
+    for (int k = 0; k < 5; ++k) v += MinvP[(size_t)(5 * q + k) * cnt + i] * tk[k];
+    y[q * nc + c] = v;
   }
 }
 
@@ -542,6 +587,7 @@ struct Krylov {
 
 struct NewtonState {
   DBuf<double> Wn, R0, R1, dt, vol, JL, JR, Minv, Pr, Py0, Py1, Xs, rowmag;
+  DBuf<double> OB, MinvP;  // couplings packed per colour for the Gauss-Seidel sweeps
   double wscale = 1.;  // |S^-1 W| (finite-difference step scale)
   RowScale winv;       // 1 / per-variable reference magnitudes
   int sweeps = 0, cycles = 1;
@@ -620,16 +666,22 @@ static void apply_prec(fcfd_ctx *x, NewtonState &ns, const T *v, T *z, const Row
   for (int i = 0; i < 5; ++i) one.s[i] = 1.;
   k_precond<double><<<gc, tb, 0, s>>>(nc, ns.Minv.p, ns.Pr.p, ns.Py0.p, one);
   double *a = ns.Py0.p;
-  // symmetric multicolour block Gauss-Seidel: colours forward, then backward
+  // symmetric multicolour block Gauss-Seidel: colours forward, then backward.
+  // Updating the same colour twice in a row changes nothing (its cells do not
+  // couple to each other), so the repeat at each turn is skipped.
   const std::vector<int> &ci = x->color_index;
-  const int ncol = (int)ci.size() - 1;
+  const int ncol = (int)ci.size() - 1, deg = x->gs_deg;
+  int last = -1;
   for (int k = 0; k < sweeps; ++k) {
     for (int pass = 0; pass < 2; ++pass)
       for (int q = 0; q < ncol; ++q) {
         const int col = pass == 0 ? q : ncol - 1 - q;
         const int cnt = ci[col + 1] - ci[col];
-        if (cnt > 0)
-          k_gs_color<<<(cnt + tb - 1) / tb, tb, 0, s>>>(x->dm, x->color_cells.p + ci[col], cnt, ns.Minv.p, ns.JL.p, ns.JR.p, ns.Pr.p, a);
+        if (cnt <= 0 || col == last) continue;
+        last = col;
+        const size_t base = (size_t)ci[col];
+        k_gs_packed<<<(int)(((size_t)cnt * kGsLanes + 127) / 128), 128, 0, s>>>(nc, deg, cnt, x->color_cells.p + base, x->gs_nbr.p + base * deg,
+                                                      ns.OB.p + base * deg * 25, ns.MinvP.p + base * 25, ns.Pr.p, a);
       }
   }
   k_cast<T><<<(5 * nc + tb - 1) / tb, tb, 0, s>>>(5 * nc, a, z);
@@ -743,6 +795,7 @@ int fcfd_newton_solve(fcfd_ctx *x, double *W, const fcfd_newton_opts *o, fcfd_ne
     ns.JL.alloc(25 * (size_t)m.nf); ns.JR.alloc(25 * (size_t)m.nf); ns.Minv.alloc(25 * (size_t)nc);
     ns.Pr.alloc(n); ns.Py0.alloc(n); ns.Py1.alloc(n); ns.Xs.alloc(n); ns.rowmag.alloc(n);
     ns.sweeps = o->precond_sweeps; ns.cycles = o->krylov_cycles > 0 ? o->krylov_cycles : 1;
+    if (ns.sweeps > 0) { ns.OB.alloc((size_t)nc * x->gs_deg * 25 + 1); ns.MinvP.alloc(25 * (size_t)nc); }
     CK(cudaMemsetAsync(ns.JR.p, 0, sizeof(double) * 25 * (size_t)m.nf, s));
     std::vector<double> vol(x->mesh->c_volume.begin(), x->mesh->c_volume.begin() + nc);
     CK(cudaMemcpyAsync(ns.vol.p, vol.data(), sizeof(double) * nc, cudaMemcpyHostToDevice, s));
@@ -809,6 +862,18 @@ int fcfd_newton_solve(fcfd_ctx *x, double *W, const fcfd_newton_opts *o, fcfd_ne
       else
         k_face_jac<false><<<(m.nf + 127) / 128, 128, 0, s>>>(x->cs, m, x->p64.W.p, x->p64.G.p, x->p64.Lm.p, x->p64.stale.p, ns.JL.p, ns.JR.p);
       k_block_jacobi<<<gc, tb, 0, s>>>(x->cs, m, ns.Wn.p, ns.vol.p, ns.dt.p, ns.JL.p, ns.JR.p, ns.Minv.p, x->err.p, wref, ns.rowmag.p);
+      if (ns.sweeps > 0) {
+        const std::vector<int> &ci = x->color_index;
+        const int deg = x->gs_deg;
+        for (size_t col = 0; col + 1 < ci.size(); ++col) {
+          const int cnt = ci[col + 1] - ci[col];
+          if (cnt <= 0) continue;
+          const size_t base = (size_t)ci[col];
+          k_pack_gs<<<(cnt + 127) / 128, 128, 0, s>>>(nc, m.nf, deg, cnt, x->color_cells.p + base, x->gs_nbr.p + base * deg,
+                                                      x->gs_src.p + base * deg, ns.JL.p, ns.JR.p, ns.Minv.p,
+                                                      ns.OB.p + base * deg * 25, ns.MinvP.p + base * 25);
+        }
+      }
       CK(cudaGetLastError());
       // GMRES norm weights: 1 / RMS row magnitude, so every equation is measured
       // in units of a relative state change (consistent across equations)
