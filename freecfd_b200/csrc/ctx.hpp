@@ -74,6 +74,10 @@ struct Pipe {
 };
 }  // namespace fcfd
 
+namespace fcfd {
+struct AdjointState;  // adjoint.cu: buffers of the reverse sweep, allocated on first use
+}
+
 using namespace fcfd;  // internal header: the context mirrors the device types
 
 struct fcfd_ctx {
@@ -96,6 +100,7 @@ struct fcfd_ctx {
   Pipe<double> p64;
   Pipe<Dual<double>> pjv;
   DBuf<double> Win, Vin, Rtmp, dt, mdot, wl;
+  AdjointState *adj = nullptr;
   DBuf<unsigned long long> ext;    // global extrema slots of the VK limiter (armed between chains)
   DBuf<unsigned long long> dtmin;  // CFL_MAX minimum of the local time step
   DBuf<int> err, argx;
@@ -111,4 +116,5 @@ constexpr int kExtremaBlocks = 296;  // 2 x 148 SMs
 template <class S>
 void launch_chain(fcfd_ctx *x, Pipe<S> &P, S *Rout, bool aos_out, S *mo, S *wo, bool frozen_limiter = false);
 int check_err(fcfd_ctx *x);
+void adjoint_free(fcfd_ctx *x);
 }  // namespace fcfd

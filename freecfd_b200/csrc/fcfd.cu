@@ -297,6 +297,7 @@ void fcfd_ctx_destroy(fcfd_ctx *x) {
   if (!x) return;
   cudaSetDevice(x->device);
   if (x->graph) cudaGraphExecDestroy(x->graph);
+  adjoint_free(x);
   if (x->stream) cudaStreamDestroy(x->stream);
   delete x;
 }

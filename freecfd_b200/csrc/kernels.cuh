@@ -819,16 +819,36 @@ __host__ __device__ __forceinline__ void vanleer(const DevCase &c, const FState<
   }
 }
 
+// Sources of the u, v, w, T gradient rows (12 values per cell) that the
+// viscous flux reads: the stored cell gradients, or local copies (adjoint
+// kernels, where they are independent inputs).
+template <class SG>
+struct GlobalGrad {
+  typedef SG value_type;
+  const SG *G;
+  int nc, pa, nb;
+  __device__ __forceinline__ SG at_pa(int i) const { return G[(3 + i) * nc + pa]; }
+  __device__ __forceinline__ SG at_nb(int i) const { return G[(3 + i) * nc + nb]; }
+};
+template <class SG>
+struct LocalGrad {
+  typedef SG value_type;
+  const SG *gpa, *gnb;
+  __device__ __forceinline__ SG at_pa(int i) const { return gpa[i]; }
+  __device__ __forceinline__ SG at_nb(int i) const { return gnb[i]; }
+};
+
 // Face difference D = F_diffusive - F_convective * A for prepared left/right
 // states (convective_face_flux + diffusive_face_flux,
-// ns_convective_face_flux.cc:32-59, ns_diffusive_face_flux.cc:28-64).  SG is
-// the type of the stored cell gradients (S itself, or double when only the
-// face states carry tangents, as in the face-Jacobian kernel).
-template <class S, class SG, bool VISCOUS>
+// ns_convective_face_flux.cc:32-59, ns_diffusive_face_flux.cc:28-64).  GS
+// supplies the parent / neighbour gradient rows (GlobalGrad or LocalGrad);
+// its value type is S itself, or double when only the face states carry
+// tangents, as in the face-Jacobian kernel.
+template <class S, class GS, bool VISCOUS>
 __device__ __forceinline__ void face_D(const DevCase &cs, const DevMesh &m, int f, const double n[3], double A, int b,
-                                       int pa, int nb, const FState<S> &L, const FState<S> &R, const SG *__restrict__ G,
-                                       const SG *__restrict__ mu_t, S D[5], S &wL) {
-  const int nf = m.nf, nt = m.nt, nc = m.nc;
+                                       int pa, int nb, const FState<S> &L, const FState<S> &R, const GS &gs,
+                                       const typename GS::value_type *__restrict__ mu_t, S D[5], S &wL) {
+  const int nf = m.nf, nt = m.nt;
   S F[5];
   if (cs.flux == 1) roe(cs, L, R, n, F, wL);
   else if (cs.flux == 2) vanleer(cs, L, R, n, F, wL);
@@ -839,11 +859,11 @@ __device__ __forceinline__ void face_D(const DevCase &cs, const DevMesh &m, int 
     S gr[12];  // u,v,w,T gradients at the face
     if (b >= 0) {
 #pragma unroll
-      for (int i = 0; i < 12; ++i) gr[i] = S(G[(3 + i) * nc + pa]);
+      for (int i = 0; i < 12; ++i) gr[i] = S(gs.at_pa(i));
     } else {
       const double wP = m.f_w[f], wN = m.f_w[nf + f];
 #pragma unroll
-      for (int i = 0; i < 12; ++i) gr[i] = S(wP * G[(3 + i) * nc + pa] + wN * G[(3 + i) * nc + nb]);
+      for (int i = 0; i < 12; ++i) gr[i] = S(wP * gs.at_pa(i) + wN * gs.at_nb(i));
     }
     const double l0 = m.c_x[nb] - m.c_x[pa], l1 = m.c_x[nt + nb] - m.c_x[nt + pa], l2 = m.c_x[2 * nt + nb] - m.c_x[2 * nt + pa];
     const double lm = sqrt(l0 * l0 + l1 * l1 + l2 * l2);
@@ -917,7 +937,8 @@ __global__ void __launch_bounds__(128) k_face_flux(DevCase cs, DevMesh m, const 
   FState<S> L, R;
   face_states(cs, m, f, n, b, pa, nb, W, G, Lm, stale, L, R, err);
   S Dv[5], wL;
-  face_D<S, S, VISCOUS>(cs, m, f, n, A, b, pa, nb, L, R, G, mu_t, Dv, wL);
+  const GlobalGrad<S> gs{G, m.nc, pa, nb};
+  face_D<S, GlobalGrad<S>, VISCOUS>(cs, m, f, n, A, b, pa, nb, L, R, gs, mu_t, Dv, wL);
 #pragma unroll
   for (int v = 0; v < 5; ++v) D[v * nf + f] = Dv[v];
   if (mdot_out) mdot_out[f] = (-Dv[0]) / A;

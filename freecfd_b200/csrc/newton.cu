@@ -23,48 +23,9 @@
 #include <vector>
 
 #include "ctx.hpp"
+#include "dn.cuh"
 
 namespace fcfd {
-
-// ------------------------------------------------------------------ 5-lane duals
-template <int N>
-struct DN {
-  double v, d[N];
-  __host__ __device__ DN() : v(0) { for (int i = 0; i < N; ++i) d[i] = 0; }
-  __host__ __device__ DN(double x) : v(x) { for (int i = 0; i < N; ++i) d[i] = 0; }
-};
-template <int N> __device__ __forceinline__ DN<N> operator+(const DN<N> &a, const DN<N> &b) { DN<N> r; r.v = a.v + b.v; for (int i = 0; i < N; ++i) r.d[i] = a.d[i] + b.d[i]; return r; }
-template <int N> __device__ __forceinline__ DN<N> operator-(const DN<N> &a, const DN<N> &b) { DN<N> r; r.v = a.v - b.v; for (int i = 0; i < N; ++i) r.d[i] = a.d[i] - b.d[i]; return r; }
-template <int N> __device__ __forceinline__ DN<N> operator-(const DN<N> &a) { DN<N> r; r.v = -a.v; for (int i = 0; i < N; ++i) r.d[i] = -a.d[i]; return r; }
-template <int N> __device__ __forceinline__ DN<N> operator*(const DN<N> &a, const DN<N> &b) { DN<N> r; r.v = a.v * b.v; for (int i = 0; i < N; ++i) r.d[i] = a.d[i] * b.v + a.v * b.d[i]; return r; }
-template <int N> __device__ __forceinline__ DN<N> operator/(const DN<N> &a, const DN<N> &b) { DN<N> r; r.v = a.v / b.v; for (int i = 0; i < N; ++i) r.d[i] = (a.d[i] - r.v * b.d[i]) / b.v; return r; }
-template <int N> __device__ __forceinline__ DN<N> operator+(const DN<N> &a, double b) { DN<N> r = a; r.v += b; return r; }
-template <int N> __device__ __forceinline__ DN<N> operator+(double a, const DN<N> &b) { DN<N> r = b; r.v += a; return r; }
-template <int N> __device__ __forceinline__ DN<N> operator-(const DN<N> &a, double b) { DN<N> r = a; r.v -= b; return r; }
-template <int N> __device__ __forceinline__ DN<N> operator-(double a, const DN<N> &b) { DN<N> r = -b; r.v += a; return r; }
-template <int N> __device__ __forceinline__ DN<N> operator*(const DN<N> &a, double b) { DN<N> r; r.v = a.v * b; for (int i = 0; i < N; ++i) r.d[i] = a.d[i] * b; return r; }
-template <int N> __device__ __forceinline__ DN<N> operator*(double a, const DN<N> &b) { return b * a; }
-template <int N> __device__ __forceinline__ DN<N> operator/(const DN<N> &a, double b) { DN<N> r; r.v = a.v / b; for (int i = 0; i < N; ++i) r.d[i] = a.d[i] / b; return r; }
-template <int N> __device__ __forceinline__ DN<N> operator/(double a, const DN<N> &b) { DN<N> r; r.v = a / b.v; for (int i = 0; i < N; ++i) r.d[i] = -r.v * b.d[i] / b.v; return r; }
-#define FCFD_DN_CMP(op)                                                                                                      \
-  template <int N> __device__ __forceinline__ bool operator op(const DN<N> &a, const DN<N> &b) { return a.v op b.v; }      \
-  template <int N> __device__ __forceinline__ bool operator op(const DN<N> &a, double b) { return a.v op b; }              \
-  template <int N> __device__ __forceinline__ bool operator op(double a, const DN<N> &b) { return a op b.v; }
-FCFD_DN_CMP(<)
-FCFD_DN_CMP(>)
-FCFD_DN_CMP(<=)
-FCFD_DN_CMP(>=)
-FCFD_DN_CMP(==)
-FCFD_DN_CMP(!=)
-#undef FCFD_DN_CMP
-template <int N> __device__ __forceinline__ DN<N> sqrt(const DN<N> &a) { DN<N> r; r.v = ::sqrt(a.v); for (int i = 0; i < N; ++i) r.d[i] = a.d[i] / (2. * r.v); return r; }
-template <int N> __device__ __forceinline__ DN<N> fabs(const DN<N> &a) { return a.v < 0. ? -a : a; }
-template <int N> __device__ __forceinline__ DN<N> pow(const DN<N> &a, double e) {
-  DN<N> r; r.v = ::pow(a.v, e);
-  const double s = (a.v == 0.) ? 0. : e * r.v / a.v;
-  for (int i = 0; i < N; ++i) r.d[i] = s * a.d[i];
-  return r;
-}
 
 typedef DN<5> D5;
 
@@ -106,6 +67,7 @@ __global__ void __launch_bounds__(128) k_face_jac(DevCase cs, DevMesh m, const d
   face_states(cs, m, f, n, b, pa, nb, W, G, Lm, stale, L, R, (int *)nullptr);
   FState<D5> Ld, Rd;
   D5 D[5], wl;
+  const GlobalGrad<double> gs{G, m.nc, pa, nb};
   seed(L, Ld, cs, n);
   if (b < 0) {
     lift(R, Rd);
@@ -115,7 +77,7 @@ __global__ void __launch_bounds__(128) k_face_jac(DevCase cs, DevMesh m, const d
     if (!apply_bc(cs, cs.bc[b], Ld, Rd, n, (int *)nullptr)) Rd.rho = D5(R.rho);
     finish(cs, Rd, n);
   }
-  face_D<D5, double, VISCOUS>(cs, m, f, n, A, b, pa, nb, Ld, Rd, G, (const double *)nullptr, D, wl);
+  face_D<D5, GlobalGrad<double>, VISCOUS>(cs, m, f, n, A, b, pa, nb, Ld, Rd, gs, (const double *)nullptr, D, wl);
 #pragma unroll
   for (int i = 0; i < 5; ++i)
 #pragma unroll
@@ -123,7 +85,7 @@ __global__ void __launch_bounds__(128) k_face_jac(DevCase cs, DevMesh m, const d
   if (b < 0) {
     lift(L, Ld);
     seed(R, Rd, cs, n);
-    face_D<D5, double, VISCOUS>(cs, m, f, n, A, b, pa, nb, Ld, Rd, G, (const double *)nullptr, D, wl);
+    face_D<D5, GlobalGrad<double>, VISCOUS>(cs, m, f, n, A, b, pa, nb, Ld, Rd, gs, (const double *)nullptr, D, wl);
 #pragma unroll
     for (int i = 0; i < 5; ++i)
 #pragma unroll

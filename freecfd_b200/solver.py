@@ -148,6 +148,36 @@ class NavierStokes:
         check(lib.fcfd_jvp(self.h, pw, pv, pr, pj, fw))
         return (R, JV) if with_residual else JV
 
+    def vjp(self, W, Rbar):
+        """Adjoint (dR/dW)^T . Rbar of the residual (backward half of jvp)."""
+        nc = self.mesh.nc
+        host = isinstance(W, np.ndarray)
+        if host:
+            W = np.ascontiguousarray(W, dtype=np.float64)
+            Rbar = np.ascontiguousarray(Rbar, dtype=np.float64)
+            Wb = np.empty((nc, 5))
+        else:
+            Wb = W.new_empty((nc, 5))
+        pw, fw = _ptr(W)
+        pr, _ = _ptr(Rbar)
+        pb, _ = _ptr(Wb)
+        check(lib.fcfd_vjp(self.h, pw, pr, pb, fw))
+        return Wb
+
+    def drag(self, W, regions, direction=(1.0, 0.0, 0.0), gradient=True):
+        """Force on the BC regions `regions` (0-based indices) and, with
+        gradient=True, d(force . direction)/dW.  Returns (force[3], grad)."""
+        nc = self.mesh.nc
+        mask = 0
+        for b in regions:
+            mask |= 1 << int(b)
+        W = np.ascontiguousarray(W, dtype=np.float64)
+        d = np.ascontiguousarray(direction, dtype=np.float64)
+        F = np.empty(3)
+        G = np.empty((nc, 5)) if gradient else None
+        check(lib.fcfd_drag(self.h, _d(W), mask, _d(d), _d(F), _d(G) if G is not None else None, 0))
+        return F, G
+
     def newton_solve(self, W, tol=1e-10, max_newton=200, krylov_dim=30, krylov_rtol=1e-2, cfl0=1.0,
                      cfl_growth=1.2, cfl_max=1e6, cfl_mode=1, ser_exponent=1.0, jvp=True, fp32_krylov=False,
                      max_seconds=0.0, raise_on_fail=True, precond_sweeps=0, krylov_cycles=1, exact_jvp=False):

@@ -136,6 +136,23 @@ int fcfd_local_dt(fcfd_ctx *ctx, const double *W, double cfl, int mode, double *
  * matrix-free Newton-Krylov solve. */
 int fcfd_jvp(fcfd_ctx *ctx, const double *W, const double *V, double *R, double *JV, int flags);
 
+/* Adjoint (VJP) of the residual: Wbar = (dR/dW)^T Rbar for a cotangent
+ * Rbar[nc][5]; the backward half of the (fcfd_jvp, fcfd_vjp) pair, exact for
+ * the discrete residual (the branches taken at W).  The reference has no
+ * adjoint; the map it transposes is the residual of
+ * NavierStokes::assemble_linear_system (ns_assemble_linear_system.cc:34-140)
+ * with calc_cell_grads (ns.cc:301-336) and calc_limiter (ns_limiters.cc). */
+int fcfd_vjp(fcfd_ctx *ctx, const double *W, const double *Rbar, double *Wbar, int flags);
+
+/* Boundary loads and their adjoint gradient.  force[3] = sum over the faces
+ * of every BC region b with bit b of bc_mask set of the convective minus
+ * diffusive momentum flux times area (the loads of
+ * ns_assemble_linear_system.cc:108-119: pressure + viscous force on the
+ * region).  If dJdW is not NULL it receives d(force . dir)/dW [nc][5] (e.g.
+ * dir = freestream direction: the drag gradient). */
+int fcfd_drag(fcfd_ctx *ctx, const double *W, uint32_t bc_mask, const double *dir, double *force, double *dJdW,
+              int flags);
+
 /* Options of the device Newton-Krylov solve. */
 typedef struct fcfd_newton_opts {
   int32_t max_newton;     /* Newton (pseudo-time) steps, default 200 */

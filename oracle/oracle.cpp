@@ -1571,9 +1571,14 @@ struct NS {
   }
 
   // ns_assemble_linear_system.cc:34-140 (residual part; no Jacobian)
-  void assemble(std::vector<S> &rhs, const std::vector<S> *mu_t_face = nullptr, double Pr_t = 0.9) {
+  // loads: optional per-BC force [bcCount][3], integrated as in
+  // ns_assemble_linear_system.cc:108-119 (convective - diffusive momentum flux
+  // of every face of the region)
+  void assemble(std::vector<S> &rhs, const std::vector<S> *mu_t_face = nullptr, double Pr_t = 0.9,
+                std::vector<S> *loads = nullptr) {
     Grid &g = O.grid;
     rhs.assign((size_t)g.cellCount * 5, S(0.));
+    if (loads) loads->assign((size_t)g.bcCount * 3, S(0.));
     S fc[5], fd[5];
     for (int m = 0; m < 5; ++m) fd[m] = S(0.);
     for (int f = 0; f < g.faceCount; ++f) {
@@ -1587,6 +1592,8 @@ struct NS {
       if (mu_t_face) { tv = (*mu_t_face)[f]; tc = O.material.Cp() * tv / Pr_t; }
       diffusive_face_flux(fd, tv, tc);
       F.mdot[f] = (fc[0] - fd[0]) / face.area;
+      if (loads && g.face[f].bc >= 0)
+        for (int i = 0; i < 3; ++i) (*loads)[(size_t)g.face[f].bc * 3 + i] += fc[i + 1] - fd[i + 1];
       for (int i = 0; i < 5; ++i) {
         S value = fd[i] - fc[i] + S(0.);
         rhs[(size_t)pa * 5 + i] += value;
@@ -1799,6 +1806,39 @@ int orc_residual_cstep(void *h, const double *W, const double *dW, double hstep,
     std::vector<CStep> rhs;
     ns.assemble(rhs);
     for (size_t k = 0; k < rhs.size(); ++k) dR[k] = rhs[k].im / hstep;
+  } catch (const std::exception &e) {
+    if (err && errlen > 0) std::snprintf(err, errlen, "%s", e.what());
+    return 1;
+  }
+  return 0;
+}
+
+// Boundary loads: force[bcCount][3] for state W, and (dW non-null) their
+// complex-step directional derivative along dW instead.
+int orc_loads(void *h, const double *W, const double *dW, double hstep, double *force, char *err, int errlen) {
+  Handle *H = static_cast<Handle *>(h);
+  Oracle &O = H->O;
+  Grid &g = O.grid;
+  Fields<CStep> F;
+  F.alloc(g.cell.size(), (size_t)g.faceCount);
+  try {
+    const double hs = dW ? hstep : 0.;
+    for (int c = 0; c < g.cellCount; ++c) {
+      auto at = [&](int k) { return CStep(W[5 * c + k], dW ? hs * dW[5 * c + k] : 0.); };
+      F.p[c] = at(0);
+      F.V[c] = V3<CStep>(at(1), at(2), at(3));
+      F.T[c] = at(4);
+      F.rho[c] = O.material.rho(F.p[c], F.T[c]);
+    }
+    for (int i = 0; i < 5; ++i)
+      for (size_t c = 0; c < g.cell.size(); ++c) F.limiter[i][c] = CStep((O.order == FIRST) ? 0. : 1.);
+    NS<CStep> ns(O, F);
+    ns.update_boundaries();
+    ns.calc_cell_grads();
+    ns.calc_limiter();
+    std::vector<CStep> rhs, loads;
+    ns.assemble(rhs, nullptr, 0.9, &loads);
+    for (size_t k = 0; k < loads.size(); ++k) force[k] = dW ? loads[k].im / hstep : loads[k].re;
   } catch (const std::exception &e) {
     if (err && errlen > 0) std::snprintf(err, errlen, "%s", e.what());
     return 1;
