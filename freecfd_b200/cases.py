@@ -61,6 +61,8 @@ class Case:
     state: np.ndarray = None     # (Nc, 5) float64 seeded primitive state p,u,v,w,T
     freestream: tuple = ()       # (p, u, v, w, T)
     workload: str = ""
+    kstate: np.ndarray = None    # (Nc, 2) seeded turbulence state k, omega (k-omega decks)
+    kfree: tuple = ()            # (k, omega) of the freestream
 
     def write_deck(self, directory: str) -> str:
         """Write the deck (and any .mat files) into ``directory``; return deck path."""
@@ -429,8 +431,17 @@ grid_1 {{
 """
     free = (p, U, 0.0, 0.0, T)
     st = seeded_state(mesh.n_cells, free, seed)
-    return Case("plate", mesh, deck, {"air": mat}, st, free,
+    case = Case("plate", mesh, deck, {"air": mat}, st, free,
                 f"rans_flat_plate_{ni}x{nj}x{nk}_hex_roe_viscous_komega")
+    if turbulent:
+        # freestream k, omega as the reference's inlet / IC formulas give them
+        # (rans.cc:112-116, rans_set_bcs.cc:61-65): intensity 1e-3, ratio 1
+        k = max(1e-10, 1.5 * (1e-3 * U) ** 2)
+        omega = rho * k / (1.0 * mu)
+        case.kfree = (k, omega)
+        rng = np.random.default_rng(seed + 1)
+        case.kstate = np.array([k, omega])[None, :] * (1.0 + 0.01 * rng.uniform(-1.0, 1.0, size=(mesh.n_cells, 2)))
+    return case
 
 
 CONFIGS = {

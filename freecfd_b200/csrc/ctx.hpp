@@ -76,6 +76,7 @@ struct Pipe {
 
 namespace fcfd {
 struct AdjointState;  // adjoint.cu: buffers of the reverse sweep, allocated on first use
+struct RansState;     // rans.cu: k-omega state and buffers (turbulent cases)
 }
 
 using namespace fcfd;  // internal header: the context mirrors the device types
@@ -101,6 +102,7 @@ struct fcfd_ctx {
   Pipe<Dual<double>> pjv;
   DBuf<double> Win, Vin, Rtmp, dt, mdot, wl;
   AdjointState *adj = nullptr;
+  RansState *rans = nullptr;
   DBuf<unsigned long long> ext;    // global extrema slots of the VK limiter (armed between chains)
   DBuf<unsigned long long> dtmin;  // CFL_MAX minimum of the local time step
   DBuf<int> err, argx;
@@ -117,4 +119,6 @@ template <class S>
 void launch_chain(fcfd_ctx *x, Pipe<S> &P, S *Rout, bool aos_out, S *mo, S *wo, bool frozen_limiter = false);
 int check_err(fcfd_ctx *x);
 void adjoint_free(fcfd_ctx *x);
+void rans_setup(fcfd_ctx *x);
+void rans_free(fcfd_ctx *x);
 }  // namespace fcfd

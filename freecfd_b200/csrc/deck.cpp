@@ -370,8 +370,19 @@ fcfd_case *read_deck(const std::string &path) {
         R.kind = K_VELOCITY;
       }
       if (r.has("mdot")) { R.kind = K_MDOT; R.mdot_fixed = true; R.mdot = r.d("mdot"); }
+      R.turb_intensity = r.d("turbulenceintensity");
+      R.turb_ratio = r.d("eddyviscosityratio");
       cs->bc.push_back(R);
     }
+    const auto &il = grid.nsubs["IC"];
+    if (!il.empty()) {
+      const Sub &r = il[0];
+      cs->ic_has_p = r.has("p"); cs->ic_has_T = r.has("T"); cs->ic_has_rho = r.has("rho");
+      cs->ic_p = r.d("p"); cs->ic_T = r.d("T"); cs->ic_rho = r.d("rho");
+      for (int k = 0; k < 3; ++k) cs->ic_V[k] = r.vv.at("V").v[k];
+    }
+    if (cs->turbulent && cs->turb_model != "k-omega")
+      throw Error(FCFD_ERR_UNSUPPORTED, "turbulence model " + cs->turb_model + " is not on the B200 path (k-omega)");
   } catch (...) {
     delete cs;
     throw;

@@ -193,6 +193,7 @@ int fcfd_ctx_create(const fcfd_mesh *mp, const fcfd_case *csp, int device, fcfd_
     o.p = r.p; o.T = r.T; o.rho = r.rho; o.qdot = r.qdot; o.p_total = r.p_total; o.T_total = r.T_total;
     o.mdot_per_area = r.mdot / m.bc_total_area[b];
     for (int k = 0; k < 3; ++k) o.V[k] = r.V[k];
+    o.T_fixed = r.T_fixed ? 1 : 0;
     if (r.thermal == TH_FIXED_Q && r.type == BC_WALL) fixed_q = true;
   }
   x->viscous = mt.sutherland || mt.prandtl || mt.mu != 0. || mt.lambda != 0. || fixed_q;
@@ -288,6 +289,7 @@ int fcfd_ctx_create(const fcfd_mesh *mp, const fcfd_case *csp, int device, fcfd_
   dm.st_keys = x->st_keys.p; dm.st_cof = x->st_cof.p; dm.st_self = x->st_self.p; dm.bface = x->bface.p;
   dm.st_recip = x->st_recip.p; dm.st_mirror = x->st_mirror.p;
   dm.outlet_faces = x->outlet.p; dm.n_outlet = x->n_outlet;
+  rans_setup(x.get());  // k-omega BC values and buffers (turbulent cases only)
   CK(cudaDeviceSynchronize());
   *out = x.release();
   API_END
@@ -298,6 +300,7 @@ void fcfd_ctx_destroy(fcfd_ctx *x) {
   cudaSetDevice(x->device);
   if (x->graph) cudaGraphExecDestroy(x->graph);
   adjoint_free(x);
+  rans_free(x);
   if (x->stream) cudaStreamDestroy(x->stream);
   delete x;
 }

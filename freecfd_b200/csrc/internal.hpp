@@ -43,6 +43,8 @@ struct BcRegion {
   double p = 0, T = 0, rho = 0, qdot = 0, mdot = 0, p_total = 0, T_total = 0;
   double V[3] = {0, 0, 0};
   double total_area = 0;  // filled by the mesh builder
+  // RANS (rans_set_bcs.cc): inlet turbulence intensity / eddy-viscosity ratio
+  double turb_intensity = 1e-4, turb_ratio = 0.1;
 };
 
 struct Material {
@@ -68,6 +70,9 @@ struct fcfd_case {
   bool turbulent = false;
   std::string turb_model;
   double k_low = 1e-10, k_high = 1e8, omega_low = 1e-2, visc_ratio_limit = 1e8, Pr_t = 0.9;
+  // uniform initial state of IC_1 (the NS face values RANS::set_bcs reads)
+  double ic_p = 0, ic_T = 0, ic_rho = 0, ic_V[3] = {0, 0, 0};
+  bool ic_has_p = false, ic_has_T = false, ic_has_rho = false;
 };
 
 struct fcfd_mesh {

@@ -114,6 +114,10 @@ struct DevBC {
   int type, kind, specified, thermal;
   double p, T, rho, qdot, mdot_per_area, p_total, T_total;
   double V[3];
+  // Variable fixedonBC flags the RANS terms read (T face value, k / omega /
+  // eddy viscosity BC values of rans_set_bcs.cc)
+  int T_fixed, kw_fixed, mut_fixed, pad_;
+  double k_bc, omega_bc, mut_bc;
 };
 constexpr int kMaxBC = 16;
 struct DevCase {

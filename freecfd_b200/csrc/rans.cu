@@ -1,0 +1,325 @@
+// k-omega RANS terms on the device, coupled to the NS residual through the
+// eddy viscosity (rans_terms.cc:39-275, rans_update_eddy_viscosity.cc:26-56,
+// rans_set_bcs.cc:25-83, rans.cc:27-71).
+//
+// One evaluation for the state (W, K = (k, omega)):
+//   ghost update + extrema (NS) -> ghost k, omega and the eddy viscosity of
+//   every cell -> its face values -> NS gradients + limiter -> outlet density
+//   -> NS face flux with mu_t (also mdot and weightL per face) -> NS gather
+//   -> LSQ gradients of k, omega -> k-omega face fluxes -> gather + sources.
+// Ghost k, omega are the BC value where the reference fixes them on the BC
+// (inlets) and the parent value otherwise: the RANS update_boundaries is
+// missing from the reference snapshot and is reconstructed like the NS one.
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "ctx.hpp"
+
+namespace fcfd {
+
+extern template __global__ void k_ghost_minmax<double>(DevCase, DevMesh, double *, unsigned long long *, int *);
+
+// rans.cc:43-49, model=k-omega (blending = 1)
+struct KOmega {
+  static constexpr double sigma_k = 0.85, sigma_omega = 0.5, beta = 0.075, beta_star = 0.09, alpha = 5. / 9.;
+};
+
+struct RansState {
+  DBuf<double> K, GK, mut, mutf, DK, RK, vol;
+};
+
+void rans_free(fcfd_ctx *x) {
+  delete x->rans;
+  x->rans = nullptr;
+}
+
+namespace {
+
+__device__ __forceinline__ double face_avg(const DevMesh &m, int f, const double *x) {
+  return m.f_w[f] * x[m.f_parent[f]] + m.f_w[m.nf + f] * x[m.f_neighbor[f]];
+}
+
+// Ghost k, omega, then mu_t = min(ratio * mu, rho k / omega) for every cell.
+__global__ void k_rans_prep(DevCase cs, DevMesh m, const double *__restrict__ W, double *__restrict__ K,
+                            double *__restrict__ mut, double ratio_limit) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nc = m.nc, nt = m.nt;
+  if (i >= nt) return;
+  if (i >= nc) {
+    const int f = m.bface[i - nc], pa = m.f_parent[f];
+    const DevBC &bc = cs.bc[m.f_bc[f]];
+    if (bc.kw_fixed) { K[i] = bc.k_bc; K[nt + i] = bc.omega_bc; }
+    else { K[i] = K[pa]; K[nt + i] = K[nt + pa]; }
+  }
+  const double p = W[i], T = W[4 * nt + i];
+  const double rho = eos_rho(cs, p, T);
+  const double mu = viscosity(cs, T);
+  const double mt = rho * K[i] / K[nt + i];
+  mut[i] = smin(ratio_limit * mu, mt);
+}
+
+// mu_t.face (variable.h:134-147): the BC value where fixed, else the average.
+__global__ void k_rans_mutf(DevCase cs, DevMesh m, const double *__restrict__ mut, double *__restrict__ mutf) {
+  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= m.nf) return;
+  const int b = m.f_bc[f];
+  mutf[f] = (b >= 0 && cs.bc[b].mut_fixed) ? cs.bc[b].mut_bc : face_avg(m, f, mut);
+}
+
+// LSQ gradients of k and omega (RANS::calc_cell_grads, rans.cc:167-173),
+// the same weights as the flow gradients in their fused form.
+__global__ void k_rans_grad(DevMesh m, const double *__restrict__ K, double *__restrict__ GK) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nc = m.nc, nt = m.nt;
+  if (c >= nc) return;
+  const double xc0 = m.c_x[c], xc1 = m.c_x[nt + c], xc2 = m.c_x[2 * nt + c];
+  const double u0[2] = {K[c], K[nt + c]};
+  double acc[6] = {0., 0., 0., 0., 0., 0.};
+  for (int j = m.st_index[c]; j < m.st_index[c + 1]; ++j) {
+    const int k = m.st_keys[j];
+    if (k == c) continue;
+    const double d0 = m.c_x[k] - xc0, d1 = m.c_x[nt + k] - xc1, d2 = m.c_x[2 * nt + k] - xc2;
+    const double w = d0 * d0 + d1 * d1 + d2 * d2;
+    for (int v = 0; v < 2; ++v) {
+      const double a = w * (K[v * nt + k] - u0[v]);
+      acc[3 * v] += a * d0; acc[3 * v + 1] += a * d1; acc[3 * v + 2] += a * d2;
+    }
+  }
+  const double C00 = m.st_cof[c], C01 = m.st_cof[nc + c], C02 = m.st_cof[2 * nc + c];
+  const double C11 = m.st_cof[3 * nc + c], C12 = m.st_cof[4 * nc + c], C22 = m.st_cof[5 * nc + c];
+  const double id = 1. / m.st_cof[6 * nc + c];
+  const double M0 = m.st_mirror[c], M1 = m.st_mirror[nc + c], M2 = m.st_mirror[2 * nc + c];
+  for (int v = 0; v < 2; ++v) {
+    const double s0 = acc[3 * v], s1 = acc[3 * v + 1], s2 = acc[3 * v + 2];
+    GK[(3 * v) * nc + c] = (C00 * s0 + C01 * s1 + C02 * s2) * id - M0 * u0[v];
+    GK[(3 * v + 1) * nc + c] = (C01 * s0 + C11 * s1 + C12 * s2) * id - M1 * u0[v];
+    GK[(3 * v + 2) * nc + c] = (C02 * s0 + C12 * s1 + C22 * s2) * id - M2 * u0[v];
+  }
+}
+
+// k and omega face fluxes: DK = diffusive - convective (rans_terms.cc:59-112,
+// get_kOmega 277-319).
+__global__ void k_rans_face(DevCase cs, DevMesh m, const double *__restrict__ W, const double *__restrict__ K,
+                            const double *__restrict__ GK, const double *__restrict__ mutf,
+                            const double *__restrict__ mdot, const double *__restrict__ wl, double *__restrict__ DK) {
+  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nf = m.nf, nc = m.nc, nt = m.nt;
+  if (f >= nf) return;
+  const int pa = m.f_parent[f], nb = m.f_neighbor[f], b = m.f_bc[f];
+  const double Tf = (b >= 0 && cs.bc[b].T_fixed) ? cs.bc[b].T : face_avg(m, f, W + 4 * nt);
+  const double lam = viscosity(cs, Tf);
+  const double turb = mutf[f];
+  const double md = mdot[f], wL = wl[f], wR = 1. - wL;
+  const double kL = K[pa], oL = K[nt + pa], kR = K[nb], oR = K[nt + nb];
+  double gk[3], go[3];
+  for (int i = 0; i < 3; ++i) {
+    if (b >= 0) { gk[i] = GK[i * nc + pa]; go[i] = GK[(3 + i) * nc + pa]; }
+    else {
+      gk[i] = m.f_w[f] * GK[i * nc + pa] + m.f_w[nf + f] * GK[i * nc + nb];
+      go[i] = m.f_w[f] * GK[(3 + i) * nc + pa] + m.f_w[nf + f] * GK[(3 + i) * nc + nb];
+    }
+  }
+  const double l0 = m.c_x[nb] - m.c_x[pa], l1 = m.c_x[nt + nb] - m.c_x[nt + pa], l2 = m.c_x[2 * nt + nb] - m.c_x[2 * nt + pa];
+  const double lm = sqrt(l0 * l0 + l1 * l1 + l2 * l2);
+  const double e[3] = {l0 / lm, l1 / lm, l2 / lm};
+  const double dk = gk[0] * e[0] + gk[1] * e[1] + gk[2] * e[2];
+  const double dw = go[0] * e[0] + go[1] * e[1] + go[2] * e[2];
+  for (int i = 0; i < 3; ++i) {
+    gk[i] = gk[i] - dk * e[i] + (kR - kL) / lm * e[i];
+    go[i] = go[i] - dw * e[i] + (oR - oL) / lm * e[i];
+  }
+  const double n[3] = {m.f_n[f], m.f_n[nf + f], m.f_n[2 * nf + f]};
+  const double A = m.f_area[f];
+  const double conv0 = md * (wL * kL + wR * kR) * A, conv1 = md * (wL * oL + wR * oR) * A;
+  const double diff0 = (lam + turb * KOmega::sigma_k) * (gk[0] * n[0] + gk[1] * n[1] + gk[2] * n[2]) * A;
+  const double diff1 = (lam + turb * KOmega::sigma_omega) * (go[0] * n[0] + go[1] * n[1] + go[2] * n[2]) * A;
+  DK[f] = diff0 - conv0;
+  DK[nf + f] = diff1 - conv1;
+}
+
+// Per cell: sum of +-DK in ascending face order, plus sources x volume
+// (rans_terms.cc:191-242).  RK is [nc][2].
+__global__ void k_rans_gather(DevCase cs, DevMesh m, const double *__restrict__ W, const double *__restrict__ K,
+                              const double *__restrict__ G, const double *__restrict__ mut,
+                              const double *__restrict__ vol, const double *__restrict__ DK, double *__restrict__ RK) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nc = m.nc, nt = m.nt, nf = m.nf;
+  if (c >= nc) return;
+  double r0 = 0., r1 = 0.;
+  for (int j = m.cf_index[c]; j < m.cf_index[c + 1]; ++j) {
+    const int e = m.cf_list[j];
+    if (e >= 0) { r0 += DK[e]; r1 += DK[nf + e]; }
+    else { r0 += -1. * DK[~e]; r1 += -1. * DK[nf + ~e]; }
+  }
+  const double dudx = G[3 * nc + c], dudy = G[4 * nc + c], dudz = G[5 * nc + c];
+  const double dvdx = G[6 * nc + c], dvdy = G[7 * nc + c], dvdz = G[8 * nc + c];
+  const double dwdx = G[9 * nc + c], dwdy = G[10 * nc + c], dwdz = G[11 * nc + c];
+  const double divU = dudx + dvdy + dwdz;
+  const double sr = sqrt(2. * (dudx * dudx + dvdy * dvdy + dwdz * dwdz) + (dudy + dvdx) * (dudy + dvdx) +
+                         (dudz + dwdx) * (dudz + dwdx) + (dvdz + dwdy) * (dvdz + dwdy));
+  const double rho = eos_rho(cs, W[c], W[4 * nt + c]);
+  const double k = K[c], om = K[nt + c], mt = mut[c];
+  double Prod = mt * (sr * sr - 2. / 3. * divU * divU) - 2. / 3. * rho * k * divU;
+  const double Dest = KOmega::beta_star * rho * om * k;
+  Prod = smin(Prod, 10. * Dest);
+  const double s0 = Prod - Dest;
+  const double s1 = KOmega::alpha * rho / mt * Prod - KOmega::beta * rho * om * om;
+  RK[2 * c] = r0 + s0 * vol[c];
+  RK[2 * c + 1] = r1 + s1 * vol[c];
+}
+
+__global__ void k_k_to_soa(const double *__restrict__ in, double *__restrict__ K, int nc, int nt) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nc) return;
+  K[c] = in[2 * c];
+  K[nt + c] = in[2 * c + 1];
+}
+
+double host_viscosity(const Material &mt, double T) {
+  if (!mt.sutherland) return mt.mu;
+  return mt.sut_mu_ref * std::pow((T + mt.Tref) / mt.sut_T_ref, 1.5) * (mt.sut_T_ref + mt.sut_S) / (T + mt.Tref + mt.sut_S);
+}
+
+}  // namespace
+
+// RANS::set_bcs values: inlets fix k, omega and mu_t from the NS face values
+// at initialisation (uniform IC state with the NS ghosts updated); no-slip
+// walls fix mu_t = 0.  Runs the ghost kernel once on the IC state.
+void rans_setup(fcfd_ctx *x) {
+  const fcfd_case &c = *x->case_ptr;
+  const fcfd_mesh &m = *x->mesh;
+  if (!c.turbulent) return;
+  if (!x->viscous) throw Error(FCFD_ERR_INPUT, "a turbulence model needs a viscous material");
+  const Material &mt = c.mat;
+  const int nc = m.nc, nb = m.nb, nt = nc + nb, nf = m.nf;
+  double p = c.ic_p, T = c.ic_T;
+  const double R = mt.R;
+  if (c.ic_has_p && c.ic_has_rho) T = (p + mt.Pref) / (R * c.ic_rho) - mt.Tref;
+  else if (c.ic_has_rho && c.ic_has_T) p = c.ic_rho * R * (T + mt.Tref) - mt.Pref;
+  std::vector<double> W(5 * (size_t)nt, 0.);
+  for (int i = 0; i < nc; ++i) {
+    W[i] = p; W[nt + i] = c.ic_V[0]; W[2 * (size_t)nt + i] = c.ic_V[1]; W[3 * (size_t)nt + i] = c.ic_V[2];
+    W[4 * (size_t)nt + i] = T;
+  }
+  CK(cudaMemcpy(x->p64.W.p, W.data(), sizeof(double) * W.size(), cudaMemcpyHostToDevice));
+  if (nb > 0) k_ghost_minmax<double><<<(nb + 255) / 256, 256, 0, x->stream>>>(x->cs, x->dm, x->p64.W.p, nullptr, x->err.p);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(x->stream));
+  CK(cudaMemcpy(W.data(), x->p64.W.p, sizeof(double) * W.size(), cudaMemcpyDeviceToHost));
+  auto rho_of = [&](double pp, double TT) { return (pp + mt.Pref) / (R * (TT + mt.Tref)); };
+  for (size_t b = 0; b < c.bc.size(); ++b) {
+    const BcRegion &r = c.bc[b];
+    DevBC &o = x->cs.bc[b];
+    o.kw_fixed = 0; o.mut_fixed = 0; o.k_bc = o.omega_bc = o.mut_bc = 0.;
+    if (r.type == BC_INLET) {
+      int fid = 0;
+      for (int f = 0; f < nf; ++f)
+        if (m.f_bc[f] == (int)b) { fid = f; break; }
+      const int pa = m.f_parent[fid], g = m.f_neighbor[fid];
+      const double w0 = m.f_w[2 * (size_t)fid], w1 = m.f_w[2 * (size_t)fid + 1];
+      const bool here = m.f_bc[fid] == (int)b;
+      const double rf = (r.rho_fixed && here) ? r.rho
+                                              : w0 * rho_of(W[pa], W[4 * (size_t)nt + pa]) + w1 * rho_of(W[g], W[4 * (size_t)nt + g]);
+      const double Tf = (r.T_fixed && here) ? r.T : w0 * W[4 * (size_t)nt + pa] + w1 * W[4 * (size_t)nt + g];
+      double Vf[3];
+      for (int k = 0; k < 3; ++k)
+        Vf[k] = (r.V_fixed && here) ? r.V[k] : w0 * W[(1 + k) * (size_t)nt + pa] + w1 * W[(1 + k) * (size_t)nt + g];
+      double kb = r.turb_intensity * std::sqrt(Vf[0] * Vf[0] + Vf[1] * Vf[1] + Vf[2] * Vf[2]);
+      kb *= 1.5 * kb;
+      kb = std::max(c.k_low, kb);
+      o.kw_fixed = 1;
+      o.k_bc = kb;
+      o.omega_bc = rf * kb / (r.turb_ratio * host_viscosity(mt, Tf));
+      o.mut_fixed = 1;
+      o.mut_bc = r.turb_ratio * host_viscosity(mt, Tf);
+    } else if (r.type == BC_WALL && r.kind != K_SLIP) {
+      o.mut_fixed = 1;
+      o.mut_bc = 0.;
+    }
+  }
+  x->rans = new RansState();
+  RansState &s = *x->rans;
+  s.K.alloc(2 * (size_t)nt); s.GK.alloc(6 * (size_t)nc); s.mut.alloc(nt); s.mutf.alloc(nf); s.DK.alloc(2 * (size_t)nf);
+  s.RK.alloc(2 * (size_t)nc);
+  std::vector<double> vol(m.c_volume.begin(), m.c_volume.begin() + nc);
+  s.vol.upload(vol);
+}
+
+// One coupled evaluation; W and K already in p64.W / rans->K (interior parts).
+static void rans_chain(fcfd_ctx *x, double *R_aos, double *RK_aos) {
+  const DevMesh &m = x->dm;
+  cudaStream_t st = x->stream;
+  RansState &s = *x->rans;
+  Pipe<double> &P = x->p64;
+  const int tb = 256;
+  const bool need_ext = x->cs.limiter == 1 && x->cs.order != 1;
+  const int ng = (m.nb + tb - 1) / tb + (need_ext ? kExtremaBlocks : 0);
+  if (ng > 0) k_ghost_minmax<double><<<ng, tb, 0, st>>>(x->cs, m, P.W.p, need_ext ? x->ext.p : nullptr, x->err.p);
+  k_rans_prep<<<(m.nt + 127) / 128, 128, 0, st>>>(x->cs, m, P.W.p, s.K.p, s.mut.p, x->case_ptr->visc_ratio_limit);
+  k_rans_mutf<<<(m.nf + 127) / 128, 128, 0, st>>>(x->cs, m, s.mut.p, s.mutf.p);
+  k_grad_limiter<double><<<(m.nc + 127) / 128, 128, 0, st>>>(x->cs, m, P.W.p, x->ext.p, nullptr, P.G.p, P.Lm.p);
+  if (m.n_outlet > 0)
+    k_outlet_rho<double><<<(m.n_outlet + 127) / 128, 128, 0, st>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p);
+  k_face_flux<double, true><<<(m.nf + 127) / 128, 128, 0, st>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p, s.mutf.p, P.D.p,
+                                                                x->mdot.p, x->wl.p, x->err.p);
+  k_gather<double, true><<<(m.nc + tb - 1) / tb, tb, 0, st>>>(m, P.D.p, R_aos, x->ext.p, x->argx.p);
+  k_rans_grad<<<(m.nc + 127) / 128, 128, 0, st>>>(m, s.K.p, s.GK.p);
+  k_rans_face<<<(m.nf + 127) / 128, 128, 0, st>>>(x->cs, m, P.W.p, s.K.p, s.GK.p, s.mutf.p, x->mdot.p, x->wl.p, s.DK.p);
+  k_rans_gather<<<(m.nc + 127) / 128, 128, 0, st>>>(x->cs, m, P.W.p, s.K.p, P.G.p, s.mut.p, s.vol.p, s.DK.p, RK_aos);
+  CK(cudaGetLastError());
+}
+
+}  // namespace fcfd
+
+using namespace fcfd;
+
+extern "C" int fcfd_rans_residual(fcfd_ctx *x, const double *W, const double *K, double *R, double *RK, int flags) {
+  try {
+    if (!x || !W || !K || !R || !RK) throw Error(FCFD_ERR_INPUT, "null argument");
+    if (!x->rans) throw Error(FCFD_ERR_INPUT, "the case has no turbulence model");
+    CK(cudaSetDevice(x->device));
+    const DevMesh &m = x->dm;
+    cudaStream_t s = x->stream;
+    const bool dev = flags & FCFD_DEVICE_PTRS;
+    const size_t n = 5 * (size_t)m.nc, nk = 2 * (size_t)m.nc;
+    const double *w = W, *k = K;
+    if (!dev) {
+      CK(cudaMemcpyAsync(x->Win.p, W, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+      CK(cudaMemcpyAsync(x->rans->RK.p, K, sizeof(double) * nk, cudaMemcpyHostToDevice, s));
+      w = x->Win.p;
+      k = x->rans->RK.p;
+    }
+    const int tb = 256;
+    k_aos_to_soa<double><<<(m.nc + tb - 1) / tb, tb, 0, s>>>(w, x->p64.W.p, m.nc, m.nt);
+    k_k_to_soa<<<(m.nc + tb - 1) / tb, tb, 0, s>>>(k, x->rans->K.p, m.nc, m.nt);
+    double *r = dev ? R : x->p64.R.p;
+    double *rk = dev ? RK : x->rans->RK.p;
+    rans_chain(x, r, rk);
+    if (!dev) {
+      CK(cudaMemcpyAsync(R, x->p64.R.p, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+      CK(cudaMemcpyAsync(RK, x->rans->RK.p, sizeof(double) * nk, cudaMemcpyDeviceToHost, s));
+    }
+    CK(cudaStreamSynchronize(s));
+    check_err(x);
+  } catch (const Error &e) {
+    set_last_error(e.what());
+    return e.code;
+  } catch (const std::exception &e) {
+    set_last_error(e.what());
+    return FCFD_ERR_INPUT;
+  }
+  return FCFD_OK;
+}
+
+extern "C" int fcfd_rans_bcs(const fcfd_ctx *x, double *out, int32_t out_len) {
+  if (!x || !out) { set_last_error("null argument"); return FCFD_ERR_INPUT; }
+  const int nbc = x->cs.nbc;
+  if (out_len < 5 * nbc) { set_last_error("output too small"); return FCFD_ERR_INPUT; }
+  for (int b = 0; b < nbc; ++b) {
+    const DevBC &o = x->cs.bc[b];
+    out[5 * b] = o.kw_fixed; out[5 * b + 1] = o.k_bc; out[5 * b + 2] = o.omega_bc;
+    out[5 * b + 3] = o.mut_fixed; out[5 * b + 4] = o.mut_bc;
+  }
+  return FCFD_OK;
+}

@@ -164,6 +164,23 @@ class NavierStokes:
         check(lib.fcfd_vjp(self.h, pw, pr, pb, fw))
         return Wb
 
+    def rans_residual(self, W, K):
+        """k-omega RANS residual: (R[nc][5] with eddy viscosity, RK[nc][2])."""
+        nc = self.mesh.nc
+        W = np.ascontiguousarray(W, dtype=np.float64)
+        K = np.ascontiguousarray(K, dtype=np.float64)
+        R = np.empty((nc, 5))
+        RK = np.empty((nc, 2))
+        check(lib.fcfd_rans_residual(self.h, _d(W), _d(K), _d(R), _d(RK), 0))
+        return R, RK
+
+    def rans_bcs(self):
+        """Per BC region: kw_fixed, k, omega, mut_fixed, mu_t."""
+        nbc = int(self.case.summary()[1][5]) if hasattr(self.case, "summary") else 16
+        out = np.zeros((16, 5))
+        check(lib.fcfd_rans_bcs(self.h, _d(out), out.size))
+        return out[:nbc]
+
     def drag(self, W, regions, direction=(1.0, 0.0, 0.0), gradient=True):
         """Force on the BC regions `regions` (0-based indices) and, with
         gradient=True, d(force . direction)/dW.  Returns (force[3], grad)."""

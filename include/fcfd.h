@@ -144,6 +144,18 @@ int fcfd_jvp(fcfd_ctx *ctx, const double *W, const double *V, double *R, double 
  * with calc_cell_grads (ns.cc:301-336) and calc_limiter (ns_limiters.cc). */
 int fcfd_vjp(fcfd_ctx *ctx, const double *W, const double *Rbar, double *Wbar, int flags);
 
+/* k-omega RANS residual for the state W[nc][5] and K[nc][2] = (k, omega):
+ * R[nc][5] is the NS residual with the eddy viscosity mu_t in the viscous
+ * flux (ns_diffusive_face_flux.cc:36-39), RK[nc][2] the k and omega
+ * right-hand side of RANS::terms (rans_terms.cc:39-275) with the eddy
+ * viscosity of rans_update_eddy_viscosity.cc:26-56 and the fixed BC values of
+ * rans_set_bcs.cc:25-83.  Only model=k-omega; FCFD_ERR_INPUT if the case has
+ * no turbulence section. */
+int fcfd_rans_residual(fcfd_ctx *ctx, const double *W, const double *K, double *R, double *RK, int flags);
+/* Fixed BC values of the RANS variables, per BC region: kw_fixed, k, omega,
+ * mut_fixed, mu_t (5 doubles each; out_len >= 5 * number of regions). */
+int fcfd_rans_bcs(const fcfd_ctx *ctx, double *out, int32_t out_len);
+
 /* Boundary loads and their adjoint gradient.  force[3] = sum over the faces
  * of every BC region b with bit b of bc_mask set of the convective minus
  * diffusive momentum flux times area (the loads of

@@ -56,6 +56,9 @@ def lib():
         L.orc_local_dt.argtypes = [vp, dp, ctypes.c_double, ctypes.c_int, dp]
         L.orc_loads.argtypes = [vp, dp, dp, ctypes.c_double, dp, ctypes.c_char_p, ctypes.c_int]
         L.orc_loads.restype = ctypes.c_int
+        L.orc_rans_residual.argtypes = [vp, dp, dp, dp, dp, ctypes.c_char_p, ctypes.c_int]
+        L.orc_rans_residual.restype = ctypes.c_int
+        L.orc_rans_bcs.argtypes = [vp, dp]
         L.orc_case_summary.argtypes = [vp, dp, ip]
         _lib = L
     return _lib
@@ -177,6 +180,24 @@ class Oracle:
         rc = lib().orc_loads(self.h, _d(W), None if dW is None else _d(dW), h, _d(out), err, 512)
         if rc != 0:
             raise RuntimeError("oracle: " + err.value.decode())
+        return out
+
+    def rans_residual(self, W, K):
+        """k-omega RANS residual: (R[nc][5] with eddy viscosity, RK[nc][2])."""
+        W = np.ascontiguousarray(W, dtype=np.float64).reshape(self.nc, 5)
+        K = np.ascontiguousarray(K, dtype=np.float64).reshape(self.nc, 2)
+        R = np.empty((self.nc, 5))
+        RK = np.empty((self.nc, 2))
+        err = ctypes.create_string_buffer(512)
+        rc = lib().orc_rans_residual(self.h, _d(W), _d(K), _d(R), _d(RK), err, 512)
+        if rc != 0:
+            raise RuntimeError("oracle: " + err.value.decode())
+        return R, RK
+
+    def rans_bcs(self):
+        nbc = int(self.case_summary()[1][5])
+        out = np.empty((nbc, 5))
+        lib().orc_rans_bcs(self.h, _d(out))
         return out
 
     def local_dt(self, W, cfl, mode=0):

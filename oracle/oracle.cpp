@@ -279,7 +279,17 @@ struct Oracle {
   // Time stepping (time_step.cc)
   double cfl_max = 1000., cfl_local = 1000.;
   bool has_cfl_max = false, has_cfl_local = false;
+  // RANS k-omega (rans.cc, rans_set_bcs.cc): options and fixed BC values
+  bool turbulent = false;
+  double kLow = 1e-10, kHigh = 1e8, omegaLow = 1e-2, ratioLimit = 1e8, Pr_t = 0.9;
+  std::vector<char> kw_fixed, mut_fixed;
+  std::vector<double> k_bc, omega_bc, mut_bc;
   std::string error;
+};
+
+// rans.cc:43-49 (model=k-omega: blending = 1 everywhere)
+struct KOmega {
+  static constexpr double sigma_k = 0.85, sigma_omega = 0.5, beta = 0.075, beta_star = 0.09, alpha = 5. / 9.;
 };
 
 // ================================================================ grid setup
@@ -1606,6 +1616,166 @@ struct NS {
   }
 };
 
+// ---------------------------------------------------------------- RANS k-omega (rans_*.cc)
+
+// RANS::set_bcs (rans_set_bcs.cc:25-83) with the NS face values it reads at
+// initialisation (uniform IC state, NS ghosts updated), and the turbulence
+// deck options (rans.cc:51-71).  Only model=k-omega is restated.
+static void setup_rans(Oracle &O) {
+  Section &g = O.input.section("grid", 0);
+  Subsection &ts = g.sub("turbulence");
+  O.turbulent = ts.is_found;
+  if (!O.turbulent) return;
+  if (ts.gs("model").value != "k-omega") throw DeckError("only the k-omega turbulence model is restated");
+  O.kLow = ts.gd("klowlimit").value; O.kHigh = ts.gd("khighlimit").value;
+  O.omegaLow = ts.gd("omegalowlimit").value; O.ratioLimit = ts.gd("viscosityratiolimit").value;
+  O.Pr_t = ts.gd("turbulentPr").value;
+  Grid &gr = O.grid;
+  const Material &m = O.material;
+  // uniform initial state of IC_1 (two of p, T, rho)
+  Subsection &ic = g.sub("IC", 0);
+  double p = ic.gd("p").value, T = ic.gd("T").value, rho = ic.gd("rho").value;
+  if (ic.gd("p").is_found && ic.gd("rho").is_found) T = m.temp(p, rho);
+  else if (ic.gd("rho").is_found && ic.gd("T").is_found) p = m.pres(rho, T);
+  const V3d &icv = ic.gv("V").value;
+  Fields<double> F;
+  F.alloc(gr.cell.size(), (size_t)gr.faceCount);
+  for (int c = 0; c < gr.cellCount; ++c) {
+    F.p[c] = p; F.T[c] = T; F.V[c] = V3<double>(icv.c[0], icv.c[1], icv.c[2]); F.rho[c] = m.rho(p, T);
+  }
+  NS<double> ns(O, F);
+  ns.update_boundaries();
+  const int count = g.sub("BC", 0).count;
+  O.kw_fixed.assign(count, 0); O.mut_fixed.assign(count, 0);
+  O.k_bc.assign(count, 0.); O.omega_bc.assign(count, 0.); O.mut_bc.assign(count, 0.);
+  for (int b = 0; b < count; ++b) {
+    Subsection &region = g.sub("BC", b);
+    const std::string type = region.gs("type").value, kind = region.gs("kind").value;
+    const double intensity = region.gd("turbulenceintensity").value, ratio = region.gd("eddyviscosityratio").value;
+    if (type == "inlet") {
+      int fid = 0;
+      for (int f = 0; f < gr.faceCount; ++f)
+        if (gr.face[f].bc == b) { fid = f; break; }
+      // NS Variable face values (variable.h:134-147)
+      double rf = 0., Tf = 0.;
+      Vec3 Vf;
+      if (O.rho_fixed[b] && gr.face[fid].bc == b) rf = O.rho_bc[b];
+      else for (auto &kv : gr.face[fid].average) rf += kv.second * F.rho[kv.first];
+      Tf = ns.face_scalar(F.T, fid, 1);
+      if (O.V_fixed[b] && gr.face[fid].bc == b) Vf = O.V_bc[b];
+      else for (auto &kv : gr.face[fid].average)
+        for (int i = 0; i < 3; ++i) Vf[i] += kv.second * F.V[kv.first][i];
+      O.kw_fixed[b] = 1;
+      double kb = intensity * fabs(Vf);
+      kb *= 1.5 * kb;
+      kb = std::max(O.kLow, kb);
+      O.k_bc[b] = kb;
+      O.omega_bc[b] = rf * kb / (ratio * m.viscosity(Tf));
+      O.mut_fixed[b] = 1;
+      O.mut_bc[b] = ratio * m.viscosity(Tf);
+    } else if (type == "wall") {
+      if (kind != "slip") { O.mut_fixed[b] = 1; O.mut_bc[b] = 0.; }
+    }
+  }
+}
+
+// RANS residual for the state (W, K): NS residual with the eddy viscosity,
+// then RANS::terms (rans_terms.cc:39-275) right-hand side.  Ghost k, omega:
+// the BC value where fixed on the BC, else the parent value (the missing
+// RANS update_boundaries, reconstructed like the NS one).
+template <class S>
+static void rans_residual(Oracle &O, Fields<S> &F, const std::vector<S> &k, const std::vector<S> &om,
+                          std::vector<S> &rhs_ns, std::vector<S> &rhs_k) {
+  Grid &g = O.grid;
+  const Material &m = O.material;
+  NS<S> ns(O, F);
+  ns.update_boundaries();
+  ns.calc_cell_grads();
+  ns.calc_limiter();
+  const size_t nt = g.cell.size();
+  std::vector<S> K(nt), Om(nt), mut(nt);
+  for (int c = 0; c < g.cellCount; ++c) { K[c] = k[c]; Om[c] = om[c]; }
+  for (int f = 0; f < g.faceCount; ++f) {
+    const int b = g.face[f].bc;
+    if (b < 0) continue;
+    const int gh = g.face[f].neighbor, pa = g.face[f].parent;
+    if (O.kw_fixed[b]) { K[gh] = S(O.k_bc[b]); Om[gh] = S(O.omega_bc[b]); }
+    else { K[gh] = K[pa]; Om[gh] = Om[pa]; }
+  }
+  // rans_update_eddy_viscosity.cc:26-56 (k-omega branch), every cell
+  for (size_t c = 0; c < nt; ++c) {
+    S mu = m.viscosity(F.T[c]);
+    mut[c] = F.rho[c] * K[c] / Om[c];
+    mut[c] = smin(S(O.ratioLimit * mu), mut[c]);
+  }
+  // mu_t.face (variable.h:134-147)
+  std::vector<S> mutf((size_t)g.faceCount);
+  for (int f = 0; f < g.faceCount; ++f) {
+    const int b = g.face[f].bc;
+    if (b >= 0 && O.mut_fixed[b]) { mutf[f] = S(O.mut_bc[b]); continue; }
+    S t(0.);
+    for (auto &kv : g.face[f].average) t += kv.second * mut[kv.first];
+    mutf[f] = t;
+  }
+  ns.assemble(rhs_ns, &mutf, O.Pr_t);
+  // RANS::calc_cell_grads (rans.cc:167-173): interior cells; ghosts keep zero
+  std::vector<V3<S>> gk(nt), go(nt);
+  for (int c = 0; c < g.cellCount; ++c) { gk[c] = ns.scalar_gradient(K, c); go[c] = ns.scalar_gradient(Om, c); }
+  rhs_k.assign((size_t)g.cellCount * 2, S(0.));
+  typedef KOmega KW;
+  for (int f = 0; f < g.faceCount; ++f) {
+    const int pa = g.face[f].parent, nb = g.face[f].neighbor, b = g.face[f].bc;
+    const S lam = m.viscosity(ns.face_scalar(F.T, f, 1));
+    const S turb = mutf[f];
+    const S md = F.mdot[f], wL = F.weightL[f], wR = 1. - wL;
+    // get_kOmega (rans_terms.cc:277-319)
+    const S kL = K[pa], oL = Om[pa], kR = K[nb], oR = Om[nb];
+    V3<S> fgk, fgo;
+    if (b >= 0) { fgk = gk[pa]; fgo = go[pa]; }
+    else { fgk = ns.face_vec(gk, f); fgo = ns.face_vec(go, f); }
+    Vec3 l2r = g.cell[nb].centroid - g.cell[pa].centroid;
+    Vec3 e = l2r.norm();
+    const double l2rmag = fabs(l2r);
+    {
+      S d = vdot(fgk, e);
+      fgk = vsub(fgk, vscale(d, e));
+      fgk = vadd(fgk, vscale((kR - kL) / l2rmag, e));
+      S d2 = vdot(fgo, e);
+      fgo = vsub(fgo, vscale(d2, e));
+      fgo = vadd(fgo, vscale((oR - oL) / l2rmag, e));
+    }
+    const double A = g.face[f].area;
+    S conv[2], diff[2];
+    conv[0] = md * (wL * kL + wR * kR) * A;
+    conv[1] = md * (wL * oL + wR * oR) * A;
+    diff[0] = (lam + turb * KW::sigma_k) * vdot(fgk, g.face[f].normal) * A;
+    diff[1] = (lam + turb * KW::sigma_omega) * vdot(fgo, g.face[f].normal) * A;
+    for (int i = 0; i < 2; ++i) {
+      S value = diff[i] - conv[i];
+      rhs_k[(size_t)pa * 2 + i] += value;
+      if (b < 0) { value = value * -1.; rhs_k[(size_t)nb * 2 + i] += value; }
+    }
+  }
+  for (int c = 0; c < g.cellCount; ++c) {
+    const V3<S> &gu = F.gradu[c], &gv = F.gradv[c], &gw = F.gradw[c];
+    const S dudx = gu[0], dudy = gu[1], dudz = gu[2], dvdx = gv[0], dvdy = gv[1], dvdz = gv[2];
+    const S dwdx = gw[0], dwdy = gw[1], dwdz = gw[2];
+    const S divU = dudx + dvdy + dwdz;
+    const S sr = sqrt(2. * (dudx * dudx + dvdy * dvdy + dwdz * dwdz) + (dudy + dvdx) * (dudy + dvdx) +
+                      (dudz + dwdx) * (dudz + dwdx) + (dvdz + dwdy) * (dvdz + dwdy));
+    S Prod = mut[c] * (sr * sr - 2. / 3. * divU * divU) - 2. / 3. * F.rho[c] * K[c] * divU;
+    const S Dest = KW::beta_star * F.rho[c] * Om[c] * K[c];
+    Prod = smin(Prod, S(10. * Dest));
+    S src0 = Prod;
+    src0 -= Dest;
+    S src1 = KW::alpha * F.rho[c] / mut[c] * Prod;
+    src1 -= KW::beta * F.rho[c] * Om[c] * Om[c];
+    const double vol = g.cell[c].volume;
+    rhs_k[(size_t)c * 2] += src0 * vol;
+    rhs_k[(size_t)c * 2 + 1] += src1 * vol;
+  }
+}
+
 // time_step.cc:143-224 (CFL_LOCAL / CFL_MAX step sizes for one time level)
 static void local_dt(Oracle &O, const double *W, double cfl, int mode, double *dt) {
   Grid &g = O.grid;
@@ -1666,6 +1836,7 @@ void *orc_create(const char *deck_path, int n_nodes, const double *xyz, int n_ce
     face_interpolation_weights(O);
     gradient_maps(O);
     H->F.alloc(g.cell.size(), (size_t)g.faceCount);
+    setup_rans(O);
   } catch (const std::exception &e) {
     if (err && errlen > 0) { std::snprintf(err, errlen, "%s", e.what()); }
     return nullptr;
@@ -1811,6 +1982,42 @@ int orc_residual_cstep(void *h, const double *W, const double *dW, double hstep,
     return 1;
   }
   return 0;
+}
+
+// RANS k-omega residual: R[nc][5] (NS with eddy viscosity) and RK[nc][2]
+// for the state W[nc][5], K[nc][2] = (k, omega).
+int orc_rans_residual(void *h, const double *W, const double *Kin, double *R, double *RK, char *err, int errlen) {
+  Handle *H = static_cast<Handle *>(h);
+  Oracle &O = H->O;
+  Grid &g = O.grid;
+  Fields<double> &F = H->F;
+  try {
+    if (!O.turbulent) throw DeckError("the deck has no turbulence section");
+    for (int c = 0; c < g.cellCount; ++c) {
+      F.p[c] = W[5 * c]; F.V[c] = V3<double>(W[5 * c + 1], W[5 * c + 2], W[5 * c + 3]); F.T[c] = W[5 * c + 4];
+      F.rho[c] = O.material.rho(F.p[c], F.T[c]);
+    }
+    for (int i = 0; i < 5; ++i)
+      for (size_t c = 0; c < g.cell.size(); ++c) F.limiter[i][c] = (O.order == FIRST) ? 0. : 1.;
+    std::vector<double> k(g.cellCount), om(g.cellCount), rns, rk;
+    for (int c = 0; c < g.cellCount; ++c) { k[c] = Kin[2 * c]; om[c] = Kin[2 * c + 1]; }
+    rans_residual(O, F, k, om, rns, rk);
+    std::memcpy(R, rns.data(), sizeof(double) * rns.size());
+    std::memcpy(RK, rk.data(), sizeof(double) * rk.size());
+  } catch (const std::exception &e) {
+    if (err && errlen > 0) std::snprintf(err, errlen, "%s", e.what());
+    return 1;
+  }
+  return 0;
+}
+
+// Fixed BC values of the RANS variables: per BC [kw_fixed, k, omega, mut_fixed, mu_t].
+void orc_rans_bcs(void *h, double *out) {
+  Oracle &O = static_cast<Handle *>(h)->O;
+  for (size_t b = 0; b < O.kw_fixed.size(); ++b) {
+    out[5 * b] = O.kw_fixed[b]; out[5 * b + 1] = O.k_bc[b]; out[5 * b + 2] = O.omega_bc[b];
+    out[5 * b + 3] = O.mut_fixed[b]; out[5 * b + 4] = O.mut_bc[b];
+  }
 }
 
 // Boundary loads: force[bcCount][3] for state W, and (dW non-null) their

@@ -129,3 +129,18 @@ def test_complex_step_matches_finite_difference(flux, oracle_mod):
     cols = [0, 1, 2, 4]  # w stays identically zero in this 2-D case
     scale = np.abs(jv[:, cols]).max(axis=0)
     assert (np.abs(jv - fd)[:, cols].max(axis=0) / scale).max() < 1e-5
+
+
+def test_oracle_rans_inlet_values(oracle_mod):
+    """RANS::set_bcs inlet values (rans_set_bcs.cc:56-65): k = max(kLow,
+    1.5 (I |V|)^2), omega = rho k / (ratio mu(T)), mu_t = ratio mu(T), with the
+    flat plate's freestream (I = 1e-3, ratio 1); no-slip wall mu_t = 0."""
+    import tempfile
+    from freecfd_b200 import cases
+    case = cases.plate_case(ni=8, nj=4, nk=2, turbulent=True)
+    o = oracle_mod.Oracle(case, tempfile.mkdtemp())
+    bcs = o.rans_bcs()
+    k, omega = case.kfree
+    assert bcs[0, 0] == 1 and abs(bcs[0, 1] - k) <= 1e-14 * k and abs(bcs[0, 2] - omega) <= 1e-12 * omega
+    assert bcs[2, 3] == 1 and bcs[2, 4] == 0.0          # wall
+    assert bcs[1, 0] == 0 and bcs[3, 0] == 0             # outlet, symmetry: extrapolated
