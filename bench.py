@@ -37,6 +37,8 @@ WORKLOADS = {
     "hypersonic": dict(fn="hypersonic_case", kw={}),
     "plate": dict(fn="plate_case", kw=dict(turbulent=False)),
     "plate64": dict(fn="plate_case", kw=dict(nk=64, turbulent=False)),
+    "plate_rans": dict(fn="plate_case", kw=dict(turbulent=True)),
+    "plate64_rans": dict(fn="plate_case", kw=dict(nk=64, turbulent=True)),
 }
 METRIC = "M faces/s residual + % HBM peak; Newton wall time to 1e-10: mixed+JVP vs plain FP64"
 UNIT = "M faces/s"
@@ -139,10 +141,16 @@ def cpu_baseline(case, seconds=12.0):
     """Single-core oracle (restatement of the reference's CPU residual)."""
     import oracle
     o = oracle.Oracle(case)
-    o.residual(case.state)
+    if case.kstate is not None:
+        def step():
+            o.rans_residual(case.state, case.kstate)
+    else:
+        def step():
+            o.residual(case.state)
+    step()
     n, t0 = 0, time.perf_counter()
     while True:
-        o.residual(case.state)
+        step()
         n += 1
         el = time.perf_counter() - t0
         if el > seconds or n >= 200:
@@ -159,12 +167,18 @@ def _ref_worker(args):
     import oracle
     case = make_case(name)
     o = oracle.Oracle(case)
+    if case.kstate is not None:
+        def step():
+            o.rans_residual(case.state, case.kstate)
+    else:
+        def step():
+            o.residual(case.state)
     for _ in range(warmup):
-        o.residual(case.state)
+        step()
     q.put(("ready", os.getpid()))
     t0 = time.perf_counter()
     for _ in range(steps):
-        o.residual(case.state)
+        step()
     el = time.perf_counter() - t0
     q.put(("done", el, o.nf))
 
@@ -225,16 +239,25 @@ def run_ours(args):
     mesh = fb.Mesh(case.mesh, cs)
     ns = fb.NavierStokes(mesh, cs, dev)
     W = np.ascontiguousarray(case.state)
-    ns.residual(W)                               # upload + first evaluation (also checks BC errors)
-    ns.time_residual(max(args.warmup, 1), True)  # warm-up steps
+    rans = case.kstate is not None
+    K = np.ascontiguousarray(case.kstate) if rans else None
+    if rans:
+        ns.rans_residual(W, K)                   # upload + first coupled evaluation
+        ns.time_rans(max(args.warmup, 1), True)
+    else:
+        ns.residual(W)                           # upload + first evaluation (also checks BC errors)
+        ns.time_residual(max(args.warmup, 1), True)  # warm-up steps
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
     with Clocks(dev) as clk:
-        t = ns.time_residual(args.steps, True)
+        t = ns.time_rans(args.steps, True) if rans else ns.time_residual(args.steps, True)
     torch.cuda.synchronize()
     ms = float(t[0])
-    kern = {"ghost_minmax": t[1], "grad_limiter": t[2], "outlet_density": t[3], "face_flux": t[4], "gather": t[5]}
+    if rans:
+        kern = {"ns_part_with_eddy_viscosity": t[1], "komega_part": t[2]}
+    else:
+        kern = {"ghost_minmax": t[1], "grad_limiter": t[2], "outlet_density": t[3], "face_flux": t[4], "gather": t[5]}
     if dist:
         x = torch.tensor([ms], device="cuda", dtype=torch.float64)
         dist.all_reduce(x, op=dist.ReduceOp.MAX)
@@ -245,13 +268,14 @@ def run_ours(args):
     Rp = torch.empty((mesh.nc, 5), dtype=torch.float64, pin_memory=True)
     Wp.numpy()[:] = W
     Wn, Rn = Wp.numpy(), Rp.numpy()
+    call = (lambda: ns.rans_residual(Wn, K)) if rans else (lambda: ns.residual(Wn, Rn))
     for _ in range(max(args.warmup, 1)):
-        ns.residual(Wn, Rn)
+        call()
     if dist:
         dist.barrier()
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        ns.residual(Wn, Rn)
+        call()
     e2e_s = (time.perf_counter() - t0) / args.steps
     if dist:
         x = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
@@ -263,11 +287,20 @@ def run_ours(args):
     achieved = B / (ms * 1e-3) / 1e9
     n_kernels = 4 + (1 if ns_has_outlet(case) else 0)
     # dominant kernel: its own algorithmic bytes over its event-timed duration
-    viscous = args.workload in ("cylinder", "plate", "plate64")          # laminar / viscous materials
+    viscous = args.workload in ("cylinder", "plate", "plate64", "plate_rans", "plate64_rans")  # viscous materials
     exact_grad = "limiter=minmod" in case.deck or "limiter=bj" in case.deck
-    top = max(("grad_limiter", "face_flux", "gather", "ghost_minmax"), key=lambda k: kern[k])
-    kb = kernel_bytes(mesh, top, viscous, exact_grad)
-    k_ach = kb / (float(kern[top]) * 1e-3) / 1e9
+    if rans:
+        # coupled step: flow arrays plus k, omega (read with ghosts), their
+        # residual, the eddy viscosity per cell and face
+        top = "rans_step"
+        kb = B + mesh.nc * 2 * 8 * 2 + (mesh.nc + mesh.nghost) * 8 + mesh.nf * 8
+        k_ms = ms
+        n_kernels = 11
+    else:
+        top = max(("grad_limiter", "face_flux", "gather", "ghost_minmax"), key=lambda k: kern[k])
+        kb = kernel_bytes(mesh, top, viscous, exact_grad)
+        k_ms = float(kern[top])
+    k_ach = kb / (k_ms * 1e-3) / 1e9
     traffic = NCU_TRAFFIC.get((args.workload, top))
     line = {"metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms, 5), "higher_is_better": True, "scaling": "weak",
@@ -275,17 +308,18 @@ def run_ours(args):
             "config": {"workload": case.workload, "cells": mesh.nc, "faces": mesh.nf, "ghosts": mesh.nghost,
                        "stencil_entries": mesh.n_grad_entries, "l2": "flushed (512 MB memset before every step)",
                        "parallelism": f"replicas x{world}"},
-            "e2e": {"value": round(e2e, 3), "unit": UNIT, "h2d_bytes_per_step": int(W.nbytes),
-                    "d2h_bytes_per_step": int(W.nbytes)},
+            "e2e": {"value": round(e2e, 3), "unit": UNIT,
+                    "h2d_bytes_per_step": int(W.nbytes + (K.nbytes if rans else 0)),
+                    "d2h_bytes_per_step": int(W.nbytes + (K.nbytes if rans else 0))},
             "roofline": {"bound": "hbm", "achieved": round(k_ach, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(k_ach / peak, 4), "traffic": traffic, "peak_kind": kind, "kernel": top,
-                         "alg_bytes_per_launch": int(kb), "ms_per_launch": round(float(kern[top]), 5)},
+                         "alg_bytes_per_launch": int(kb), "ms_per_launch": round(k_ms, 5)},
             "step_roofline": {"achieved": round(achieved, 1), "frac": round(achieved / peak, 4), "alg_bytes": int(B),
                               "unit_of_work": "one residual evaluation (all kernels)"},
             "kernels_ms": {k: round(float(v), 5) for k, v in kern.items()},
             "gpu_launches": n_kernels * args.steps,
             "clocks": clk.summary()}
-    if not args.no_newton:
+    if not args.no_newton and not rans:
         line["newton"] = run_newton(fb, cs, mesh, case, dev, dist)
     if rank == 0 and world == 1 and not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline(case, args.cpu_seconds)

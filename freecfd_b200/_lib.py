@@ -25,7 +25,7 @@ EXPORTED = [
     "fcfd_mesh_create", "fcfd_mesh_destroy", "fcfd_mesh_sizes", "fcfd_mesh_connectivity", "fcfd_mesh_geometry",
     "fcfd_mesh_lsq",
     "fcfd_ctx_create", "fcfd_ctx_destroy", "fcfd_ctx_set_exact_gradients", "fcfd_residual", "fcfd_last_stages", "fcfd_local_dt",
-    "fcfd_time_residual", "fcfd_point_flux", "fcfd_jvp", "fcfd_vjp", "fcfd_drag", "fcfd_rans_residual", "fcfd_rans_bcs", "fcfd_newton_solve", "fcfd_local_dt_cflmax_noalloc",
+    "fcfd_time_residual", "fcfd_point_flux", "fcfd_jvp", "fcfd_vjp", "fcfd_drag", "fcfd_rans_residual", "fcfd_rans_bcs", "fcfd_time_rans", "fcfd_newton_solve", "fcfd_local_dt_cflmax_noalloc",
 ]
 
 
@@ -96,6 +96,7 @@ def _load():
     L.fcfd_vjp.argtypes = [vp, vp, vp, vp, ctypes.c_int]
     L.fcfd_rans_residual.argtypes = [vp, vp, vp, vp, vp, ctypes.c_int]
     L.fcfd_rans_bcs.argtypes = [vp, vp, ctypes.c_int32]
+    L.fcfd_time_rans.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp, ctypes.c_int]
     L.fcfd_drag.argtypes = [vp, vp, ctypes.c_uint32, vp, vp, vp, ctypes.c_int]
     L.fcfd_newton_solve.argtypes = [vp, dp, ctypes.POINTER(NewtonOpts), ctypes.POINTER(NewtonReport)]
     L.fcfd_local_dt_cflmax_noalloc.argtypes = [vp, vp, ctypes.c_int32, ctypes.c_double, ctypes.c_double,

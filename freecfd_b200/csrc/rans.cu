@@ -247,7 +247,9 @@ void rans_setup(fcfd_ctx *x) {
 }
 
 // One coupled evaluation; W and K already in p64.W / rans->K (interior parts).
-static void rans_chain(fcfd_ctx *x, double *R_aos, double *RK_aos) {
+// With ev (3 events), ev[1] is recorded after the NS part (its gather) and
+// ev[2] after the k-omega part.
+static void rans_chain(fcfd_ctx *x, double *R_aos, double *RK_aos, cudaEvent_t *ev = nullptr) {
   const DevMesh &m = x->dm;
   cudaStream_t st = x->stream;
   RansState &s = *x->rans;
@@ -264,9 +266,11 @@ static void rans_chain(fcfd_ctx *x, double *R_aos, double *RK_aos) {
   k_face_flux<double, true><<<(m.nf + 127) / 128, 128, 0, st>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p, s.mutf.p, P.D.p,
                                                                 x->mdot.p, x->wl.p, x->err.p);
   k_gather<double, true><<<(m.nc + tb - 1) / tb, tb, 0, st>>>(m, P.D.p, R_aos, x->ext.p, x->argx.p);
+  if (ev) CK(cudaEventRecord(ev[1], st));
   k_rans_grad<<<(m.nc + 127) / 128, 128, 0, st>>>(m, s.K.p, s.GK.p);
   k_rans_face<<<(m.nf + 127) / 128, 128, 0, st>>>(x->cs, m, P.W.p, s.K.p, s.GK.p, s.mutf.p, x->mdot.p, x->wl.p, s.DK.p);
   k_rans_gather<<<(m.nc + 127) / 128, 128, 0, st>>>(x->cs, m, P.W.p, s.K.p, P.G.p, s.mut.p, s.vol.p, s.DK.p, RK_aos);
+  if (ev) CK(cudaEventRecord(ev[2], st));
   CK(cudaGetLastError());
 }
 
@@ -302,6 +306,40 @@ extern "C" int fcfd_rans_residual(fcfd_ctx *x, const double *W, const double *K,
     }
     CK(cudaStreamSynchronize(s));
     check_err(x);
+  } catch (const Error &e) {
+    set_last_error(e.what());
+    return e.code;
+  } catch (const std::exception &e) {
+    set_last_error(e.what());
+    return FCFD_ERR_INPUT;
+  }
+  return FCFD_OK;
+}
+
+// Device time of the coupled NS + k-omega residual on the state last passed
+// to fcfd_rans_residual: out[0] total ms per evaluation, out[1] the NS part
+// (with the eddy viscosity), out[2] the k-omega part; L2 flushed before each
+// evaluation when flush_l2 is set.
+extern "C" int fcfd_time_rans(fcfd_ctx *x, int reps, int flush_l2, double *out, int out_len) {
+  try {
+    if (!x || !out || reps < 1) throw Error(FCFD_ERR_INPUT, "bad argument");
+    if (!x->rans) throw Error(FCFD_ERR_INPUT, "the case has no turbulence model");
+    CK(cudaSetDevice(x->device));
+    cudaStream_t s = x->stream;
+    if (flush_l2 && x->flush.n == 0) x->flush.alloc((size_t)512 << 20);
+    Timing t;
+    double acc[3] = {0., 0., 0.};
+    for (int r = 0; r < reps; ++r) {
+      if (flush_l2) CK(cudaMemsetAsync(x->flush.p, r & 0xff, x->flush.n, s));
+      CK(cudaEventRecord(t.ev[0], s));
+      rans_chain(x, x->p64.R.p, x->rans->RK.p, t.ev);
+      CK(cudaEventSynchronize(t.ev[2]));
+      float ms;
+      CK(cudaEventElapsedTime(&ms, t.ev[0], t.ev[2])); acc[0] += ms;
+      CK(cudaEventElapsedTime(&ms, t.ev[0], t.ev[1])); acc[1] += ms;
+      CK(cudaEventElapsedTime(&ms, t.ev[1], t.ev[2])); acc[2] += ms;
+    }
+    for (int k = 0; k < 3 && k < out_len; ++k) out[k] = acc[k] / reps;
   } catch (const Error &e) {
     set_last_error(e.what());
     return e.code;

@@ -174,6 +174,12 @@ class NavierStokes:
         check(lib.fcfd_rans_residual(self.h, _d(W), _d(K), _d(R), _d(RK), 0))
         return R, RK
 
+    def time_rans(self, reps: int = 50, flush_l2: bool = True):
+        """[total, NS part, k-omega part] ms per coupled residual (device events)."""
+        out = np.zeros(3)
+        check(lib.fcfd_time_rans(self.h, int(reps), int(bool(flush_l2)), _d(out), out.size))
+        return out
+
     def rans_bcs(self):
         """Per BC region: kw_fixed, k, omega, mut_fixed, mu_t."""
         nbc = int(self.case.summary()[1][5]) if hasattr(self.case, "summary") else 16

@@ -152,6 +152,12 @@ int fcfd_vjp(fcfd_ctx *ctx, const double *W, const double *Rbar, double *Wbar, i
  * rans_set_bcs.cc:25-83.  Only model=k-omega; FCFD_ERR_INPUT if the case has
  * no turbulence section. */
 int fcfd_rans_residual(fcfd_ctx *ctx, const double *W, const double *K, double *R, double *RK, int flags);
+/* Device time (CUDA events) of the coupled NS + k-omega residual on the
+ * state of the last fcfd_rans_residual call: out[0] ms per evaluation,
+ * out[1] the NS part, out[2] the k-omega part; the L2 cache is flushed before
+ * each evaluation when flush_l2 != 0.  Benchmark entry point, no counterpart
+ * in the reference. */
+int fcfd_time_rans(fcfd_ctx *ctx, int reps, int flush_l2, double *out, int out_len);
 /* Fixed BC values of the RANS variables, per BC region: kw_fixed, k, omega,
  * mut_fixed, mu_t (5 doubles each; out_len >= 5 * number of regions). */
 int fcfd_rans_bcs(const fcfd_ctx *ctx, double *out, int32_t out_len);
