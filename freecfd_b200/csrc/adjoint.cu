@@ -659,7 +659,7 @@ static void run_adjoint(fcfd_ctx *x, const double *Rbar_soa, unsigned int mask, 
   const int ng = (m.nb + tb - 1) / tb + (need_ext ? kExtremaBlocks : 0);
   if (ng > 0) k_ghost_minmax<double><<<ng, tb, 0, s>>>(x->cs, m, P.W.p, need_ext ? x->ext.p : nullptr, x->err.p);
   if (need_ext) k_argext<double><<<(m.nc + tb - 1) / tb, tb, 0, s>>>(m, P.W.p, x->ext.p, x->argx.p);
-  k_grad_limiter<double><<<(m.nc + 127) / 128, 128, 0, s>>>(x->cs, m, P.W.p, x->ext.p, nullptr, P.G.p, P.Lm.p);
+  launch_grad_limiter<double>(x->cs, m, P.W.p, x->ext.p, nullptr, P.G.p, P.Lm.p, s);
   if (m.n_outlet > 0)
     k_outlet_rho<double><<<(m.n_outlet + 127) / 128, 128, 0, s>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p);
   // reverse

@@ -118,6 +118,17 @@ constexpr int kExtremaBlocks = 296;  // 2 x 148 SMs
 template <class S>
 void launch_chain(fcfd_ctx *x, Pipe<S> &P, S *Rout, bool aos_out, S *mo, S *wo, bool frozen_limiter = false);
 int check_err(fcfd_ctx *x);
+
+// Gradient + limiter launch: the fused-gradient and bit-exact instantiations
+// are separate kernels so each gets the registers its own path needs.
+template <class S>
+inline void launch_grad_limiter(const DevCase &cs, const DevMesh &m, const S *W, const unsigned long long *ext,
+                                const int *argx, S *G, S *Lm, cudaStream_t s) {
+  if (cs.fast_grad)
+    k_grad_limiter<S, true><<<(m.nc + 127) / 128, 128, 0, s>>>(cs, m, W, ext, argx, G, Lm);
+  else
+    k_grad_limiter<S, false><<<(m.nc + 127) / 128, 128, 0, s>>>(cs, m, W, ext, argx, G, Lm);
+}
 void adjoint_free(fcfd_ctx *x);
 void rans_setup(fcfd_ctx *x);
 void rans_free(fcfd_ctx *x);

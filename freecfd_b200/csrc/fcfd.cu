@@ -41,7 +41,7 @@ void launch_chain(fcfd_ctx *x, Pipe<S> &P, S *Rout, bool aos_out, S *mo, S *wo, 
     k_argext<S><<<(m.nc + tb - 1) / tb, tb, 0, s>>>(m, P.W.p, x->ext.p, x->argx.p);
     argx = x->argx.p;
   }
-  k_grad_limiter<S><<<(m.nc + 127) / 128, 128, 0, s>>>(csl, m, P.W.p, x->ext.p, argx, P.G.p, P.Lm.p);
+  launch_grad_limiter<S>(csl, m, P.W.p, x->ext.p, argx, P.G.p, P.Lm.p, s);
   if (m.n_outlet > 0)
     k_outlet_rho<S><<<(m.n_outlet + 127) / 128, 128, 0, s>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p);
   if (x->viscous)
@@ -390,7 +390,7 @@ int fcfd_time_residual(fcfd_ctx *x, int reps, int flush_l2, double *out, int out
     Pipe<double> &P = x->p64;
     if (ng > 0) k_ghost_minmax<double><<<ng, tb, 0, s>>>(x->cs, m, P.W.p, need_ext ? x->ext.p : nullptr, x->err.p);
     CK(cudaEventRecord(t.ev[1], s));
-    k_grad_limiter<double><<<(m.nc + 127) / 128, 128, 0, s>>>(x->cs, m, P.W.p, x->ext.p, nullptr, P.G.p, P.Lm.p);
+    launch_grad_limiter<double>(x->cs, m, P.W.p, x->ext.p, nullptr, P.G.p, P.Lm.p, s);
     CK(cudaEventRecord(t.ev[2], s));
     if (m.n_outlet > 0)
       k_outlet_rho<double><<<(m.n_outlet + 127) / 128, 128, 0, s>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p);

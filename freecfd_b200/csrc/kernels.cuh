@@ -14,6 +14,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <type_traits>
+
 namespace fcfd {
 
 // ------------------------------------------------------------------ scalar ops
@@ -458,8 +460,10 @@ __global__ void k_split_dual(const Dual<T> *__restrict__ R, double *__restrict__
 
 // LSQ gradient (bit-exact restatement of Variable::cell_gradient over the
 // lsqr_grad_map weights) + limiter, one thread per interior cell.
-template <class S>
-__global__ void __launch_bounds__(128) k_grad_limiter(DevCase cs, DevMesh m, const S *__restrict__ W,
+// The FP64 bit-exact instantiation runs at six blocks per SM (register cap),
+// measured 8 % faster on the prism mesh; the others keep their registers.
+template <class S, bool FAST>
+__global__ void __launch_bounds__(128, (!FAST && std::is_same<S, double>::value) ? 6 : 1) k_grad_limiter(DevCase cs, DevMesh m, const S *__restrict__ W,
                                                       const unsigned long long *__restrict__ ext, const int *__restrict__ argx,
                                                       S *__restrict__ G, S *__restrict__ Lm) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
@@ -473,7 +477,7 @@ __global__ void __launch_bounds__(128) k_grad_limiter(DevCase cs, DevMesh m, con
 #pragma unroll
   for (int i = 0; i < 15; ++i) g[i] = S(0.);
   const int j0 = m.st_index[c], j1 = m.st_index[c + 1];
-  if (cs.fast_grad) {
+  if (FAST) {
     // Continuous limiters only (VK with K > 0, none, first order): the same
     // weighted least-squares gradient in the compact form
     //   grad = C . sum_k w_k d_k (phi_k - phi_c) / det - mirror * phi_c

@@ -260,7 +260,7 @@ static void rans_chain(fcfd_ctx *x, double *R_aos, double *RK_aos, cudaEvent_t *
   if (ng > 0) k_ghost_minmax<double><<<ng, tb, 0, st>>>(x->cs, m, P.W.p, need_ext ? x->ext.p : nullptr, x->err.p);
   k_rans_prep<<<(m.nt + 127) / 128, 128, 0, st>>>(x->cs, m, P.W.p, s.K.p, s.mut.p, x->case_ptr->visc_ratio_limit);
   k_rans_mutf<<<(m.nf + 127) / 128, 128, 0, st>>>(x->cs, m, s.mut.p, s.mutf.p);
-  k_grad_limiter<double><<<(m.nc + 127) / 128, 128, 0, st>>>(x->cs, m, P.W.p, x->ext.p, nullptr, P.G.p, P.Lm.p);
+  launch_grad_limiter<double>(x->cs, m, P.W.p, x->ext.p, nullptr, P.G.p, P.Lm.p, st);
   if (m.n_outlet > 0)
     k_outlet_rho<double><<<(m.n_outlet + 127) / 128, 128, 0, st>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p);
   k_face_flux<double, true><<<(m.nf + 127) / 128, 128, 0, st>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p, s.mutf.p, P.D.p,
