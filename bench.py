@@ -338,14 +338,14 @@ NEWTON_KW = dict(tol=1e-10, max_newton=400, cfl0=2.0, cfl_max=1e6, krylov_rtol=1
 def run_newton(fb, cs, mesh, case, dev, dist):
     """Steady solve from the seeded state until |R_mass|/|R_mass0| <= 1e-10:
     plain FP64 (finite-difference J.v, FP64 Krylov) against mixed (tangent
-    J.v kernels, FP32 Krylov basis and preconditioner application, FP64 outer
-    residual).  Wall time of the whole call (host state in, host state out);
+    J.v kernels evaluated in FP32, FP32 Krylov basis, FP32 Gauss-Seidel
+    preconditioner; FP64 outer residual, dot products and Gram-Schmidt).  Wall time of the whole call (host state in, host state out);
     replicas under torchrun, max over ranks."""
     import torch
     out = {}
     states = {}
     variants = (("plain_fp64_fd", dict(jvp=False)),
-                ("mixed_jvp_fp32", dict(jvp=True, exact_jvp=True, fp32_krylov=True)))
+                ("mixed_jvp_fp32", dict(jvp=True, fp32_jvp=True, fp32_krylov=True)))
     for label, opts in variants:
         ns = fb.NavierStokes(mesh, cs, dev)
         ns.newton_solve(case.state, **dict(NEWTON_KW, max_newton=2), raise_on_fail=False, **opts)  # warm-up

@@ -100,6 +100,7 @@ struct fcfd_ctx {
   // state arrays
   Pipe<double> p64;
   Pipe<Dual<double>> pjv;
+  Pipe<Dual<float>> pjv32;  // FP32 tangent chain (mixed-precision Newton-Krylov)
   DBuf<double> Win, Vin, Rtmp, dt, mdot, wl;
   AdjointState *adj = nullptr;
   RansState *rans = nullptr;
@@ -110,6 +111,7 @@ struct fcfd_ctx {
   int n_outlet = 0;
   cudaGraphExec_t graph = nullptr;
   bool newton_frozen = false;
+  bool newton_f32 = false;  // Krylov matvecs through the FP32 tangent chain
 };
 
 

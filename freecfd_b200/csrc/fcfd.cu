@@ -17,6 +17,7 @@ namespace fcfd {
 // defined in ghost.cu (compiled with -fmad=false)
 extern template __global__ void k_ghost_minmax<double>(DevCase, DevMesh, double *, unsigned long long *, int *);
 extern template __global__ void k_ghost_minmax<Dual<double>>(DevCase, DevMesh, Dual<double> *, unsigned long long *, int *);
+extern template __global__ void k_ghost_minmax<Dual<float>>(DevCase, DevMesh, Dual<float> *, unsigned long long *, int *);
 
 fcfd_case *read_deck(const std::string &path);
 fcfd_mesh *build_mesh(const fcfd_raw_mesh &raw, fcfd_case &cs);
@@ -69,6 +70,7 @@ int check_err(fcfd_ctx *x) {
 
 template void launch_chain<double>(fcfd_ctx *, Pipe<double> &, double *, bool, double *, double *, bool);
 template void launch_chain<Dual<double>>(fcfd_ctx *, Pipe<Dual<double>> &, Dual<double> *, bool, Dual<double> *, Dual<double> *, bool);
+template void launch_chain<Dual<float>>(fcfd_ctx *, Pipe<Dual<float>> &, Dual<float> *, bool, Dual<float> *, Dual<float> *, bool);
 
 }  // namespace fcfd
 
@@ -429,19 +431,27 @@ int fcfd_jvp(fcfd_ctx *x, const double *W, const double *V, double *R, double *J
   if (!x || !W || !V || !JV) throw Error(FCFD_ERR_INPUT, "null argument");
   CK(cudaSetDevice(x->device));
   const DevMesh &m = x->dm;
-  if (!x->pjv.ready) x->pjv.alloc(m.nc, m.nf, m.nb);
   const bool dev = flags & FCFD_DEVICE_PTRS;
+  const bool f32 = flags & FCFD_JVP_FP32;
+  if (!f32 && !x->pjv.ready) x->pjv.alloc(m.nc, m.nf, m.nb);
+  if (f32 && !x->pjv32.ready) x->pjv32.alloc(m.nc, m.nf, m.nb);
   const double *w = W, *v = V;
   if (!dev) {
     CK(cudaMemcpyAsync(x->Win.p, W, sizeof(double) * 5 * m.nc, cudaMemcpyHostToDevice, x->stream));
     CK(cudaMemcpyAsync(x->Vin.p, V, sizeof(double) * 5 * m.nc, cudaMemcpyHostToDevice, x->stream));
     w = x->Win.p; v = x->Vin.p;
   }
-  k_seed_dual<double><<<(m.nc + 255) / 256, 256, 0, x->stream>>>(w, v, x->pjv.W.p, m.nc, m.nt);
-  launch_chain<Dual<double>>(x, x->pjv, x->pjv.R.p, false, nullptr, nullptr);
   double *rout = R ? (dev ? R : x->Rtmp.p) : nullptr;
   double *jout = dev ? JV : x->Vin.p;
-  k_split_dual<double><<<(m.nc + 255) / 256, 256, 0, x->stream>>>(x->pjv.R.p, rout, jout, m.nc);
+  if (f32) {
+    k_seed_dual<float><<<(m.nc + 255) / 256, 256, 0, x->stream>>>(w, v, x->pjv32.W.p, m.nc, m.nt);
+    launch_chain<Dual<float>>(x, x->pjv32, x->pjv32.R.p, false, nullptr, nullptr);
+    k_split_dual<float><<<(m.nc + 255) / 256, 256, 0, x->stream>>>(x->pjv32.R.p, rout, jout, m.nc);
+  } else {
+    k_seed_dual<double><<<(m.nc + 255) / 256, 256, 0, x->stream>>>(w, v, x->pjv.W.p, m.nc, m.nt);
+    launch_chain<Dual<double>>(x, x->pjv, x->pjv.R.p, false, nullptr, nullptr);
+    k_split_dual<double><<<(m.nc + 255) / 256, 256, 0, x->stream>>>(x->pjv.R.p, rout, jout, m.nc);
+  }
   CK(cudaGetLastError());
   if (!dev) {
     if (R) CK(cudaMemcpyAsync(R, x->Rtmp.p, sizeof(double) * 5 * m.nc, cudaMemcpyDeviceToHost, x->stream));

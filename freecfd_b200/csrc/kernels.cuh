@@ -98,6 +98,13 @@ __device__ __forceinline__ Dual<double> div_rn(Dual<double> a, Dual<double> b) {
   const double q = __ddiv_rn(a.v, b.v);
   return Dual<double>(q, (a.d - q * b.d) / b.v);
 }
+__device__ __forceinline__ Dual<float> mul_rn(Dual<float> a, Dual<float> b) { return Dual<float>(__fmul_rn(a.v, b.v), a.d * b.v + a.v * b.d); }
+__device__ __forceinline__ Dual<float> add_rn(Dual<float> a, Dual<float> b) { return Dual<float>(__fadd_rn(a.v, b.v), a.d + b.d); }
+__device__ __forceinline__ Dual<float> sub_rn(Dual<float> a, Dual<float> b) { return Dual<float>(__fsub_rn(a.v, b.v), a.d - b.d); }
+__device__ __forceinline__ Dual<float> div_rn(Dual<float> a, Dual<float> b) {
+  const float q = __fdiv_rn(a.v, b.v);
+  return Dual<float>(q, (a.d - q * b.d) / b.v);
+}
 __host__ __device__ __forceinline__ double val(double x) { return x; }
 __host__ __device__ __forceinline__ float val(float x) { return x; }
 template <class T> __host__ __device__ __forceinline__ T val(const Dual<T> &x) { return x.v; }

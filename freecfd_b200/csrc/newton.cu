@@ -226,21 +226,22 @@ __global__ void k_jacobi_sweep(DevMesh m, const double *__restrict__ Minv, const
 // Pack one colour's couplings for the Gauss-Seidel kernel: the signed
 // off-diagonal blocks (slot-major [deg][25][cnt]) and the inverse diagonal
 // blocks ([25][cnt]), so that consecutive threads read consecutive words.
+template <class P>
 __global__ void k_pack_gs(int nc, int nf, int deg, int cnt, const int *__restrict__ cells, const int *__restrict__ nbr,
                           const int *__restrict__ src, const double *__restrict__ JL, const double *__restrict__ JR,
-                          const double *__restrict__ Minv, double *__restrict__ OB, double *__restrict__ MinvP) {
+                          const double *__restrict__ Minv, P *__restrict__ OB, P *__restrict__ MinvP) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= cnt) return;
   const int c = cells[i];
 #pragma unroll
-  for (int q = 0; q < 25; ++q) MinvP[(size_t)q * cnt + i] = Minv[(size_t)q * nc + c];
+  for (int q = 0; q < 25; ++q) MinvP[(size_t)q * cnt + i] = P(Minv[(size_t)q * nc + c]);
   for (int sl = 0; sl < deg; ++sl) {
     const int o = nbr[(size_t)sl * cnt + i], e = src[(size_t)sl * cnt + i];
     const int f = e >= 0 ? e : ~e;
     const double *J = e >= 0 ? JR : JL;
     const double sg = e >= 0 ? 1. : -1.;
 #pragma unroll
-    for (int q = 0; q < 25; ++q) OB[((size_t)sl * 25 + q) * cnt + i] = o >= 0 ? sg * J[(size_t)q * nf + f] : 0.;
+    for (int q = 0; q < 25; ++q) OB[((size_t)sl * 25 + q) * cnt + i] = P(o >= 0 ? sg * J[(size_t)q * nf + f] : 0.);
   }
 }
 
@@ -251,13 +252,14 @@ __global__ void k_pack_gs(int nc, int nf, int deg, int cnt, const int *__restric
 // the rows meet through warp shuffles for the diagonal solve.
 constexpr int kGsLanes = 8;
 constexpr int kGsMaxDeg = 6;  // interior faces per cell of hexes, prisms, tetrahedra
+template <class P>
 __global__ void k_gs_packed(int nc, int deg, int cnt, const int *__restrict__ cells, const int *__restrict__ nbr,
-                            const double *__restrict__ OB, const double *__restrict__ MinvP, const double *__restrict__ r,
-                            double *__restrict__ y) {
+                            const P *__restrict__ OB, const P *__restrict__ MinvP, const P *__restrict__ r,
+                            P *__restrict__ y) {
   const int gt = blockIdx.x * blockDim.x + threadIdx.x;
   const int i = gt / kGsLanes, q = gt % kGsLanes;
   const bool act = i < cnt && q < 5;
-  double t = 0.;
+  P t = P(0.);
   int c = 0;
   if (act) {
     c = cells[i];
@@ -268,16 +270,16 @@ __global__ void k_gs_packed(int nc, int deg, int cnt, const int *__restrict__ ce
       int o[kGsMaxDeg];
 #pragma unroll
       for (int sl = 0; sl < kGsMaxDeg; ++sl) o[sl] = sl < deg ? nbr[(size_t)sl * cnt + i] : -1;
-      double yv[kGsMaxDeg][5];
+      P yv[kGsMaxDeg][5];
 #pragma unroll
       for (int sl = 0; sl < kGsMaxDeg; ++sl)
 #pragma unroll
-        for (int k = 0; k < 5; ++k) yv[sl][k] = o[sl] >= 0 ? y[k * nc + o[sl]] : 0.;
+        for (int k = 0; k < 5; ++k) yv[sl][k] = o[sl] >= 0 ? y[k * nc + o[sl]] : P(0.);
 #pragma unroll
       for (int sl = 0; sl < kGsMaxDeg; ++sl) {
         if (o[sl] < 0) continue;
-        const double *B = OB + ((size_t)sl * 25 + 5 * q) * cnt + i;
-        double a = 0.;
+        const P *B = OB + ((size_t)sl * 25 + 5 * q) * cnt + i;
+        P a = P(0.);
 #pragma unroll
         for (int k = 0; k < 5; ++k) a += B[(size_t)k * cnt] * yv[sl][k];
         t += a;
@@ -286,8 +288,8 @@ __global__ void k_gs_packed(int nc, int deg, int cnt, const int *__restrict__ ce
       for (int sl = 0; sl < deg; ++sl) {
         const int o = nbr[(size_t)sl * cnt + i];
         if (o < 0) continue;
-        const double *B = OB + ((size_t)sl * 25 + 5 * q) * cnt + i;
-        double a = 0.;
+        const P *B = OB + ((size_t)sl * 25 + 5 * q) * cnt + i;
+        P a = P(0.);
 #pragma unroll
         for (int k = 0; k < 5; ++k) a += B[(size_t)k * cnt] * y[k * nc + o];
         t += a;
@@ -296,11 +298,11 @@ __global__ void k_gs_packed(int nc, int deg, int cnt, const int *__restrict__ ce
   }
   // every lane takes part in the shuffles (blockDim is a multiple of 32)
   const int lane0 = (threadIdx.x & 31) & ~(kGsLanes - 1);
-  double tk[5];
+  P tk[5];
 #pragma unroll
   for (int k = 0; k < 5; ++k) tk[k] = __shfl_sync(0xffffffffu, t, lane0 + k);
   if (act) {
-    double v = 0.;
+    P v = P(0.);
 #pragma unroll
     for (int k = 0; k < 5; ++k) v += MinvP[(size_t)(5 * q + k) * cnt + i] * tk[k];
     y[q * nc + c] = v;
@@ -324,20 +326,20 @@ __global__ void k_load_state(int nc, int nt, const double *__restrict__ Wn, cons
 #pragma unroll
   for (int v = 0; v < 5; ++v) W[v * nt + c] = Wn[v * nc + c] + (dir ? eps * double(dir[v * nc + c]) : 0.);
 }
-template <class T>
-__global__ void k_load_dual(int nc, int nt, const double *__restrict__ Wn, const T *__restrict__ dir, Dual<double> *__restrict__ W) {
+template <class T, class D>
+__global__ void k_load_dual(int nc, int nt, const double *__restrict__ Wn, const T *__restrict__ dir, Dual<D> *__restrict__ W) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= nc) return;
 #pragma unroll
-  for (int v = 0; v < 5; ++v) W[v * nt + c] = Dual<double>(Wn[v * nc + c], double(dir[v * nc + c]));
+  for (int v = 0; v < 5; ++v) W[v * nt + c] = Dual<D>(D(Wn[v * nc + c]), D(dir[v * nc + c]));
 }
 
 // y = (V P/dt) z - Jz, Jz from a finite difference (R1 - R0)/eps or a tangent run
-template <class T>
+template <class T, class D = double>
 __global__ void k_matvec_finish(DevCase cs, int nc, const double *__restrict__ Wn, const double *__restrict__ vol,
                                 const double *__restrict__ dt, const T *__restrict__ z, const double *__restrict__ R1,
                                 const double *__restrict__ R0, double eps_num, const double *__restrict__ zz,
-                                const Dual<double> *__restrict__ JV, T *__restrict__ y, RowScale rs) {
+                                const Dual<D> *__restrict__ JV, T *__restrict__ y, RowScale rs) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= nc) return;
   const double inv_eps = JV ? 0. : 1. / fd_eps(eps_num, zz);
@@ -352,7 +354,7 @@ __global__ void k_matvec_finish(DevCase cs, int nc, const double *__restrict__ W
     double a = 0.;
 #pragma unroll
     for (int k = 0; k < 5; ++k) a += P[5 * i + k] * zv[k];
-    const double jz = JV ? JV[i * nc + c].d : (R1[i * nc + c] - R0[i * nc + c]) * inv_eps;
+    const double jz = JV ? double(JV[i * nc + c].d) : (R1[i * nc + c] - R0[i * nc + c]) * inv_eps;
     y[i * nc + c] = T(rs.s[i] * (s * a - jz));
   }
 }
@@ -550,23 +552,26 @@ struct Krylov {
 struct NewtonState {
   DBuf<double> Wn, R0, R1, dt, vol, JL, JR, Minv, Pr, Py0, Py1, Xs, rowmag;
   DBuf<double> OB, MinvP;  // couplings packed per colour for the Gauss-Seidel sweeps
+  // FP32 copies for the mixed-precision preconditioner (fp32_krylov)
+  DBuf<float> OB32, MinvP32, Pr32, Py32;
+  bool prec32 = false;
   double wscale = 1.;  // |S^-1 W| (finite-difference step scale)
   RowScale winv;       // 1 / per-variable reference magnitudes
   int sweeps = 0, cycles = 1;
 };
-template <class T>
-__global__ void k_unscale(int nc, const T *__restrict__ v, RowScale rs, double *__restrict__ out) {
+template <class T, class P>
+__global__ void k_unscale(int nc, const T *__restrict__ v, RowScale rs, P *__restrict__ out) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= nc) return;
-  for (int k = 0; k < 5; ++k) out[k * nc + c] = double(v[k * nc + c]) / rs.s[k];
+  for (int k = 0; k < 5; ++k) out[k * nc + c] = P(double(v[k * nc + c]) / rs.s[k]);
 }
 template <class T>
 __global__ void k_axpy_to(int n, const double *__restrict__ b, const T *__restrict__ w, T *__restrict__ out) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) out[i] = T(b[i] - double(w[i]));
 }
-template <class T>
-__global__ void k_cast(int n, const double *__restrict__ a, T *__restrict__ b) {
+template <class T, class A = double>
+__global__ void k_cast(int n, const A *__restrict__ a, T *__restrict__ b) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) b[i] = T(a[i]);
 }
@@ -591,12 +596,22 @@ static void matvec(fcfd_ctx *x, NewtonState &ns, int mode, const T *z, T *y, con
     // reference magnitudes: eps = sqrt(eps_mach) (1 + |S^-1 W|) / |S^-1 z|
     const double eps_num = 1.4901161193847656e-08 * (1. + ns.wscale);
     eval_residual<T>(x, ns.Wn.p, ns.R1.p, z, eps_num, zz);
-    k_matvec_finish<T><<<gb, tb, 0, s>>>(x->cs, m.nc, ns.Wn.p, ns.vol.p, ns.dt.p, z, ns.R1.p, ns.R0.p, eps_num, zz, nullptr, y, rs);
+    k_matvec_finish<T, double><<<gb, tb, 0, s>>>(x->cs, m.nc, ns.Wn.p, ns.vol.p, ns.dt.p, z, ns.R1.p, ns.R0.p, eps_num, zz,
+                                                 (const Dual<double> *)nullptr, y, rs);
   } else {
-    if (!x->pjv.ready) x->pjv.alloc(m.nc, m.nf, m.nb);
-    k_load_dual<T><<<gb, tb, 0, s>>>(m.nc, m.nt, ns.Wn.p, z, x->pjv.W.p);
-    launch_chain<Dual<double>>(x, x->pjv, x->pjv.R.p, false, nullptr, nullptr, x->newton_frozen);
-    k_matvec_finish<T><<<gb, tb, 0, s>>>(x->cs, m.nc, ns.Wn.p, ns.vol.p, ns.dt.p, z, nullptr, nullptr, 0., nullptr, x->pjv.R.p, y, rs);
+    if (x->newton_f32) {
+      if (!x->pjv32.ready) x->pjv32.alloc(m.nc, m.nf, m.nb);
+      k_load_dual<T, float><<<gb, tb, 0, s>>>(m.nc, m.nt, ns.Wn.p, z, x->pjv32.W.p);
+      launch_chain<Dual<float>>(x, x->pjv32, x->pjv32.R.p, false, nullptr, nullptr, x->newton_frozen);
+      k_matvec_finish<T, float><<<gb, tb, 0, s>>>(x->cs, m.nc, ns.Wn.p, ns.vol.p, ns.dt.p, z, nullptr, nullptr, 0., nullptr,
+                                                  x->pjv32.R.p, y, rs);
+    } else {
+      if (!x->pjv.ready) x->pjv.alloc(m.nc, m.nf, m.nb);
+      k_load_dual<T, double><<<gb, tb, 0, s>>>(m.nc, m.nt, ns.Wn.p, z, x->pjv.W.p);
+      launch_chain<Dual<double>>(x, x->pjv, x->pjv.R.p, false, nullptr, nullptr, x->newton_frozen);
+      k_matvec_finish<T, double><<<gb, tb, 0, s>>>(x->cs, m.nc, ns.Wn.p, ns.vol.p, ns.dt.p, z, nullptr, nullptr, 0., nullptr,
+                                                   x->pjv.R.p, y, rs);
+    }
   }
   CK(cudaGetLastError());
 }
@@ -622,31 +637,41 @@ static void apply_prec(fcfd_ctx *x, NewtonState &ns, const T *v, T *z, const Row
     k_precond<T><<<gc, tb, 0, s>>>(nc, ns.Minv.p, v, z, rs);
     return;
   }
-  // r = D^-1 v (double), y0 = Binv r
-  k_unscale<T><<<gc, tb, 0, s>>>(nc, v, rs, ns.Pr.p);
+  // r = D^-1 v, y0 = Binv r; then symmetric multicolour block Gauss-Seidel:
+  // colours forward, then backward.  Updating the same colour twice in a row
+  // changes nothing (its cells do not couple to each other), so the repeat at
+  // each turn is skipped.  FP64 or, with the FP32 preconditioner, FP32
+  // couplings, vectors and arithmetic.
   RowScale one;
   for (int i = 0; i < 5; ++i) one.s[i] = 1.;
-  k_precond<double><<<gc, tb, 0, s>>>(nc, ns.Minv.p, ns.Pr.p, ns.Py0.p, one);
-  double *a = ns.Py0.p;
-  // symmetric multicolour block Gauss-Seidel: colours forward, then backward.
-  // Updating the same colour twice in a row changes nothing (its cells do not
-  // couple to each other), so the repeat at each turn is skipped.
-  const std::vector<int> &ci = x->color_index;
-  const int ncol = (int)ci.size() - 1, deg = x->gs_deg;
-  int last = -1;
-  for (int k = 0; k < sweeps; ++k) {
-    for (int pass = 0; pass < 2; ++pass)
-      for (int q = 0; q < ncol; ++q) {
-        const int col = pass == 0 ? q : ncol - 1 - q;
-        const int cnt = ci[col + 1] - ci[col];
-        if (cnt <= 0 || col == last) continue;
-        last = col;
-        const size_t base = (size_t)ci[col];
-        k_gs_packed<<<(int)(((size_t)cnt * kGsLanes + 127) / 128), 128, 0, s>>>(nc, deg, cnt, x->color_cells.p + base, x->gs_nbr.p + base * deg,
-                                                      ns.OB.p + base * deg * 25, ns.MinvP.p + base * 25, ns.Pr.p, a);
-      }
+  auto sweep = [&](auto *OB, auto *MinvP, auto *r, auto *a) {
+    const std::vector<int> &ci = x->color_index;
+    const int ncol = (int)ci.size() - 1, deg = x->gs_deg;
+    int last = -1;
+    for (int k = 0; k < sweeps; ++k) {
+      for (int pass = 0; pass < 2; ++pass)
+        for (int q = 0; q < ncol; ++q) {
+          const int col = pass == 0 ? q : ncol - 1 - q;
+          const int cnt = ci[col + 1] - ci[col];
+          if (cnt <= 0 || col == last) continue;
+          last = col;
+          const size_t base = (size_t)ci[col];
+          k_gs_packed<<<(int)(((size_t)cnt * kGsLanes + 127) / 128), 128, 0, s>>>(
+              nc, deg, cnt, x->color_cells.p + base, x->gs_nbr.p + base * deg, OB + base * deg * 25, MinvP + base * 25, r, a);
+        }
+    }
+  };
+  if (ns.prec32) {
+    k_unscale<T, float><<<gc, tb, 0, s>>>(nc, v, rs, ns.Pr32.p);
+    k_precond<float><<<gc, tb, 0, s>>>(nc, ns.Minv.p, ns.Pr32.p, ns.Py32.p, one);
+    sweep(ns.OB32.p, ns.MinvP32.p, ns.Pr32.p, ns.Py32.p);
+    k_cast<T, float><<<(5 * nc + tb - 1) / tb, tb, 0, s>>>(5 * nc, ns.Py32.p, z);
+  } else {
+    k_unscale<T, double><<<gc, tb, 0, s>>>(nc, v, rs, ns.Pr.p);
+    k_precond<double><<<gc, tb, 0, s>>>(nc, ns.Minv.p, ns.Pr.p, ns.Py0.p, one);
+    sweep(ns.OB.p, ns.MinvP.p, ns.Pr.p, ns.Py0.p);
+    k_cast<T, double><<<(5 * nc + tb - 1) / tb, tb, 0, s>>>(5 * nc, ns.Py0.p, z);
   }
-  k_cast<T><<<(5 * nc + tb - 1) / tb, tb, 0, s>>>(5 * nc, a, z);
 }
 
 // Right-preconditioned GMRES(m) with up to `cycles` restarts.
@@ -757,7 +782,15 @@ int fcfd_newton_solve(fcfd_ctx *x, double *W, const fcfd_newton_opts *o, fcfd_ne
     ns.JL.alloc(25 * (size_t)m.nf); ns.JR.alloc(25 * (size_t)m.nf); ns.Minv.alloc(25 * (size_t)nc);
     ns.Pr.alloc(n); ns.Py0.alloc(n); ns.Py1.alloc(n); ns.Xs.alloc(n); ns.rowmag.alloc(n);
     ns.sweeps = o->precond_sweeps; ns.cycles = o->krylov_cycles > 0 ? o->krylov_cycles : 1;
-    if (ns.sweeps > 0) { ns.OB.alloc((size_t)nc * x->gs_deg * 25 + 1); ns.MinvP.alloc(25 * (size_t)nc); }
+    ns.prec32 = o->fp32_krylov != 0;
+    if (ns.sweeps > 0) {
+      if (ns.prec32) {
+        ns.OB32.alloc((size_t)nc * x->gs_deg * 25 + 1); ns.MinvP32.alloc(25 * (size_t)nc);
+        ns.Pr32.alloc(5 * (size_t)nc); ns.Py32.alloc(5 * (size_t)nc);
+      } else {
+        ns.OB.alloc((size_t)nc * x->gs_deg * 25 + 1); ns.MinvP.alloc(25 * (size_t)nc);
+      }
+    }
     CK(cudaMemsetAsync(ns.JR.p, 0, sizeof(double) * 25 * (size_t)m.nf, s));
     std::vector<double> vol(x->mesh->c_volume.begin(), x->mesh->c_volume.begin() + nc);
     CK(cudaMemcpyAsync(ns.vol.p, vol.data(), sizeof(double) * nc, cudaMemcpyHostToDevice, s));
@@ -768,6 +801,7 @@ int fcfd_newton_solve(fcfd_ctx *x, double *W, const fcfd_newton_opts *o, fcfd_ne
     Krylov<float> K32;
     const bool f32 = o->fp32_krylov != 0;
     x->newton_frozen = o->jvp_mode == 1;
+    x->newton_f32 = o->jvp_mode == 3;
     const int jmode = o->jvp_mode == 0 ? 0 : 1;
     if (f32) K32.alloc(x, mdim); else K64.alloc(x, mdim);
     DBuf<double> part, hh;
@@ -831,9 +865,16 @@ int fcfd_newton_solve(fcfd_ctx *x, double *W, const fcfd_newton_opts *o, fcfd_ne
           const int cnt = ci[col + 1] - ci[col];
           if (cnt <= 0) continue;
           const size_t base = (size_t)ci[col];
-          k_pack_gs<<<(cnt + 127) / 128, 128, 0, s>>>(nc, m.nf, deg, cnt, x->color_cells.p + base, x->gs_nbr.p + base * deg,
-                                                      x->gs_src.p + base * deg, ns.JL.p, ns.JR.p, ns.Minv.p,
-                                                      ns.OB.p + base * deg * 25, ns.MinvP.p + base * 25);
+          if (ns.prec32)
+            k_pack_gs<float><<<(cnt + 127) / 128, 128, 0, s>>>(nc, m.nf, deg, cnt, x->color_cells.p + base,
+                                                               x->gs_nbr.p + base * deg, x->gs_src.p + base * deg, ns.JL.p,
+                                                               ns.JR.p, ns.Minv.p, ns.OB32.p + base * deg * 25,
+                                                               ns.MinvP32.p + base * 25);
+          else
+            k_pack_gs<double><<<(cnt + 127) / 128, 128, 0, s>>>(nc, m.nf, deg, cnt, x->color_cells.p + base,
+                                                                x->gs_nbr.p + base * deg, x->gs_src.p + base * deg, ns.JL.p,
+                                                                ns.JR.p, ns.Minv.p, ns.OB.p + base * deg * 25,
+                                                                ns.MinvP.p + base * 25);
         }
       }
       CK(cudaGetLastError());

@@ -129,8 +129,9 @@ class NavierStokes:
         check(lib.fcfd_residual(self.h, pw, pr, fw))
         return out
 
-    def jvp(self, W, V, with_residual: bool = False):
-        """Directional derivative (dR/dW).V of the residual (forward tangent)."""
+    def jvp(self, W, V, with_residual: bool = False, fp32: bool = False):
+        """Directional derivative (dR/dW).V of the residual (forward tangent);
+        fp32=True evaluates the tangent chain in single precision."""
         nc = self.mesh.nc
         host = isinstance(W, np.ndarray)
         if host:
@@ -145,7 +146,7 @@ class NavierStokes:
         pv, _ = _ptr(V)
         pj, _ = _ptr(JV)
         pr = _ptr(R)[0] if R is not None else None
-        check(lib.fcfd_jvp(self.h, pw, pv, pr, pj, fw))
+        check(lib.fcfd_jvp(self.h, pw, pv, pr, pj, fw | (4 if fp32 else 0)))
         return (R, JV) if with_residual else JV
 
     def vjp(self, W, Rbar):
@@ -203,12 +204,14 @@ class NavierStokes:
 
     def newton_solve(self, W, tol=1e-10, max_newton=200, krylov_dim=30, krylov_rtol=1e-2, cfl0=1.0,
                      cfl_growth=1.2, cfl_max=1e6, cfl_mode=1, ser_exponent=1.0, jvp=True, fp32_krylov=False,
-                     max_seconds=0.0, raise_on_fail=True, precond_sweeps=0, krylov_cycles=1, exact_jvp=False):
+                     max_seconds=0.0, raise_on_fail=True, precond_sweeps=0, krylov_cycles=1, exact_jvp=False,
+                     fp32_jvp=False):
         """Steady solve R(W) = 0 (pseudo-transient Newton-Krylov on the device).
         Returns (W_converged, report dict)."""
         W = np.array(W, dtype=np.float64, order="C", copy=True)
         o = NewtonOpts(int(max_newton), float(tol), int(krylov_dim), float(krylov_rtol), float(cfl0), float(cfl_growth),
-                       float(cfl_max), int(cfl_mode), float(ser_exponent), (2 if exact_jvp else 1) if jvp else 0,
+                       float(cfl_max), int(cfl_mode), float(ser_exponent),
+                       (3 if fp32_jvp else (2 if exact_jvp else 1)) if jvp else 0,
                        int(bool(fp32_krylov)), float(max_seconds), int(precond_sweeps), int(krylov_cycles))
         r = NewtonReport()
         rc = lib.fcfd_newton_solve(self.h, _d(W), ctypes.byref(o), ctypes.byref(r))

@@ -38,7 +38,8 @@ enum fcfd_status {
 };
 
 enum fcfd_flags {
-  FCFD_DEVICE_PTRS = 1 /* input/output pointers are device pointers on the context's device */
+  FCFD_DEVICE_PTRS = 1, /* input/output pointers are device pointers on the context's device */
+  FCFD_JVP_FP32 = 4     /* fcfd_jvp: evaluate the tangent chain in FP32 (value and derivative) */
 };
 
 enum fcfd_precision { FCFD_FP64 = 0, FCFD_FP32 = 1 };
@@ -184,8 +185,11 @@ typedef struct fcfd_newton_opts {
   double ser_exponent;
   int32_t jvp_mode;       /* 0: finite-difference J.v of the FP64 residual; 1: tangent (dual-number)
                              kernels with the limiter held fixed (frozen-limiter Jacobian);
-                             2: tangent kernels, exact (limiter differentiated too) */
-  int32_t fp32_krylov;    /* 1: Krylov basis and preconditioned vectors in FP32 (dot products in FP64) */
+                             2: tangent kernels, exact (limiter differentiated too);
+                             3: as 2 with the tangent chain in FP32 (mixed precision: the FP64
+                                residual stays the outer Newton residual) */
+  int32_t fp32_krylov;    /* 1: Krylov basis, preconditioner couplings, vectors and Gauss-Seidel
+                             arithmetic in FP32 (dot products and Gram-Schmidt in FP64) */
   double max_seconds;     /* wall-clock cap (0: none) */
   int32_t precond_sweeps; /* symmetric multicolour block Gauss-Seidel sweeps on the first-order
                              operator (0: block-Jacobi, the block diagonal only) */

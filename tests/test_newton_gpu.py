@@ -37,7 +37,8 @@ def wedge(oracle_mod, fb):
 @pytest.mark.gpu
 @pytest.mark.parametrize("label,opts", [("fd64", dict(jvp=False)),
                                         ("jvp64", dict(jvp=True, exact_jvp=True)),
-                                        ("jvp_fp32_krylov", dict(jvp=True, exact_jvp=True, fp32_krylov=True))])
+                                        ("jvp_fp32_krylov", dict(jvp=True, exact_jvp=True, fp32_krylov=True)),
+                                        ("mixed_fp32_tangent", dict(jvp=True, fp32_jvp=True, fp32_krylov=True))])
 def test_newton_cylinder_converges(label, opts, cylinder):
     case, o, ns = cylinder
     W, rep = ns.newton_solve(case.state, **KW, **opts)
@@ -49,13 +50,13 @@ def test_newton_cylinder_converges(label, opts, cylinder):
 
 @pytest.mark.gpu
 def test_newton_variants_agree(cylinder):
-    """Plain FP64 (finite-difference J.v, FP64 Krylov) and mixed (tangent J.v,
-    FP32 Krylov) reach the same steady state: to 1e-7 relative, since the 1e-10
+    """Plain FP64 (finite-difference J.v, FP64 Krylov) and mixed (FP32 tangent
+    J.v, FP32 Krylov, FP64 outer residual) reach the same steady state: to 1e-7 relative, since the 1e-10
     residual tolerance bounds the state error only through the conditioning of
     the Jacobian."""
     case, o, ns = cylinder
     Wa, _ = ns.newton_solve(case.state, jvp=False, **KW)
-    Wb, _ = ns.newton_solve(case.state, jvp=True, exact_jvp=True, fp32_krylov=True, **KW)
+    Wb, _ = ns.newton_solve(case.state, jvp=True, fp32_jvp=True, fp32_krylov=True, **KW)
     # velocity components share one scale: w is rounding noise on this
     # one-layer mesh and its own maximum would divide by ~0
     scale = np.abs(Wa).max(axis=0)
