@@ -335,6 +335,20 @@ NEWTON_KW = dict(tol=1e-10, max_newton=400, cfl0=2.0, cfl_max=1e6, krylov_rtol=1
                  krylov_cycles=3)
 
 
+def profile_newton(args):
+    """Only the two Newton arms, capped at --profile-newton steps (a short,
+    reproducible run for launch-list profiles); prints their report."""
+    import torch
+    import tempfile
+    import freecfd_b200 as fb
+    torch.cuda.set_device(0)
+    case = make_case(args.workload)
+    cs = fb.Case(case.write_deck(tempfile.mkdtemp(prefix="fcfd_bench_")))
+    mesh = fb.Mesh(case.mesh, cs)
+    NEWTON_KW["max_newton"] = int(args.profile_newton)
+    print(json.dumps({"workload": case.workload, "newton": run_newton(fb, cs, mesh, case, 0, None)}), flush=True)
+
+
 def run_newton(fb, cs, mesh, case, dev, dist):
     """Steady solve from the seeded state until |R_mass|/|R_mass0| <= 1e-10:
     plain FP64 (finite-difference J.v, FP64 Krylov) against mixed (tangent
@@ -377,7 +391,7 @@ def run_newton(fb, cs, mesh, case, dev, dist):
 # ncu captures of the same kernels; the capture commands are in profiles/.
 NCU_TRAFFIC = {
     ("cylinder", "grad_limiter"): 17762816, ("cylinder", "face_flux"): 22143744,
-    ("hypersonic", "grad_limiter"): 176979200, ("hypersonic", "face_flux"): 141528064,
+    ("hypersonic", "grad_limiter"): 191846912, ("hypersonic", "face_flux"): 141227264,
 }
 
 
@@ -396,8 +410,12 @@ def main():
     ap.add_argument("--ref-workers", type=int, default=64)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-newton", action="store_true")
+    ap.add_argument("--profile-newton", type=int, default=0,
+                    help="run only the two Newton arms, capped at this many Newton steps")
     args = ap.parse_args()
-    if args.impl == "reference":
+    if args.profile_newton > 0:
+        profile_newton(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)
