@@ -266,6 +266,97 @@ def plate_mesh(ni: int = 384, nj: int = 192, nk: int = 4, plate: float = 2.0,
     return RawMesh(nodes, idx, conn, [inlet, outlet, wall, sym], dimension=3)
 
 
+def box_mesh(nx: int = 6, ny: int = 4, nz: int = 3, kind: str = "tet", seed: int = 7,
+             size=(1.0, 0.5, 0.375), jitter: float = 0.15):
+    """3-D box of non-hex elements, for the element types the benchmark meshes
+    do not use.  kind="tet": every hex split into six tetrahedra around its
+    main diagonal (conforming across hexes); kind="hexpyr": a checkerboard of
+    hexes and hexes split into six pyramids around a centre node (the quads
+    still match).  Interior nodes are jittered by up to `jitter` x spacing.
+
+    BC regions (deck order): 1 inlet x=0, 2 outlet x=Lx, 3 slip wall y=0,
+    4 symmetry (y=Ly, z=0, z=Lz).
+    """
+    Lx, Ly, Lz = size
+    xs, ys, zs = np.linspace(0, Lx, nx + 1), np.linspace(0, Ly, ny + 1), np.linspace(0, Lz, nz + 1)
+    Z, Y, X = np.meshgrid(zs, ys, xs, indexing="ij")
+    nodes = np.stack([X.ravel(), Y.ravel(), Z.ravel()], axis=1).astype(np.float64)
+    nid = lambda i, j, k: (k * (ny + 1) + j) * (nx + 1) + i
+    ii = np.tile(np.arange(nx + 1), (nz + 1) * (ny + 1))
+    jj = np.tile(np.repeat(np.arange(ny + 1), nx + 1), nz + 1)
+    kk = np.repeat(np.arange(nz + 1), (ny + 1) * (nx + 1))
+    inner = (ii > 0) & (ii < nx) & (jj > 0) & (jj < ny) & (kk > 0) & (kk < nz)
+    rng = np.random.default_rng(seed)
+    h = np.array([Lx / nx, Ly / ny, Lz / nz])
+    nodes[inner] += jitter * h * rng.uniform(-1.0, 1.0, size=(int(inner.sum()), 3))
+    cells = []
+    extra = []
+    for k in range(nz):
+        for j in range(ny):
+            for i in range(nx):
+                v = [nid(i, j, k), nid(i + 1, j, k), nid(i + 1, j + 1, k), nid(i, j + 1, k),
+                     nid(i, j, k + 1), nid(i + 1, j, k + 1), nid(i + 1, j + 1, k + 1), nid(i, j + 1, k + 1)]
+                if kind == "tet":
+                    for a, b, c in ((1, 2, 6), (2, 3, 6), (3, 7, 6), (7, 4, 6), (4, 5, 6), (5, 1, 6)):
+                        t = [v[0], v[a], v[b], v[c]]
+                        P = nodes[t]
+                        if np.dot(np.cross(P[1] - P[0], P[2] - P[0]), P[3] - P[0]) < 0:
+                            t[1], t[2] = t[2], t[1]
+                        cells.append(t)
+                elif (i + j + k) % 2 == 0:
+                    cells.append(v)
+                else:
+                    ctr = len(nodes) + len(extra)
+                    extra.append(nodes[v].mean(axis=0))
+                    # hex faces (outward), each the base of one pyramid with the apex inside
+                    for f in ((0, 3, 2, 1), (4, 5, 6, 7), (1, 2, 6, 5), (0, 4, 7, 3), (1, 5, 4, 0), (2, 3, 7, 6)):
+                        a, b, c, d = (v[q] for q in f)
+                        cells.append([a, d, c, b, ctr])
+    if extra:
+        nodes = np.vstack([nodes, np.array(extra)])
+    idx = np.zeros(len(cells) + 1, dtype=np.int32)
+    idx[1:] = np.cumsum([len(c) for c in cells])
+    conn = np.concatenate([np.asarray(c, dtype=np.int32) for c in cells])
+    nb = (nx + 1) * (ny + 1) * (nz + 1)
+    sel = lambda m: np.nonzero(m)[0].astype(np.int32)
+    inlet, outlet, wall = sel(ii == 0), sel(ii == nx), sel(jj == 0)
+    sym = sel((jj == ny) | (kk == 0) | (kk == nz))
+    assert nb == ii.size
+    return RawMesh(nodes, idx, conn, [inlet, outlet, wall, sym], dimension=3)
+
+
+def box_case(kind="tet", nx=6, ny=4, nz=3, seed=1234, flux="AUSM+up", limiter="vk", threshold=1.0) -> Case:
+    """Inviscid M=0.6 flow through the non-hex box (parity coverage of the
+    tetrahedron and pyramid face tables, LSQ stencils and geometry)."""
+    mesh = box_mesh(nx, ny, nz, kind)
+    p, T, M = 101325.0, 300.0, 0.6
+    U = M * math.sqrt(1.4 * R_AIR * T)
+    rho = p / (R_AIR * T)
+    deck = f"""// Box {nx}x{ny}x{nz} split into {kind} elements, M={M}
+reference {{Mach={_fmt(M)}; p=0.; T=0.;}}
+time marching {{ CFLmax=50.; number of steps=500; }}
+grid_1 {{
+ file=box.cgns;
+ dimension=3;
+ equations=navier stokes;
+ material (viscosity=0.; molar mass={_fmt(MW_AIR)}; gamma=1.4;);
+ gradients (hex method=lsqr; prism method=lsqr; other method=lsqr;);
+ navier stokes (limiter={limiter}; limiter threshold={_fmt(threshold)}; convective flux={flux};);
+ write output ( volume variables=[V,p,T]; surface variables=[p]; );
+ IC_1 (rho={_fmt(rho)}; V={_vec((U, 0.0, 0.0))}; p={_fmt(p)};);
+ BC_1 (type=inlet; rho={_fmt(rho)}; V={_vec((U, 0.0, 0.0))};);
+ BC_2 (type=outlet; p={_fmt(p)};);
+ BC_3 (type=wall; kind=slip;);
+ BC_4 (type=symmetry;);
+}}
+"""
+    free = (p, U, 0.0, 0.0, T)
+    st = seeded_state(mesh.n_cells, free, seed)
+    st[:, 2] = 0.02 * U * np.random.default_rng(seed + 2).uniform(-1.0, 1.0, mesh.n_cells)
+    st[:, 3] = 0.02 * U * np.random.default_rng(seed + 3).uniform(-1.0, 1.0, mesh.n_cells)
+    return Case("box", mesh, deck, {}, st, free, f"euler_box_{nx}x{ny}x{nz}_{kind}_{flux}")
+
+
 # ----------------------------------------------------------------------------
 # decks
 # ----------------------------------------------------------------------------

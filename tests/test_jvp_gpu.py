@@ -8,7 +8,7 @@ the residual is smooth along the direction (no limiter switch inside +-h)."""
 import numpy as np
 import pytest
 
-from tests.util import SMALL, build_pair, rel_err
+from tests.util import ELEMENTS, SMALL, build_pair, rel_err
 
 
 def _dirs(shape, seed, n):
@@ -86,3 +86,18 @@ def test_fp32_tangent_chain(family, oracle_mod, fb):
         cols = [0, 1, 2, 4]
         err = rel_err(j32[:, cols], j64[:, cols])
         assert err.max() <= 1e-4, err
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("family", sorted(ELEMENTS))
+def test_jvp_tets_pyramids(family, oracle_mod, fb):
+    """Tangent kernels on tetrahedra and pyramids vs the complex step."""
+    case = ELEMENTS[family](flux="Roe", limiter="vk")
+    o, cs, m = build_pair(case, oracle_mod, fb)
+    ns = fb.NavierStokes(m, cs, 0)
+    scale = np.abs(case.state).max(axis=0)
+    for V in _dirs(case.state.shape, 23, 2):
+        V = V * scale
+        jv = ns.jvp(case.state, V)
+        ref = o.residual_cstep(case.state, V)
+        assert rel_err(jv, ref).max() <= 1e-10

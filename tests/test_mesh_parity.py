@@ -4,21 +4,21 @@ face_interpolation_weights / lsqr_grad_map — bit-exact (CPU only)."""
 import numpy as np
 import pytest
 
-from tests.util import SMALL, build_pair
+from tests.util import ALL, build_pair
 
 
-@pytest.mark.parametrize("family", sorted(SMALL))
+@pytest.mark.parametrize("family", sorted(ALL))
 def test_connectivity_bit_exact(family, oracle_mod, fb):
-    o, cs, m = build_pair(SMALL[family](), oracle_mod, fb)
+    o, cs, m = build_pair(ALL[family](), oracle_mod, fb)
     co, cp = o.connectivity(), m.connectivity()
     assert (o.nc, o.nf, o.nghost) == (m.nc, m.nf, m.nghost)
     for k in co:
         assert np.array_equal(co[k], cp[k]), k
 
 
-@pytest.mark.parametrize("family", sorted(SMALL))
+@pytest.mark.parametrize("family", sorted(ALL))
 def test_geometry_bit_exact(family, oracle_mod, fb):
-    o, cs, m = build_pair(SMALL[family](), oracle_mod, fb)
+    o, cs, m = build_pair(ALL[family](), oracle_mod, fb)
     go, gp = o.geometry(), m.geometry()
     for k in go:
         a, b = np.asarray(go[k]), np.asarray(gp[k])
@@ -27,13 +27,13 @@ def test_geometry_bit_exact(family, oracle_mod, fb):
                               b.view(np.uint64) if b.dtype == np.float64 else b), k
 
 
-@pytest.mark.parametrize("family", sorted(SMALL))
+@pytest.mark.parametrize("family", sorted(ALL))
 def test_lsq_weights_bit_exact(family, oracle_mod, fb):
     """The gradient kernel rebuilds each lsqr_grad_map weight from centroids,
     per-cell cofactors/determinant and the precomputed self weight.  Redo that
     arithmetic here (numpy rounds every operation once, like the kernel's
     __dmul_rn/__dadd_rn/__ddiv_rn) and compare with the oracle's std::map."""
-    o, cs, m = build_pair(SMALL[family](), oracle_mod, fb)
+    o, cs, m = build_pair(ALL[family](), oracle_mod, fb)
     cof, selfw = m.lsq_data()
     g = m.geometry()
     conn = m.connectivity()
@@ -56,17 +56,17 @@ def test_lsq_weights_bit_exact(family, oracle_mod, fb):
     assert np.array_equal(out.view(np.uint64), w_or.view(np.uint64))
 
 
-@pytest.mark.parametrize("family", sorted(SMALL))
+@pytest.mark.parametrize("family", sorted(ALL))
 def test_lsq_stencil_keys(family, oracle_mod, fb):
-    o, cs, m = build_pair(SMALL[family](), oracle_mod, fb)
+    o, cs, m = build_pair(ALL[family](), oracle_mod, fb)
     co, cp = o.connectivity(), m.connectivity()
     assert np.array_equal(co["grad_index"], cp["grad_index"])
     assert np.array_equal(co["grad_keys"], cp["grad_keys"])
 
 
-@pytest.mark.parametrize("family", sorted(SMALL))
+@pytest.mark.parametrize("family", sorted(ALL))
 def test_case_summary(family, oracle_mod, fb):
-    o, cs, m = build_pair(SMALL[family](), oracle_mod, fb)
+    o, cs, m = build_pair(ALL[family](), oracle_mod, fb)
     do, io = o.case_summary()
     dp, ip = cs.summary()
     assert np.array_equal(do[:12], dp[:12])

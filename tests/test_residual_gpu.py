@@ -18,7 +18,7 @@ import numpy as np
 import pytest
 
 from freecfd_b200 import cases
-from tests.util import SMALL, build_pair, flux_scale, rel_err, res_err
+from tests.util import ELEMENTS, SMALL, build_pair, flux_scale, rel_err, res_err
 
 TOL = 1e-12
 BITWISE = {"wedge", "hypersonic"}
@@ -85,6 +85,23 @@ def test_residual_parity(family, flux, limiter, oracle_mod, fb):
     # side is a rounding decision and mdot*weightL vanishes either way.
     big = np.abs(ref["mdot"]) > 1e-9 * np.abs(ref["mdot"]).max()
     assert np.array_equal(st["weightL"][big], ref["weightL"][big])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("family", sorted(ELEMENTS))
+@pytest.mark.parametrize("flux,limiter", [("AUSM+up", "vk"), ("Roe", "minmod"), ("vanLeer", "bj"), ("Roe", "none")])
+def test_residual_parity_tets_pyramids(family, flux, limiter, oracle_mod, fb):
+    """Tetrahedra and pyramids (face tables, LSQ stencils of non-hex cells,
+    triangle faces): residual parity on the jittered box meshes."""
+    case = ELEMENTS[family](flux=flux, limiter=limiter)
+    o, cs, m, ns = _ctx(case, oracle_mod, fb, exact=limiter in ("minmod", "bj"))
+    ref = o.residual(case.state, full=True)
+    R = ns.residual(case.state)
+    st = ns.stages()
+    assert rel_err(st["ghost"], ref["ghost"]).max() <= 1e-14
+    assert grad_err(st["grads"], ref["grads"], m.nc).max() <= 1e-12
+    assert rel_err(st["limiter"], ref["limiter"]).max() <= 1e-11
+    assert res_err(R, ref["R"]).max() <= TOL
 
 
 @pytest.mark.gpu

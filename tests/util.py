@@ -15,6 +15,14 @@ SMALL = {
 }
 
 
+# Tetrahedra and pyramids (the benchmark meshes are hexes and prisms only)
+ELEMENTS = {
+    "box_tet": lambda **kw: cases.box_case("tet", **kw),
+    "box_hexpyr": lambda **kw: cases.box_case("hexpyr", **kw),
+}
+ALL = {**SMALL, **ELEMENTS}
+
+
 def build_pair(case, oracle_mod, fb):
     """Oracle + product objects for the same case (decks in a temp dir)."""
     d = tempfile.mkdtemp(prefix="fcfd_")
