@@ -325,7 +325,8 @@ def box_mesh(nx: int = 6, ny: int = 4, nz: int = 3, kind: str = "tet", seed: int
     return RawMesh(nodes, idx, conn, [inlet, outlet, wall, sym], dimension=3)
 
 
-def box_case(kind="tet", nx=6, ny=4, nz=3, seed=1234, flux="AUSM+up", limiter="vk", threshold=1.0) -> Case:
+def box_case(kind="tet", nx=6, ny=4, nz=3, seed=1234, flux="AUSM+up", limiter="vk", threshold=1.0,
+             grad="lsqr") -> Case:
     """Inviscid M=0.6 flow through the non-hex box (parity coverage of the
     tetrahedron and pyramid face tables, LSQ stencils and geometry)."""
     mesh = box_mesh(nx, ny, nz, kind)
@@ -340,7 +341,7 @@ grid_1 {{
  dimension=3;
  equations=navier stokes;
  material (viscosity=0.; molar mass={_fmt(MW_AIR)}; gamma=1.4;);
- gradients (hex method=lsqr; prism method=lsqr; other method=lsqr;);
+ gradients (hex method={grad}; prism method={grad}; other method={grad};);
  navier stokes (limiter={limiter}; limiter threshold={_fmt(threshold)}; convective flux={flux};);
  write output ( volume variables=[V,p,T]; surface variables=[p]; );
  IC_1 (rho={_fmt(rho)}; V={_vec((U, 0.0, 0.0))}; p={_fmt(p)};);
@@ -394,7 +395,7 @@ def seeded_state(n_cells: int, free: tuple, seed: int, amp: float = 0.01) -> np.
 
 
 def wedge_case(ni=120, nj=60, seed=1234, flux="Roe", limiter="vk", threshold=1.0,
-               order="second") -> Case:
+               order="second", grad="lsqr") -> Case:
     mesh = wedge_mesh(ni, nj)
     p, T, M = 101325.0, 300.0, 2.5
     a = math.sqrt(1.4 * R_AIR * T)
@@ -407,7 +408,7 @@ grid_1 {{
  dimension=2;
  equations=navier stokes;
  material (viscosity=0.; molar mass={_fmt(MW_AIR)}; gamma=1.4;);
- gradients (hex method=lsqr; prism method=lsqr;);
+ gradients (hex method={grad}; prism method={grad};);
  navier stokes (limiter={limiter}; limiter threshold={_fmt(threshold)}; order={order}; convective flux={flux};);
  write output ( volume variables=[V,p,T]; surface variables=[p]; );
  IC_1 (p={_fmt(p)}; T={_fmt(T)}; V={_vec((U, 0.0, 0.0))};);

@@ -695,6 +695,7 @@ extern "C" {
 int fcfd_vjp(fcfd_ctx *x, const double *W, const double *Rbar, double *Wbar, int flags) {
   try {
     if (!x || !W || !Rbar || !Wbar) throw Error(FCFD_ERR_INPUT, "null argument");
+    if (x->green_gauss) throw Error(FCFD_ERR_UNSUPPORTED, "the adjoint covers least-squares gradients only");
     CK(cudaSetDevice(x->device));
     const DevMesh &m = x->dm;
     cudaStream_t s = x->stream;
@@ -730,6 +731,7 @@ int fcfd_vjp(fcfd_ctx *x, const double *W, const double *Rbar, double *Wbar, int
 int fcfd_drag(fcfd_ctx *x, const double *W, uint32_t bc_mask, const double *dir, double *force, double *dJdW, int flags) {
   try {
     if (!x || !W || !dir || !force) throw Error(FCFD_ERR_INPUT, "null argument");
+    if (dJdW && x->green_gauss) throw Error(FCFD_ERR_UNSUPPORTED, "the adjoint covers least-squares gradients only");
     CK(cudaSetDevice(x->device));
     const DevMesh &m = x->dm;
     cudaStream_t s = x->stream;

@@ -196,6 +196,8 @@ int fcfd_ctx_create(const fcfd_mesh *mp, const fcfd_case *csp, int device, fcfd_
     o.mdot_per_area = r.mdot / m.bc_total_area[b];
     for (int k = 0; k < 3; ++k) o.V[k] = r.V[k];
     o.T_fixed = r.T_fixed ? 1 : 0;
+    o.p_fixed = r.p_fixed ? 1 : 0;
+    o.V_fixed = r.V_fixed ? 1 : 0;
     if (r.thermal == TH_FIXED_Q && r.type == BC_WALL) fixed_q = true;
   }
   x->viscous = mt.sutherland || mt.prandtl || mt.mu != 0. || mt.lambda != 0. || fixed_q;
@@ -222,6 +224,12 @@ int fcfd_ctx_create(const fcfd_mesh *mp, const fcfd_case *csp, int device, fcfd_
   x->st_index.upload(m.st_index); x->st_keys.upload(m.st_keys);
   x->st_cof.upload(soa(m.st_cof, nc, 7)); x->st_self.upload(soa(m.st_self, nc, 3));
   x->st_recip.upload(m.st_recip); x->st_mirror.upload(soa(m.st_mirror, nc, 3));
+  {
+    std::vector<double> vol(m.c_volume.begin(), m.c_volume.begin() + nc);
+    x->c_vol.upload(vol);
+    for (int cc = 0; cc < nc; ++cc)
+      if (m.st_index[cc] == m.st_index[cc + 1]) { x->green_gauss = true; break; }
+  }
   std::vector<int32_t> bface(nb), outl;
   for (int f = 0; f < nf; ++f) {
     if (m.f_bc[f] >= 0) {
@@ -289,7 +297,7 @@ int fcfd_ctx_create(const fcfd_mesh *mp, const fcfd_case *csp, int device, fcfd_
   dm.f_n = x->f_n.p; dm.f_area = x->f_area.p; dm.f_x = x->f_x.p; dm.f_w = x->f_w.p; dm.c_x = x->c_x.p;
   dm.c_len = x->c_len.p; dm.cf_index = x->cf_index.p; dm.cf_list = x->cf_list.p; dm.st_index = x->st_index.p;
   dm.st_keys = x->st_keys.p; dm.st_cof = x->st_cof.p; dm.st_self = x->st_self.p; dm.bface = x->bface.p;
-  dm.st_recip = x->st_recip.p; dm.st_mirror = x->st_mirror.p;
+  dm.st_recip = x->st_recip.p; dm.st_mirror = x->st_mirror.p; dm.c_vol = x->c_vol.p;
   dm.outlet_faces = x->outlet.p; dm.n_outlet = x->n_outlet;
   rans_setup(x.get());  // k-omega BC values and buffers (turbulent cases only)
   CK(cudaDeviceSynchronize());

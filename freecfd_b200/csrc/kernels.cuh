@@ -127,6 +127,7 @@ struct DevBC {
   // eddy viscosity BC values of rans_set_bcs.cc)
   int T_fixed, kw_fixed, mut_fixed, pad_;
   double k_bc, omega_bc, mut_bc;
+  int p_fixed, V_fixed;  // p / V fixed on the BC (their Green-Gauss face values)
 };
 constexpr int kMaxBC = 16;
 struct DevCase {
@@ -149,6 +150,7 @@ struct DevMesh {
   const double *st_cof;                    // [7][nc]
   const double *st_self;                   // [3][nc]
   const double *st_recip;                  // [nc] 1/det where the reciprocal division is exact, else 0
+  const double *c_vol;                     // [nc] cell volumes (Green-Gauss gradients)
   const double *st_mirror;                 // [3][nc] summed symmetry-mirror weights
   const int *bface;                        // boundary faces in ghost order [nb]
   const int *outlet_faces;                 // outlet boundary faces [n_outlet]
@@ -350,6 +352,46 @@ __device__ __forceinline__ void recon_state(const DevCase &c, const DevMesh &m, 
 
 // ------------------------------------------------------------------ kernels
 
+// Green-Gauss gradient of cell c (Variable::cell_gradient's fallback for an
+// empty gradient map, variable.h:204-213): sum over the cell's faces in
+// ascending order of the face value x (n A / V), negated on the neighbour
+// side; the face value is the BC value where the variable is fixed on the BC,
+// else the face average w_p phi_p + w_n phi_n.  Rounded operations in the
+// reference's order.
+template <class S>
+__device__ void green_gauss(const DevCase &cs, const DevMesh &m, const S *__restrict__ W, int c, S g[15]) {
+  const int nt = m.nt, nf = m.nf;
+  const double vol = m.c_vol[c];
+#pragma unroll
+  for (int i = 0; i < 15; ++i) g[i] = S(0.);
+  for (int j = m.cf_index[c]; j < m.cf_index[c + 1]; ++j) {
+    const int e = m.cf_list[j];
+    const int f = e >= 0 ? e : ~e;
+    const double A = m.f_area[f];
+    double av[3];
+    for (int i = 0; i < 3; ++i) {
+      av[i] = div_rn(mul_rn(m.f_n[i * nf + f], A), vol);
+      if (e < 0) av[i] = mul_rn(av[i], -1.);
+    }
+    const int b = m.f_bc[f], pa = m.f_parent[f], nb = m.f_neighbor[f];
+    const double w0 = m.f_w[f], w1 = m.f_w[nf + f];
+#pragma unroll
+    for (int v = 0; v < 5; ++v) {
+      S fv;
+      bool fixed = false;
+      if (b >= 0) {
+        const DevBC &bc = cs.bc[b];
+        if (v == 0 && bc.p_fixed) { fv = S(bc.p); fixed = true; }
+        else if (v == 4 && bc.T_fixed) { fv = S(bc.T); fixed = true; }
+        else if (v >= 1 && v <= 3 && bc.V_fixed) { fv = S(bc.V[v - 1]); fixed = true; }
+      }
+      if (!fixed) fv = add_rn(add_rn(S(0.), mul_rn(S(w0), W[v * nt + pa])), mul_rn(S(w1), W[v * nt + nb]));
+#pragma unroll
+      for (int i = 0; i < 3; ++i) g[3 * v + i] = add_rn(g[3 * v + i], mul_rn(fv, S(av[i])));
+    }
+  }
+}
+
 // AoS [nc][5] -> SoA W[5][nt]
 template <class S>
 __global__ void k_aos_to_soa(const S *__restrict__ in, S *__restrict__ W, int nc, int nt) {
@@ -484,7 +526,9 @@ __global__ void __launch_bounds__(128, (!FAST && std::is_same<S, double>::value)
 #pragma unroll
   for (int i = 0; i < 15; ++i) g[i] = S(0.);
   const int j0 = m.st_index[c], j1 = m.st_index[c + 1];
-  if (FAST) {
+  if (j0 == j1) {
+    green_gauss(cs, m, W, c, g);
+  } else if (FAST) {
     // Continuous limiters only (VK with K > 0, none, first order): the same
     // weighted least-squares gradient in the compact form
     //   grad = C . sum_k w_k d_k (phi_k - phi_c) / det - mirror * phi_c

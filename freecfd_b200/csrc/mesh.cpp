@@ -469,7 +469,12 @@ fcfd_mesh *build_mesh(const fcfd_raw_mesh &raw, fcfd_case &cs) {
         int nn = raw.conn_index[c + 1] - raw.conn_index[c];
         int meth = (nn == 8) ? cs.hex_method : (nn == 6 ? cs.prism_method : cs.other_method);
         if (meth == GM_CURVILINEAR) throw Error(FCFD_ERR_UNSUPPORTED, "curvilinear gradients are not supported; set hex/prism method=lsqr");
-        if (meth == GM_GREENGAUSS) throw Error(FCFD_ERR_UNSUPPORTED, "Green-Gauss gradients are not supported on the B200 path");
+        if (meth == GM_GREENGAUSS) {
+          // empty gradient map: the gradient falls back to Green-Gauss
+          // (variable.h:204-213), evaluated per face on the device
+          m.st_index[c + 1] = (int)m.st_keys.size();
+          continue;
+        }
         m.has_lsq[c] = 1;
         st.clear(); dist.clear(); w.clear();
         P3 xc = ccent(c);

@@ -191,6 +191,7 @@ void rans_setup(fcfd_ctx *x) {
   const fcfd_mesh &m = *x->mesh;
   if (!c.turbulent) return;
   if (!x->viscous) throw Error(FCFD_ERR_INPUT, "a turbulence model needs a viscous material");
+  if (x->green_gauss) throw Error(FCFD_ERR_UNSUPPORTED, "the k-omega terms cover least-squares gradients only");
   const Material &mt = c.mat;
   const int nc = m.nc, nb = m.nb, nt = nc + nb, nf = m.nf;
   double p = c.ic_p, T = c.ic_T;

@@ -958,7 +958,8 @@ struct NS {
   NS(Oracle &o, Fields<S> &f) : O(o), F(f) {}
 
   // Variable<double>::cell_gradient (variable.h:193-216) for scalars
-  V3<S> scalar_gradient(const std::vector<S> &phi, int c) {
+  // which: 0 p, 1 T (their BC-fixed face values), 2 neither
+  V3<S> scalar_gradient(const std::vector<S> &phi, int c, int which = 2) {
     V3<S> grad;
     Grid &g = O.grid;
     if (!g.cell[c].gradMap.empty()) {
@@ -969,7 +970,7 @@ struct NS {
         int f = g.cell[c].faces[cf];
         Vec3 areaVec = g.face[f].normal * g.face[f].area / g.cell[c].volume;
         if (g.face[f].parent != c) areaVec *= -1.;
-        S fv = face_scalar(phi, f, 0);
+        S fv = face_scalar(phi, f, which);
         for (int i = 0; i < 3; ++i) grad[i] += fv * areaVec[i];
       }
     }
@@ -998,8 +999,8 @@ struct NS {
   void calc_cell_grads() {
     Grid &g = O.grid;
     for (int c = 0; c < g.cellCount; ++c) {
-      F.gradp[c] = scalar_gradient(F.p, c);
-      F.gradT[c] = scalar_gradient(F.T, c);
+      F.gradp[c] = scalar_gradient(F.p, c, 0);
+      F.gradT[c] = scalar_gradient(F.T, c, 1);
       V3<S> gx, gy, gz;  // V.cell_gradient(c): grad[i] is a Vec3D (d/dx_i of V)
       if (!g.cell[c].gradMap.empty()) {
         for (auto &kv : g.cell[c].gradMap) {
@@ -1008,7 +1009,21 @@ struct NS {
           gz = vadd(gz, vscale(kv.second[2], F.V[kv.first]));
         }
       } else {
-        throw DeckError("Green-Gauss gradients of V are not restated");
+        // Green-Gauss fallback (variable.h:204-213) for the Vec3D variable:
+        // d/dx_i of V += V.face(f) * areaVec[i], V.face the BC value where V
+        // is fixed on the BC, else the face average
+        for (size_t cf = 0; cf < g.cell[c].faces.size(); ++cf) {
+          int f = g.cell[c].faces[cf];
+          Vec3 areaVec = g.face[f].normal * g.face[f].area / g.cell[c].volume;
+          if (g.face[f].parent != c) areaVec *= -1.;
+          const int b = g.face[f].bc;
+          V3<S> Vf;
+          if (b >= 0 && O.V_fixed[b]) Vf = V3<S>(S(O.V_bc[b][0]), S(O.V_bc[b][1]), S(O.V_bc[b][2]));
+          else Vf = face_vec(F.V, f);
+          gx = vadd(gx, vscale(areaVec[0], Vf));
+          gy = vadd(gy, vscale(areaVec[1], Vf));
+          gz = vadd(gz, vscale(areaVec[2], Vf));
+        }
       }
       F.gradu[c] = V3<S>(gx[0], gy[0], gz[0]);
       F.gradv[c] = V3<S>(gx[1], gy[1], gz[1]);

@@ -187,3 +187,36 @@ def test_conservation_full_cylinder(oracle_mod, fb):
     s, sr = R.sum(axis=0), ref.sum(axis=0)
     scale = np.maximum(np.abs(ref).sum(axis=0), 1e-6 * np.abs(ref).sum(axis=0).max())
     assert (np.abs(s - sr) / scale).max() < 1e-12
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("family,limiter", [("wedge", "vk"), ("wedge", "minmod"), ("box_hexpyr", "vk"),
+                                            ("box_tet", "minmod")])
+def test_green_gauss_gradients(family, limiter, oracle_mod, fb):
+    """gradients (... method=greengauss): empty gradient maps, so the gradient
+    is the Green-Gauss fallback of Variable::cell_gradient (variable.h:204-213)
+    with BC-fixed face values; evaluated with rounded operations in the
+    reference's order, bit-exact where the ghosts are (wedge)."""
+    if family == "wedge":
+        case = cases.wedge_case(ni=24, nj=12, limiter=limiter, grad="greengauss")
+    else:
+        case = ELEMENTS[family](limiter=limiter, grad="greengauss")
+    o, cs, m, ns = _ctx(case, oracle_mod, fb)
+    assert m.n_grad_entries == 0
+    ref = o.residual(case.state, full=True)
+    R = ns.residual(case.state)
+    st = ns.stages()
+    if family == "wedge":
+        assert np.array_equal(st["grads"], ref["grads"][: m.nc])
+        assert np.array_equal(st["limiter"], ref["limiter"])
+    else:
+        assert grad_err(st["grads"], ref["grads"], m.nc).max() <= 1e-13
+        assert rel_err(st["limiter"], ref["limiter"]).max() <= 1e-11
+    assert res_err(R, ref["R"]).max() <= TOL
+    # the tangent chain goes through the same fallback
+    V = np.random.default_rng(3).standard_normal(case.state.shape) * np.abs(case.state).max(axis=0)
+    jv, cs_ = ns.jvp(case.state, V), o.residual_cstep(case.state, V)
+    cols = [k for k in range(5) if np.abs(cs_[:, k]).max() > 1e-12 * np.abs(cs_).max()]
+    assert rel_err(jv[:, cols], cs_[:, cols]).max() <= 1e-10
+    with pytest.raises(fb.FcfdError):          # the adjoint covers least-squares gradients only
+        ns.vjp(case.state, np.ones_like(case.state))
