@@ -395,7 +395,7 @@ def seeded_state(n_cells: int, free: tuple, seed: int, amp: float = 0.01) -> np.
 
 
 def wedge_case(ni=120, nj=60, seed=1234, flux="Roe", limiter="vk", threshold=1.0,
-               order="second", grad="lsqr") -> Case:
+               order="second", grad="lsqr", ns_extra="") -> Case:
     mesh = wedge_mesh(ni, nj)
     p, T, M = 101325.0, 300.0, 2.5
     a = math.sqrt(1.4 * R_AIR * T)
@@ -409,7 +409,7 @@ grid_1 {{
  equations=navier stokes;
  material (viscosity=0.; molar mass={_fmt(MW_AIR)}; gamma=1.4;);
  gradients (hex method={grad}; prism method={grad};);
- navier stokes (limiter={limiter}; limiter threshold={_fmt(threshold)}; order={order}; convective flux={flux};);
+ navier stokes (limiter={limiter}; limiter threshold={_fmt(threshold)}; order={order}; convective flux={flux};{ns_extra});
  write output ( volume variables=[V,p,T]; surface variables=[p]; );
  IC_1 (p={_fmt(p)}; T={_fmt(T)}; V={_vec((U, 0.0, 0.0))};);
  BC_1 (type=inlet; p={_fmt(p)}; T={_fmt(T)}; V={_vec((U, 0.0, 0.0))};);
@@ -425,7 +425,7 @@ grid_1 {{
 
 
 def cylinder_case(ntheta=256, nr=128, seed=1234, flux="Roe", limiter="vk",
-                  threshold=1.0, r1=15.0, dr0=1e-3) -> Case:
+                  threshold=1.0, r1=15.0, dr0=1e-3, ns_extra="") -> Case:
     mesh = cylinder_mesh(ntheta, nr, r1=r1, dr0=dr0)
     p, T, M, Re, D = 101325.0, 300.0, 0.2, 40.0, 1.0
     a = math.sqrt(1.4 * R_AIR * T)
@@ -442,7 +442,7 @@ grid_1 {{
  equations=navier stokes;
  material=air;
  gradients (hex method=lsqr; prism method=lsqr;);
- navier stokes (limiter={limiter}; limiter threshold={_fmt(threshold)}; convective flux={flux};);
+ navier stokes (limiter={limiter}; limiter threshold={_fmt(threshold)}; convective flux={flux};{ns_extra});
  write output ( volume variables=[V,p,T]; surface variables=[p]; load frequency=1; include bcs=[1]; );
  IC_1 (rho={_fmt(rho)}; V={_vec((U, 0.0, 0.0))}; p={_fmt(p)};);
  BC_1 (type=wall;);
@@ -458,7 +458,7 @@ grid_1 {{
 
 
 def hypersonic_case(ntheta=512, nr=256, seed=1234, flux="AUSM+up", limiter="minmod",
-                    r1=2.5, dr0=2e-3, jitter_seed=4321) -> Case:
+                    r1=2.5, dr0=2e-3, jitter_seed=4321, ns_extra="") -> Case:
     mesh = cylinder_mesh(ntheta, nr, r1=r1, dr0=dr0 * 256.0 / nr, jitter=0.1,
                          seed=jitter_seed, prisms=True)
     p, T, M = 2000.0, 220.0, 8.0
@@ -473,7 +473,7 @@ grid_1 {{
  equations=navier stokes;
  material (viscosity=0.; molar mass={_fmt(MW_AIR)}; gamma=1.4;);
  gradients (hex method=lsqr; prism method=lsqr;);
- navier stokes (limiter={limiter}; convective flux={flux};);
+ navier stokes (limiter={limiter}; convective flux={flux};{ns_extra});
  write output ( volume variables=[V,p,T]; surface variables=[p]; );
  IC_1 (p={_fmt(p)}; T={_fmt(T)}; V={_vec((U, 0.0, 0.0))};);
  BC_1 (type=wall; kind=slip;);
@@ -489,7 +489,7 @@ grid_1 {{
 
 
 def plate_case(ni=384, nj=192, nk=4, seed=1234, flux="Roe", limiter="vk",
-               threshold=1.0, turbulent=True) -> Case:
+               threshold=1.0, turbulent=True, ns_extra="") -> Case:
     L, ReL = 2.0, 5e6
     p, T, M = 101325.0, 300.0, 0.2
     a = math.sqrt(1.4 * R_AIR * T)
@@ -512,7 +512,7 @@ grid_1 {{
  equations=navier stokes;
  material=air;
  gradients (hex method=lsqr; prism method=lsqr;);
-{turb} navier stokes (limiter={limiter}; limiter threshold={_fmt(threshold)}; convective flux={flux};);
+{turb} navier stokes (limiter={limiter}; limiter threshold={_fmt(threshold)}; convective flux={flux};{ns_extra});
  write output ( volume variables=[V,p,T]; surface variables=[p]; );
  IC_1 (rho={_fmt(rho)}; V={_vec((U, 0.0, 0.0))}; p={_fmt(p)};{tin});
  BC_1 (type=inlet; rho={_fmt(rho)}; V={_vec((U, 0.0, 0.0))};{tin});

@@ -78,7 +78,7 @@ __device__ __forceinline__ void state_from(const DevCase &cs, FState<DA> &s, con
 
 // D_f and the right density of face f from its local inputs (the same
 // sequence as face_states + face_D).
-template <bool VISCOUS>
+template <bool VISCOUS, int FX>
 __device__ void face_from_inputs(const DevCase &cs, const DevMesh &m, int f, const double n[3], double A, int b, int pa,
                                  int nb, const Seeds &in, DA D[5], DA &rhoR) {
   FState<DA> L, R;
@@ -94,7 +94,7 @@ __device__ void face_from_inputs(const DevCase &cs, const DevMesh &m, int f, con
   rhoR = R.rho;
   DA wL;
   const SeedGrad gs{&in};
-  face_D<DA, SeedGrad, VISCOUS>(cs, m, f, n, A, b, pa, nb, L, R, gs, (const DA *)nullptr, D, wL);
+  face_D<DA, SeedGrad, VISCOUS, FX>(cs, m, f, n, A, b, pa, nb, L, R, gs, (const DA *)nullptr, D, wL);
 }
 
 // Forward values of face f's local inputs.
@@ -137,7 +137,7 @@ __device__ int active_inputs(const DevCase &cs, int b, int act[U_N]) {
 }
 
 // Face stage: FA[i][f] = sum_v Dbar_v dD_v/du_i.
-template <bool VISCOUS>
+template <bool VISCOUS, int FX>
 __global__ void __launch_bounds__(128) k_face_adj(DevCase cs, DevMesh m, const double *__restrict__ W,
                                                   const double *__restrict__ G, const double *__restrict__ Lm,
                                                   const double *__restrict__ stale, const double *__restrict__ Rbar,
@@ -166,7 +166,7 @@ __global__ void __launch_bounds__(128) k_face_adj(DevCase cs, DevMesh m, const d
       in.u = u;
       for (int l = 0; l < kLanes; ++l) in.chunk[l] = (k0 + l < na) ? act[k0 + l] : -1;
       DA D[5], rhoR;
-      face_from_inputs<VISCOUS>(cs, m, f, n, A, b, pa, nb, in, D, rhoR);
+      face_from_inputs<VISCOUS, FX>(cs, m, f, n, A, b, pa, nb, in, D, rhoR);
       for (int l = 0; l < kLanes; ++l) {
         if (in.chunk[l] < 0) continue;
         double s = 0.;
@@ -180,7 +180,7 @@ __global__ void __launch_bounds__(128) k_face_adj(DevCase cs, DevMesh m, const d
 
 // Stale-density stage: an outlet face that read the right density of an
 // earlier face (cached_right_rho) hands that adjoint to the earlier face.
-template <bool VISCOUS>
+template <bool VISCOUS, int FX>
 __global__ void k_stale_adj(DevCase cs, DevMesh m, const double *__restrict__ W, const double *__restrict__ G,
                             const double *__restrict__ Lm, const double *__restrict__ stale, double *__restrict__ FA) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -214,7 +214,7 @@ __global__ void k_stale_adj(DevCase cs, DevMesh m, const double *__restrict__ W,
       in.u = u;
       for (int l = 0; l < kLanes; ++l) in.chunk[l] = (k0 + l < na) ? act[k0 + l] : -1;
       DA D[5], rhoR;
-      face_from_inputs<VISCOUS>(cs, m, g, n, A, b, pa, nb, in, D, rhoR);
+      face_from_inputs<VISCOUS, FX>(cs, m, g, n, A, b, pa, nb, in, D, rhoR);
       for (int l = 0; l < kLanes; ++l)
         if (in.chunk[l] >= 0 && rhoR.d[l] != 0.) atomicAdd(&FA[(size_t)in.chunk[l] * nf + g], sb * rhoR.d[l]);
     }
@@ -665,12 +665,12 @@ static void run_adjoint(fcfd_ctx *x, const double *Rbar_soa, unsigned int mask, 
   // reverse
   const int gf = (m.nf + 127) / 128, gc = (m.nc + 127) / 128;
   if (x->viscous)
-    k_face_adj<true><<<gf, 128, 0, s>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p, Rbar_soa, mask, dir[0], dir[1], dir[2], a.FA.p);
+    FCFD_BY_FLUX(x->cs.flux, k_face_adj<true, FX><<<gf, 128, 0, s>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p, Rbar_soa, mask, dir[0], dir[1], dir[2], a.FA.p));
   else
-    k_face_adj<false><<<gf, 128, 0, s>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p, Rbar_soa, mask, dir[0], dir[1], dir[2], a.FA.p);
+    FCFD_BY_FLUX(x->cs.flux, k_face_adj<false, FX><<<gf, 128, 0, s>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p, Rbar_soa, mask, dir[0], dir[1], dir[2], a.FA.p));
   if (m.n_outlet > 0) {
-    if (x->viscous) k_stale_adj<true><<<(m.n_outlet + 127) / 128, 128, 0, s>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p, a.FA.p);
-    else k_stale_adj<false><<<(m.n_outlet + 127) / 128, 128, 0, s>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p, a.FA.p);
+    if (x->viscous) FCFD_BY_FLUX(x->cs.flux, k_stale_adj<true, FX><<<(m.n_outlet + 127) / 128, 128, 0, s>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p, a.FA.p));
+    else FCFD_BY_FLUX(x->cs.flux, k_stale_adj<false, FX><<<(m.n_outlet + 127) / 128, 128, 0, s>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p, a.FA.p));
   }
   CK(cudaMemsetAsync(a.Wlim.p, 0, sizeof(double) * 5 * (size_t)m.nt, s));
   if (x->viscous)

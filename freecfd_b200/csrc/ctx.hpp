@@ -96,7 +96,7 @@ struct fcfd_ctx {
   // colour]: the neighbour across each interior face and the signed face
   DBuf<int> gs_nbr, gs_src;
   int gs_deg = 0;
-  DBuf<double> f_n, f_area, f_x, f_w, c_x, c_len, st_cof, st_self, st_recip, st_mirror, c_vol;
+  DBuf<double> f_n, f_area, f_x, f_w, c_x, c_len, st_cof, st_self, st_recip, st_mirror, c_vol, f_wall, f_diss;
   bool green_gauss = false;  // some cells take the Green-Gauss gradient
   // state arrays
   Pipe<double> p64;

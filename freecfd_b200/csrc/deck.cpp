@@ -245,7 +245,11 @@ fcfd_case *read_deck(const std::string &path) {
     if (fl == "AUSM+up") cs->flux = FLUX_AUSM_PLUS_UP;
     else if (fl == "Roe") cs->flux = FLUX_ROE;
     else if (fl == "vanLeer") cs->flux = FLUX_VAN_LEER;
-    else throw Error(FCFD_ERR_UNSUPPORTED, "convective flux " + fl + " is not on the B200 path (Roe, AUSM+up, vanLeer)");
+    else if (fl == "SD-SLAU") cs->flux = FLUX_SD_SLAU;
+    else if (fl == "SW") cs->flux = FLUX_SW;
+    else throw Error(FCFD_ERR_UNSUPPORTED, "convective flux " + fl + " is not on the B200 path (Roe, AUSM+up, vanLeer, SD-SLAU, SW)");
+    cs->wdiss = nss.d("walldissipation");
+    cs->bl_height = nss.d("BLheight");
     cs->Minf = ref.d("Mach");
     cs->hex_method = grad_method(grid.subs["gradients"].s("hexmethod"));
     cs->prism_method = grad_method(grid.subs["gradients"].s("prismmethod"));

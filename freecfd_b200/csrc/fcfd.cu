@@ -46,9 +46,9 @@ void launch_chain(fcfd_ctx *x, Pipe<S> &P, S *Rout, bool aos_out, S *mo, S *wo, 
   if (m.n_outlet > 0)
     k_outlet_rho<S><<<(m.n_outlet + 127) / 128, 128, 0, s>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p);
   if (x->viscous)
-    k_face_flux<S, true><<<(m.nf + 127) / 128, 128, 0, s>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p, (const S *)nullptr, P.D.p, mo, wo, x->err.p);
+    FCFD_BY_FLUX(x->cs.flux, k_face_flux<S, true, FX><<<(m.nf + 127) / 128, 128, 0, s>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p, (const S *)nullptr, P.D.p, mo, wo, x->err.p));
   else
-    k_face_flux<S, false><<<(m.nf + 127) / 128, 128, 0, s>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p, (const S *)nullptr, P.D.p, mo, wo, x->err.p);
+    FCFD_BY_FLUX(x->cs.flux, k_face_flux<S, false, FX><<<(m.nf + 127) / 128, 128, 0, s>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p, (const S *)nullptr, P.D.p, mo, wo, x->err.p));
   if (aos_out)
     k_gather<S, true><<<(m.nc + tb - 1) / tb, tb, 0, s>>>(m, P.D.p, Rout, x->ext.p, x->argx.p);
   else
@@ -187,6 +187,7 @@ int fcfd_ctx_create(const fcfd_mesh *mp, const fcfd_case *csp, int device, fcfd_
   d.Lref = m.length_scale; d.Cp = mt.Cp(); d.mu = mt.mu; d.lambda = mt.lambda; d.sut_mu_ref = mt.sut_mu_ref;
   d.sut_T_ref = mt.sut_T_ref; d.sut_S = mt.sut_S; d.Pr = mt.Pr; d.Pr_t = c.Pr_t; d.sutherland = mt.sutherland;
   d.prandtl = mt.prandtl; d.flux = c.flux; d.limiter = c.limiter; d.order = c.order; d.nbc = (int)c.bc.size();
+  d.wdiss = c.wdiss; d.bl_height = c.bl_height;
   bool fixed_q = false;
   for (size_t b = 0; b < c.bc.size(); ++b) {
     const BcRegion &r = c.bc[b];
@@ -224,6 +225,11 @@ int fcfd_ctx_create(const fcfd_mesh *mp, const fcfd_case *csp, int device, fcfd_
   x->st_index.upload(m.st_index); x->st_keys.upload(m.st_keys);
   x->st_cof.upload(soa(m.st_cof, nc, 7)); x->st_self.upload(soa(m.st_self, nc, 3));
   x->st_recip.upload(m.st_recip); x->st_mirror.upload(soa(m.st_mirror, nc, 3));
+  if (c.flux == FLUX_SW) {
+    if ((int)m.f_wall.size() != nf || (int)m.f_diss.size() != nf)
+      throw Error(FCFD_ERR_INPUT, "the Steger-Warming flux needs a mesh built with a Steger-Warming case (face wall distances)");
+    x->f_wall.upload(m.f_wall); x->f_diss.upload(m.f_diss);
+  }
   {
     std::vector<double> vol(m.c_volume.begin(), m.c_volume.begin() + nc);
     x->c_vol.upload(vol);
@@ -298,6 +304,7 @@ int fcfd_ctx_create(const fcfd_mesh *mp, const fcfd_case *csp, int device, fcfd_
   dm.c_len = x->c_len.p; dm.cf_index = x->cf_index.p; dm.cf_list = x->cf_list.p; dm.st_index = x->st_index.p;
   dm.st_keys = x->st_keys.p; dm.st_cof = x->st_cof.p; dm.st_self = x->st_self.p; dm.bface = x->bface.p;
   dm.st_recip = x->st_recip.p; dm.st_mirror = x->st_mirror.p; dm.c_vol = x->c_vol.p;
+  dm.f_wall = x->f_wall.p; dm.f_diss = x->f_diss.p;
   dm.outlet_faces = x->outlet.p; dm.n_outlet = x->n_outlet;
   rans_setup(x.get());  // k-omega BC values and buffers (turbulent cases only)
   CK(cudaDeviceSynchronize());
@@ -406,9 +413,9 @@ int fcfd_time_residual(fcfd_ctx *x, int reps, int flush_l2, double *out, int out
       k_outlet_rho<double><<<(m.n_outlet + 127) / 128, 128, 0, s>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p);
     CK(cudaEventRecord(t.ev[3], s));
     if (x->viscous)
-      k_face_flux<double, true><<<(m.nf + 127) / 128, 128, 0, s>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p, nullptr, P.D.p, nullptr, nullptr, x->err.p);
+      FCFD_BY_FLUX(x->cs.flux, k_face_flux<double, true, FX><<<(m.nf + 127) / 128, 128, 0, s>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p, nullptr, P.D.p, nullptr, nullptr, x->err.p));
     else
-      k_face_flux<double, false><<<(m.nf + 127) / 128, 128, 0, s>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p, nullptr, P.D.p, nullptr, nullptr, x->err.p);
+      FCFD_BY_FLUX(x->cs.flux, k_face_flux<double, false, FX><<<(m.nf + 127) / 128, 128, 0, s>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p, nullptr, P.D.p, nullptr, nullptr, x->err.p));
     CK(cudaEventRecord(t.ev[4], s));
     k_gather<double, false><<<(m.nc + tb - 1) / tb, tb, 0, s>>>(m, P.D.p, P.R.p, x->ext.p, x->argx.p);
     CK(cudaEventRecord(t.ev[5], s));
@@ -483,7 +490,8 @@ int fcfd_point_flux(int flux, const double *L, const double *R, const double *n,
   if (flux == FLUX_ROE) roe(c, a, b, n, F, wl);
   else if (flux == FLUX_VAN_LEER) vanleer(c, a, b, n, F, wl);
   else if (flux == FLUX_AUSM_PLUS_UP) ausm(c, a, b, n, F, wl);
-  else throw Error(FCFD_ERR_UNSUPPORTED, "unknown flux");
+  else if (flux == FLUX_SD_SLAU) sdslau(c, a, b, n, F, wl);
+  else throw Error(FCFD_ERR_UNSUPPORTED, "point flux: 1 Roe, 2 Van Leer, 3 AUSM+up, 4 SD-SLAU (Steger-Warming needs face wall data)");
   for (int k = 0; k < 5; ++k) out[k] = F[k];
   if (weightL) *weightL = wl;
   API_END

@@ -27,7 +27,7 @@ enum BcSpec { SP_RHO = 1, SP_P = 2, SP_T = 3, SP_STATE = 4 };
 // Options (src/navier_stokes/ns.h:38-52)
 enum Limiter { LIM_NONE = -1, LIM_VK = 1, LIM_BJ = 2, LIM_MINMOD = 3 };
 enum Order { ORDER_FIRST = 1, ORDER_SECOND = 2 };
-enum Flux { FLUX_ROE = 1, FLUX_VAN_LEER = 2, FLUX_AUSM_PLUS_UP = 3 };
+enum Flux { FLUX_ROE = 1, FLUX_VAN_LEER = 2, FLUX_AUSM_PLUS_UP = 3, FLUX_SD_SLAU = 4, FLUX_SW = 5 };
 enum GradMethod { GM_CURVILINEAR = 1, GM_LSQR = 2, GM_GREENGAUSS = 3 };
 enum Interp { IP_WTLI = 0, IP_IDW = 1, IP_SIMPLE = 2 };
 
@@ -60,6 +60,7 @@ struct fcfd_case {
   int dimension = 3;
   int flux = fcfd::FLUX_AUSM_PLUS_UP, limiter = fcfd::LIM_VK, order = fcfd::ORDER_SECOND;
   double limiter_threshold = 0, Minf = 1;
+  double wdiss = 0.3, bl_height = 0;  // Steger-Warming wall dissipation (ns.cc:76-77)
   int hex_method = fcfd::GM_CURVILINEAR, prism_method = fcfd::GM_CURVILINEAR, other_method = fcfd::GM_LSQR;
   int interp = fcfd::IP_WTLI, stencil_size = 2;
   fcfd::Material mat;
@@ -85,6 +86,7 @@ struct fcfd_mesh {
   std::vector<uint8_t> f_symmetry;
   // cells: interior [0,nc), ghosts [nc, nc+nb)
   std::vector<double> c_centroid, c_volume, c_length, c_wall;
+  std::vector<double> f_wall, f_diss;                         // face wall distance / dissipation factor (Steger-Warming only)
   std::vector<int32_t> c_bc;                                 // ghost -> bc index (-1 interior)
   std::vector<int32_t> cf_index, cf_list;                    // interior cell -> faces (ascending)
   std::vector<int32_t> nbr_index, nbr_list;                  // interior cell -> neighborCells

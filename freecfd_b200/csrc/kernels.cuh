@@ -115,6 +115,22 @@ template <class T> struct Mk<Dual<T>> { __host__ __device__ static Dual<T> of(do
 template <class T> __host__ __device__ __forceinline__ T tan_of(const Dual<T> &x) { return x.d; }
 
 // std::max / std::min semantics: max(a,b) = (a<b)?b:a, min(a,b) = (b<a)?b:a
+// Runs the statement with the compile-time flux selector FX of face_D bound
+// to the case's convective flux (4 SD-SLAU, 5 Steger-Warming, else 0).
+#define FCFD_BY_FLUX(flux, ...)                       \
+  do {                                                \
+    if ((flux) == 4) {                                \
+      constexpr int FX = 4;                           \
+      __VA_ARGS__;                                    \
+    } else if ((flux) == 5) {                         \
+      constexpr int FX = 5;                           \
+      __VA_ARGS__;                                    \
+    } else {                                          \
+      constexpr int FX = 0;                           \
+      __VA_ARGS__;                                    \
+    }                                                 \
+  } while (0)
+
 template <class S> __host__ __device__ __forceinline__ S smax(const S &a, const S &b) { return (a < b) ? b : a; }
 template <class S> __host__ __device__ __forceinline__ S smin(const S &a, const S &b) { return (b < a) ? b : a; }
 
@@ -134,6 +150,7 @@ struct DevCase {
   double gamma, R, Pref, Tref, Minf, K, Lref, Cp;
   double mu, lambda, sut_mu_ref, sut_T_ref, sut_S, Pr;
   double Pr_t;
+  double wdiss, bl_height;  // Steger-Warming wall dissipation and boundary-layer height
   int sutherland, prandtl, flux, limiter, order, viscous, nbc, frozen_limiter;
   int fast_grad, pad_;
   DevBC bc[kMaxBC];
@@ -154,6 +171,7 @@ struct DevMesh {
   const double *st_mirror;                 // [3][nc] summed symmetry-mirror weights
   const int *bface;                        // boundary faces in ghost order [nb]
   const int *outlet_faces;                 // outlet boundary faces [n_outlet]
+  const double *f_wall, *f_diss;           // [nf] wall distance, dissipation factor (Steger-Warming only)
   int n_outlet;
 };
 
@@ -878,6 +896,124 @@ __host__ __device__ __forceinline__ void vanleer(const DevCase &c, const FState<
   }
 }
 
+// SD-SLAU (ns_sd_slau.cc:37-94) in xyz.  alpha = 0 (ns_sd_slau.cc:47)
+// removes the alpha terms of B+ and B-.  The pressure sensor theta
+// (ns_sd_slau.cc:68-71) is identically 1: max_delta_p is |delta_p| itself
+// (ns_sd_slau.cc:64), so with x = |delta_p| / p_ave >= 0 the ratio
+// (Csd2 x + Csd1) / (x + Csd1), Csd2 = 10 > 1, is >= 1 after rounding too
+// (every step is monotone) and min(1, theta^2) returns the constant 1 for every
+// state with positive absolute pressure.  The speed-of-sound scale keeps the
+// reference's Mhat = min(1, sqrt(0.5 (|V_L|^2 + |V_R|^2) / a)) (a, not a^2).
+template <class S>
+__host__ __device__ __forceinline__ void sdslau(const DevCase &c, const FState<S> &L, const FState<S> &R, const double n[3], S F[5], S &wL) {
+  const S a = 0.5 * (L.a + R.a);
+  const S qL = L.V[0] * L.V[0] + L.V[1] * L.V[1] + L.V[2] * L.V[2];
+  const S qR = R.V[0] * R.V[0] + R.V[1] * R.V[1] + R.V[2] * R.V[2];
+  const S Mhat = smin(S(1.), S(sqrt(0.5 * (qL + qR) / a)));
+  const S chi = (1. - Mhat) * (1. - Mhat);
+  const S Mp = L.Vn / a, Mm = R.Vn / a;
+  const S Bp = (fabs(Mp) < 1.) ? S(0.25 * (2. - Mp) * (Mp + 1.) * (Mp + 1.)) : S((Mp > 0.) ? 1. : 0.);
+  const S Bm = (fabs(Mm) < 1.) ? S(0.25 * (2. + Mm) * (Mm - 1.) * (Mm - 1.)) : S((Mm < 0.) ? 1. : 0.);
+  const S pave = 0.5 * (L.p + R.p) + c.Pref;
+  const S dp = R.p - L.p;
+  S p = pave - 0.5 * (Bp - Bm) * dp + (1. - chi) * (Bp + Bm - 1.) * pave;
+  const S g = -smax(smin(Mp, S(0.)), S(-1.)) * smin(smax(Mm, S(0.)), S(1.));
+  const S aL = fabs(L.Vn), aR = fabs(R.Vn);
+  const S Vn = (L.rho * aL + R.rho * aR) / (L.rho + R.rho);
+  const S Vp = (1. - g) * Vn + g * aL;
+  const S Vm = (1. - g) * Vn + g * aR;
+  const S mdot = 0.5 * (L.rho * (L.Vn + Vp) + R.rho * (R.Vn - Vm) - smax(S(0.), S(1. - Vn / a)) * dp / a);
+  p = p - c.Pref;
+  F[0] = mdot;
+  const FState<S> &U = (mdot > 0.) ? L : R;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) F[1 + i] = mdot * U.V[i] + p * n[i];
+  F[4] = mdot * U.H;
+  wL = (mdot > 0.) ? S(1.) : S(0.);
+}
+
+// sqrt(x^2 + e^2) whose tangent is 0 where the value is 0 (|x| at x = e = 0
+// has no derivative; the value is the reference's)
+template <class S>
+__host__ __device__ __forceinline__ S hypot0(const S &q) {
+  return (q == 0.) ? S(0.) : S(sqrt(q));
+}
+
+// Steger-Warming flux-vector splitting with wall dissipation
+// (Stegger_Warming_flux, ns_stegger_warming.cc:23-145) in xyz.  Per signal
+// the reference forms Jacob = L diag(Lambda) R in the rotated frame at the
+// w-weighted state and adds Jacob Q of the upwind side.  Here the product is
+// applied right to left and the rotated rows are written with frame-free
+// vectors (u = weighted velocity, m = rho V of the upwind side, un = u.n):
+//   r0 = (a^2 - gs) Q0 + beta (u.m - Q4),  r3,4 = (gs -+ un a) Q0 +- a (m.n) - beta (u.m - Q4),
+//   rows 1-2 = the tangential part of d = m - u Q0,
+// then with s_k = Lambda_k r_k and st = Lambda_0 (d - n (d.n)):
+//   F0 = c,  Fm = c u + 0.5 a (s3 - s4) / a^2 n + st,
+//   F4 = eta s0 + u.st + 0.5 (H (s3 + s4) + a un (s3 - s4)) / a^2,
+//   c = (s0 + 0.5 (s3 + s4)) / a^2.
+// The pressure and temperature enter as stored (gauge values, as in the
+// reference); weightL ends as w, the value the second pass leaves.
+template <class S>
+__host__ __device__ __forceinline__ void sw(const DevCase &c, const FState<S> &L, const FState<S> &R, const double n[3],
+                                            double diss, double wall_d, S F[5], S &wL) {
+  const double alpha = 6.;
+  const double beta = c.gamma * c.R / c.Cp;
+  const S dpr = fabs(L.p - R.p) / smin(L.p, R.p);
+  const S w = 0.5 / (alpha * alpha * dpr * dpr + 1.);
+#pragma unroll
+  for (int k = 0; k < 5; ++k) F[k] = S(0.);
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const double sg = h ? -1. : 1.;
+    const S wl = h ? w : S(1. - w);
+    const S wr = 1. - wl;
+    const S p = wl * L.p + wr * R.p;
+    S u[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) u[i] = wl * L.V[i] + wr * R.V[i];
+    const S V2 = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
+    const S un = u[0] * n[0] + u[1] * n[1] + u[2] * n[2];
+    const S T = wl * L.T + wr * R.T;
+    const S rho = wl * L.rho + wr * R.rho;
+    const S a2 = (1. + beta) * p / rho;
+    const S a = sqrt(a2);
+    const S H = 0.5 * V2 + a2 / (c.gamma - 1.);
+    const S gs = c.R * T + beta * (0.5 * V2 - c.Cp * T / c.gamma);
+    const S eta = (beta * V2 - gs) / (beta * a2);
+    const S eps = (wall_d > c.bl_height) ? S(c.wdiss * (a + hypot0(V2))) : S(c.wdiss * diss * (a + fabs(un)));
+    const S e2 = eps * eps;
+    const S l0 = 0.5 * (un + sg * hypot0(S(un * un + e2)));
+    const S up = un + a, um = un - a;
+    const S l3 = 0.5 * (up + sg * hypot0(S(up * up + e2)));
+    const S l4 = 0.5 * (um + sg * hypot0(S(um * um + e2)));
+    const FState<S> &U = h ? R : L;
+    const S Q0 = U.rho, Q4 = U.rho * U.H - U.p;
+    S mm[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) mm[i] = U.rho * U.V[i];
+    const S um_ = u[0] * mm[0] + u[1] * mm[1] + u[2] * mm[2];
+    const S mn = mm[0] * n[0] + mm[1] * n[1] + mm[2] * n[2];
+    const S bq = beta * (um_ - Q4);
+    const S s0 = l0 * ((a2 - gs) * Q0 + bq);
+    const S s3 = l3 * ((gs - un * a) * Q0 + a * mn - bq);
+    const S s4 = l4 * ((gs + un * a) * Q0 - a * mn - bq);
+    S d[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) d[i] = mm[i] - u[i] * Q0;
+    const S dn = d[0] * n[0] + d[1] * n[1] + d[2] * n[2];
+    S st[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) st[i] = l0 * (d[i] - dn * n[i]);
+    const S cc = (s0 + 0.5 * (s3 + s4)) / a2;
+    const S cn = 0.5 * a * (s3 - s4) / a2;
+    F[0] = F[0] + cc;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) F[1 + i] = F[1 + i] + cc * u[i] + cn * n[i] + st[i];
+    F[4] = F[4] + eta * s0 + (u[0] * st[0] + u[1] * st[1] + u[2] * st[2]) + 0.5 * (H * (s3 + s4)) / a2 + un * cn;
+  }
+  wL = w;
+}
+
 // Sources of the u, v, w, T gradient rows (12 values per cell) that the
 // viscous flux reads: the stored cell gradients, or local copies (adjoint
 // kernels, where they are independent inputs).
@@ -903,13 +1039,21 @@ struct LocalGrad {
 // supplies the parent / neighbour gradient rows (GlobalGrad or LocalGrad);
 // its value type is S itself, or double when only the face states carry
 // tangents, as in the face-Jacobian kernel.
-template <class S, class GS, bool VISCOUS>
+//
+// FX selects the convective flux at compile time: 0 = Roe / Van Leer /
+// AUSM+up chosen at run time by cs.flux (ns.h:48-53 numbering), 4 = SD-SLAU,
+// 5 = Steger-Warming.  Kernels are instantiated per selector (FCFD_BY_FLUX)
+// so the larger SD-SLAU and Steger-Warming bodies add no registers to the
+// other fluxes' kernels.
+template <class S, class GS, bool VISCOUS, int FX>
 __device__ __forceinline__ void face_D(const DevCase &cs, const DevMesh &m, int f, const double n[3], double A, int b,
                                        int pa, int nb, const FState<S> &L, const FState<S> &R, const GS &gs,
                                        const typename GS::value_type *__restrict__ mu_t, S D[5], S &wL) {
   const int nf = m.nf, nt = m.nt;
   S F[5];
-  if (cs.flux == 1) roe(cs, L, R, n, F, wL);
+  if (FX == 4) sdslau(cs, L, R, n, F, wL);
+  else if (FX == 5) sw(cs, L, R, n, m.f_diss[f], m.f_wall[f], F, wL);
+  else if (cs.flux == 1) roe(cs, L, R, n, F, wL);
   else if (cs.flux == 2) vanleer(cs, L, R, n, F, wL);
   else ausm(cs, L, R, n, F, wL);
   S Fd[5] = {S(0.), S(0.), S(0.), S(0.), S(0.)};
@@ -982,7 +1126,7 @@ __device__ __forceinline__ void face_states(const DevCase &cs, const DevMesh &m,
 }
 
 // Face flux: reconstruction, BCs, inviscid + viscous flux; D = Fd - Fc.
-template <class S, bool VISCOUS>
+template <class S, bool VISCOUS, int FX>
 __global__ void __launch_bounds__(128) k_face_flux(DevCase cs, DevMesh m, const S *__restrict__ W, const S *__restrict__ G,
                                                    const S *__restrict__ Lm, const S *__restrict__ stale,
                                                    const S *__restrict__ mu_t, S *__restrict__ D, S *__restrict__ mdot_out,
@@ -997,7 +1141,7 @@ __global__ void __launch_bounds__(128) k_face_flux(DevCase cs, DevMesh m, const 
   face_states(cs, m, f, n, b, pa, nb, W, G, Lm, stale, L, R, err);
   S Dv[5], wL;
   const GlobalGrad<S> gs{G, m.nc, pa, nb};
-  face_D<S, GlobalGrad<S>, VISCOUS>(cs, m, f, n, A, b, pa, nb, L, R, gs, mu_t, Dv, wL);
+  face_D<S, GlobalGrad<S>, VISCOUS, FX>(cs, m, f, n, A, b, pa, nb, L, R, gs, mu_t, Dv, wL);
 #pragma unroll
   for (int v = 0; v < 5; ++v) D[v * nf + f] = Dv[v];
   if (mdot_out) mdot_out[f] = (-Dv[0]) / A;

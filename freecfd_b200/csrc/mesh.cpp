@@ -378,6 +378,30 @@ fcfd_mesh *build_mesh(const fcfd_raw_mesh &raw, fcfd_case &cs) {
       }
       m.c_wall[c] = best;
     }
+    // face wall distances and dissipation factors (set_bcs.cc:228-249), read
+    // by the Steger-Warming flux only: the first closest wall face gives fN
+    if (cs.flux == FLUX_SW) {
+      m.f_wall.assign(nf, 1.e20);
+      m.f_diss.assign(nf, 0.);
+#pragma omp parallel for schedule(static)
+      for (int f = 0; f < nf; ++f) {
+        int b = m.f_bc[f];
+        if (b < 0 || cs.bc[b].type != BC_WALL || cs.bc[b].kind == K_SLIP) {
+          double best = 1.e20;
+          P3 fN{0., 0., 0.}, x = fcent(f);
+          for (int w : walls) {
+            double d = mag(sub(x, fcent(w)));
+            if (best > d) { best = d; fN = fnormal(w); }
+          }
+          P3 nn = fnormal(f);
+          m.f_wall[f] = best;
+          m.f_diss[f] = 1. - std::fabs(fN.x * nn.x + fN.y * nn.y + fN.z * nn.z);
+        } else {
+          m.f_wall[f] = 0.;
+          m.f_diss[f] = 0.;
+        }
+      }
+    }
     // ---------------- cell length scales (main.cc:456-489)
     for (int c = 0; c < nc; ++c) {
       double ls = 1.e20;

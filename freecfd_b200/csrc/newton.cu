@@ -53,7 +53,7 @@ __device__ __forceinline__ void lift(const FState<double> &s, FState<D5> &o) {
 
 // Per face: JL = dD/dW_left and (interior faces) JR = dD/dW_right, [25][nf],
 // entry (i,k) = d D_i / d W_k at index (5i+k)*nf + f.
-template <bool VISCOUS>
+template <bool VISCOUS, int FX>
 __global__ void __launch_bounds__(128) k_face_jac(DevCase cs, DevMesh m, const double *__restrict__ W, const double *__restrict__ G,
                                                   const double *__restrict__ Lm, const double *__restrict__ stale,
                                                   double *__restrict__ JL, double *__restrict__ JR) {
@@ -77,7 +77,7 @@ __global__ void __launch_bounds__(128) k_face_jac(DevCase cs, DevMesh m, const d
     if (!apply_bc(cs, cs.bc[b], Ld, Rd, n, (int *)nullptr)) Rd.rho = D5(R.rho);
     finish(cs, Rd, n);
   }
-  face_D<D5, GlobalGrad<double>, VISCOUS>(cs, m, f, n, A, b, pa, nb, Ld, Rd, gs, (const double *)nullptr, D, wl);
+  face_D<D5, GlobalGrad<double>, VISCOUS, FX>(cs, m, f, n, A, b, pa, nb, Ld, Rd, gs, (const double *)nullptr, D, wl);
 #pragma unroll
   for (int i = 0; i < 5; ++i)
 #pragma unroll
@@ -85,7 +85,7 @@ __global__ void __launch_bounds__(128) k_face_jac(DevCase cs, DevMesh m, const d
   if (b < 0) {
     lift(L, Ld);
     seed(R, Rd, cs, n);
-    face_D<D5, GlobalGrad<double>, VISCOUS>(cs, m, f, n, A, b, pa, nb, Ld, Rd, gs, (const double *)nullptr, D, wl);
+    face_D<D5, GlobalGrad<double>, VISCOUS, FX>(cs, m, f, n, A, b, pa, nb, Ld, Rd, gs, (const double *)nullptr, D, wl);
 #pragma unroll
     for (int i = 0; i < 5; ++i)
 #pragma unroll
@@ -854,9 +854,9 @@ int fcfd_newton_solve(fcfd_ctx *x, double *W, const fcfd_newton_opts *o, fcfd_ne
       }
       // block-Jacobi preconditioner from the first-order face Jacobians
       if (x->viscous)
-        k_face_jac<true><<<(m.nf + 127) / 128, 128, 0, s>>>(x->cs, m, x->p64.W.p, x->p64.G.p, x->p64.Lm.p, x->p64.stale.p, ns.JL.p, ns.JR.p);
+        FCFD_BY_FLUX(x->cs.flux, k_face_jac<true, FX><<<(m.nf + 127) / 128, 128, 0, s>>>(x->cs, m, x->p64.W.p, x->p64.G.p, x->p64.Lm.p, x->p64.stale.p, ns.JL.p, ns.JR.p));
       else
-        k_face_jac<false><<<(m.nf + 127) / 128, 128, 0, s>>>(x->cs, m, x->p64.W.p, x->p64.G.p, x->p64.Lm.p, x->p64.stale.p, ns.JL.p, ns.JR.p);
+        FCFD_BY_FLUX(x->cs.flux, k_face_jac<false, FX><<<(m.nf + 127) / 128, 128, 0, s>>>(x->cs, m, x->p64.W.p, x->p64.G.p, x->p64.Lm.p, x->p64.stale.p, ns.JL.p, ns.JR.p));
       k_block_jacobi<<<gc, tb, 0, s>>>(x->cs, m, ns.Wn.p, ns.vol.p, ns.dt.p, ns.JL.p, ns.JR.p, ns.Minv.p, x->err.p, wref, ns.rowmag.p);
       if (ns.sweeps > 0) {
         const std::vector<int> &ci = x->color_index;

@@ -234,7 +234,11 @@ int fcfd_local_dt_cflmax_noalloc(const double *W, const double *length, int32_t 
 
 /* Point fluxes in the reference's rotated-frame signature
  * (roe_flux ns_roe.cc:25, AUSMplusUP_flux ns_ausm_plus_up.cc:35,
- * vanLeer_flux ns_vanleer.cc:25).  L/R = (p,u,v,w,T) face states,
+ * vanLeer_flux ns_vanleer.cc:25, SD_SLAU_flux ns_sd_slau.cc:37), flux
+ * numbered as ns.h:48-53 (1 Roe, 2 Van Leer, 3 AUSM+up, 4 SD-SLAU).  The
+ * Steger-Warming flux (5) needs the face's wall distance and dissipation
+ * factor and is not offered here (FCFD_ERR_UNSUPPORTED); it runs inside the
+ * residual.  L/R = (p,u,v,w,T) face states,
  * n = unit normal; out[5] = xyz flux per unit area (convective_face_flux
  * ns_convective_face_flux.cc:32-59 without the area factor).  Material is
  * given by gamma, R and the gauge offsets Pref/Tref. */

@@ -268,6 +268,7 @@ struct Oracle {
   // NavierStokes options (ns.cc:33-102)
   int order = SECOND, limiter_function = VK, flux = AUSM_PLUS_UP;
   double limiter_threshold = 0., Minf = 1.;
+  double wdiss = 0.3, bl_height = 0.;  // ns.cc:76-77
   int hex_method = LSQR, prism_method = LSQR, other_method = LSQR;
   int interp_method = WTLI, stencil_size = 2;
   // Variable<TYPE>::fixedonBC / bcValue for the NS variables (ns_set_bcs.cc)
@@ -806,8 +807,12 @@ static void setup_physics(Oracle &O, const std::string &deck_dir) {
   if (fl == "AUSM+up") O.flux = AUSM_PLUS_UP;
   else if (fl == "Roe") O.flux = ROE;
   else if (fl == "vanLeer") O.flux = VAN_LEER;
+  else if (fl == "SD-SLAU") O.flux = SD_SLAU;
+  else if (fl == "SW") O.flux = SW;
   else throw DeckError("convective flux " + fl + " is not on the restated path");
   O.Minf = O.input.section("reference").gd("Mach").value;
+  O.wdiss = ns.gd("walldissipation").value;
+  O.bl_height = ns.gd("BLheight").value;
   O.hex_method = method_of(g.sub("gradients").gs("hexmethod").value);
   O.prism_method = method_of(g.sub("gradients").gs("prismmethod").value);
   O.other_method = method_of(g.sub("gradients").gs("othermethod").value);
@@ -1503,6 +1508,118 @@ struct NS {
     }
   }
 
+  // ns_sd_slau.cc:37-94, term by term (Csd1 = 0.1, Csd2 = 10, alpha = 0;
+  // max_delta_p = |delta_p| as at ns_sd_slau.cc:64)
+  static double signum(const S &x) { double r = re_(x); return double((r > 0) - (r < 0)); }
+  void sdslau_flux(CellState<S> &L, CellState<S> &R, S fn[5], S &wL) {
+    const double Csd1 = 0.1, Csd2 = 10., Pref = O.material.Pref;
+    S a = 0.5 * (L.a + R.a);
+    S LV2 = L.V[0] * L.V[0] + L.V[1] * L.V[1] + L.V[2] * L.V[2];
+    S RV2 = R.V[0] * R.V[0] + R.V[1] * R.V[1] + R.V[2] * R.V[2];
+    S Mhat = smin(S(1.), S(sqrt(0.5 * (LV2 + RV2) / a)));
+    S chi = (1. - Mhat) * (1. - Mhat);
+    S Mplus = L.Vn[0] / a;
+    S Mminus = R.Vn[0] / a;
+    S Bplus, Bminus;
+    double alpha = 3. / 16. * (-4. + 5. * 0. * 0.);
+    alpha = 0.;
+    if (fabs(Mplus) < 1.) Bplus = 0.25 * (2. - Mplus) * (Mplus + 1.) * (Mplus + 1.) + alpha * Mplus * (Mplus - 1.) * (Mplus - 1.);
+    else Bplus = S(0.5 * (1. + signum(Mplus)));
+    if (fabs(Mminus) < 1.) Bminus = 0.25 * (2. + Mminus) * (Mminus - 1.) * (Mminus - 1.) - alpha * Mminus * (Mminus - 1.) * (Mminus - 1.);
+    else Bminus = S(0.5 * (1. + signum(-1. * Mminus)));
+    S ave_p = 0.5 * (L.p + R.p) + Pref;
+    S delta_p = R.p - L.p;
+    S p = ave_p - 0.5 * (Bplus - Bminus) * delta_p + (1. - chi) * (Bplus + Bminus - 1.) * ave_p;
+    S max_delta_p = fabs(delta_p);
+    S g = -1. * smax(smin(Mplus, S(0.)), S(-1.)) * smin(smax(Mminus, S(0.)), S(1.));
+    S Vn = (L.rho * fabs(L.Vn[0]) + R.rho * fabs(R.Vn[0])) / (L.rho + R.rho);
+    S Vnplus = (1. - g) * Vn + g * fabs(L.Vn[0]);
+    S Vnminus = (1. - g) * Vn + g * fabs(R.Vn[0]);
+    S theta = (Csd2 * fabs(delta_p) / ave_p + Csd1) / (max_delta_p / ave_p + Csd1);
+    theta = smin(S(1.), S(theta * theta));
+    S mdot = 0.5 * (L.rho * (L.Vn[0] + Vnplus) + R.rho * (R.Vn[0] - Vnminus) - theta * smax(S(0.), S(1. - Vn / a)) * delta_p / a);
+    p -= Pref;
+    fn[0] = mdot;
+    if (mdot > 0.) {
+      fn[1] = mdot * L.Vn[0] + p; fn[2] = mdot * L.Vn[1]; fn[3] = mdot * L.Vn[2]; fn[4] = mdot * L.H; wL = S(1.);
+    } else {
+      fn[1] = mdot * R.Vn[0] + p; fn[2] = mdot * R.Vn[1]; fn[3] = mdot * R.Vn[2]; fn[4] = mdot * R.H; wL = S(0.);
+    }
+  }
+
+  // sqrt whose complex-step tangent is 0 where the value is 0 (the kink of
+  // |x| at 0); the value is sqrt's
+  static S sqrt0(const S &q) { return re_(q) == 0. ? S(0.) : S(sqrt(q)); }
+
+  // ns_stegger_warming.cc:23-145, in the rotated frame with the explicit
+  // 5x5 products: Jacob = (L diag(Lambda)) R per signal, flux += Jacob Q.
+  void sw_flux(CellState<S> &L, CellState<S> &R, S fn[5], S &wL) {
+    const Face &gf = O.grid.face[face.index];
+    const double alpha = 6., RW = 8314.47215 / O.material.Mw, gam = O.material.gamma;
+    const double Cp = O.material.Cp();
+    const double beta = gam * RW / Cp;
+    for (int i = 0; i < 5; ++i) fn[i] = S(0.);
+    S deltap = fabs(L.p - R.p) / smin(L.p, R.p);
+    S w = 0.5 / (alpha * alpha * deltap * deltap + 1.);
+    for (int h = 0; h <= 1; ++h) {
+      double signal = std::pow(-1., h);
+      S weightL = (signal > 0.) ? S(1. - w) : w;
+      S weightR = 1. - weightL;
+      wL = weightL;
+      S p = weightL * L.p + weightR * R.p;
+      V3<S> V;
+      for (int i = 0; i < 3; ++i) V[i] = weightL * L.Vn[i] + weightR * R.Vn[i];
+      S V2 = sqrt0(V[0] * V[0] + V[1] * V[1] + V[2] * V[2]);
+      S Vmag = V2;
+      V2 = V2 * V2;
+      S T = weightL * L.T + weightR * R.T;
+      S rho = weightL * L.rho + weightR * R.rho;
+      S a = sqrt((1. + beta) * p / rho);
+      S a2 = a * a;
+      S H = 0.5 * V2 + a2 / (gam - 1.);
+      S gamma_s = RW * T + beta * (0.5 * V2 - Cp * T / gam);
+      S eta = (beta * V2 - gamma_s) / (beta * a2);
+      S Lm[5][5], Rm[5][5], Jac[5][5], Lam[5], Q[5];
+      for (int i = 0; i < 5; ++i) for (int j = 0; j < 5; ++j) { Lm[i][j] = S(0.); Rm[i][j] = S(0.); }
+      Lm[0][0] = 1.0 / a2;
+      Lm[0][3] = 0.5 / a2; Lm[0][4] = 0.5 / a2;
+      Lm[1][0] = V[0] / a2; Lm[2][0] = V[1] / a2; Lm[3][0] = V[2] / a2;
+      Lm[1][3] = 0.5 * (V[0] + a) / a2;
+      Lm[1][4] = 0.5 * (V[0] - a) / a2;
+      Lm[2][1] = S(1.);
+      Lm[2][3] = 0.5 * V[1] / a2; Lm[2][4] = Lm[2][3];
+      Lm[3][2] = S(1.);
+      Lm[3][3] = 0.5 * V[2] / a2; Lm[3][4] = Lm[3][3];
+      Lm[4][0] = eta; Lm[4][1] = V[1]; Lm[4][2] = V[2];
+      Lm[4][3] = 0.5 * (H + a * V[0]) / a2;
+      Lm[4][4] = 0.5 * (H - a * V[0]) / a2;
+      S eps;
+      if (gf.closest_wall_distance > O.bl_height) eps = O.wdiss * (a + Vmag);
+      else eps = O.wdiss * gf.dissipation_factor * (a + fabs(V[0]));
+      Lam[0] = 0.5 * (V[0] + signal * sqrt0(V[0] * V[0] + eps * eps));
+      Lam[1] = Lam[0]; Lam[2] = Lam[0];
+      Lam[3] = 0.5 * (V[0] + a + signal * sqrt0((V[0] + a) * (V[0] + a) + eps * eps));
+      Lam[4] = 0.5 * (V[0] - a + signal * sqrt0((V[0] - a) * (V[0] - a) + eps * eps));
+      for (int i = 0; i < 5; ++i) for (int j = 0; j < 5; ++j) Lm[i][j] = Lm[i][j] * Lam[j];
+      Rm[0][0] = a2 - gamma_s; Rm[0][1] = beta * V[0]; Rm[0][2] = beta * V[1]; Rm[0][3] = beta * V[2]; Rm[0][4] = S(-beta);
+      Rm[1][0] = -1. * V[1]; Rm[1][2] = S(1.);
+      Rm[2][0] = -1. * V[2]; Rm[2][3] = S(1.);
+      Rm[3][0] = gamma_s - V[0] * a; Rm[3][1] = a - beta * V[0]; Rm[3][2] = -beta * V[1]; Rm[3][3] = -beta * V[2];
+      Rm[4][0] = gamma_s + V[0] * a; Rm[4][1] = -1. * a - beta * V[0]; Rm[4][2] = -beta * V[1]; Rm[4][3] = -beta * V[2];
+      Rm[3][4] = S(beta); Rm[4][4] = S(beta);
+      for (int i = 0; i < 5; ++i)
+        for (int j = 0; j < 5; ++j) {
+          Jac[i][j] = S(0.);
+          for (int k = 0; k < 5; ++k) Jac[i][j] += Lm[i][k] * Rm[k][j];
+        }
+      CellState<S> &U = (signal > 0.) ? L : R;
+      Q[0] = U.rho;
+      Q[1] = U.rho * U.Vn[0]; Q[2] = U.rho * U.Vn[1]; Q[3] = U.rho * U.Vn[2];
+      Q[4] = U.rho * U.H - U.p;
+      for (int i = 0; i < 5; ++i) for (int j = 0; j < 5; ++j) fn[i] += Jac[i][j] * Q[j];
+    }
+  }
+
   // ns_vanleer.cc:25-66
   void vanleer_flux(CellState<S> &L, CellState<S> &R, S fn[5], S &wL) {
     double Gamma = O.material.gamma, Pref = O.material.Pref;
@@ -1537,6 +1654,8 @@ struct NS {
     S &wL = F.weightL[face.index];
     if (O.flux == ROE) roe_flux(L, R, fn, wL);
     else if (O.flux == VAN_LEER) vanleer_flux(L, R, fn, wL);
+    else if (O.flux == SD_SLAU) sdslau_flux(L, R, fn, wL);
+    else if (O.flux == SW) sw_flux(L, R, fn, wL);
     else ausm_flux(L, R, fn, wL);
     const Vec3 &n = face.normal, &t1 = face.tangent1, &t2 = face.tangent2;
     flux[0] = fn[0] * face.area;

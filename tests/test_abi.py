@@ -34,7 +34,7 @@ def test_bad_deck_returns_status(fb, tmp_path):
 def test_unsupported_flux_is_reported(fb, tmp_path):
     import pytest
     from freecfd_b200 import cases
-    c = cases.wedge_case(ni=4, nj=3, flux="SD-SLAU")
+    c = cases.wedge_case(ni=4, nj=3, flux="HLLC")
     with pytest.raises(fb.FcfdError) as e:
         fb.Case(c.write_deck(str(tmp_path)))
     assert e.value.code == 7

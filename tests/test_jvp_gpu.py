@@ -22,7 +22,8 @@ def _dirs(shape, seed, n):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("family", sorted(SMALL))
-@pytest.mark.parametrize("flux,limiter", [("Roe", "vk"), ("AUSM+up", "minmod"), ("vanLeer", "vk"), ("Roe", "none")])
+@pytest.mark.parametrize("flux,limiter", [("Roe", "vk"), ("AUSM+up", "minmod"), ("vanLeer", "vk"), ("Roe", "none"),
+                                          ("SD-SLAU", "vk"), ("SW", "vk"), ("SW", "minmod")])
 def test_jvp_matches_complex_step(family, flux, limiter, oracle_mod, fb):
     case = SMALL[family](flux=flux, limiter=limiter)
     o, cs, m = build_pair(case, oracle_mod, fb)
@@ -90,9 +91,10 @@ def test_fp32_tangent_chain(family, oracle_mod, fb):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("family", sorted(ELEMENTS))
-def test_jvp_tets_pyramids(family, oracle_mod, fb):
+@pytest.mark.parametrize("flux", ["Roe", "SD-SLAU", "SW"])
+def test_jvp_tets_pyramids(family, flux, oracle_mod, fb):
     """Tangent kernels on tetrahedra and pyramids vs the complex step."""
-    case = ELEMENTS[family](flux="Roe", limiter="vk")
+    case = ELEMENTS[family](flux=flux, limiter="vk")
     o, cs, m = build_pair(case, oracle_mod, fb)
     ns = fb.NavierStokes(m, cs, 0)
     scale = np.abs(case.state).max(axis=0)

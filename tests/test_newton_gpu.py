@@ -84,3 +84,21 @@ def test_newton_reports_nonconvergence(wedge, fb):
     with pytest.raises(fb.FcfdError) as e:
         ns.newton_solve(case.state, tol=1e-10, max_newton=3)
     assert e.value.code == 4
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("flux", ["SD-SLAU", "SW"])
+@pytest.mark.parametrize("label,opts", [("fd64", dict(jvp=False)),
+                                        ("mixed_fp32_tangent", dict(jvp=True, fp32_jvp=True, fp32_krylov=True))])
+def test_newton_other_fluxes(flux, label, opts, oracle_mod, fb):
+    """SD-SLAU and Steger-Warming through the whole Newton path (their face
+    Jacobian kernels in the block preconditioner, tangent kernels in J.v):
+    laminar cylinder 48x24, unlimited second order."""
+    case = cases.cylinder_case(ntheta=48, nr=24, limiter="none", flux=flux)
+    o, cs, m = build_pair(case, oracle_mod, fb)
+    ns = fb.NavierStokes(m, cs, 0)
+    W, rep = ns.newton_solve(case.state, **KW, **opts)
+    assert rep["status"] == 0, rep
+    r0 = np.linalg.norm(o.residual(case.state)[:, 0])
+    r = np.linalg.norm(o.residual(W)[:, 0])
+    assert r <= 1e-9 * r0, (r, r0)

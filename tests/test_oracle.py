@@ -7,7 +7,9 @@ itself relies on and by identities of the discretisation:
   * LSQ gradient exactness for a linear field (the reference's gradient-test
     IC mode, ns.cc:161-185) — checked through the stored gradient weights;
   * flux consistency F(U,U) = physical flux (ns_roe.cc, ns_ausm_plus_up.cc,
-    ns_vanleer.cc);
+    ns_vanleer.cc, ns_sd_slau.cc, ns_stegger_warming.cc): a uniform state
+    leaves every cell away from non-symmetry boundaries with a zero residual up to the
+    rounding of its cancelling face fluxes;
   * a closed symmetry box at rest has zero residual;
   * conservation: interior faces cancel in the sum of residuals;
   * committed golden vectors (tests/golden/) generated by
@@ -93,6 +95,66 @@ def test_mass_conservation(family, oracle_mod):
     expect = -(out["mdot"][bnd] * A[bnd]).sum()
     scale = np.abs(out["mdot"] * A).sum()
     assert abs(total - expect) <= 1e-12 * scale
+
+
+@pytest.mark.parametrize("flux", ["Roe", "AUSM+up", "vanLeer", "SD-SLAU", "SW"])
+@pytest.mark.parametrize("family", ["wedge", "hypersonic", "plate"])
+def test_freestream_preservation(family, flux, oracle_mod):
+    """Flux consistency: with a uniform state every face flux is the physical
+    flux of that state, so cells with no boundary face have R = 0 up to the
+    rounding of their cancelling face fluxes (Steger-Warming: A+ Q + A- Q =
+    A Q = F(Q), the eigen-split of the perfect-gas flux Jacobian with
+    beta = gamma R / Cp = gamma - 1).  First order: the LSQ map's dropped
+    symmetry-mirror values (lsqr_grad_map.cc:66-96) give a uniform field
+    non-zero gradients next to symmetry planes, which second order would
+    reconstruct into the face states."""
+    from tests.util import flux_scale
+    case = (SMALL[family](flux=flux, order="first") if family == "wedge"
+            else SMALL[family](flux=flux, ns_extra=" order=first;"))
+    o = oracle_mod.Oracle(case)
+    W = np.tile(np.asarray(case.freestream), (o.nc, 1))
+    R = o.residual(W)
+    conn = o.connectivity()
+    nc = o.nc
+    fp, fn, fbc = conn["face_parent"], conn["face_neighbor"], conn["face_bc"]
+    # symmetry ghosts mirror the uniform state onto itself (V tangential);
+    # other ghosts (walls, inlets, outlets) differ from it and enter a cell's
+    # residual through its boundary faces and through the LSQ gradients of
+    # the cells on either side of its faces
+    real = np.array([b >= 0 and not _is_sym(case, b) for b in fbc])
+    bad_ghost = set(fn[real].tolist())
+    gi, gk = conn["grad_index"], conn["grad_keys"]
+    dirty = np.array([any(k in bad_ghost for k in gk[gi[c]:gi[c + 1]]) for c in range(nc)])
+    inner = np.ones(nc, bool)
+    for f in range(len(fp)):
+        if real[f]:
+            inner[fp[f]] = False
+        elif fbc[f] < 0 and (dirty[fp[f]] or dirty[fn[f]]):
+            inner[fp[f]] = inner[fn[f]] = False
+    inner &= ~dirty
+    assert inner.sum() > 0
+    scale = flux_scale(case, o.geometry())
+    assert (np.abs(R[inner]).max(axis=0) <= 1e-11 * scale).all(), np.abs(R[inner]).max(axis=0) / scale
+
+
+@pytest.mark.parametrize("flux", ["SD-SLAU", "SW"])
+@pytest.mark.parametrize("family", ["cylinder", "hypersonic"])
+def test_complex_step_other_fluxes(family, flux, oracle_mod):
+    """SD-SLAU and Steger-Warming: complex step vs central differences on a
+    state with v perturbed (no face sits on the |V.n| = 0 kink) and an
+    unlimited reconstruction."""
+    from tests.test_vjp_gpu import _generic
+    case = SMALL[family](flux=flux, limiter="none")
+    o = oracle_mod.Oracle(case)
+    W = _generic(case)
+    rng = np.random.default_rng(7)
+    dW = rng.standard_normal(W.shape) * np.abs(W).max(axis=0) * np.array([1.0, 1.0, 1.0, 0.0, 1.0])
+    jv = o.residual_cstep(W, dW)
+    h = 1e-7
+    fd = (o.residual(W + h * dW) - o.residual(W - h * dW)) / (2 * h)
+    cols = [0, 1, 2, 4]
+    scale = np.abs(jv[:, cols]).max(axis=0)
+    assert (np.abs(jv - fd)[:, cols].max(axis=0) / scale).max() < 1e-5
 
 
 def test_golden_vectors(oracle_mod):

@@ -33,7 +33,8 @@ def test_rans_bc_values(oracle_mod, fb):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("size,limiter,flux", [((8, 4, 2), "vk", "Roe"), ((24, 12, 3), "vk", "Roe"),
-                                               ((24, 12, 3), "none", "AUSM+up"), ((24, 12, 3), "minmod", "vanLeer")])
+                                               ((24, 12, 3), "none", "AUSM+up"), ((24, 12, 3), "minmod", "vanLeer"),
+                                               ((24, 12, 3), "vk", "SD-SLAU"), ((24, 12, 3), "vk", "SW")])
 def test_rans_residual_parity(size, limiter, flux, oracle_mod, fb):
     ni, nj, nk = size
     case = _plate(ni=ni, nj=nj, nk=nk, limiter=limiter, flux=flux)
@@ -41,8 +42,10 @@ def test_rans_residual_parity(size, limiter, flux, oracle_mod, fb):
     ns = fb.NavierStokes(m, cs, 0)
     R, RK = ns.rans_residual(case.state, case.kstate)
     Ro, RKo = o.rans_residual(case.state, case.kstate)
-    assert res_err(R, Ro).max() <= 1e-12
-    assert _krel(RK, RKo).max() <= 1e-12, _krel(RK, RKo)
+    # Steger-Warming: split-flux rounding grows like 1/M (test_residual_gpu.tol)
+    t = 1e-11 if flux == "SW" else 1e-12
+    assert res_err(R, Ro).max() <= t
+    assert _krel(RK, RKo).max() <= t, _krel(RK, RKo)
     # the eddy viscosity changes the NS residual (it is really coupled)
     assert np.abs(R - ns.residual(case.state)).max() > 1e-6 * np.abs(R).max()
 

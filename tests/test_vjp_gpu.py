@@ -50,7 +50,9 @@ def _jacobian_cs(o, W):
 @pytest.mark.parametrize("family,flux,limiter", [("wedge", "Roe", "vk"), ("wedge", "AUSM+up", "minmod"),
                                                  ("wedge", "vanLeer", "bj"), ("cylinder", "Roe", "vk"),
                                                  ("cylinder", "AUSM+up", "none"), ("hypersonic", "AUSM+up", "minmod"),
-                                                 ("plate", "Roe", "vk")])
+                                                 ("plate", "Roe", "vk"), ("wedge", "SD-SLAU", "minmod"),
+                                                 ("cylinder", "SW", "vk"), ("hypersonic", "SW", "none"),
+                                                 ("plate", "SD-SLAU", "vk")])
 def test_vjp_matches_jacobian_transpose(family, flux, limiter, oracle_mod, fb):
     case = TINY[family](flux=flux, limiter=limiter)
     o, cs, m = build_pair(case, oracle_mod, fb)
