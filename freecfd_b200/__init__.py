@@ -8,7 +8,7 @@ C ABI in include/fcfd.h.  Importing this package loads libfcfd_b200.so; there
 is no CPU fallback.
 """
 from ._lib import FcfdError, LIB_PATH, build, lib  # noqa: F401
-from .solver import Case, Mesh, NavierStokes, point_flux  # noqa: F401
+from .solver import Case, Mesh, NavierStokes, point_flux, read_restart, write_restart  # noqa: F401
 from . import cases  # noqa: F401
 
 FLUX = {"Roe": 1, "vanLeer": 2, "AUSM+up": 3, "SD-SLAU": 4, "SW": 5}

@@ -26,6 +26,7 @@ EXPORTED = [
     "fcfd_mesh_lsq",
     "fcfd_ctx_create", "fcfd_ctx_destroy", "fcfd_ctx_set_exact_gradients", "fcfd_residual", "fcfd_last_stages", "fcfd_local_dt",
     "fcfd_time_residual", "fcfd_point_flux", "fcfd_jvp", "fcfd_vjp", "fcfd_drag", "fcfd_rans_residual", "fcfd_rans_bcs", "fcfd_time_rans", "fcfd_newton_solve", "fcfd_local_dt_cflmax_noalloc",
+    "fcfd_run", "fcfd_restart_write", "fcfd_restart_read",
 ]
 
 
@@ -49,6 +50,18 @@ class _RawMesh(ctypes.Structure):
                 ("n_cells", ctypes.c_int32), ("conn_index", ctypes.POINTER(ctypes.c_int32)),
                 ("conn", ctypes.POINTER(ctypes.c_int32)), ("n_bc", ctypes.c_int32),
                 ("bc_index", ctypes.POINTER(ctypes.c_int32)), ("bc_nodes", ctypes.POINTER(ctypes.c_int32))]
+
+
+class RunOpts(ctypes.Structure):
+    _fields_ = [("work_dir", ctypes.c_char_p), ("restart_step", ctypes.c_int32), ("max_steps", ctypes.c_int32),
+                ("jvp_mode", ctypes.c_int32), ("fp32_krylov", ctypes.c_int32), ("precond_sweeps", ctypes.c_int32),
+                ("echo", ctypes.c_int32)]
+
+
+class RunReport(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int32), ("steps", ctypes.c_int32), ("krylov_iterations", ctypes.c_int32),
+                ("pad", ctypes.c_int32), ("time", ctypes.c_double), ("res", ctypes.c_double),
+                ("wall_seconds", ctypes.c_double)]
 
 
 class NewtonOpts(ctypes.Structure):
@@ -102,6 +115,11 @@ def _load():
     L.fcfd_local_dt_cflmax_noalloc.argtypes = [vp, vp, ctypes.c_int32, ctypes.c_double, ctypes.c_double,
                                                 ctypes.c_double, ctypes.c_double, ctypes.c_double, vp, vp]
     L.fcfd_time_residual.argtypes = [vp, ctypes.c_int, ctypes.c_int, dp, ctypes.c_int]
+    L.fcfd_run.argtypes = [vp, dp, ctypes.POINTER(RunOpts), ctypes.POINTER(RunReport)]
+    L.fcfd_restart_write.argtypes = [ctypes.c_char_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_double, dp, dp,
+                                     ctypes.c_int32, ctypes.c_int32, dp, dp, dp, dp]
+    L.fcfd_restart_read.argtypes = [ctypes.c_char_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, dp, dp, dp,
+                                    dp, dp, dp]
     L.fcfd_point_flux.argtypes = [ctypes.c_int, dp, dp, dp, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                   ctypes.c_double, ctypes.c_double, dp, dp]
     for name in EXPORTED:

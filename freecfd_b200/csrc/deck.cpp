@@ -74,6 +74,7 @@ struct Block {
   std::map<std::string, D> dv;
   std::map<std::string, S> sv;
   std::map<std::string, V> vv;
+  std::map<std::string, std::vector<std::string>> slv;     // string lists, split at ','
   std::string where;
 
   void need(const std::string &k) const { throw Error(FCFD_ERR_INPUT, "required input entry " + where + " -> " + k + " could not be found"); }
@@ -109,6 +110,17 @@ struct Block {
     for (auto &r : slreg) {
       bool f = take(text, r.first + "=[", "];", val, true, "({;");
       if (!f && r.second) need(r.first);
+      std::vector<std::string> items;
+      if (f) {
+        size_t b = 0;
+        for (;;) {
+          size_t e = val.find(',', b);
+          items.push_back(val.substr(b, e == std::string::npos ? std::string::npos : e - b));
+          if (e == std::string::npos) break;
+          b = e + 1;
+        }
+      }
+      slv[r.first] = items;
     }
   }
   double d(const std::string &k) const { return dv.at(k).v; }
@@ -164,7 +176,54 @@ int grad_method(const std::string &s) {
   return GM_CURVILINEAR;
 }
 
+// timemarching and pseudotime sections (read_inputs.cc:152-176) and the step
+// type logic of set_time_step_options (time_step.cc:25-60)
+TimeMarching parse_time_marching(std::string &text) {
+  const bool req = true, opt = false;
+  Sec tm;
+  tm.where = "timemarching";
+  tm.sreg = {{"integrator", {opt, "backwardEuler"}}, {"schedulefile", {opt, "none"}}};
+  tm.dreg = {{"stepsize", {opt, 1.}}, {"CFLmax", {opt, 1000.}}, {"CFLlocal", {opt, 1000.}}};
+  tm.ireg = {{"numberofsteps", {req, 0}}, {"updatefrequency", {opt, 1000000}}};
+  Sub ramp; ramp.dreg = {{"initial", {opt, 1.}}, {"growth", {opt, 1.2}}};
+  tm.subs = {{"ramp", ramp}};
+  tm.read_from(text, "timemarching", true);
+  Sec ps;
+  ps.where = "pseudotime";
+  ps.sreg = {{"preconditioner", {opt, "none"}}};
+  ps.dreg = {{"residualtolerance", {opt, 1e-8}}, {"stepsize", {opt, 1.}}, {"CFLmax", {opt, 1000.}}, {"CFLlocal", {opt, 1000.}}};
+  ps.ireg = {{"numberofsteps", {opt, 1}}, {"updatefrequency", {opt, 1000000}}};
+  Sub psramp; psramp.dreg = {{"initial", {opt, 1.}}, {"growth", {opt, 1.2}}};
+  ps.subs = {{"ramp", psramp}};
+  ps.read_from(text, "pseudotime", false);
+  TimeMarching t;
+  t.n_steps = tm.i("numberofsteps");
+  t.update_freq = tm.i("updatefrequency");
+  t.ramp = tm.subs["ramp"].found;
+  t.ramp_initial = tm.subs["ramp"].d("initial");
+  t.ramp_growth = tm.subs["ramp"].d("growth");
+  t.stepsize = tm.d("stepsize");
+  t.cfl_max = tm.d("CFLmax");
+  t.cfl_local = tm.d("CFLlocal");
+  if (tm.has("stepsize")) t.type = TS_FIXED;
+  if (tm.has("CFLmax")) {
+    if (t.type == TS_FIXED) throw Error(FCFD_ERR_INPUT, "input entry timemarching -> CFLmax can't be specified together with stepsize");
+    t.type = TS_CFL_MAX;
+  } else if (tm.has("CFLlocal")) {
+    if (t.type == TS_FIXED) throw Error(FCFD_ERR_INPUT, "input entry timemarching -> CFLlocal can't be specified together with stepsize");
+    t.type = TS_CFL_LOCAL;
+  }
+  if (tm.has_s("schedulefile")) t.schedule_file = tm.s("schedulefile");
+  t.ps_steps = ps.i("numberofsteps");
+  return t;
+}
+
 }  // namespace
+
+TimeMarching read_time_marching(const std::string &path) {
+  std::string text = clean(slurp(path));
+  return parse_time_marching(text);
+}
 
 fcfd_case *read_deck(const std::string &path) {
   const bool req = true, opt = false;
@@ -223,17 +282,23 @@ fcfd_case *read_deck(const std::string &path) {
   if (ngrids > 1) throw Error(FCFD_ERR_UNSUPPORTED, "multi-grid decks are outside the residual path");
   grid.read_from(text, "grid_1", true);
 
-  Sec tm;
-  tm.where = "timemarching";
-  tm.sreg = {{"integrator", {opt, "backwardEuler"}}, {"schedulefile", {opt, "none"}}};
-  tm.dreg = {{"stepsize", {opt, 1.}}, {"CFLmax", {opt, 1000.}}, {"CFLlocal", {opt, 1000.}}};
-  tm.ireg = {{"numberofsteps", {req, 0}}, {"updatefrequency", {opt, 1000000}}};
-  Sub ramp; ramp.dreg = {{"initial", {opt, 1.}}, {"growth", {opt, 1.2}}};
-  tm.subs = {{"ramp", ramp}};
-  tm.read_from(text, "timemarching", true);
+  const TimeMarching tmo = parse_time_marching(text);
 
   auto cs = new fcfd_case();
   try {
+    cs->tm = tmo;
+    cs->deck_path = path;
+    {
+      const Sub &wo = grid.subs["writeoutput"];
+      cs->restart_freq = wo.i("restartfrequency");
+      cs->load_freq = wo.i("loadfrequency");
+      for (int k = 0; k < 3; ++k) cs->moment_center[k] = wo.vv.at("momentcenter").v[k];
+      for (const std::string &b : wo.slv.at("includebcs")) cs->load_bcs.push_back(std::atoi(b.c_str()) - 1);
+      const Sub &nsl = grid.subs["navierstokes"];
+      cs->lin_rtol = nsl.d("relativetolerance");
+      cs->lin_abstol = nsl.d("absolutetolerance");
+      cs->lin_maxits = nsl.i("maximumiterations");
+    }
     cs->dimension = grid.i("dimension");
     const Sub &nss = grid.subs["navierstokes"];
     const std::string &lim = nss.s("limiter");
@@ -257,10 +322,10 @@ fcfd_case *read_deck(const std::string &path) {
     const std::string &im = grid.subs["interpolation"].s("method");
     cs->interp = im == "idw" ? IP_IDW : im == "simple" ? IP_SIMPLE : IP_WTLI;
     cs->stencil_size = grid.subs["interpolation"].i("stencilsize");
-    cs->has_cfl_max = tm.has("CFLmax");
-    cs->has_cfl_local = tm.has("CFLlocal");
-    cs->cfl_max = tm.d("CFLmax");
-    cs->cfl_local = tm.d("CFLlocal");
+    cs->has_cfl_max = tmo.type == TS_CFL_MAX;
+    cs->has_cfl_local = tmo.type == TS_CFL_LOCAL;
+    cs->cfl_max = tmo.cfl_max;
+    cs->cfl_local = tmo.cfl_local;
     const Sub &ts = grid.subs["turbulence"];
     cs->turbulent = ts.found;
     cs->turb_model = ts.s("model");

@@ -54,6 +54,22 @@ struct Material {
   double Cp() const { return gamma * R / (gamma - 1.); }
 };
 
+// Time marching options (read_inputs.cc:152-176, set_time_step_options
+// time_step.cc:25-67): step type, CFL ramp, schedule file, pseudo-time steps.
+enum { TS_NONE = 0, TS_FIXED = 1, TS_CFL_MAX = 2, TS_CFL_LOCAL = 3 };
+struct TimeMarching {
+  int type = TS_NONE;
+  double stepsize = 1., cfl_max = 1000., cfl_local = 1000.;
+  bool ramp = false;
+  double ramp_initial = 1., ramp_growth = 1.2;
+  int n_steps = 0, update_freq = 1000000;
+  std::string schedule_file;  // empty: none
+  int ps_steps = 1;           // pseudotime -> numberofsteps (dual time stepping when > 1)
+};
+// Parses the timemarching / pseudotime sections of a deck file (also used to
+// re-read them every `updatefrequency` steps, update_time_step_options).
+TimeMarching read_time_marching(const std::string &path);
+
 }  // namespace fcfd
 
 struct fcfd_case {
@@ -67,6 +83,15 @@ struct fcfd_case {
   std::vector<fcfd::BcRegion> bc;
   double cfl_max = 1000, cfl_local = 1000;
   bool has_cfl_max = false, has_cfl_local = false;
+  // driver options: time marching, output frequencies (main.cc:227-249), the
+  // linear-solver tolerances of navierstokes (ns.cc:37-39), the deck's path
+  fcfd::TimeMarching tm;
+  int restart_freq = 1000000, load_freq = 1000000;
+  double moment_center[3] = {0., 0., 0.};
+  std::vector<int> load_bcs;  // writeoutput -> includebcs, 0-based
+  double lin_rtol = 1e-6, lin_abstol = 1e-12;
+  int lin_maxits = 10;
+  std::string deck_path;
   // turbulence (rans.cc:48-70)
   bool turbulent = false;
   std::string turb_model;

@@ -17,9 +17,14 @@
 //   * GMRES(m) with right preconditioning; Gram-Schmidt (classical, applied
 //     twice) accumulates every dot product in FP64 with a fixed reduction
 //     order, so a solve is bit-reproducible.
+#include <sys/stat.h>
+
 #include <chrono>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
+#include <fstream>
+#include <string>
 #include <vector>
 
 #include "ctx.hpp"
@@ -677,7 +682,7 @@ static void apply_prec(fcfd_ctx *x, NewtonState &ns, const T *v, T *z, const Row
 // Right-preconditioned GMRES(m) with up to `cycles` restarts.
 template <class T>
 static void gmres(fcfd_ctx *x, NewtonState &ns, Krylov<T> &K, int mode, double rtol, double *dW, int &iters, double &relres,
-                  const RowScale &rs) {
+                  const RowScale &rs, double abstol = 0.) {
   const int n = K.n, m = K.m, nc = K.nc;
   cudaStream_t s = x->stream;
   const int tb = 256, gn = (n + tb - 1) / tb, gc = (nc + tb - 1) / tb;
@@ -743,7 +748,7 @@ static void gmres(fcfd_ctx *x, NewtonState &ns, Krylov<T> &K, int mode, double r
       k = j + 1;
       ++iters;
       relres = std::fabs(g[j + 1]) / bnorm;
-      if (relres <= rtol || !(hn > 0.)) { done = true; break; }
+      if (relres <= rtol || std::fabs(g[j + 1]) <= abstol || !(hn > 0.)) { done = true; break; }
     }
     std::vector<double> y(k, 0.);
     for (int i = k - 1; i >= 0; --i) {
@@ -762,6 +767,205 @@ static void gmres(fcfd_ctx *x, NewtonState &ns, Krylov<T> &K, int mode, double r
   CK(cudaGetLastError());
 }
 
+// Buffers of the implicit solve; volumes uploaded.
+static void alloc_state(fcfd_ctx *x, NewtonState &ns, int sweeps, int cycles, bool prec32) {
+  const DevMesh &m = x->dm;
+  const int nc = m.nc, n = 5 * nc;
+  cudaStream_t s = x->stream;
+  ns.Wn.alloc(n); ns.R0.alloc(n); ns.R1.alloc(n); ns.dt.alloc(nc); ns.vol.alloc(nc);
+  ns.JL.alloc(25 * (size_t)m.nf); ns.JR.alloc(25 * (size_t)m.nf); ns.Minv.alloc(25 * (size_t)nc);
+  ns.Pr.alloc(n); ns.Py0.alloc(n); ns.Py1.alloc(n); ns.Xs.alloc(n); ns.rowmag.alloc(n);
+  ns.sweeps = sweeps; ns.cycles = cycles > 0 ? cycles : 1;
+  ns.prec32 = prec32;
+  if (ns.sweeps > 0) {
+    if (ns.prec32) {
+      ns.OB32.alloc((size_t)nc * x->gs_deg * 25 + 1); ns.MinvP32.alloc(25 * (size_t)nc);
+      ns.Pr32.alloc(5 * (size_t)nc); ns.Py32.alloc(5 * (size_t)nc);
+    } else {
+      ns.OB.alloc((size_t)nc * x->gs_deg * 25 + 1); ns.MinvP.alloc(25 * (size_t)nc);
+    }
+  }
+  CK(cudaMemsetAsync(ns.JR.p, 0, sizeof(double) * 25 * (size_t)m.nf, s));
+  std::vector<double> vol(x->mesh->c_volume.begin(), x->mesh->c_volume.begin() + nc);
+  CK(cudaMemcpyAsync(ns.vol.p, vol.data(), sizeof(double) * nc, cudaMemcpyHostToDevice, s));
+  CK(cudaStreamSynchronize(s));
+}
+
+// One linearised backward-Euler solve at the state the last residual loaded
+// (ns.Wn, residual in ns.R0, local time step in ns.dt): the preconditioner
+// from the first-order face Jacobians, then GMRES for (V P/dt - J) dW = R0 into
+// ns.R1.  Shared by the Newton solve and the time-marching driver.
+struct LinearSolve {
+  int iters = 0;
+  double relres = 0.;
+};
+static LinearSolve implicit_solve(fcfd_ctx *x, NewtonState &ns, Krylov<double> &K64, Krylov<float> &K32, bool f32, int jmode,
+                                  double krtol, double abstol, DBuf<double> &part, DBuf<double> &hh) {
+  const DevMesh &m = x->dm;
+  const int nc = m.nc;
+  cudaStream_t s = x->stream;
+  const int tb = 256, gc = (nc + tb - 1) / tb;
+  // reference state magnitudes: RMS of |p+Pref|, |V|, |T+Tref|
+  RowScale wref;
+  double wn[5];
+  {
+    double rp = dnorm(x, part, hh, ns.Wn.p, nc), ru = dnorm(x, part, hh, ns.Wn.p + nc, nc);
+    double rv = dnorm(x, part, hh, ns.Wn.p + 2 * (size_t)nc, nc), rw = dnorm(x, part, hh, ns.Wn.p + 3 * (size_t)nc, nc);
+    double rT = dnorm(x, part, hh, ns.Wn.p + 4 * (size_t)nc, nc);
+    wn[0] = rp; wn[1] = ru; wn[2] = rv; wn[3] = rw; wn[4] = rT;
+    const double sq = std::sqrt((double)nc);
+    double U = std::sqrt(ru * ru + rv * rv + rw * rw) / sq;
+    wref.s[0] = rp / sq + std::fabs(x->cs.Pref);
+    wref.s[4] = rT / sq + std::fabs(x->cs.Tref);
+    if (!(U > 0.)) U = std::sqrt(x->cs.gamma * x->cs.R * wref.s[4]);
+    wref.s[1] = wref.s[2] = wref.s[3] = U;
+  }
+  // block-Jacobi preconditioner from the first-order face Jacobians
+  if (x->viscous)
+    FCFD_BY_FLUX(x->cs.flux, k_face_jac<true, FX><<<(m.nf + 127) / 128, 128, 0, s>>>(x->cs, m, x->p64.W.p, x->p64.G.p, x->p64.Lm.p, x->p64.stale.p, ns.JL.p, ns.JR.p));
+  else
+    FCFD_BY_FLUX(x->cs.flux, k_face_jac<false, FX><<<(m.nf + 127) / 128, 128, 0, s>>>(x->cs, m, x->p64.W.p, x->p64.G.p, x->p64.Lm.p, x->p64.stale.p, ns.JL.p, ns.JR.p));
+  k_block_jacobi<<<gc, tb, 0, s>>>(x->cs, m, ns.Wn.p, ns.vol.p, ns.dt.p, ns.JL.p, ns.JR.p, ns.Minv.p, x->err.p, wref, ns.rowmag.p);
+  if (ns.sweeps > 0) {
+    const std::vector<int> &ci = x->color_index;
+    const int deg = x->gs_deg;
+    for (size_t col = 0; col + 1 < ci.size(); ++col) {
+      const int cnt = ci[col + 1] - ci[col];
+      if (cnt <= 0) continue;
+      const size_t base = (size_t)ci[col];
+      if (ns.prec32)
+        k_pack_gs<float><<<(cnt + 127) / 128, 128, 0, s>>>(nc, m.nf, deg, cnt, x->color_cells.p + base,
+                                                           x->gs_nbr.p + base * deg, x->gs_src.p + base * deg, ns.JL.p,
+                                                           ns.JR.p, ns.Minv.p, ns.OB32.p + base * deg * 25,
+                                                           ns.MinvP32.p + base * 25);
+      else
+        k_pack_gs<double><<<(cnt + 127) / 128, 128, 0, s>>>(nc, m.nf, deg, cnt, x->color_cells.p + base,
+                                                            x->gs_nbr.p + base * deg, x->gs_src.p + base * deg, ns.JL.p,
+                                                            ns.JR.p, ns.Minv.p, ns.OB.p + base * deg * 25,
+                                                            ns.MinvP.p + base * 25);
+    }
+  }
+  CK(cudaGetLastError());
+  // GMRES norm weights: 1 / RMS row magnitude, so every equation is measured
+  // in units of a relative state change (consistent across equations)
+  RowScale rs;
+  for (int v = 0; v < 5; ++v) {
+    const double r = dnorm(x, part, hh, ns.rowmag.p + (size_t)v * nc, nc) / std::sqrt((double)nc);
+    rs.s[v] = (r > 0.) ? 1. / r : 1.;
+  }
+  for (int v = 0; v < 5; ++v) ns.winv.s[v] = 1. / wref.s[v];
+  {
+    // |S^-1 W| from the per-variable norms
+    double q = 0.;
+    for (int v = 0; v < 5; ++v) q += wn[v] * wn[v] * ns.winv.s[v] * ns.winv.s[v];
+    ns.wscale = std::sqrt(q);
+  }
+  LinearSolve out;
+  if (f32) gmres<float>(x, ns, K32, jmode, krtol, ns.R1.p, out.iters, out.relres, rs, abstol);
+  else gmres<double>(x, ns, K64, jmode, krtol, ns.R1.p, out.iters, out.relres, rs, abstol);
+  return out;
+}
+
+// ------------------------------------------------------------------ time-marching driver kernels
+
+// max over cells of (|V| + a) dt / lengthScale (update_time_step,
+// time_step.cc:202-214) as an order key; dt_c = dt[c], or dt0 when dt is null
+__global__ void k_max_cfl(DevCase cs, DevMesh m, const double *__restrict__ W, const double *__restrict__ dt, double dt0,
+                          unsigned long long *__restrict__ key) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= m.nc) return;
+  const int nt = m.nt;
+  const double p = W[c], u = W[nt + c], v = W[2 * nt + c], w = W[3 * nt + c], T = W[4 * nt + c];
+  const double a = sound(cs, p, T);
+  const double d = dt ? dt[c] : dt0;
+  atomicMax(key, okey((sqrt(u * u + v * v + w * w) + a) * d / m.c_len[c]));
+}
+
+__global__ void k_fill_value(int n, double *__restrict__ out, double v) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = v;
+}
+
+// W += dW (update_variables, ns.cc:338-396) with the per-block partial sums of
+// dp^2/dt^2, |dV|^2/dt^2, dT^2/dt^2; err bit 8 on a NaN/Inf update
+__global__ void k_update_res(int nc, double *__restrict__ Wn, const double *__restrict__ dW, const double *__restrict__ dt,
+                             double *__restrict__ part, int *__restrict__ err) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  double r[3] = {0., 0., 0.};
+  if (c < nc) {
+    double d[5];
+    bool bad = false;
+    for (int k = 0; k < 5; ++k) {
+      d[k] = dW[(size_t)k * nc + c];
+      if (!isfinite(d[k])) bad = true;
+    }
+    if (bad) atomicOr(err, 8);
+    for (int k = 0; k < 5; ++k) Wn[(size_t)k * nc + c] += d[k];
+    const double dt2 = dt[c] * dt[c];
+    r[0] = d[0] * d[0] / dt2;
+    r[1] = d[1] * d[1] / dt2 + d[2] * d[2] / dt2 + d[3] * d[3] / dt2;
+    r[2] = d[4] * d[4] / dt2;
+  }
+  __shared__ double sh[3][8];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for (int i = 0; i < 3; ++i) {
+    double t = r[i];
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+    if (lane == 0) sh[i][wid] = t;
+  }
+  __syncthreads();
+  if (threadIdx.x < 3) {
+    double t = 0.;
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) t += sh[threadIdx.x][k];
+    part[(size_t)blockIdx.x * 3 + threadIdx.x] = t;
+  }
+}
+
+// Boundary loads of the residual just evaluated (ns_assemble_linear_system.cc:
+// 108-119): per listed BC j, force += F_conv - F_diff of the momentum
+// equations (= -D), moment += (x_f - center) x force_f; per-block partial sums
+// part[blk][j][6]
+constexpr int kLoadBlock = 256;
+__global__ void __launch_bounds__(kLoadBlock) k_loads_moment(DevMesh m, const double *__restrict__ D, int nlist,
+                                                            const int *__restrict__ list, double cx, double cy, double cz,
+                                                            double *__restrict__ part) {
+  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+  __shared__ double sh[kMaxBC][6][kLoadBlock / 32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  int j = -1;
+  double F[3] = {0., 0., 0.}, M[3] = {0., 0., 0.};
+  if (f < m.nf) {
+    const int b = m.f_bc[f];
+    for (int q = 0; q < nlist; ++q)
+      if (list[q] == b) { j = q; break; }
+    if (j >= 0) {
+      for (int i = 0; i < 3; ++i) F[i] = -D[(size_t)(1 + i) * m.nf + f];
+      const double r0 = m.f_x[f] - cx, r1 = m.f_x[m.nf + f] - cy, r2 = m.f_x[2 * m.nf + f] - cz;
+      M[0] = r1 * F[2] - r2 * F[1];
+      M[1] = r2 * F[0] - r0 * F[2];
+      M[2] = r0 * F[1] - r1 * F[0];
+    }
+  }
+  for (int q = 0; q < nlist; ++q)
+    for (int i = 0; i < 6; ++i) {
+      double t = (j == q) ? (i < 3 ? F[i] : M[i - 3]) : 0.;
+      for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+      if (lane == 0) sh[q][i][wid] = t;
+    }
+  __syncthreads();
+  if (threadIdx.x < nlist * 6) {
+    const int q = threadIdx.x / 6, i = threadIdx.x % 6;
+    double t = 0.;
+    for (int k = 0; k < kLoadBlock / 32; ++k) t += sh[q][i][k];
+    part[((size_t)blockIdx.x * nlist + q) * 6 + i] = t;
+  }
+}
+
+void restart_write(const char *dir, int gid, int step, double time, const double *first_res, const double *rans_first,
+                   int n_cells, int n_nodes, const double *W, const double *dt, const double *K, const double *mu_t);
+void restart_read(const char *dir, int gid, int step, int n_cells, double *time, double *first_res, double *rans_first,
+                  double *W, double *K, double *mu_t);
+
 }  // namespace fcfd
 
 using namespace fcfd;
@@ -778,22 +982,7 @@ int fcfd_newton_solve(fcfd_ctx *x, double *W, const fcfd_newton_opts *o, fcfd_ne
     const int tb = 256, gc = (nc + tb - 1) / tb, gn = (n + tb - 1) / tb;
     std::memset(rep, 0, sizeof(*rep));
     NewtonState ns;
-    ns.Wn.alloc(n); ns.R0.alloc(n); ns.R1.alloc(n); ns.dt.alloc(nc); ns.vol.alloc(nc);
-    ns.JL.alloc(25 * (size_t)m.nf); ns.JR.alloc(25 * (size_t)m.nf); ns.Minv.alloc(25 * (size_t)nc);
-    ns.Pr.alloc(n); ns.Py0.alloc(n); ns.Py1.alloc(n); ns.Xs.alloc(n); ns.rowmag.alloc(n);
-    ns.sweeps = o->precond_sweeps; ns.cycles = o->krylov_cycles > 0 ? o->krylov_cycles : 1;
-    ns.prec32 = o->fp32_krylov != 0;
-    if (ns.sweeps > 0) {
-      if (ns.prec32) {
-        ns.OB32.alloc((size_t)nc * x->gs_deg * 25 + 1); ns.MinvP32.alloc(25 * (size_t)nc);
-        ns.Pr32.alloc(5 * (size_t)nc); ns.Py32.alloc(5 * (size_t)nc);
-      } else {
-        ns.OB.alloc((size_t)nc * x->gs_deg * 25 + 1); ns.MinvP.alloc(25 * (size_t)nc);
-      }
-    }
-    CK(cudaMemsetAsync(ns.JR.p, 0, sizeof(double) * 25 * (size_t)m.nf, s));
-    std::vector<double> vol(x->mesh->c_volume.begin(), x->mesh->c_volume.begin() + nc);
-    CK(cudaMemcpyAsync(ns.vol.p, vol.data(), sizeof(double) * nc, cudaMemcpyHostToDevice, s));
+    alloc_state(x, ns, o->precond_sweeps, o->krylov_cycles, o->fp32_krylov != 0);
     CK(cudaMemcpyAsync(x->Win.p, W, sizeof(double) * n, cudaMemcpyHostToDevice, s));
     k_aos_to_soa_nc<<<gc, tb, 0, s>>>(x->Win.p, ns.Wn.p, nc);
     const int mdim = o->krylov_dim > 0 ? o->krylov_dim : 30;
@@ -837,66 +1026,9 @@ int fcfd_newton_solve(fcfd_ctx *x, double *W, const fcfd_newton_opts *o, fcfd_ne
           std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() > o->max_seconds) break;
       // local time step on the current state (loaded by the last residual)
       k_local_dt<double><<<gc, tb, 0, s>>>(x->cs, m, x->p64.W.p, ns.dt.p, cfl, nullptr);
-      // reference state magnitudes: RMS of |p+Pref|, |V|, |T+Tref|
-      RowScale wref;
-      double wn[5];
-      {
-        double rp = dnorm(x, part, hh, ns.Wn.p, nc), ru = dnorm(x, part, hh, ns.Wn.p + nc, nc);
-        double rv = dnorm(x, part, hh, ns.Wn.p + 2 * (size_t)nc, nc), rw = dnorm(x, part, hh, ns.Wn.p + 3 * (size_t)nc, nc);
-        double rT = dnorm(x, part, hh, ns.Wn.p + 4 * (size_t)nc, nc);
-        wn[0] = rp; wn[1] = ru; wn[2] = rv; wn[3] = rw; wn[4] = rT;
-        const double sq = std::sqrt((double)nc);
-        double U = std::sqrt(ru * ru + rv * rv + rw * rw) / sq;
-        wref.s[0] = rp / sq + std::fabs(x->cs.Pref);
-        wref.s[4] = rT / sq + std::fabs(x->cs.Tref);
-        if (!(U > 0.)) U = std::sqrt(x->cs.gamma * x->cs.R * wref.s[4]);
-        wref.s[1] = wref.s[2] = wref.s[3] = U;
-      }
-      // block-Jacobi preconditioner from the first-order face Jacobians
-      if (x->viscous)
-        FCFD_BY_FLUX(x->cs.flux, k_face_jac<true, FX><<<(m.nf + 127) / 128, 128, 0, s>>>(x->cs, m, x->p64.W.p, x->p64.G.p, x->p64.Lm.p, x->p64.stale.p, ns.JL.p, ns.JR.p));
-      else
-        FCFD_BY_FLUX(x->cs.flux, k_face_jac<false, FX><<<(m.nf + 127) / 128, 128, 0, s>>>(x->cs, m, x->p64.W.p, x->p64.G.p, x->p64.Lm.p, x->p64.stale.p, ns.JL.p, ns.JR.p));
-      k_block_jacobi<<<gc, tb, 0, s>>>(x->cs, m, ns.Wn.p, ns.vol.p, ns.dt.p, ns.JL.p, ns.JR.p, ns.Minv.p, x->err.p, wref, ns.rowmag.p);
-      if (ns.sweeps > 0) {
-        const std::vector<int> &ci = x->color_index;
-        const int deg = x->gs_deg;
-        for (size_t col = 0; col + 1 < ci.size(); ++col) {
-          const int cnt = ci[col + 1] - ci[col];
-          if (cnt <= 0) continue;
-          const size_t base = (size_t)ci[col];
-          if (ns.prec32)
-            k_pack_gs<float><<<(cnt + 127) / 128, 128, 0, s>>>(nc, m.nf, deg, cnt, x->color_cells.p + base,
-                                                               x->gs_nbr.p + base * deg, x->gs_src.p + base * deg, ns.JL.p,
-                                                               ns.JR.p, ns.Minv.p, ns.OB32.p + base * deg * 25,
-                                                               ns.MinvP32.p + base * 25);
-          else
-            k_pack_gs<double><<<(cnt + 127) / 128, 128, 0, s>>>(nc, m.nf, deg, cnt, x->color_cells.p + base,
-                                                                x->gs_nbr.p + base * deg, x->gs_src.p + base * deg, ns.JL.p,
-                                                                ns.JR.p, ns.Minv.p, ns.OB.p + base * deg * 25,
-                                                                ns.MinvP.p + base * 25);
-        }
-      }
-      CK(cudaGetLastError());
-      // GMRES norm weights: 1 / RMS row magnitude, so every equation is measured
-      // in units of a relative state change (consistent across equations)
-      RowScale rs;
-      for (int v = 0; v < 5; ++v) {
-        const double r = dnorm(x, part, hh, ns.rowmag.p + (size_t)v * nc, nc) / std::sqrt((double)nc);
-        rs.s[v] = (r > 0.) ? 1. / r : 1.;
-      }
-      for (int v = 0; v < 5; ++v) ns.winv.s[v] = 1. / wref.s[v];
-      {
-        // |S^-1 W| from the per-variable norms
-        double q = 0.;
-        for (int v = 0; v < 5; ++v) q += wn[v] * wn[v] * ns.winv.s[v] * ns.winv.s[v];
-        ns.wscale = std::sqrt(q);
-      }
-      int kit = 0;
-      double rr = 0.;
       const double krtol = o->krylov_rtol > 0 ? o->krylov_rtol : 1e-2;
-      if (f32) gmres<float>(x, ns, K32, jmode, krtol, ns.R1.p, kit, rr, rs);
-      else gmres<double>(x, ns, K64, jmode, krtol, ns.R1.p, kit, rr, rs);
+      const LinearSolve ls = implicit_solve(x, ns, K64, K32, f32, jmode, krtol, 0., part, hh);
+      const int kit = ls.iters;
       rep->krylov_iterations += kit;
       // relax the update so that p and T change by at most 20 % per step
       CK(cudaMemsetAsync(key.p, 0, sizeof(unsigned long long), s));
@@ -966,6 +1098,252 @@ int fcfd_newton_solve(fcfd_ctx *x, double *W, const fcfd_newton_opts *o, fcfd_ne
     return FCFD_ERR_INPUT;
   }
   return FCFD_OK;
+}
+
+// Deck-driven time loop (main.cc:294-438) for one laminar / Euler grid: per
+// step update_time_step (time_step.cc:143-224: ramp, CFL schedule file, FIXED /
+// CFL_MAX / CFL_LOCAL step, max CFL, physical time), one implicit
+// backward-Euler step (NavierStokes::solve, ns.cc:104-118: residual, boundary
+// loads, (V P/dt - J) dW = R by GMRES with the deck's relative / absolute
+// tolerance and iteration cap, W += dW), the residual measure of
+// update_variables (ns.cc:338-396), convergence.dat and screen lines
+// (main.cc:351-369), loads files (write_loads, write_volume_output.cc:65-85),
+// restart files (write_restart.cc:45-100; also when a file named dump_restart
+// appears in the run directory), and every `updatefrequency` steps a re-read
+// of the deck's timemarching section (update_time_step_options).
+int fcfd_run(fcfd_ctx *x, double *W, const fcfd_run_opts *o, fcfd_run_report *rep) {
+  try {
+    if (!x || !W || !o || !rep) throw Error(FCFD_ERR_INPUT, "null argument");
+    CK(cudaSetDevice(x->device));
+    std::memset(rep, 0, sizeof(*rep));
+    const fcfd_case &cs = *x->case_ptr;
+    if (cs.turbulent) throw Error(FCFD_ERR_UNSUPPORTED, "the time-marching driver runs laminar / Euler cases (no implicit k-omega step)");
+    TimeMarching tm = cs.tm;
+    if (tm.ps_steps > 1) throw Error(FCFD_ERR_UNSUPPORTED, "pseudo-time (dual time stepping) iterations are not on the B200 path");
+    if ((int)cs.load_bcs.size() > kMaxBC) throw Error(FCFD_ERR_UNSUPPORTED, "more than 16 load BCs");
+    const DevMesh &m = x->dm;
+    const int nc = m.nc, n = 5 * nc;
+    cudaStream_t s = x->stream;
+    const int tb = 256, gc = (nc + tb - 1) / tb;
+    const std::string wd = (o->work_dir && *o->work_dir) ? std::string(o->work_dir) : std::string(".");
+    auto in_dir = [&](const std::string &f) { return (!f.empty() && f[0] == '/') ? f : wd + "/" + f; };
+    auto exists = [](const std::string &f) { std::ifstream t(f); return t.good(); };
+    const int restart_step = o->restart_step > 0 ? o->restart_step : 0;
+    double time = 0.;
+    double first[3] = {0., 0., 0.};
+    if (restart_step > 0) {
+      double rf[2];
+      restart_read(wd.c_str(), 1, restart_step, nc, &time, first, rf, W, nullptr, nullptr);
+    }
+    // solver state (one GMRES cycle of at most `maximumiterations` vectors)
+    NewtonState ns;
+    alloc_state(x, ns, o->precond_sweeps, 1, o->fp32_krylov != 0);
+    const int mdim = cs.lin_maxits > 0 ? cs.lin_maxits : 10;
+    Krylov<double> K64;
+    Krylov<float> K32;
+    const bool f32 = o->fp32_krylov != 0;
+    x->newton_frozen = o->jvp_mode == 1;
+    x->newton_f32 = o->jvp_mode == 3;
+    const int jmode = o->jvp_mode == 0 ? 0 : 1;
+    if (f32) K32.alloc(x, mdim); else K64.alloc(x, mdim);
+    DBuf<double> part, hh, lpart, hdt;
+    part.alloc(kRedBlocks); hh.alloc(1);
+    DBuf<unsigned long long> key;
+    key.alloc(1);
+    DBuf<int> lbcs;
+    const int nl = (int)cs.load_bcs.size();
+    const int nlb = (m.nf + kLoadBlock - 1) / kLoadBlock;
+    if (nl > 0) { lbcs.upload(cs.load_bcs); lpart.alloc((size_t)nlb * nl * 6); }
+    DBuf<double> upart;
+    upart.alloc((size_t)gc * 3);
+    CK(cudaMemcpyAsync(x->Win.p, W, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+    k_aos_to_soa_nc<<<gc, tb, 0, s>>>(x->Win.p, ns.Wn.p, nc);
+    // schedule file (set_time_step_options, time_step.cc:44-58)
+    bool schedule = false;
+    auto check_schedule = [&]() {
+      schedule = false;
+      if (!tm.schedule_file.empty()) {
+        if (exists(in_dir(tm.schedule_file))) { tm.type = TS_CFL_MAX; schedule = true; }
+        else if (o->echo) std::printf("[W] CFL schedule file %s is not found, continuing\n", tm.schedule_file.c_str());
+      }
+    };
+    check_schedule();
+    if (tm.type == TS_NONE) throw Error(FCFD_ERR_INPUT, "timemarching needs stepsize, CFLmax or CFLlocal");
+    double cfl_max = tm.cfl_max, cfl_local = tm.cfl_local, ts_cur = tm.stepsize;
+    double cfl_max_target = cfl_max, cfl_local_target = cfl_local, ts_target = ts_cur;
+    bool ramp = tm.ramp;
+    int n_steps = o->max_steps > 0 ? o->max_steps : tm.n_steps;
+    int update_freq = tm.update_freq > 0 ? tm.update_freq : 1000000;
+    const int load_freq = cs.load_freq > 0 ? cs.load_freq : 1000000;
+    const int restart_freq = cs.restart_freq > 0 ? cs.restart_freq : 1000000;
+    // convergence.dat (main.cc:302-305): appended to on a restart
+    const std::string conv_name = wd + "/convergence.dat";
+    FILE *conv = std::fopen(conv_name.c_str(), (restart_step > 0 && exists(conv_name)) ? "a" : "w");
+    if (!conv) throw Error(FCFD_ERR_INPUT, "convergence.dat could not be opened in " + wd);
+    struct Closer { FILE *f; ~Closer() { if (f) std::fclose(f); } } closer{conv};
+    if (o->echo) {
+      std::printf("[I] Beginning time loop\n\n");
+      std::printf("=============================================================================================================\n");
+      std::printf("step -- for each grid -> [grid-no  time  -- for each equation -> {cfl-max linear-iterations total-residual} ]\n");
+      std::printf("=============================================================================================================\n");
+    }
+    if (nl > 0) mkdir((wd + "/volume_output").c_str(), S_IRWXU);
+    std::vector<double> host_W(n), host_dt(nc);
+    auto save_restart = [&](int step) {
+      k_soa_to_aos_nc<<<gc, tb, 0, s>>>(ns.Wn.p, x->Win.p, nc);
+      CK(cudaMemcpyAsync(host_W.data(), x->Win.p, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+      CK(cudaMemcpyAsync(host_dt.data(), ns.dt.p, sizeof(double) * nc, cudaMemcpyDeviceToHost, s));
+      CK(cudaStreamSynchronize(s));
+      restart_write(wd.c_str(), 1, step, time, first, nullptr, nc, (int)(x->mesh->nodes.size() / 3), host_W.data(),
+                    host_dt.data(), nullptr, nullptr);
+    };
+    auto t0 = std::chrono::steady_clock::now();
+    int status = FCFD_OK;
+    double res = 0.;
+    for (int step = restart_step + 1; step <= n_steps + restart_step; ++step) {
+      const bool last = step == n_steps + restart_step;
+      // ---- update_time_step (time_step.cc:143-224)
+      if (ramp) {
+        if (step == 1) {
+          if (tm.type == TS_FIXED) ts_cur = tm.ramp_initial;
+          if (tm.type == TS_CFL_MAX) cfl_max = tm.ramp_initial;
+          if (tm.type == TS_CFL_LOCAL) cfl_local = tm.ramp_initial;
+        } else {
+          if (tm.type == TS_FIXED) ts_cur = std::min(ts_cur * tm.ramp_growth, ts_target);
+          if (tm.type == TS_CFL_MAX) cfl_max = std::min(cfl_max * tm.ramp_growth, cfl_max_target);
+          if (tm.type == TS_CFL_LOCAL) cfl_local = std::min(cfl_local * tm.ramp_growth, cfl_local_target);
+        }
+      }
+      // the state and its residual (the residual also loads W into the
+      // gradient / limiter pipeline that the time step reads)
+      eval_residual<double>(x, ns.Wn.p, ns.R0.p, (const double *)nullptr, 0.);
+      double max_cfl = -1.;
+      if (tm.type == TS_FIXED) {
+        k_fill_value<<<gc, tb, 0, s>>>(nc, ns.dt.p, ts_cur);
+      } else if (tm.type == TS_CFL_MAX) {
+        if (schedule) {
+          std::ifstream f(in_dir(tm.schedule_file));
+          int st;
+          double val;
+          while (f >> st >> val) {
+            if (step > st) { cfl_max = val; ramp = false; }
+            else break;
+          }
+        }
+        CK(cudaMemsetAsync(x->dtmin.p, 0xFF, sizeof(unsigned long long), s));
+        k_local_dt<double><<<gc, tb, 0, s>>>(x->cs, m, x->p64.W.p, ns.dt.p, cfl_max, x->dtmin.p);
+        k_fill_min<double><<<gc, tb, 0, s>>>(nc, ns.dt.p, x->dtmin.p);
+        unsigned long long kmin = 0;
+        CK(cudaMemcpyAsync(&kmin, x->dtmin.p, sizeof(kmin), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        unsigned long long b = (kmin >> 63) ? (kmin & 0x7fffffffffffffffull) : ~kmin;
+        std::memcpy(&ts_cur, &b, sizeof(ts_cur));
+      } else {
+        CK(cudaMemsetAsync(x->dtmin.p, 0xFF, sizeof(unsigned long long), s));
+        k_local_dt<double><<<gc, tb, 0, s>>>(x->cs, m, x->p64.W.p, ns.dt.p, cfl_local, x->dtmin.p);
+      }
+      if (tm.type == TS_CFL_LOCAL) {
+        unsigned long long kmin = 0;
+        CK(cudaMemcpyAsync(&kmin, x->dtmin.p, sizeof(kmin), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        unsigned long long b = (kmin >> 63) ? (kmin & 0x7fffffffffffffffull) : ~kmin;
+        std::memcpy(&ts_cur, &b, sizeof(ts_cur));
+        max_cfl = cfl_local;
+      } else {
+        CK(cudaMemsetAsync(key.p, 0, sizeof(unsigned long long), s));
+        k_max_cfl<<<gc, tb, 0, s>>>(x->cs, m, x->p64.W.p, nullptr, ts_cur, key.p);
+        unsigned long long kmax = 0;
+        CK(cudaMemcpyAsync(&kmax, key.p, sizeof(kmax), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        unsigned long long b = (kmax >> 63) ? (kmax & 0x7fffffffffffffffull) : ~kmax;
+        std::memcpy(&max_cfl, &b, sizeof(max_cfl));
+      }
+      time += ts_cur;
+      // ---- boundary loads of this step's residual (before the Krylov solve
+      // evaluates residuals at other states)
+      std::vector<double> loads(6 * (size_t)nl, 0.);
+      if (nl > 0 && step % load_freq == 0) {
+        k_loads_moment<<<nlb, kLoadBlock, 0, s>>>(m, x->p64.D.p, nl, lbcs.p, cs.moment_center[0], cs.moment_center[1],
+                                                  cs.moment_center[2], lpart.p);
+        std::vector<double> hp((size_t)nlb * nl * 6);
+        CK(cudaMemcpyAsync(hp.data(), lpart.p, sizeof(double) * hp.size(), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        for (int bl = 0; bl < nlb; ++bl)
+          for (size_t k = 0; k < loads.size(); ++k) loads[k] += hp[(size_t)bl * nl * 6 + k];
+      }
+      // ---- implicit step
+      const LinearSolve ls = implicit_solve(x, ns, K64, K32, f32, jmode, cs.lin_rtol, cs.lin_abstol, part, hh);
+      rep->krylov_iterations += ls.iters;
+      CK(cudaMemsetAsync(x->err.p, 0, sizeof(int), s));
+      k_update_res<<<gc, tb, 0, s>>>(nc, ns.Wn.p, ns.R1.p, ns.dt.p, upart.p, x->err.p);
+      std::vector<double> hu((size_t)gc * 3);
+      int h = 0;
+      CK(cudaMemcpyAsync(hu.data(), upart.p, sizeof(double) * hu.size(), cudaMemcpyDeviceToHost, s));
+      CK(cudaMemcpyAsync(&h, x->err.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+      CK(cudaStreamSynchronize(s));
+      if (h & 8) {
+        CK(cudaMemsetAsync(x->err.p, 0, sizeof(int), s));
+        status = FCFD_ERR_DIVERGED;
+        set_last_error("Divergence detected (NaN/Inf update) at time step " + std::to_string(step));
+        rep->steps = step - restart_step;
+        break;
+      }
+      double tot[3] = {0., 0., 0.};
+      for (int bl = 0; bl < gc; ++bl)
+        for (int i = 0; i < 3; ++i) tot[i] += hu[(size_t)bl * 3 + i];
+      if (step == 1)
+        for (int i = 0; i < 3; ++i) first[i] = std::sqrt(tot[i]);
+      res = 0.;
+      for (int i = 0; i < 3; ++i) res += std::sqrt(tot[i]) / first[i] / 3.;
+      // ---- screen and convergence.dat lines (main.cc:351-369)
+      std::fprintf(conv, "%d\t%d\t%.3e\t%.3e\t%d\t%.3e\n", step, 1, time, max_cfl, ls.iters, res);
+      std::fflush(conv);
+      if (o->echo) std::printf("%d\t%d\t%.3e\t%.3e\t%d\t%.3e\n", step, 1, time, max_cfl, ls.iters, res);
+      rep->steps = step - restart_step;
+      // ---- restart and loads files
+      if (step % restart_freq == 0 || last) save_restart(step);
+      if (nl > 0 && step % load_freq == 0) {
+        for (int j = 0; j < nl; ++j) {
+          const std::string fn = wd + "/volume_output/loads_grid_1_BC_" + std::to_string(cs.load_bcs[j] + 1) + ".dat";
+          FILE *lf = std::fopen(fn.c_str(), "a");
+          if (!lf) throw Error(FCFD_ERR_INPUT, "loads file " + fn + " could not be opened");
+          const double *q = &loads[6 * (size_t)j];
+          std::fprintf(lf, "%d\t%.8e\t%.8e\t%.8e\t%.8e\t%.8e\t%.8e\t%.8e\n", step, time, q[0], q[1], q[2], q[3], q[4], q[5]);
+          std::fclose(lf);
+        }
+      }
+      // ---- option re-read (main.cc:386-390)
+      if (step % update_freq == 0) {
+        tm = read_time_marching(cs.deck_path);
+        check_schedule();
+        cfl_max = cfl_max_target = tm.cfl_max;
+        cfl_local = cfl_local_target = tm.cfl_local;
+        ts_cur = ts_target = tm.stepsize;
+        ramp = tm.ramp;
+        update_freq = tm.update_freq > 0 ? tm.update_freq : 1000000;
+        if (o->max_steps <= 0) n_steps = tm.n_steps;
+      }
+      if (exists(wd + "/dump_restart")) {
+        save_restart(step);
+        std::remove((wd + "/dump_restart").c_str());
+      }
+    }
+    rep->wall_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    rep->time = time;
+    rep->res = res;
+    rep->status = status;
+    k_soa_to_aos_nc<<<gc, tb, 0, s>>>(ns.Wn.p, x->Win.p, nc);
+    CK(cudaMemcpyAsync(W, x->Win.p, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (o->echo) std::printf("[I] Wall time = %g second\n", rep->wall_seconds);
+    return status;
+  } catch (const Error &e) {
+    set_last_error(e.what());
+    return e.code;
+  } catch (const std::exception &e) {
+    set_last_error(e.what());
+    return FCFD_ERR_INPUT;
+  }
 }
 
 }  // extern "C"

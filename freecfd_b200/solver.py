@@ -16,7 +16,7 @@ import tempfile
 
 import numpy as np
 
-from ._lib import NewtonOpts, NewtonReport, _RawMesh, _d, _i, _ptr, check, lib, FcfdError
+from ._lib import NewtonOpts, NewtonReport, RunOpts, RunReport, _RawMesh, _d, _i, _ptr, check, lib, FcfdError
 
 
 class Case:
@@ -222,6 +222,24 @@ class NavierStokes:
             raise FcfdError(rc, lib.fcfd_last_error().decode() + f" after {r.newton_iterations} steps")
         return W, rep
 
+    def run(self, W, work_dir=".", restart_step=0, max_steps=0, jvp=False, fp32_krylov=False, precond_sweeps=0,
+            echo=False, raise_on_fail=True):
+        """The deck's time loop (the reference's main program): per step the
+        CFL schedule, one implicit backward-Euler step, convergence.dat,
+        loads and restart files under ``work_dir``.  ``restart_step`` > 0
+        starts from the restart files of that step (W is then only the
+        output buffer).  Returns (W_final, report dict)."""
+        W = np.array(W, dtype=np.float64, order="C", copy=True)
+        o = RunOpts(os.fsencode(str(work_dir)), int(restart_step), int(max_steps), 1 if jvp else 0,
+                    int(bool(fp32_krylov)), int(precond_sweeps), int(bool(echo)))
+        r = RunReport()
+        rc = lib.fcfd_run(self.h, _d(W), ctypes.byref(o), ctypes.byref(r))
+        rep = dict(status=r.status, steps=r.steps, krylov_iterations=r.krylov_iterations, time=r.time, res=r.res,
+                   wall_seconds=r.wall_seconds)
+        if rc != 0 and raise_on_fail:
+            raise FcfdError(rc, lib.fcfd_last_error().decode() + f" after {r.steps} steps")
+        return W, rep
+
     def stages(self):
         m = self.mesh
         out = dict(grads=np.empty((m.nc, 15)), limiter=np.empty((m.nc, 5)), ghost=np.empty((m.nghost, 5)),
@@ -247,6 +265,37 @@ class NavierStokes:
         if getattr(self, "h", None):
             lib.fcfd_ctx_destroy(self.h)
             self.h = None
+
+
+def write_restart(work_dir, step: int, W, time: float, first_res, n_nodes: int, dt=None, K=None, mu_t=None,
+                  rans_first_res=None, gid: int = 1):
+    """Restart files in the reference's layout (write_restart.cc) under
+    ``work_dir``/restart: partition map, <step>/time.dat, raw doubles per
+    cell.  W[nc][5] = (p,u,v,w,T), K[nc][2] = (k, omega)."""
+    W = np.ascontiguousarray(W, dtype=np.float64)
+    nc = W.shape[0]
+    first = np.ascontiguousarray(first_res, dtype=np.float64)
+    rf = None if rans_first_res is None else np.ascontiguousarray(rans_first_res, dtype=np.float64)
+    arr = [None if a is None else np.ascontiguousarray(a, dtype=np.float64) for a in (dt, K, mu_t)]
+    check(lib.fcfd_restart_write(os.fsencode(str(work_dir)), int(gid), int(step), float(time), _d(first), _d(rf),
+                                 int(nc), int(n_nodes), _d(W), _d(arr[0]), _d(arr[1]), _d(arr[2])))
+
+
+def read_restart(work_dir, step: int, n_cells: int, turbulent: bool = False, gid: int = 1):
+    """Reads the files of write_restart (or of the reference's write_restart).
+    Returns dict(time, first_res, rans_first_res, W[, K, mu_t])."""
+    t = np.zeros(1)
+    first = np.zeros(3)
+    rf = np.zeros(2)
+    W = np.zeros((n_cells, 5))
+    K = np.zeros((n_cells, 2)) if turbulent else None
+    mu_t = np.zeros(n_cells) if turbulent else None
+    check(lib.fcfd_restart_read(os.fsencode(str(work_dir)), int(gid), int(step), int(n_cells), _d(t), _d(first), _d(rf),
+                                _d(W), _d(K), _d(mu_t)))
+    out = dict(time=float(t[0]), first_res=first, rans_first_res=rf, W=W)
+    if turbulent:
+        out.update(K=K, mu_t=mu_t)
+    return out
 
 
 def point_flux(flux: int, L, R, n, gamma=1.4, gas_R=287.0, Pref=0.0, Tref=0.0, Minf=1.0):

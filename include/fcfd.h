@@ -212,6 +212,61 @@ typedef struct fcfd_newton_report {
  * Returns FCFD_ERR_NOT_CONVERGED / FCFD_ERR_DIVERGED with the report filled. */
 int fcfd_newton_solve(fcfd_ctx *ctx, double *W, const fcfd_newton_opts *opts, fcfd_newton_report *report);
 
+/* Deck-driven time loop (main.cc:294-438) for one laminar or Euler grid,
+ * replacing the reference's main program after set-up.  Per time step:
+ * update_time_step (time_step.cc:143-224: CFL ramp, schedule file, FIXED /
+ * CFL_MAX / CFL_LOCAL step, max CFL, physical time), one implicit
+ * backward-Euler step (NavierStokes::solve, ns.cc:104-118) solved by GMRES
+ * with the deck's navierstokes relative tolerance, absolute tolerance (in the
+ * row-scaled norm) and maximum iterations (one cycle), W += dW, the residual
+ * of update_variables (ns.cc:338-396), a convergence.dat line (main.cc:
+ * 351-369: step, grid, time, max CFL, linear iterations, residual), loads files
+ * volume_output/loads_grid_1_BC_<b>.dat (write_loads, write_volume_output.cc:
+ * 65-85) every loadfrequency steps, restart files every restartfrequency
+ * steps, at the last step and when a file named dump_restart appears in the
+ * run directory (write_restart.cc:45-100), and every updatefrequency steps a
+ * re-read of the deck's timemarching section.  The implicit operator is the
+ * full Jacobian (jvp_mode as in fcfd_newton_opts), preconditioned by the
+ * first-order one; the reference solves with its first-order FD Jacobian.
+ * Turbulent decks and pseudo-time sub-iterations return
+ * FCFD_ERR_UNSUPPORTED; a NaN/Inf update returns FCFD_ERR_DIVERGED (the
+ * reference aborts).  W[nc][5] host, in/out. */
+typedef struct fcfd_run_opts {
+  const char *work_dir;   /* run directory (the reference's working directory); NULL: "." */
+  int32_t restart_step;   /* > 0: read restart/<step>/ from work_dir and continue with step+1 */
+  int32_t max_steps;      /* > 0: overrides timemarching -> numberofsteps */
+  int32_t jvp_mode;       /* J.v of the implicit operator, as in fcfd_newton_opts */
+  int32_t fp32_krylov;    /* as in fcfd_newton_opts */
+  int32_t precond_sweeps; /* as in fcfd_newton_opts */
+  int32_t echo;           /* 1: also print the reference's screen lines to stdout */
+} fcfd_run_opts;
+
+typedef struct fcfd_run_report {
+  int32_t status, steps, krylov_iterations, pad;
+  double time, res, wall_seconds;
+} fcfd_run_report;
+
+int fcfd_run(fcfd_ctx *ctx, double *W, const fcfd_run_opts *opts, fcfd_run_report *report);
+
+/* Restart files in the reference's layout under <dir>/restart/ (dir NULL:
+ * "."): partitionMap_<gid>.dat, <step>/time.dat and raw native-endian doubles
+ * per cell <step>/{dt,p,V,T[,k,omega,mu_t]}.<gid> (write_restart.cc:45-100,
+ * ns_write_restart.cc:25-35, rans_write_restart.cc:25-35,
+ * Variable::dump_cell_data variable.h:229-245).  gid = the grid number of
+ * the file names (1 for grid_1); one partition, global id of cell c = c.
+ * first_res[3] = the NS residual normalisations, rans_first_res[2] the RANS
+ * ones (NULL writes -1 -1); W[nc][5] = (p,u,v,w,T); dt[nc] may be NULL;
+ * K[nc][2] = (k, omega) and mu_t[nc] may be NULL (laminar). */
+int fcfd_restart_write(const char *dir, int32_t gid, int32_t step, double time, const double *first_res,
+                       const double *rans_first_res, int32_t n_cells, int32_t n_nodes, const double *W,
+                       const double *dt, const double *K, const double *mu_t);
+/* Reads the files fcfd_restart_write (or the reference) wrote, placing each
+ * value by the global cell id of the partition map (read_restart.cc:44-102,
+ * Variable::read_cell_data variable.h:248-271).  Any output may be NULL
+ * except W. */
+int fcfd_restart_read(const char *dir, int32_t gid, int32_t step, int32_t n_cells, double *time, double *first_res,
+                      double *rans_first_res, double *W, double *K, double *mu_t);
+
 /* Device timing of the residual: runs `reps` residual evaluations on the
  * resident state (captured in one CUDA graph) and returns per-kernel average
  * milliseconds: out[0] total per residual, out[1..] per kernel (see fcfd.cu). */

@@ -54,7 +54,7 @@ def lib():
         L.orc_residual_cstep.argtypes = [vp, dp, dp, ctypes.c_double, dp, ctypes.c_char_p, ctypes.c_int]
         L.orc_residual_cstep.restype = ctypes.c_int
         L.orc_local_dt.argtypes = [vp, dp, ctypes.c_double, ctypes.c_int, dp]
-        L.orc_loads.argtypes = [vp, dp, dp, ctypes.c_double, dp, ctypes.c_char_p, ctypes.c_int]
+        L.orc_loads.argtypes = [vp, dp, dp, ctypes.c_double, dp, dp, ctypes.c_char_p, ctypes.c_int]
         L.orc_loads.restype = ctypes.c_int
         L.orc_rans_residual.argtypes = [vp, dp, dp, dp, dp, ctypes.c_char_p, ctypes.c_int]
         L.orc_rans_residual.restype = ctypes.c_int
@@ -167,20 +167,23 @@ class Oracle:
             raise RuntimeError("oracle: " + err.value.decode())
         return dR
 
-    def loads(self, W, dW=None, h=1e-30):
+    def loads(self, W, dW=None, h=1e-30, moments=False):
         """Force on every boundary region [n_bc][3] (convective minus diffusive
         momentum flux summed over the region's faces); with dW, its
-        complex-step directional derivative along dW."""
+        complex-step directional derivative along dW.  moments=True returns
+        (force, moment about the deck's moment center)."""
         W = np.ascontiguousarray(W, dtype=np.float64).reshape(self.nc, 5)
         nbc = int(self.case_summary()[1][5])
         out = np.empty((nbc, 3))
         err = ctypes.create_string_buffer(512)
         if dW is not None:
             dW = np.ascontiguousarray(dW, dtype=np.float64).reshape(self.nc, 5)
-        rc = lib().orc_loads(self.h, _d(W), None if dW is None else _d(dW), h, _d(out), err, 512)
+        mom = np.empty((nbc, 3)) if moments else None
+        rc = lib().orc_loads(self.h, _d(W), None if dW is None else _d(dW), h, _d(out), None if mom is None else _d(mom),
+                             err, 512)
         if rc != 0:
             raise RuntimeError("oracle: " + err.value.decode())
-        return out
+        return (out, mom) if moments else out
 
     def rans_residual(self, W, K):
         """k-omega RANS residual: (R[nc][5] with eddy viscosity, RK[nc][2])."""

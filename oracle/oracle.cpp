@@ -269,6 +269,7 @@ struct Oracle {
   int order = SECOND, limiter_function = VK, flux = AUSM_PLUS_UP;
   double limiter_threshold = 0., Minf = 1.;
   double wdiss = 0.3, bl_height = 0.;  // ns.cc:76-77
+  Vec3 moment_center;                  // writeoutput -> momentcenter (main.cc:240)
   int hex_method = LSQR, prism_method = LSQR, other_method = LSQR;
   int interp_method = WTLI, stencil_size = 2;
   // Variable<TYPE>::fixedonBC / bcValue for the NS variables (ns_set_bcs.cc)
@@ -811,6 +812,10 @@ static void setup_physics(Oracle &O, const std::string &deck_dir) {
   else if (fl == "SW") O.flux = SW;
   else throw DeckError("convective flux " + fl + " is not on the restated path");
   O.Minf = O.input.section("reference").gd("Mach").value;
+  {
+    const V3d &mc = g.sub("writeoutput").gv("momentcenter").value;
+    O.moment_center = Vec3(mc.c[0], mc.c[1], mc.c[2]);
+  }
   O.wdiss = ns.gd("walldissipation").value;
   O.bl_height = ns.gd("BLheight").value;
   O.hex_method = method_of(g.sub("gradients").gs("hexmethod").value);
@@ -1715,14 +1720,14 @@ struct NS {
   }
 
   // ns_assemble_linear_system.cc:34-140 (residual part; no Jacobian)
-  // loads: optional per-BC force [bcCount][3], integrated as in
+  // loads: optional per-BC force and moment [bcCount][6], integrated as in
   // ns_assemble_linear_system.cc:108-119 (convective - diffusive momentum flux
-  // of every face of the region)
+  // of every face of the region; moment (x_f - moment center) x that flux)
   void assemble(std::vector<S> &rhs, const std::vector<S> *mu_t_face = nullptr, double Pr_t = 0.9,
                 std::vector<S> *loads = nullptr) {
     Grid &g = O.grid;
     rhs.assign((size_t)g.cellCount * 5, S(0.));
-    if (loads) loads->assign((size_t)g.bcCount * 3, S(0.));
+    if (loads) loads->assign((size_t)g.bcCount * 6, S(0.));
     S fc[5], fd[5];
     for (int m = 0; m < 5; ++m) fd[m] = S(0.);
     for (int f = 0; f < g.faceCount; ++f) {
@@ -1736,8 +1741,16 @@ struct NS {
       if (mu_t_face) { tv = (*mu_t_face)[f]; tc = O.material.Cp() * tv / Pr_t; }
       diffusive_face_flux(fd, tv, tc);
       F.mdot[f] = (fc[0] - fd[0]) / face.area;
-      if (loads && g.face[f].bc >= 0)
-        for (int i = 0; i < 3; ++i) (*loads)[(size_t)g.face[f].bc * 3 + i] += fc[i + 1] - fd[i + 1];
+      if (loads && g.face[f].bc >= 0) {
+        S t[3];
+        for (int i = 0; i < 3; ++i) t[i] = fc[i + 1] - fd[i + 1];
+        const Vec3 r = g.face[f].centroid - O.moment_center;
+        S *L = &(*loads)[(size_t)g.face[f].bc * 6];
+        for (int i = 0; i < 3; ++i) L[i] += t[i];
+        L[3] += r[1] * t[2] - r[2] * t[1];
+        L[4] += r[2] * t[0] - r[0] * t[2];
+        L[5] += r[0] * t[1] - r[1] * t[0];
+      }
       for (int i = 0; i < 5; ++i) {
         S value = fd[i] - fc[i] + S(0.);
         rhs[(size_t)pa * 5 + i] += value;
@@ -2154,9 +2167,11 @@ void orc_rans_bcs(void *h, double *out) {
   }
 }
 
-// Boundary loads: force[bcCount][3] for state W, and (dW non-null) their
-// complex-step directional derivative along dW instead.
-int orc_loads(void *h, const double *W, const double *dW, double hstep, double *force, char *err, int errlen) {
+// Boundary loads: force[bcCount][3] (and, non-null, moment[bcCount][3] about
+// the deck's moment center) for state W, and (dW non-null) their complex-step
+// directional derivatives along dW instead.
+int orc_loads(void *h, const double *W, const double *dW, double hstep, double *force, double *moment, char *err,
+              int errlen) {
   Handle *H = static_cast<Handle *>(h);
   Oracle &O = H->O;
   Grid &g = O.grid;
@@ -2179,7 +2194,12 @@ int orc_loads(void *h, const double *W, const double *dW, double hstep, double *
     ns.calc_limiter();
     std::vector<CStep> rhs, loads;
     ns.assemble(rhs, nullptr, 0.9, &loads);
-    for (size_t k = 0; k < loads.size(); ++k) force[k] = dW ? loads[k].im / hstep : loads[k].re;
+    for (int b = 0; b < g.bcCount; ++b)
+      for (int i = 0; i < 3; ++i) {
+        const CStep &fv = loads[(size_t)b * 6 + i], &mv = loads[(size_t)b * 6 + 3 + i];
+        force[b * 3 + i] = dW ? fv.im / hstep : fv.re;
+        if (moment) moment[b * 3 + i] = dW ? mv.im / hstep : mv.re;
+      }
   } catch (const std::exception &e) {
     if (err && errlen > 0) std::snprintf(err, errlen, "%s", e.what());
     return 1;
