@@ -84,6 +84,9 @@ using namespace fcfd;  // internal header: the context mirrors the device types
 struct fcfd_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
+  // outlet-face fluxes run on `side`, forked from and joined back to `stream`
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   DevCase cs{};
   DevMesh dm{};
   const fcfd_mesh *mesh = nullptr;
@@ -131,6 +134,30 @@ inline void launch_grad_limiter(const DevCase &cs, const DevMesh &m, const S *W,
     k_grad_limiter<S, true><<<(m.nc + 127) / 128, 128, 0, s>>>(cs, m, W, ext, argx, G, Lm);
   else
     k_grad_limiter<S, false><<<(m.nc + 127) / 128, 128, 0, s>>>(cs, m, W, ext, argx, G, Lm);
+}
+// Face fluxes of one residual: the main launch over all faces and, when the
+// mesh has outlet faces, the outlet-face launch (stale right densities) on the
+// side stream, forked after the gradient kernel and joined before the gather.
+template <class S>
+inline void launch_faces(fcfd_ctx *x, Pipe<S> &P, const S *mu_t, S *mo, S *wo, cudaStream_t s) {
+  const DevMesh &m = x->dm;
+  const bool side = m.n_outlet > 0;
+  if (side) {
+    CK(cudaEventRecord(x->ev_fork, s));
+    CK(cudaStreamWaitEvent(x->side, x->ev_fork, 0));
+    const int g = (m.n_outlet + 127) / 128;
+    if (x->viscous)
+      FCFD_BY_FLUX(x->cs.flux, k_face_flux<S, true, FX, true><<<g, 128, 0, x->side>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p, mu_t, P.D.p, mo, wo, x->err.p));
+    else
+      FCFD_BY_FLUX(x->cs.flux, k_face_flux<S, false, FX, true><<<g, 128, 0, x->side>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p, mu_t, P.D.p, mo, wo, x->err.p));
+    CK(cudaEventRecord(x->ev_join, x->side));
+  }
+  const int g = (m.nf + 127) / 128;
+  if (x->viscous)
+    FCFD_BY_FLUX(x->cs.flux, k_face_flux<S, true, FX, false><<<g, 128, 0, s>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p, mu_t, P.D.p, mo, wo, x->err.p));
+  else
+    FCFD_BY_FLUX(x->cs.flux, k_face_flux<S, false, FX, false><<<g, 128, 0, s>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p, mu_t, P.D.p, mo, wo, x->err.p));
+  if (side) CK(cudaStreamWaitEvent(s, x->ev_join, 0));
 }
 void adjoint_free(fcfd_ctx *x);
 void rans_setup(fcfd_ctx *x);

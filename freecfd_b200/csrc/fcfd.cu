@@ -43,16 +43,11 @@ void launch_chain(fcfd_ctx *x, Pipe<S> &P, S *Rout, bool aos_out, S *mo, S *wo, 
     argx = x->argx.p;
   }
   launch_grad_limiter<S>(csl, m, P.W.p, x->ext.p, argx, P.G.p, P.Lm.p, s);
-  if (m.n_outlet > 0)
-    k_outlet_rho<S><<<(m.n_outlet + 127) / 128, 128, 0, s>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p);
-  if (x->viscous)
-    FCFD_BY_FLUX(x->cs.flux, k_face_flux<S, true, FX><<<(m.nf + 127) / 128, 128, 0, s>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p, (const S *)nullptr, P.D.p, mo, wo, x->err.p));
-  else
-    FCFD_BY_FLUX(x->cs.flux, k_face_flux<S, false, FX><<<(m.nf + 127) / 128, 128, 0, s>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p, (const S *)nullptr, P.D.p, mo, wo, x->err.p));
+  launch_faces<S>(x, P, (const S *)nullptr, mo, wo, s);
   if (aos_out)
-    k_gather<S, true><<<(m.nc + tb - 1) / tb, tb, 0, s>>>(m, P.D.p, Rout, x->ext.p, x->argx.p);
+    k_gather<S, true><<<(5 * m.nc + tb - 1) / tb, tb, 0, s>>>(m, P.D.p, Rout, x->ext.p, x->argx.p);
   else
-    k_gather<S, false><<<(m.nc + tb - 1) / tb, tb, 0, s>>>(m, P.D.p, Rout, x->ext.p, x->argx.p);
+    k_gather<S, false><<<(5 * m.nc + tb - 1) / tb, tb, 0, s>>>(m, P.D.p, Rout, x->ext.p, x->argx.p);
   CK(cudaGetLastError());
 }
 
@@ -179,6 +174,9 @@ int fcfd_ctx_create(const fcfd_mesh *mp, const fcfd_case *csp, int device, fcfd_
   x->device = device;
   CK(cudaSetDevice(device));
   CK(cudaStreamCreateWithFlags(&x->stream, cudaStreamNonBlocking));
+  CK(cudaStreamCreateWithFlags(&x->side, cudaStreamNonBlocking));
+  CK(cudaEventCreateWithFlags(&x->ev_fork, cudaEventDisableTiming));
+  CK(cudaEventCreateWithFlags(&x->ev_join, cudaEventDisableTiming));
   x->mesh = mp;
   x->case_ptr = csp;
   DevCase &d = x->cs;
@@ -318,6 +316,9 @@ void fcfd_ctx_destroy(fcfd_ctx *x) {
   if (x->graph) cudaGraphExecDestroy(x->graph);
   adjoint_free(x);
   rans_free(x);
+  if (x->ev_fork) cudaEventDestroy(x->ev_fork);
+  if (x->ev_join) cudaEventDestroy(x->ev_join);
+  if (x->side) cudaStreamDestroy(x->side);
   if (x->stream) cudaStreamDestroy(x->stream);
   delete x;
 }
@@ -387,9 +388,13 @@ int fcfd_local_dt(fcfd_ctx *x, const double *W, double cfl, int mode, double *dt
   API_END
 }
 
-// out[0] = average ms per residual (whole chain, CUDA-event timed on the
-// context stream); out[1..5] = ghost+minmax, grad+limiter, outlet density,
-// face flux, gather; out[6] = ms per residual from a CUDA-graph replay.
+// out[0] = average ms per residual: the whole chain (ghost states + extrema,
+// gradient + limiter, face flux with the stale outlet densities, gather)
+// between two CUDA events on the context stream, nothing else in between;
+// out[1..5] = per-kernel averages from a second pass with an event after
+// every kernel: ghost+extrema, gradient+limiter, (unused: the outlet density
+// is computed inside the face flux), face flux, gather.  L2 is flushed (a
+// 512 MB memset) before every residual when flush_l2 is set.
 int fcfd_time_residual(fcfd_ctx *x, int reps, int flush_l2, double *out, int out_len) {
   API_BEGIN
   CK(cudaSetDevice(x->device));
@@ -399,30 +404,41 @@ int fcfd_time_residual(fcfd_ctx *x, int reps, int flush_l2, double *out, int out
   Timing t;
   double acc[6] = {0, 0, 0, 0, 0, 0};
   const int tb = 256;
+  Pipe<double> &P = x->p64;
+  const bool need_ext = x->cs.limiter == 1 && x->cs.order != 1;
+  const int ng = (m.nb + tb - 1) / tb + (need_ext ? kExtremaBlocks : 0);
+  auto kernel = [&](int k) {
+    if (k == 0) {
+      if (ng > 0) k_ghost_minmax<double><<<ng, tb, 0, s>>>(x->cs, m, P.W.p, need_ext ? x->ext.p : nullptr, x->err.p);
+    } else if (k == 1) {
+      launch_grad_limiter<double>(x->cs, m, P.W.p, x->ext.p, nullptr, P.G.p, P.Lm.p, s);
+    } else if (k == 3) {
+      launch_faces<double>(x, P, nullptr, nullptr, nullptr, s);
+    } else if (k == 4) {
+      k_gather<double, false><<<(5 * m.nc + tb - 1) / tb, tb, 0, s>>>(m, P.D.p, P.R.p, x->ext.p, x->argx.p);
+    }
+  };
   for (int r = 0; r < reps; ++r) {
     if (flush_l2) CK(cudaMemsetAsync(x->flush.p, r & 0xff, x->flush.n, s));
     CK(cudaEventRecord(t.ev[0], s));
-    const bool need_ext = x->cs.limiter == 1 && x->cs.order != 1;
-    const int ng = (m.nb + tb - 1) / tb + (need_ext ? kExtremaBlocks : 0);
-    Pipe<double> &P = x->p64;
-    if (ng > 0) k_ghost_minmax<double><<<ng, tb, 0, s>>>(x->cs, m, P.W.p, need_ext ? x->ext.p : nullptr, x->err.p);
-    CK(cudaEventRecord(t.ev[1], s));
-    launch_grad_limiter<double>(x->cs, m, P.W.p, x->ext.p, nullptr, P.G.p, P.Lm.p, s);
-    CK(cudaEventRecord(t.ev[2], s));
-    if (m.n_outlet > 0)
-      k_outlet_rho<double><<<(m.n_outlet + 127) / 128, 128, 0, s>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p);
-    CK(cudaEventRecord(t.ev[3], s));
-    if (x->viscous)
-      FCFD_BY_FLUX(x->cs.flux, k_face_flux<double, true, FX><<<(m.nf + 127) / 128, 128, 0, s>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p, nullptr, P.D.p, nullptr, nullptr, x->err.p));
-    else
-      FCFD_BY_FLUX(x->cs.flux, k_face_flux<double, false, FX><<<(m.nf + 127) / 128, 128, 0, s>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p, nullptr, P.D.p, nullptr, nullptr, x->err.p));
-    CK(cudaEventRecord(t.ev[4], s));
-    k_gather<double, false><<<(m.nc + tb - 1) / tb, tb, 0, s>>>(m, P.D.p, P.R.p, x->ext.p, x->argx.p);
+    for (int k = 0; k < 5; ++k) kernel(k);
     CK(cudaEventRecord(t.ev[5], s));
     CK(cudaGetLastError());
     CK(cudaEventSynchronize(t.ev[5]));
     float ms;
-    CK(cudaEventElapsedTime(&ms, t.ev[0], t.ev[5])); acc[0] += ms;
+    CK(cudaEventElapsedTime(&ms, t.ev[0], t.ev[5]));
+    acc[0] += ms;
+  }
+  for (int r = 0; r < reps; ++r) {
+    if (flush_l2) CK(cudaMemsetAsync(x->flush.p, r & 0xff, x->flush.n, s));
+    CK(cudaEventRecord(t.ev[0], s));
+    for (int k = 0; k < 5; ++k) {
+      kernel(k);
+      CK(cudaEventRecord(t.ev[k + 1], s));
+    }
+    CK(cudaGetLastError());
+    CK(cudaEventSynchronize(t.ev[5]));
+    float ms;
     for (int k = 0; k < 5; ++k) { CK(cudaEventElapsedTime(&ms, t.ev[k], t.ev[k + 1])); acc[k + 1] += ms; }
   }
   for (int k = 0; k < 6 && k < out_len; ++k) out[k] = acc[k] / reps;

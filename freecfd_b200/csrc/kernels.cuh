@@ -537,9 +537,6 @@ __global__ void __launch_bounds__(128, (!FAST && std::is_same<S, double>::value)
   const int nc = m.nc, nt = m.nt;
   if (c >= nc) return;
   const double xc0 = m.c_x[c], xc1 = m.c_x[nt + c], xc2 = m.c_x[2 * nt + c];
-  const double C00 = m.st_cof[c], C01 = m.st_cof[nc + c], C02 = m.st_cof[2 * nc + c];
-  const double C11 = m.st_cof[3 * nc + c], C12 = m.st_cof[4 * nc + c], C22 = m.st_cof[5 * nc + c];
-  const double det = m.st_cof[6 * nc + c];
   S g[15];
 #pragma unroll
   for (int i = 0; i < 15; ++i) g[i] = S(0.);
@@ -557,6 +554,7 @@ __global__ void __launch_bounds__(128, (!FAST && std::is_same<S, double>::value)
     S acc[15];
 #pragma unroll
     for (int i = 0; i < 15; ++i) acc[i] = S(0.);
+#pragma unroll 4
     for (int j = j0; j < j1; ++j) {
       const int k = m.st_keys[j];
       if (k == c) continue;
@@ -570,7 +568,9 @@ __global__ void __launch_bounds__(128, (!FAST && std::is_same<S, double>::value)
         acc[3 * v + 2] = acc[3 * v + 2] + a * d2;
       }
     }
-    const double id = 1. / det;
+    const double C00 = m.st_cof[c], C01 = m.st_cof[nc + c], C02 = m.st_cof[2 * nc + c];
+    const double C11 = m.st_cof[3 * nc + c], C12 = m.st_cof[4 * nc + c], C22 = m.st_cof[5 * nc + c];
+    const double id = 1. / m.st_cof[6 * nc + c];
     const double M0 = m.st_mirror[c], M1 = m.st_mirror[nc + c], M2 = m.st_mirror[2 * nc + c];
 #pragma unroll
     for (int v = 0; v < 5; ++v) {
@@ -583,6 +583,11 @@ __global__ void __launch_bounds__(128, (!FAST && std::is_same<S, double>::value)
     // Bit-exact: every weight rebuilt with the reference's rounded operations.
     // The division by det uses the reciprocal with one fused correction where
     // the mesh builder verified it returns the IEEE quotient for every weight.
+    // (Weights precomputed on the host and streamed from HBM measured slower:
+    // 200 against 190 us on the prism mesh.)
+    const double C00 = m.st_cof[c], C01 = m.st_cof[nc + c], C02 = m.st_cof[2 * nc + c];
+    const double C11 = m.st_cof[3 * nc + c], C12 = m.st_cof[4 * nc + c], C22 = m.st_cof[5 * nc + c];
+    const double det = m.st_cof[6 * nc + c];
     const double rc = m.st_recip[c];
     auto qdiv = [&](double x) -> double {
       if (rc != 0.) {
@@ -1107,11 +1112,15 @@ __device__ __forceinline__ void face_D(const DevCase &cs, const DevMesh &m, int 
 }
 
 // Left / right states of face f (reconstruction, or the boundary condition
-// with the cached density where the BC branch leaves it untouched).
-template <class S>
-__device__ __forceinline__ void face_states(const DevCase &cs, const DevMesh &m, int f, const double n[3], int b, int pa,
+// with the cached density where the BC branch leaves it untouched).  STALE:
+// 0 reads the cached density from `stale`; 1 returns false instead (the face
+// is left to the outlet kernel); 2 computes it here (the walk back of
+// cached_right_rho) and stores it in `stale`.  Returns true when the states
+// are complete.
+template <class S, int STALE = 0>
+__device__ __forceinline__ bool face_states(const DevCase &cs, const DevMesh &m, int f, const double n[3], int b, int pa,
                                             int nb, const S *__restrict__ W, const S *__restrict__ G, const S *__restrict__ Lm,
-                                            const S *__restrict__ stale, FState<S> &L, FState<S> &R, int *err) {
+                                            S *stale, FState<S> &L, FState<S> &R, int *err) {
   const int nf = m.nf, nt = m.nt, nc = m.nc;
   const double xf[3] = {m.f_x[f], m.f_x[nf + f], m.f_x[2 * nf + f]};
   recon_state(cs, m, W, G, Lm, pa, xf, L, n);
@@ -1120,25 +1129,42 @@ __device__ __forceinline__ void face_states(const DevCase &cs, const DevMesh &m,
   } else {
     R.pc = W[nb]; R.Vc[0] = W[nt + nb]; R.Vc[1] = W[2 * nt + nb]; R.Vc[2] = W[3 * nt + nb]; R.Tc = W[4 * nt + nb];
     R.rho = S(0.);
-    if (!apply_bc(cs, cs.bc[b], L, R, n, err)) R.rho = stale[nb - nc];
+    if (!apply_bc(cs, cs.bc[b], L, R, n, err)) {
+      if (STALE == 1) return false;
+      if (STALE == 2) {
+        R.rho = cached_right_rho(cs, m, W, G, Lm, f);
+        stale[nb - nc] = R.rho;
+      } else {
+        R.rho = stale[nb - nc];
+      }
+    } else if (STALE == 2) {
+      return false;
+    }
     finish(cs, R, n);
   }
+  return true;
 }
 
 // Face flux: reconstruction, BCs, inviscid + viscous flux; D = Fd - Fc.
-template <class S, bool VISCOUS, int FX>
+// OUTLET = false: every face except the outlet faces whose BC branch leaves
+// the right density to the state cache; OUTLET = true: those faces only
+// (thread i takes outlet face i), with the cached density computed in place
+// and stored in `stale` for the face-Jacobian kernel.  The two launches write
+// disjoint faces and run concurrently.
+template <class S, bool VISCOUS, int FX, bool OUTLET>
 __global__ void __launch_bounds__(128) k_face_flux(DevCase cs, DevMesh m, const S *__restrict__ W, const S *__restrict__ G,
-                                                   const S *__restrict__ Lm, const S *__restrict__ stale,
+                                                   const S *__restrict__ Lm, S *stale,
                                                    const S *__restrict__ mu_t, S *__restrict__ D, S *__restrict__ mdot_out,
                                                    S *__restrict__ wl_out, int *err) {
-  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int nf = m.nf;
-  if (f >= nf) return;
+  if (i >= (OUTLET ? m.n_outlet : nf)) return;
+  const int f = OUTLET ? m.outlet_faces[i] : i;
   const int pa = m.f_parent[f], nb = m.f_neighbor[f], b = m.f_bc[f];
   const double n[3] = {m.f_n[f], m.f_n[nf + f], m.f_n[2 * nf + f]};
   const double A = m.f_area[f];
   FState<S> L, R;
-  face_states(cs, m, f, n, b, pa, nb, W, G, Lm, stale, L, R, err);
+  if (!face_states<S, OUTLET ? 2 : 1>(cs, m, f, n, b, pa, nb, W, G, Lm, stale, L, R, err)) return;
   S Dv[5], wL;
   const GlobalGrad<S> gs{G, m.nc, pa, nb};
   face_D<S, GlobalGrad<S>, VISCOUS, FX>(cs, m, f, n, A, b, pa, nb, L, R, gs, mu_t, Dv, wL);
@@ -1165,28 +1191,35 @@ __device__ __forceinline__ void reset_extrema(unsigned long long *ext, int *argx
 template <class S, bool AOS>
 __global__ void k_gather(DevMesh m, const S *__restrict__ D, S *__restrict__ R, unsigned long long *ext, int *argx) {
   reset_extrema(ext, argx);
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= m.nc) return;
-  const int nf = m.nf;
-  S r[5] = {S(0.), S(0.), S(0.), S(0.), S(0.)};
-  for (int j = m.cf_index[c]; j < m.cf_index[c + 1]; ++j) {
+  // one thread per (cell, equation): 5 nc threads, equation-major so that a
+  // warp covers consecutive cells of one equation
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nc = m.nc;
+  if (t >= 5 * nc) return;
+  const int v = t / nc, c = t - v * nc;
+  const S *Dv = D + (size_t)v * m.nf;
+  const int j0 = m.cf_index[c], j1 = m.cf_index[c + 1];
+  S r = S(0.);
+  int j = j0;
+  // face ids first (up to 6 at once), then the D values, summed in ascending
+  // face order
+  for (; j + 6 <= j1; j += 6) {
+    int e[6];
+#pragma unroll
+    for (int q = 0; q < 6; ++q) e[q] = m.cf_list[j + q];
+    S d[6];
+#pragma unroll
+    for (int q = 0; q < 6; ++q) d[q] = Dv[e[q] >= 0 ? e[q] : ~e[q]];
+#pragma unroll
+    for (int q = 0; q < 6; ++q) r = r + ((e[q] >= 0 ? d[q] : -1. * d[q]) + 0.);
+  }
+  for (; j < j1; ++j) {
     const int e = m.cf_list[j];
-    if (e >= 0) {
-#pragma unroll
-      for (int v = 0; v < 5; ++v) r[v] = r[v] + (D[v * nf + e] + 0.);
-    } else {
-      const int f = ~e;
-#pragma unroll
-      for (int v = 0; v < 5; ++v) r[v] = r[v] + (-1. * D[v * nf + f] + 0.);
-    }
+    if (e >= 0) r = r + (Dv[e] + 0.);
+    else r = r + (-1. * Dv[~e] + 0.);
   }
-  if (AOS) {
-#pragma unroll
-    for (int v = 0; v < 5; ++v) R[5 * c + v] = r[v];
-  } else {
-#pragma unroll
-    for (int v = 0; v < 5; ++v) R[v * m.nc + c] = r[v];
-  }
+  if (AOS) R[5 * c + v] = r;
+  else R[(size_t)v * nc + c] = r;
 }
 
 // Local time step (time_step.cc:143-224).

@@ -69,7 +69,7 @@ __global__ void __launch_bounds__(128) k_face_jac(DevCase cs, DevMesh m, const d
   const double n[3] = {m.f_n[f], m.f_n[nf + f], m.f_n[2 * nf + f]};
   const double A = m.f_area[f];
   FState<double> L, R;
-  face_states(cs, m, f, n, b, pa, nb, W, G, Lm, stale, L, R, (int *)nullptr);
+  face_states(cs, m, f, n, b, pa, nb, W, G, Lm, const_cast<double *>(stale), L, R, (int *)nullptr);
   FState<D5> Ld, Rd;
   D5 D[5], wl;
   const GlobalGrad<double> gs{G, m.nc, pa, nb};

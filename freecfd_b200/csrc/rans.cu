@@ -262,11 +262,8 @@ static void rans_chain(fcfd_ctx *x, double *R_aos, double *RK_aos, cudaEvent_t *
   k_rans_prep<<<(m.nt + 127) / 128, 128, 0, st>>>(x->cs, m, P.W.p, s.K.p, s.mut.p, x->case_ptr->visc_ratio_limit);
   k_rans_mutf<<<(m.nf + 127) / 128, 128, 0, st>>>(x->cs, m, s.mut.p, s.mutf.p);
   launch_grad_limiter<double>(x->cs, m, P.W.p, x->ext.p, nullptr, P.G.p, P.Lm.p, st);
-  if (m.n_outlet > 0)
-    k_outlet_rho<double><<<(m.n_outlet + 127) / 128, 128, 0, st>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p);
-  FCFD_BY_FLUX(x->cs.flux, k_face_flux<double, true, FX><<<(m.nf + 127) / 128, 128, 0, st>>>(
-                               x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p, s.mutf.p, P.D.p, x->mdot.p, x->wl.p, x->err.p));
-  k_gather<double, true><<<(m.nc + tb - 1) / tb, tb, 0, st>>>(m, P.D.p, R_aos, x->ext.p, x->argx.p);
+  launch_faces<double>(x, P, s.mutf.p, x->mdot.p, x->wl.p, st);
+  k_gather<double, true><<<(5 * m.nc + tb - 1) / tb, tb, 0, st>>>(m, P.D.p, R_aos, x->ext.p, x->argx.p);
   if (ev) CK(cudaEventRecord(ev[1], st));
   k_rans_grad<<<(m.nc + 127) / 128, 128, 0, st>>>(m, s.K.p, s.GK.p);
   k_rans_face<<<(m.nf + 127) / 128, 128, 0, st>>>(x->cs, m, P.W.p, s.K.p, s.GK.p, s.mutf.p, x->mdot.p, x->wl.p, s.DK.p);
