@@ -26,7 +26,7 @@ EXPORTED = [
     "fcfd_mesh_lsq",
     "fcfd_ctx_create", "fcfd_ctx_destroy", "fcfd_ctx_set_exact_gradients", "fcfd_residual", "fcfd_last_stages", "fcfd_local_dt",
     "fcfd_time_residual", "fcfd_point_flux", "fcfd_jvp", "fcfd_vjp", "fcfd_drag", "fcfd_rans_residual", "fcfd_rans_bcs", "fcfd_time_rans", "fcfd_newton_solve", "fcfd_local_dt_cflmax_noalloc",
-    "fcfd_run", "fcfd_restart_write", "fcfd_restart_read",
+    "fcfd_run", "fcfd_restart_write", "fcfd_restart_read", "fcfd_mesh_from_tecplot",
 ]
 
 
@@ -116,6 +116,8 @@ def _load():
                                                 ctypes.c_double, ctypes.c_double, ctypes.c_double, vp, vp]
     L.fcfd_time_residual.argtypes = [vp, ctypes.c_int, ctypes.c_int, dp, ctypes.c_int]
     L.fcfd_run.argtypes = [vp, dp, ctypes.POINTER(RunOpts), ctypes.POINTER(RunReport)]
+    L.fcfd_mesh_from_tecplot.argtypes = [ctypes.c_char_p, vp, ctypes.POINTER(ctypes.c_void_p), ctypes.c_char_p,
+                                         ctypes.c_int32]
     L.fcfd_restart_write.argtypes = [ctypes.c_char_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_double, dp, dp,
                                      ctypes.c_int32, ctypes.c_int32, dp, dp, dp, dp]
     L.fcfd_restart_read.argtypes = [ctypes.c_char_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, dp, dp, dp,

@@ -542,3 +542,83 @@ CONFIGS = {
     "hypersonic": hypersonic_case,
     "plate": plate_case,
 }
+
+
+# ----------------------------------------------------------------------------
+# Tecplot FEPolyhedron grid files (the face-based input of grid_reader_tec.cc)
+# ----------------------------------------------------------------------------
+
+# element face tables (local node numbers, normals pointing out of the cell)
+_ELEMENT_FACES = {
+    8: ((0, 3, 2, 1), (4, 5, 6, 7), (1, 2, 6, 5), (0, 4, 7, 3), (1, 5, 4, 0), (2, 3, 7, 6)),
+    6: ((0, 2, 1), (3, 4, 5), (0, 3, 5, 2), (1, 2, 5, 4), (0, 1, 4, 3)),
+    5: ((0, 3, 2, 1), (0, 1, 4), (1, 2, 4), (3, 4, 2), (0, 4, 3)),
+    4: ((0, 2, 1), (1, 2, 3), (0, 3, 2), (0, 1, 3)),
+}
+
+
+def mesh_faces(mesh: RawMesh, order: str = "cells", seed: int = 0):
+    """Faces of a CELL-type mesh: node lists oriented out of the left cell,
+    left / right cells (0-based, -1 for a boundary face).  ``order`` "cells"
+    lists them as the cells are visited (each face once, by its first cell);
+    "shuffled" permutes that list with ``seed``."""
+    first = {}
+    faces, left, right = [], [], []
+    for c in range(mesh.n_cells):
+        nodes = mesh.conn[mesh.conn_index[c]:mesh.conn_index[c + 1]]
+        for t in _ELEMENT_FACES[len(nodes)]:
+            fn = tuple(int(nodes[k]) for k in t)
+            key = tuple(sorted(fn))
+            if key in first:
+                right[first[key]] = c
+            else:
+                first[key] = len(faces)
+                faces.append(fn)
+                left.append(c)
+                right.append(-1)
+    if order == "shuffled":
+        perm = np.random.default_rng(seed).permutation(len(faces))
+        faces = [faces[i] for i in perm]
+        left = [left[i] for i in perm]
+        right = [right[i] for i in perm]
+    return faces, np.array(left, np.int64), np.array(right, np.int64)
+
+
+def write_tecplot(mesh: RawMesh, path: str, bc_names=None, order: str = "cells", seed: int = 0) -> str:
+    """Write ``mesh`` as a Tecplot FEPolyhedron file in the layout
+    grid_reader_tec.cc reads: volume zone (block-packed coordinates, face node
+    counts, 1-based face nodes, left and right elements, each block after one
+    comment line), then one zone per BC region (``ZONE T="name"`` on its own
+    line, then its node count and the coordinates of its nodes)."""
+    faces, left, right = mesh_faces(mesh, order, seed)
+    names = bc_names or ["BC_%d" % (b + 1) for b in range(len(mesh.bc_nodes))]
+
+    def block(vals, fmt):
+        out = []
+        for i in range(0, len(vals), 8):
+            out.append(" ".join(fmt % v for v in vals[i:i + 8]))
+        return "\n".join(out) + "\n"
+
+    nn = mesh.nodes.shape[0]
+    with open(path, "w") as fh:
+        fh.write('TITLE="freecfd_b200 grid"\nVARIABLES="X","Y","Z"\nZONE T="volume"\n')
+        fh.write("ZONETYPE=FEPolyhedron, DATAPACKING=BLOCK, Nodes=%d, Elements=%d, Faces=%d, TotalNumFaceNodes=%d, "
+                 "NumConnectedBoundaryFaces=0, TotalNumBoundaryConnections=0\n"
+                 % (nn, mesh.n_cells, len(faces), sum(len(f) for f in faces)))
+        for i in range(3):
+            fh.write(block([float(x) for x in mesh.nodes[:, i]], "%.17g"))
+        fh.write("# node count per face\n")
+        fh.write(block([len(f) for f in faces], "%d"))
+        fh.write("# face nodes\n")
+        fh.write(block([n + 1 for f in faces for n in f], "%d"))
+        fh.write("# left elements\n")
+        fh.write(block([int(c) + 1 for c in left], "%d"))
+        fh.write("# right elements\n")
+        fh.write(block([int(c) + 1 for c in right], "%d"))
+        for b, nodes in enumerate(mesh.bc_nodes):
+            nodes = np.asarray(nodes)
+            fh.write('ZONE T="%s"\n' % names[b])
+            fh.write("ZONETYPE=FEQUADRILATERAL, DATAPACKING=BLOCK, Nodes=%d, Elements=0\n" % len(nodes))
+            for i in range(3):
+                fh.write(block([float(x) for x in mesh.nodes[nodes, i]], "%.17g"))
+    return path

@@ -113,7 +113,8 @@ struct fcfd_ctx {
   DBuf<int> err, argx;
   DBuf<unsigned char> flush;
   int n_outlet = 0;
-  cudaGraphExec_t graph = nullptr;
+  cudaGraphExec_t graph = nullptr;  // the timed residual chain
+  int graph_fast_grad = -1;
   bool newton_frozen = false;
   bool newton_f32 = false;  // Krylov matvecs through the FP32 tangent chain
 };

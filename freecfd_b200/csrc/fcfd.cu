@@ -20,7 +20,7 @@ extern template __global__ void k_ghost_minmax<Dual<double>>(DevCase, DevMesh, D
 extern template __global__ void k_ghost_minmax<Dual<float>>(DevCase, DevMesh, Dual<float> *, unsigned long long *, int *);
 
 fcfd_case *read_deck(const std::string &path);
-fcfd_mesh *build_mesh(const fcfd_raw_mesh &raw, fcfd_case &cs);
+fcfd_mesh *build_mesh(const fcfd_raw_mesh &raw, fcfd_case &cs, const FaceInput *faces = nullptr);
 
 static thread_local std::string g_last_error;
 void set_last_error(const std::string &m) { g_last_error = m; }
@@ -389,8 +389,8 @@ int fcfd_local_dt(fcfd_ctx *x, const double *W, double cfl, int mode, double *dt
 }
 
 // out[0] = average ms per residual: the whole chain (ghost states + extrema,
-// gradient + limiter, face flux with the stale outlet densities, gather)
-// between two CUDA events on the context stream, nothing else in between;
+// gradient + limiter, face flux with the stale outlet densities, gather),
+// replayed as one CUDA graph between two CUDA events on the context stream;
 // out[1..5] = per-kernel averages from a second pass with an event after
 // every kernel: ghost+extrema, gradient+limiter, (unused: the outlet density
 // is computed inside the face flux), face flux, gather.  L2 is flushed (a
@@ -418,10 +418,22 @@ int fcfd_time_residual(fcfd_ctx *x, int reps, int flush_l2, double *out, int out
       k_gather<double, false><<<(5 * m.nc + tb - 1) / tb, tb, 0, s>>>(m, P.D.p, P.R.p, x->ext.p, x->argx.p);
     }
   };
+  // the chain as one CUDA graph (captured once per context and case
+  // settings), replayed between the two events
+  if (!x->graph || x->graph_fast_grad != x->cs.fast_grad) {
+    if (x->graph) { cudaGraphExecDestroy(x->graph); x->graph = nullptr; }
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    for (int k = 0; k < 5; ++k) kernel(k);
+    CK(cudaStreamEndCapture(s, &g));
+    CK(cudaGraphInstantiate(&x->graph, g, 0));
+    CK(cudaGraphDestroy(g));
+    x->graph_fast_grad = x->cs.fast_grad;
+  }
   for (int r = 0; r < reps; ++r) {
     if (flush_l2) CK(cudaMemsetAsync(x->flush.p, r & 0xff, x->flush.n, s));
     CK(cudaEventRecord(t.ev[0], s));
-    for (int k = 0; k < 5; ++k) kernel(k);
+    CK(cudaGraphLaunch(x->graph, s));
     CK(cudaEventRecord(t.ev[5], s));
     CK(cudaGetLastError());
     CK(cudaEventSynchronize(t.ev[5]));

@@ -66,6 +66,14 @@ struct TimeMarching {
   std::string schedule_file;  // empty: none
   int ps_steps = 1;           // pseudotime -> numberofsteps (dual time stepping when > 1)
 };
+// Faces of a face-based grid (the FACE raw type of grid_reader_tec.cc): node
+// lists (0-based global node ids, CSR) and left / right cells (-1: none), in
+// file order.
+struct FaceInput {
+  int n_faces = 0;
+  const int32_t *index = nullptr, *nodes = nullptr, *left = nullptr, *right = nullptr;
+};
+
 // Parses the timemarching / pseudotime sections of a deck file (also used to
 // re-read them every `updatefrequency` steps, update_time_step_options).
 TimeMarching read_time_marching(const std::string &path);

@@ -71,7 +71,10 @@ bool in_box(const P3 &p, const double *c1, const double *c2) {
 
 }  // namespace
 
-fcfd_mesh *build_mesh(const fcfd_raw_mesh &raw, fcfd_case &cs) {
+// `faces` non-null: a face-based grid (create_faces2,
+// grid_create_elements.cc:444-553), whose cell node lists in `raw` are the
+// sorted node sets of the cells (grid_reader_tec.cc:236-262).
+fcfd_mesh *build_mesh(const fcfd_raw_mesh &raw, fcfd_case &cs, const FaceInput *faces) {
   auto M = new fcfd_mesh();
   fcfd_mesh &m = *M;
   try {
@@ -143,9 +146,68 @@ fcfd_mesh *build_mesh(const fcfd_raw_mesh &raw, fcfd_case &cs) {
       throw Error(FCFD_ERR_MESH, "unsupported element with " + std::to_string(nn) + " nodes");
     };
     std::unordered_map<FaceKey, std::pair<int32_t, int32_t>, FaceKeyHash> first;  // key -> (cell, other cell)
-    first.reserve((size_t)nc * 4);
+    first.reserve(faces ? 0 : (size_t)nc * 4);
     std::vector<int32_t> cell_nf(nc);
-    for (int c = 0; c < nc; ++c) {
+    // boundary face -> BC region by the region node sets (grid_create_elements.cc:318-363,
+    // 498-541): the face's nodes must all be in the region; where several
+    // regions match, the first one that does not also hold every node of the
+    // parent cell wins; -2 (UNASSIGNED_FACE) when none matches
+    auto match_bc = [&](const int *fn, int fnn, int c) {
+      std::vector<int> matched;
+      int cell_matched = -1;
+      for (int b = 0; b < nbc; ++b) {
+        bool all = true;
+        for (int k = 0; k < fnn; ++k) if (!bcmask[b][fn[k]]) { all = false; break; }
+        if (all) matched.push_back(b);
+        if (cell_matched == -1) {
+          bool callm = true;
+          for (int k = raw.conn_index[c]; k < raw.conn_index[c + 1]; ++k) if (!bcmask[b][cnodes[k]]) { callm = false; break; }
+          if (callm) cell_matched = b;
+        }
+      }
+      int bcv = -2;
+      if (matched.size() > 1) {
+        for (int b : matched) if (b != cell_matched) { bcv = b; break; }
+      } else if (matched.size() == 1) {
+        bcv = matched[0];
+      }
+      return bcv;
+    };
+    m.cf_index.assign(nc + 1, 0);
+    std::vector<std::vector<int32_t>> cfaces(nc);
+    if (faces) {
+      // file order; parent = left cell, neighbour = right cell.  The
+      // reference first pads every cell's face list with one zero per face
+      // (a resize meant as a reserve, grid_create_elements.cc:107-121) and
+      // then appends the faces, which would add face 0 to every cell's
+      // volume and stencil; the lists here hold the cell's faces only.
+      for (int f = 0; f < faces->n_faces; ++f) {
+        const int pa = faces->left[f], nb = faces->right[f];
+        if (pa < 0 || pa >= nc) throw Error(FCFD_ERR_MESH, "face " + std::to_string(f) + " has no left cell");
+        if (nb >= nc) throw Error(FCFD_ERR_MESH, "face " + std::to_string(f) + " has a right cell out of range");
+        const int fnn = faces->index[f + 1] - faces->index[f];
+        if (fnn < 3 || fnn > 4) throw Error(FCFD_ERR_UNSUPPORTED, "faces with " + std::to_string(fnn) + " nodes are not supported");
+        int fn[4] = {-1, -1, -1, -1};
+        for (int k = 0; k < fnn; ++k) {
+          const int gid = faces->nodes[faces->index[f] + k];
+          if (gid < 0 || gid >= raw.n_nodes || g2l[gid] < 0) throw Error(FCFD_ERR_MESH, "face node out of range");
+          fn[k] = g2l[gid];
+        }
+        int bcv = -1;
+        if (nb < 0) {
+          bcv = match_bc(fn, fnn, pa);
+          if (bcv < 0) throw Error(FCFD_ERR_MESH, "couldn't find BC for face " + std::to_string(f));
+        }
+        m.f_parent.push_back(pa);
+        m.f_neighbor.push_back(nb);
+        m.f_bc.push_back(bcv);
+        for (int k = 0; k < 4; ++k) m.f_nodes.push_back(fn[k]);
+        m.f_nn.push_back((uint8_t)fnn);
+        cfaces[pa].push_back(f);
+        if (nb >= 0) cfaces[nb].push_back(f);
+      }
+    }
+    for (int c = 0; c < nc && !faces; ++c) {
       int nn = raw.conn_index[c + 1] - raw.conn_index[c];
       int nfc = nfaces_of(nn);
       cell_nf[c] = nfc;
@@ -163,9 +225,7 @@ fcfd_mesh *build_mesh(const fcfd_raw_mesh &raw, fcfd_case &cs) {
         }
       }
     }
-    m.cf_index.assign(nc + 1, 0);
-    std::vector<std::vector<int32_t>> cfaces(nc);
-    for (int c = 0; c < nc; ++c) {
+    for (int c = 0; c < nc && !faces; ++c) {
       int nn = raw.conn_index[c + 1] - raw.conn_index[c];
       for (int cf = 0; cf < cell_nf[c]; ++cf) {
         const int *t = ftable(nn, cf);
@@ -180,27 +240,7 @@ fcfd_mesh *build_mesh(const fcfd_raw_mesh &raw, fcfd_case &cs) {
         m.f_parent.push_back(c);
         int nb = own.second;
         int bcv = -1;  // INTERNAL_FACE
-        if (nb < 0) {
-          // boundary: match against BC node sets (grid_create_elements.cc:318-363)
-          std::vector<int> matched;
-          int cell_matched = -1;
-          for (int b = 0; b < nbc; ++b) {
-            bool all = true;
-            for (int k = 0; k < fnn; ++k) if (!bcmask[b][fn[k]]) { all = false; break; }
-            if (all) matched.push_back(b);
-            if (cell_matched == -1) {
-              bool callm = true;
-              for (int k = raw.conn_index[c]; k < raw.conn_index[c + 1]; ++k) if (!bcmask[b][cnodes[k]]) { callm = false; break; }
-              if (callm) cell_matched = b;
-            }
-          }
-          bcv = -2;  // UNASSIGNED_FACE
-          if (matched.size() > 1) {
-            for (int b : matched) if (b != cell_matched) { bcv = b; break; }
-          } else if (matched.size() == 1) {
-            bcv = matched[0];
-          }
-        }
+        if (nb < 0) bcv = match_bc(fn, fnn, c);
         m.f_neighbor.push_back(nb);
         m.f_bc.push_back(bcv);
         for (int k = 0; k < 4; ++k) m.f_nodes.push_back(fn[k]);

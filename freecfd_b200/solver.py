@@ -54,15 +54,24 @@ class Case:
 class Mesh:
     """Reference-order connectivity, geometry and LSQ stencils (Grid)."""
 
-    def __init__(self, raw, case: Case):
-        self._keep = [np.ascontiguousarray(raw.nodes, np.float64), np.ascontiguousarray(raw.conn_index, np.int32),
-                      np.ascontiguousarray(raw.conn, np.int32)]
-        bidx, bflat = raw.bc_csr()
-        self._keep += [np.ascontiguousarray(bidx, np.int32), np.ascontiguousarray(bflat, np.int32)]
-        nodes, cidx, conn, bidx, bflat = self._keep
-        r = _RawMesh(nodes.shape[0], _d(nodes), raw.n_cells, _i(cidx), _i(conn), len(raw.bc_nodes), _i(bidx), _i(bflat))
+    def __init__(self, raw, case: Case, tecplot: str = None):
+        """From a CELL-type raw grid, or (``tecplot`` = path, raw None) from a
+        Tecplot FEPolyhedron grid file (Grid::readTEC + create_faces2)."""
         h = ctypes.c_void_p()
-        check(lib.fcfd_mesh_create(ctypes.byref(r), case.h, ctypes.byref(h)))
+        self.bc_names = []
+        if tecplot is not None:
+            names = ctypes.create_string_buffer(4096)
+            check(lib.fcfd_mesh_from_tecplot(os.fsencode(str(tecplot)), case.h, ctypes.byref(h), names, 4096))
+            self.bc_names = [s for s in names.value.decode().split("\n") if s]
+        else:
+            self._keep = [np.ascontiguousarray(raw.nodes, np.float64), np.ascontiguousarray(raw.conn_index, np.int32),
+                          np.ascontiguousarray(raw.conn, np.int32)]
+            bidx, bflat = raw.bc_csr()
+            self._keep += [np.ascontiguousarray(bidx, np.int32), np.ascontiguousarray(bflat, np.int32)]
+            nodes, cidx, conn, bidx, bflat = self._keep
+            r = _RawMesh(nodes.shape[0], _d(nodes), raw.n_cells, _i(cidx), _i(conn), len(raw.bc_nodes), _i(bidx),
+                         _i(bflat))
+            check(lib.fcfd_mesh_create(ctypes.byref(r), case.h, ctypes.byref(h)))
         self.h = h
         s = (ctypes.c_int64 * 8)()
         check(lib.fcfd_mesh_sizes(self.h, s))

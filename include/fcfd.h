@@ -84,6 +84,14 @@ int fcfd_case_summary(const fcfd_case *cs, double *dv, int32_t *iv, int32_t iv_l
  * (src/gradient_maps.cc:39-78, src/lsqr_grad_map.cc:32-99). */
 int fcfd_mesh_create(const fcfd_raw_mesh *raw, const fcfd_case *cs, fcfd_mesh **out);
 void fcfd_mesh_destroy(fcfd_mesh *m);
+/* Read a Tecplot FEPolyhedron grid file (the deck's `format=tecplot`,
+ * Grid::readTEC src/grid/grid_reader_tec.cc:36-278) and build the mesh from
+ * its faces (Grid::create_faces2, grid_create_elements.cc:444-553): face
+ * order, parent / neighbour = the file's left / right elements, boundary
+ * regions from the boundary zones in file order (BC_1 = first zone).  Faces
+ * have 3 or 4 nodes.  bc_names (may be NULL) receives the zone names,
+ * newline-separated. */
+int fcfd_mesh_from_tecplot(const char *path, const fcfd_case *cs, fcfd_mesh **out, char *bc_names, int32_t bc_names_len);
 /* out[8] = n_cells, n_faces, n_ghosts, n_total, n_nodes, stencil entries,
  *          cell-face entries, neighbour entries */
 int fcfd_mesh_sizes(const fcfd_mesh *m, int64_t *out);

@@ -40,6 +40,8 @@ def lib():
         dp = ctypes.POINTER(ctypes.c_double)
         ip = ctypes.POINTER(ctypes.c_int)
         L.orc_create.restype = vp
+        L.orc_create_tecplot.restype = vp
+        L.orc_create_tecplot.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int]
         L.orc_create.argtypes = [ctypes.c_char_p, ctypes.c_int, dp, ctypes.c_int, ip, ip, ctypes.c_int, ip, ip,
                                  ctypes.c_char_p, ctypes.c_int]
         L.orc_destroy.argtypes = [vp]
@@ -75,21 +77,26 @@ def _i(a):
 class Oracle:
     """Handle on one oracle grid + case (reference ordering throughout)."""
 
-    def __init__(self, case, workdir: str | None = None):
+    def __init__(self, case, workdir: str | None = None, tecplot: str | None = None):
+        """The case's deck with its CELL-type mesh, or (``tecplot`` = path) with
+        the Tecplot FEPolyhedron grid file read by the restated readTEC."""
         L = lib()
         self._tmp = None
         if workdir is None:
             self._tmp = tempfile.TemporaryDirectory()
             workdir = self._tmp.name
         deck = case.write_deck(workdir)
-        m = case.mesh
-        nodes = np.ascontiguousarray(m.nodes, dtype=np.float64)
-        cidx = np.ascontiguousarray(m.conn_index, dtype=np.int32)
-        conn = np.ascontiguousarray(m.conn, dtype=np.int32)
-        bidx, bflat = m.bc_csr()
         err = ctypes.create_string_buffer(512)
-        self.h = L.orc_create(deck.encode(), nodes.shape[0], _d(nodes), m.n_cells, _i(cidx), _i(conn),
-                              len(m.bc_nodes), _i(bidx), _i(bflat), err, 512)
+        if tecplot is not None:
+            self.h = L.orc_create_tecplot(deck.encode(), str(tecplot).encode(), err, 512)
+        else:
+            m = case.mesh
+            nodes = np.ascontiguousarray(m.nodes, dtype=np.float64)
+            cidx = np.ascontiguousarray(m.conn_index, dtype=np.int32)
+            conn = np.ascontiguousarray(m.conn, dtype=np.int32)
+            bidx, bflat = m.bc_csr()
+            self.h = L.orc_create(deck.encode(), nodes.shape[0], _d(nodes), m.n_cells, _i(cidx), _i(conn),
+                                  len(m.bc_nodes), _i(bidx), _i(bflat), err, 512)
         if not self.h:
             raise RuntimeError("oracle: " + err.value.decode())
         s = (ctypes.c_longlong * 8)()

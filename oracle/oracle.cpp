@@ -297,7 +297,8 @@ struct KOmega {
 // ================================================================ grid setup
 
 // grid_create_elements.cc:27-182 (single partition: every cell is owned by rank 0)
-static void create_nodes_cells(Grid &g, const double *xyz, int n_nodes, int n_cells, const int *cidx, const int *conn) {
+static void create_nodes_cells(Grid &g, const double *xyz, int n_nodes, int n_cells, const int *cidx, const int *conn,
+                               std::map<int, int> *g2l_out = nullptr) {
   std::map<int, int> nodeGlobal2Local;
   g.cell.reserve(n_cells);
   g.nodeCount = 0;
@@ -362,6 +363,7 @@ static void create_nodes_cells(Grid &g, const double *xyz, int n_nodes, int n_ce
     }
     s.swap(t);
   }
+  if (g2l_out) g2l_out->swap(nodeGlobal2Local);
 }
 
 // grid_create_elements.cc:184-412
@@ -454,6 +456,219 @@ static void create_faces(Grid &g) {
       }
     }
     g.cell[c].faces.resize(g.cell[c].faces.size() - degenerate_face_count);
+  }
+  for (int f = 0; f < g.faceCount; ++f) {
+    for (size_t n = 0; n < g.face[f].nodes.size(); ++n) g.faceNode(f, (int)n).faces.push_back(f);
+    g.face[f].symmetry = false;
+  }
+}
+
+// ---------------------------------------------------------------- face-based (Tecplot) grids
+
+// grid_reader_tec.cc:36-278: Grid::readTEC.  Stream semantics kept: header
+// lines up to the first line starting (after blanks) with a digit or '-',
+// split at ',' then '=' (StringExplode, inputs.cc:363-376); block-packed
+// coordinates; one optional comment line before each later block; 1-based
+// indices.  Boundary zones: header lines read while the next line is not
+// numeric (the grabbed ZONE line is processed after that test), ZONET names a
+// new region, Nodes its node count; every zone node goes to the region of the
+// last ZONET as the nearest boundary-face node (kd_nearest3; here an exact
+// coordinate match, else the nearest, lowest id among equals).  Cell node
+// lists: the sorted node set of each cell's faces (the reference's last face
+// reads one index past faceConnIndex, grid_reader_tec.cc:240-243; for closed
+// cells its nodes are in the set through the cell's other faces).
+struct TecRaw {
+  int nNodes = 0, nCells = 0, nFaces = 0;
+  std::vector<double> xyz;
+  std::vector<int> faceNodeCount, faceConnIndex, faceConnectivity, left, right;
+  std::vector<std::set<int>> bocoNodes;
+  std::vector<int> cellConnIndex, cellConnectivity;
+};
+
+static bool tec_first_numeric(std::istream &f) {
+  while (std::isspace(f.peek())) f.get();
+  int c = f.peek();
+  return c == '-' || (c >= '0' && c <= '9');
+}
+static std::string tec_strip(const std::string &s) {
+  std::string o;
+  for (char c : s) if (!std::isspace((unsigned char)c)) o.push_back(c);
+  return o;
+}
+static void tec_explode(std::string str, const std::string &sep, std::vector<std::string> *out) {
+  size_t found = str.find_first_of(sep);
+  while (found != std::string::npos) {
+    if (found > 0) out->push_back(str.substr(0, found));
+    str = str.substr(found + 1);
+    found = str.find_first_of(sep);
+  }
+  if (str.length() > 0) out->push_back(str);
+}
+
+static TecRaw read_tec(const std::string &fileName) {
+  TecRaw raw;
+  std::ifstream file(fileName.c_str(), std::ios::in | std::ios::binary);
+  if (!file.is_open()) throw DeckError("grid file " + fileName + " could not be found");
+  std::string line;
+  while (true) {
+    if (tec_first_numeric(file)) break;
+    if (!std::getline(file, line)) throw DeckError("error reading grid file " + fileName);
+    line = tec_strip(line);
+    std::vector<std::string> expression;
+    tec_explode(line, ",", &expression);
+    for (size_t i = 0; i < expression.size(); ++i) {
+      std::vector<std::string> temp;
+      tec_explode(expression[i], "=", &temp);
+      if (temp.size() != 2) continue;
+      if (temp[0] == "Nodes") raw.nNodes = std::atoi(temp[1].c_str());
+      else if (temp[0] == "Elements") raw.nCells = std::atoi(temp[1].c_str());
+      else if (temp[0] == "Faces") raw.nFaces = std::atoi(temp[1].c_str());
+      else if (temp[0] == "ZONETYPE" && temp[1] != "FEPolyhedron") throw DeckError("ZONETYPE=" + temp[1] + " is not supported");
+      else if (temp[0] == "DATAPACKING" && temp[1] != "BLOCK") throw DeckError("DATAPACKING=" + temp[1] + " is not supported");
+      else if (temp[0] == "NumConnectedBoundaryFaces" && std::atoi(temp[1].c_str()) != 0) throw DeckError("NumConnectedBoundaryFaces>0");
+      else if (temp[0] == "TotalNumBoundaryConnections" && std::atoi(temp[1].c_str()) != 0) throw DeckError("TotalNumBoundaryConnections>0");
+    }
+  }
+  raw.xyz.assign(3 * (size_t)raw.nNodes, 0.);
+  for (int i = 0; i < 3; ++i) for (int n = 0; n < raw.nNodes; ++n) file >> raw.xyz[3 * (size_t)n + i];
+  if (!tec_first_numeric(file)) std::getline(file, line);
+  raw.faceNodeCount.resize(raw.nFaces);
+  raw.faceConnIndex.resize(raw.nFaces);
+  int size = 0;
+  for (int f = 0; f < raw.nFaces; ++f) {
+    file >> raw.faceNodeCount[f];
+    raw.faceConnIndex[f] = size;
+    size += raw.faceNodeCount[f];
+  }
+  if (!tec_first_numeric(file)) std::getline(file, line);
+  raw.faceConnectivity.resize(size);
+  for (int i = 0; i < size; ++i) { file >> raw.faceConnectivity[i]; raw.faceConnectivity[i]--; }
+  if (!tec_first_numeric(file)) std::getline(file, line);
+  raw.left.resize(raw.nFaces);
+  for (int f = 0; f < raw.nFaces; ++f) file >> raw.left[f];
+  if (!tec_first_numeric(file)) std::getline(file, line);
+  raw.right.resize(raw.nFaces);
+  for (int f = 0; f < raw.nFaces; ++f) file >> raw.right[f];
+  for (int f = 0; f < raw.nFaces; ++f) { raw.right[f]--; raw.left[f]--; }
+  if (!file.good()) throw DeckError("grid file " + fileName + " is truncated");
+  // boundary-face nodes (the kd-tree contents)
+  std::vector<int> bnodes;
+  {
+    std::set<int> s;
+    for (int f = 0; f < raw.nFaces; ++f)
+      if (raw.right[f] < 0 || raw.left[f] < 0)
+        for (int k = 0; k < raw.faceNodeCount[f]; ++k) s.insert(raw.faceConnectivity[raw.faceConnIndex[f] + k]);
+    bnodes.assign(s.begin(), s.end());
+  }
+  auto nearest = [&](const double *q) {
+    int best = -1;
+    double bd = INFINITY;
+    for (int n : bnodes) {
+      const double *x = &raw.xyz[3 * (size_t)n];
+      if (x[0] == q[0] && x[1] == q[1] && x[2] == q[2]) return n;
+      double d = (x[0] - q[0]) * (x[0] - q[0]) + (x[1] - q[1]) * (x[1] - q[1]) + (x[2] - q[2]) * (x[2] - q[2]);
+      if (d < bd) { bd = d; best = n; }
+    }
+    return best;
+  };
+  int bc_count = 0;
+  bool line_grabbed = false;
+  while (true) {
+    int bcNodeCount = 0;
+    while (true) {
+      if (tec_first_numeric(file)) break;
+      if (!line_grabbed) {
+        if (!std::getline(file, line)) throw DeckError("error reading grid file " + fileName);
+      }
+      line_grabbed = false;
+      line = tec_strip(line);
+      std::vector<std::string> expression;
+      tec_explode(line, ",", &expression);
+      for (size_t i = 0; i < expression.size(); ++i) {
+        std::vector<std::string> temp;
+        tec_explode(expression[i], "=", &temp);
+        if (temp.size() != 2) continue;
+        if (temp[0] == "ZONET") bc_count++;
+        else if (temp[0] == "Nodes") bcNodeCount = std::atoi(temp[1].c_str());
+      }
+    }
+    if (bc_count == 0) throw DeckError("grid file: boundary zone without ZONE T=");
+    std::vector<double> bcnodes(3 * (size_t)bcNodeCount);
+    for (int i = 0; i < 3; ++i) for (int n = 0; n < bcNodeCount; ++n) file >> bcnodes[3 * (size_t)n + i];
+    raw.bocoNodes.resize(bc_count);
+    for (int n = 0; n < bcNodeCount; ++n) {
+      int id = nearest(&bcnodes[3 * (size_t)n]);
+      if (id >= 0) raw.bocoNodes[bc_count - 1].insert(id);
+    }
+    while (true) {
+      std::getline(file, line);
+      line = tec_strip(line);
+      line_grabbed = true;
+      if (line.substr(0, 4) == "ZONE") break;
+      if (file.eof()) break;
+    }
+    if (file.eof()) break;
+  }
+  std::vector<std::set<int>> cellnodes(raw.nCells);
+  for (int f = 0; f < raw.nFaces; ++f)
+    for (int k = 0; k < raw.faceNodeCount[f]; ++k) {
+      int n = raw.faceConnectivity[raw.faceConnIndex[f] + k];
+      if (raw.left[f] >= 0) cellnodes[raw.left[f]].insert(n);
+      if (raw.right[f] >= 0) cellnodes[raw.right[f]].insert(n);
+    }
+  raw.cellConnIndex.assign(raw.nCells + 1, 0);
+  for (int c = 0; c < raw.nCells; ++c) {
+    raw.cellConnIndex[c + 1] = raw.cellConnIndex[c] + (int)cellnodes[c].size();
+    raw.cellConnectivity.insert(raw.cellConnectivity.end(), cellnodes[c].begin(), cellnodes[c].end());
+  }
+  return raw;
+}
+
+// grid_create_elements.cc:444-553: faces in file order, parent = left,
+// neighbour = right, boundary regions from the node sets.  Each cell's face
+// list is its faces in file order (the reference pads the list with one zero
+// per face first, grid_create_elements.cc:107-121, which adds face 0 to every
+// cell's face loops; not restated).
+static void create_faces2(Grid &g, const TecRaw &raw, const std::map<int, int> &g2l) {
+  for (int c = 0; c < g.cellCount; ++c) g.cell[c].faces.clear();
+  g.faceCount = 0;
+  for (int f = 0; f < raw.nFaces; ++f) {
+    int parent = raw.left[f], neighbor = raw.right[f];
+    if (parent < 0) throw DeckError("face without a left element");
+    Face tf;
+    tf.bc = (neighbor < 0) ? UNASSIGNED_FACE : INTERNAL_FACE;
+    tf.parent = parent;
+    tf.neighbor = neighbor;
+    tf.nodes.resize(raw.faceNodeCount[f]);
+    for (size_t fn = 0; fn < tf.nodes.size(); ++fn) tf.nodes[fn] = g2l.at(raw.faceConnectivity[raw.faceConnIndex[f] + fn]);
+    if (tf.bc == UNASSIGNED_FACE) {
+      std::vector<int> face_matched_bcs;
+      int cell_matched_bc = -1;
+      for (size_t nbc = 0; nbc < g.bocoNodes.size(); ++nbc) {
+        bool match = true;
+        for (size_t i = 0; i < tf.nodes.size(); ++i)
+          if (g.bocoNodes[nbc].find(tf.nodes[i]) == g.bocoNodes[nbc].end()) { match = false; break; }
+        if (match) face_matched_bcs.push_back((int)nbc);
+        if (cell_matched_bc == -1) {
+          match = true;
+          for (size_t i = 0; i < g.cell[tf.parent].nodes.size(); ++i)
+            if (g.bocoNodes[nbc].find(g.cell[tf.parent].nodes[i]) == g.bocoNodes[nbc].end()) { match = false; break; }
+          if (match) cell_matched_bc = (int)nbc;
+        }
+      }
+      if (face_matched_bcs.size() > 1) {
+        for (size_t fbc = 0; fbc < face_matched_bcs.size(); ++fbc)
+          if (face_matched_bcs[fbc] != cell_matched_bc) { tf.bc = face_matched_bcs[fbc]; break; }
+      } else if (face_matched_bcs.size() == 1) {
+        tf.bc = face_matched_bcs[0];
+      } else {
+        throw DeckError("couldn't find BC for face " + std::to_string(f));
+      }
+    }
+    g.cell[tf.parent].faces.push_back((int)g.face.size());
+    if (tf.bc == INTERNAL_FACE) g.cell[tf.neighbor].faces.push_back((int)g.face.size());
+    g.face.push_back(tf);
+    ++g.faceCount;
   }
   for (int f = 0; f < g.faceCount; ++f) {
     for (size_t n = 0; n < g.face[f].nodes.size(); ++n) g.faceNode(f, (int)n).faces.push_back(f);
@@ -1975,6 +2190,39 @@ void *orc_create(const char *deck_path, int n_nodes, const double *xyz, int n_ce
     create_nodes_cells(g, xyz, n_nodes, n_cells, cidx, conn);
     create_faces(g);
     g.bcCount = n_bc;
+    areas_volumes(g);
+    create_boundary_ghosts(g);
+    set_bcs_global(O);
+    setup_physics(O, dir);
+    set_lengthScales(O);
+    face_interpolation_weights(O);
+    gradient_maps(O);
+    H->F.alloc(g.cell.size(), (size_t)g.faceCount);
+    setup_rans(O);
+  } catch (const std::exception &e) {
+    if (err && errlen > 0) { std::snprintf(err, errlen, "%s", e.what()); }
+    return nullptr;
+  }
+  return H.release();
+}
+
+// Build the oracle from a deck file and a Tecplot FEPolyhedron grid file.
+void *orc_create_tecplot(const char *deck_path, const char *grid_path, char *err, int errlen) {
+  auto H = std::make_unique<Handle>();
+  try {
+    Oracle &O = H->O;
+    O.input.setFile(deck_path);
+    register_deck_schema(O.input);
+    std::string dp(deck_path);
+    size_t slash = dp.find_last_of('/');
+    std::string dir = (slash == std::string::npos) ? std::string() : dp.substr(0, slash);
+    Grid &g = O.grid;
+    TecRaw raw = read_tec(grid_path);
+    g.bocoNodes = raw.bocoNodes;
+    std::map<int, int> g2l;
+    create_nodes_cells(g, raw.xyz.data(), raw.nNodes, raw.nCells, raw.cellConnIndex.data(), raw.cellConnectivity.data(), &g2l);
+    create_faces2(g, raw, g2l);
+    g.bcCount = (int)raw.bocoNodes.size();
     areas_volumes(g);
     create_boundary_ghosts(g);
     set_bcs_global(O);
