@@ -38,6 +38,16 @@ struct RowScale {
   double s[5];  // per-equation weight of the GMRES norm
 };
 
+// Per-Newton-step scalars of the Krylov iteration.  The kernels read them from
+// device memory, so an iteration captured once as a CUDA graph stays valid
+// when they change from one Newton step to the next.
+struct IterConsts {
+  RowScale rs;     // GMRES row weights
+  RowScale winv;   // 1 / per-variable reference magnitudes
+  RowScale one;    // unit weights
+  double eps_num;  // finite-difference step numerator
+};
+
 // ------------------------------------------------------------------ face Jacobians
 __device__ __forceinline__ void seed(const FState<double> &s, FState<D5> &o, const DevCase &cs, const double n[3]) {
   // perturbations of state_perturb (ns_assemble_linear_system.cc:417-458):
@@ -174,12 +184,13 @@ __global__ void k_block_jacobi(DevCase cs, DevMesh m, const double *__restrict__
 // z = Minv x (per-cell 5x5), vectors [5][nc] of type T
 // z = Minv (D^-1 x): right preconditioner of the row-scaled system D A
 template <class T>
-__global__ void k_precond(int nc, const double *__restrict__ Minv, const T *__restrict__ x, T *__restrict__ z, RowScale rs) {
+__global__ void k_precond(int nc, const double *__restrict__ Minv, const T *__restrict__ x, T *__restrict__ z,
+                          const RowScale *__restrict__ rs) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= nc) return;
   double xv[5];
 #pragma unroll
-  for (int k = 0; k < 5; ++k) xv[k] = double(x[k * nc + c]) / rs.s[k];
+  for (int k = 0; k < 5; ++k) xv[k] = double(x[k * nc + c]) / rs->s[k];
 #pragma unroll
   for (int i = 0; i < 5; ++i) {
     double s = 0.;
@@ -317,17 +328,18 @@ __global__ void k_gs_packed(int nc, int deg, int cnt, const int *__restrict__ ce
 // copy a [5][nc] state into the residual chain's [5][nt] array (+ optional eps*dir)
 // Finite-difference step eps = eps_num / |z| with |z|^2 read from the device
 // (eps_num alone where zz is null or |z| = 0).
-__device__ __forceinline__ double fd_eps(double eps_num, const double *zz) {
+__device__ __forceinline__ double fd_eps(const double *eps_p, const double *zz) {
+  const double eps_num = eps_p ? *eps_p : 0.;
   if (!zz) return eps_num;
   const double q = *zz;
   return q > 0. ? eps_num / sqrt(q) : eps_num;
 }
 template <class T>
-__global__ void k_load_state(int nc, int nt, const double *__restrict__ Wn, const T *__restrict__ dir, double eps_num,
-                             const double *__restrict__ zz, double *__restrict__ W) {
+__global__ void k_load_state(int nc, int nt, const double *__restrict__ Wn, const T *__restrict__ dir,
+                             const double *__restrict__ eps_num, const double *__restrict__ zz, double *__restrict__ W) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= nc) return;
-  const double eps = fd_eps(eps_num, zz);
+  const double eps = dir ? fd_eps(eps_num, zz) : 0.;
 #pragma unroll
   for (int v = 0; v < 5; ++v) W[v * nt + c] = Wn[v * nc + c] + (dir ? eps * double(dir[v * nc + c]) : 0.);
 }
@@ -343,11 +355,11 @@ __global__ void k_load_dual(int nc, int nt, const double *__restrict__ Wn, const
 template <class T, class D = double>
 __global__ void k_matvec_finish(DevCase cs, int nc, const double *__restrict__ Wn, const double *__restrict__ vol,
                                 const double *__restrict__ dt, const T *__restrict__ z, const double *__restrict__ R1,
-                                const double *__restrict__ R0, double eps_num, const double *__restrict__ zz,
-                                const Dual<D> *__restrict__ JV, T *__restrict__ y, RowScale rs) {
+                                const double *__restrict__ R0, const IterConsts *__restrict__ ic, const double *__restrict__ zz,
+                                const Dual<D> *__restrict__ JV, T *__restrict__ y) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= nc) return;
-  const double inv_eps = JV ? 0. : 1. / fd_eps(eps_num, zz);
+  const double inv_eps = JV ? 0. : 1. / fd_eps(&ic->eps_num, zz);
   double P[25];
   cons2prim(cs, Wn[c], Wn[nc + c], Wn[2 * nc + c], Wn[3 * nc + c], Wn[4 * nc + c], P);
   const double s = vol[c] / dt[c];
@@ -360,7 +372,7 @@ __global__ void k_matvec_finish(DevCase cs, int nc, const double *__restrict__ W
 #pragma unroll
     for (int k = 0; k < 5; ++k) a += P[5 * i + k] * zv[k];
     const double jz = JV ? double(JV[i * nc + c].d) : (R1[i * nc + c] - R0[i * nc + c]) * inv_eps;
-    y[i * nc + c] = T(rs.s[i] * (s * a - jz));
+    y[i * nc + c] = T(ic->rs.s[i] * (s * a - jz));
   }
 }
 
@@ -474,10 +486,10 @@ __global__ void k_gather_vol(int nc, const double *__restrict__ v, double *__res
 // ------------------------------------------------------------------ solver
 // part[block] = sum over this block's slice of (z_i / wref_v)^2, v = i / nc
 template <class T>
-__global__ void k_wdot(int n, int nc, const T *__restrict__ z, RowScale winv, double *__restrict__ part) {
+__global__ void k_wdot(int n, int nc, const T *__restrict__ z, const RowScale *__restrict__ winv, double *__restrict__ part) {
   double s = 0.;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const double q = double(z[i]) * winv.s[i / nc];
+    const double q = double(z[i]) * winv->s[i / nc];
     s += q * q;
   }
   __shared__ double sh[32];
@@ -505,10 +517,17 @@ struct Krylov {
   DBuf<T> V, w, tmpT;
   DBuf<double> part, hd;  // hd: [0,m+1) first CGS pass, [m+1,2m+2) second, [2m+2] |w|^2, [2m+3] |z|^2
   double *hp = nullptr;   // pinned host mirror of hd
+  // one CUDA graph per basis index j of the Arnoldi step (preconditioner,
+  // J.v, both Gram-Schmidt passes, normalisation, copy of hd to hp),
+  // captured at its first use and replayed for every later cycle and Newton
+  // step of the solve
+  std::vector<cudaGraphExec_t> graphs;
   Krylov() = default;
   Krylov(const Krylov &) = delete;
   Krylov &operator=(const Krylov &) = delete;
   ~Krylov() {
+    for (cudaGraphExec_t g : graphs)
+      if (g) cudaGraphExecDestroy(g);
     if (hp) cudaFreeHost(hp);
   }
   void alloc(fcfd_ctx *ctx, int krylov_dim) {
@@ -517,6 +536,7 @@ struct Krylov {
     V.alloc((size_t)(m + 1) * n); w.alloc(n); tmpT.alloc(n);
     part.alloc((size_t)nparts * (m + 1)); hd.alloc(2 * (size_t)m + 4);
     CK(cudaMallocHost((void **)&hp, sizeof(double) * (2 * (size_t)m + 4)));
+    graphs.assign(m, nullptr);
   }
   double *h1() { return hd.p; }
   double *h2() { return hd.p + m + 1; }
@@ -530,8 +550,11 @@ struct Krylov {
     k_sum_parts<<<nv, 256, 0, s>>>(nparts, part.p, out);
   }
   // bring hd back to the host (the one synchronisation of a GMRES iteration)
-  void fetch() {
+  void fetch_async() {
     CK(cudaMemcpyAsync(hp, hd.p, sizeof(double) * (2 * (size_t)m + 4), cudaMemcpyDeviceToHost, x->stream));
+  }
+  void fetch() {
+    fetch_async();
     CK(cudaStreamSynchronize(x->stream));
   }
   double norm(const T *u) {
@@ -540,7 +563,7 @@ struct Krylov {
     return std::sqrt(hp[2 * m + 2]);
   }
   // |S^-1 u|^2 on the device (S = per-variable reference magnitudes)
-  void wnorm2_dev(const T *u, const RowScale &winv, double *out) {
+  void wnorm2_dev(const T *u, const RowScale *winv, double *out) {
     cudaStream_t s = x->stream;
     k_wdot<T><<<nparts, 256, 0, s>>>(n, nc, u, winv, part.p);
     k_sum_parts<<<1, 256, 0, s>>>(nparts, part.p, out);
@@ -563,12 +586,14 @@ struct NewtonState {
   double wscale = 1.;  // |S^-1 W| (finite-difference step scale)
   RowScale winv;       // 1 / per-variable reference magnitudes
   int sweeps = 0, cycles = 1;
+  IterConsts hic;      // host copy of the iteration scalars
+  DBuf<IterConsts> ic; // their device copy
 };
 template <class T, class P>
-__global__ void k_unscale(int nc, const T *__restrict__ v, RowScale rs, P *__restrict__ out) {
+__global__ void k_unscale(int nc, const T *__restrict__ v, const RowScale *__restrict__ rs, P *__restrict__ out) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= nc) return;
-  for (int k = 0; k < 5; ++k) out[k * nc + c] = P(double(v[k * nc + c]) / rs.s[k]);
+  for (int k = 0; k < 5; ++k) out[k * nc + c] = P(double(v[k * nc + c]) / rs->s[k]);
 }
 template <class T>
 __global__ void k_axpy_to(int n, const double *__restrict__ b, const T *__restrict__ w, T *__restrict__ out) {
@@ -583,39 +608,49 @@ __global__ void k_cast(int n, const A *__restrict__ a, T *__restrict__ b) {
 
 // residual of the [5][nc] state (+ eps*dir) into R (SoA [5][nc])
 template <class T>
-static void eval_residual(fcfd_ctx *x, const double *Wn, double *R, const T *dir, double eps,
+static void eval_residual(fcfd_ctx *x, const double *Wn, double *R, const T *dir, const double *eps,
                           const double *zz = nullptr) {
   const DevMesh &m = x->dm;
   k_load_state<T><<<(m.nc + 255) / 256, 256, 0, x->stream>>>(m.nc, m.nt, Wn, dir, eps, zz, x->p64.W.p);
   launch_chain<double>(x, x->p64, R, false, nullptr, nullptr);
 }
 
-// y = (V P/dt - dR/dW) z; zz: device |z|^2 (finite-difference mode only)
+// Tangent-chain buffers of the J.v mode, allocated before any capture.
+static void prepare_matvec(fcfd_ctx *x, int mode) {
+  const DevMesh &m = x->dm;
+  if (mode == 0) return;
+  if (x->newton_f32) {
+    if (!x->pjv32.ready) x->pjv32.alloc(m.nc, m.nf, m.nb);
+  } else {
+    if (!x->pjv.ready) x->pjv.alloc(m.nc, m.nf, m.nb);
+  }
+}
+
+// y = (V P/dt - dR/dW) z; zz: device |z|^2 (finite-difference mode only).
+// Finite differences are taken in variables scaled by their reference
+// magnitudes: eps = sqrt(eps_mach) (1 + |S^-1 W|) / |S^-1 z|, the numerator
+// in ns.ic.
 template <class T>
-static void matvec(fcfd_ctx *x, NewtonState &ns, int mode, const T *z, T *y, const double *zz, const RowScale &rs) {
+static void matvec(fcfd_ctx *x, NewtonState &ns, int mode, const T *z, T *y, const double *zz) {
   const DevMesh &m = x->dm;
   cudaStream_t s = x->stream;
   const int tb = 256, gb = (m.nc + tb - 1) / tb;
+  prepare_matvec(x, mode);
   if (mode == 0) {
-    // finite difference of the FP64 residual in variables scaled by their
-    // reference magnitudes: eps = sqrt(eps_mach) (1 + |S^-1 W|) / |S^-1 z|
-    const double eps_num = 1.4901161193847656e-08 * (1. + ns.wscale);
-    eval_residual<T>(x, ns.Wn.p, ns.R1.p, z, eps_num, zz);
-    k_matvec_finish<T, double><<<gb, tb, 0, s>>>(x->cs, m.nc, ns.Wn.p, ns.vol.p, ns.dt.p, z, ns.R1.p, ns.R0.p, eps_num, zz,
-                                                 (const Dual<double> *)nullptr, y, rs);
+    eval_residual<T>(x, ns.Wn.p, ns.R1.p, z, &ns.ic.p->eps_num, zz);
+    k_matvec_finish<T, double><<<gb, tb, 0, s>>>(x->cs, m.nc, ns.Wn.p, ns.vol.p, ns.dt.p, z, ns.R1.p, ns.R0.p, ns.ic.p, zz,
+                                                 (const Dual<double> *)nullptr, y);
   } else {
     if (x->newton_f32) {
-      if (!x->pjv32.ready) x->pjv32.alloc(m.nc, m.nf, m.nb);
       k_load_dual<T, float><<<gb, tb, 0, s>>>(m.nc, m.nt, ns.Wn.p, z, x->pjv32.W.p);
       launch_chain<Dual<float>>(x, x->pjv32, x->pjv32.R.p, false, nullptr, nullptr, x->newton_frozen);
-      k_matvec_finish<T, float><<<gb, tb, 0, s>>>(x->cs, m.nc, ns.Wn.p, ns.vol.p, ns.dt.p, z, nullptr, nullptr, 0., nullptr,
-                                                  x->pjv32.R.p, y, rs);
+      k_matvec_finish<T, float><<<gb, tb, 0, s>>>(x->cs, m.nc, ns.Wn.p, ns.vol.p, ns.dt.p, z, nullptr, nullptr, ns.ic.p,
+                                                  nullptr, x->pjv32.R.p, y);
     } else {
-      if (!x->pjv.ready) x->pjv.alloc(m.nc, m.nf, m.nb);
       k_load_dual<T, double><<<gb, tb, 0, s>>>(m.nc, m.nt, ns.Wn.p, z, x->pjv.W.p);
       launch_chain<Dual<double>>(x, x->pjv, x->pjv.R.p, false, nullptr, nullptr, x->newton_frozen);
-      k_matvec_finish<T, double><<<gb, tb, 0, s>>>(x->cs, m.nc, ns.Wn.p, ns.vol.p, ns.dt.p, z, nullptr, nullptr, 0., nullptr,
-                                                   x->pjv.R.p, y, rs);
+      k_matvec_finish<T, double><<<gb, tb, 0, s>>>(x->cs, m.nc, ns.Wn.p, ns.vol.p, ns.dt.p, z, nullptr, nullptr, ns.ic.p,
+                                                   nullptr, x->pjv.R.p, y);
     }
   }
   CK(cudaGetLastError());
@@ -635,9 +670,10 @@ static double dnorm(fcfd_ctx *x, DBuf<double> &part, DBuf<double> &h, const doub
 // Preconditioner: z = M^-1 D^-1 v with M^-1 = `sweeps` symmetric multicolour
 // block Gauss-Seidel sweeps on the first-order operator (0: block diagonal alone).
 template <class T>
-static void apply_prec(fcfd_ctx *x, NewtonState &ns, const T *v, T *z, const RowScale &rs, int sweeps) {
+static void apply_prec(fcfd_ctx *x, NewtonState &ns, const T *v, T *z, int sweeps) {
   const int nc = x->dm.nc, tb = 256, gc = (nc + tb - 1) / tb;
   cudaStream_t s = x->stream;
+  const RowScale *rs = &ns.ic.p->rs, *one = &ns.ic.p->one;
   if (sweeps <= 0) {
     k_precond<T><<<gc, tb, 0, s>>>(nc, ns.Minv.p, v, z, rs);
     return;
@@ -647,8 +683,6 @@ static void apply_prec(fcfd_ctx *x, NewtonState &ns, const T *v, T *z, const Row
   // changes nothing (its cells do not couple to each other), so the repeat at
   // each turn is skipped.  FP64 or, with the FP32 preconditioner, FP32
   // couplings, vectors and arithmetic.
-  RowScale one;
-  for (int i = 0; i < 5; ++i) one.s[i] = 1.;
   auto sweep = [&](auto *OB, auto *MinvP, auto *r, auto *a) {
     const std::vector<int> &ci = x->color_index;
     const int ncol = (int)ci.size() - 1, deg = x->gs_deg;
@@ -688,6 +722,7 @@ static void gmres(fcfd_ctx *x, NewtonState &ns, Krylov<T> &K, int mode, double r
   const int tb = 256, gn = (n + tb - 1) / tb, gc = (nc + tb - 1) / tb;
   iters = 0;
   relres = 1.;
+  prepare_matvec(x, mode);
   // scaled right-hand side b = D R0; x0 = 0
   k_rowscale_copy<<<gc, tb, 0, s>>>(nc, ns.R0.p, rs, 1., dW);
   const double bnorm = K.norm64(dW);
@@ -703,8 +738,8 @@ static void gmres(fcfd_ctx *x, NewtonState &ns, Krylov<T> &K, int mode, double r
       // r = b - (D A M^-1 D^-1 ...) applied to the current solution: recompute through one matvec of
       // z = M^-1 D^-1 (sum) already folded into Xs (physical units): r = D (R0 - A Xs)
       k_cast<T><<<gn, tb, 0, s>>>(n, ns.Xs.p, K.tmpT.p);
-      if (mode == 0) K.wnorm2_dev(K.tmpT.p, ns.winv, K.zz());
-      matvec<T>(x, ns, mode, K.tmpT.p, K.w.p, K.zz(), rs);
+      if (mode == 0) K.wnorm2_dev(K.tmpT.p, &ns.ic.p->winv, K.zz());
+      matvec<T>(x, ns, mode, K.tmpT.p, K.w.p, K.zz());
       k_rowscale_copy<<<gc, tb, 0, s>>>(nc, ns.R0.p, rs, 1., dW);
       k_axpy_to<T><<<gn, tb, 0, s>>>(n, dW, K.w.p, K.V.p);  // V0 = b - A x (unnormalised)
       beta = K.norm(K.V.p);
@@ -716,19 +751,28 @@ static void gmres(fcfd_ctx *x, NewtonState &ns, Krylov<T> &K, int mode, double r
     int k = 0;
     bool done = false;
     for (int j = 0; j < m; ++j) {
-      T *vj = K.V.p + (size_t)j * n;
-      T *w = K.V.p + (size_t)(j + 1) * n;
-      apply_prec<T>(x, ns, vj, K.tmpT.p, rs, ns.sweeps);
-      if (mode == 0) K.wnorm2_dev(K.tmpT.p, ns.winv, K.zz());
-      matvec<T>(x, ns, mode, K.tmpT.p, w, K.zz(), rs);
-      // classical Gram-Schmidt twice, coefficients kept on the device
-      K.dots_dev(j + 1, K.V.p, w, K.h1());
-      k_sub_combo<T><<<gn, tb, 0, s>>>(n, j + 1, K.V.p, (size_t)n, K.h1(), w);
-      K.dots_dev(j + 1, K.V.p, w, K.h2());
-      k_sub_combo<T><<<gn, tb, 0, s>>>(n, j + 1, K.V.p, (size_t)n, K.h2(), w);
-      K.dots_dev(1, w, w, K.ww());
-      k_scale_rsqrt<T><<<gn, tb, 0, s>>>(n, K.ww(), w);
-      K.fetch();
+      if (!K.graphs[j]) {
+        T *vj = K.V.p + (size_t)j * n;
+        T *w = K.V.p + (size_t)(j + 1) * n;
+        cudaGraph_t gr = nullptr;
+        CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        apply_prec<T>(x, ns, vj, K.tmpT.p, ns.sweeps);
+        if (mode == 0) K.wnorm2_dev(K.tmpT.p, &ns.ic.p->winv, K.zz());
+        matvec<T>(x, ns, mode, K.tmpT.p, w, K.zz());
+        // classical Gram-Schmidt twice, coefficients kept on the device
+        K.dots_dev(j + 1, K.V.p, w, K.h1());
+        k_sub_combo<T><<<gn, tb, 0, s>>>(n, j + 1, K.V.p, (size_t)n, K.h1(), w);
+        K.dots_dev(j + 1, K.V.p, w, K.h2());
+        k_sub_combo<T><<<gn, tb, 0, s>>>(n, j + 1, K.V.p, (size_t)n, K.h2(), w);
+        K.dots_dev(1, w, w, K.ww());
+        k_scale_rsqrt<T><<<gn, tb, 0, s>>>(n, K.ww(), w);
+        K.fetch_async();
+        CK(cudaStreamEndCapture(s, &gr));
+        CK(cudaGraphInstantiate(&K.graphs[j], gr, 0));
+        CK(cudaGraphDestroy(gr));
+      }
+      CK(cudaGraphLaunch(K.graphs[j], s));
+      CK(cudaStreamSynchronize(s));
       const double hn = std::sqrt(K.hp[2 * m + 2]);
       for (int i = 0; i <= j; ++i) H[(size_t)i * m + j] = K.hp[i] + K.hp[m + 1 + i];
       H[(size_t)(j + 1) * m + j] = hn;
@@ -759,7 +803,7 @@ static void gmres(fcfd_ctx *x, NewtonState &ns, Krylov<T> &K, int mode, double r
     std::copy(y.begin(), y.end(), K.hp);
     CK(cudaMemcpyAsync(K.hd.p, K.hp, sizeof(double) * k, cudaMemcpyHostToDevice, s));
     k_combo<T><<<gn, tb, 0, s>>>(n, k, K.V.p, (size_t)n, K.hd.p, K.w.p);
-    apply_prec<T>(x, ns, K.w.p, K.tmpT.p, rs, ns.sweeps);
+    apply_prec<T>(x, ns, K.w.p, K.tmpT.p, ns.sweeps);
     k_update<T><<<gn, tb, 0, s>>>(n, ns.Xs.p, K.tmpT.p, 1., x->err.p);
     if (done) break;
   }
@@ -775,6 +819,7 @@ static void alloc_state(fcfd_ctx *x, NewtonState &ns, int sweeps, int cycles, bo
   ns.Wn.alloc(n); ns.R0.alloc(n); ns.R1.alloc(n); ns.dt.alloc(nc); ns.vol.alloc(nc);
   ns.JL.alloc(25 * (size_t)m.nf); ns.JR.alloc(25 * (size_t)m.nf); ns.Minv.alloc(25 * (size_t)nc);
   ns.Pr.alloc(n); ns.Py0.alloc(n); ns.Py1.alloc(n); ns.Xs.alloc(n); ns.rowmag.alloc(n);
+  ns.ic.alloc(1);
   ns.sweeps = sweeps; ns.cycles = cycles > 0 ? cycles : 1;
   ns.prec32 = prec32;
   if (ns.sweeps > 0) {
@@ -860,6 +905,11 @@ static LinearSolve implicit_solve(fcfd_ctx *x, NewtonState &ns, Krylov<double> &
     for (int v = 0; v < 5; ++v) q += wn[v] * wn[v] * ns.winv.s[v] * ns.winv.s[v];
     ns.wscale = std::sqrt(q);
   }
+  ns.hic.rs = rs;
+  ns.hic.winv = ns.winv;
+  for (int v = 0; v < 5; ++v) ns.hic.one.s[v] = 1.;
+  ns.hic.eps_num = 1.4901161193847656e-08 * (1. + ns.wscale);
+  CK(cudaMemcpyAsync(ns.ic.p, &ns.hic, sizeof(IterConsts), cudaMemcpyHostToDevice, s));
   LinearSolve out;
   if (f32) gmres<float>(x, ns, K32, jmode, krtol, ns.R1.p, out.iters, out.relres, rs, abstol);
   else gmres<double>(x, ns, K64, jmode, krtol, ns.R1.p, out.iters, out.relres, rs, abstol);
@@ -1001,7 +1051,7 @@ int fcfd_newton_solve(fcfd_ctx *x, double *W, const fcfd_newton_opts *o, fcfd_ne
     key.alloc(1);
     CK(cudaStreamSynchronize(s));
     auto t0 = std::chrono::steady_clock::now();
-    eval_residual<double>(x, ns.Wn.p, ns.R0.p, (const double *)nullptr, 0.);
+    eval_residual<double>(x, ns.Wn.p, ns.R0.p, (const double *)nullptr, (const double *)nullptr);
     check_err(x);
     auto row_norms = [&](double out[5]) {
       for (int v = 0; v < 5; ++v) out[v] = dnorm(x, part, hh, ns.R0.p + (size_t)v * nc, nc);
@@ -1049,7 +1099,7 @@ int fcfd_newton_solve(fcfd_ctx *x, double *W, const fcfd_newton_opts *o, fcfd_ne
       CK(cudaStreamSynchronize(s));
       double rnew = NAN;
       if (!(h & 8)) {
-        eval_residual<double>(x, ns.Wn.p, ns.R0.p, (const double *)nullptr, 0.);
+        eval_residual<double>(x, ns.Wn.p, ns.R0.p, (const double *)nullptr, (const double *)nullptr);
         CK(cudaMemcpyAsync(&h, x->err.p, sizeof(int), cudaMemcpyDeviceToHost, s));
         CK(cudaStreamSynchronize(s));
         row_norms(rows);
@@ -1061,7 +1111,7 @@ int fcfd_newton_solve(fcfd_ctx *x, double *W, const fcfd_newton_opts *o, fcfd_ne
         // reject the step: restore the state, cut the CFL, re-evaluate
         if (++rejects > 12) { status = FCFD_ERR_DIVERGED; break; }
         CK(cudaMemcpyAsync(ns.Wn.p, Wsave.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
-        eval_residual<double>(x, ns.Wn.p, ns.R0.p, (const double *)nullptr, 0.);
+        eval_residual<double>(x, ns.Wn.p, ns.R0.p, (const double *)nullptr, (const double *)nullptr);
         row_norms(rows);
         cfl = std::max(cfl * 0.25, 1e-3);
         cfl_prev = cfl;
@@ -1216,7 +1266,7 @@ int fcfd_run(fcfd_ctx *x, double *W, const fcfd_run_opts *o, fcfd_run_report *re
       }
       // the state and its residual (the residual also loads W into the
       // gradient / limiter pipeline that the time step reads)
-      eval_residual<double>(x, ns.Wn.p, ns.R0.p, (const double *)nullptr, 0.);
+      eval_residual<double>(x, ns.Wn.p, ns.R0.p, (const double *)nullptr, (const double *)nullptr);
       double max_cfl = -1.;
       if (tm.type == TS_FIXED) {
         k_fill_value<<<gc, tb, 0, s>>>(nc, ns.dt.p, ts_cur);
