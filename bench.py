@@ -377,12 +377,22 @@ def run_newton(fb, cs, mesh, case, dev, dist):
         out[label] = {"seconds": round(el, 4), "converged": rep["status"] == 0,
                       "newton_iterations": rep["newton_iterations"], "krylov_iterations": rep["krylov_iterations"],
                       "mass_residual_drop": float(rep["res_final"] / rep["res0"])}
+        if "type=wall;" in case.deck and case.name == "cylinder":
+            # drag coefficient of the wall (BC_1): Fx / (0.5 rho U^2 D span), D = 1
+            F, _ = ns.drag(W, [0], (1.0, 0.0, 0.0), gradient=False)
+            p, U, T = case.freestream[0], case.freestream[1], case.freestream[4]
+            rho = p / (287.0 * T)
+            span = float(np.ptp(case.mesh.nodes[:, 2]))
+            out[label]["drag_coefficient"] = float(F[0] / (0.5 * rho * U * U * 1.0 * span))
         del ns
     a, b = states["plain_fp64_fd"], states["mixed_jvp_fp32"]
     scale = np.abs(a).max(axis=0)
     scale[1:4] = np.abs(a[:, 1:4]).max()
     out["speedup_mixed_vs_plain"] = round(out["plain_fp64_fd"]["seconds"] / out["mixed_jvp_fp32"]["seconds"], 3)
     out["state_rel_diff_mixed_vs_plain"] = float((np.abs(a - b).max(axis=0) / scale).max())
+    if "drag_coefficient" in out["plain_fp64_fd"]:
+        cp, cm = out["plain_fp64_fd"]["drag_coefficient"], out["mixed_jvp_fp32"]["drag_coefficient"]
+        out["drag_coefficient_rel_diff_mixed_vs_plain"] = abs(cm - cp) / abs(cp)
     out["settings"] = dict(NEWTON_KW)
     return out
 

@@ -167,6 +167,13 @@ int fcfd_rans_residual(fcfd_ctx *ctx, const double *W, const double *K, double *
  * each evaluation when flush_l2 != 0.  Benchmark entry point, no counterpart
  * in the reference. */
 int fcfd_time_rans(fcfd_ctx *ctx, int reps, int flush_l2, double *out, int out_len);
+/* Forward tangent of the coupled residual: (JV, JVK) = d(R, RK)/d(W, K)
+ * applied to (V[nc][5], VK[nc][2]), evaluated by the same kernels as
+ * fcfd_rans_residual on dual numbers (the eddy viscosity, the k-omega fluxes
+ * and sources and their coupling into the NS viscous flux all carry the
+ * tangent).  R and RK (both or neither) receive the residual. */
+int fcfd_rans_jvp(fcfd_ctx *ctx, const double *W, const double *K, const double *V, const double *VK, double *R,
+                  double *RK, double *JV, double *JVK, int flags);
 /* Fixed BC values of the RANS variables, per BC region: kw_fixed, k, omega,
  * mut_fixed, mu_t (5 doubles each; out_len >= 5 * number of regions). */
 int fcfd_rans_bcs(const fcfd_ctx *ctx, double *out, int32_t out_len);

@@ -58,6 +58,8 @@ def lib():
         L.orc_local_dt.argtypes = [vp, dp, ctypes.c_double, ctypes.c_int, dp]
         L.orc_loads.argtypes = [vp, dp, dp, ctypes.c_double, dp, dp, ctypes.c_char_p, ctypes.c_int]
         L.orc_loads.restype = ctypes.c_int
+        L.orc_rans_residual_cstep.argtypes = [vp, dp, dp, dp, dp, ctypes.c_double, dp, dp, ctypes.c_char_p, ctypes.c_int]
+        L.orc_rans_residual_cstep.restype = ctypes.c_int
         L.orc_rans_residual.argtypes = [vp, dp, dp, dp, dp, ctypes.c_char_p, ctypes.c_int]
         L.orc_rans_residual.restype = ctypes.c_int
         L.orc_rans_bcs.argtypes = [vp, dp]
@@ -203,6 +205,16 @@ class Oracle:
         if rc != 0:
             raise RuntimeError("oracle: " + err.value.decode())
         return R, RK
+
+    def rans_residual_cstep(self, W, K, dW, dK, h=1e-30):
+        """Complex-step directional derivative of the RANS residual along (dW, dK)."""
+        a = [np.ascontiguousarray(x, dtype=np.float64).reshape(self.nc, n) for x, n in ((W, 5), (K, 2), (dW, 5), (dK, 2))]
+        dR, dRK = np.empty((self.nc, 5)), np.empty((self.nc, 2))
+        err = ctypes.create_string_buffer(512)
+        rc = lib().orc_rans_residual_cstep(self.h, *[_d(x) for x in a], h, _d(dR), _d(dRK), err, 512)
+        if rc != 0:
+            raise RuntimeError("oracle: " + err.value.decode())
+        return dR, dRK
 
     def rans_bcs(self):
         nbc = int(self.case_summary()[1][5])

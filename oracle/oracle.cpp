@@ -2406,6 +2406,41 @@ int orc_rans_residual(void *h, const double *W, const double *Kin, double *R, do
   return 0;
 }
 
+// Complex-step directional derivative of the RANS residual along (dW, dK):
+// dR[nc][5], dRK[nc][2].
+int orc_rans_residual_cstep(void *h, const double *W, const double *Kin, const double *dW, const double *dK, double hstep,
+                            double *dR, double *dRK, char *err, int errlen) {
+  Handle *H = static_cast<Handle *>(h);
+  Oracle &O = H->O;
+  Grid &g = O.grid;
+  Fields<CStep> F;
+  F.alloc(g.cell.size(), (size_t)g.faceCount);
+  try {
+    if (!O.turbulent) throw DeckError("the deck has no turbulence section");
+    for (int c = 0; c < g.cellCount; ++c) {
+      auto at = [&](int k) { return CStep(W[5 * c + k], hstep * dW[5 * c + k]); };
+      F.p[c] = at(0);
+      F.V[c] = V3<CStep>(at(1), at(2), at(3));
+      F.T[c] = at(4);
+      F.rho[c] = O.material.rho(F.p[c], F.T[c]);
+    }
+    for (int i = 0; i < 5; ++i)
+      for (size_t c = 0; c < g.cell.size(); ++c) F.limiter[i][c] = CStep((O.order == FIRST) ? 0. : 1.);
+    std::vector<CStep> k(g.cellCount), om(g.cellCount), rns, rk;
+    for (int c = 0; c < g.cellCount; ++c) {
+      k[c] = CStep(Kin[2 * c], hstep * dK[2 * c]);
+      om[c] = CStep(Kin[2 * c + 1], hstep * dK[2 * c + 1]);
+    }
+    rans_residual(O, F, k, om, rns, rk);
+    for (size_t i = 0; i < rns.size(); ++i) dR[i] = rns[i].im / hstep;
+    for (size_t i = 0; i < rk.size(); ++i) dRK[i] = rk[i].im / hstep;
+  } catch (const std::exception &e) {
+    if (err && errlen > 0) std::snprintf(err, errlen, "%s", e.what());
+    return 1;
+  }
+  return 0;
+}
+
 // Fixed BC values of the RANS variables: per BC [kw_fixed, k, omega, mut_fixed, mu_t].
 void orc_rans_bcs(void *h, double *out) {
   Oracle &O = static_cast<Handle *>(h)->O;

@@ -102,3 +102,18 @@ def test_newton_other_fluxes(flux, label, opts, oracle_mod, fb):
     r0 = np.linalg.norm(o.residual(case.state)[:, 0])
     r = np.linalg.norm(o.residual(W)[:, 0])
     assert r <= 1e-9 * r0, (r, r0)
+
+
+@pytest.mark.gpu
+def test_newton_drag_coefficient(cylinder):
+    """The wall drag at the converged states: the plain FP64 arm's against the
+    oracle's loads at that state (1e-12), and the mixed arm's against the plain
+    arm's (1e-6: the states agree to ~1e-7 relative)."""
+    case, o, ns = cylinder
+    Wa, _ = ns.newton_solve(case.state, jvp=False, **KW)
+    Wb, _ = ns.newton_solve(case.state, jvp=True, fp32_jvp=True, fp32_krylov=True, **KW)
+    Fa = ns.drag(Wa, [0], gradient=False)[0]
+    Fb = ns.drag(Wb, [0], gradient=False)[0]
+    Fo = o.loads(Wa)[0]
+    assert np.abs(Fa - Fo).max() <= 1e-12 * np.abs(Fo).max()
+    assert abs(Fb[0] - Fa[0]) <= 1e-6 * abs(Fa[0])

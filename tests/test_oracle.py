@@ -206,3 +206,24 @@ def test_oracle_rans_inlet_values(oracle_mod):
     assert bcs[0, 0] == 1 and abs(bcs[0, 1] - k) <= 1e-14 * k and abs(bcs[0, 2] - omega) <= 1e-12 * omega
     assert bcs[2, 3] == 1 and bcs[2, 4] == 0.0          # wall
     assert bcs[1, 0] == 0 and bcs[3, 0] == 0             # outlet, symmetry: extrapolated
+
+
+def test_rans_complex_step_matches_finite_difference(oracle_mod):
+    """The oracle's complex step of the coupled RANS residual agrees with
+    central differences of its own residual (limiter off, v perturbed)."""
+    case = cases.plate_case(ni=8, nj=4, nk=2, turbulent=True, limiter="none")
+    o = oracle_mod.Oracle(case)
+    W = case.state.copy()
+    rng = np.random.default_rng(3)
+    W[:, 2] = 0.02 * W[:, 1] * rng.uniform(-1.0, 1.0, W.shape[0])
+    K = case.kstate
+    dW = rng.standard_normal(W.shape) * np.abs(W).max(axis=0) * np.array([1, 1, 1, 0, 1]) * 1e-3
+    dK = rng.standard_normal(K.shape) * np.abs(K).max(axis=0) * 1e-3
+    dR, dRK = o.rans_residual_cstep(W, K, dW, dK)
+    h = 1e-6
+    Rp, RKp = o.rans_residual(W + h * dW, K + h * dK)
+    Rm, RKm = o.rans_residual(W - h * dW, K - h * dK)
+    cols = [0, 1, 2, 4]
+    e1 = (np.abs(dR - (Rp - Rm) / (2 * h))[:, cols].max(axis=0) / np.abs(dR[:, cols]).max(axis=0)).max()
+    e2 = (np.abs(dRK - (RKp - RKm) / (2 * h)).max(axis=0) / np.abs(dRK).max(axis=0)).max()
+    assert e1 < 1e-5 and e2 < 1e-5, (e1, e2)

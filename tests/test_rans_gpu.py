@@ -69,3 +69,62 @@ def test_rans_rejects_laminar_case(fb, oracle_mod):
     ns = fb.NavierStokes(m, cs, 0)
     with pytest.raises(fb.FcfdError):
         ns.rans_residual(case.state, np.ones((m.nc, 2)))
+
+
+def _generic(case, seed=3):
+    """Seeded state with v perturbed too, so no face sits on a |V.n| = 0 or
+    limiter tie (the complex step decides those by the h^2 term)."""
+    W = case.state.copy()
+    rng = np.random.default_rng(seed)
+    W[:, 2] = 0.02 * W[:, 1] * rng.uniform(-1.0, 1.0, W.shape[0])
+    return W
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("size,limiter,flux", [((8, 4, 2), "vk", "Roe"), ((12, 6, 3), "none", "AUSM+up"),
+                                               ((12, 6, 3), "minmod", "vanLeer"), ((12, 6, 3), "vk", "SD-SLAU")])
+def test_rans_jvp_matches_complex_step(size, limiter, flux, oracle_mod, fb):
+    """Tangent of the coupled NS + k-omega residual (dual numbers through the
+    eddy viscosity, the k-omega fluxes and sources) against the oracle's
+    complex step (h = 1e-30) along seeded directions in (W, K)."""
+    ni, nj, nk = size
+    case = _plate(ni=ni, nj=nj, nk=nk, limiter=limiter, flux=flux)
+    o, cs, m = build_pair(case, oracle_mod, fb)
+    ns = fb.NavierStokes(m, cs, 0)
+    W, K = _generic(case), case.kstate
+    rng = np.random.default_rng(17)
+    for _ in range(2):
+        V = rng.standard_normal(W.shape) * np.abs(W).max(axis=0) * 1e-3
+        VK = rng.standard_normal(K.shape) * np.abs(K).max(axis=0) * 1e-3
+        R, RK, JV, JVK = ns.rans_jvp(W, K, V, VK, with_residual=True)
+        R0, RK0 = ns.rans_residual(W, K)
+        assert res_err(R, R0).max() <= 1e-13 and _krel(RK, RK0).max() <= 1e-13
+        dR, dRK = o.rans_residual_cstep(W, K, V, VK)
+        cols = [k for k in range(5) if np.abs(dR[:, k]).max() > 1e-12 * np.abs(dR).max()]
+        err = np.abs(JV - dR)[:, cols].max(axis=0) / np.abs(dR[:, cols]).max(axis=0)
+        assert err.max() <= 1e-10, err
+        assert _krel(JVK, dRK).max() <= 1e-10, _krel(JVK, dRK)
+
+
+@pytest.mark.gpu
+def test_rans_jvp_matches_central_difference(oracle_mod, fb):
+    """The tangent against FP64 central differences (h = 1e-6) of the device's
+    own coupled residual, limiter off (smooth), 8 seeded directions."""
+    case = _plate(ni=16, nj=8, nk=2, limiter="none", flux="Roe")
+    o, cs, m = build_pair(case, oracle_mod, fb)
+    ns = fb.NavierStokes(m, cs, 0)
+    W, K = _generic(case), case.kstate
+    rng = np.random.default_rng(23)
+    worst = 0.0
+    for _ in range(8):
+        V = rng.standard_normal(W.shape) * np.abs(W).max(axis=0) * np.array([1, 1, 1, 0, 1]) * 1e-3
+        VK = rng.standard_normal(K.shape) * np.abs(K).max(axis=0) * 1e-3
+        JV, JVK = ns.rans_jvp(W, K, V, VK)
+        h = 1e-6
+        Rp, RKp = ns.rans_residual(W + h * V, K + h * VK)
+        Rm, RKm = ns.rans_residual(W - h * V, K - h * VK)
+        fd, fdk = (Rp - Rm) / (2 * h), (RKp - RKm) / (2 * h)
+        cols = [0, 1, 2, 4]
+        worst = max(worst, (np.abs(JV - fd)[:, cols].max(axis=0) / np.abs(fd[:, cols]).max(axis=0)).max(),
+                    _krel(JVK, fdk).max())
+    assert worst <= 1e-5, worst
