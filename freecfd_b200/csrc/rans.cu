@@ -20,6 +20,7 @@ namespace fcfd {
 
 extern template __global__ void k_ghost_minmax<double>(DevCase, DevMesh, double *, unsigned long long *, int *);
 extern template __global__ void k_ghost_minmax<Dual<double>>(DevCase, DevMesh, Dual<double> *, unsigned long long *, int *);
+extern template __global__ void k_ghost_minmax<Dual<float>>(DevCase, DevMesh, Dual<float> *, unsigned long long *, int *);
 
 // rans.cc:43-49, model=k-omega (blending = 1)
 struct KOmega {
@@ -42,6 +43,7 @@ struct RansBuf {
 struct RansState {
   RansBuf<double> b;
   RansBuf<Dual<double>> d;  // tangent buffers, allocated by the first fcfd_rans_jvp
+  RansBuf<Dual<float>> f;   // the same for the FP32 tangent
   DBuf<double> vol;
 };
 
@@ -201,19 +203,21 @@ __global__ void k_k_to_soa(const double *__restrict__ in, double *__restrict__ K
 }
 
 // (value, tangent) AoS [nc][2] -> SoA duals with ghosts; duals -> AoS parts
-__global__ void k_seed_kdual(const double *__restrict__ k, const double *__restrict__ dk, Dual<double> *__restrict__ K,
+template <class T>
+__global__ void k_seed_kdual(const double *__restrict__ k, const double *__restrict__ dk, Dual<T> *__restrict__ K,
                              int nc, int nt) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= nc) return;
-  K[c] = Dual<double>(k[2 * c], dk[2 * c]);
-  K[nt + c] = Dual<double>(k[2 * c + 1], dk[2 * c + 1]);
+  K[c] = Dual<T>(T(k[2 * c]), T(dk[2 * c]));
+  K[nt + c] = Dual<T>(T(k[2 * c + 1]), T(dk[2 * c + 1]));
 }
-__global__ void k_split_kdual(const Dual<double> *__restrict__ RK, double *__restrict__ rk, double *__restrict__ drk, int nc) {
+template <class T>
+__global__ void k_split_kdual(const Dual<T> *__restrict__ RK, double *__restrict__ rk, double *__restrict__ drk, int nc) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= nc) return;
   for (int v = 0; v < 2; ++v) {
-    if (rk) rk[2 * c + v] = RK[2 * c + v].v;
-    drk[2 * c + v] = RK[2 * c + v].d;
+    if (rk) rk[2 * c + v] = double(RK[2 * c + v].v);
+    drk[2 * c + v] = double(RK[2 * c + v].d);
   }
 }
 
@@ -374,9 +378,13 @@ extern "C" int fcfd_rans_jvp(fcfd_ctx *x, const double *W, const double *K, cons
     cudaStream_t s = x->stream;
     const bool dev = flags & FCFD_DEVICE_PTRS;
     const size_t n = 5 * (size_t)m.nc, nk = 2 * (size_t)m.nc;
-    if (!x->pjv.ready) x->pjv.alloc(m.nc, m.nf, m.nb);
+    const bool f32 = flags & FCFD_JVP_FP32;
+    if (!f32 && !x->pjv.ready) x->pjv.alloc(m.nc, m.nf, m.nb);
+    if (f32 && !x->pjv32.ready) x->pjv32.alloc(m.nc, m.nf, m.nb);
     RansBuf<Dual<double>> &d = x->rans->d;
-    if (!d.ready) d.alloc(m.nc, m.nt, m.nf);
+    RansBuf<Dual<float>> &d32 = x->rans->f;
+    if (!f32 && !d.ready) d.alloc(m.nc, m.nt, m.nf);
+    if (f32 && !d32.ready) d32.alloc(m.nc, m.nt, m.nf);
     // host staging: W, V in Win / Vin; K, VK in the double k-omega buffers
     const double *w = W, *v = V, *k = K, *vk = VK;
     if (!dev) {
@@ -387,15 +395,23 @@ extern "C" int fcfd_rans_jvp(fcfd_ctx *x, const double *W, const double *K, cons
       w = x->Win.p; v = x->Vin.p; k = x->rans->b.RK.p; vk = x->rans->b.DK.p;
     }
     const int tb = 256;
-    k_seed_dual<double><<<(m.nc + tb - 1) / tb, tb, 0, s>>>(w, v, x->pjv.W.p, m.nc, m.nt);
-    k_seed_kdual<<<(m.nc + tb - 1) / tb, tb, 0, s>>>(k, vk, d.K.p, m.nc, m.nt);
-    rans_chain<Dual<double>, false>(x, x->pjv, d, d.mdot.p, d.wl.p, x->pjv.R.p, d.RK.p);
     double *r = R ? (dev ? R : x->Rtmp.p) : nullptr;
     double *jv = dev ? JV : x->Vin.p;
     double *rk = R ? (dev ? RK : x->rans->b.RK.p) : nullptr;
     double *jk = dev ? JVK : x->rans->b.DK.p;
-    k_split_dual<double><<<(m.nc + tb - 1) / tb, tb, 0, s>>>(x->pjv.R.p, r, jv, m.nc);
-    k_split_kdual<<<(m.nc + tb - 1) / tb, tb, 0, s>>>(d.RK.p, rk, jk, m.nc);
+    if (f32) {
+      k_seed_dual<float><<<(m.nc + tb - 1) / tb, tb, 0, s>>>(w, v, x->pjv32.W.p, m.nc, m.nt);
+      k_seed_kdual<float><<<(m.nc + tb - 1) / tb, tb, 0, s>>>(k, vk, d32.K.p, m.nc, m.nt);
+      rans_chain<Dual<float>, false>(x, x->pjv32, d32, d32.mdot.p, d32.wl.p, x->pjv32.R.p, d32.RK.p);
+      k_split_dual<float><<<(m.nc + tb - 1) / tb, tb, 0, s>>>(x->pjv32.R.p, r, jv, m.nc);
+      k_split_kdual<float><<<(m.nc + tb - 1) / tb, tb, 0, s>>>(d32.RK.p, rk, jk, m.nc);
+    } else {
+      k_seed_dual<double><<<(m.nc + tb - 1) / tb, tb, 0, s>>>(w, v, x->pjv.W.p, m.nc, m.nt);
+      k_seed_kdual<double><<<(m.nc + tb - 1) / tb, tb, 0, s>>>(k, vk, d.K.p, m.nc, m.nt);
+      rans_chain<Dual<double>, false>(x, x->pjv, d, d.mdot.p, d.wl.p, x->pjv.R.p, d.RK.p);
+      k_split_dual<double><<<(m.nc + tb - 1) / tb, tb, 0, s>>>(x->pjv.R.p, r, jv, m.nc);
+      k_split_kdual<double><<<(m.nc + tb - 1) / tb, tb, 0, s>>>(d.RK.p, rk, jk, m.nc);
+    }
     CK(cudaGetLastError());
     if (!dev) {
       if (R) {

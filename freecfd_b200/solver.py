@@ -184,15 +184,16 @@ class NavierStokes:
         check(lib.fcfd_rans_residual(self.h, _d(W), _d(K), _d(R), _d(RK), 0))
         return R, RK
 
-    def rans_jvp(self, W, K, V, VK, with_residual: bool = False):
+    def rans_jvp(self, W, K, V, VK, with_residual: bool = False, fp32: bool = False):
         """Tangent of the coupled residual along (V, VK): (JV[nc][5], JVK[nc][2]),
-        with (R, RK) first when with_residual."""
+        with (R, RK) first when with_residual; fp32 runs the tangent chain in
+        single precision."""
         nc = self.mesh.nc
         arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (W, K, V, VK)]
         JV, JVK = np.empty((nc, 5)), np.empty((nc, 2))
         R = np.empty((nc, 5)) if with_residual else None
         RK = np.empty((nc, 2)) if with_residual else None
-        check(lib.fcfd_rans_jvp(self.h, *[_d(a) for a in arrs], _d(R), _d(RK), _d(JV), _d(JVK), 0))
+        check(lib.fcfd_rans_jvp(self.h, *[_d(a) for a in arrs], _d(R), _d(RK), _d(JV), _d(JVK), 4 if fp32 else 0))
         return (R, RK, JV, JVK) if with_residual else (JV, JVK)
 
     def time_rans(self, reps: int = 50, flush_l2: bool = True):

@@ -171,7 +171,8 @@ int fcfd_time_rans(fcfd_ctx *ctx, int reps, int flush_l2, double *out, int out_l
  * applied to (V[nc][5], VK[nc][2]), evaluated by the same kernels as
  * fcfd_rans_residual on dual numbers (the eddy viscosity, the k-omega fluxes
  * and sources and their coupling into the NS viscous flux all carry the
- * tangent).  R and RK (both or neither) receive the residual. */
+ * tangent).  R and RK (both or neither) receive the residual.  flags may
+ * add FCFD_JVP_FP32: the tangent chain in single precision (as fcfd_jvp). */
 int fcfd_rans_jvp(fcfd_ctx *ctx, const double *W, const double *K, const double *V, const double *VK, double *R,
                   double *RK, double *JV, double *JVK, int flags);
 /* Fixed BC values of the RANS variables, per BC region: kw_fixed, k, omega,

@@ -128,3 +128,24 @@ def test_rans_jvp_matches_central_difference(oracle_mod, fb):
         worst = max(worst, (np.abs(JV - fd)[:, cols].max(axis=0) / np.abs(fd[:, cols]).max(axis=0)).max(),
                     _krel(JVK, fdk).max())
     assert worst <= 1e-5, worst
+
+
+@pytest.mark.gpu
+def test_rans_jvp_fp32(oracle_mod, fb):
+    """The FP32 tangent chain of the coupled residual (mixed-precision inner
+    products) agrees with the FP64 tangent to single-precision accuracy:
+    <= 1e-4 normwise per equation."""
+    case = _plate(ni=16, nj=8, nk=2, limiter="none", flux="Roe")
+    o, cs, m = build_pair(case, oracle_mod, fb)
+    ns = fb.NavierStokes(m, cs, 0)
+    W, K = _generic(case), case.kstate
+    rng = np.random.default_rng(29)
+    for _ in range(2):
+        V = rng.standard_normal(W.shape) * np.abs(W).max(axis=0) * np.array([1, 1, 1, 0, 1]) * 1e-3
+        VK = rng.standard_normal(K.shape) * np.abs(K).max(axis=0) * 1e-3
+        JV, JVK = ns.rans_jvp(W, K, V, VK)
+        JV32, JVK32 = ns.rans_jvp(W, K, V, VK, fp32=True)
+        cols = [0, 1, 2, 4]
+        err = np.abs(JV32 - JV)[:, cols].max(axis=0) / np.abs(JV[:, cols]).max(axis=0)
+        assert err.max() <= 1e-4, err
+        assert _krel(JVK32, JVK).max() <= 1e-4, _krel(JVK32, JVK)
