@@ -25,6 +25,7 @@
 #include <cstring>
 #include <fstream>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "ctx.hpp"
@@ -197,6 +198,29 @@ __global__ void k_precond(int nc, const double *__restrict__ Minv, const T *__re
 #pragma unroll
     for (int k = 0; k < 5; ++k) s += Minv[(5 * i + k) * nc + c] * xv[k];
     z[i * nc + c] = T(s);
+  }
+}
+
+// r = D^-1 v rounded to the preconditioner's type P, y = Minv r: the start of
+// the Gauss-Seidel preconditioner in one pass
+template <class T, class P>
+__global__ void k_precond_split(int nc, const double *__restrict__ Minv, const T *__restrict__ v,
+                                const RowScale *__restrict__ rs, P *__restrict__ r, P *__restrict__ y) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nc) return;
+  double xv[5];
+#pragma unroll
+  for (int k = 0; k < 5; ++k) {
+    const P rk = P(double(v[k * nc + c]) / rs->s[k]);
+    r[k * nc + c] = rk;
+    xv[k] = double(rk);
+  }
+#pragma unroll
+  for (int i = 0; i < 5; ++i) {
+    double s = 0.;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) s += Minv[(5 * i + k) * nc + c] * xv[k];
+    y[i * nc + c] = P(s);
   }
 }
 
@@ -379,9 +403,13 @@ __global__ void k_matvec_finish(DevCase cs, int nc, const double *__restrict__ W
 // ------------------------------------------------------------------ Krylov vector kernels
 constexpr int kRedBlocks = 592;  // 4 x 148
 
+__device__ void last_block_sum(int nparts, const double *part, double *__restrict__ out, unsigned *__restrict__ count);
 template <class T>
-__global__ void k_dots(int n, int nv, const T *__restrict__ V, size_t ld, const T *__restrict__ w, double *__restrict__ part) {
-  // part[v*gridDim.x + block] = sum over this block's slice of V_v . w
+__global__ void k_dots(int n, int nv, const T *__restrict__ V, size_t ld, const T *__restrict__ w, double *__restrict__ part,
+                       double *__restrict__ out = nullptr, unsigned *__restrict__ count = nullptr) {
+  // part[v*gridDim.x + block] = sum over this block's slice of V_v . w; with
+  // counters (one per column, blockDim == 256) the column's last block also
+  // writes out[v]
   const int v = blockIdx.y;
   const T *a = V + (size_t)v * ld;
   double s = 0.;
@@ -395,6 +423,7 @@ __global__ void k_dots(int n, int nv, const T *__restrict__ V, size_t ld, const 
     for (int k = 0; k < (int)(blockDim.x >> 5); ++k) t += sh[k];
     part[v * gridDim.x + blockIdx.x] = t;
   }
+  if (count) last_block_sum(gridDim.x, part + (size_t)v * gridDim.x, out + v, count + v);
   (void)nv;
 }
 __global__ void k_sum_parts(int nparts, const double *__restrict__ part, double *__restrict__ out) {
@@ -484,9 +513,38 @@ __global__ void k_gather_vol(int nc, const double *__restrict__ v, double *__res
 }
 
 // ------------------------------------------------------------------ solver
+// Second pass of a dot product inside the kernel that wrote its block
+// partials: the block of column v that finishes last adds part[0..nparts)
+// exactly as k_sum_parts does (same thread strides, shuffles and warp order,
+// so the sum is bit-identical) and re-arms the column's counter for the next
+// launch.  Blocks of kFusedThreads threads.
+constexpr int kFusedThreads = 256;
+__device__ void last_block_sum(int nparts, const double *part, double *__restrict__ out, unsigned *__restrict__ count) {
+  __shared__ unsigned ticket;
+  __shared__ double shs[kFusedThreads / 32];
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) ticket = atomicAdd(count, 1u);
+  __syncthreads();
+  if (ticket != (unsigned)nparts - 1u) return;
+  __threadfence();
+  double s = 0.;
+  for (int i = threadIdx.x; i < nparts; i += kFusedThreads) s += __ldcg(part + i);
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) shs[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.;
+    for (int k = 0; k < kFusedThreads / 32; ++k) t += shs[k];
+    *out = t;
+    *count = 0u;
+  }
+}
+
 // part[block] = sum over this block's slice of (z_i / wref_v)^2, v = i / nc
 template <class T>
-__global__ void k_wdot(int n, int nc, const T *__restrict__ z, const RowScale *__restrict__ winv, double *__restrict__ part) {
+__global__ void k_wdot(int n, int nc, const T *__restrict__ z, const RowScale *__restrict__ winv, double *__restrict__ part,
+                       double *__restrict__ out = nullptr, unsigned *__restrict__ count = nullptr) {
   double s = 0.;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const double q = double(z[i]) * winv->s[i / nc];
@@ -501,6 +559,8 @@ __global__ void k_wdot(int n, int nc, const T *__restrict__ z, const RowScale *_
     for (int k = 0; k < (int)(blockDim.x >> 5); ++k) t += sh[k];
     part[blockIdx.x] = t;
   }
+  // with a counter (blockDim == kFusedThreads): the last block also forms the sum
+  if (count) last_block_sum(gridDim.x, part, out, count);
 }
 
 template <class T>
@@ -510,12 +570,14 @@ __global__ void k_scale_rsqrt(int n, const double *__restrict__ ss, T *__restric
   if (i < n && q > 0.) b[i] = T(double(b[i]) / sqrt(q));
 }
 
+
 template <class T>
 struct Krylov {
   fcfd_ctx *x = nullptr;
   int n = 0, nc = 0, m = 0, nparts = 1;
   DBuf<T> V, w, tmpT;
   DBuf<double> part, hd;  // hd: [0,m+1) first CGS pass, [m+1,2m+2) second, [2m+2] |w|^2, [2m+3] |z|^2
+  DBuf<unsigned> count;   // per-column arrival counters of the single-launch dot products (re-armed by each launch)
   double *hp = nullptr;   // pinned host mirror of hd
   // one CUDA graph per basis index j of the Arnoldi step (preconditioner,
   // J.v, both Gram-Schmidt passes, normalisation, copy of hd to hp),
@@ -534,7 +596,8 @@ struct Krylov {
     x = ctx; nc = ctx->dm.nc; n = 5 * nc; m = krylov_dim;
     nparts = std::min(kRedBlocks, std::max(1, (n + 1023) / 1024));
     V.alloc((size_t)(m + 1) * n); w.alloc(n); tmpT.alloc(n);
-    part.alloc((size_t)nparts * (m + 1)); hd.alloc(2 * (size_t)m + 4);
+    part.alloc((size_t)nparts * (m + 1)); hd.alloc(2 * (size_t)m + 4); count.alloc(m + 1);
+    CK(cudaMemsetAsync(count.p, 0, sizeof(unsigned) * (m + 1), x->stream));
     CK(cudaMallocHost((void **)&hp, sizeof(double) * (2 * (size_t)m + 4)));
     graphs.assign(m, nullptr);
   }
@@ -548,6 +611,10 @@ struct Krylov {
     dim3 g(nparts, nv);
     k_dots<T><<<g, 256, 0, s>>>(n, nv, Vb, (size_t)n, u, part.p);
     k_sum_parts<<<nv, 256, 0, s>>>(nparts, part.p, out);
+  }
+  // out[v] = Vb_v . u for v < nv in one launch (the column's last block adds the partials)
+  void dots_fused(int nv, const T *Vb, const T *u, double *out) {
+    k_dots<T><<<dim3(nparts, nv), kFusedThreads, 0, x->stream>>>(n, nv, Vb, (size_t)n, u, part.p, out, count.p);
   }
   // bring hd back to the host (the one synchronisation of a GMRES iteration)
   void fetch_async() {
@@ -565,8 +632,7 @@ struct Krylov {
   // |S^-1 u|^2 on the device (S = per-variable reference magnitudes)
   void wnorm2_dev(const T *u, const RowScale *winv, double *out) {
     cudaStream_t s = x->stream;
-    k_wdot<T><<<nparts, 256, 0, s>>>(n, nc, u, winv, part.p);
-    k_sum_parts<<<1, 256, 0, s>>>(nparts, part.p, out);
+    k_wdot<T><<<nparts, kFusedThreads, 0, s>>>(n, nc, u, winv, part.p, out, count.p);
   }
   double norm64(const double *u) {
     cudaStream_t s = x->stream;
@@ -589,12 +655,6 @@ struct NewtonState {
   IterConsts hic;      // host copy of the iteration scalars
   DBuf<IterConsts> ic; // their device copy
 };
-template <class T, class P>
-__global__ void k_unscale(int nc, const T *__restrict__ v, const RowScale *__restrict__ rs, P *__restrict__ out) {
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= nc) return;
-  for (int k = 0; k < 5; ++k) out[k * nc + c] = P(double(v[k * nc + c]) / rs->s[k]);
-}
 template <class T>
 __global__ void k_axpy_to(int n, const double *__restrict__ b, const T *__restrict__ w, T *__restrict__ out) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -673,7 +733,7 @@ template <class T>
 static void apply_prec(fcfd_ctx *x, NewtonState &ns, const T *v, T *z, int sweeps) {
   const int nc = x->dm.nc, tb = 256, gc = (nc + tb - 1) / tb;
   cudaStream_t s = x->stream;
-  const RowScale *rs = &ns.ic.p->rs, *one = &ns.ic.p->one;
+  const RowScale *rs = &ns.ic.p->rs;
   if (sweeps <= 0) {
     k_precond<T><<<gc, tb, 0, s>>>(nc, ns.Minv.p, v, z, rs);
     return;
@@ -700,17 +760,22 @@ static void apply_prec(fcfd_ctx *x, NewtonState &ns, const T *v, T *z, int sweep
         }
     }
   };
-  if (ns.prec32) {
-    k_unscale<T, float><<<gc, tb, 0, s>>>(nc, v, rs, ns.Pr32.p);
-    k_precond<float><<<gc, tb, 0, s>>>(nc, ns.Minv.p, ns.Pr32.p, ns.Py32.p, one);
-    sweep(ns.OB32.p, ns.MinvP32.p, ns.Pr32.p, ns.Py32.p);
-    k_cast<T, float><<<(5 * nc + tb - 1) / tb, tb, 0, s>>>(5 * nc, ns.Py32.p, z);
-  } else {
-    k_unscale<T, double><<<gc, tb, 0, s>>>(nc, v, rs, ns.Pr.p);
-    k_precond<double><<<gc, tb, 0, s>>>(nc, ns.Minv.p, ns.Pr.p, ns.Py0.p, one);
-    sweep(ns.OB.p, ns.MinvP.p, ns.Pr.p, ns.Py0.p);
-    k_cast<T, double><<<(5 * nc + tb - 1) / tb, tb, 0, s>>>(5 * nc, ns.Py0.p, z);
-  }
+  // the sweeps run in place on z itself when it has the preconditioner's type
+  auto run = [&](auto *OB, auto *MinvP, auto *r, auto *y) {
+    using P = std::remove_pointer_t<decltype(y)>;
+    if constexpr (std::is_same_v<P, T>) {
+      k_precond_split<T, P><<<gc, tb, 0, s>>>(nc, ns.Minv.p, v, rs, r, z);
+      sweep(OB, MinvP, r, z);
+    } else {
+      k_precond_split<T, P><<<gc, tb, 0, s>>>(nc, ns.Minv.p, v, rs, r, y);
+      sweep(OB, MinvP, r, y);
+      k_cast<T, P><<<(5 * nc + tb - 1) / tb, tb, 0, s>>>(5 * nc, y, z);
+    }
+  };
+  if (ns.prec32)
+    run(ns.OB32.p, ns.MinvP32.p, ns.Pr32.p, ns.Py32.p);
+  else
+    run(ns.OB.p, ns.MinvP.p, ns.Pr.p, ns.Py0.p);
 }
 
 // Right-preconditioned GMRES(m) with up to `cycles` restarts.
@@ -760,11 +825,11 @@ static void gmres(fcfd_ctx *x, NewtonState &ns, Krylov<T> &K, int mode, double r
         if (mode == 0) K.wnorm2_dev(K.tmpT.p, &ns.ic.p->winv, K.zz());
         matvec<T>(x, ns, mode, K.tmpT.p, w, K.zz());
         // classical Gram-Schmidt twice, coefficients kept on the device
-        K.dots_dev(j + 1, K.V.p, w, K.h1());
+        K.dots_fused(j + 1, K.V.p, w, K.h1());
         k_sub_combo<T><<<gn, tb, 0, s>>>(n, j + 1, K.V.p, (size_t)n, K.h1(), w);
-        K.dots_dev(j + 1, K.V.p, w, K.h2());
+        K.dots_fused(j + 1, K.V.p, w, K.h2());
         k_sub_combo<T><<<gn, tb, 0, s>>>(n, j + 1, K.V.p, (size_t)n, K.h2(), w);
-        K.dots_dev(1, w, w, K.ww());
+        K.dots_fused(1, w, w, K.ww());
         k_scale_rsqrt<T><<<gn, tb, 0, s>>>(n, K.ww(), w);
         K.fetch_async();
         CK(cudaStreamEndCapture(s, &gr));
