@@ -117,6 +117,10 @@ struct fcfd_ctx {
   int graph_fast_grad = -1;
   bool newton_frozen = false;
   bool newton_f32 = false;  // Krylov matvecs through the FP32 tangent chain
+  // one rank's part of a domain-decomposed residual: `dm` with the partition
+  // lists set (the PART instantiations of the chain's kernels use it)
+  DevMesh dmp{};
+  DBuf<int> part_cells, part_faces, part_outlet, part_ghosts;
 };
 
 
@@ -128,36 +132,41 @@ int check_err(fcfd_ctx *x);
 
 // Gradient + limiter launch: the fused-gradient and bit-exact instantiations
 // are separate kernels so each gets the registers its own path needs.
-template <class S>
+// PART: the gradient cells of one rank of a domain decomposition (m = dmp).
+template <class S, bool PART = false>
 inline void launch_grad_limiter(const DevCase &cs, const DevMesh &m, const S *W, const unsigned long long *ext,
                                 const int *argx, S *G, S *Lm, cudaStream_t s) {
+  const int g = ((PART ? m.n_part_cells : m.nc) + 127) / 128;
+  if (g == 0) return;
   if (cs.fast_grad)
-    k_grad_limiter<S, true><<<(m.nc + 127) / 128, 128, 0, s>>>(cs, m, W, ext, argx, G, Lm);
+    k_grad_limiter<S, true, PART><<<g, 128, 0, s>>>(cs, m, W, ext, argx, G, Lm);
   else
-    k_grad_limiter<S, false><<<(m.nc + 127) / 128, 128, 0, s>>>(cs, m, W, ext, argx, G, Lm);
+    k_grad_limiter<S, false, PART><<<g, 128, 0, s>>>(cs, m, W, ext, argx, G, Lm);
 }
 // Face fluxes of one residual: the main launch over all faces and, when the
 // mesh has outlet faces, the outlet-face launch (stale right densities) on the
 // side stream, forked after the gradient kernel and joined before the gather.
-template <class S>
+// PART: the faces of one rank of a domain decomposition (x->dmp).
+template <class S, bool PART = false>
 inline void launch_faces(fcfd_ctx *x, Pipe<S> &P, const S *mu_t, S *mo, S *wo, cudaStream_t s) {
-  const DevMesh &m = x->dm;
-  const bool side = m.n_outlet > 0;
+  const DevMesh &m = PART ? x->dmp : x->dm;
+  const int no = PART ? m.n_part_outlet : m.n_outlet, nfl = PART ? m.n_part_faces : m.nf;
+  const bool side = no > 0;
   if (side) {
     CK(cudaEventRecord(x->ev_fork, s));
     CK(cudaStreamWaitEvent(x->side, x->ev_fork, 0));
-    const int g = (m.n_outlet + 127) / 128;
+    const int g = (no + 127) / 128;
     if (x->viscous)
-      FCFD_BY_FLUX(x->cs.flux, k_face_flux<S, true, FX, true><<<g, 128, 0, x->side>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p, mu_t, P.D.p, mo, wo, x->err.p));
+      FCFD_BY_FLUX(x->cs.flux, k_face_flux<S, true, FX, true, PART><<<g, 128, 0, x->side>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p, mu_t, P.D.p, mo, wo, x->err.p));
     else
-      FCFD_BY_FLUX(x->cs.flux, k_face_flux<S, false, FX, true><<<g, 128, 0, x->side>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p, mu_t, P.D.p, mo, wo, x->err.p));
+      FCFD_BY_FLUX(x->cs.flux, k_face_flux<S, false, FX, true, PART><<<g, 128, 0, x->side>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p, mu_t, P.D.p, mo, wo, x->err.p));
     CK(cudaEventRecord(x->ev_join, x->side));
   }
-  const int g = (m.nf + 127) / 128;
-  if (x->viscous)
-    FCFD_BY_FLUX(x->cs.flux, k_face_flux<S, true, FX, false><<<g, 128, 0, s>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p, mu_t, P.D.p, mo, wo, x->err.p));
-  else
-    FCFD_BY_FLUX(x->cs.flux, k_face_flux<S, false, FX, false><<<g, 128, 0, s>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p, mu_t, P.D.p, mo, wo, x->err.p));
+  const int g = (nfl + 127) / 128;
+  if (g > 0 && x->viscous)
+    FCFD_BY_FLUX(x->cs.flux, k_face_flux<S, true, FX, false, PART><<<g, 128, 0, s>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p, mu_t, P.D.p, mo, wo, x->err.p));
+  else if (g > 0)
+    FCFD_BY_FLUX(x->cs.flux, k_face_flux<S, false, FX, false, PART><<<g, 128, 0, s>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p, mu_t, P.D.p, mo, wo, x->err.p));
   if (side) CK(cudaStreamWaitEvent(s, x->ev_join, 0));
 }
 void adjoint_free(fcfd_ctx *x);

@@ -44,10 +44,11 @@ void launch_chain(fcfd_ctx *x, Pipe<S> &P, S *Rout, bool aos_out, S *mo, S *wo, 
   }
   launch_grad_limiter<S>(csl, m, P.W.p, x->ext.p, argx, P.G.p, P.Lm.p, s);
   launch_faces<S>(x, P, (const S *)nullptr, mo, wo, s);
+  const int gg = (5 * m.nc + tb - 1) / tb;
   if (aos_out)
-    k_gather<S, true><<<(5 * m.nc + tb - 1) / tb, tb, 0, s>>>(m, P.D.p, Rout, x->ext.p, x->argx.p);
+    k_gather<S, true><<<gg, tb, 0, s>>>(m, P.D.p, Rout, x->ext.p, x->argx.p);
   else
-    k_gather<S, false><<<(5 * m.nc + tb - 1) / tb, tb, 0, s>>>(m, P.D.p, Rout, x->ext.p, x->argx.p);
+    k_gather<S, false><<<gg, tb, 0, s>>>(m, P.D.p, Rout, x->ext.p, x->argx.p);
   CK(cudaGetLastError());
 }
 

@@ -173,7 +173,17 @@ struct DevMesh {
   const int *outlet_faces;                 // outlet boundary faces [n_outlet]
   const double *f_wall, *f_diss;           // [nf] wall distance, dissipation factor (Steger-Warming only)
   int n_outlet;
+  // Partitioned evaluation (one rank of a domain decomposition; null lists =
+  // the whole mesh): cells whose gradient and limiter are formed, faces whose
+  // flux is formed, indices into outlet_faces, ghost indices to update, and
+  // the owned cells [own_lo, own_hi) (extrema and gather).
+  const int *part_cells = nullptr, *part_faces = nullptr, *part_outlet = nullptr, *part_ghosts = nullptr;
+  int n_part_cells = 0, n_part_faces = 0, n_part_outlet = 0, n_part_ghosts = 0;
+  int own_lo = 0, own_hi = 0;
 };
+// thread counts of the ghost and gather kernels (partition-aware)
+__host__ __device__ inline int n_ghost_threads(const DevMesh &m) { return m.part_ghosts ? m.n_part_ghosts : m.nb; }
+__host__ __device__ inline int n_owned(const DevMesh &m) { return m.part_cells ? m.own_hi - m.own_lo : m.nc; }
 
 enum { T_SYM = 1, T_WALL = 2, T_INLET = 3, T_OUTLET = 4 };
 enum { KN_NONE = -1, KN_NO_REVERSE = 1, KN_DAMP_REVERSE = 2, KN_VELOCITY = 3, KN_MDOT = 4, KN_SLIP = 5, KN_STAGNATION = 6,
@@ -435,10 +445,12 @@ __device__ __forceinline__ double okey_inv(unsigned long long k) {
 template <class S>
 __global__ void k_ghost_minmax(DevCase cs, DevMesh m, S *__restrict__ W, unsigned long long *__restrict__ ext, int *err) {
   const int nt = m.nt;
-  const int ghost_blocks = (m.nb + blockDim.x - 1) / blockDim.x;
+  const int nbl = n_ghost_threads(m);
+  const int ghost_blocks = (nbl + blockDim.x - 1) / blockDim.x;
   if ((int)blockIdx.x < ghost_blocks) {
-    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
-    if (tid >= m.nb) return;
+    int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid >= nbl) return;
+    if (m.part_ghosts) tid = m.part_ghosts[tid];
     const int f = m.bface[tid];
     const int pa = m.f_parent[f];
     const int b = m.f_bc[f];
@@ -456,7 +468,10 @@ __global__ void k_ghost_minmax(DevCase cs, DevMesh m, S *__restrict__ W, unsigne
   // shuffles, a shared-memory block reduction and one atomic per block/slot.
   const int eb = blockIdx.x - ghost_blocks, neb = gridDim.x - ghost_blocks;
   double mx[4] = {-INFINITY, -INFINITY, -INFINITY, -INFINITY}, mn[4] = {INFINITY, INFINITY, INFINITY, INFINITY};
-  for (int c = eb * blockDim.x + threadIdx.x; c < m.nc; c += neb * blockDim.x) {
+  // over the owned cells of a partition (global ids, so the quirk slots keep
+  // their meaning), else over all interior cells
+  const int c0 = m.part_cells ? m.own_lo : 0, c1 = m.part_cells ? m.own_hi : m.nc;
+  for (int c = c0 + eb * blockDim.x + threadIdx.x; c < c1; c += neb * blockDim.x) {
     const double p = val(W[c]), u = val(W[nt + c]), v = val(W[2 * nt + c]);
     mx[0] = fmax(mx[0], p); mn[0] = fmin(mn[0], p);
     mx[1] = fmax(mx[1], u); mn[1] = fmin(mn[1], u);
@@ -529,13 +544,20 @@ __global__ void k_split_dual(const Dual<T> *__restrict__ R, double *__restrict__
 // lsqr_grad_map weights) + limiter, one thread per interior cell.
 // The FP64 bit-exact instantiation runs at six blocks per SM (register cap),
 // measured 8 % faster on the prism mesh; the others keep their registers.
-template <class S, bool FAST>
+template <class S, bool FAST, bool PART = false>
 __global__ void __launch_bounds__(128, (!FAST && std::is_same<S, double>::value) ? 6 : 1) k_grad_limiter(DevCase cs, DevMesh m, const S *__restrict__ W,
                                                       const unsigned long long *__restrict__ ext, const int *__restrict__ argx,
                                                       S *__restrict__ G, S *__restrict__ Lm) {
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int nc = m.nc, nt = m.nt;
-  if (c >= nc) return;
+  // PART: one rank's gradient cells of a domain decomposition
+  int c = i;
+  if constexpr (PART) {
+    if (i >= m.n_part_cells) return;
+    c = m.part_cells[i];
+  } else {
+    if (i >= nc) return;
+  }
   const double xc0 = m.c_x[c], xc1 = m.c_x[nt + c], xc2 = m.c_x[2 * nt + c];
   S g[15];
 #pragma unroll
@@ -1151,15 +1173,22 @@ __device__ __forceinline__ bool face_states(const DevCase &cs, const DevMesh &m,
 // (thread i takes outlet face i), with the cached density computed in place
 // and stored in `stale` for the face-Jacobian kernel.  The two launches write
 // disjoint faces and run concurrently.
-template <class S, bool VISCOUS, int FX, bool OUTLET>
+template <class S, bool VISCOUS, int FX, bool OUTLET, bool PART = false>
 __global__ void __launch_bounds__(128) k_face_flux(DevCase cs, DevMesh m, const S *__restrict__ W, const S *__restrict__ G,
                                                    const S *__restrict__ Lm, S *stale,
                                                    const S *__restrict__ mu_t, S *__restrict__ D, S *__restrict__ mdot_out,
                                                    S *__restrict__ wl_out, int *err) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int nf = m.nf;
-  if (i >= (OUTLET ? m.n_outlet : nf)) return;
-  const int f = OUTLET ? m.outlet_faces[i] : i;
+  // PART: one rank's faces of a domain decomposition
+  int f;
+  if constexpr (PART) {
+    if (i >= (OUTLET ? m.n_part_outlet : m.n_part_faces)) return;
+    f = OUTLET ? m.outlet_faces[m.part_outlet[i]] : m.part_faces[i];
+  } else {
+    if (i >= (OUTLET ? m.n_outlet : nf)) return;
+    f = OUTLET ? m.outlet_faces[i] : i;
+  }
   const int pa = m.f_parent[f], nb = m.f_neighbor[f], b = m.f_bc[f];
   const double n[3] = {m.f_n[f], m.f_n[nf + f], m.f_n[2 * nf + f]};
   const double A = m.f_area[f];
@@ -1194,9 +1223,9 @@ __global__ void k_gather(DevMesh m, const S *__restrict__ D, S *__restrict__ R, 
   // one thread per (cell, equation): 5 nc threads, equation-major so that a
   // warp covers consecutive cells of one equation
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  const int nc = m.nc;
-  if (t >= 5 * nc) return;
-  const int v = t / nc, c = t - v * nc;
+  const int nc = m.nc, no = n_owned(m), lo = m.part_cells ? m.own_lo : 0;
+  if (t >= 5 * no) return;
+  const int v = t / no, c = lo + (t - v * no);
   const S *Dv = D + (size_t)v * m.nf;
   const int j0 = m.cf_index[c], j1 = m.cf_index[c + 1];
   S r = S(0.);

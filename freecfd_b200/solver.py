@@ -138,6 +138,31 @@ class NavierStokes:
         check(lib.fcfd_residual(self.h, pw, pr, fw))
         return out
 
+    def set_partition(self, lo: int, hi: int):
+        """Evaluate only the part of the residual that owned cells [lo, hi)
+        need (lo = hi = 0: the whole mesh again)."""
+        check(lib.fcfd_ctx_set_partition(self.h, int(lo), int(hi)))
+        self.partition = (int(lo), int(hi)) if hi > lo else None
+
+    def partition_extrema(self, W):
+        """Phase 1 of the partitioned residual: load W [nc][5] (owned and halo
+        rows current), update this part's ghosts; returns the 8 VK extrema of
+        the owned cells (combine over ranks: max of even, min of odd slots)."""
+        if isinstance(W, np.ndarray):
+            W = np.ascontiguousarray(W, dtype=np.float64)
+        pw, fw = _ptr(W)
+        ext = np.empty(8)
+        check(lib.fcfd_partition_extrema(self.h, pw, _d(ext), fw))
+        return ext
+
+    def partition_residual(self, ext, out):
+        """Phase 2: rows [lo, hi) of R (numpy [nc][5] or CUDA tensor) from the
+        extrema combined over all ranks."""
+        ext = np.ascontiguousarray(ext, dtype=np.float64)
+        pr, fr = _ptr(out)
+        check(lib.fcfd_partition_residual(self.h, _d(ext), pr, fr))
+        return out
+
     def jvp(self, W, V, with_residual: bool = False, fp32: bool = False):
         """Directional derivative (dR/dW).V of the residual (forward tangent);
         fp32=True evaluates the tangent chain in single precision."""

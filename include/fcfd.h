@@ -175,6 +175,31 @@ int fcfd_time_rans(fcfd_ctx *ctx, int reps, int flush_l2, double *out, int out_l
  * add FCFD_JVP_FP32: the tangent chain in single precision (as fcfd_jvp). */
 int fcfd_rans_jvp(fcfd_ctx *ctx, const double *W, const double *K, const double *V, const double *VK, double *R,
                   double *RK, double *JV, double *JVK, int flags);
+/* Domain decomposition: one rank's part of the residual.  Replaces the
+ * partition-ghost exchange of the reference's MPI runs
+ * (NavierStokes::mpi_update_ghost_primitives / mpi_update_ghost_gradients,
+ * navier_stokes/ns_mpi.cc:62-140, called from ns.cc:92-115) and the extrema
+ * all-reduce of find_min_max (ns.cc:425-427).  A rank owns the global cells
+ * [lo, hi).  fcfd_partition_sets (host only, no device needed) returns
+ * counts[4] = {cells whose gradient is formed, faces whose flux is formed,
+ * halo cells, ghosts updated} and, where the arrays are not NULL, the
+ * gradient cells, the faces and the halo cells (not owned; their states must
+ * be current before phase 1; ascending global ids).  Gradients are
+ * recomputed on the halo, so only states are exchanged.
+ *
+ * fcfd_ctx_set_partition selects the range on a context (lo = hi = 0: none).
+ * fcfd_partition_extrema (phase 1) loads W [nc][5] and returns ext[8]: the
+ * VK limiter's extrema over the owned cells (max p, min p, max u, min u,
+ * max v, min v, max p and min p below the last cell; -inf/+inf where empty),
+ * to be combined over the ranks with max (even slots) and min (odd slots).
+ * fcfd_partition_residual (phase 2) takes the combined ext and writes rows
+ * [lo, hi) of R [nc][5]: bit for bit the single-domain residual's rows. */
+int fcfd_partition_sets(const fcfd_mesh *mesh, const fcfd_case *cs, int lo, int hi, int counts[4], int *grad_cells,
+                        int *faces, int *halo);
+int fcfd_ctx_set_partition(fcfd_ctx *ctx, int lo, int hi);
+int fcfd_partition_extrema(fcfd_ctx *ctx, const double *W, double ext[8], int flags);
+int fcfd_partition_residual(fcfd_ctx *ctx, const double ext[8], double *R, int flags);
+
 /* Fixed BC values of the RANS variables, per BC region: kw_fixed, k, omega,
  * mut_fixed, mu_t (5 doubles each; out_len >= 5 * number of regions). */
 int fcfd_rans_bcs(const fcfd_ctx *ctx, double *out, int32_t out_len);

@@ -1,0 +1,101 @@
+"""Domain-decomposed residual on the device: every part of a 2- and 3-way
+split evaluated in its own context, with the states of all cells outside the
+part's owned range and halo replaced by a different (valid) state, the VK
+extrema combined over the parts as the ranks' all-reduce does; the owned
+rows equal the single-domain residual bit for bit (the reference's MPI runs
+exchange partition ghosts, ns_mpi.cc:62-140, and all-reduce the extrema,
+ns.cc:425-427, so each rank's residual rows are the global ones)."""
+import numpy as np
+import pytest
+
+from freecfd_b200.partition import HaloPlan
+from tests.util import ALL, SMALL
+
+
+def _setup(fb, case):
+    import tempfile
+    d = tempfile.mkdtemp(prefix="fcfd_partg_")
+    cs = fb.Case(case.write_deck(d))
+    return cs, fb.Mesh(case.mesh, cs)
+
+
+def _partitioned(fb, case, cs, m, nparts, exact=False, device=False):
+    plan = HaloPlan(m, cs, nparts)
+    state = case.state
+    rng = np.random.default_rng(11)
+    other = state * (1 + 0.05 * rng.uniform(-1, 1, state.shape))
+    parts = []
+    for r, (lo, hi) in enumerate(plan.ranges):
+        ns = fb.NavierStokes(m, cs, 0, exact_gradients=exact)
+        ns.set_partition(lo, hi)
+        W = other.copy()
+        W[lo:hi] = state[lo:hi]
+        h = plan.halo_cells(r)
+        W[h] = state[h]
+        if device:
+            import torch
+            W = torch.as_tensor(W, device="cuda")
+        parts.append((ns, W, lo, hi))
+    exts = np.array([ns.partition_extrema(W) for ns, W, _, _ in parts])
+    ext = np.where(np.arange(8) % 2 == 0, exts.max(axis=0), exts.min(axis=0))
+    R = np.full((m.nc, 5), np.nan)
+    for ns, W, lo, hi in parts:
+        if device:
+            import torch
+            out = torch.full((m.nc, 5), float("nan"), dtype=torch.float64, device="cuda")
+            ns.partition_residual(ext, out)
+            out = out.cpu().numpy()
+        else:
+            out = np.full((m.nc, 5), np.nan)
+            ns.partition_residual(ext, out)
+        assert np.isnan(out[:lo]).all() and np.isnan(out[hi:]).all()
+        R[lo:hi] = out[lo:hi]
+    return R
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("nparts", [2, 3])
+@pytest.mark.parametrize("family", sorted(ALL))
+def test_partitioned_residual_bit_exact(family, nparts, fb):
+    case = ALL[family]()
+    cs, m = _setup(fb, case)
+    ref = fb.NavierStokes(m, cs, 0).residual(case.state)
+    R = _partitioned(fb, case, cs, m, nparts)
+    assert np.array_equal(R.view(np.uint64), ref.view(np.uint64))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("family,kw", [("wedge", dict(limiter="minmod")), ("cylinder", dict(flux="AUSM+up")),
+                                       ("hypersonic", dict(limiter="vk")), ("plate", dict(flux="SD-SLAU"))])
+def test_partitioned_residual_exact_gradients_and_fluxes(family, kw, fb):
+    case = SMALL[family](**kw)
+    cs, m = _setup(fb, case)
+    ref = fb.NavierStokes(m, cs, 0, exact_gradients=True).residual(case.state)
+    R = _partitioned(fb, case, cs, m, 4, exact=True)
+    assert np.array_equal(R.view(np.uint64), ref.view(np.uint64))
+
+
+@pytest.mark.gpu
+def test_partitioned_residual_device_pointers(fb):
+    case = SMALL["cylinder"]()
+    cs, m = _setup(fb, case)
+    ref = fb.NavierStokes(m, cs, 0).residual(case.state)
+    R = _partitioned(fb, case, cs, m, 3, device=True)
+    assert np.array_equal(R.view(np.uint64), ref.view(np.uint64))
+
+
+@pytest.mark.gpu
+def test_partition_errors(fb):
+    case = SMALL["wedge"]()
+    cs, m = _setup(fb, case)
+    ns = fb.NavierStokes(m, cs, 0)
+    with pytest.raises(fb.FcfdError):
+        ns.partition_extrema(case.state)  # no partition selected
+    with pytest.raises(fb.FcfdError):
+        ns.set_partition(0, m.nc + 1)
+    ns.set_partition(0, m.nc // 2)
+    ns.set_partition(0, 0)
+    # the whole-mesh residual is unaffected by a partition set and cleared
+    R = ns.residual(case.state)
+    ref = fb.NavierStokes(m, cs, 0).residual(case.state)
+    assert np.array_equal(R, ref)
