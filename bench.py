@@ -319,6 +319,8 @@ def run_ours(args):
             "kernels_ms": {k: round(float(v), 5) for k, v in kern.items()},
             "gpu_launches": n_kernels * args.steps,
             "clocks": clk.summary()}
+    if (world > 1 or args.decomposed) and args.workload == "cylinder":
+        line["decomposed"] = run_decomposed(fb, world, rank, dev, dist, args.steps, args.warmup)
     if not args.no_newton and not rans:
         line["newton"] = run_newton(fb, cs, mesh, case, dev, dist)
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -329,6 +331,48 @@ def run_ours(args):
     if dist:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def run_decomposed(fb, world, rank, dev, dist, steps, warmup):
+    """One residual of a cylinder mesh N times as deep radially (256 x 128N
+    cells, weak scaling) split over the N ranks in contiguous cell ranges:
+    per step the halo states are exchanged (NCCL point-to-point), the VK
+    extrema all-reduced and each rank evaluates its owned rows.  Wall time
+    between synchronised points (the extrema pass through the host), max
+    over ranks."""
+    import tempfile
+
+    import torch
+    from freecfd_b200 import cases
+    from freecfd_b200.partition import HaloPlan, PartitionedResidual
+    case = cases.cylinder_case(ntheta=256, nr=128 * world)
+    cs = fb.Case(case.write_deck(tempfile.mkdtemp(prefix="fcfd_dd_")))
+    mesh = fb.Mesh(case.mesh, cs)
+    plan = HaloPlan(mesh, cs, world)
+    ns = fb.NavierStokes(mesh, cs, dev)
+    W = torch.as_tensor(np.ascontiguousarray(case.state), device="cuda")
+    R = torch.empty_like(W)
+    res = PartitionedResidual(ns, plan, rank, W)
+    for _ in range(max(warmup, 1)):
+        res(R)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        res(R)
+    torch.cuda.synchronize()
+    el = time.perf_counter() - t0
+    halo = len(plan.halo_cells(rank))
+    x = torch.tensor([el, float(res.ex.bytes_per_exchange), float(halo)], device="cuda", dtype=torch.float64)
+    if dist:
+        dist.all_reduce(x, op=dist.ReduceOp.MAX)
+    el, nbytes, halo = (float(v) for v in x.cpu())
+    del res, ns
+    return {"workload": f"laminar_cylinder_256x{128 * world}x1_hex_roe_viscous split in {world} contiguous ranges",
+            "cells": mesh.nc, "faces": mesh.nf, "value": round(mesh.nf * steps / el / 1e6, 3), "unit": UNIT,
+            "ms_per_step": round(1e3 * el / steps, 5), "scaling": "weak", "timing": "wall, max over ranks",
+            "halo_cells_max": int(halo), "halo_bytes_received_per_step_max": int(nbytes)}
 
 
 # 20 symmetric Gauss-Seidel sweeps: the fastest setting of both arms within a
@@ -437,6 +481,8 @@ def main():
     ap.add_argument("--ref-workers", type=int, default=64)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-newton", action="store_true")
+    ap.add_argument("--decomposed", action="store_true",
+                    help="also time the domain-decomposed residual (always on under torchrun)")
     ap.add_argument("--profile-newton", type=int, default=0,
                     help="run only the two Newton arms, capped at this many Newton steps")
     args = ap.parse_args()

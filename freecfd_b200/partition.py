@@ -12,8 +12,6 @@ the owned rows of R depend on, so the state is exchanged once per residual and
 gradients are recomputed on the halo instead of being exchanged.  The owned
 rows equal the single-domain residual bit for bit.
 """
-import ctypes
-
 import numpy as np
 
 from ._lib import _i, check, lib
@@ -95,6 +93,8 @@ def combine_extrema(ext, device=None):
     ones (one all-reduce, odd slots negated)."""
     import torch
     import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()):
+        return np.asarray(ext, dtype=np.float64)
     t = torch.as_tensor(np.asarray(ext, dtype=np.float64).copy(), device=device)
     t[1::2] = -t[1::2]
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -118,6 +118,10 @@ class PartitionedResidual:
 
     def __call__(self, R):
         self.ex.exchange()
+        if self.W.is_cuda:
+            # the unpacking ran on torch's stream; the library reads W on its own
+            import torch
+            torch.cuda.current_stream(self.W.device).synchronize()
         ext = self.ns.partition_extrema(self.W)
         ext = combine_extrema(ext, self.W.device)
         return self.ns.partition_residual(ext, R)
