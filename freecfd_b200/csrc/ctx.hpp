@@ -115,6 +115,13 @@ struct fcfd_ctx {
   int n_outlet = 0;
   cudaGraphExec_t graph = nullptr;  // the timed residual chain
   int graph_fast_grad = -1;
+  // fcfd_residual with pinned host buffers: copy in, chain, copy out and the
+  // error flag as one graph, kept for the last (W, R) pair
+  cudaGraphExec_t host_graph = nullptr;
+  const double *host_graph_W = nullptr;
+  double *host_graph_R = nullptr;
+  int host_graph_fast_grad = -1;
+  int *err_pinned = nullptr;
   bool newton_frozen = false;
   bool newton_f32 = false;  // Krylov matvecs through the FP32 tangent chain
   // one rank's part of a domain-decomposed residual: `dm` with the partition

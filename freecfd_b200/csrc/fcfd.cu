@@ -315,6 +315,8 @@ void fcfd_ctx_destroy(fcfd_ctx *x) {
   if (!x) return;
   cudaSetDevice(x->device);
   if (x->graph) cudaGraphExecDestroy(x->graph);
+  if (x->host_graph) cudaGraphExecDestroy(x->host_graph);
+  if (x->err_pinned) cudaFreeHost(x->err_pinned);
   adjoint_free(x);
   rans_free(x);
   if (x->ev_fork) cudaEventDestroy(x->ev_fork);
@@ -324,12 +326,48 @@ void fcfd_ctx_destroy(fcfd_ctx *x) {
   delete x;
 }
 
+// page-locked (pinned or registered) host memory
+static bool host_pinned(const void *p) {
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost;
+}
+
 int fcfd_residual(fcfd_ctx *x, const double *W, double *R, int flags) {
   API_BEGIN
   if (!x || !W || !R) throw Error(FCFD_ERR_INPUT, "null argument");
   CK(cudaSetDevice(x->device));
   const DevMesh &m = x->dm;
   const bool dev = flags & FCFD_DEVICE_PTRS;
+  if (!dev && host_pinned(W) && host_pinned(R)) {
+    // one graph launch: host-to-device copy, the chain, device-to-host copy
+    // and the error flag, then one synchronisation
+    cudaStream_t s = x->stream;
+    if (!x->err_pinned) CK(cudaMallocHost((void **)&x->err_pinned, sizeof(int)));
+    if (!x->host_graph || x->host_graph_W != W || x->host_graph_R != R || x->host_graph_fast_grad != x->cs.fast_grad) {
+      if (x->host_graph) { CK(cudaGraphExecDestroy(x->host_graph)); x->host_graph = nullptr; }
+      cudaGraph_t g = nullptr;
+      CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+      CK(cudaMemcpyAsync(x->Win.p, W, sizeof(double) * 5 * m.nc, cudaMemcpyHostToDevice, s));
+      k_aos_to_soa<double><<<(m.nc + 255) / 256, 256, 0, s>>>(x->Win.p, x->p64.W.p, m.nc, m.nt);
+      launch_chain<double>(x, x->p64, x->Rtmp.p, true, x->mdot.p, x->wl.p);
+      CK(cudaMemcpyAsync(R, x->Rtmp.p, sizeof(double) * 5 * m.nc, cudaMemcpyDeviceToHost, s));
+      CK(cudaMemcpyAsync(x->err_pinned, x->err.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+      CK(cudaStreamEndCapture(s, &g));
+      CK(cudaGraphInstantiate(&x->host_graph, g, 0));
+      CK(cudaGraphDestroy(g));
+      x->host_graph_W = W;
+      x->host_graph_R = R;
+      x->host_graph_fast_grad = x->cs.fast_grad;
+    }
+    CK(cudaGraphLaunch(x->host_graph, s));
+    CK(cudaStreamSynchronize(s));
+    if (*x->err_pinned) check_err(x);  // reports and clears the flag
+    return FCFD_OK;
+  }
   const double *win = W;
   if (!dev) {
     CK(cudaMemcpyAsync(x->Win.p, W, sizeof(double) * 5 * m.nc, cudaMemcpyHostToDevice, x->stream));

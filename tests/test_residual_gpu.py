@@ -192,6 +192,38 @@ def test_determinism_and_device_pointers(oracle_mod, fb):
 
 
 @pytest.mark.gpu
+def test_pinned_host_buffers(oracle_mod, fb):
+    """Page-locked W and R take the one-graph path (copies, chain and error
+    flag replayed as a CUDA graph): same bits as pageable buffers, for a new
+    state in the same buffers and for another buffer pair; a BC error raised
+    inside the graph is reported and cleared."""
+    import torch
+    case = SMALL["cylinder"]()
+    o, cs, m, ns = _ctx(case, oracle_mod, fb)
+    ref = ns.residual(case.state)
+    bufs = [(torch.empty((m.nc, 5), dtype=torch.float64, pin_memory=True),
+             torch.empty((m.nc, 5), dtype=torch.float64, pin_memory=True)) for _ in range(2)]
+    W2 = case.state * (1 + 1e-3 * np.random.default_rng(5).uniform(-1, 1, case.state.shape))
+    ref2 = ns.residual(W2)
+    for Wp, Rp in bufs:
+        for W, r in ((case.state, ref), (W2, ref2), (case.state, ref)):
+            Wp.numpy()[:] = W
+            ns.residual(Wp.numpy(), Rp.numpy())
+            assert np.array_equal(Rp.numpy(), r)
+    # supersonic flow into the inlet, whose deck gives rho and V only
+    Wbad = case.state.copy()
+    Wbad[:, 1] = 1500.0
+    Wp, Rp = bufs[0]
+    Wp.numpy()[:] = Wbad
+    with pytest.raises(fb.FcfdError) as e:
+        ns.residual(Wp.numpy(), Rp.numpy())
+    assert e.value.code == 8
+    Wp.numpy()[:] = case.state
+    ns.residual(Wp.numpy(), Rp.numpy())
+    assert np.array_equal(Rp.numpy(), ref)
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("mode", [0, 1])
 def test_local_dt(mode, oracle_mod, fb):
     case = SMALL["wedge"]()
