@@ -128,6 +128,7 @@ struct fcfd_ctx {
   // lists set (the PART instantiations of the chain's kernels use it)
   DevMesh dmp{};
   DBuf<int> part_cells, part_faces, part_outlet, part_ghosts;
+  DBuf<int> face_order;  // faces grouped by kind (DevMesh::face_list of the whole mesh)
 };
 
 
@@ -157,7 +158,7 @@ inline void launch_grad_limiter(const DevCase &cs, const DevMesh &m, const S *W,
 template <class S, bool PART = false>
 inline void launch_faces(fcfd_ctx *x, Pipe<S> &P, const S *mu_t, S *mo, S *wo, cudaStream_t s) {
   const DevMesh &m = PART ? x->dmp : x->dm;
-  const int no = PART ? m.n_part_outlet : m.n_outlet, nfl = PART ? m.n_part_faces : m.nf;
+  const int no = PART ? m.n_part_outlet : m.n_outlet, nfl = (PART || x->viscous) ? m.n_face_list : m.nf;
   const bool side = no > 0;
   if (side) {
     CK(cudaEventRecord(x->ev_fork, s));

@@ -1,6 +1,7 @@
 // C ABI, device context and residual pipeline of libfcfd_b200.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -243,6 +244,14 @@ int fcfd_ctx_create(const fcfd_mesh *mp, const fcfd_case *csp, int device, fcfd_
     }
   }
   x->bface.upload(bface);
+  {
+    // main face launch order: interior faces, then each BC region's faces
+    // (face order within a group), so that a warp's faces take one branch
+    std::vector<int32_t> order(nf);
+    for (int f = 0; f < nf; ++f) order[f] = f;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return m.f_bc[a] < m.f_bc[b]; });
+    x->face_order.upload(order);
+  }
   x->color_cells.upload(m.color_cells);
   x->color_index = m.color_index;
   {
@@ -305,6 +314,7 @@ int fcfd_ctx_create(const fcfd_mesh *mp, const fcfd_case *csp, int device, fcfd_
   dm.st_recip = x->st_recip.p; dm.st_mirror = x->st_mirror.p; dm.c_vol = x->c_vol.p;
   dm.f_wall = x->f_wall.p; dm.f_diss = x->f_diss.p;
   dm.outlet_faces = x->outlet.p; dm.n_outlet = x->n_outlet;
+  dm.face_list = x->face_order.p; dm.n_face_list = nf;
   rans_setup(x.get());  // k-omega BC values and buffers (turbulent cases only)
   CK(cudaDeviceSynchronize());
   *out = x.release();

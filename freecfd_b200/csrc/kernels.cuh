@@ -173,12 +173,19 @@ struct DevMesh {
   const int *outlet_faces;                 // outlet boundary faces [n_outlet]
   const double *f_wall, *f_diss;           // [nf] wall distance, dissipation factor (Steger-Warming only)
   int n_outlet;
+  // Faces of the viscous or partitioned main face-flux launch, thread i
+  // taking face_list[i]: the whole mesh grouped by kind (interior faces, then
+  // each BC region's, each group in face order) so that a warp's faces take
+  // the same branch, or one rank's faces of a domain decomposition, grouped
+  // the same way.
+  const int *face_list = nullptr;
+  int n_face_list = 0;
   // Partitioned evaluation (one rank of a domain decomposition; null lists =
-  // the whole mesh): cells whose gradient and limiter are formed, faces whose
-  // flux is formed, indices into outlet_faces, ghost indices to update, and
-  // the owned cells [own_lo, own_hi) (extrema and gather).
-  const int *part_cells = nullptr, *part_faces = nullptr, *part_outlet = nullptr, *part_ghosts = nullptr;
-  int n_part_cells = 0, n_part_faces = 0, n_part_outlet = 0, n_part_ghosts = 0;
+  // the whole mesh): cells whose gradient and limiter are formed, indices
+  // into outlet_faces, ghost indices to update, and the owned cells
+  // [own_lo, own_hi) (extrema and gather).
+  const int *part_cells = nullptr, *part_outlet = nullptr, *part_ghosts = nullptr;
+  int n_part_cells = 0, n_part_outlet = 0, n_part_ghosts = 0;
   int own_lo = 0, own_hi = 0;
 };
 // thread counts of the ghost and gather kernels (partition-aware)
@@ -1180,14 +1187,26 @@ __global__ void __launch_bounds__(128) k_face_flux(DevCase cs, DevMesh m, const 
                                                    S *__restrict__ wl_out, int *err) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int nf = m.nf;
-  // PART: one rank's faces of a domain decomposition
+  // main launch: face_list when viscous (faces grouped by kind: an interior
+  // viscous face costs several boundary faces, so mixed warps would run both
+  // paths) or partitioned, else face order (inviscid faces are cheap enough
+  // that the coalesced face arrays matter more); outlet launch: all outlet
+  // faces, or (PART) one rank's
   int f;
-  if constexpr (PART) {
-    if (i >= (OUTLET ? m.n_part_outlet : m.n_part_faces)) return;
-    f = OUTLET ? m.outlet_faces[m.part_outlet[i]] : m.part_faces[i];
+  if constexpr (OUTLET) {
+    if constexpr (PART) {
+      if (i >= m.n_part_outlet) return;
+      f = m.outlet_faces[m.part_outlet[i]];
+    } else {
+      if (i >= m.n_outlet) return;
+      f = m.outlet_faces[i];
+    }
+  } else if constexpr (VISCOUS || PART) {
+    if (i >= m.n_face_list) return;
+    f = m.face_list[i];
   } else {
-    if (i >= (OUTLET ? m.n_outlet : nf)) return;
-    f = OUTLET ? m.outlet_faces[i] : i;
+    if (i >= nf) return;
+    f = i;
   }
   const int pa = m.f_parent[f], nb = m.f_neighbor[f], b = m.f_bc[f];
   const double n[3] = {m.f_n[f], m.f_n[nf + f], m.f_n[2 * nf + f]};

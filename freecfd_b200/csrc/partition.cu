@@ -98,6 +98,9 @@ PartSets partition_sets(const fcfd_mesh &m, const fcfd_case &c, int lo, int hi) 
   }
   for (int t = 0; t < nb; ++t)
     if (cur[m.f_parent[bface[t]]]) P.ghosts.push_back(t);
+  // faces grouped by kind like the whole mesh's face list (interior, then
+  // each BC region), face order within a group
+  std::stable_sort(P.faces.begin(), P.faces.end(), [&](int a, int b) { return m.f_bc[a] < m.f_bc[b]; });
   return P;
 }
 
@@ -163,7 +166,7 @@ extern "C" int fcfd_ctx_set_partition(fcfd_ctx *x, int lo, int hi) {
     x->part_ghosts.upload(P.ghosts.empty() ? std::vector<int>{0} : P.ghosts);
     DevMesh d = x->dm;
     d.part_cells = x->part_cells.p; d.n_part_cells = (int)P.grad.size();
-    d.part_faces = x->part_faces.p; d.n_part_faces = (int)P.faces.size();
+    d.face_list = x->part_faces.p; d.n_face_list = (int)P.faces.size();
     d.part_outlet = x->part_outlet.p; d.n_part_outlet = (int)P.outlet_idx.size();
     d.part_ghosts = x->part_ghosts.p; d.n_part_ghosts = (int)P.ghosts.size();
     d.own_lo = lo; d.own_hi = hi;
