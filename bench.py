@@ -461,7 +461,7 @@ def run_newton(fb, cs, mesh, case, dev, dist, reference_state=True):
 # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) from
 # ncu captures of the same kernels; the capture commands are in profiles/.
 NCU_TRAFFIC = {
-    ("cylinder", "grad_limiter"): 17762816, ("cylinder", "face_flux"): 22143744,
+    ("cylinder", "grad_limiter"): 17766656, ("cylinder", "face_flux"): 22753280,
     ("hypersonic", "grad_limiter"): 191846912, ("hypersonic", "face_flux"): 141227264,
 }
 
