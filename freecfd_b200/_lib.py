@@ -28,6 +28,7 @@ EXPORTED = [
     "fcfd_time_residual", "fcfd_point_flux", "fcfd_jvp", "fcfd_vjp", "fcfd_drag", "fcfd_rans_residual", "fcfd_rans_bcs", "fcfd_time_rans", "fcfd_newton_solve", "fcfd_local_dt_cflmax_noalloc",
     "fcfd_run", "fcfd_restart_write", "fcfd_restart_read", "fcfd_mesh_from_tecplot", "fcfd_rans_jvp",
     "fcfd_partition_sets", "fcfd_ctx_set_partition", "fcfd_partition_extrema", "fcfd_partition_residual",
+    "fcfd_ctx_stream",
 ]
 
 
@@ -128,8 +129,9 @@ def _load():
                                   ctypes.c_double, ctypes.c_double, dp, dp]
     L.fcfd_partition_sets.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int, ip, ip, ip, ip]
     L.fcfd_ctx_set_partition.argtypes = [vp, ctypes.c_int, ctypes.c_int]
-    L.fcfd_partition_extrema.argtypes = [vp, vp, dp, ctypes.c_int]
-    L.fcfd_partition_residual.argtypes = [vp, dp, vp, ctypes.c_int]
+    L.fcfd_partition_extrema.argtypes = [vp, vp, vp, ctypes.c_int]
+    L.fcfd_partition_residual.argtypes = [vp, vp, vp, ctypes.c_int]
+    L.fcfd_ctx_stream.argtypes = [vp, ctypes.POINTER(vp)]
     for name in EXPORTED:
         getattr(L, name)
     return L

@@ -117,6 +117,23 @@ double host_okey_inv(unsigned long long k) {
   return x;
 }
 
+// extrema slots: arm (even: max, key 0; odd: min, all ones), read out as
+// doubles (+-inf where no cell reached the slot), set from doubles
+__global__ void k_ext_arm(unsigned long long *key) {
+  const int t = threadIdx.x;
+  if (t < 8) key[t] = (t & 1) ? ~0ull : 0ull;
+}
+__global__ void k_ext_out(const unsigned long long *__restrict__ key, double *__restrict__ ext) {
+  const int t = threadIdx.x;
+  if (t >= 8) return;
+  const unsigned long long k = key[t], armed = (t & 1) ? ~0ull : 0ull;
+  ext[t] = (k == armed) ? ((t & 1) ? INFINITY : -INFINITY) : okey_inv(k);
+}
+__global__ void k_ext_in(const double *__restrict__ ext, unsigned long long *__restrict__ key) {
+  const int t = threadIdx.x;
+  if (t < 8) key[t] = okey(ext[t]);
+}
+
 template <class F>
 int api(F &&body) {
   try {
@@ -175,12 +192,23 @@ extern "C" int fcfd_ctx_set_partition(fcfd_ctx *x, int lo, int hi) {
   });
 }
 
+// The stream a context's work runs on, for callers that enqueue their own
+// work around it (a halo exchange, the extrema all-reduce).
+extern "C" int fcfd_ctx_stream(const fcfd_ctx *x, void **stream) {
+  return api([&] {
+    if (!x || !stream) throw Error(FCFD_ERR_INPUT, "null argument");
+    *stream = (void *)x->stream;
+  });
+}
+
 // Phase 1 of a partitioned residual: load W (all rows; only owned and halo
 // rows need be current), update the partition's ghosts and reduce the VK
 // extrema over the owned cells.  ext[0..8): max p, min p, max u, min u,
 // max v, min v, max p and min p over cells below the last one (+-inf where
 // the owned range has no such cell); combine across ranks with max (even
-// slots) and min (odd slots).
+// slots) and min (odd slots).  With FCFD_DEVICE_PTRS, W and ext are device
+// pointers and the call only enqueues work on the context's stream (BC
+// errors are reported by phase 2).
 extern "C" int fcfd_partition_extrema(fcfd_ctx *x, const double *W, double ext[8], int flags) {
   return api([&] {
     if (!x || !W || !ext) throw Error(FCFD_ERR_INPUT, "null argument");
@@ -194,12 +222,17 @@ extern "C" int fcfd_partition_extrema(fcfd_ctx *x, const double *W, double ext[8
       win = x->Win.p;
     }
     k_aos_to_soa<double><<<(m.nc + 255) / 256, 256, 0, s>>>(win, x->p64.W.p, m.nc, m.nt);
-    const unsigned long long armed[8] = {0ull, ~0ull, 0ull, ~0ull, 0ull, ~0ull, 0ull, ~0ull};
-    CK(cudaMemcpyAsync(x->ext.p, armed, sizeof(armed), cudaMemcpyHostToDevice, s));
+    k_ext_arm<<<1, 32, 0, s>>>(x->ext.p);
     const bool need_ext = x->cs.limiter == 1 && x->cs.order != 1;
     const int tb = 256;
     const int ng = (n_ghost_threads(m) + tb - 1) / tb + (need_ext ? kExtremaBlocks : 0);
     if (ng > 0) k_ghost_minmax<double><<<ng, tb, 0, s>>>(x->cs, m, x->p64.W.p, need_ext ? x->ext.p : nullptr, x->err.p);
+    if (flags & FCFD_DEVICE_PTRS) {
+      k_ext_out<<<1, 32, 0, s>>>(x->ext.p, ext);
+      CK(cudaGetLastError());
+      return;
+    }
+    const unsigned long long armed[8] = {0ull, ~0ull, 0ull, ~0ull, 0ull, ~0ull, 0ull, ~0ull};
     unsigned long long k[8];
     CK(cudaMemcpyAsync(k, x->ext.p, sizeof(k), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
@@ -211,6 +244,7 @@ extern "C" int fcfd_partition_extrema(fcfd_ctx *x, const double *W, double ext[8
 // Phase 2: with the extrema combined over all ranks, gradient + limiter,
 // face fluxes and the gather of the owned rows (R [nc][5]; only rows
 // [lo, hi) are written).  Uses the state and ghosts of the last phase 1.
+// With FCFD_DEVICE_PTRS, ext and R are device pointers.
 extern "C" int fcfd_partition_residual(fcfd_ctx *x, const double ext[8], double *R, int flags) {
   return api([&] {
     if (!x || !ext || !R) throw Error(FCFD_ERR_INPUT, "null argument");
@@ -218,13 +252,17 @@ extern "C" int fcfd_partition_residual(fcfd_ctx *x, const double ext[8], double 
     CK(cudaSetDevice(x->device));
     const DevMesh &m = x->dmp;
     cudaStream_t s = x->stream;
-    unsigned long long k[8];
-    for (int i = 0; i < 8; ++i) k[i] = host_okey(ext[i]);
-    CK(cudaMemcpyAsync(x->ext.p, k, sizeof(k), cudaMemcpyHostToDevice, s));
+    const bool dev = flags & FCFD_DEVICE_PTRS;
+    if (dev) {
+      k_ext_in<<<1, 32, 0, s>>>(ext, x->ext.p);
+    } else {
+      unsigned long long k[8];
+      for (int i = 0; i < 8; ++i) k[i] = host_okey(ext[i]);
+      CK(cudaMemcpyAsync(x->ext.p, k, sizeof(k), cudaMemcpyHostToDevice, s));
+    }
     Pipe<double> &P = x->p64;
     launch_grad_limiter<double, true>(x->cs, m, P.W.p, x->ext.p, nullptr, P.G.p, P.Lm.p, s);
     launch_faces<double, true>(x, P, (const double *)nullptr, x->mdot.p, x->wl.p, s);
-    const bool dev = flags & FCFD_DEVICE_PTRS;
     double *rout = dev ? R : x->Rtmp.p;
     const int tb = 256;
     k_gather<double, true><<<(5 * n_owned(m) + tb - 1) / tb, tb, 0, s>>>(m, P.D.p, rout, x->ext.p, x->argx.p);

@@ -90,38 +90,47 @@ class HaloExchange:
 
 def combine_extrema(ext, device=None):
     """The VK extrema over all ranks: max of the even slots, min of the odd
-    ones (one all-reduce, odd slots negated)."""
+    ones (one all-reduce, odd slots negated).  A torch tensor is combined in
+    place on the current stream; host values come back as numpy."""
     import torch
     import torch.distributed as dist
+    inplace = isinstance(ext, torch.Tensor)
     if not (dist.is_available() and dist.is_initialized()):
-        return np.asarray(ext, dtype=np.float64)
-    t = torch.as_tensor(np.asarray(ext, dtype=np.float64).copy(), device=device)
+        return ext if inplace else np.asarray(ext, dtype=np.float64)
+    t = ext if inplace else torch.as_tensor(np.asarray(ext, dtype=np.float64).copy(), device=device)
     t[1::2] = -t[1::2]
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     t[1::2] = -t[1::2]
-    return t.cpu().numpy()
+    return t if inplace else t.cpu().numpy()
 
 
 class PartitionedResidual:
     """R(W) of one rank: halo exchange, owned extrema, all-reduce, owned rows.
 
-    ``W`` and ``R`` are [nc][5] float64 arrays on the rank's device (torch
-    tensors); only the owned rows of R are written and only owned + halo
-    rows of W are read."""
+    ``W`` and ``R`` are [nc][5] float64 CUDA tensors on the rank's device;
+    only the owned rows of R are written and only owned + halo rows of W are
+    read.  Everything is enqueued on the library context's stream (the
+    exchange's packing, the NCCL point-to-point and all-reduce, the two
+    library phases), so a step has one host synchronisation: the error check
+    at the end of phase 2."""
 
     def __init__(self, ns, plan: HaloPlan, rank: int, W):
+        import torch
         self.ns, self.plan, self.rank = ns, plan, rank
         self.lo, self.hi = plan.ranges[rank]
         ns.set_partition(self.lo, self.hi)
         self.ex = HaloExchange(plan, rank, W)
         self.W = W
+        self.ext = W.new_empty(8)
+        self.stream = torch.cuda.ExternalStream(ns.stream_handle(), device=W.device)
 
     def __call__(self, R):
-        self.ex.exchange()
-        if self.W.is_cuda:
-            # the unpacking ran on torch's stream; the library reads W on its own
-            import torch
-            torch.cuda.current_stream(self.W.device).synchronize()
-        ext = self.ns.partition_extrema(self.W)
-        ext = combine_extrema(ext, self.W.device)
-        return self.ns.partition_residual(ext, R)
+        import torch
+        # W may have been written on torch's stream (a state update)
+        self.stream.wait_stream(torch.cuda.current_stream(self.W.device))
+        with torch.cuda.stream(self.stream):
+            self.ex.exchange()
+            self.ns.partition_extrema(self.W, out=self.ext)
+            combine_extrema(self.ext)
+            self.ns.partition_residual(self.ext, R)
+        return R

@@ -144,24 +144,41 @@ class NavierStokes:
         check(lib.fcfd_ctx_set_partition(self.h, int(lo), int(hi)))
         self.partition = (int(lo), int(hi)) if hi > lo else None
 
-    def partition_extrema(self, W):
+    def partition_extrema(self, W, out=None):
         """Phase 1 of the partitioned residual: load W [nc][5] (owned and halo
         rows current), update this part's ghosts; returns the 8 VK extrema of
-        the owned cells (combine over ranks: max of even, min of odd slots)."""
+        the owned cells (combine over ranks: max of even, min of odd slots).
+        For a CUDA tensor W the extrema are a CUDA tensor (``out``, 8
+        doubles, if given) filled on the context's stream without a host
+        synchronisation."""
         if isinstance(W, np.ndarray):
             W = np.ascontiguousarray(W, dtype=np.float64)
+            ext = np.empty(8)
+        else:
+            ext = out if out is not None else W.new_empty(8)
         pw, fw = _ptr(W)
-        ext = np.empty(8)
-        check(lib.fcfd_partition_extrema(self.h, pw, _d(ext), fw))
+        pe, fe = _ptr(ext)
+        check(lib.fcfd_partition_extrema(self.h, pw, pe, fw))
         return ext
 
     def partition_residual(self, ext, out):
         """Phase 2: rows [lo, hi) of R (numpy [nc][5] or CUDA tensor) from the
-        extrema combined over all ranks."""
-        ext = np.ascontiguousarray(ext, dtype=np.float64)
+        extrema combined over all ranks (a CUDA tensor with a CUDA R)."""
+        if isinstance(out, np.ndarray):
+            ext = np.ascontiguousarray(np.asarray(ext, dtype=np.float64))
+        elif isinstance(ext, np.ndarray):
+            import torch
+            ext = torch.as_tensor(ext, device=out.device)
+        pe, _ = _ptr(ext)
         pr, fr = _ptr(out)
-        check(lib.fcfd_partition_residual(self.h, _d(ext), pr, fr))
+        check(lib.fcfd_partition_residual(self.h, pe, pr, fr))
         return out
+
+    def stream_handle(self) -> int:
+        """The cudaStream_t this context enqueues its work on (as an int)."""
+        s = ctypes.c_void_p()
+        check(lib.fcfd_ctx_stream(self.h, ctypes.byref(s)))
+        return int(s.value or 0)
 
     def jvp(self, W, V, with_residual: bool = False, fp32: bool = False):
         """Directional derivative (dR/dW).V of the residual (forward tangent);

@@ -193,12 +193,18 @@ int fcfd_rans_jvp(fcfd_ctx *ctx, const double *W, const double *K, const double 
  * max v, min v, max p and min p below the last cell; -inf/+inf where empty),
  * to be combined over the ranks with max (even slots) and min (odd slots).
  * fcfd_partition_residual (phase 2) takes the combined ext and writes rows
- * [lo, hi) of R [nc][5]: bit for bit the single-domain residual's rows. */
+ * [lo, hi) of R [nc][5]: bit for bit the single-domain residual's rows.
+ * With FCFD_DEVICE_PTRS, W, ext and R are device pointers; phase 1 then only
+ * enqueues work on the context's stream (fcfd_ctx_stream), so the caller can
+ * all-reduce ext on that stream and call phase 2 without a host round trip
+ * (phase 2 synchronises once and reports BC errors of both phases). */
 int fcfd_partition_sets(const fcfd_mesh *mesh, const fcfd_case *cs, int lo, int hi, int counts[4], int *grad_cells,
                         int *faces, int *halo);
 int fcfd_ctx_set_partition(fcfd_ctx *ctx, int lo, int hi);
 int fcfd_partition_extrema(fcfd_ctx *ctx, const double *W, double ext[8], int flags);
 int fcfd_partition_residual(fcfd_ctx *ctx, const double ext[8], double *R, int flags);
+/* The CUDA stream (cudaStream_t) the context's work is enqueued on. */
+int fcfd_ctx_stream(const fcfd_ctx *ctx, void **stream);
 
 /* Fixed BC values of the RANS variables, per BC region: kw_fixed, k, omega,
  * mut_fixed, mu_t (5 doubles each; out_len >= 5 * number of regions). */

@@ -36,8 +36,14 @@ def _partitioned(fb, case, cs, m, nparts, exact=False, device=False):
             import torch
             W = torch.as_tensor(W, device="cuda")
         parts.append((ns, W, lo, hi))
-    exts = np.array([ns.partition_extrema(W) for ns, W, _, _ in parts])
-    ext = np.where(np.arange(8) % 2 == 0, exts.max(axis=0), exts.min(axis=0))
+    if device:
+        import torch
+        e = torch.stack([ns.partition_extrema(W) for ns, W, _, _ in parts])
+        torch.cuda.synchronize()
+        ext = torch.where(torch.arange(8, device="cuda") % 2 == 0, e.max(dim=0).values, e.min(dim=0).values)
+    else:
+        exts = np.array([ns.partition_extrema(W) for ns, W, _, _ in parts])
+        ext = np.where(np.arange(8) % 2 == 0, exts.max(axis=0), exts.min(axis=0))
     R = np.full((m.nc, 5), np.nan)
     for ns, W, lo, hi in parts:
         if device:
@@ -82,6 +88,27 @@ def test_partitioned_residual_device_pointers(fb):
     ref = fb.NavierStokes(m, cs, 0).residual(case.state)
     R = _partitioned(fb, case, cs, m, 3, device=True)
     assert np.array_equal(R.view(np.uint64), ref.view(np.uint64))
+
+
+@pytest.mark.gpu
+def test_partitioned_residual_one_stream(fb):
+    """PartitionedResidual (one rank, no process group): exchange, extrema and
+    both phases enqueued on the context's stream; equals the single-domain
+    residual, also after the state changes."""
+    import torch
+    from freecfd_b200.partition import PartitionedResidual
+    case = SMALL["cylinder"]()
+    cs, m = _setup(fb, case)
+    ns0 = fb.NavierStokes(m, cs, 0)
+    plan = HaloPlan(m, cs, 1)
+    W = torch.as_tensor(case.state, device="cuda")
+    R = torch.full_like(W, float("nan"))
+    res = PartitionedResidual(fb.NavierStokes(m, cs, 0), plan, 0, W)
+    for k in range(3):
+        Wk = case.state * (1 + 1e-3 * k)
+        W.copy_(torch.as_tensor(Wk))
+        res(R)
+        assert np.array_equal(R.cpu().numpy(), ns0.residual(Wk))
 
 
 @pytest.mark.gpu
