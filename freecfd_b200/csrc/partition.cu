@@ -176,6 +176,8 @@ extern "C" int fcfd_ctx_set_partition(fcfd_ctx *x, int lo, int hi) {
       x->dmp = DevMesh{};
       return;
     }
+    if (x->case_ptr->turbulent)
+      throw Error(FCFD_ERR_UNSUPPORTED, "the partitioned residual covers laminar and Euler cases (no k-omega terms)");
     const PartSets P = partition_sets(*x->mesh, *x->case_ptr, lo, hi);
     x->part_cells.upload(P.grad);
     x->part_faces.upload(P.faces);

@@ -187,7 +187,8 @@ int fcfd_rans_jvp(fcfd_ctx *ctx, const double *W, const double *K, const double 
  * be current before phase 1; ascending global ids).  Gradients are
  * recomputed on the halo, so only states are exchanged.
  *
- * fcfd_ctx_set_partition selects the range on a context (lo = hi = 0: none).
+ * fcfd_ctx_set_partition selects the range on a context (lo = hi = 0: none;
+ * FCFD_ERR_UNSUPPORTED for k-omega cases).
  * fcfd_partition_extrema (phase 1) loads W [nc][5] and returns ext[8]: the
  * VK limiter's extrema over the owned cells (max p, min p, max u, min u,
  * max v, min v, max p and min p below the last cell; -inf/+inf where empty),

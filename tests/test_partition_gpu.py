@@ -122,6 +122,12 @@ def test_partition_errors(fb):
         ns.set_partition(0, m.nc + 1)
     ns.set_partition(0, m.nc // 2)
     ns.set_partition(0, 0)
+    from freecfd_b200 import cases
+    plate = cases.plate_case(ni=8, nj=4, nk=2)  # k-omega deck
+    pcs, pm = _setup(fb, plate)
+    with pytest.raises(fb.FcfdError) as e:
+        fb.NavierStokes(pm, pcs, 0).set_partition(0, pm.nc // 2)
+    assert e.value.code == 7
     # the whole-mesh residual is unaffected by a partition set and cleared
     R = ns.residual(case.state)
     ref = fb.NavierStokes(m, cs, 0).residual(case.state)
