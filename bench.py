@@ -470,6 +470,7 @@ def run_newton(fb, cs, mesh, case, dev, dist, reference_state=True):
 NCU_TRAFFIC = {
     ("cylinder", "grad_limiter"): 17766656, ("cylinder", "face_flux"): 22753280,
     ("hypersonic", "grad_limiter"): 191846912, ("hypersonic", "face_flux"): 141227264,
+    ("plate", "grad_limiter"): 159035648, ("plate", "face_flux"): 320413440,
 }
 
 
