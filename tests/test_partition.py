@@ -26,11 +26,26 @@ def _mesh(fb, family, **kw):
     return case, cs, fb.Mesh(case.mesh, cs)
 
 
-@pytest.mark.parametrize("family", sorted(ALL))
+def _tecplot_mesh(fb, family):
+    import os
+    import tempfile
+
+    from freecfd_b200 import cases
+    case = ALL[family]()
+    d = tempfile.mkdtemp(prefix="fcfd_partt_")
+    path = cases.write_tecplot(case.mesh, os.path.join(d, "grid.dat"), order="shuffled", seed=7)
+    cs = fb.Case(case.write_deck(d))
+    return case, cs, fb.Mesh(None, cs, tecplot=path)
+
+
+@pytest.mark.parametrize("family", sorted(ALL) + ["tecplot_wedge", "tecplot_hypersonic"])
 @pytest.mark.parametrize("nparts", [2, 3])
 def test_partition_sets_are_closed(family, nparts, fb):
     from freecfd_b200.partition import block_ranges, partition_sets
-    case, cs, m = _mesh(fb, family)
+    if family.startswith("tecplot_"):
+        case, cs, m = _tecplot_mesh(fb, family[len("tecplot_"):])  # faces in shuffled order
+    else:
+        case, cs, m = _mesh(fb, family)
     con = m.connectivity()
     nc, parent, nbr, fbc = m.nc, con["face_parent"], con["face_neighbor"], con["face_bc"]
     cfi, cfl = con["cell_face_index"], con["cell_faces"]
