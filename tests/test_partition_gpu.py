@@ -132,6 +132,35 @@ def test_partitioned_residual_one_stream(fb):
 
 
 @pytest.mark.gpu
+def test_partitioned_residual_nccl_process_group(fb):
+    """The same step inside an NCCL process group (one rank): the extrema
+    all-reduce runs on the library's stream through NCCL; the halo exchange
+    has no peers.  Owned rows equal the single-domain residual."""
+    import socket
+
+    import torch
+    import torch.distributed as dist
+    from freecfd_b200.partition import PartitionedResidual
+    with socket.socket() as so:
+        so.bind(("127.0.0.1", 0))
+        port = so.getsockname()[1]
+    dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1)
+    try:
+        case = SMALL["wedge"]()
+        cs, m = _setup(fb, case)
+        ref = fb.NavierStokes(m, cs, 0).residual(case.state)
+        W = torch.as_tensor(case.state, device="cuda")
+        R = torch.full_like(W, float("nan"))
+        res = PartitionedResidual(fb.NavierStokes(m, cs, 0), HaloPlan(m, cs, 1), 0, W)
+        for _ in range(2):
+            res(R)
+        assert np.array_equal(R.cpu().numpy(), ref)
+        del res
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.gpu
 def test_partition_errors(fb):
     case = SMALL["wedge"]()
     cs, m = _setup(fb, case)
