@@ -64,6 +64,7 @@ def lib():
         L.orc_rans_residual.restype = ctypes.c_int
         L.orc_rans_bcs.argtypes = [vp, dp]
         L.orc_case_summary.argtypes = [vp, dp, ip]
+        L.orc_time_terms.argtypes = [vp, dp, dp, dp]
         _lib = L
     return _lib
 
@@ -227,6 +228,14 @@ class Oracle:
         dt = np.empty(self.nc)
         lib().orc_local_dt(self.h, _d(W), float(cfl), int(mode), _d(dt))
         return dt
+
+    def time_terms(self, W, dt):
+        """Diagonal blocks P(W_c) V_c / dt_c (nc, 5, 5) of NavierStokes::time_terms."""
+        W = np.ascontiguousarray(W, dtype=np.float64).reshape(self.nc, 5)
+        dt = np.ascontiguousarray(dt, dtype=np.float64).reshape(self.nc)
+        out = np.empty((self.nc, 5, 5))
+        lib().orc_time_terms(self.h, _d(W), _d(dt), _d(out))
+        return out
 
     def case_summary(self):
         d = np.empty(13)

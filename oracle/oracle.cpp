@@ -23,14 +23,17 @@
 //                                 ns_vanleer.cc, ns_convective_face_flux.cc,
 //                                 ns_diffusive_face_flux.cc, ns_set_bcs.cc
 //   time_step.cc                  update_time_step 143-224
+//   navier_stokes/ns_time_terms.cc cons2prim 26-56, time_terms 107-186
 //
-// Parity status: the reference cannot be compiled here (MPI, PETSc, ParMETIS,
-// CGNS are absent) and two of its sources are missing, so there is no
-// reference binary to run against.  This restatement is pinned by the
-// known-answer properties the reference itself relies on (linear-field LSQ
-// exactness, uniform-flow preservation, flux consistency, conservation); see
-// tests/test_oracle.py.  NavierStokes::update_boundaries is declared and called
-// by the reference but its source file is absent; update_boundaries() below is
+// Parity status: pinned.  The reference's own sources compile here against
+// single-process stand-ins for MPI, PETSc, ParMETIS and CGNS (oracle/ref,
+// `make ref`), and tests/test_reference_pin.py requires this restatement to
+// reproduce that compiled reference's doubles bit for bit (mesh, geometry,
+// LSQ weights, ghosts, gradients, limiters, residual, mdot, k-omega terms,
+// time terms, time step) over every mesh family, flux and limiter; the
+// golden vectors in tests/golden/ are the compiled reference's outputs.
+// NavierStokes::update_boundaries is declared and called by the reference but
+// its source file is absent; update_boundaries() below is
 // a documented reconstruction (first-order ghost update, as at initialise).
 #include <algorithm>
 #include <cmath>
@@ -2493,6 +2496,40 @@ int orc_loads(void *h, const double *W, const double *dW, double hstep, double *
 // Local time step (mode 0: CFL_LOCAL; mode 1: CFL_MAX global minimum).
 void orc_local_dt(void *h, const double *W, double cfl, int mode, double *dt) {
   local_dt(static_cast<Handle *>(h)->O, W, cfl, mode, dt);
+}
+
+// NavierStokes::cons2prim (ns_time_terms.cc:26-56) and the dt part of
+// NavierStokes::time_terms (ns_time_terms.cc:140-158, ps_step_max = 1): the
+// diagonal block P[i][j] * volume / dt of cell c, blocks[c][5][5], for the
+// state W[nc][5] and local time steps dt[nc].  rho = EOS(p, T) as
+// update_variables (ns.cc:357) leaves it; Cp is the ideal-gas value.
+void orc_time_terms(void *h, const double *W, const double *dt, double *blocks) {
+  Oracle &O = static_cast<Handle *>(h)->O;
+  const Grid &g = O.grid;
+  const Material &m = O.material;
+  for (int c = 0; c < g.cellCount; ++c) {
+    const double p = W[5 * c], T = W[5 * c + 4];
+    const Vec3 V(W[5 * c + 1], W[5 * c + 2], W[5 * c + 3]);
+    const double rho = m.rho(p, T);
+    const double pressure = p + m.Pref;
+    const double temperature = T + m.Tref;
+    const double drho_dT = -1. * rho / temperature;
+    const double drho_dp = rho / pressure;
+    const double c_p = m.Cp();
+    const double H = c_p * temperature + 0.5 * (V[0] * V[0] + V[1] * V[1] + V[2] * V[2]);
+    double P[5][5] = {{0.}};
+    P[0][0] = drho_dp; P[0][4] = drho_dT;
+    P[1][0] = drho_dp * V[0]; P[1][1] = rho; P[1][4] = drho_dT * V[0];
+    P[2][0] = drho_dp * V[1]; P[2][2] = rho; P[2][4] = drho_dT * V[1];
+    P[3][0] = drho_dp * V[2]; P[3][3] = rho; P[3][4] = drho_dT * V[2];
+    P[4][0] = drho_dp * H - 1.;
+    P[4][1] = rho * V[0];
+    P[4][2] = rho * V[1];
+    P[4][3] = rho * V[2];
+    P[4][4] = drho_dT * H + rho * c_p;
+    for (int i = 0; i < 5; ++i)
+      for (int j = 0; j < 5; ++j) blocks[25 * (size_t)c + 5 * i + j] = P[i][j] * g.cell[c].volume / dt[c];
+  }
 }
 
 // Parsed case summary (for deck-parser parity with the product):

@@ -1,9 +1,11 @@
 """Pins of the CPU oracle.
 
-The reference cannot be compiled here (it needs MPI, PETSc, ParMETIS and
-CGNS; two of its sources are missing) and ships no tests or golden outputs.
-The oracle is pinned instead by the known-answer behaviour the reference
-itself relies on and by identities of the discretisation:
+The reference ships no tests or golden outputs, and its build needs MPI,
+PETSc, ParMETIS and CGNS.  Its path is nevertheless compiled here from its
+own sources against single-process stand-ins for those libraries (oracle/ref,
+`make -C oracle ref`), so the oracle is pinned against the reference's own
+doubles, and in addition by the known-answer behaviour the reference relies
+on and by identities of the discretisation:
   * LSQ gradient exactness for a linear field (the reference's gradient-test
     IC mode, ns.cc:161-185) — checked through the stored gradient weights;
   * flux consistency F(U,U) = physical flux (ns_roe.cc, ns_ausm_plus_up.cc,
@@ -12,9 +14,11 @@ itself relies on and by identities of the discretisation:
     rounding of its cancelling face fluxes;
   * a closed symmetry box at rest has zero residual;
   * conservation: interior faces cancel in the sum of residuals;
-  * committed golden vectors (tests/golden/) generated by
-    tests/golden/make_golden.py from this oracle, so that any later change
-    to the restatement shows up.
+  * committed golden vectors (tests/golden/) that tests/golden/make_golden.py
+    produced by running the reference itself (its own sources compiled into
+    oracle/_ref/freecfd_ref); tests/test_reference_pin.py compares the oracle
+    with that compiled reference directly, over every mesh family, flux,
+    limiter and the k-omega terms.
 """
 import os
 
@@ -157,20 +161,31 @@ def test_complex_step_other_fluxes(family, flux, oracle_mod):
     assert (np.abs(jv - fd)[:, cols].max(axis=0) / scale).max() < 1e-5
 
 
-def test_golden_vectors(oracle_mod):
-    path = os.path.join(ROOT, "tests", "golden", "wedge_12x6.npz")
-    gold = np.load(path)
-    case = cases.wedge_case(ni=12, nj=6)
-    o = oracle_mod.Oracle(case)
+GOLDEN = {
+    "wedge_12x6": lambda: cases.wedge_case(ni=12, nj=6),
+    "hypersonic_16x8": lambda: cases.hypersonic_case(ntheta=16, nr=8),
+    "cylinder_16x8": lambda: cases.cylinder_case(ntheta=16, nr=8),
+    "box_tet_4x3x2": lambda: cases.box_case("tet", nx=4, ny=3, nz=2),
+    "plate_komega_8x4x2": lambda: cases.plate_case(ni=8, nj=4, nk=2),
+}
+
+
+@pytest.mark.parametrize("name", sorted(GOLDEN))
+def test_golden_vectors(name, oracle_mod):
+    """The oracle reproduces, bit for bit, the doubles the reference itself
+    computed (tests/golden/make_golden.py runs the compiled reference)."""
+    gold = np.load(os.path.join(ROOT, "tests", "golden", name + ".npz"))
+    o = oracle_mod.Oracle(GOLDEN[name]())
+    if "RK" in gold.files:
+        R, RK = o.rans_residual(gold["W"], gold["K"])
+        assert np.array_equal(R, gold["R"])
+        assert np.array_equal(RK, gold["RK"])
+        return
     out = o.residual(gold["W"], full=True)
-    assert np.array_equal(out["R"], gold["R"])
-    assert np.array_equal(out["limiter"], gold["limiter"])
-    path = os.path.join(ROOT, "tests", "golden", "hypersonic_16x8.npz")
-    gold = np.load(path)
-    case = cases.hypersonic_case(ntheta=16, nr=8)
-    o = oracle_mod.Oracle(case)
-    out = o.residual(gold["W"], full=True)
-    assert np.array_equal(out["R"], gold["R"])
+    for k in ("R", "limiter", "grads", "mdot", "ghost"):
+        assert np.array_equal(out[k].view(np.uint64), gold[k].view(np.uint64)), k
+    if "time_terms" in gold.files:
+        assert np.array_equal(o.time_terms(gold["W"], gold["dt"]) + 0.0, gold["time_terms"] + 0.0)
 
 
 @pytest.mark.parametrize("flux", ["AUSM+up", "vanLeer"])
