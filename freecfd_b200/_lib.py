@@ -28,7 +28,7 @@ EXPORTED = [
     "fcfd_time_residual", "fcfd_point_flux", "fcfd_jvp", "fcfd_vjp", "fcfd_drag", "fcfd_rans_residual", "fcfd_rans_bcs", "fcfd_time_rans", "fcfd_newton_solve", "fcfd_local_dt_cflmax_noalloc",
     "fcfd_run", "fcfd_restart_write", "fcfd_restart_read", "fcfd_mesh_from_tecplot", "fcfd_rans_jvp",
     "fcfd_partition_sets", "fcfd_ctx_set_partition", "fcfd_partition_extrema", "fcfd_partition_residual",
-    "fcfd_ctx_stream",
+    "fcfd_ctx_stream", "fcfd_diag_blocks",
 ]
 
 
@@ -132,6 +132,7 @@ def _load():
     L.fcfd_partition_extrema.argtypes = [vp, vp, vp, ctypes.c_int]
     L.fcfd_partition_residual.argtypes = [vp, vp, vp, ctypes.c_int]
     L.fcfd_ctx_stream.argtypes = [vp, ctypes.POINTER(vp)]
+    L.fcfd_diag_blocks.argtypes = [vp, dp, dp, dp]
     for name in EXPORTED:
         getattr(L, name)
     return L

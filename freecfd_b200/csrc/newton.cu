@@ -124,15 +124,14 @@ __device__ __forceinline__ void cons2prim(const DevCase &cs, double p, double u,
   P[20] = drho_dp * H - 1.; P[21] = rho * u; P[22] = rho * v; P[23] = rho * w; P[24] = drho_dT * H + rho * c_p;
 }
 
-// Block assembly + inversion (Gauss-Jordan, partial pivoting): Minv_c = (V P/dt - J_cc)^-1
-__global__ void k_block_jacobi(DevCase cs, DevMesh m, const double *__restrict__ Wn, const double *__restrict__ vol,
-                               const double *__restrict__ dt, const double *__restrict__ JL, const double *__restrict__ JR,
-                               double *__restrict__ Minv, int *__restrict__ err, RowScale wref,
-                               double *__restrict__ rowmag) {
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+// Diagonal block of cell c of the implicit operator: V P/dt - J_cc, J_cc the
+// cell's own first-order face Jacobians in ascending face order (minus the
+// parent side's JL, plus the neighbour side's JR).
+__device__ __forceinline__ void diag_block(const DevCase &cs, const DevMesh &m, const double *__restrict__ Wn,
+                                           const double *__restrict__ vol, const double *__restrict__ dt,
+                                           const double *__restrict__ JL, const double *__restrict__ JR, int c,
+                                           double B[25]) {
   const int nc = m.nc, nf = m.nf;
-  if (c >= nc) return;
-  double B[25];
   cons2prim(cs, Wn[c], Wn[nc + c], Wn[2 * nc + c], Wn[3 * nc + c], Wn[4 * nc + c], B);
   const double s = vol[c] / dt[c];
 #pragma unroll
@@ -148,6 +147,30 @@ __global__ void k_block_jacobi(DevCase cs, DevMesh m, const double *__restrict__
       for (int i = 0; i < 25; ++i) B[i] += JR[i * nf + f];
     }
   }
+}
+
+// The assembled diagonal blocks themselves, [nc][25] (fcfd_diag_blocks).
+__global__ void k_diag_blocks(DevCase cs, DevMesh m, const double *__restrict__ Wn, const double *__restrict__ vol,
+                              const double *__restrict__ dt, const double *__restrict__ JL, const double *__restrict__ JR,
+                              double *__restrict__ out) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= m.nc) return;
+  double B[25];
+  diag_block(cs, m, Wn, vol, dt, JL, JR, c, B);
+#pragma unroll
+  for (int i = 0; i < 25; ++i) out[25 * (size_t)c + i] = B[i];
+}
+
+// Block assembly + inversion (Gauss-Jordan, partial pivoting): Minv_c = (V P/dt - J_cc)^-1
+__global__ void k_block_jacobi(DevCase cs, DevMesh m, const double *__restrict__ Wn, const double *__restrict__ vol,
+                               const double *__restrict__ dt, const double *__restrict__ JL, const double *__restrict__ JR,
+                               double *__restrict__ Minv, int *__restrict__ err, RowScale wref,
+                               double *__restrict__ rowmag) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nc = m.nc;
+  if (c >= nc) return;
+  double B[25];
+  diag_block(cs, m, Wn, vol, dt, JL, JR, c, B);
   // magnitude of each equation's row for reference state changes: sum_k |B_ik| Wref_k
 #pragma unroll
   for (int i = 0; i < 5; ++i) {
@@ -901,6 +924,17 @@ static void alloc_state(fcfd_ctx *x, NewtonState &ns, int sweeps, int cycles, bo
   CK(cudaStreamSynchronize(s));
 }
 
+// First-order face Jacobians JL, JR [25][nf] at the state of the last residual
+// chain run on x->p64 (states, gradients, limiters and stale densities).
+static void launch_face_jac(fcfd_ctx *x, double *JL, double *JR) {
+  const DevMesh &m = x->dm;
+  cudaStream_t s = x->stream;
+  if (x->viscous)
+    FCFD_BY_FLUX(x->cs.flux, k_face_jac<true, FX><<<(m.nf + 127) / 128, 128, 0, s>>>(x->cs, m, x->p64.W.p, x->p64.G.p, x->p64.Lm.p, x->p64.stale.p, JL, JR));
+  else
+    FCFD_BY_FLUX(x->cs.flux, k_face_jac<false, FX><<<(m.nf + 127) / 128, 128, 0, s>>>(x->cs, m, x->p64.W.p, x->p64.G.p, x->p64.Lm.p, x->p64.stale.p, JL, JR));
+}
+
 // One linearised backward-Euler solve at the state the last residual loaded
 // (ns.Wn, residual in ns.R0, local time step in ns.dt): the preconditioner
 // from the first-order face Jacobians, then GMRES for (V P/dt - J) dW = R0 into
@@ -931,10 +965,7 @@ static LinearSolve implicit_solve(fcfd_ctx *x, NewtonState &ns, Krylov<double> &
     wref.s[1] = wref.s[2] = wref.s[3] = U;
   }
   // block-Jacobi preconditioner from the first-order face Jacobians
-  if (x->viscous)
-    FCFD_BY_FLUX(x->cs.flux, k_face_jac<true, FX><<<(m.nf + 127) / 128, 128, 0, s>>>(x->cs, m, x->p64.W.p, x->p64.G.p, x->p64.Lm.p, x->p64.stale.p, ns.JL.p, ns.JR.p));
-  else
-    FCFD_BY_FLUX(x->cs.flux, k_face_jac<false, FX><<<(m.nf + 127) / 128, 128, 0, s>>>(x->cs, m, x->p64.W.p, x->p64.G.p, x->p64.Lm.p, x->p64.stale.p, ns.JL.p, ns.JR.p));
+  launch_face_jac(x, ns.JL.p, ns.JR.p);
   k_block_jacobi<<<gc, tb, 0, s>>>(x->cs, m, ns.Wn.p, ns.vol.p, ns.dt.p, ns.JL.p, ns.JR.p, ns.Minv.p, x->err.p, wref, ns.rowmag.p);
   if (ns.sweeps > 0) {
     const std::vector<int> &ci = x->color_index;
@@ -1205,6 +1236,47 @@ int fcfd_newton_solve(fcfd_ctx *x, double *W, const fcfd_newton_opts *o, fcfd_ne
       set_last_error(status == FCFD_ERR_DIVERGED ? "Newton iteration diverged (NaN/Inf update)" : "Newton iteration did not reach the tolerance");
       return status;
     }
+  } catch (const Error &e) {
+    set_last_error(e.what());
+    return e.code;
+  } catch (const std::exception &e) {
+    set_last_error(e.what());
+    return FCFD_ERR_INPUT;
+  }
+  return FCFD_OK;
+}
+
+// Diagonal blocks V P/dt - J_cc of the implicit operator at the state W[nc][5]
+// (host) and local time steps dt[nc] (host): the matrix the block
+// preconditioner of fcfd_newton_solve / fcfd_run inverts, the counterpart of
+// the diagonal of the matrix NavierStokes::time_terms (ns_time_terms.cc:
+// 107-186, cons2prim 26-56) and assemble_linear_system's first-order Jacobian
+// (ns_assemble_linear_system.cc:142-190) build.  blocks[nc][5][5] (row =
+// equation, column = primitive variable).
+int fcfd_diag_blocks(fcfd_ctx *x, const double *W, const double *dt, double *blocks) {
+  try {
+    if (!x || !W || !dt || !blocks) throw Error(FCFD_ERR_INPUT, "null argument");
+    CK(cudaSetDevice(x->device));
+    const DevMesh &m = x->dm;
+    const int nc = m.nc, n = 5 * nc;
+    cudaStream_t s = x->stream;
+    const int tb = 256, gc = (nc + tb - 1) / tb;
+    DBuf<double> Wn, R, dtd, vol, JL, JR, B;
+    Wn.alloc(n); R.alloc(n); dtd.alloc(nc); vol.alloc(nc);
+    JL.alloc(25 * (size_t)m.nf); JR.alloc(25 * (size_t)m.nf); B.alloc(25 * (size_t)nc);
+    CK(cudaMemsetAsync(JR.p, 0, sizeof(double) * 25 * (size_t)m.nf, s));
+    std::vector<double> hv(x->mesh->c_volume.begin(), x->mesh->c_volume.begin() + nc);
+    CK(cudaMemcpyAsync(vol.p, hv.data(), sizeof(double) * nc, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(dtd.p, dt, sizeof(double) * nc, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(x->Win.p, W, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+    k_aos_to_soa_nc<<<gc, tb, 0, s>>>(x->Win.p, Wn.p, nc);
+    eval_residual<double>(x, Wn.p, R.p, (const double *)nullptr, (const double *)nullptr);
+    launch_face_jac(x, JL.p, JR.p);
+    k_diag_blocks<<<gc, tb, 0, s>>>(x->cs, m, Wn.p, vol.p, dtd.p, JL.p, JR.p, B.p);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(blocks, B.p, sizeof(double) * 25 * (size_t)nc, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    check_err(x);
   } catch (const Error &e) {
     set_last_error(e.what());
     return e.code;

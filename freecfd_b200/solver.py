@@ -319,6 +319,18 @@ class NavierStokes:
         check(lib.fcfd_local_dt(self.h, pw, float(cfl), int(mode), ctypes.c_void_p(dt.ctypes.data), fw))
         return dt
 
+    def diag_blocks(self, W, dt):
+        """Diagonal blocks V P/dt - J_cc (nc, 5, 5) of the implicit operator
+        at state W and local time steps dt: the counterpart of the diagonal
+        of NavierStokes::time_terms (ns_time_terms.cc:107-186) plus
+        assemble_linear_system's first-order Jacobian."""
+        nc = self.mesh.nc
+        W = np.ascontiguousarray(W, dtype=np.float64).reshape(nc, 5)
+        dt = np.ascontiguousarray(dt, dtype=np.float64).reshape(nc)
+        out = np.empty((nc, 5, 5))
+        check(lib.fcfd_diag_blocks(self.h, _d(W), _d(dt), _d(out)))
+        return out
+
     def time_residual(self, reps: int = 50, flush_l2: bool = True):
         out = np.zeros(8)
         check(lib.fcfd_time_residual(self.h, int(reps), int(bool(flush_l2)), _d(out), out.size))

@@ -260,6 +260,17 @@ typedef struct fcfd_newton_report {
  * Returns FCFD_ERR_NOT_CONVERGED / FCFD_ERR_DIVERGED with the report filled. */
 int fcfd_newton_solve(fcfd_ctx *ctx, double *W, const fcfd_newton_opts *opts, fcfd_newton_report *report);
 
+/* Diagonal blocks V P/dt - J_cc of the implicit operator at the state W[nc][5]
+ * and local time steps dt[nc] (both host): the matrix the block
+ * preconditioner of fcfd_newton_solve / fcfd_run inverts.  Replaces the
+ * diagonal of the matrix that NavierStokes::time_terms (P V / dt,
+ * ns_time_terms.cc:107-186 with cons2prim 26-56) and assemble_linear_system's
+ * first-order Jacobian (get_jacobians, ns_assemble_linear_system.cc:142-267)
+ * build; here J_cc is the exact derivative of the first-order face fluxes
+ * (the reference takes finite differences).  blocks[nc][5][5], row =
+ * equation (mass, momentum x/y/z, energy), column = primitive (p,u,v,w,T). */
+int fcfd_diag_blocks(fcfd_ctx *ctx, const double *W, const double *dt, double *blocks);
+
 /* Deck-driven time loop (main.cc:294-438) for one laminar or Euler grid,
  * replacing the reference's main program after set-up.  Per time step:
  * update_time_step (time_step.cc:143-224: CFL ramp, schedule file, FIXED /
