@@ -12,8 +12,11 @@ and output copies inside the timed region.
     python -m torch.distributed.run --nproc-per-node N bench.py --gpus N ...
 
 Multi-GPU runs are replicas: every rank evaluates its own copy of the mesh
-(weak scaling, no data-path collective).  ``--impl reference`` times the CPU
-restatement of the reference's residual on the host cores instead.
+(weak scaling, no data-path collective).  ``--impl reference`` times the
+reference itself -- Free CFD's own sources compiled into oracle/_ref/freecfd_ref
+-- on the host cores instead, one process per core.  The default run also
+checks the timed residual against the oracle (untimed) and prints residual
+lines for the hypersonic, plate and plate64 workloads.
 """
 from __future__ import annotations
 
@@ -44,10 +47,32 @@ METRIC = "M faces/s residual + % HBM peak; Newton wall time to 1e-10: mixed+JVP 
 UNIT = "M faces/s"
 
 
+def load_cases():
+    """freecfd_b200/cases.py on its own (it needs numpy only): the reference
+    arm must not import the freecfd_b200 package, whose __init__ loads the
+    CUDA library."""
+    import importlib.util
+    mod = sys.modules.get("fcfd_bench_cases")
+    if mod is None:
+        spec = importlib.util.spec_from_file_location("fcfd_bench_cases",
+                                                      os.path.join(ROOT, "freecfd_b200", "cases.py"))
+        mod = importlib.util.module_from_spec(spec)
+        sys.modules["fcfd_bench_cases"] = mod
+        spec.loader.exec_module(mod)
+    return mod
+
+
 def make_case(name):
-    from freecfd_b200 import cases
     w = WORKLOADS[name]
-    return getattr(cases, w["fn"])(**w["kw"])
+    return getattr(load_cases(), w["fn"])(**w["kw"])
+
+
+def bench_config(case, counts, world):
+    """The `config` object, identical in both arms: the workload and its sizes."""
+    return {"workload": case.workload, "cells": int(counts["cells"]), "faces": int(counts["faces"]),
+            "ghosts": int(counts["ghosts"]), "stencil_entries": int(counts["stencil_entries"]),
+            "l2": "GPU arm: 512 MB memset flushes L2 before every step",
+            "parallelism": f"replicas x{world}"}
 
 
 def alg_bytes(m, s=8):
@@ -137,8 +162,8 @@ class Clocks:
                 "reasons": reasons, "samples": len(self.samples)}
 
 
-def cpu_baseline(case, seconds=12.0):
-    """Single-core oracle (restatement of the reference's CPU residual)."""
+def port_baseline(case, seconds=4.0):
+    """The oracle (C++ restatement, right-hand side only) on one core."""
     import oracle
     o = oracle.Oracle(case)
     if case.kstate is not None:
@@ -158,64 +183,178 @@ def cpu_baseline(case, seconds=12.0):
     v = o.nf * n / el / 1e6
     o.close()
     return {"value": round(v, 4), "unit": UNIT, "cores": 1, "kind": "port",
-            "sample": f"{n} full residual evaluations of the same workload ({o.nf} faces) in {el:.1f} s, "
-                      f"single-threaded C++ restatement (-O2, no FMA)"}
+            "sample": f"{n} residual evaluations (right-hand side only) of the same workload ({o.nf} faces) in "
+                      f"{el:.1f} s, single-threaded C++ restatement (-O2, no FMA)"}
 
 
-def _ref_worker(args):
-    name, steps, warmup, q = args
-    import oracle
-    case = make_case(name)
-    o = oracle.Oracle(case)
-    if case.kstate is not None:
-        def step():
-            o.rans_residual(case.state, case.kstate)
-    else:
-        def step():
-            o.residual(case.state)
-    for _ in range(warmup):
-        step()
-    q.put(("ready", os.getpid()))
-    t0 = time.perf_counter()
-    for _ in range(steps):
-        step()
-    el = time.perf_counter() - t0
-    q.put(("done", el, o.nf))
+def _mem_available_gb():
+    try:
+        with open("/proc/meminfo") as fh:
+            for line in fh:
+                if line.startswith("MemAvailable:"):
+                    return int(line.split()[1]) / 1048576.0
+    except OSError:
+        pass
+    return None
+
+
+def reference_workers(case, cap):
+    """Processes for the reference: one per host core, at most `cap`, and no
+    more than half the available memory holds (a process keeps one mesh copy:
+    about 6.5 kB per cell)."""
+    n = max(1, min(os.cpu_count() or 1, cap))
+    mem = _mem_available_gb()
+    if mem:
+        per = max(0.05, 6.5e3 * case.mesh.n_cells / 1e9)
+        n = max(1, min(n, int(0.5 * mem / per)))
+    return n
+
+
+def reference_throughput(case, procs, evals, warmup):
+    """The reference itself (oracle/_ref/freecfd_ref: Free CFD's own sources)
+    in `procs` concurrent processes, each holding its own copy of the mesh
+    like one MPI rank per core without exchanges.  Each process times
+    `evals` residual evaluations after `warmup` (the reference's
+    calc_cell_grads, calc_limiter and assemble_linear_system, whose face loop
+    also forms the first-order finite-difference Jacobian, with the matrix
+    inserts switched off).  Throughput = procs x faces x evals / the slowest
+    process's time."""
+    from oracle import reference
+    ref = reference.Reference(case)
+    cmd = ref.bench_command(case.state, evals, warmup, case.kstate)
+    ps = [subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True) for _ in range(procs)]
+    outs = []
+    for p in ps:
+        out, err = p.communicate(timeout=7200)
+        if p.returncode != 0:
+            raise RuntimeError(f"freecfd_ref bench failed: {err.strip()[-500:]}")
+        line = [x for x in out.splitlines() if x.startswith("FCFD_REF_RESULT ")][-1]
+        outs.append(json.loads(line[len("FCFD_REF_RESULT "):]))
+    ref.close()
+    el = max(o["seconds"] for o in outs)
+    nf = outs[0]["nf"]
+    return {"value": procs * nf * evals / el / 1e6, "seconds": el, "sizes": outs[0], "procs": procs,
+            "evals": evals, "setup_seconds": max(o["setup_seconds"] for o in outs)}
+
+
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as fh:
+            for line in fh:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
+
+
+def cpu_baseline(case, seconds, cap):
+    """The reference on the host cores for a bounded sample (about `seconds`
+    of work per process)."""
+    from oracle import reference
+    if not reference.available():
+        return port_baseline(case, seconds)
+    procs = reference_workers(case, cap)
+    evals = max(2, int(round(seconds * 0.3e6 / max(case.mesh.n_cells * 4, 1))))
+    r = reference_throughput(case, procs, evals, 1)
+    return {"value": round(r["value"], 4), "unit": UNIT, "cores": procs, "kind": "reference",
+            "sample": f"{procs} processes x {evals} residual evaluations of the same workload "
+                      f"({r['sizes']['nf']} faces) by the reference's own code (oracle/_ref/freecfd_ref), "
+                      f"one mesh copy per process; each evaluation is the reference's calc_cell_grads + "
+                      f"calc_limiter + assemble_linear_system, whose face loop also forms its finite-difference "
+                      f"Jacobian", "host_cpu": cpu_model(), "nproc": os.cpu_count()}
 
 
 def run_reference(args):
-    import multiprocessing as mp
     rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
     if rank != 0:
         return
-    ctx = mp.get_context("spawn")
-    ncpu = os.cpu_count() or 1
-    workers = max(1, min(ncpu, args.ref_workers))
-    q = ctx.Manager().Queue()
-    steps = args.steps
-    procs = [ctx.Process(target=_ref_worker, args=((args.workload, steps, args.warmup, q),)) for _ in range(workers)]
-    for p in procs:
-        p.start()
-    done = []
-    while len(done) < workers:
-        msg = q.get(timeout=3600)
-        if msg[0] == "done":
-            done.append(msg)
-    for p in procs:
-        p.join()
-    el = max(d[1] for d in done)
-    nf = done[0][2]
-    value = workers * nf * steps / el / 1e6
+    from oracle import reference
     case = make_case(args.workload)
-    line = {"metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": args.gpus, "steps": steps,
-            "warmup": args.warmup, "ms_per_step": round(1e3 * el / steps, 4), "higher_is_better": True,
+    if reference.available():
+        procs = reference_workers(case, args.ref_workers)
+        r = reference_throughput(case, procs, args.steps, args.warmup)
+        value, el, sz, kind = r["value"], r["seconds"], r["sizes"], "reference"
+        sample = (f"{procs} processes x {args.steps} timed residual evaluations (after {args.warmup}) of the "
+                  f"reference's own code, compiled from its sources (oracle/_ref/freecfd_ref), one mesh copy per "
+                  f"process like one MPI rank per core; each evaluation is calc_cell_grads + calc_limiter + "
+                  f"assemble_linear_system, whose face loop also forms the first-order finite-difference Jacobian "
+                  f"(matrix inserts switched off)")
+        counts = dict(cells=sz["nc"], faces=sz["nf"], ghosts=sz["nghost"], stencil_entries=sz["n_grad_entries"])
+    else:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/freecfd_ref (the reference compiled from "
+                                                              "its sources) was not built"}), flush=True)
+        return
+    line = {"metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(1e3 * el / args.steps, 4), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
-            "config": {"workload": case.workload, "faces": nf, "cells": case.mesh.n_cells},
-            "cpu_baseline": {"value": round(value, 4), "unit": UNIT, "cores": workers, "kind": "port",
-                             "sample": f"{workers} processes x {steps} full residual evaluations each (one mesh copy "
-                                       f"per core, like one MPI rank per core), C++ restatement of the reference"},
+            "config": bench_config(case, counts, world),
+            "cpu_baseline": {"value": round(value, 4), "unit": UNIT, "cores": procs, "kind": kind,
+                             "sample": sample, "host_cpu": cpu_model(), "nproc": os.cpu_count()},
             "e2e": {"value": round(value, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if not args.no_cpu:
+        line["port_residual_only"] = port_baseline(case, 4.0)
     print(json.dumps(line), flush=True)
+
+
+def parity_check(ns, case):
+    """Untimed: the timed workload's residual against the oracle (which the
+    pin tests hold bit-exact to the compiled reference), normwise relative per
+    equation with the three momentum components sharing one scale."""
+    import oracle
+    o = oracle.Oracle(case)
+    if case.kstate is not None:
+        R, RK = ns.rans_residual(case.state, case.kstate)
+        ref, refk = o.rans_residual(case.state, case.kstate)
+    else:
+        R, ref = ns.residual(case.state), o.residual(case.state)
+    o.close()
+    scale = np.abs(ref).max(axis=0)
+    scale[1:4] = scale[1:4].max()
+    err = np.abs(R - ref).max(axis=0) / np.maximum(scale, 1e-300)
+    out = {"max_normwise_rel": float(err.max()), "per_equation": [float(e) for e in err], "bar": 1e-12,
+           "against": "oracle (bit-exact to the reference compiled from its sources)"}
+    if case.kstate is not None:
+        ek = np.abs(RK - refk).max(axis=0) / np.maximum(np.abs(refk).max(axis=0), 1e-300)
+        out["komega_per_equation"] = [float(e) for e in ek]
+        out["max_normwise_rel"] = float(max(err.max(), ek.max()))
+    return out
+
+
+def residual_subline(fb, name, dev, steps, warmup, parity):
+    """One more workload's residual: M faces/s, the step's algorithmic bytes
+    over its time, the dominant kernel's roofline fraction and, where the
+    oracle finishes in seconds, its parity."""
+    import tempfile
+    case = make_case(name)
+    cs = fb.Case(case.write_deck(tempfile.mkdtemp(prefix="fcfd_bench_")))
+    mesh = fb.Mesh(case.mesh, cs)
+    ns = fb.NavierStokes(mesh, cs, dev)
+    ns.residual(case.state)
+    ns.time_residual(max(warmup, 1), True)
+    t = ns.time_residual(steps, True)
+    ms = float(t[0])
+    kern = {"ghost_minmax": t[1], "grad_limiter": t[2], "outlet_density": t[3], "face_flux": t[4], "gather": t[5]}
+    peak, kind = peaks()
+    B = alg_bytes(mesh)
+    top = max(("grad_limiter", "face_flux", "gather", "ghost_minmax"), key=lambda k: kern[k])
+    viscous = "viscosity=0." not in case.deck
+    exact_grad = "limiter=minmod" in case.deck or "limiter=bj" in case.deck
+    kb = kernel_bytes(mesh, top, viscous, exact_grad)
+    out = {"workload": case.workload, "cells": mesh.nc, "faces": mesh.nf, "steps": steps,
+           "ms_per_step": round(ms, 5), "value": round(mesh.nf / (ms * 1e-3) / 1e6, 3), "unit": UNIT,
+           "step_roofline": {"achieved": round(B / (ms * 1e-3) / 1e9, 1), "frac": round(B / (ms * 1e-3) / 1e9 / peak, 4),
+                             "alg_bytes": int(B), "peak": peak, "peak_kind": kind},
+           "roofline": {"kernel": top, "alg_bytes_per_launch": int(kb), "ms_per_launch": round(float(kern[top]), 5),
+                        "achieved": round(kb / (float(kern[top]) * 1e-3) / 1e9, 1),
+                        "frac": round(kb / (float(kern[top]) * 1e-3) / 1e9 / peak, 4),
+                        "traffic": NCU_TRAFFIC.get((name, top))},
+           "kernels_ms": {k: round(float(v), 5) for k, v in kern.items()}}
+    if parity:
+        out["parity_err"] = parity_check(ns, case)
+    del ns
+    return out
 
 
 def run_ours(args):
@@ -305,9 +444,8 @@ def run_ours(args):
     line = {"metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms, 5), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": case.workload, "cells": mesh.nc, "faces": mesh.nf, "ghosts": mesh.nghost,
-                       "stencil_entries": mesh.n_grad_entries, "l2": "flushed (512 MB memset before every step)",
-                       "parallelism": f"replicas x{world}"},
+            "config": bench_config(case, dict(cells=mesh.nc, faces=mesh.nf, ghosts=mesh.nghost,
+                                              stencil_entries=mesh.n_grad_entries), world),
             "e2e": {"value": round(e2e, 3), "unit": UNIT,
                     "h2d_bytes_per_step": int(W.nbytes + (K.nbytes if rans else 0)),
                     "d2h_bytes_per_step": int(W.nbytes + (K.nbytes if rans else 0))},
@@ -319,12 +457,17 @@ def run_ours(args):
             "kernels_ms": {k: round(float(v), 5) for k, v in kern.items()},
             "gpu_launches": n_kernels * args.steps,
             "clocks": clk.summary()}
+    if rank == 0 and not args.no_parity:
+        line["parity_err"] = parity_check(ns, case)
+    if not args.no_sublines and args.workload == "cylinder":
+        line["workloads"] = [residual_subline(fb, w, dev, min(args.steps, 20), args.warmup, w != "plate64")
+                             for w in ("hypersonic", "plate", "plate64")]
     if (world > 1 or args.decomposed) and args.workload == "cylinder":
         line["decomposed"] = run_decomposed(fb, world, rank, dev, dist, args.steps, args.warmup)
     if not args.no_newton and not rans:
         line["newton"] = run_newton(fb, cs, mesh, case, dev, dist)
     if rank == 0 and world == 1 and not args.no_cpu:
-        line["cpu_baseline"] = cpu_baseline(case, args.cpu_seconds)
+        line["cpu_baseline"] = cpu_baseline(case, args.cpu_seconds, args.ref_workers)
     if rank == 0:
         print(json.dumps(line), flush=True)
     del ns
@@ -489,6 +632,9 @@ def main():
     ap.add_argument("--ref-workers", type=int, default=64)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-newton", action="store_true")
+    ap.add_argument("--no-parity", action="store_true", help="skip the untimed oracle check of the timed workload")
+    ap.add_argument("--no-sublines", action="store_true",
+                    help="skip the residual lines of the hypersonic, plate and plate64 workloads")
     ap.add_argument("--decomposed", action="store_true",
                     help="also time the domain-decomposed residual (always on under torchrun)")
     ap.add_argument("--profile-newton", type=int, default=0,

@@ -21,7 +21,7 @@
 //             finite-difference face Jacobians of assemble_linear_system plus
 //             time_terms' P V / dt
 //   dt        update_time_step (time_step.cc:143-224) at time step 1
-//   bench     the residual repeated for a bounded time (CPU baseline)
+//   bench     a given number of residual evaluations, timed (CPU baseline)
 //
 // Five pieces are supplied here because the snapshot of the reference lacks
 // them or they cannot compile or run as compiled today:
@@ -509,21 +509,26 @@ static void cmd_dt(const std::string &wpath, const std::string &out) {
   write_bin(out + "/dt.f64", d);
 }
 
-static std::string cmd_bench(const std::string &wpath, double min_seconds, const std::string &kpath) {
+// `evals` timed residual evaluations after `warmup` untimed ones, the state
+// reloaded before each (as update_variables would have changed it).
+static std::string cmd_bench(const std::string &wpath, int evals, int warmup, const std::string &kpath) {
   const int nc = grid[0].cellCount;
   const bool turb = !kpath.empty();
-  set_state(read_bin<double>(wpath, 5 * (size_t)nc));
-  if (turb) set_turbulence(read_bin<double>(kpath, 2 * (size_t)nc));
-  residual(turb);  // warm-up
-  int evals = 0;
-  const double t0 = now_s();
-  double t1 = t0;
-  do {
-    set_state(read_bin<double>(wpath, 5 * (size_t)nc));
+  const std::vector<double> W = read_bin<double>(wpath, 5 * (size_t)nc);
+  std::vector<double> K;
+  if (turb) K = read_bin<double>(kpath, 2 * (size_t)nc);
+  for (int i = 0; i < warmup; ++i) {
+    set_state(W);
+    if (turb) set_turbulence(K);
     residual(turb);
-    ++evals;
-    t1 = now_s();
-  } while (t1 - t0 < min_seconds);
+  }
+  const double t0 = now_s();
+  for (int i = 0; i < evals; ++i) {
+    set_state(W);
+    if (turb) set_turbulence(K);
+    residual(turb);
+  }
+  const double t1 = now_s();
   std::ostringstream s;
   s.precision(17);
   s << "\"evaluations\": " << evals << ", \"seconds\": " << (t1 - t0);
@@ -558,7 +563,8 @@ int main(int argc, char **argv) {
     else if (cmd == "timeterms" && a.size() == 3) cmd_timeterms(a[0], a[1], a[2]);
     else if (cmd == "dt" && a.size() == 2) cmd_dt(a[0], a[1]);
     else if (cmd == "diagblocks" && a.size() == 3) cmd_diagblocks(a[0], a[1], a[2]);
-    else if (cmd == "bench" && (a.size() == 2 || a.size() == 3)) extra = cmd_bench(a[0], atof(a[1].c_str()), a.size() == 3 ? a[2] : "");
+    else if (cmd == "bench" && (a.size() == 3 || a.size() == 4))
+      extra = cmd_bench(a[0], atoi(a[1].c_str()), atoi(a[2].c_str()), a.size() == 4 ? a[3] : "");
     else throw std::runtime_error("unknown command or wrong arguments: " + cmd);
     Grid &g = grid[0];
     long long st = 0, cf = 0;

@@ -185,10 +185,14 @@ class Reference:
         nc = s["nc"]
         return a[:nc], float(a[nc]), float(a[nc + 1])
 
-    def bench(self, W, seconds: float, K=None) -> dict:
-        """Residual evaluations repeated for at least ``seconds`` in one
-        process: {'evaluations', 'seconds', 'setup_seconds', sizes...}."""
-        args = [self._put("W.bin", W), str(float(seconds))]
+    def bench_command(self, W, evals: int, warmup: int, K=None) -> list:
+        """Command line of `evals` timed residual evaluations after `warmup`
+        untimed ones (one process; prints {'evaluations', 'seconds', ...})."""
+        args = [self._put("W.bin", W), str(int(evals)), str(int(warmup))]
         if K is not None:
             args.append(self._put("K.bin", K))
-        return self.run("bench", *args)
+        return [BINARY, self.dir, self.deck, "bench", *args]
+
+    def bench(self, W, evals: int, warmup: int = 1, K=None) -> dict:
+        cmd = self.bench_command(W, evals, warmup, K)
+        return self.run("bench", *cmd[4:])
