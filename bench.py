@@ -389,9 +389,16 @@ def run_ours(args):
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
+    # the K timed steps are repeated until the block lasts a second, so the
+    # clock sampler sees the GPU under this load; the median repeat is reported
+    reps = []
     with Clocks(dev) as clk:
-        t = ns.time_rans(args.steps, True) if rans else ns.time_residual(args.steps, True)
+        t_start = time.perf_counter()
+        while not reps or (time.perf_counter() - t_start < 1.0 and len(reps) < 2000):
+            reps.append(ns.time_rans(args.steps, True) if rans else ns.time_residual(args.steps, True))
     torch.cuda.synchronize()
+    reps.sort(key=lambda r: float(r[0]))
+    t = reps[len(reps) // 2]
     ms = float(t[0])
     if rans:
         kern = {"ns_part_with_eddy_viscosity": t[1], "komega_part": t[2]}
@@ -456,6 +463,9 @@ def run_ours(args):
                               "unit_of_work": "one residual evaluation (all kernels)"},
             "kernels_ms": {k: round(float(v), 5) for k, v in kern.items()},
             "gpu_launches": n_kernels * args.steps,
+            "timed_repeats": {"count": len(reps), "reported": "median repeat of K steps",
+                              "ms_per_step_min": round(float(reps[0][0]), 5),
+                              "ms_per_step_max": round(float(reps[-1][0]), 5)},
             "clocks": clk.summary()}
     if rank == 0 and not args.no_parity:
         line["parity_err"] = parity_check(ns, case)

@@ -524,7 +524,8 @@ grid_1 {{
     free = (p, U, 0.0, 0.0, T)
     st = seeded_state(mesh.n_cells, free, seed)
     case = Case("plate", mesh, deck, {"air": mat}, st, free,
-                f"rans_flat_plate_{ni}x{nj}x{nk}_hex_roe_viscous_komega")
+                f"rans_flat_plate_{ni}x{nj}x{nk}_hex_roe_viscous_komega" if turbulent else
+                f"laminar_flat_plate_{ni}x{nj}x{nk}_hex_roe_viscous")
     if turbulent:
         # freestream k, omega as the reference's inlet / IC formulas give them
         # (rans.cc:112-116, rans_set_bcs.cc:61-65): intensity 1e-3, ratio 1

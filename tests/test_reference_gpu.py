@@ -111,20 +111,27 @@ def test_diag_blocks_against_reference(family, fb, oracle_mod):
     """The preconditioner's diagonal blocks V P/dt - J_cc.  The time-term part
     (cons2prim, ns_time_terms.cc:26-56,107-186) is isolated by evaluating the
     blocks at dt and 2 dt: the difference is P V / (2 dt), compared with the
-    oracle's restatement (bit-exact to the reference) at 1e-14.  J_cc is the
-    exact derivative of the first-order face fluxes here and a one-sided
-    finite difference in the reference (get_jacobians), so the two agree to
-    the finite difference's truncation error: 1e-5 of each block row's
-    largest entry."""
+    oracle's restatement (bit-exact to the reference) at 1e-13 of each block
+    row.  J_cc is the exact derivative of the first-order face fluxes here and
+    a one-sided finite difference with step 1.5e-7 in the reference
+    (get_jacobians, ns_assemble_linear_system.cc:197-267), so the two agree
+    to the finite difference's error: 1e-5 normwise per equation (largest
+    difference over cells and columns over the equation's largest entry).
+    The seeded states have v = 0 exactly, which puts faces whose normal is
+    along y on the kink of the upwind switches, where a one-sided difference
+    and a derivative pick different branches; a small seeded v moves the
+    state off the kinks."""
     case = {"wedge": lambda: cases.wedge_case(ni=24, nj=12),
             "cylinder": lambda: cases.cylinder_case(ntheta=32, nr=16),
             "hypersonic": lambda: cases.hypersonic_case(ntheta=32, nr=16)}[family]()
+    W = case.state.copy()
+    W[:, 2] += 1e-3 * case.freestream[1] * np.random.default_rng(7).uniform(-1.0, 1.0, W.shape[0])
     m, ns = _ns(case, fb)
     dt = np.random.default_rng(5).uniform(0.5, 2.0, m.nc) * 1e-5
-    B1 = ns.diag_blocks(case.state, dt)
-    B2 = ns.diag_blocks(case.state, 2.0 * dt)
+    B1 = ns.diag_blocks(W, dt)
+    B2 = ns.diag_blocks(W, 2.0 * dt)
     o = oracle_mod.Oracle(case)
-    tt = o.time_terms(case.state, dt)
+    tt = o.time_terms(W, dt)
     half = B1 - B2
     scale = np.maximum(np.abs(tt).max(axis=2, keepdims=True), 1e-300)
     assert (np.abs(half - 0.5 * tt) / scale).max() <= 1e-13
@@ -132,8 +139,6 @@ def test_diag_blocks_against_reference(family, fb, oracle_mod):
     from oracle import reference
     if not reference.available():
         pytest.skip("the compiled reference did not travel with the repository")
-    Jref = tt - reference.Reference(case).diag_blocks(case.state, dt)
-    row = np.maximum(np.abs(Jref).max(axis=2, keepdims=True), 1e-300)
-    err = (np.abs(Jdev - Jref) / row).max()
-    print(f"J_cc rel err vs reference FD {err:.3e}")
-    assert err <= 1e-3
+    Jref = tt - reference.Reference(case).diag_blocks(W, dt)
+    err = np.abs(Jdev - Jref).max(axis=(0, 2)) / np.abs(Jref).max(axis=(0, 2))
+    assert err.max() <= 1e-5, err
