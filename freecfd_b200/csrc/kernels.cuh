@@ -1281,7 +1281,9 @@ __global__ void k_local_dt(DevCase cs, DevMesh m, const S *__restrict__ W, S *__
   const S a = sound(cs, p, T);
   const S v_dt = cfl * m.c_len[c] / (sqrt(u * u + v * v + w * w) + a);
   dt[c] = v_dt;
-  if (minkey) atomicMin(minkey, okey(val(v_dt)));
+  // a NaN step drops out of the minimum, as it does in update_time_step's
+  // std::min (time_step.cc:181-186)
+  if (minkey && val(v_dt) == val(v_dt)) atomicMin(minkey, okey(val(v_dt)));
 }
 
 template <class S>

@@ -129,15 +129,24 @@ extern "C" int fcfd_local_dt_cflmax_noalloc(const double *W, const double *lengt
     set_last_error(err);
     return FCFD_ERR_CUDA;
   }
+  // An error left by the caller's earlier work is reported as such and left
+  // in place for the caller's own check; only errors of the launches below
+  // are taken (and cleared) here.
+  cudaError_t e = cudaPeekAtLastError();
+  if (e != cudaSuccess) {
+    set_last_error(std::string("fcfd_local_dt_cflmax_noalloc: a CUDA error from earlier work on this thread is "
+                               "pending (nothing launched): ") + cudaGetErrorString(e));
+    return FCFD_ERR_CUDA;
+  }
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const int nblocks = (n_cells + kThreads - 1) / kThreads;
   const Gas g{gamma, gas_R, Pref, Tref, cfl};
   k_dt_cells<<<nblocks, kThreads, 0, s>>>(W, length, n_cells, g, dt, scratch);
   k_dt_reduce<<<1, kThreads, 0, s>>>(nblocks, scratch);
   k_dt_fill<<<nblocks, kThreads, 0, s>>>(n_cells, dt, scratch);
-  cudaError_t e = cudaGetLastError();
+  e = cudaGetLastError();
   if (e != cudaSuccess) {
-    set_last_error(std::string("fcfd_local_dt_cflmax_noalloc: ") + cudaGetErrorString(e));
+    set_last_error(std::string("fcfd_local_dt_cflmax_noalloc: launch failed: ") + cudaGetErrorString(e));
     return FCFD_ERR_CUDA;
   }
   return FCFD_OK;

@@ -341,8 +341,14 @@ int fcfd_time_residual(fcfd_ctx *ctx, int reps, int flush_l2, double *out, int o
  * minimum is a file-scope __device__ array of 4096+32 doubles, so n_cells is
  * limited to 1,048,576 (larger sizes return FCFD_ERR_INPUT).  The first call
  * on a device looks up the array's device address (cudaGetSymbolAddress);
- * make that first call before any stream capture.  Every call shares the one
- * array: calls that overlap on the GPU race and must be serialised. */
+ * make that first call before any stream capture.  That address is kept for
+ * the life of the process: after cudaDeviceReset on a device the library must
+ * not be called on that device again.  A cell whose time step is NaN is left
+ * out of the minimum, as std::min leaves it out in update_time_step
+ * (time_step.cc:181-186); fcfd_local_dt does the same.  A CUDA error already
+ * pending on the calling thread is reported (FCFD_ERR_CUDA) without launching
+ * and without clearing it.  Every call shares the one array: calls that
+ * overlap on the GPU race and must be serialised. */
 int fcfd_local_dt_cflmax_noalloc(const double *W, const double *length, int32_t n_cells, double gamma, double gas_R,
                                  double Pref, double Tref, double cfl, double *dt, void *stream);
 

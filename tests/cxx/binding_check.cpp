@@ -1,0 +1,90 @@
+// A C++ caller of libfcfd_b200.so through include/fcfd.h, written the way the
+// binding in INTEGRATION.md would call it from inside the reference
+// (NavierStokes::b200_init / b200_residual): parse the deck, build the mesh
+// from CELL-type raw arrays, create a device context, evaluate a residual, and
+// report errors through status codes and fcfd_last_error().
+//
+// Usage: binding_check <deck> <mesh.bin> [<W.bin> <R.bin>]
+//   mesh.bin: int32 n_nodes, n_cells, n_bc, conn_len, bc_len, then
+//             xyz[n_nodes*3] f64, conn_index[n_cells+1], conn[conn_len],
+//             bc_index[n_bc+1], bc_nodes[bc_len] (int32)
+// Prints one line of key=value pairs.
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <vector>
+
+#include "fcfd.h"
+
+template <class T>
+static bool get(std::ifstream &f, T *p, size_t n) {
+  f.read(reinterpret_cast<char *>(p), (std::streamsize)(n * sizeof(T)));
+  return (bool)f;
+}
+
+int main(int argc, char **argv) {
+  if (argc != 3 && argc != 5) {
+    std::fprintf(stderr, "usage: %s <deck> <mesh.bin> [<W.bin> <R.bin>]\n", argv[0]);
+    return 2;
+  }
+  std::printf("version=%s", fcfd_version());
+
+  // error path: a deck that does not exist is FCFD_ERR_INPUT with a message
+  fcfd_case *bad = nullptr;
+  const int rc_bad = fcfd_case_from_deck("/nonexistent/deck.in", &bad);
+  std::printf(" missing_deck_rc=%d missing_deck_msg_len=%zu", rc_bad, std::strlen(fcfd_last_error()));
+
+  fcfd_case *cs = nullptr;
+  int rc = fcfd_case_from_deck(argv[1], &cs);
+  std::printf(" deck_rc=%d", rc);
+  if (rc) { std::printf(" error=\"%s\"\n", fcfd_last_error()); return 1; }
+
+  std::ifstream f(argv[2], std::ios::binary);
+  int32_t hdr[5];
+  if (!get(f, hdr, 5)) { std::printf(" mesh_file=unreadable\n"); return 1; }
+  const int32_t n_nodes = hdr[0], n_cells = hdr[1], n_bc = hdr[2], conn_len = hdr[3], bc_len = hdr[4];
+  std::vector<double> xyz(3 * (size_t)n_nodes);
+  std::vector<int32_t> cidx(n_cells + 1), conn(conn_len), bidx(n_bc + 1), bnodes(bc_len);
+  if (!get(f, xyz.data(), xyz.size()) || !get(f, cidx.data(), cidx.size()) || !get(f, conn.data(), conn.size()) ||
+      !get(f, bidx.data(), bidx.size()) || !get(f, bnodes.data(), bnodes.size())) {
+    std::printf(" mesh_file=short\n");
+    return 1;
+  }
+  fcfd_raw_mesh raw{n_nodes, xyz.data(), n_cells, cidx.data(), conn.data(), n_bc, bidx.data(), bnodes.data()};
+  fcfd_mesh *mesh = nullptr;
+  rc = fcfd_mesh_create(&raw, cs, &mesh);
+  std::printf(" mesh_rc=%d", rc);
+  if (rc) { std::printf(" error=\"%s\"\n", fcfd_last_error()); return 1; }
+  int64_t sz[8];
+  fcfd_mesh_sizes(mesh, sz);
+  std::printf(" n_cells=%lld n_faces=%lld n_ghosts=%lld", (long long)sz[0], (long long)sz[1], (long long)sz[2]);
+
+  // error path: a mesh with a cell of 7 nodes is rejected, not aborted
+  std::vector<int32_t> cidx7(cidx);
+  cidx7[1] = cidx7[0] + 7;
+  fcfd_raw_mesh raw7 = raw;
+  raw7.n_cells = 1;
+  raw7.conn_index = cidx7.data();
+  fcfd_mesh *m7 = nullptr;
+  const int rc7 = fcfd_mesh_create(&raw7, cs, &m7);
+  std::printf(" bad_mesh_rc=%d", rc7);
+  if (m7) fcfd_mesh_destroy(m7);
+
+  fcfd_ctx *ctx = nullptr;
+  rc = fcfd_ctx_create(mesh, cs, 0, &ctx);
+  std::printf(" ctx_rc=%d", rc);
+  if (rc == FCFD_OK && argc == 5) {
+    std::vector<double> W(5 * (size_t)n_cells), R(5 * (size_t)n_cells);
+    std::ifstream fw(argv[3], std::ios::binary);
+    if (!get(fw, W.data(), W.size())) { std::printf(" state_file=short\n"); return 1; }
+    rc = fcfd_residual(ctx, W.data(), R.data(), 0);
+    std::printf(" residual_rc=%d", rc);
+    std::ofstream fr(argv[4], std::ios::binary);
+    fr.write(reinterpret_cast<const char *>(R.data()), (std::streamsize)(R.size() * sizeof(double)));
+  }
+  if (ctx) fcfd_ctx_destroy(ctx);
+  fcfd_mesh_destroy(mesh);
+  fcfd_case_destroy(cs);
+  std::printf("\n");
+  return 0;
+}
