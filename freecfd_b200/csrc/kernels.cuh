@@ -206,7 +206,10 @@ template <class S> __host__ __device__ __forceinline__ S eos_T(const DevCase &c,
 template <class S> __host__ __device__ __forceinline__ S sound(const DevCase &c, S p, S T) { return sqrt(c.gamma * (p + c.Pref) / eos_rho(c, p, T)); }
 template <class S> __device__ __forceinline__ S viscosity(const DevCase &c, S T) {
   if (!c.sutherland) return S(c.mu);
-  return c.sut_mu_ref * pow((T + c.Tref) / c.sut_T_ref, 1.5) * (c.sut_T_ref + c.sut_S) / (T + c.Tref + c.sut_S);
+  // Sutherland (material.cc:126-131); t^1.5 as t * sqrt(t) (the reference's
+  // pow(t, 1.5) to rounding, at a fraction of pow's instructions)
+  const S t = (T + c.Tref) / c.sut_T_ref;
+  return c.sut_mu_ref * (t * sqrt(t)) * (c.sut_T_ref + c.sut_S) / (T + c.Tref + c.sut_S);
 }
 template <class S> __device__ __forceinline__ S therm_cond(const DevCase &c, S T) {
   if (!c.prandtl) return S(c.lambda);
@@ -225,6 +228,17 @@ struct FState {
 template <class S>
 __host__ __device__ __forceinline__ void finish(const DevCase &c, FState<S> &s, const double n[3]) {
   s.a = sound(c, s.p, s.T);
+  s.H = s.a * s.a / (c.gamma - 1.) + 0.5 * (s.V[0] * s.V[0] + s.V[1] * s.V[1] + s.V[2] * s.V[2]);
+  s.Vn = s.V[0] * n[0] + s.V[1] * n[1] + s.V[2] * n[2];
+}
+
+// finish() for a state whose rho was just set to eos_rho(p, T): the sound
+// speed reuses that density instead of recomputing it (the same doubles as
+// finish(); the low-Mach energy flux cancels so strongly that even a
+// one-rounding change of a or H shows in the residual).
+template <class S>
+__host__ __device__ __forceinline__ void finish_eos(const DevCase &c, FState<S> &s, const double n[3]) {
+  s.a = sqrt(c.gamma * (s.p + c.Pref) / s.rho);
   s.H = s.a * s.a / (c.gamma - 1.) + 0.5 * (s.V[0] * s.V[0] + s.V[1] * s.V[1] + s.V[2] * s.V[2]);
   s.Vn = s.V[0] * n[0] + s.V[1] * n[1] + s.V[2] * n[2];
 }
@@ -382,7 +396,7 @@ __device__ __forceinline__ void recon_state(const DevCase &c, const DevMesh &m, 
   s.pc = W[k]; s.Vc[0] = W[nt + k]; s.Vc[1] = W[2 * nt + k]; s.Vc[2] = W[3 * nt + k]; s.Tc = W[4 * nt + k];
   s.p = q[0]; s.V[0] = q[1]; s.V[1] = q[2]; s.V[2] = q[3]; s.T = q[4];
   s.rho = eos_rho(c, s.p, s.T);
-  finish(c, s, n);
+  finish_eos(c, s, n);
 }
 
 // ------------------------------------------------------------------ kernels
@@ -1103,20 +1117,21 @@ __device__ __forceinline__ void face_D(const DevCase &cs, const DevMesh &m, int 
       for (int i = 0; i < 12; ++i) gr[i] = S(wP * gs.at_pa(i) + wN * gs.at_nb(i));
     }
     const double l0 = m.c_x[nb] - m.c_x[pa], l1 = m.c_x[nt + nb] - m.c_x[nt + pa], l2 = m.c_x[2 * nt + nb] - m.c_x[2 * nt + pa];
-    const double lm = sqrt(l0 * l0 + l1 * l1 + l2 * l2);
-    const double e0 = l0 / lm, e1 = l1 / lm, e2 = l2 / lm;
+    const double ilm = 1. / sqrt(l0 * l0 + l1 * l1 + l2 * l2);
+    const double e0 = l0 * ilm, e1 = l1 * ilm, e2 = l2 * ilm;
     const S dc[4] = {R.Vc[0] - L.Vc[0], R.Vc[1] - L.Vc[1], R.Vc[2] - L.Vc[2], R.Tc - L.Tc};
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
       const S dn = gr[3 * q] * e0 + gr[3 * q + 1] * e1 + gr[3 * q + 2] * e2;
-      const S s = dc[q] / lm - dn;
+      const S s = dc[q] * ilm - dn;
       gr[3 * q] = gr[3 * q] + s * e0;
       gr[3 * q + 1] = gr[3 * q + 1] + s * e1;
       gr[3 * q + 2] = gr[3 * q + 2] + s * e2;
     }
     const S Vf[3] = {0.5 * (L.V[0] + R.V[0]), 0.5 * (L.V[1] + R.V[1]), 0.5 * (L.V[2] + R.V[2])};
     const S Tf = 0.5 * (L.T + R.T);
-    S mu = viscosity(cs, Tf), lam = therm_cond(cs, Tf);
+    S mu = viscosity(cs, Tf);
+    S lam = cs.prandtl ? cs.Cp * mu / cs.Pr : S(cs.lambda);  // therm_cond without a second viscosity
     if (mu_t) {
       const S mt = S(mu_t[f]);
       mu = mu + mt;
