@@ -530,8 +530,12 @@ def run_decomposed(fb, world, rank, dev, dist, steps, warmup):
 
 # 20 symmetric Gauss-Seidel sweeps: the fastest setting of both arms within a
 # few percent in a sweep-count scan (4 to 32 sweeps) on this workload
+# stop_all_rows: the solve ends when the mass, momentum and energy residuals
+# have all dropped by 1e-10 (the mass residual alone leaves the nearly passive
+# low-Mach temperature field less converged); the time of the mass residual's
+# 1e-10 drop is reported as well
 NEWTON_KW = dict(tol=1e-10, max_newton=400, cfl0=2.0, cfl_max=1e6, krylov_rtol=1e-3, precond_sweeps=20,
-                 krylov_cycles=3)
+                 krylov_cycles=3, stop_all_rows=True)
 
 
 def profile_newton(args):
@@ -581,8 +585,10 @@ def run_newton(fb, cs, mesh, case, dev, dist, reference_state=True):
         el = min(runs)
         states[label] = W
         out[label] = {"seconds": round(el, 4), "seconds_runs": runs, "converged": rep["status"] == 0,
+                      "seconds_to_mass_1e-10": round(float(rep["seconds_to_tol"]), 4),
                       "newton_iterations": rep["newton_iterations"], "krylov_iterations": rep["krylov_iterations"],
-                      "mass_residual_drop": float(rep["res_final"] / rep["res0"])}
+                      "mass_residual_drop": float(rep["res_final"] / rep["res0"]),
+                      "final_drop_mass_momentum_energy": [float(x) for x in rep["rows_final"]]}
         if "type=wall;" in case.deck and case.name == "cylinder":
             # drag coefficient of the wall (BC_1): Fx / (0.5 rho U^2 D span), D = 1
             F, _ = ns.drag(W, [0], (1.0, 0.0, 0.0), gradient=False)
@@ -595,6 +601,8 @@ def run_newton(fb, cs, mesh, case, dev, dist, reference_state=True):
     scale = np.abs(a).max(axis=0)
     scale[1:4] = np.abs(a[:, 1:4]).max()
     out["speedup_mixed_vs_plain"] = round(out["plain_fp64_fd"]["seconds"] / out["mixed_jvp_fp32"]["seconds"], 3)
+    out["speedup_mixed_vs_plain_to_mass_1e-10"] = round(
+        out["plain_fp64_fd"]["seconds_to_mass_1e-10"] / out["mixed_jvp_fp32"]["seconds_to_mass_1e-10"], 3)
     out["state_rel_diff_mixed_vs_plain"] = float((np.abs(a - b).max(axis=0) / scale).max())
     if "drag_coefficient" in out["plain_fp64_fd"]:
         cp, cm = out["plain_fp64_fd"]["drag_coefficient"], out["mixed_jvp_fp32"]["drag_coefficient"]
@@ -611,6 +619,15 @@ def run_newton(fb, cs, mesh, case, dev, dist, reference_state=True):
         out["fp64_reference_state"] = {"mass_residual_drop": float(out["plain_fp64_fd"]["mass_residual_drop"]
                                                                    * rep["res_final"] / rep["res0"]),
                                        "newton_iterations": rep["newton_iterations"]}
+        # the reference state checked in the oracle's (the reference's) own
+        # discretisation: its residual norm per equation over the seeded
+        # state's
+        import oracle
+        o = oracle.Oracle(case)
+        r_ref, r_0 = o.residual(ref), o.residual(case.state)
+        o.close()
+        out["fp64_reference_state"]["oracle_residual_drop"] = [
+            float(np.linalg.norm(r_ref[:, v]) / max(np.linalg.norm(r_0[:, v]), 1e-300)) for v in range(5)]
         for label, W in states.items():
             err = np.abs(W - ref).max(axis=0) / scale
             out[label]["state_rel_err_vs_fp64_reference"] = dict(zip(("p", "u", "v", "w", "T"), map(float, err)))

@@ -71,14 +71,16 @@ class NewtonOpts(ctypes.Structure):
                 ("krylov_rtol", ctypes.c_double), ("cfl0", ctypes.c_double), ("cfl_growth", ctypes.c_double),
                 ("cfl_max", ctypes.c_double), ("cfl_mode", ctypes.c_int32), ("ser_exponent", ctypes.c_double),
                 ("jvp_mode", ctypes.c_int32), ("fp32_krylov", ctypes.c_int32), ("max_seconds", ctypes.c_double),
-                ("precond_sweeps", ctypes.c_int32), ("krylov_cycles", ctypes.c_int32)]
+                ("precond_sweeps", ctypes.c_int32), ("krylov_cycles", ctypes.c_int32),
+                ("stop_all_rows", ctypes.c_int32)]
 
 
 class NewtonReport(ctypes.Structure):
     _fields_ = [("status", ctypes.c_int32), ("newton_iterations", ctypes.c_int32),
                 ("krylov_iterations", ctypes.c_int32), ("pad", ctypes.c_int32), ("res0", ctypes.c_double),
                 ("res_final", ctypes.c_double), ("wall_seconds", ctypes.c_double), ("last_cfl", ctypes.c_double),
-                ("history", ctypes.c_double * 512)]
+                ("history", ctypes.c_double * 512), ("rows_final", ctypes.c_double * 3),
+                ("seconds_to_tol", ctypes.c_double)]
 
 
 def _load():

@@ -242,12 +242,16 @@ typedef struct fcfd_newton_opts {
   int32_t precond_sweeps; /* symmetric multicolour block Gauss-Seidel sweeps on the first-order
                              operator (0: block-Jacobi, the block diagonal only) */
   int32_t krylov_cycles;  /* GMRES(m) restarts per Newton step (default 1) */
+  int32_t stop_all_rows;  /* 1: stop only when the momentum (x,y,z together) and energy residual
+                             norms have also dropped by tol from their initial values */
 } fcfd_newton_opts;
 
 typedef struct fcfd_newton_report {
   int32_t status, newton_iterations, krylov_iterations, pad;
   double res0, res_final, wall_seconds, last_cfl;
   double history[512];    /* |R_mass| / |R_mass(W0)| per Newton step */
+  double rows_final[3];   /* final / initial norm of the mass, momentum and energy residual */
+  double seconds_to_tol;  /* wall time when |R_mass| first dropped by tol */
 } fcfd_newton_report;
 
 /* Steady solve R(W) = 0 by pseudo-transient matrix-free Newton-Krylov on the
