@@ -80,7 +80,7 @@ class NewtonReport(ctypes.Structure):
                 ("krylov_iterations", ctypes.c_int32), ("pad", ctypes.c_int32), ("res0", ctypes.c_double),
                 ("res_final", ctypes.c_double), ("wall_seconds", ctypes.c_double), ("last_cfl", ctypes.c_double),
                 ("history", ctypes.c_double * 512), ("rows_final", ctypes.c_double * 3),
-                ("seconds_to_tol", ctypes.c_double)]
+                ("seconds_to_tol", ctypes.c_double), ("seconds_history", ctypes.c_double * 512)]
 
 
 def _load():

@@ -1135,8 +1135,8 @@ int fcfd_newton_solve(fcfd_ctx *x, double *W, const fcfd_newton_opts *o, fcfd_ne
     Krylov<double> K64;
     Krylov<float> K32;
     const bool f32 = o->fp32_krylov != 0;
-    x->newton_frozen = o->jvp_mode == 1;
-    x->newton_f32 = o->jvp_mode == 3;
+    x->newton_frozen = o->jvp_mode == 1 || o->jvp_mode == 4;
+    x->newton_f32 = o->jvp_mode == 3 || o->jvp_mode == 4;
     const int jmode = o->jvp_mode == 0 ? 0 : 1;
     if (f32) K32.alloc(x, mdim); else K64.alloc(x, mdim);
     DBuf<double> part, hh;
@@ -1170,7 +1170,10 @@ int fcfd_newton_solve(fcfd_ctx *x, double *W, const fcfd_newton_opts *o, fcfd_ne
     const int hist = (int)(sizeof(rep->history) / sizeof(rep->history[0]));
     int rejects = 0;
     for (int it = 0; it < maxit; ++it) {
-      if (it < hist) rep->history[it] = rm / r0;
+      if (it < hist) {
+        rep->history[it] = rm / r0;
+        rep->seconds_history[it] = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+      }
       if (rm <= o->tol * r0) {
         if (rep->seconds_to_tol < 0.)
           rep->seconds_to_tol = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
@@ -1345,8 +1348,8 @@ int fcfd_run(fcfd_ctx *x, double *W, const fcfd_run_opts *o, fcfd_run_report *re
     Krylov<double> K64;
     Krylov<float> K32;
     const bool f32 = o->fp32_krylov != 0;
-    x->newton_frozen = o->jvp_mode == 1;
-    x->newton_f32 = o->jvp_mode == 3;
+    x->newton_frozen = o->jvp_mode == 1 || o->jvp_mode == 4;
+    x->newton_f32 = o->jvp_mode == 3 || o->jvp_mode == 4;
     const int jmode = o->jvp_mode == 0 ? 0 : 1;
     if (f32) K32.alloc(x, mdim); else K64.alloc(x, mdim);
     DBuf<double> part, hh, lpart, hdt;

@@ -235,7 +235,8 @@ typedef struct fcfd_newton_opts {
                              kernels with the limiter held fixed (frozen-limiter Jacobian);
                              2: tangent kernels, exact (limiter differentiated too);
                              3: as 2 with the tangent chain in FP32 (mixed precision: the FP64
-                                residual stays the outer Newton residual) */
+                                residual stays the outer Newton residual);
+                             4: as 1 (limiter held fixed) with the tangent chain in FP32 */
   int32_t fp32_krylov;    /* 1: Krylov basis, preconditioner couplings, vectors and Gauss-Seidel
                              arithmetic in FP32 (dot products and Gram-Schmidt in FP64) */
   double max_seconds;     /* wall-clock cap (0: none) */
@@ -252,6 +253,7 @@ typedef struct fcfd_newton_report {
   double history[512];    /* |R_mass| / |R_mass(W0)| per Newton step */
   double rows_final[3];   /* final / initial norm of the mass, momentum and energy residual */
   double seconds_to_tol;  /* wall time when |R_mass| first dropped by tol */
+  double seconds_history[512]; /* wall time at each history[] entry */
 } fcfd_newton_report;
 
 /* Steady solve R(W) = 0 by pseudo-transient matrix-free Newton-Krylov on the
