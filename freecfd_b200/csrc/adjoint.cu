@@ -27,9 +27,11 @@
 //      over the transposed stencil (deterministic);
 //   5. ghost stage: ghost states are the first-order boundary update of the
 //      parent cell, differentiated per boundary face and gathered per cell.
-// Accumulations that cross cells without a fixed owner (limiter neighbours,
-// stale density, the global extrema) use atomics, so the last bits of Wbar can
-// vary between runs; every other sum has a fixed order.
+// Every accumulation has a fixed order, so Wbar is the same bits on every run:
+// limiter-neighbour contributions are written per (variable, face, side) and
+// gathered per cell in face order, the outlet faces' stale-density adjoints are
+// summed per target face in outlet order, and the global extrema's adjoints go
+// through per-block partial sums added by one block.
 #include <cmath>
 #include <vector>
 
@@ -136,6 +138,25 @@ __device__ int active_inputs(const DevCase &cs, int b, int act[U_N]) {
   return na;
 }
 
+// Limiter-extreme adjoints of each interior cell: the contributions its face
+// neighbours left across the shared faces (k_cell_adj's Wface, side 0 = from
+// the parent, side 1 = from the neighbour), summed in the cell's ascending
+// face order.  Writes Wlim of the interior cells; ghost entries stay zero.
+__global__ void k_wlim_gather(DevMesh m, const double *__restrict__ Wface, double *__restrict__ Wlim) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nc = m.nc, nf = m.nf;
+  if (t >= 5 * nc) return;
+  const int v = t / nc, c = t - v * nc;
+  double acc = 0.;
+  for (int j = m.cf_index[c]; j < m.cf_index[c + 1]; ++j) {
+    const int e = m.cf_list[j];
+    // c is the parent of face e: the neighbour's contribution (side 1);
+    // c is the neighbour of face ~e: the parent's (side 0)
+    acc += e >= 0 ? Wface[((size_t)v * 2 + 1) * nf + e] : Wface[((size_t)v * 2) * nf + ~e];
+  }
+  Wlim[(size_t)v * m.nt + c] = acc;
+}
+
 // Face stage: FA[i][f] = sum_v Dbar_v dD_v/du_i.
 template <bool VISCOUS, int FX>
 __global__ void __launch_bounds__(128) k_face_adj(DevCase cs, DevMesh m, const double *__restrict__ W,
@@ -182,20 +203,19 @@ __global__ void __launch_bounds__(128) k_face_adj(DevCase cs, DevMesh m, const d
 // earlier face (cached_right_rho) hands that adjoint to the earlier face.
 template <bool VISCOUS, int FX>
 __global__ void k_stale_adj(DevCase cs, DevMesh m, const double *__restrict__ W, const double *__restrict__ G,
-                            const double *__restrict__ Lm, const double *__restrict__ stale, double *__restrict__ FA) {
+                            const double *__restrict__ Lm, const double *__restrict__ stale, const double *__restrict__ FA,
+                            double *__restrict__ SC, int *__restrict__ tgt) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= m.n_outlet) return;
   const int nf = m.nf;
   const int f = m.outlet_faces[i];
   const double sb = FA[(size_t)U_STALE * nf + f];
-  if (sb == 0.) return;
-  // walk back exactly as cached_right_rho does
+  // walk back exactly as cached_right_rho does; the target is recorded even
+  // when this face's seed is zero, so that faces sharing a target stay one run
   for (int g = f - 1; g >= 0; --g) {
     const double n[3] = {m.f_n[g], m.f_n[nf + g], m.f_n[2 * nf + g]};
     const double A = m.f_area[g];
     const int pa = m.f_parent[g], nb = m.f_neighbor[g], b = m.f_bc[g];
-    double u[U_N];
-    face_inputs(m, g, b, pa, nb, W, G, Lm, stale, u);
     bool sets = true;
     if (b >= 0) {
       FState<double> L, R;
@@ -207,6 +227,10 @@ __global__ void k_stale_adj(DevCase cs, DevMesh m, const double *__restrict__ W,
       sets = apply_bc(cs, cs.bc[b], L, R, n, (int *)nullptr);
     }
     if (!sets) continue;
+    tgt[i] = g;
+    if (sb == 0.) return;
+    double u[U_N];
+    face_inputs(m, g, b, pa, nb, W, G, Lm, stale, u);
     int act[U_N];
     const int na = active_inputs<VISCOUS>(cs, b, act);
     for (int k0 = 0; k0 < na; k0 += kLanes) {
@@ -216,9 +240,29 @@ __global__ void k_stale_adj(DevCase cs, DevMesh m, const double *__restrict__ W,
       DA D[5], rhoR;
       face_from_inputs<VISCOUS, FX>(cs, m, g, n, A, b, pa, nb, in, D, rhoR);
       for (int l = 0; l < kLanes; ++l)
-        if (in.chunk[l] >= 0 && rhoR.d[l] != 0.) atomicAdd(&FA[(size_t)in.chunk[l] * nf + g], sb * rhoR.d[l]);
+        if (in.chunk[l] >= 0) SC[(size_t)in.chunk[l] * m.n_outlet + i] = sb * rhoR.d[l];
     }
     return;
+  }
+}
+
+// Adds the outlet faces' stale-density adjoints to the faces whose right
+// density they read.  Outlet faces are in ascending face order and so are
+// their targets (the last earlier face that sets the density), so the faces
+// sharing a target form one contiguous run: its first thread sums the run in
+// order and is the only writer of that target's adjoints (deterministic).
+__global__ void k_stale_apply(int n_outlet, int nf, const double *__restrict__ SC, const int *__restrict__ tgt,
+                              double *__restrict__ FA) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_outlet) return;
+  const int g = tgt[i];
+  if (g < 0 || (i > 0 && tgt[i - 1] == g)) return;
+  int j1 = i + 1;
+  while (j1 < n_outlet && tgt[j1] == g) ++j1;
+  for (int k = 0; k < U_N; ++k) {
+    double acc = 0.;
+    for (int j = i; j < j1; ++j) acc += SC[(size_t)k * n_outlet + j];
+    if (acc != 0.) FA[(size_t)k * nf + g] += acc;
   }
 }
 
@@ -249,14 +293,15 @@ __device__ __forceinline__ S lim_ratio(int limiter, const S &u0, const S &g0, co
 }
 
 // Cell stage (with the limiter adjoint).  Outputs the cell's own state and
-// gradient adjoints; neighbour / extrema contributions go to Wlim (atomics)
-// and to per-block partial sums of the eps^2 adjoints.
+// gradient adjoints; the contribution to the neighbour holding a limiter's
+// extreme goes to Wface (one slot per variable, face and side, so no two
+// threads write one slot) and the eps^2 adjoints to per-block partial sums.
 template <bool VISCOUS>
 __global__ void __launch_bounds__(128) k_cell_adj(DevCase cs, DevMesh m, const double *__restrict__ W,
                                                   const double *__restrict__ G, const double *__restrict__ Lm,
                                                   const unsigned long long *__restrict__ ext, const double *__restrict__ FA,
                                                   double *__restrict__ Wcell, double *__restrict__ Gb,
-                                                  double *__restrict__ Wlim, double *__restrict__ e2part) {
+                                                  double *__restrict__ Wface, double *__restrict__ e2part) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   const int nc = m.nc, nt = m.nt, nf = m.nf;
   double e2b[5] = {0., 0., 0., 0., 0.};
@@ -408,7 +453,9 @@ __global__ void __launch_bounds__(128) k_cell_adj(DevCase cs, DevMesh m, const d
         const D6 r = lim_ratio<D6>(cs.limiter, a0, a1, a2, a3, a4, a5, bcf);
         wb[v] += s * r.d[0];
         gb[3 * v] += s * r.d[1]; gb[3 * v + 1] += s * r.d[2]; gb[3 * v + 2] += s * r.d[3];
-        if (bx != c) atomicAdd(&Wlim[(size_t)v * nt + bx], s * r.d[4]);
+        // the extreme sits across face bf: this cell's contribution to it,
+        // kept per (variable, face, side) and gathered in face order later
+        if (bx != c) Wface[((size_t)v * 2 + (m.f_parent[bf] == c ? 0 : 1)) * nf + bf] = s * r.d[4];
         e2b[v] += s * r.d[5];
       }
     }
@@ -599,7 +646,8 @@ __global__ void k_rearm(unsigned long long *ext, int *argx) {
 
 struct AdjBufs {
   DBuf<double> FA, Wcell, Gb, Wlim, Wgrad, GA, e2part, Rb, out;
-  DBuf<int> tr_index, tr_cell;
+  DBuf<double> Wface, SC;  // per-face-side limiter contributions; outlet faces' stale-density adjoints
+  DBuf<int> tr_index, tr_cell, tgt;
   bool ready = false;
 };
 
@@ -637,6 +685,9 @@ static AdjBufs &adj_bufs(fcfd_ctx *x) {
   a.Wcell.alloc(5 * (size_t)nc);
   a.Gb.alloc(15 * (size_t)nc);
   a.Wlim.alloc(5 * (size_t)nt);
+  a.Wface.alloc(10 * (size_t)m.nf);
+  a.SC.alloc((size_t)U_N * std::max(m.n_outlet, 1));
+  a.tgt.alloc((size_t)std::max(m.n_outlet, 1));
   a.Wgrad.alloc(5 * (size_t)nt);
   a.GA.alloc(5 * (size_t)std::max(m.nb, 1));
   a.e2part.alloc(5 * (size_t)((nc + 127) / 128 + 1));
@@ -669,14 +720,20 @@ static void run_adjoint(fcfd_ctx *x, const double *Rbar_soa, unsigned int mask, 
   else
     FCFD_BY_FLUX(x->cs.flux, k_face_adj<false, FX><<<gf, 128, 0, s>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p, Rbar_soa, mask, dir[0], dir[1], dir[2], a.FA.p));
   if (m.n_outlet > 0) {
-    if (x->viscous) FCFD_BY_FLUX(x->cs.flux, k_stale_adj<true, FX><<<(m.n_outlet + 127) / 128, 128, 0, s>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p, a.FA.p));
-    else FCFD_BY_FLUX(x->cs.flux, k_stale_adj<false, FX><<<(m.n_outlet + 127) / 128, 128, 0, s>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p, a.FA.p));
+    const int go = (m.n_outlet + 127) / 128;
+    CK(cudaMemsetAsync(a.SC.p, 0, sizeof(double) * U_N * (size_t)m.n_outlet, s));
+    CK(cudaMemsetAsync(a.tgt.p, 0xFF, sizeof(int) * (size_t)m.n_outlet, s));
+    if (x->viscous) FCFD_BY_FLUX(x->cs.flux, k_stale_adj<true, FX><<<go, 128, 0, s>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p, a.FA.p, a.SC.p, a.tgt.p));
+    else FCFD_BY_FLUX(x->cs.flux, k_stale_adj<false, FX><<<go, 128, 0, s>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p, a.FA.p, a.SC.p, a.tgt.p));
+    k_stale_apply<<<go, 128, 0, s>>>(m.n_outlet, m.nf, a.SC.p, a.tgt.p, a.FA.p);
   }
   CK(cudaMemsetAsync(a.Wlim.p, 0, sizeof(double) * 5 * (size_t)m.nt, s));
+  CK(cudaMemsetAsync(a.Wface.p, 0, sizeof(double) * 10 * (size_t)m.nf, s));
   if (x->viscous)
-    k_cell_adj<true><<<gc, 128, 0, s>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, x->ext.p, a.FA.p, a.Wcell.p, a.Gb.p, a.Wlim.p, a.e2part.p);
+    k_cell_adj<true><<<gc, 128, 0, s>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, x->ext.p, a.FA.p, a.Wcell.p, a.Gb.p, a.Wface.p, a.e2part.p);
   else
-    k_cell_adj<false><<<gc, 128, 0, s>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, x->ext.p, a.FA.p, a.Wcell.p, a.Gb.p, a.Wlim.p, a.e2part.p);
+    k_cell_adj<false><<<gc, 128, 0, s>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, x->ext.p, a.FA.p, a.Wcell.p, a.Gb.p, a.Wface.p, a.e2part.p);
+  k_wlim_gather<<<(5 * m.nc + 255) / 256, 256, 0, s>>>(m, a.Wface.p, a.Wlim.p);
   if (need_ext) k_e2_adj<<<1, 32, 0, s>>>(x->cs, m, P.W.p, x->ext.p, x->argx.p, a.e2part.p, gc, a.Wlim.p);
   k_grad_adj<<<(m.nt + 127) / 128, 128, 0, s>>>(m, a.tr_index.p, a.tr_cell.p, a.Gb.p, a.Wgrad.p);
   if (m.nb > 0) k_ghost_adj<<<(m.nb + 127) / 128, 128, 0, s>>>(x->cs, m, P.W.p, a.FA.p, a.Wgrad.p, a.Wlim.p, a.GA.p);
