@@ -476,6 +476,8 @@ def run_ours(args):
         line["decomposed"] = run_decomposed(fb, world, rank, dev, dist, args.steps, args.warmup)
     if not args.no_newton and not rans:
         line["newton"] = run_newton(fb, cs, mesh, case, dev, dist)
+        if args.workload == "cylinder" and world == 1:
+            line["rans_newton"] = run_rans_newton(fb, dev)
     if rank == 0 and world == 1 and not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline(case, args.cpu_seconds, args.ref_workers)
     if rank == 0:
@@ -530,12 +532,24 @@ def run_decomposed(fb, world, rank, dev, dist, steps, warmup):
 
 # 20 symmetric Gauss-Seidel sweeps: the fastest setting of both arms within a
 # few percent in a sweep-count scan (4 to 32 sweeps) on this workload
-# stop_all_rows: the solve ends when the mass, momentum and energy residuals
-# have all dropped by 1e-10 (the mass residual alone leaves the nearly passive
-# low-Mach temperature field less converged); the time of the mass residual's
-# 1e-10 drop is reported as well
-NEWTON_KW = dict(tol=1e-10, max_newton=400, cfl0=2.0, cfl_max=1e6, krylov_rtol=1e-3, precond_sweeps=20,
+# The metric's time is the wall time to a 1e-10 drop of the mass residual.
+# The solve then continues (final tightening) until the mass, momentum and
+# energy residuals have all dropped by 1e-11 (stop_all_rows): the mass
+# residual alone leaves the nearly passive low-Mach temperature field less
+# converged, and the tightened state is the one compared with the FP64
+# reference state.
+NEWTON_TIME_TOL = 1e-10
+NEWTON_KW = dict(tol=1e-11, max_newton=400, cfl0=2.0, cfl_max=1e6, krylov_rtol=1e-3, precond_sweeps=20,
                  krylov_cycles=3, stop_all_rows=True)
+
+
+def time_to_drop(rep, drop):
+    """Wall seconds of the first Newton step whose mass residual drop is at
+    or below `drop` (from the solve's per-step history)."""
+    for h, t in zip(rep["history"], rep["seconds_history"]):
+        if h <= drop:
+            return float(t)
+    return -1.0
 
 
 def profile_newton(args):
@@ -572,20 +586,22 @@ def run_newton(fb, cs, mesh, case, dev, dist, reference_state=True):
         # two timed solves from the same seeded state (identical iterations);
         # the faster is reported, both are listed (host-side launch and
         # synchronisation noise differs between boxes)
-        runs = []
+        runs, runs_tol = [], []
         for _ in range(2 if NEWTON_KW["max_newton"] > 10 else 1):
             t0 = time.perf_counter()
             W, rep = ns.newton_solve(case.state, **NEWTON_KW, raise_on_fail=False, **opts)
             el = time.perf_counter() - t0
+            el_tol = time_to_drop(rep, NEWTON_TIME_TOL)
             if dist:
-                x = torch.tensor([el], device="cuda", dtype=torch.float64)
+                x = torch.tensor([el, el_tol], device="cuda", dtype=torch.float64)
                 dist.all_reduce(x, op=dist.ReduceOp.MAX)
-                el = float(x.item())
+                el, el_tol = (float(v) for v in x.cpu())
             runs.append(round(el, 4))
+            runs_tol.append(round(el_tol, 4))
         el = min(runs)
         states[label] = W
-        out[label] = {"seconds": round(el, 4), "seconds_runs": runs, "converged": rep["status"] == 0,
-                      "seconds_to_mass_1e-10": round(float(rep["seconds_to_tol"]), 4),
+        out[label] = {"seconds_to_mass_1e-10": min(runs_tol), "seconds_to_mass_1e-10_runs": runs_tol,
+                      "seconds_with_tightening": round(el, 4), "seconds_runs": runs, "converged": rep["status"] == 0,
                       "newton_iterations": rep["newton_iterations"], "krylov_iterations": rep["krylov_iterations"],
                       "mass_residual_drop": float(rep["res_final"] / rep["res0"]),
                       "final_drop_mass_momentum_energy": [float(x) for x in rep["rows_final"]]}
@@ -600,9 +616,10 @@ def run_newton(fb, cs, mesh, case, dev, dist, reference_state=True):
     a, b = states["plain_fp64_fd"], states["mixed_jvp_fp32"]
     scale = np.abs(a).max(axis=0)
     scale[1:4] = np.abs(a[:, 1:4]).max()
-    out["speedup_mixed_vs_plain"] = round(out["plain_fp64_fd"]["seconds"] / out["mixed_jvp_fp32"]["seconds"], 3)
-    out["speedup_mixed_vs_plain_to_mass_1e-10"] = round(
+    out["speedup_mixed_vs_plain"] = round(
         out["plain_fp64_fd"]["seconds_to_mass_1e-10"] / out["mixed_jvp_fp32"]["seconds_to_mass_1e-10"], 3)
+    out["speedup_mixed_vs_plain_with_tightening"] = round(
+        out["plain_fp64_fd"]["seconds_with_tightening"] / out["mixed_jvp_fp32"]["seconds_with_tightening"], 3)
     out["state_rel_diff_mixed_vs_plain"] = float((np.abs(a - b).max(axis=0) / scale).max())
     if "drag_coefficient" in out["plain_fp64_fd"]:
         cp, cm = out["plain_fp64_fd"]["drag_coefficient"], out["mixed_jvp_fp32"]["drag_coefficient"]
@@ -632,6 +649,52 @@ def run_newton(fb, cs, mesh, case, dev, dist, reference_state=True):
             err = np.abs(W - ref).max(axis=0) / scale
             out[label]["state_rel_err_vs_fp64_reference"] = dict(zip(("p", "u", "v", "w", "T"), map(float, err)))
     out["settings"] = dict(NEWTON_KW)
+    return out
+
+
+# coupled flow + k-omega Newton-Krylov on the turbulent plate: SER on the
+# largest per-equation drop, k and omega clipped at their lower limits
+RANS_NEWTON_KW = dict(tol=1e-10, max_newton=400, cfl0=1.0, cfl_max=1e6, krylov_dim=40, krylov_rtol=1e-2,
+                      cfl_mode=2, stop_all_rows=True)
+
+
+def run_rans_newton(fb, dev):
+    """Config 5 (k-omega flat plate 384x192x4): the coupled Newton solve from
+    the seeded state with FP64 finite-difference J.v (plain) and with the
+    FP32 coupled tangent chain (mixed), the same settings and step cap; wall
+    time, per-equation residual drops, and the skin-friction drag coefficient
+    of the no-slip wall (BC_3) of each arm."""
+    import tempfile
+    case = make_case("plate_rans")
+    cs = fb.Case(case.write_deck(tempfile.mkdtemp(prefix="fcfd_bench_")))
+    mesh = fb.Mesh(case.mesh, cs)
+    p, U, T = case.freestream[0], case.freestream[1], case.freestream[4]
+    rho = p / (287.0 * T)
+    nodes = case.mesh.nodes
+    span = float(np.ptp(nodes[:, 2]))
+    out, states = {}, {}
+    for label, kw in (("plain_fp64_fd", {}), ("mixed_jvp_fp32", dict(fp32_jvp=True))):
+        ns = fb.NavierStokes(mesh, cs, dev)
+        t0 = time.perf_counter()
+        W, K, rep = ns.rans_newton_solve(case.state, case.kstate, raise_on_fail=False, **RANS_NEWTON_KW, **kw)
+        el = time.perf_counter() - t0
+        F, _ = ns.drag(W, [2], (1.0, 0.0, 0.0), gradient=False)
+        cf = float(F[0] / (0.5 * rho * U * U * 2.0 * span))
+        states[label] = (W, K)
+        out[label] = {"seconds": round(el, 3), "converged": rep["status"] == 0, "newton_iterations": rep["newton_iterations"],
+                      "krylov_iterations": rep["krylov_iterations"],
+                      "final_drop_mass_momentum_energy": [float(v) for v in rep["rows_final"]],
+                      "final_drop_k_omega": [float(v) for v in rep["kw_final"]],
+                      "skin_friction_drag_coefficient": cf}
+        del ns
+    (Wa, Ka), (Wb, Kb) = states["plain_fp64_fd"], states["mixed_jvp_fp32"]
+    out["state_rel_diff_mixed_vs_plain"] = float(max((np.abs(Wa - Wb).max(axis=0) / np.abs(Wa).max(axis=0)).max(),
+                                                    (np.abs(Ka - Kb).max(axis=0) / np.abs(Ka).max(axis=0)).max()))
+    ca, cb = out["plain_fp64_fd"]["skin_friction_drag_coefficient"], out["mixed_jvp_fp32"]["skin_friction_drag_coefficient"]
+    out["skin_friction_rel_diff_mixed_vs_plain"] = abs(cb - ca) / abs(ca)
+    out["speedup_mixed_vs_plain"] = round(out["plain_fp64_fd"]["seconds"] / out["mixed_jvp_fp32"]["seconds"], 3)
+    out["workload"] = case.workload
+    out["settings"] = dict(RANS_NEWTON_KW)
     return out
 
 

@@ -28,7 +28,7 @@ EXPORTED = [
     "fcfd_time_residual", "fcfd_point_flux", "fcfd_jvp", "fcfd_vjp", "fcfd_drag", "fcfd_rans_residual", "fcfd_rans_bcs", "fcfd_time_rans", "fcfd_newton_solve", "fcfd_local_dt_cflmax_noalloc",
     "fcfd_run", "fcfd_restart_write", "fcfd_restart_read", "fcfd_mesh_from_tecplot", "fcfd_rans_jvp",
     "fcfd_partition_sets", "fcfd_ctx_set_partition", "fcfd_partition_extrema", "fcfd_partition_residual",
-    "fcfd_ctx_stream", "fcfd_diag_blocks",
+    "fcfd_ctx_stream", "fcfd_diag_blocks", "fcfd_rans_newton_solve",
 ]
 
 
@@ -80,7 +80,8 @@ class NewtonReport(ctypes.Structure):
                 ("krylov_iterations", ctypes.c_int32), ("pad", ctypes.c_int32), ("res0", ctypes.c_double),
                 ("res_final", ctypes.c_double), ("wall_seconds", ctypes.c_double), ("last_cfl", ctypes.c_double),
                 ("history", ctypes.c_double * 512), ("rows_final", ctypes.c_double * 3),
-                ("seconds_to_tol", ctypes.c_double), ("seconds_history", ctypes.c_double * 512)]
+                ("seconds_to_tol", ctypes.c_double), ("seconds_history", ctypes.c_double * 512),
+                ("kw_final", ctypes.c_double * 2)]
 
 
 def _load():
@@ -135,6 +136,7 @@ def _load():
     L.fcfd_partition_residual.argtypes = [vp, vp, vp, ctypes.c_int]
     L.fcfd_ctx_stream.argtypes = [vp, ctypes.POINTER(vp)]
     L.fcfd_diag_blocks.argtypes = [vp, dp, dp, dp]
+    L.fcfd_rans_newton_solve.argtypes = [vp, dp, dp, ctypes.POINTER(NewtonOpts), ctypes.POINTER(NewtonReport)]
     for name in EXPORTED:
         getattr(L, name)
     return L

@@ -177,6 +177,10 @@ inline void launch_faces(fcfd_ctx *x, Pipe<S> &P, const S *mu_t, S *mo, S *wo, c
     FCFD_BY_FLUX(x->cs.flux, k_face_flux<S, false, FX, false, PART><<<g, 128, 0, s>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p, mu_t, P.D.p, mo, wo, x->err.p));
   if (side) CK(cudaStreamWaitEvent(s, x->ev_join, 0));
 }
+// newton.cu: inverse flow-equation blocks of the block-Jacobi preconditioner
+// at the state of the last residual chain (see there).
+void ns_block_inverse(fcfd_ctx *x, const double *Wn, const double *vol, const double *dt, const double *mutf,
+                      double *JL, double *JR, double *Minv, double *rowmag);
 void adjoint_free(fcfd_ctx *x);
 void rans_setup(fcfd_ctx *x);
 void rans_free(fcfd_ctx *x);

@@ -72,7 +72,8 @@ __device__ __forceinline__ void lift(const FState<double> &s, FState<D5> &o) {
 template <bool VISCOUS, int FX>
 __global__ void __launch_bounds__(128) k_face_jac(DevCase cs, DevMesh m, const double *__restrict__ W, const double *__restrict__ G,
                                                   const double *__restrict__ Lm, const double *__restrict__ stale,
-                                                  double *__restrict__ JL, double *__restrict__ JR) {
+                                                  double *__restrict__ JL, double *__restrict__ JR,
+                                                  const double *__restrict__ mutf = nullptr) {
   const int f = blockIdx.x * blockDim.x + threadIdx.x;
   const int nf = m.nf;
   if (f >= nf) return;
@@ -93,7 +94,7 @@ __global__ void __launch_bounds__(128) k_face_jac(DevCase cs, DevMesh m, const d
     if (!apply_bc(cs, cs.bc[b], Ld, Rd, n, (int *)nullptr)) Rd.rho = D5(R.rho);
     finish(cs, Rd, n);
   }
-  face_D<D5, GlobalGrad<double>, VISCOUS, FX>(cs, m, f, n, A, b, pa, nb, Ld, Rd, gs, (const double *)nullptr, D, wl);
+  face_D<D5, GlobalGrad<double>, VISCOUS, FX>(cs, m, f, n, A, b, pa, nb, Ld, Rd, gs, mutf, D, wl);
 #pragma unroll
   for (int i = 0; i < 5; ++i)
 #pragma unroll
@@ -101,7 +102,7 @@ __global__ void __launch_bounds__(128) k_face_jac(DevCase cs, DevMesh m, const d
   if (b < 0) {
     lift(L, Ld);
     seed(R, Rd, cs, n);
-    face_D<D5, GlobalGrad<double>, VISCOUS, FX>(cs, m, f, n, A, b, pa, nb, Ld, Rd, gs, (const double *)nullptr, D, wl);
+    face_D<D5, GlobalGrad<double>, VISCOUS, FX>(cs, m, f, n, A, b, pa, nb, Ld, Rd, gs, mutf, D, wl);
 #pragma unroll
     for (int i = 0; i < 5; ++i)
 #pragma unroll
@@ -926,13 +927,32 @@ static void alloc_state(fcfd_ctx *x, NewtonState &ns, int sweeps, int cycles, bo
 
 // First-order face Jacobians JL, JR [25][nf] at the state of the last residual
 // chain run on x->p64 (states, gradients, limiters and stale densities).
-static void launch_face_jac(fcfd_ctx *x, double *JL, double *JR) {
+// mutf: face eddy viscosities of a turbulent case (added to the viscosity of
+// the viscous flux), or null.
+static void launch_face_jac(fcfd_ctx *x, double *JL, double *JR, const double *mutf = nullptr) {
   const DevMesh &m = x->dm;
   cudaStream_t s = x->stream;
   if (x->viscous)
-    FCFD_BY_FLUX(x->cs.flux, k_face_jac<true, FX><<<(m.nf + 127) / 128, 128, 0, s>>>(x->cs, m, x->p64.W.p, x->p64.G.p, x->p64.Lm.p, x->p64.stale.p, JL, JR));
+    FCFD_BY_FLUX(x->cs.flux, k_face_jac<true, FX><<<(m.nf + 127) / 128, 128, 0, s>>>(x->cs, m, x->p64.W.p, x->p64.G.p, x->p64.Lm.p, x->p64.stale.p, JL, JR, mutf));
   else
-    FCFD_BY_FLUX(x->cs.flux, k_face_jac<false, FX><<<(m.nf + 127) / 128, 128, 0, s>>>(x->cs, m, x->p64.W.p, x->p64.G.p, x->p64.Lm.p, x->p64.stale.p, JL, JR));
+    FCFD_BY_FLUX(x->cs.flux, k_face_jac<false, FX><<<(m.nf + 127) / 128, 128, 0, s>>>(x->cs, m, x->p64.W.p, x->p64.G.p, x->p64.Lm.p, x->p64.stale.p, JL, JR, mutf));
+}
+
+// Inverse block-Jacobi blocks (V P/dt - J_cc)^-1 [25][nc] of the flow
+// equations at the state of the last residual chain run on x->p64 (Wn its
+// [5][nc] copy), with the face eddy viscosities mutf of a turbulent case
+// (null: laminar).  JL, JR: [25][nf] scratch.  Used by the coupled k-omega
+// Newton solve (rans.cu).
+void ns_block_inverse(fcfd_ctx *x, const double *Wn, const double *vol, const double *dt, const double *mutf,
+                      double *JL, double *JR, double *Minv, double *rowmag) {
+  const DevMesh &m = x->dm;
+  cudaStream_t s = x->stream;
+  CK(cudaMemsetAsync(JR, 0, sizeof(double) * 25 * (size_t)m.nf, s));
+  launch_face_jac(x, JL, JR, mutf);
+  RowScale wref;
+  for (int v = 0; v < 5; ++v) wref.s[v] = 1.;
+  k_block_jacobi<<<(m.nc + 255) / 256, 256, 0, s>>>(x->cs, m, Wn, vol, dt, JL, JR, Minv, x->err.p, wref, rowmag);
+  CK(cudaGetLastError());
 }
 
 // One linearised backward-Euler solve at the state the last residual loaded

@@ -11,7 +11,9 @@
 // (inlets) and the parent value otherwise: the RANS update_boundaries is
 // missing from the reference snapshot and is reconstructed like the NS one.
 #include <algorithm>
+#include <chrono>
 #include <cmath>
+#include <cstring>
 #include <vector>
 
 #include "ctx.hpp"
@@ -475,6 +477,524 @@ extern "C" int fcfd_rans_bcs(const fcfd_ctx *x, double *out, int32_t out_len) {
     const DevBC &o = x->cs.bc[b];
     out[5 * b] = o.kw_fixed; out[5 * b + 1] = o.k_bc; out[5 * b + 2] = o.omega_bc;
     out[5 * b + 3] = o.mut_fixed; out[5 * b + 4] = o.mut_bc;
+  }
+  return FCFD_OK;
+}
+
+// ------------------------------------------------------------------ coupled k-omega Newton-Krylov
+//
+// Steady solve of the coupled flow + k-omega residual F(X) = (R(W, K), RK(W, K))
+// by pseudo-transient Newton-Krylov: (D - dF/dX) dX = F(X), X += alpha dX,
+// with D the time terms (V P/dt for the flow equations, ns_time_terms.cc:
+// 107-186; rho V/dt on both k-omega rows, rans_time_terms.cc:25-87) and the
+// local time step of the flow (time_step.cc:143-224).  The reference solves
+// the two systems one after the other (NavierStokes::solve then RANS::solve,
+// ns.cc:104-118, rans.cc:85-98); here they are one Newton system on
+// X = [p u v w T k omega] (SoA [7][nc]).  J.v: a finite difference of the
+// FP64 coupled residual, or the coupled tangent chain in FP32 (the mixed
+// arm).  Preconditioner: block Jacobi, the flow blocks from the first-order
+// face Jacobians with the face eddy viscosities (newton.cu), the k and omega
+// rows by a diagonal of the time term, the first-order upwind convection and
+// diffusion across the cell's faces and the destruction terms' derivatives.
+// GMRES(m), right preconditioned, FP64 classical Gram-Schmidt twice, each
+// equation weighted by the inverse of its initial residual norm.
+namespace fcfd {
+namespace kwn {
+
+constexpr int kNv = 7;
+constexpr int kRedBlk = 592;  // 4 x 148 blocks for the reductions
+
+// X (SoA [7][nc]) + eps z -> the chain's W [5][nt] and K [2][nt] (interiors)
+__global__ void k_x_load(int nc, int nt, const double *__restrict__ X, const double *__restrict__ z, double eps,
+                         double *__restrict__ W, double *__restrict__ K) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nc) return;
+#pragma unroll
+  for (int v = 0; v < 5; ++v) W[v * nt + c] = X[v * nc + c] + (z ? eps * z[v * nc + c] : 0.);
+#pragma unroll
+  for (int v = 0; v < 2; ++v) K[v * nt + c] = X[(5 + v) * nc + c] + (z ? eps * z[(5 + v) * nc + c] : 0.);
+}
+
+// X and the direction z as FP32 duals of the tangent chain
+__global__ void k_x_load_dual(int nc, int nt, const double *__restrict__ X, const double *__restrict__ z,
+                              Dual<float> *__restrict__ W, Dual<float> *__restrict__ K) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nc) return;
+#pragma unroll
+  for (int v = 0; v < 5; ++v) W[v * nt + c] = Dual<float>(float(X[v * nc + c]), float(z[v * nc + c]));
+#pragma unroll
+  for (int v = 0; v < 2; ++v) K[v * nt + c] = Dual<float>(float(X[(5 + v) * nc + c]), float(z[(5 + v) * nc + c]));
+}
+
+// k-omega residual AoS [nc][2] -> planes 5, 6 of F
+__global__ void k_rk_planes(int nc, const double *__restrict__ RK, double *__restrict__ F) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nc) return;
+  F[5 * nc + c] = RK[2 * c];
+  F[6 * nc + c] = RK[2 * c + 1];
+}
+
+// tangent parts of the FP32 chain's outputs -> Jz [7][nc]
+__global__ void k_dual_planes(int nc, const Dual<float> *__restrict__ R, const Dual<float> *__restrict__ RK,
+                              double *__restrict__ Jz) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nc) return;
+#pragma unroll
+  for (int v = 0; v < 5; ++v) Jz[v * nc + c] = double(R[v * nc + c].d);
+  Jz[5 * nc + c] = double(RK[2 * c].d);
+  Jz[6 * nc + c] = double(RK[2 * c + 1].d);
+}
+
+// y = wr * (D z - Jz): D the time terms; Jz = (F1 - F0) * inv_eps, or the
+// tangent (F0 null).  wr: per-equation weights.
+struct Wt7 {
+  double s[kNv];
+};
+__global__ void k_kw_matvec(DevCase cs, int nc, const double *__restrict__ X, const double *__restrict__ vol,
+                            const double *__restrict__ dt, const double *__restrict__ z, const double *__restrict__ F1,
+                            const double *__restrict__ F0, double inv_eps, Wt7 wr, double *__restrict__ y) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nc) return;
+  const double p = X[c], u = X[nc + c], v = X[2 * nc + c], w = X[3 * nc + c], T = X[4 * nc + c];
+  const double pressure = p + cs.Pref, temperature = T + cs.Tref;
+  const double rho = pressure / (cs.R * temperature);
+  const double drho_dT = -1. * rho / temperature, drho_dp = rho / pressure;
+  const double H = cs.Cp * temperature + 0.5 * (u * u + v * v + w * w);
+  const double s = vol[c] / dt[c];
+  double zv[kNv];
+#pragma unroll
+  for (int k = 0; k < kNv; ++k) zv[k] = z[k * nc + c];
+  double Dz[kNv];
+  Dz[0] = s * (drho_dp * zv[0] + drho_dT * zv[4]);
+  Dz[1] = s * (drho_dp * u * zv[0] + rho * zv[1] + drho_dT * u * zv[4]);
+  Dz[2] = s * (drho_dp * v * zv[0] + rho * zv[2] + drho_dT * v * zv[4]);
+  Dz[3] = s * (drho_dp * w * zv[0] + rho * zv[3] + drho_dT * w * zv[4]);
+  Dz[4] = s * ((drho_dp * H - 1.) * zv[0] + rho * u * zv[1] + rho * v * zv[2] + rho * w * zv[3] +
+               (drho_dT * H + rho * cs.Cp) * zv[4]);
+  Dz[5] = s * rho * zv[5];
+  Dz[6] = s * rho * zv[6];
+#pragma unroll
+  for (int k = 0; k < kNv; ++k) {
+    const double jz = F0 ? (F1[k * nc + c] - F0[k * nc + c]) * inv_eps : F1[k * nc + c];
+    y[k * nc + c] = wr.s[k] * (Dz[k] - jz);
+  }
+}
+
+// Diagonal of the k and omega rows: rho V/dt, the outflow and diffusion
+// coefficients over the cell's faces (first-order upwind convection with the
+// faces' mass fluxes, (mu + sigma mu_t) A / |l2r|) and the derivatives of
+// the destruction terms (beta* rho omega for k, 2 beta rho omega for omega).
+__global__ void k_kw_diag(DevCase cs, DevMesh m, const double *__restrict__ X, const double *__restrict__ vol,
+                          const double *__restrict__ dt, const double *__restrict__ mdot, const double *__restrict__ mutf,
+                          double *__restrict__ dk) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nc = m.nc, nt = m.nt, nf = m.nf;
+  if (c >= nc) return;
+  const double p = X[c], T = X[4 * nc + c], om = X[6 * nc + c];
+  const double rho = (p + cs.Pref) / (cs.R * (T + cs.Tref));
+  const double mu = viscosity(cs, T);
+  double conv = 0., dk0 = 0., dk1 = 0.;
+  for (int j = m.cf_index[c]; j < m.cf_index[c + 1]; ++j) {
+    const int e = m.cf_list[j];
+    const int f = e >= 0 ? e : ~e;
+    const double A = m.f_area[f];
+    const double out = (e >= 0 ? mdot[f] : -mdot[f]) * A;  // mass leaving the cell through f
+    if (out > 0.) conv += out;
+    const int o = e >= 0 ? m.f_neighbor[f] : m.f_parent[f];
+    const double l0 = m.c_x[o] - m.c_x[c], l1 = m.c_x[nt + o] - m.c_x[nt + c], l2 = m.c_x[2 * nt + o] - m.c_x[2 * nt + c];
+    const double il = A / sqrt(l0 * l0 + l1 * l1 + l2 * l2);
+    dk0 += (mu + KOmega::sigma_k * mutf[f]) * il;
+    dk1 += (mu + KOmega::sigma_omega * mutf[f]) * il;
+  }
+  const double t = rho * vol[c] / dt[c];
+  dk[c] = t + conv + dk0 + KOmega::beta_star * rho * om * vol[c];
+  dk[nc + c] = t + conv + dk1 + 2. * KOmega::beta * rho * om * vol[c];
+}
+
+// z = M^-1 v: flow rows through the inverse blocks, k and omega rows by the
+// diagonal; v carries the equation weights wr (removed first).
+__global__ void k_kw_prec(int nc, const double *__restrict__ Minv, const double *__restrict__ dk, Wt7 iwr,
+                          const double *__restrict__ v, double *__restrict__ z) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nc) return;
+  double b[5];
+#pragma unroll
+  for (int k = 0; k < 5; ++k) b[k] = iwr.s[k] * v[k * nc + c];
+#pragma unroll
+  for (int i = 0; i < 5; ++i) {
+    double s = 0.;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) s += Minv[(5 * i + k) * nc + c] * b[k];
+    z[i * nc + c] = s;
+  }
+  z[5 * nc + c] = iwr.s[5] * v[5 * nc + c] / dk[c];
+  z[6 * nc + c] = iwr.s[6] * v[6 * nc + c] / dk[nc + c];
+}
+
+// part[j * gridDim.x + b] = block b's share of V_j . w (j < nv)
+__global__ void k_kw_dots(int n, int nv, const double *__restrict__ V, size_t ld, const double *__restrict__ w,
+                          double *__restrict__ part) {
+  const int j = blockIdx.y;
+  const double *a = V + (size_t)j * ld;
+  double s = 0.;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) s += a[i] * w[i];
+  __shared__ double sh[32];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double t = threadIdx.x < blockDim.x / 32 ? sh[threadIdx.x] : 0.;
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+    if (threadIdx.x == 0) part[(size_t)j * gridDim.x + blockIdx.x] = t;
+  }
+}
+
+// w -= sum_j h[j] V_j (h in device memory), then optionally out = w * scale
+__global__ void k_kw_sub(int n, int nv, const double *__restrict__ V, size_t ld, const double *__restrict__ h,
+                         double *__restrict__ w) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double s = w[i];
+  for (int j = 0; j < nv; ++j) s -= h[j] * V[(size_t)j * ld + i];
+  w[i] = s;
+}
+__global__ void k_kw_scale(int n, double a, const double *__restrict__ x, double *__restrict__ y) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) y[i] = a * x[i];
+}
+__global__ void k_kw_combo(int n, int nv, const double *__restrict__ V, size_t ld, const double *__restrict__ yk,
+                           double *__restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double s = 0.;
+  for (int j = 0; j < nv; ++j) s += yk[j] * V[(size_t)j * ld + i];
+  out[i] = s;
+}
+
+// largest relative change |dp|/(p+Pref), |dT|/(T+Tref) and relative
+// decrease -dk/k, -domega/omega (ordered-key maxima in key[0], key[1])
+__global__ void k_kw_change(DevCase cs, int nc, const double *__restrict__ X, const double *__restrict__ dX,
+                            unsigned long long *__restrict__ key) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nc) return;
+  const double a = fmax(fabs(dX[c]) / fabs(X[c] + cs.Pref), fabs(dX[4 * nc + c]) / fabs(X[4 * nc + c] + cs.Tref));
+  const double b = fmax(-dX[5 * nc + c] / X[5 * nc + c], -dX[6 * nc + c] / X[6 * nc + c]);
+  atomicMax(&key[0], okey(a == a ? a : 1e300));
+  atomicMax(&key[1], okey(b == b ? b : 1e300));
+}
+
+// X += alpha dX with k, omega kept at or above their lower limits
+__global__ void k_kw_update(int nc, double *__restrict__ X, const double *__restrict__ dX, double alpha, double klow,
+                            double omlow) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= kNv * nc) return;
+  double x = X[i] + alpha * dX[i];
+  if (i >= 5 * nc && i < 6 * nc) x = fmax(x, klow);
+  if (i >= 6 * nc) x = fmax(x, omlow);
+  X[i] = x;
+}
+
+// Device buffers of one coupled Newton solve.
+struct KwSolve {
+  DBuf<double> X, Xsave, F0, F1, Jz, dt, vol, Minv, JL, JR, rowmag, dk, Vb, w, z, part, h, x, dX;
+  DBuf<unsigned long long> key;
+  std::vector<double> hpart;
+};
+
+// sum of the per-block partials of nv dot products, in block order (host)
+static void kw_dots(fcfd_ctx *x, KwSolve &S, int n, int nv, const double *V, size_t ld, const double *w, double *out) {
+  cudaStream_t s = x->stream;
+  k_kw_dots<<<dim3(kRedBlk, nv), 256, 0, s>>>(n, nv, V, ld, w, S.part.p);
+  S.hpart.resize((size_t)kRedBlk * nv);
+  CK(cudaMemcpyAsync(S.hpart.data(), S.part.p, sizeof(double) * kRedBlk * nv, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  for (int j = 0; j < nv; ++j) {
+    double t = 0.;
+    for (int b = 0; b < kRedBlk; ++b) t += S.hpart[(size_t)j * kRedBlk + b];
+    out[j] = t;
+  }
+}
+
+// F = F(X) into out (SoA [7][nc]); X + eps z when z is given.  Leaves the
+// chain's state (gradients, limiters, mdot, eddy viscosities) of that point
+// in x->p64 / x->rans->b.
+static void kw_residual(fcfd_ctx *x, const double *X, const double *z, double eps, double *out) {
+  const DevMesh &m = x->dm;
+  cudaStream_t s = x->stream;
+  const int gc = (m.nc + 255) / 256;
+  RansBuf<double> &b = x->rans->b;
+  k_x_load<<<gc, 256, 0, s>>>(m.nc, m.nt, X, z, eps, x->p64.W.p, b.K.p);
+  rans_chain<double, false>(x, x->p64, b, x->mdot.p, x->wl.p, out, b.RK.p);
+  k_rk_planes<<<gc, 256, 0, s>>>(m.nc, b.RK.p, out);
+}
+
+// Jz of the coupled FP32 tangent chain at X along z
+static void kw_tangent32(fcfd_ctx *x, const double *X, const double *z, double *Jz) {
+  const DevMesh &m = x->dm;
+  cudaStream_t s = x->stream;
+  const int gc = (m.nc + 255) / 256;
+  if (!x->pjv32.ready) x->pjv32.alloc(m.nc, m.nf, m.nb);
+  RansBuf<Dual<float>> &d = x->rans->f;
+  if (!d.ready) d.alloc(m.nc, m.nt, m.nf);
+  k_x_load_dual<<<gc, 256, 0, s>>>(m.nc, m.nt, X, z, x->pjv32.W.p, d.K.p);
+  rans_chain<Dual<float>, false>(x, x->pjv32, d, d.mdot.p, d.wl.p, x->pjv32.R.p, d.RK.p);
+  k_dual_planes<<<gc, 256, 0, s>>>(m.nc, x->pjv32.R.p, d.RK.p, Jz);
+}
+
+}  // namespace kwn
+}  // namespace fcfd
+
+using namespace fcfd::kwn;
+
+extern "C" int fcfd_rans_newton_solve(fcfd_ctx *x, double *W, double *K, const fcfd_newton_opts *o,
+                                      fcfd_newton_report *rep) {
+  try {
+    if (!x || !W || !K || !o || !rep) throw Error(FCFD_ERR_INPUT, "null argument");
+    if (!x->rans) throw Error(FCFD_ERR_INPUT, "the case has no turbulence model");
+    CK(cudaSetDevice(x->device));
+    const DevMesh &m = x->dm;
+    const int nc = m.nc, n = kNv * nc;
+    cudaStream_t s = x->stream;
+    const int gc = (nc + 255) / 256, gn = (n + 255) / 256;
+    std::memset(rep, 0, sizeof(*rep));
+    rep->seconds_to_tol = -1.;
+    const int mdim = o->krylov_dim > 0 ? o->krylov_dim : 30;
+    const int mode = o->jvp_mode;  // 0: FD in FP64, else the FP32 tangent chain
+    KwSolve S;
+    S.X.alloc(n); S.Xsave.alloc(n); S.F0.alloc(n); S.F1.alloc(n); S.Jz.alloc(n); S.dt.alloc(nc); S.vol.alloc(nc);
+    S.Minv.alloc(25 * (size_t)nc); S.JL.alloc(25 * (size_t)m.nf); S.JR.alloc(25 * (size_t)m.nf);
+    S.rowmag.alloc(5 * (size_t)nc); S.dk.alloc(2 * (size_t)nc);
+    S.Vb.alloc((size_t)(mdim + 1) * n); S.w.alloc(n); S.z.alloc(n); S.part.alloc((size_t)kRedBlk * (mdim + 1));
+    S.h.alloc(mdim + 1); S.x.alloc(n); S.dX.alloc(n); S.key.alloc(2);
+    // X from the host's AoS W[nc][5], K[nc][2]
+    {
+      std::vector<double> hx((size_t)n);
+      for (int c = 0; c < nc; ++c) {
+        for (int v = 0; v < 5; ++v) hx[(size_t)v * nc + c] = W[5 * (size_t)c + v];
+        for (int v = 0; v < 2; ++v) hx[(size_t)(5 + v) * nc + c] = K[2 * (size_t)c + v];
+      }
+      CK(cudaMemcpyAsync(S.X.p, hx.data(), sizeof(double) * n, cudaMemcpyHostToDevice, s));
+      std::vector<double> vol(x->mesh->c_volume.begin(), x->mesh->c_volume.begin() + nc);
+      CK(cudaMemcpyAsync(S.vol.p, vol.data(), sizeof(double) * nc, cudaMemcpyHostToDevice, s));
+      CK(cudaStreamSynchronize(s));
+    }
+    const double klow = x->case_ptr->k_low, omlow = x->case_ptr->omega_low;
+    auto t0 = std::chrono::steady_clock::now();
+    auto seconds = [&]() { return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count(); };
+    // per-equation residual norms (momentum x, y, z together)
+    double r0[kNv], rn[kNv];
+    auto norms = [&](const double *F, double out[kNv]) {
+      const int nd = 1;
+      for (int v = 0; v < kNv; ++v) {
+        double d;
+        kw_dots(x, S, nc, nd, F + (size_t)v * nc, 0, F + (size_t)v * nc, &d);
+        out[v] = std::sqrt(d);
+      }
+    };
+    kw_residual(x, S.X.p, nullptr, 0., S.F0.p);
+    check_err(x);
+    norms(S.F0.p, r0);
+    auto mom = [](const double r[kNv]) { return std::sqrt(r[1] * r[1] + r[2] * r[2] + r[3] * r[3]); };
+    const double m0 = mom(r0);
+    std::copy(r0, r0 + kNv, rn);
+    // equation weights: the inverse of each equation's initial norm (momentum as one)
+    Wt7 wr, iwr;
+    for (int v = 0; v < kNv; ++v) {
+      const double r = (v >= 1 && v <= 3) ? m0 : r0[v];
+      wr.s[v] = r > 0. ? 1. / r : 1.;
+      iwr.s[v] = 1. / wr.s[v];
+    }
+    rep->res0 = r0[0];
+    const double cfl0 = o->cfl0 > 0 ? o->cfl0 : 1.;
+    const double cflmax = o->cfl_max > 0 ? o->cfl_max : 1e6;
+    double cfl = cfl0, cfl_prev = cfl0;
+    const int maxit = o->max_newton > 0 ? o->max_newton : 200;
+    const int hist = (int)(sizeof(rep->history) / sizeof(rep->history[0]));
+    const double krtol = o->krylov_rtol > 0 ? o->krylov_rtol : 1e-2;
+    int status = FCFD_ERR_NOT_CONVERGED, rejects = 0;
+    // combined drop of all equations (the largest per-equation drop)
+    auto drop_all = [&](const double r[kNv]) {
+      double d = 0.;
+      for (int v = 0; v < kNv; ++v) {
+        if (v >= 1 && v <= 3) continue;
+        if (r0[v] > 0.) d = std::max(d, r[v] / r0[v]);
+      }
+      if (m0 > 0.) d = std::max(d, mom(r) / m0);
+      return d;
+    };
+    for (int it = 0; it < maxit; ++it) {
+      const double rm = rn[0] / r0[0], ra = drop_all(rn);
+      if (it < hist) { rep->history[it] = rm; rep->seconds_history[it] = seconds(); }
+      if (rm <= o->tol && rep->seconds_to_tol < 0.) rep->seconds_to_tol = seconds();
+      if ((o->stop_all_rows ? ra : rm) <= o->tol) { status = FCFD_OK; break; }
+      if (o->max_seconds > 0 && seconds() > o->max_seconds) break;
+      // time step, preconditioner at X (the chain's state of F0 is current)
+      k_local_dt<double><<<gc, 256, 0, s>>>(x->cs, m, x->p64.W.p, S.dt.p, cfl, nullptr);
+      ns_block_inverse(x, S.X.p, S.vol.p, S.dt.p, x->rans->b.mutf.p, S.JL.p, S.JR.p, S.Minv.p, S.rowmag.p);
+      k_kw_diag<<<gc, 256, 0, s>>>(x->cs, m, S.X.p, S.vol.p, S.dt.p, x->mdot.p, x->rans->b.mutf.p, S.dk.p);
+      CK(cudaMemcpyAsync(S.Xsave.p, S.X.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+      // GMRES(m), one cycle, on wr (D - J) M^-1 u = wr F0, dX = M^-1 u
+      // |S^-1 X| for the finite-difference step (S: the equations' scales)
+      double xn = 0.;
+      {
+        double d[kNv];
+        norms(S.X.p, d);
+        const double ref[kNv] = {std::fabs(x->cs.Pref) + d[0] / std::sqrt((double)nc), 0., 0., 0.,
+                                 std::fabs(x->cs.Tref) + d[4] / std::sqrt((double)nc), d[5] / std::sqrt((double)nc),
+                                 d[6] / std::sqrt((double)nc)};
+        double U = std::sqrt(d[1] * d[1] + d[2] * d[2] + d[3] * d[3]) / std::sqrt((double)nc);
+        for (int v = 0; v < kNv; ++v) {
+          const double r = (v >= 1 && v <= 3) ? U : ref[v];
+          if (r > 0.) xn += (d[v] / r) * (d[v] / r);
+        }
+        xn = std::sqrt(xn);
+      }
+      for (int v = 0; v < kNv; ++v)
+        k_kw_scale<<<gc, 256, 0, s>>>(nc, wr.s[v], S.F0.p + (size_t)v * nc, S.w.p + (size_t)v * nc);
+      double beta;
+      kw_dots(x, S, n, 1, S.w.p, 0, S.w.p, &beta);
+      beta = std::sqrt(beta);
+      int kit = 0;
+      std::vector<double> H((size_t)(mdim + 1) * mdim, 0.), g(mdim + 1, 0.), cs_(mdim), sn(mdim);
+      g[0] = beta;
+      if (beta > 0.) {
+        k_kw_scale<<<gn, 256, 0, s>>>(n, 1. / beta, S.w.p, S.Vb.p);
+        for (int j = 0; j < mdim; ++j) {
+          double *vj = S.Vb.p + (size_t)j * n;
+          // z = M^-1 v_j, then w = wr (D z - J z)
+          k_kw_prec<<<gc, 256, 0, s>>>(nc, S.Minv.p, S.dk.p, iwr, vj, S.z.p);
+          if (mode == 0) {
+            double zn;
+            kw_dots(x, S, n, 1, S.z.p, 0, S.z.p, &zn);
+            zn = std::sqrt(zn);
+            const double eps = zn > 0. ? 1.4901161193847656e-08 * (1. + xn) / zn : 1e-8;
+            kw_residual(x, S.X.p, S.z.p, eps, S.F1.p);
+            k_kw_matvec<<<gc, 256, 0, s>>>(x->cs, nc, S.X.p, S.vol.p, S.dt.p, S.z.p, S.F1.p, S.F0.p, 1. / eps, wr, S.w.p);
+          } else {
+            kw_tangent32(x, S.X.p, S.z.p, S.Jz.p);
+            k_kw_matvec<<<gc, 256, 0, s>>>(x->cs, nc, S.X.p, S.vol.p, S.dt.p, S.z.p, S.Jz.p, nullptr, 0., wr, S.w.p);
+          }
+          // classical Gram-Schmidt, twice
+          std::vector<double> hc(j + 1, 0.), hh(j + 1);
+          for (int pass = 0; pass < 2; ++pass) {
+            kw_dots(x, S, n, j + 1, S.Vb.p, (size_t)n, S.w.p, hh.data());
+            CK(cudaMemcpyAsync(S.h.p, hh.data(), sizeof(double) * (j + 1), cudaMemcpyHostToDevice, s));
+            k_kw_sub<<<gn, 256, 0, s>>>(n, j + 1, S.Vb.p, (size_t)n, S.h.p, S.w.p);
+            for (int i = 0; i <= j; ++i) hc[i] += hh[i];
+          }
+          double hn;
+          kw_dots(x, S, n, 1, S.w.p, 0, S.w.p, &hn);
+          hn = std::sqrt(hn);
+          for (int i = 0; i <= j; ++i) H[(size_t)i * mdim + j] = hc[i];
+          H[(size_t)(j + 1) * mdim + j] = hn;
+          if (hn > 0.) k_kw_scale<<<gn, 256, 0, s>>>(n, 1. / hn, S.w.p, S.Vb.p + (size_t)(j + 1) * n);
+          // Givens rotations of the new column
+          for (int i = 0; i < j; ++i) {
+            const double a = H[(size_t)i * mdim + j], b = H[(size_t)(i + 1) * mdim + j];
+            H[(size_t)i * mdim + j] = cs_[i] * a + sn[i] * b;
+            H[(size_t)(i + 1) * mdim + j] = -sn[i] * a + cs_[i] * b;
+          }
+          const double a = H[(size_t)j * mdim + j], b = H[(size_t)(j + 1) * mdim + j];
+          const double r = std::hypot(a, b);
+          cs_[j] = r > 0. ? a / r : 1.;
+          sn[j] = r > 0. ? b / r : 0.;
+          H[(size_t)j * mdim + j] = r;
+          H[(size_t)(j + 1) * mdim + j] = 0.;
+          g[j + 1] = -sn[j] * g[j];
+          g[j] = cs_[j] * g[j];
+          kit = j + 1;
+          if (std::fabs(g[j + 1]) <= krtol * beta || hn == 0.) break;
+        }
+        // y = H^-1 g, u = V y, dX = M^-1 u
+        std::vector<double> y(kit, 0.);
+        for (int i = kit - 1; i >= 0; --i) {
+          double t = g[i];
+          for (int k = i + 1; k < kit; ++k) t -= H[(size_t)i * mdim + k] * y[k];
+          y[i] = t / H[(size_t)i * mdim + i];
+        }
+        CK(cudaMemcpyAsync(S.h.p, y.data(), sizeof(double) * kit, cudaMemcpyHostToDevice, s));
+        k_kw_combo<<<gn, 256, 0, s>>>(n, kit, S.Vb.p, (size_t)n, S.h.p, S.x.p);
+        k_kw_prec<<<gc, 256, 0, s>>>(nc, S.Minv.p, S.dk.p, iwr, S.x.p, S.dX.p);
+      } else {
+        CK(cudaMemsetAsync(S.dX.p, 0, sizeof(double) * n, s));
+      }
+      rep->krylov_iterations += kit;
+      // relaxation: |dp/p|, |dT/T| <= 0.2
+      CK(cudaMemsetAsync(S.key.p, 0, 2 * sizeof(unsigned long long), s));
+      k_kw_change<<<gc, 256, 0, s>>>(x->cs, nc, S.X.p, S.dX.p, S.key.p);
+      unsigned long long kh[2];
+      CK(cudaMemcpyAsync(kh, S.key.p, sizeof(kh), cudaMemcpyDeviceToHost, s));
+      CK(cudaStreamSynchronize(s));
+      auto unkey = [](unsigned long long k) {
+        unsigned long long b = (k >> 63) ? (k & 0x7fffffffffffffffull) : ~k;
+        double d;
+        std::memcpy(&d, &b, sizeof(d));
+        return d;
+      };
+      // p and T limit the step; k and omega are clipped at their lower limits
+      // instead (one cell's k heading for zero would otherwise stall the step)
+      const double da = unkey(kh[0]);
+      double alpha = 1.;
+      if (da > 0.2) alpha = std::min(alpha, 0.2 / da);
+      k_kw_update<<<gn, 256, 0, s>>>(nc, S.X.p, S.dX.p, alpha, klow, omlow);
+      kw_residual(x, S.X.p, nullptr, 0., S.F1.p);
+      int herr = 0;
+      CK(cudaMemcpyAsync(&herr, x->err.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+      CK(cudaStreamSynchronize(s));
+      if (herr) CK(cudaMemsetAsync(x->err.p, 0, sizeof(int), s));
+      double rnew[kNv];
+      norms(S.F1.p, rnew);
+      rep->newton_iterations = it + 1;
+      bool finite = !herr;
+      for (int v = 0; v < kNv; ++v) finite = finite && std::isfinite(rnew[v]);
+      if (!finite) {
+        if (++rejects > 12) { status = FCFD_ERR_DIVERGED; break; }
+        CK(cudaMemcpyAsync(S.X.p, S.Xsave.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+        kw_residual(x, S.X.p, nullptr, 0., S.F0.p);
+        cfl = std::max(cfl * 0.25, 1e-3);
+        cfl_prev = cfl;
+        continue;
+      }
+      rejects = 0;
+      CK(cudaMemcpyAsync(S.F0.p, S.F1.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+      std::copy(rnew, rnew + kNv, rn);
+      rep->last_cfl = cfl;
+      // switched evolution/relaxation on the mass residual (cfl_mode 1) or on
+      // the largest per-equation drop (cfl_mode 2)
+      const double dr = o->cfl_mode == 2 ? drop_all(rn) : rn[0] / r0[0];
+      double next = cfl0 * std::pow(1. / std::max(dr, 1e-300), o->ser_exponent > 0 ? o->ser_exponent : 1.);
+      next = std::min(next, cfl_prev * 2.);
+      cfl_prev = cfl;
+      cfl = std::min(std::max(next, 1e-3), cflmax);
+    }
+    CK(cudaStreamSynchronize(s));
+    rep->wall_seconds = seconds();
+    rep->res_final = rn[0];
+    rep->rows_final[0] = rn[0] / r0[0];
+    rep->rows_final[1] = m0 > 0. ? mom(rn) / m0 : 0.;
+    rep->rows_final[2] = r0[4] > 0. ? rn[4] / r0[4] : 0.;
+    rep->kw_final[0] = r0[5] > 0. ? rn[5] / r0[5] : 0.;
+    rep->kw_final[1] = r0[6] > 0. ? rn[6] / r0[6] : 0.;
+    rep->status = status;
+    {
+      std::vector<double> hx((size_t)n);
+      CK(cudaMemcpy(hx.data(), S.X.p, sizeof(double) * n, cudaMemcpyDeviceToHost));
+      for (int c = 0; c < nc; ++c) {
+        for (int v = 0; v < 5; ++v) W[5 * (size_t)c + v] = hx[(size_t)v * nc + c];
+        for (int v = 0; v < 2; ++v) K[2 * (size_t)c + v] = hx[(size_t)(5 + v) * nc + c];
+      }
+    }
+    if (status != FCFD_OK) {
+      set_last_error(status == FCFD_ERR_DIVERGED ? "k-omega Newton iteration diverged (NaN/Inf)"
+                                                 : "k-omega Newton iteration did not reach the tolerance");
+      return status;
+    }
+  } catch (const Error &e) {
+    set_last_error(e.what());
+    return e.code;
+  } catch (const std::exception &e) {
+    set_last_error(e.what());
+    return FCFD_ERR_INPUT;
   }
   return FCFD_OK;
 }

@@ -290,6 +290,29 @@ class NavierStokes:
             raise FcfdError(rc, lib.fcfd_last_error().decode() + f" after {r.newton_iterations} steps")
         return W, rep
 
+    def rans_newton_solve(self, W, K, tol=1e-10, max_newton=200, krylov_dim=30, krylov_rtol=1e-2, cfl0=1.0,
+                          cfl_max=1e6, ser_exponent=1.0, fp32_jvp=False, max_seconds=0.0, stop_all_rows=False,
+                          raise_on_fail=True, cfl_mode=1):
+        """Coupled steady solve of the flow and k-omega residuals (turbulent
+        decks): pseudo-transient Newton-Krylov on (p,u,v,w,T,k,omega), J.v by
+        FP64 finite differences or (fp32_jvp) the FP32 coupled tangent chain.
+        Returns (W, K, report dict)."""
+        W = np.array(W, dtype=np.float64, order="C", copy=True)
+        K = np.array(K, dtype=np.float64, order="C", copy=True)
+        o = NewtonOpts(int(max_newton), float(tol), int(krylov_dim), float(krylov_rtol), float(cfl0), 1.2,
+                       float(cfl_max), int(cfl_mode), float(ser_exponent), 3 if fp32_jvp else 0, 0, float(max_seconds), 0, 1,
+                       int(bool(stop_all_rows)))
+        r = NewtonReport()
+        rc = lib.fcfd_rans_newton_solve(self.h, _d(W), _d(K), ctypes.byref(o), ctypes.byref(r))
+        n = r.newton_iterations
+        rep = dict(status=r.status, newton_iterations=n, krylov_iterations=r.krylov_iterations, res0=r.res0,
+                   res_final=r.res_final, wall_seconds=r.wall_seconds, last_cfl=r.last_cfl,
+                   history=np.array(r.history[:n + 1]), seconds_history=np.array(r.seconds_history[:n + 1]),
+                   rows_final=list(r.rows_final), kw_final=list(r.kw_final), seconds_to_tol=r.seconds_to_tol)
+        if rc != 0 and raise_on_fail:
+            raise FcfdError(rc, lib.fcfd_last_error().decode() + f" after {n} steps")
+        return W, K, rep
+
     def run(self, W, work_dir=".", restart_step=0, max_steps=0, jvp=False, fp32_krylov=False, precond_sweeps=0,
             echo=False, raise_on_fail=True):
         """The deck's time loop (the reference's main program): per step the

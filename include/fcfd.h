@@ -254,6 +254,7 @@ typedef struct fcfd_newton_report {
   double rows_final[3];   /* final / initial norm of the mass, momentum and energy residual */
   double seconds_to_tol;  /* wall time when |R_mass| first dropped by tol */
   double seconds_history[512]; /* wall time at each history[] entry */
+  double kw_final[2];     /* fcfd_rans_newton_solve: final / initial norm of the k and omega residuals */
 } fcfd_newton_report;
 
 /* Steady solve R(W) = 0 by pseudo-transient matrix-free Newton-Krylov on the
@@ -276,6 +277,24 @@ int fcfd_newton_solve(fcfd_ctx *ctx, double *W, const fcfd_newton_opts *opts, fc
  * (the reference takes finite differences).  blocks[nc][5][5], row =
  * equation (mass, momentum x/y/z, energy), column = primitive (p,u,v,w,T). */
 int fcfd_diag_blocks(fcfd_ctx *ctx, const double *W, const double *dt, double *blocks);
+
+/* Coupled steady solve of the flow and k-omega residuals (turbulent decks):
+ * pseudo-transient Newton-Krylov on X = (p,u,v,w,T,k,omega) per cell, one
+ * system where the reference solves NavierStokes::solve and then RANS::solve
+ * (ns.cc:104-118, rans.cc:85-98), each with its own time terms
+ * (ns_time_terms.cc:107-186, rans_time_terms.cc:25-87).  J.v by a finite
+ * difference of the FP64 coupled residual (jvp_mode 0) or the coupled tangent
+ * chain in FP32 (any other jvp_mode); block-Jacobi preconditioner (the flow
+ * blocks from first-order face Jacobians with the eddy viscosity, a diagonal
+ * for k and omega); GMRES(krylov_dim), one cycle per step, FP64 Gram-Schmidt.
+ * Uses tol, max_newton, krylov_dim, krylov_rtol, cfl0, cfl_max,
+ * cfl_mode (SER on the mass residual, or 2: on the largest per-equation
+ * drop), ser_exponent, max_seconds and
+ * stop_all_rows (all seven equations instead of the mass residual alone).
+ * W[nc][5] and K[nc][2] host, in/out; k and omega are kept at or above the
+ * deck's klowlimit / omegalowlimit. */
+int fcfd_rans_newton_solve(fcfd_ctx *ctx, double *W, double *K, const fcfd_newton_opts *opts,
+                           fcfd_newton_report *report);
 
 /* Deck-driven time loop (main.cc:294-438) for one laminar or Euler grid,
  * replacing the reference's main program after set-up.  Per time step:
