@@ -134,6 +134,7 @@ struct fcfd_ctx {
 
 namespace fcfd {
 constexpr int kExtremaBlocks = 296;  // 2 x 148 SMs
+constexpr int kPairGradCells = 148 * 512;
 template <class S>
 void launch_chain(fcfd_ctx *x, Pipe<S> &P, S *Rout, bool aos_out, S *mo, S *wo, bool frozen_limiter = false);
 int check_err(fcfd_ctx *x);
@@ -146,6 +147,15 @@ inline void launch_grad_limiter(const DevCase &cs, const DevMesh &m, const S *W,
                                 const int *argx, S *G, S *Lm, cudaStream_t s) {
   const int g = ((PART ? m.n_part_cells : m.nc) + 127) / 128;
   if (g == 0) return;
+  if constexpr (std::is_same<S, double>::value) {
+    // meshes too small to fill the GPU with one thread per cell (fewer than
+    // 148 SMs x 512 cells) take two threads per cell
+    const int ncell = PART ? m.n_part_cells : m.nc;
+    if (cs.fast_grad && cs.pair_grad && ncell < kPairGradCells) {
+      k_grad_limiter_pair<PART><<<(ncell + 31) / 32, 64, 0, s>>>(cs, m, W, ext, G, Lm);
+      return;
+    }
+  }
   if (cs.fast_grad)
     k_grad_limiter<S, true, PART><<<g, 128, 0, s>>>(cs, m, W, ext, argx, G, Lm);
   else

@@ -236,6 +236,7 @@ int fcfd_ctx_create(const fcfd_mesh *mp, const fcfd_case *csp, int device, fcfd_
     for (int cc = 0; cc < nc; ++cc)
       if (m.st_index[cc] == m.st_index[cc + 1]) { x->green_gauss = true; break; }
   }
+  d.pair_grad = x->green_gauss ? 0 : 1;
   std::vector<int32_t> bface(nb), outl;
   for (int f = 0; f < nf; ++f) {
     if (m.f_bc[f] >= 0) {

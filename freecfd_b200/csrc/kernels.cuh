@@ -152,7 +152,8 @@ struct DevCase {
   double Pr_t;
   double wdiss, bl_height;  // Steger-Warming wall dissipation and boundary-layer height
   int sutherland, prandtl, flux, limiter, order, viscous, nbc, frozen_limiter;
-  int fast_grad, pad_;
+  int fast_grad;
+  int pair_grad;  // every cell has a gradient stencil: the two-threads-per-cell gradient may run
   DevBC bc[kMaxBC];
 };
 
@@ -778,6 +779,170 @@ __global__ void __launch_bounds__(128, (!FAST && std::is_same<S, double>::value)
   }
 #pragma unroll
   for (int v = 0; v < 5; ++v) Lm[v * nc + c] = phi[v];
+}
+
+// LSQ gradient + continuous limiter (VK with K > 0, none, first order), FP64,
+// two threads per cell for meshes too small to fill the GPU with one thread
+// per cell.  A block is 32 consecutive cells and two warps: warp h takes half
+// h of every cell's stencil entries (so each warp reads the j-th entries of 32
+// consecutive cells, the coalesced pattern of k_grad_limiter) and half of its
+// faces in the limiter's two face loops; partial sums, extremes and limiter
+// minima meet in shared memory.  Same operations as k_grad_limiter's FAST path
+// except that the stencil sum is formed in two parts.  Cells with an
+// empty gradient map (Green-Gauss) are not handled (DevCase::pair_grad).
+// PART: one rank's gradient cells of a domain decomposition.
+template <bool PART = false>
+__global__ void __launch_bounds__(64) k_grad_limiter_pair(DevCase cs, DevMesh m, const double *__restrict__ W,
+                                                          const unsigned long long *__restrict__ ext,
+                                                          double *__restrict__ G, double *__restrict__ Lm) {
+  __shared__ double part[2][15][32];
+  const int lane = threadIdx.x & 31, h = threadIdx.x >> 5;
+  const int nc = m.nc, nt = m.nt;
+  const int ncell = PART ? m.n_part_cells : nc;
+  const int ci = blockIdx.x * 32 + lane;
+  const bool act = ci < ncell;
+  const int c = act ? (PART ? m.part_cells[ci] : ci) : 0;
+  double acc[15];
+#pragma unroll
+  for (int i = 0; i < 15; ++i) acc[i] = 0.;
+  double u0[5] = {0., 0., 0., 0., 0.};
+  double xc0 = 0., xc1 = 0., xc2 = 0.;
+  if (act) {
+    xc0 = m.c_x[c]; xc1 = m.c_x[nt + c]; xc2 = m.c_x[2 * nt + c];
+#pragma unroll
+    for (int v = 0; v < 5; ++v) u0[v] = W[v * nt + c];
+    const int j0 = m.st_index[c], j1 = m.st_index[c + 1], mid = (j0 + j1) >> 1;
+    const int a = h == 0 ? j0 : mid, b = h == 0 ? mid : j1;
+#pragma unroll 4
+    for (int j = a; j < b; ++j) {
+      const int k = m.st_keys[j];
+      if (k == c) continue;
+      const double d0 = m.c_x[k] - xc0, d1 = m.c_x[nt + k] - xc1, d2 = m.c_x[2 * nt + k] - xc2;
+      const double w = d0 * d0 + d1 * d1 + d2 * d2;
+#pragma unroll
+      for (int v = 0; v < 5; ++v) {
+        const double q = w * (W[v * nt + k] - u0[v]);
+        acc[3 * v] = acc[3 * v] + q * d0;
+        acc[3 * v + 1] = acc[3 * v + 1] + q * d1;
+        acc[3 * v + 2] = acc[3 * v + 2] + q * d2;
+      }
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < 15; ++i) part[h][i][lane] = acc[i];
+  __syncthreads();
+  double g[15];
+  {
+    const double C00 = m.st_cof[c], C01 = m.st_cof[nc + c], C02 = m.st_cof[2 * nc + c];
+    const double C11 = m.st_cof[3 * nc + c], C12 = m.st_cof[4 * nc + c], C22 = m.st_cof[5 * nc + c];
+    const double id = 1. / m.st_cof[6 * nc + c];
+    const double M0 = m.st_mirror[c], M1 = m.st_mirror[nc + c], M2 = m.st_mirror[2 * nc + c];
+#pragma unroll
+    for (int v = 0; v < 5; ++v) {
+      const double s0 = part[0][3 * v][lane] + part[1][3 * v][lane];
+      const double s1 = part[0][3 * v + 1][lane] + part[1][3 * v + 1][lane];
+      const double s2 = part[0][3 * v + 2][lane] + part[1][3 * v + 2][lane];
+      g[3 * v] = (C00 * s0 + C01 * s1 + C02 * s2) * id - M0 * u0[v];
+      g[3 * v + 1] = (C01 * s0 + C11 * s1 + C12 * s2) * id - M1 * u0[v];
+      g[3 * v + 2] = (C02 * s0 + C12 * s1 + C22 * s2) * id - M2 * u0[v];
+    }
+  }
+  // warp 0 writes the gradients of p, u, v; warp 1 those of w, T
+  if (act) {
+#pragma unroll
+    for (int i = 0; i < 15; ++i)
+      if ((h == 0) == (i < 9)) G[i * nc + c] = g[i];
+  }
+  double phi[5];
+#pragma unroll
+  for (int v = 0; v < 5; ++v) phi[v] = cs.order == 1 ? 0. : 1.;
+  if (cs.order != 1 && cs.limiter == 1) {
+    // the cell's faces are split between the warps as its stencil was: the
+    // neighbour extremes and the per-face limiter values are each reduced over
+    // both halves through shared memory (max, min: independent of the order)
+    __shared__ double ext_s[2][10][32];
+    __shared__ double phi_s[2][5][32];
+    const int f0 = act ? m.cf_index[c] : 0, f1 = act ? m.cf_index[c + 1] : 0, fm = (f0 + f1) >> 1;
+    const int fa = h == 0 ? f0 : fm, fb = h == 0 ? fm : f1;
+    double umax[5], umin[5];
+#pragma unroll
+    for (int v = 0; v < 5; ++v) umax[v] = umin[v] = u0[v];
+#pragma unroll 2
+    for (int j = fa; j < fb; ++j) {
+      const int e = m.cf_list[j];
+      const int f = e >= 0 ? e : ~e;
+      const int nb = e >= 0 ? m.f_neighbor[f] : m.f_parent[f];
+#pragma unroll
+      for (int v = 0; v < 5; ++v) {
+        const double x = W[v * nt + nb];
+        umax[v] = smax(umax[v], x);
+        umin[v] = smin(umin[v], x);
+      }
+    }
+#pragma unroll
+    for (int v = 0; v < 5; ++v) { ext_s[h][v][lane] = umax[v]; ext_s[h][5 + v][lane] = umin[v]; }
+    // find_min_max with its index quirks (see k_grad_limiter)
+    double eps2[5];
+    {
+      const double pmax = okey_inv(ext[0]), pmin = okey_inv(ext[1]);
+      const double T0 = W[4 * nt + 0], wl = W[3 * nt + nc - 1];
+      double qmax[5], qmin[5];
+      qmax[0] = pmax; qmin[0] = pmin;
+      qmax[1] = okey_inv(ext[2]); qmin[1] = okey_inv(ext[3]);
+      qmax[2] = okey_inv(ext[4]); qmin[2] = okey_inv(ext[5]);
+      double q4M = T0, q4m = T0;
+      if (nc > 1) {
+        const double a = okey_inv(ext[6]), b = okey_inv(ext[7]);
+        if (T0 < a) q4M = a;
+        if (b < T0) q4m = b;
+      }
+      qmax[3] = q4M; if (q4M < wl) qmax[3] = wl;
+      qmin[3] = q4m; if (wl < q4m) qmin[3] = wl;
+      qmax[4] = T0; if (T0 < pmax) qmax[4] = pmax;
+      qmin[4] = T0; if (pmin < T0) qmin[4] = pmin;
+#pragma unroll
+      for (int v = 0; v < 5; ++v) {
+        const double eps = fabs(qmax[v] - qmin[v]) / cs.Lref;
+        const double e = 1.e-6 * cs.K * eps;
+        eps2[v] = e * e;
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int v = 0; v < 5; ++v) {
+      umax[v] = smax(ext_s[0][v][lane], ext_s[1][v][lane]);
+      umin[v] = smin(ext_s[0][5 + v][lane], ext_s[1][5 + v][lane]);
+    }
+#pragma unroll 2
+    for (int j = fa; j < fb; ++j) {
+      const int e = m.cf_list[j];
+      const int f = e >= 0 ? e : ~e;
+      const double cf0 = sub_rn(m.f_x[f], xc0), cf1 = sub_rn(m.f_x[m.nf + f], xc1), cf2 = sub_rn(m.f_x[2 * m.nf + f], xc2);
+#pragma unroll
+      for (int v = 0; v < 5; ++v) {
+        const double dM = add_rn(add_rn(mul_rn(g[3 * v], cf0), mul_rn(g[3 * v + 1], cf1)), mul_rn(g[3 * v + 2], cf2));
+        double dP = u0[v];
+        if (dM > 0.) dP = sub_rn(umax[v], dP);
+        else if (dM < 0.) dP = sub_rn(umin[v], dP);
+        const double dP2 = mul_rn(dP, dP), dM2 = mul_rn(dM, dM);
+        if (dM != 0.) {
+          const double num = add_rn(add_rn(dP2, eps2[v]), mul_rn(mul_rn(2., dM), dP));
+          const double den = add_rn(add_rn(add_rn(dP2, mul_rn(2., dM2)), mul_rn(dM, dP)), eps2[v]);
+          phi[v] = smin(phi[v], div_rn(num, den));
+        }
+      }
+    }
+#pragma unroll
+    for (int v = 0; v < 5; ++v) phi_s[h][v][lane] = phi[v];
+    __syncthreads();
+#pragma unroll
+    for (int v = 0; v < 5; ++v) phi[v] = smin(phi_s[0][v][lane], phi_s[1][v][lane]);
+  }
+  if (act) {
+#pragma unroll
+    for (int v = 0; v < 5; ++v)
+      if ((h == 0) == (v < 3)) Lm[v * nc + c] = phi[v];
+  }
 }
 
 // Density the reference's `right` state cache holds when face f is reached:
