@@ -701,9 +701,9 @@ def run_rans_newton(fb, dev):
 # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) from
 # ncu captures of the same kernels; the capture commands are in profiles/.
 NCU_TRAFFIC = {
-    ("cylinder", "grad_limiter"): 17766656, ("cylinder", "face_flux"): 22753280,
+    ("cylinder", "grad_limiter"): 17764096, ("cylinder", "face_flux"): 20554752,
     ("hypersonic", "grad_limiter"): 191846912, ("hypersonic", "face_flux"): 141227264,
-    ("plate", "grad_limiter"): 159035648, ("plate", "face_flux"): 320413440,
+    ("plate", "grad_limiter"): 155463936, ("plate", "face_flux"): 196130048,
 }
 
 
