@@ -353,7 +353,93 @@ def residual_subline(fb, name, dev, steps, warmup, parity):
            "kernels_ms": {k: round(float(v), 5) for k, v in kern.items()}}
     if parity:
         out["parity_err"] = parity_check(ns, case)
+    if name == "hypersonic":
+        out["mixed_precision"] = mixed_subline(ns, mesh, case, steps, parity)
     del ns
+    return out
+
+
+def flux_scale(case, geo, gamma=1.4, R=287.0):
+    """Per-equation magnitude of one face's freestream flux times the
+    largest face area (the terms whose cancellation forms the residual)."""
+    p, u, v, w, T = case.freestream
+    rho = p / (R * T)
+    U = float(np.sqrt(u * u + v * v + w * w))
+    H = gamma / (gamma - 1.0) * R * T + 0.5 * U * U
+    A = float(np.max(geo["face_area"]))
+    mom = (rho * U * U + p) * A
+    return np.array([rho * U * A, mom, mom, mom, rho * U * H * A])
+
+
+def mixed_subline(ns, mesh, case, steps, parity, shock_ratio=2.0):
+    """The hypersonic residual with the face pass in FP32 and FP64 on the
+    faces across a pressure jump (fcfd_residual_mixed, shock_ratio 2), on the
+    seeded freestream state and on a state with a bow-shock jump; time per
+    evaluation (L2 flushed), FP64 faces, and the error against the FP64
+    oracle in units of the face-flux scale."""
+    cm = load_cases()
+    geo = mesh.geometry()
+    out = {"shock_ratio": shock_ratio, "states": {}}
+    for label, W in (("seeded_freestream", case.state),
+                     ("bow_shock_jump", cm.hypersonic_shock_state(case, geo["cell_centroid"]))):
+        W = np.ascontiguousarray(W)
+        ns.residual(W)
+        ns.time_residual(2, True)
+        t64 = ns.time_residual(steps, True)
+        R, n64 = ns.residual_mixed(W, shock_ratio)
+        ns.time_residual_mixed(2, True, shock_ratio)
+        ms, _ = ns.time_residual_mixed(steps, True, shock_ratio)
+        d = {"fp64_ms_per_step": round(float(t64[0]), 5), "mixed_ms_per_step": round(ms, 5),
+             "speedup": round(float(t64[0]) / ms, 3), "fp64_faces": n64, "faces": mesh.nf,
+             "value": round(mesh.nf / (ms * 1e-3) / 1e6, 3), "unit": UNIT}
+        if parity:
+            import oracle
+            o = oracle.Oracle(case)
+            ref = o.residual(W)
+            o.close()
+            err = np.abs(R - ref).max(axis=0) / flux_scale(case, geo)
+            d["err_vs_fp64_oracle_of_flux_scale"] = [float(e) for e in err]
+        out["states"][label] = d
+    return out
+
+
+def renumber_subline(fb, dev, steps, warmup):
+    """The laminar plate 384x192x4 residual in three cell orders: the
+    generator's i-j-k order, a seeded random order (an unordered grid) and the
+    reverse Cuthill-McKee order of the shuffled grid (fcfd_mesh_rcm).  Same
+    discretisation each time; the times show what cell order costs the
+    gathers."""
+    import tempfile
+    cm = load_cases()
+    base = make_case("plate")
+    out = {"workload": base.workload, "orders": {}}
+    sh = cm.shuffle_case(base, 0)
+    for label in ("generated", "shuffled", "rcm_of_shuffled"):
+        if label == "generated":
+            case = base
+        elif label == "shuffled":
+            case = sh
+        cs = fb.Case(case.write_deck(tempfile.mkdtemp(prefix="fcfd_bench_")))
+        if label == "rcm_of_shuffled":
+            msh = fb.Mesh(sh.mesh, cs)
+            t0 = time.perf_counter()
+            perm = msh.rcm_order()
+            out["rcm_host_seconds"] = round(time.perf_counter() - t0, 4)
+            del msh
+            case = cm.renumber_case(sh, perm, "rcm")
+        mesh = fb.Mesh(case.mesh, cs)
+        conn = mesh.connectivity()
+        ns = fb.NavierStokes(mesh, cs, dev)
+        ns.residual(case.state)
+        ns.time_residual(max(warmup, 1), True)
+        t = ns.time_residual(steps, True)
+        ms = float(t[0])
+        out["orders"][label] = {"ms_per_step": round(ms, 5), "value": round(mesh.nf / (ms * 1e-3) / 1e6, 3),
+                                "unit": UNIT,
+                                "bandwidth": cm.bandwidth(conn["face_parent"], conn["face_neighbor"], conn["face_bc"]),
+                                "kernels_ms": {k: round(float(v), 5) for k, v in zip(
+                                    ("ghost_minmax", "grad_limiter", "outlet_density", "face_flux", "gather"), t[1:6])}}
+        del ns
     return out
 
 
@@ -472,6 +558,8 @@ def run_ours(args):
     if not args.no_sublines and args.workload == "cylinder":
         line["workloads"] = [residual_subline(fb, w, dev, min(args.steps, 20), args.warmup, w != "plate64")
                              for w in ("hypersonic", "plate", "plate64")]
+        if world == 1:
+            line["renumbering"] = renumber_subline(fb, dev, min(args.steps, 20), args.warmup)
     if (world > 1 or args.decomposed) and args.workload == "cylinder":
         line["decomposed"] = run_decomposed(fb, world, rank, dev, dist, args.steps, args.warmup)
     if not args.no_newton and not rans:

@@ -23,12 +23,13 @@ STATUS = {0: "OK", 1: "ERR_INPUT", 2: "ERR_MESH", 3: "ERR_DIVERGED", 4: "ERR_NOT
 EXPORTED = [
     "fcfd_last_error", "fcfd_version", "fcfd_case_from_deck", "fcfd_case_destroy", "fcfd_case_summary",
     "fcfd_mesh_create", "fcfd_mesh_destroy", "fcfd_mesh_sizes", "fcfd_mesh_connectivity", "fcfd_mesh_geometry",
-    "fcfd_mesh_lsq",
+    "fcfd_mesh_lsq", "fcfd_mesh_rcm", "fcfd_mesh_grad_weights",
     "fcfd_ctx_create", "fcfd_ctx_destroy", "fcfd_ctx_set_exact_gradients", "fcfd_residual", "fcfd_last_stages", "fcfd_local_dt",
     "fcfd_time_residual", "fcfd_point_flux", "fcfd_jvp", "fcfd_vjp", "fcfd_drag", "fcfd_rans_residual", "fcfd_rans_bcs", "fcfd_time_rans", "fcfd_newton_solve", "fcfd_local_dt_cflmax_noalloc",
     "fcfd_run", "fcfd_restart_write", "fcfd_restart_read", "fcfd_mesh_from_tecplot", "fcfd_rans_jvp",
     "fcfd_partition_sets", "fcfd_ctx_set_partition", "fcfd_partition_extrema", "fcfd_partition_residual",
-    "fcfd_ctx_stream", "fcfd_diag_blocks", "fcfd_rans_newton_solve",
+    "fcfd_ctx_stream", "fcfd_diag_blocks", "fcfd_rans_newton_solve", "fcfd_residual_mixed",
+    "fcfd_time_residual_mixed",
 ]
 
 
@@ -72,7 +73,7 @@ class NewtonOpts(ctypes.Structure):
                 ("cfl_max", ctypes.c_double), ("cfl_mode", ctypes.c_int32), ("ser_exponent", ctypes.c_double),
                 ("jvp_mode", ctypes.c_int32), ("fp32_krylov", ctypes.c_int32), ("max_seconds", ctypes.c_double),
                 ("precond_sweeps", ctypes.c_int32), ("krylov_cycles", ctypes.c_int32),
-                ("stop_all_rows", ctypes.c_int32)]
+                ("stop_all_rows", ctypes.c_int32), ("gs_launch", ctypes.c_int32)]
 
 
 class NewtonReport(ctypes.Structure):
@@ -103,6 +104,10 @@ def _load():
     L.fcfd_mesh_connectivity.argtypes = [vp] + [ip] * 10
     L.fcfd_mesh_geometry.argtypes = [vp] + [dp] * 9
     L.fcfd_mesh_lsq.argtypes = [vp, dp, dp]
+    L.fcfd_mesh_rcm.argtypes = [vp, ip]
+    L.fcfd_mesh_grad_weights.argtypes = [vp, dp]
+    L.fcfd_residual_mixed.argtypes = [vp, vp, vp, ctypes.c_double, ctypes.c_int32, i64p]
+    L.fcfd_time_residual_mixed.argtypes = [vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_double, dp]
     L.fcfd_ctx_create.argtypes = [vp, vp, ctypes.c_int, ctypes.POINTER(vp)]
     L.fcfd_ctx_destroy.argtypes = [vp]
     L.fcfd_ctx_destroy.restype = None

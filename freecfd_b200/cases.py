@@ -425,7 +425,7 @@ grid_1 {{
 
 
 def cylinder_case(ntheta=256, nr=128, seed=1234, flux="Roe", limiter="vk",
-                  threshold=1.0, r1=15.0, dr0=1e-3, ns_extra="") -> Case:
+                  threshold=1.0, r1=15.0, dr0=1e-3, ns_extra="", grad="lsqr") -> Case:
     mesh = cylinder_mesh(ntheta, nr, r1=r1, dr0=dr0)
     p, T, M, Re, D = 101325.0, 300.0, 0.2, 40.0, 1.0
     a = math.sqrt(1.4 * R_AIR * T)
@@ -441,7 +441,7 @@ grid_1 {{
  dimension=2;
  equations=navier stokes;
  material=air;
- gradients (hex method=lsqr; prism method=lsqr;);
+ gradients (hex method={grad}; prism method={grad};);
  navier stokes (limiter={limiter}; limiter threshold={_fmt(threshold)}; convective flux={flux};{ns_extra});
  write output ( volume variables=[V,p,T]; surface variables=[p]; load frequency=1; include bcs=[1]; );
  IC_1 (rho={_fmt(rho)}; V={_vec((U, 0.0, 0.0))}; p={_fmt(p)};);
@@ -458,7 +458,7 @@ grid_1 {{
 
 
 def hypersonic_case(ntheta=512, nr=256, seed=1234, flux="AUSM+up", limiter="minmod",
-                    r1=2.5, dr0=2e-3, jitter_seed=4321, ns_extra="") -> Case:
+                    r1=2.5, dr0=2e-3, jitter_seed=4321, ns_extra="", grad="lsqr") -> Case:
     mesh = cylinder_mesh(ntheta, nr, r1=r1, dr0=dr0 * 256.0 / nr, jitter=0.1,
                          seed=jitter_seed, prisms=True)
     p, T, M = 2000.0, 220.0, 8.0
@@ -472,7 +472,7 @@ grid_1 {{
  dimension=2;
  equations=navier stokes;
  material (viscosity=0.; molar mass={_fmt(MW_AIR)}; gamma=1.4;);
- gradients (hex method=lsqr; prism method=lsqr;);
+ gradients (hex method={grad}; prism method={grad};);
  navier stokes (limiter={limiter}; convective flux={flux};{ns_extra});
  write output ( volume variables=[V,p,T]; surface variables=[p]; );
  IC_1 (p={_fmt(p)}; T={_fmt(T)}; V={_vec((U, 0.0, 0.0))};);
@@ -489,7 +489,7 @@ grid_1 {{
 
 
 def plate_case(ni=384, nj=192, nk=4, seed=1234, flux="Roe", limiter="vk",
-               threshold=1.0, turbulent=True, ns_extra="") -> Case:
+               threshold=1.0, turbulent=True, ns_extra="", grad="lsqr") -> Case:
     L, ReL = 2.0, 5e6
     p, T, M = 101325.0, 300.0, 0.2
     a = math.sqrt(1.4 * R_AIR * T)
@@ -511,7 +511,7 @@ grid_1 {{
  dimension=3;
  equations=navier stokes;
  material=air;
- gradients (hex method=lsqr; prism method=lsqr;);
+ gradients (hex method={grad}; prism method={grad};);
 {turb} navier stokes (limiter={limiter}; limiter threshold={_fmt(threshold)}; convective flux={flux};{ns_extra});
  write output ( volume variables=[V,p,T]; surface variables=[p]; );
  IC_1 (rho={_fmt(rho)}; V={_vec((U, 0.0, 0.0))}; p={_fmt(p)};{tin});
@@ -623,3 +623,71 @@ def write_tecplot(mesh: RawMesh, path: str, bc_names=None, order: str = "cells",
             for i in range(3):
                 fh.write(block([float(x) for x in mesh.nodes[nodes, i]], "%.17g"))
     return path
+
+
+# ----------------------------------------------------------------------------
+# cell renumbering
+# ----------------------------------------------------------------------------
+def renumber_cells(mesh: RawMesh, perm) -> RawMesh:
+    """The same grid with its elements listed in the order `perm` (perm[new]
+    = old): new cell i is old cell perm[i], with its node list unchanged.
+    Nodes and boundary regions are untouched, so every face, normal, area,
+    centroid and volume is the same; only cell and face numbering change
+    (faces are discovered in the new cell order)."""
+    perm = np.asarray(perm, dtype=np.int64)
+    n = mesh.n_cells
+    if perm.shape != (n,) or not np.array_equal(np.sort(perm), np.arange(n)):
+        raise ValueError("perm must be a permutation of the cell indices")
+    ci = np.asarray(mesh.conn_index, dtype=np.int64)
+    sizes = ci[1:] - ci[:-1]
+    new_sizes = sizes[perm]
+    idx = np.zeros(n + 1, dtype=np.int32)
+    idx[1:] = np.cumsum(new_sizes)
+    take = np.concatenate([np.arange(ci[o], ci[o + 1]) for o in perm]) if n else np.zeros(0, np.int64)
+    return RawMesh(mesh.nodes, idx, np.ascontiguousarray(mesh.conn[take], dtype=np.int32),
+                   list(mesh.bc_nodes), mesh.dimension)
+
+
+def renumber_case(case: Case, perm, label: str = "renumbered") -> Case:
+    """`case` on its grid renumbered by `perm` (perm[new] = old), with the
+    seeded cell states permuted the same way."""
+    perm = np.asarray(perm, dtype=np.int64)
+    return Case(case.name, renumber_cells(case.mesh, perm), case.deck, dict(case.materials),
+                None if case.state is None else np.ascontiguousarray(case.state[perm]), case.freestream,
+                f"{case.workload}_{label}", None if case.kstate is None else np.ascontiguousarray(case.kstate[perm]),
+                case.kfree)
+
+
+def shuffle_case(case: Case, seed: int = 0) -> Case:
+    """`case` with its cells listed in a seeded random order: a grid whose
+    element order carries no locality (an unordered export)."""
+    perm = np.random.default_rng(seed).permutation(case.mesh.n_cells)
+    return renumber_case(case, perm, f"shuffled{seed}")
+
+
+def bandwidth(face_parent, face_neighbor, face_bc) -> int:
+    """Largest |parent - neighbour| over interior faces (matrix bandwidth)."""
+    fp, fn = np.asarray(face_parent), np.asarray(face_neighbor)
+    m = np.asarray(face_bc) < 0
+    return int(np.abs(fp[m] - fn[m]).max()) if m.any() else 0
+
+
+def hypersonic_shock_state(case: Case, centroids, radius: float = 1.2, seed: int = 7, mach: float = 8.0,
+                           gamma: float = 1.4) -> np.ndarray:
+    """A state with a captured bow-shock jump for the hypersonic cylinder:
+    the seeded freestream state, with the cells whose centroid lies within
+    `radius` of the axis replaced by the normal-shock state of the freestream
+    (Rankine-Hugoniot p2/p1, T2/T1, u2/u1 at `mach`), plus a 1 % seeded
+    perturbation.  The pressure jumps ~75x across one ring of faces."""
+    p1, u1, v1, w1, T1 = case.freestream
+    M2 = mach * mach
+    pr = 1.0 + 2.0 * gamma / (gamma + 1.0) * (M2 - 1.0)
+    rr = (gamma + 1.0) * M2 / ((gamma - 1.0) * M2 + 2.0)
+    W = case.state.copy()
+    x = np.asarray(centroids)[: W.shape[0]]
+    inside = np.hypot(x[:, 0], x[:, 1]) < radius
+    rng = np.random.default_rng(seed)
+    jit = 1.0 + 0.01 * rng.uniform(-1.0, 1.0, (int(inside.sum()), 5))
+    post = np.array([p1 * pr, u1 / rr, v1 / rr, w1 / rr, T1 * pr / rr])
+    W[inside] = post * jit
+    return W

@@ -526,7 +526,7 @@ __global__ void k_e2_adj(DevCase cs, DevMesh m, const double *__restrict__ W, co
 // Gradient stage: Wgrad_k = sum over cells c whose stencil holds k of
 // w_ck . Gbar_c (transposed stencil, ascending c).
 __global__ void k_grad_adj(DevMesh m, const int *__restrict__ tr_index, const int *__restrict__ tr_cell,
-                           const double *__restrict__ Gb, double *__restrict__ Wgrad) {
+                           const int *__restrict__ tr_entry, const double *__restrict__ Gb, double *__restrict__ Wgrad) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   const int nc = m.nc, nt = m.nt;
   if (k >= nt) return;
@@ -535,7 +535,11 @@ __global__ void k_grad_adj(DevMesh m, const int *__restrict__ tr_index, const in
   for (int j = tr_index[k]; j < tr_index[k + 1]; ++j) {
     const int c = tr_cell[j];
     double wt[3];
-    if (c == k) {
+    if (m.st_w) {
+      // stored map weights (curvilinear cases): entry tr_entry[j] of c's map
+      const size_t e = (size_t)tr_entry[j];
+      wt[0] = m.st_w[3 * e]; wt[1] = m.st_w[3 * e + 1]; wt[2] = m.st_w[3 * e + 2];
+    } else if (c == k) {
       wt[0] = m.st_self[c]; wt[1] = m.st_self[nc + c]; wt[2] = m.st_self[2 * nc + c];
     } else {
       const double d0 = xk[0] - m.c_x[c], d1 = xk[1] - m.c_x[nt + c], d2 = xk[2] - m.c_x[2 * nt + c];
@@ -647,7 +651,7 @@ __global__ void k_rearm(unsigned long long *ext, int *argx) {
 struct AdjBufs {
   DBuf<double> FA, Wcell, Gb, Wlim, Wgrad, GA, e2part, Rb, out;
   DBuf<double> Wface, SC;  // per-face-side limiter contributions; outlet faces' stale-density adjoints
-  DBuf<int> tr_index, tr_cell, tgt;
+  DBuf<int> tr_index, tr_cell, tr_entry, tgt;
   bool ready = false;
 };
 
@@ -675,12 +679,15 @@ static AdjBufs &adj_bufs(fcfd_ctx *x) {
   for (int c = 0; c < nc; ++c)
     for (int j = h.st_index[c]; j < h.st_index[c + 1]; ++j) cnt[h.st_keys[j] + 1]++;
   for (int k = 0; k < nt; ++k) cnt[k + 1] += cnt[k];
-  std::vector<int> cells(cnt[nt]);
+  std::vector<int> cells(cnt[nt]), entries(cnt[nt]);
   std::vector<int> fill(cnt.begin(), cnt.end() - 1);
   for (int c = 0; c < nc; ++c)
-    for (int j = h.st_index[c]; j < h.st_index[c + 1]; ++j) cells[fill[h.st_keys[j]]++] = c;
+    for (int j = h.st_index[c]; j < h.st_index[c + 1]; ++j) {
+      entries[fill[h.st_keys[j]]] = j;
+      cells[fill[h.st_keys[j]]++] = c;
+    }
   a.tr_index.upload(cnt);
-  if (!cells.empty()) a.tr_cell.upload(cells);
+  if (!cells.empty()) { a.tr_cell.upload(cells); a.tr_entry.upload(entries); }
   a.FA.alloc((size_t)U_N * m.nf);
   a.Wcell.alloc(5 * (size_t)nc);
   a.Gb.alloc(15 * (size_t)nc);
@@ -735,7 +742,7 @@ static void run_adjoint(fcfd_ctx *x, const double *Rbar_soa, unsigned int mask, 
     k_cell_adj<false><<<gc, 128, 0, s>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, x->ext.p, a.FA.p, a.Wcell.p, a.Gb.p, a.Wface.p, a.e2part.p);
   k_wlim_gather<<<(5 * m.nc + 255) / 256, 256, 0, s>>>(m, a.Wface.p, a.Wlim.p);
   if (need_ext) k_e2_adj<<<1, 32, 0, s>>>(x->cs, m, P.W.p, x->ext.p, x->argx.p, a.e2part.p, gc, a.Wlim.p);
-  k_grad_adj<<<(m.nt + 127) / 128, 128, 0, s>>>(m, a.tr_index.p, a.tr_cell.p, a.Gb.p, a.Wgrad.p);
+  k_grad_adj<<<(m.nt + 127) / 128, 128, 0, s>>>(m, a.tr_index.p, a.tr_cell.p, a.tr_entry.p, a.Gb.p, a.Wgrad.p);
   if (m.nb > 0) k_ghost_adj<<<(m.nb + 127) / 128, 128, 0, s>>>(x->cs, m, P.W.p, a.FA.p, a.Wgrad.p, a.Wlim.p, a.GA.p);
   if (aos) k_final_adj<true><<<(m.nc + tb - 1) / tb, tb, 0, s>>>(m, a.Wcell.p, a.Wgrad.p, a.Wlim.p, a.GA.p, out);
   else k_final_adj<false><<<(m.nc + tb - 1) / tb, tb, 0, s>>>(m, a.Wcell.p, a.Wgrad.p, a.Wlim.p, a.GA.p, out);

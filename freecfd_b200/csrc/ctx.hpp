@@ -100,6 +100,7 @@ struct fcfd_ctx {
   DBuf<int> gs_nbr, gs_src;
   int gs_deg = 0;
   DBuf<double> f_n, f_area, f_x, f_w, c_x, c_len, st_cof, st_self, st_recip, st_mirror, c_vol, f_wall, f_diss;
+  DBuf<double> st_w;  // stored gradient-map weights [E][3] (curvilinear cases)
   bool green_gauss = false;  // some cells take the Green-Gauss gradient
   // state arrays
   Pipe<double> p64;
@@ -129,6 +130,8 @@ struct fcfd_ctx {
   DevMesh dmp{};
   DBuf<int> part_cells, part_faces, part_outlet, part_ghosts;
   DBuf<int> face_order;  // faces grouped by kind (DevMesh::face_list of the whole mesh)
+  // mixed-precision residual: faces sent to the FP64 pass, and their count
+  DBuf<int> mx_list, mx_count;
 };
 
 
@@ -192,6 +195,8 @@ inline void launch_faces(fcfd_ctx *x, Pipe<S> &P, const S *mu_t, S *mo, S *wo, c
 void ns_block_inverse(fcfd_ctx *x, const double *Wn, const double *vol, const double *dt, const double *mutf,
                       double *JL, double *JR, double *Minv, double *rowmag);
 void adjoint_free(fcfd_ctx *x);
+// mixed.cu: FP32 face pass + FP64 pass over the shock-flagged faces
+void launch_mixed_faces(fcfd_ctx *x, double shock_ratio, int *list, int *count, cudaStream_t s);
 void rans_setup(fcfd_ctx *x);
 void rans_free(fcfd_ctx *x);
 }  // namespace fcfd

@@ -22,6 +22,7 @@ extern template __global__ void k_ghost_minmax<Dual<float>>(DevCase, DevMesh, Du
 
 fcfd_case *read_deck(const std::string &path);
 fcfd_mesh *build_mesh(const fcfd_raw_mesh &raw, fcfd_case &cs, const FaceInput *faces = nullptr);
+void rcm_order(const fcfd_mesh &m, std::vector<int32_t> &perm);
 
 static thread_local std::string g_last_error;
 void set_last_error(const std::string &m) { g_last_error = m; }
@@ -50,6 +51,41 @@ void launch_chain(fcfd_ctx *x, Pipe<S> &P, S *Rout, bool aos_out, S *mo, S *wo, 
     k_gather<S, true><<<gg, tb, 0, s>>>(m, P.D.p, Rout, x->ext.p, x->argx.p);
   else
     k_gather<S, false><<<gg, tb, 0, s>>>(m, P.D.p, Rout, x->ext.p, x->argx.p);
+  CK(cudaGetLastError());
+}
+
+// Mixed-precision residual chain on x->p64 (state already in P.W): FP64
+// ghosts, extrema, gradients and limiters; the stale-density outlet faces in
+// FP64 on the side stream; the FP32 face pass with the shock-flagged faces
+// in FP64 (mixed.cu); the FP64 gather into Rout ([nc][5]).
+static void launch_mixed(fcfd_ctx *x, double shock_ratio, double *Rout) {
+  const DevMesh &m = x->dm;
+  cudaStream_t s = x->stream;
+  Pipe<double> &P = x->p64;
+  if (x->mx_count.n == 0) {
+    x->mx_list.alloc(m.nf > 0 ? m.nf : 1);
+    x->mx_count.alloc(1);
+  }
+  const int tb = 256;
+  const bool need_ext = x->cs.limiter == 1 && x->cs.order != 1;
+  const int ng = (m.nb + tb - 1) / tb + (need_ext ? kExtremaBlocks : 0);
+  if (ng > 0) k_ghost_minmax<double><<<ng, tb, 0, s>>>(x->cs, m, P.W.p, need_ext ? x->ext.p : nullptr, x->err.p);
+  launch_grad_limiter<double>(x->cs, m, P.W.p, x->ext.p, nullptr, P.G.p, P.Lm.p, s);
+  CK(cudaMemsetAsync(x->mx_count.p, 0, sizeof(int), s));
+  const bool side = m.n_outlet > 0;
+  if (side) {
+    CK(cudaEventRecord(x->ev_fork, s));
+    CK(cudaStreamWaitEvent(x->side, x->ev_fork, 0));
+    const int g = (m.n_outlet + 127) / 128;
+    if (x->viscous)
+      FCFD_BY_FLUX(x->cs.flux, k_face_flux<double, true, FX, true><<<g, 128, 0, x->side>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p, nullptr, P.D.p, nullptr, nullptr, x->err.p));
+    else
+      FCFD_BY_FLUX(x->cs.flux, k_face_flux<double, false, FX, true><<<g, 128, 0, x->side>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p, nullptr, P.D.p, nullptr, nullptr, x->err.p));
+    CK(cudaEventRecord(x->ev_join, x->side));
+  }
+  launch_mixed_faces(x, shock_ratio, x->mx_list.p, x->mx_count.p, s);
+  if (side) CK(cudaStreamWaitEvent(s, x->ev_join, 0));
+  k_gather<double, true><<<(5 * m.nc + tb - 1) / tb, tb, 0, s>>>(m, P.D.p, Rout, x->ext.p, x->argx.p);
   CK(cudaGetLastError());
 }
 
@@ -163,6 +199,23 @@ int fcfd_mesh_lsq(const fcfd_mesh *m, double *cofactors, double *self_weight) {
   API_END
 }
 
+int fcfd_mesh_grad_weights(const fcfd_mesh *m, double *weights) {
+  API_BEGIN
+  if (!m || !weights) throw Error(FCFD_ERR_INPUT, "null argument");
+  if (!m->grad_weights) throw Error(FCFD_ERR_UNSUPPORTED, "the mesh keeps no stored gradient weights (no curvilinear cell)");
+  std::memcpy(weights, m->st_w.data(), m->st_w.size() * sizeof(double));
+  API_END
+}
+
+int fcfd_mesh_rcm(const fcfd_mesh *m, int32_t *perm) {
+  API_BEGIN
+  if (!m || !perm) throw Error(FCFD_ERR_INPUT, "null argument");
+  std::vector<int32_t> p;
+  rcm_order(*m, p);
+  std::memcpy(perm, p.data(), sizeof(int32_t) * p.size());
+  API_END
+}
+
 int fcfd_ctx_create(const fcfd_mesh *mp, const fcfd_case *csp, int device, fcfd_ctx **out) {
   API_BEGIN
   if (!mp || !csp || !out) throw Error(FCFD_ERR_INPUT, "null argument");
@@ -225,6 +278,12 @@ int fcfd_ctx_create(const fcfd_mesh *mp, const fcfd_case *csp, int device, fcfd_
   x->st_index.upload(m.st_index); x->st_keys.upload(m.st_keys);
   x->st_cof.upload(soa(m.st_cof, nc, 7)); x->st_self.upload(soa(m.st_self, nc, 3));
   x->st_recip.upload(m.st_recip); x->st_mirror.upload(soa(m.st_mirror, nc, 3));
+  if (m.grad_weights) {
+    // stored map weights (a curvilinear case): the gradient sums them in key
+    // order; the fused and two-warp least-squares forms do not apply
+    x->st_w.upload(m.st_w);
+    d.fast_grad = 0;
+  }
   if (c.flux == FLUX_SW) {
     if ((int)m.f_wall.size() != nf || (int)m.f_diss.size() != nf)
       throw Error(FCFD_ERR_INPUT, "the Steger-Warming flux needs a mesh built with a Steger-Warming case (face wall distances)");
@@ -236,7 +295,7 @@ int fcfd_ctx_create(const fcfd_mesh *mp, const fcfd_case *csp, int device, fcfd_
     for (int cc = 0; cc < nc; ++cc)
       if (m.st_index[cc] == m.st_index[cc + 1]) { x->green_gauss = true; break; }
   }
-  d.pair_grad = x->green_gauss ? 0 : 1;
+  d.pair_grad = (x->green_gauss || m.grad_weights) ? 0 : 1;
   std::vector<int32_t> bface(nb), outl;
   for (int f = 0; f < nf; ++f) {
     if (m.f_bc[f] >= 0) {
@@ -322,6 +381,7 @@ int fcfd_ctx_create(const fcfd_mesh *mp, const fcfd_case *csp, int device, fcfd_
   dm.c_len = x->c_len.p; dm.cf_index = x->cf_index.p; dm.cf_list = x->cf_list.p; dm.st_index = x->st_index.p;
   dm.st_keys = x->st_keys.p; dm.st_cof = x->st_cof.p; dm.st_self = x->st_self.p; dm.bface = x->bface.p;
   dm.st_recip = x->st_recip.p; dm.st_mirror = x->st_mirror.p; dm.c_vol = x->c_vol.p;
+  dm.st_w = x->st_w.p;
   dm.f_wall = x->f_wall.p; dm.f_diss = x->f_diss.p;
   dm.outlet_faces = x->outlet.p; dm.n_outlet = x->n_outlet;
   dm.face_list = x->face_order.p; dm.n_face_list = nf;
@@ -454,6 +514,59 @@ int fcfd_local_dt(fcfd_ctx *x, const double *W, double cfl, int mode, double *dt
 // every kernel: ghost+extrema, gradient+limiter, (unused: the outlet density
 // is computed inside the face flux), face flux, gather.  L2 is flushed (a
 // 512 MB memset) before every residual when flush_l2 is set.
+int fcfd_residual_mixed(fcfd_ctx *x, const double *W, double *R, double shock_ratio, int32_t flags,
+                        int64_t *n_fp64_faces) {
+  API_BEGIN
+  if (!x || !W || !R) throw Error(FCFD_ERR_INPUT, "null argument");
+  if (!(shock_ratio == shock_ratio)) throw Error(FCFD_ERR_INPUT, "shock_ratio is NaN");
+  CK(cudaSetDevice(x->device));
+  const DevMesh &m = x->dm;
+  cudaStream_t s = x->stream;
+  const bool dev = flags & FCFD_DEVICE_PTRS;
+  const double *win = W;
+  if (!dev) {
+    CK(cudaMemcpyAsync(x->Win.p, W, sizeof(double) * 5 * m.nc, cudaMemcpyHostToDevice, s));
+    win = x->Win.p;
+  }
+  k_aos_to_soa<double><<<(m.nc + 255) / 256, 256, 0, s>>>(win, x->p64.W.p, m.nc, m.nt);
+  double *rout = dev ? R : x->Rtmp.p;
+  launch_mixed(x, shock_ratio, rout);
+  if (!dev) CK(cudaMemcpyAsync(R, x->Rtmp.p, sizeof(double) * 5 * m.nc, cudaMemcpyDeviceToHost, s));
+  int cnt = 0;
+  CK(cudaMemcpyAsync(&cnt, x->mx_count.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  if (n_fp64_faces) *n_fp64_faces = cnt;
+  check_err(x);
+  API_END
+}
+
+int fcfd_time_residual_mixed(fcfd_ctx *x, int32_t reps, int32_t flush_l2, double shock_ratio, double *out) {
+  API_BEGIN
+  if (!x || !out || reps < 1) throw Error(FCFD_ERR_INPUT, "bad argument");
+  CK(cudaSetDevice(x->device));
+  cudaStream_t s = x->stream;
+  if (flush_l2 && x->flush.n == 0) x->flush.alloc((size_t)512 << 20);
+  Timing t;
+  double acc = 0.;
+  for (int r = 0; r < reps; ++r) {
+    if (flush_l2) CK(cudaMemsetAsync(x->flush.p, r & 0xff, x->flush.n, s));
+    CK(cudaEventRecord(t.ev[0], s));
+    launch_mixed(x, shock_ratio, x->p64.R.p);
+    CK(cudaEventRecord(t.ev[1], s));
+    CK(cudaEventSynchronize(t.ev[1]));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, t.ev[0], t.ev[1]));
+    acc += ms;
+  }
+  int cnt = 0;
+  CK(cudaMemcpyAsync(&cnt, x->mx_count.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  out[0] = acc / reps;
+  out[1] = cnt;
+  check_err(x);
+  API_END
+}
+
 int fcfd_time_residual(fcfd_ctx *x, int reps, int flush_l2, double *out, int out_len) {
   API_BEGIN
   CK(cudaSetDevice(x->device));
@@ -519,7 +632,7 @@ int fcfd_time_residual(fcfd_ctx *x, int reps, int flush_l2, double *out, int out
 int fcfd_ctx_set_exact_gradients(fcfd_ctx *x, int exact) {
   API_BEGIN
   if (!x) throw Error(FCFD_ERR_INPUT, "null context");
-  if (exact) x->cs.fast_grad = 0;
+  if (exact || x->dm.st_w) x->cs.fast_grad = 0;
   else {
     const fcfd_case *c = x->case_ptr;
     x->cs.fast_grad = (c->order == ORDER_FIRST || c->limiter == LIM_NONE || (c->limiter == LIM_VK && c->limiter_threshold > 0.)) ? 1 : 0;

@@ -130,6 +130,10 @@ struct fcfd_mesh {
   std::vector<double> st_recip;                              // [nc]: 1/det where the reciprocal division is exact, else 0
   std::vector<double> st_mirror;                             // [nc][3]: sum of the symmetry-mirror weights
   std::vector<uint8_t> has_lsq;                              // 1 if gradMap non-empty
+  // gradient maps as weights per stencil entry ([E][3], key order), built
+  // when some cell takes the curvilinear map (curvilinear_grad_map.cc)
+  bool grad_weights = false;
+  std::vector<double> st_w;
   std::vector<int32_t> color_index, color_cells;             // face-neighbour colouring
   std::vector<double> nodes;                                 // [nnode][3]
   double length_scale = 0, total_volume = 0;

@@ -105,12 +105,64 @@ __device__ __forceinline__ Dual<float> div_rn(Dual<float> a, Dual<float> b) {
   const float q = __fdiv_rn(a.v, b.v);
   return Dual<float>(q, (a.d - q * b.d) / b.v);
 }
+// ------------------------------------------------------------------ FP32 scalar
+// The scalar of the FP32 face pass of the mixed-precision residual: float
+// storage and float arithmetic, with every double operand (case constants,
+// geometry) rounded to float first -- the arithmetic Dual<float> gives its
+// value part, without the tangent.  A plain `float` would not do: the
+// kernels' double constants would promote each expression back to FP64.
+struct F32 {
+  float v;
+  __host__ __device__ F32() : v(0.f) {}
+  __host__ __device__ F32(double x) : v(float(x)) {}
+  __host__ __device__ static F32 of(float x) {
+    F32 r;
+    r.v = x;
+    return r;
+  }
+};
+__host__ __device__ __forceinline__ F32 operator+(F32 a, F32 b) { return F32::of(a.v + b.v); }
+__host__ __device__ __forceinline__ F32 operator-(F32 a, F32 b) { return F32::of(a.v - b.v); }
+__host__ __device__ __forceinline__ F32 operator*(F32 a, F32 b) { return F32::of(a.v * b.v); }
+__host__ __device__ __forceinline__ F32 operator/(F32 a, F32 b) { return F32::of(a.v / b.v); }
+__host__ __device__ __forceinline__ F32 operator-(F32 a) { return F32::of(-a.v); }
+__host__ __device__ __forceinline__ F32 operator+(F32 a, double b) { return F32::of(a.v + float(b)); }
+__host__ __device__ __forceinline__ F32 operator+(double a, F32 b) { return F32::of(float(a) + b.v); }
+__host__ __device__ __forceinline__ F32 operator-(F32 a, double b) { return F32::of(a.v - float(b)); }
+__host__ __device__ __forceinline__ F32 operator-(double a, F32 b) { return F32::of(float(a) - b.v); }
+__host__ __device__ __forceinline__ F32 operator*(F32 a, double b) { return F32::of(a.v * float(b)); }
+__host__ __device__ __forceinline__ F32 operator*(double a, F32 b) { return F32::of(float(a) * b.v); }
+__host__ __device__ __forceinline__ F32 operator/(F32 a, double b) { return F32::of(a.v / float(b)); }
+__host__ __device__ __forceinline__ F32 operator/(double a, F32 b) { return F32::of(float(a) / b.v); }
+#define FCFD_F32_CMP(op)                                                                                   \
+  __host__ __device__ __forceinline__ bool operator op(F32 a, F32 b) { return a.v op b.v; }                \
+  __host__ __device__ __forceinline__ bool operator op(F32 a, double b) { return a.v op float(b); }        \
+  __host__ __device__ __forceinline__ bool operator op(double a, F32 b) { return float(a) op b.v; }
+FCFD_F32_CMP(<)
+FCFD_F32_CMP(>)
+FCFD_F32_CMP(<=)
+FCFD_F32_CMP(>=)
+FCFD_F32_CMP(==)
+FCFD_F32_CMP(!=)
+#undef FCFD_F32_CMP
+__host__ __device__ __forceinline__ F32 sqrt(F32 a) { return F32::of(sqrtf(a.v)); }
+__host__ __device__ __forceinline__ F32 fabs(F32 a) { return F32::of(fabsf(a.v)); }
+__host__ __device__ __forceinline__ F32 pow(F32 a, double e) { return F32::of(powf(a.v, float(e))); }
+__host__ __device__ __forceinline__ F32 tanh(F32 a) { return F32::of(tanhf(a.v)); }
+__device__ __forceinline__ F32 mul_rn(F32 a, F32 b) { return F32::of(__fmul_rn(a.v, b.v)); }
+__device__ __forceinline__ F32 add_rn(F32 a, F32 b) { return F32::of(__fadd_rn(a.v, b.v)); }
+__device__ __forceinline__ F32 sub_rn(F32 a, F32 b) { return F32::of(__fsub_rn(a.v, b.v)); }
+__device__ __forceinline__ F32 div_rn(F32 a, F32 b) { return F32::of(__fdiv_rn(a.v, b.v)); }
+__host__ __device__ __forceinline__ float val(F32 x) { return x.v; }
+__host__ __device__ __forceinline__ double tan_of(F32) { return 0.; }
+
 __host__ __device__ __forceinline__ double val(double x) { return x; }
 __host__ __device__ __forceinline__ float val(float x) { return x; }
 template <class T> __host__ __device__ __forceinline__ T val(const Dual<T> &x) { return x.v; }
 __host__ __device__ __forceinline__ double tan_of(double) { return 0.; }
 template <class S> struct Mk;
 template <> struct Mk<double> { __host__ __device__ static double of(double v, double) { return v; } };
+template <> struct Mk<F32> { __host__ __device__ static F32 of(double v, double) { return F32(v); } };
 template <class T> struct Mk<Dual<T>> { __host__ __device__ static Dual<T> of(double v, double d) { return Dual<T>(T(v), T(d)); } };
 template <class T> __host__ __device__ __forceinline__ T tan_of(const Dual<T> &x) { return x.d; }
 
@@ -170,6 +222,7 @@ struct DevMesh {
   const double *st_recip;                  // [nc] 1/det where the reciprocal division is exact, else 0
   const double *c_vol;                     // [nc] cell volumes (Green-Gauss gradients)
   const double *st_mirror;                 // [3][nc] summed symmetry-mirror weights
+  const double *st_w = nullptr;            // [E][3] stored map weights (curvilinear cases), else null
   const int *bface;                        // boundary faces in ghost order [nb]
   const int *outlet_faces;                 // outlet boundary faces [n_outlet]
   const double *f_wall, *f_diss;           // [nf] wall distance, dissipation factor (Steger-Warming only)
@@ -383,8 +436,10 @@ __device__ __forceinline__ void centre_state(const DevCase &c, const S *W, int n
 
 // Reconstructed state of cell k at face point xf (left_state_update,
 // ns_assemble_linear_system.cc:269-294).
-template <class S>
-__device__ __forceinline__ void recon_state(const DevCase &c, const DevMesh &m, const S *W, const S *G, const S *Lm, int k,
+// SA: the element type of W, G, Lm (S itself, or double under the FP32 face
+// pass of the mixed-precision residual, which loads FP64 arrays).
+template <class S, class SA = S>
+__device__ __forceinline__ void recon_state(const DevCase &c, const DevMesh &m, const SA *W, const SA *G, const SA *Lm, int k,
                                             const double xf[3], FState<S> &s, const double n[3]) {
   const int nt = m.nt, nc = m.nc;
   const double d0 = xf[0] - m.c_x[k], d1 = xf[1] - m.c_x[nt + k], d2 = xf[2] - m.c_x[2 * nt + k];
@@ -629,6 +684,21 @@ __global__ void __launch_bounds__(128, (!FAST && std::is_same<S, double>::value)
     // the mesh builder verified it returns the IEEE quotient for every weight.
     // (Weights precomputed on the host and streamed from HBM measured slower:
     // 200 against 190 us on the prism mesh.)
+    if (m.st_w) {
+      // stored map weights (curvilinear maps, and the least-squares maps of a
+      // mesh that has any): grad += weight * phi in key order
+      for (int j = j0; j < j1; ++j) {
+        const int k = m.st_keys[j];
+        const double wt0 = m.st_w[3 * (size_t)j], wt1 = m.st_w[3 * (size_t)j + 1], wt2 = m.st_w[3 * (size_t)j + 2];
+#pragma unroll
+        for (int v = 0; v < 5; ++v) {
+          const S phi = W[v * nt + k];
+          g[3 * v] = add_rn(g[3 * v], mul_rn(S(wt0), phi));
+          g[3 * v + 1] = add_rn(g[3 * v + 1], mul_rn(S(wt1), phi));
+          g[3 * v + 2] = add_rn(g[3 * v + 2], mul_rn(S(wt2), phi));
+        }
+      }
+    }
     const double C00 = m.st_cof[c], C01 = m.st_cof[nc + c], C02 = m.st_cof[2 * nc + c];
     const double C11 = m.st_cof[3 * nc + c], C12 = m.st_cof[4 * nc + c], C22 = m.st_cof[5 * nc + c];
     const double det = m.st_cof[6 * nc + c];
@@ -641,7 +711,7 @@ __global__ void __launch_bounds__(128, (!FAST && std::is_same<S, double>::value)
       }
       return __ddiv_rn(x, det);
     };
-    for (int j = j0; j < j1; ++j) {
+    for (int j = m.st_w ? j1 : j0; j < j1; ++j) {
       const int k = m.st_keys[j];
       double wt0, wt1, wt2;
       if (k == c) {
@@ -1326,15 +1396,15 @@ __device__ __forceinline__ void face_D(const DevCase &cs, const DevMesh &m, int 
 // is left to the outlet kernel); 2 computes it here (the walk back of
 // cached_right_rho) and stores it in `stale`.  Returns true when the states
 // are complete.
-template <class S, int STALE = 0>
+template <class S, int STALE = 0, class SA = S>
 __device__ __forceinline__ bool face_states(const DevCase &cs, const DevMesh &m, int f, const double n[3], int b, int pa,
-                                            int nb, const S *__restrict__ W, const S *__restrict__ G, const S *__restrict__ Lm,
+                                            int nb, const SA *__restrict__ W, const SA *__restrict__ G, const SA *__restrict__ Lm,
                                             S *stale, FState<S> &L, FState<S> &R, int *err) {
   const int nf = m.nf, nt = m.nt, nc = m.nc;
   const double xf[3] = {m.f_x[f], m.f_x[nf + f], m.f_x[2 * nf + f]};
-  recon_state(cs, m, W, G, Lm, pa, xf, L, n);
+  recon_state<S, SA>(cs, m, W, G, Lm, pa, xf, L, n);
   if (b < 0) {
-    recon_state(cs, m, W, G, Lm, nb, xf, R, n);
+    recon_state<S, SA>(cs, m, W, G, Lm, nb, xf, R, n);
   } else {
     R.pc = W[nb]; R.Vc[0] = W[nt + nb]; R.Vc[1] = W[2 * nt + nb]; R.Vc[2] = W[3 * nt + nb]; R.Tc = W[4 * nt + nb];
     R.rho = S(0.);

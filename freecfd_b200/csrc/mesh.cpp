@@ -17,6 +17,7 @@
 #include <array>
 #include <cmath>
 #include <cstring>
+#include <map>
 #include <unordered_map>
 
 #include "internal.hpp"
@@ -74,6 +75,123 @@ bool in_box(const P3 &p, const double *c1, const double *c2) {
 // `faces` non-null: a face-based grid (create_faces2,
 // grid_create_elements.cc:444-553), whose cell node lists in `raw` are the
 // sorted node sets of the cells (grid_reader_tec.cc:236-262).
+// Curvilinear gradient map of cell c (curvilinear_grad_map.cc:28-228): three
+// pairs of the cell's faces define a local (xi, eta, zeta) frame; Jac row i
+// is the centroid of the cell across face "plus" of pair i minus the centroid
+// across face "minus"; the gradient is Jac^-T applied to the pair
+// differences, i.e. weights +-Jac_invT[i] on the six cells across the faces,
+// accumulated into a map keyed by cell (std::map order).
+//   hexahedra: the faces (positions in the cell's face list, ascending) are
+//     taken in turn, each paired with the most opposite outward normal among
+//     the later faces not yet paired (first minimum of the dot product).  The
+//     reference erases the current element of the std::set it is iterating
+//     and then increments that iterator (lines 58-77: undefined behaviour);
+//     this is the pairing that loop is written to produce.
+//   other cells: every ordered choice of three face pairs over the cell's
+//     faces (ascending face ids, the nested loops of lines 97-153), keeping
+//     the first that maximises the determinant.
+// Throws FCFD_ERR_MESH where no positive determinant exists (the reference
+// would then index cell -1).
+static void curvilinear_map(const fcfd_mesh &m, int c, bool hexa, const std::vector<double> &cx,
+                            std::map<int32_t, P3> &gm) {
+  const int j0 = m.cf_index[c], nfc = m.cf_index[c + 1] - j0;
+  auto cent = [&](int k) { return P3{cx[3 * (size_t)k], cx[3 * (size_t)k + 1], cx[3 * (size_t)k + 2]}; };
+  auto across = [&](int f) {
+    int o = m.f_neighbor[f];
+    if (o == c) o = m.f_parent[f];
+    return o;
+  };
+  auto outward = [&](int f) {
+    P3 n{m.f_normal[3 * (size_t)f], m.f_normal[3 * (size_t)f + 1], m.f_normal[3 * (size_t)f + 2]};
+    if (m.f_parent[f] != c) n = scl(-1., n);
+    return n;
+  };
+  int cp[6] = {-1, -1, -1, -1, -1, -1};
+  P3 J[3] = {{0., 0., 0.}, {0., 0., 0.}, {0., 0., 0.}};
+  if (hexa) {
+    std::vector<int> rest;
+    for (int k = 0; k < nfc; ++k) rest.push_back(k);
+    int fp[6] = {-1, -1, -1, -1, -1, -1};
+    int counter = 0;
+    while (!rest.empty() && counter < 3) {
+      const int a = rest[0];
+      const P3 my = outward(m.cf_list[j0 + a]);
+      double minp = 1.e20;
+      int b = -1;
+      for (size_t t = 1; t < rest.size(); ++t) {
+        const double pr = dot(my, outward(m.cf_list[j0 + rest[t]]));
+        if (pr < minp) { minp = pr; b = rest[t]; }
+      }
+      if (b < 0) throw Error(FCFD_ERR_MESH, "curvilinear gradient: a hexahedron face without an opposite face");
+      fp[2 * counter + 1] = a;
+      fp[2 * counter] = b;
+      rest.erase(std::remove(rest.begin(), rest.end(), b), rest.end());
+      rest.erase(rest.begin());
+      ++counter;
+    }
+    if (counter < 3) throw Error(FCFD_ERR_MESH, "curvilinear gradient: a hexahedron without three face pairs");
+    for (int i = 0; i < 3; ++i) {
+      cp[2 * i + 1] = across(m.cf_list[j0 + fp[2 * i + 1]]);
+      cp[2 * i] = across(m.cf_list[j0 + fp[2 * i]]);
+      J[i] = sub(cent(cp[2 * i + 1]), cent(cp[2 * i]));
+    }
+  } else {
+    std::vector<int> F(m.cf_list.begin() + j0, m.cf_list.begin() + j0 + nfc);
+    std::sort(F.begin(), F.end());
+    F.erase(std::unique(F.begin(), F.end()), F.end());
+    const int n = (int)F.size();
+    double max_det = 0.;
+    bool found = false;
+    int t[6];
+    P3 T[3];
+    for (int i1 = 0; i1 < n; ++i1)
+      for (int i2 = i1; i2 < n; ++i2) {
+        t[1] = across(F[i2]); t[0] = across(F[i1]);
+        T[0] = sub(cent(t[1]), cent(t[0]));
+        for (int i3 = i1; i3 < n; ++i3)
+          for (int i4 = i3; i4 < n; ++i4) {
+            t[3] = across(F[i4]); t[2] = across(F[i3]);
+            T[1] = sub(cent(t[3]), cent(t[2]));
+            for (int i5 = i2; i5 < n; ++i5)
+              for (int i6 = i5; i6 < n; ++i6) {
+                t[5] = across(F[i6]); t[4] = across(F[i5]);
+                T[2] = sub(cent(t[5]), cent(t[4]));
+                const double det = dot(T[0], crs(T[1], T[2]));
+                if (det > max_det) {
+                  max_det = det;
+                  found = true;
+                  for (int q = 0; q < 6; ++q) cp[q] = t[q];
+                  for (int q = 0; q < 3; ++q) J[q] = T[q];
+                }
+              }
+          }
+      }
+    if (!found) throw Error(FCFD_ERR_MESH, "curvilinear gradient: no face pairs with a positive determinant");
+  }
+  const double det = dot(J[0], crs(J[1], J[2]));
+  const double a00 = J[0].x, a01 = J[0].y, a02 = J[0].z, a10 = J[1].x, a11 = J[1].y, a12 = J[1].z;
+  const double a20 = J[2].x, a21 = J[2].y, a22 = J[2].z;
+  P3 I[3];
+  I[0].x = (a11 * a22 - a12 * a21) / det;
+  I[1].x = (a02 * a21 - a01 * a22) / det;
+  I[2].x = (a01 * a12 - a02 * a11) / det;
+  I[0].y = (a12 * a20 - a10 * a22) / det;
+  I[1].y = (a00 * a22 - a02 * a20) / det;
+  I[2].y = (a02 * a10 - a00 * a12) / det;
+  I[0].z = (a10 * a21 - a11 * a20) / det;
+  I[1].z = (a01 * a20 - a00 * a21) / det;
+  I[2].z = (a00 * a11 - a01 * a10) / det;
+  gm.clear();
+  gm.insert({cp[0], scl(-1., I[0])});
+  for (int q = 1; q < 6; ++q) {
+    const P3 &v = I[q / 2];
+    const bool plus = (q & 1) != 0;
+    auto it = gm.find(cp[q]);
+    if (it == gm.end()) gm.insert({cp[q], plus ? v : scl(-1., v)});
+    else it->second = plus ? add(it->second, v) : sub(it->second, v);
+  }
+}
+
 fcfd_mesh *build_mesh(const fcfd_raw_mesh &raw, fcfd_case &cs, const FaceInput *faces) {
   auto M = new fcfd_mesh();
   fcfd_mesh &m = *M;
@@ -529,10 +647,29 @@ fcfd_mesh *build_mesh(const fcfd_raw_mesh &raw, fcfd_case &cs, const FaceInput *
       std::vector<int32_t> st;
       std::vector<P3> dist;
       std::vector<double> w;
+      auto method_of = [&](int c) {
+        const int nn = raw.conn_index[c + 1] - raw.conn_index[c];
+        return (nn == 8) ? cs.hex_method : (nn == 6 ? cs.prism_method : cs.other_method);
+      };
+      // With any curvilinear cell every gradient map is stored as weights per
+      // stencil entry (st_w), in the entries' key order: the device sums
+      // w . phi over them instead of rebuilding least-squares weights.
+      for (int c = 0; c < nc; ++c)
+        if (method_of(c) == GM_CURVILINEAR) m.grad_weights = true;
+      std::map<int32_t, P3> gm;
       for (int c = 0; c < nc; ++c) {
-        int nn = raw.conn_index[c + 1] - raw.conn_index[c];
-        int meth = (nn == 8) ? cs.hex_method : (nn == 6 ? cs.prism_method : cs.other_method);
-        if (meth == GM_CURVILINEAR) throw Error(FCFD_ERR_UNSUPPORTED, "curvilinear gradients are not supported; set hex/prism method=lsqr");
+        const int nn = raw.conn_index[c + 1] - raw.conn_index[c];
+        const int meth = method_of(c);
+        if (meth == GM_CURVILINEAR) {
+          curvilinear_map(m, c, nn == 8, m.c_centroid, gm);
+          m.has_lsq[c] = 1;
+          for (const auto &kv : gm) {
+            m.st_keys.push_back(kv.first);
+            m.st_w.push_back(kv.second.x); m.st_w.push_back(kv.second.y); m.st_w.push_back(kv.second.z);
+          }
+          m.st_index[c + 1] = (int)m.st_keys.size();
+          continue;
+        }
         if (meth == GM_GREENGAUSS) {
           // empty gradient map: the gradient falls back to Green-Gauss
           // (variable.h:204-213), evaluated per face on the device
@@ -607,6 +744,24 @@ fcfd_mesh *build_mesh(const fcfd_raw_mesh &raw, fcfd_case &cs, const FaceInput *
         keys.erase(std::unique(keys.begin(), keys.end()), keys.end());
         m.st_keys.insert(m.st_keys.end(), keys.begin(), keys.end());
         m.st_index[c + 1] = (int)m.st_keys.size();
+        if (m.grad_weights) {
+          // the map's weights: each neighbour's own insert (its first and
+          // only occurrence), the accumulated self entry
+          for (int32_t key : keys) {
+            if (key == c) {
+              m.st_w.push_back(s0); m.st_w.push_back(s1); m.st_w.push_back(s2);
+              continue;
+            }
+            size_t k = 0;
+            while (st[k] != key) ++k;
+            const P3 &dk = dist[k];
+            double w0 = w[k] * (dk.x * C00 + dk.y * C01 + dk.z * C02);
+            double w1 = w[k] * (dk.x * C01 + dk.y * C11 + dk.z * C12);
+            double w2 = w[k] * (dk.x * C02 + dk.y * C12 + dk.z * C22);
+            w0 /= det; w1 /= det; w2 /= det;
+            m.st_w.push_back(w0); m.st_w.push_back(w1); m.st_w.push_back(w2);
+          }
+        }
       }
     }
   } catch (...) {
@@ -614,6 +769,127 @@ fcfd_mesh *build_mesh(const fcfd_raw_mesh &raw, fcfd_case &cs, const FaceInput *
     throw;
   }
   return M;
+}
+
+// Reverse Cuthill-McKee order of the interior cells over the face-neighbour
+// graph (interior faces).  The reference orders its cells by the element
+// order of the grid file and, when partitioned, by ParMETIS
+// (grid_partition.cc:25-141); a grid whose elements come unordered (a
+// face-based Tecplot file, a shuffled export) leaves the face kernels'
+// gathers scattered over memory.  This order (Cuthill & McKee 1969, reversed
+// as in George 1971) keeps face neighbours close in index, so the cells a
+// warp gathers share cache lines.  Per connected component (taken in order of
+// their lowest-numbered least-degree cell): a pseudo-peripheral start cell
+// (Gibbs-Poole-Stockmeyer / George-Liu search: breadth-first level sets from
+// the current start, move to the least-degree cell of the last level while
+// the eccentricity grows), then breadth-first from it, each cell's unvisited
+// neighbours in ascending (degree, index); the whole sequence is reversed.
+// perm[new] = old.  Deterministic: ties always go to the lower index.
+void rcm_order(const fcfd_mesh &m, std::vector<int32_t> &perm) {
+  const int nc = m.nc;
+  std::vector<int32_t> ai(nc + 1, 0), aj;
+  for (int f = 0; f < m.nf; ++f) {
+    if (m.f_bc[f] >= 0) continue;
+    const int a = m.f_parent[f], b = m.f_neighbor[f];
+    if (a < 0 || b < 0 || a >= nc || b >= nc || a == b) continue;
+    ai[a + 1]++; ai[b + 1]++;
+  }
+  for (int c = 0; c < nc; ++c) ai[c + 1] += ai[c];
+  aj.resize(ai[nc]);
+  {
+    std::vector<int32_t> fill(ai.begin(), ai.end() - 1);
+    for (int f = 0; f < m.nf; ++f) {
+      if (m.f_bc[f] >= 0) continue;
+      const int a = m.f_parent[f], b = m.f_neighbor[f];
+      if (a < 0 || b < 0 || a >= nc || b >= nc || a == b) continue;
+      aj[fill[a]++] = b;
+      aj[fill[b]++] = a;
+    }
+  }
+  // distinct neighbours (two cells can share more than one face), then
+  // ascending (degree, index)
+  std::vector<int32_t> deg(nc);
+  {
+    std::vector<int32_t> ai2(nc + 1, 0), aj2;
+    aj2.reserve(aj.size());
+    for (int c = 0; c < nc; ++c) {
+      std::vector<int32_t> v(aj.begin() + ai[c], aj.begin() + ai[c + 1]);
+      std::sort(v.begin(), v.end());
+      v.erase(std::unique(v.begin(), v.end()), v.end());
+      aj2.insert(aj2.end(), v.begin(), v.end());
+      ai2[c + 1] = (int32_t)aj2.size();
+    }
+    ai.swap(ai2);
+    aj.swap(aj2);
+    for (int c = 0; c < nc; ++c) deg[c] = ai[c + 1] - ai[c];
+    for (int c = 0; c < nc; ++c)
+      std::sort(aj.begin() + ai[c], aj.begin() + ai[c + 1],
+                [&](int32_t a, int32_t b) { return deg[a] != deg[b] ? deg[a] < deg[b] : a < b; });
+  }
+  std::vector<uint8_t> done(nc, 0);
+  std::vector<int32_t> level(nc, -1), order;
+  order.reserve(nc);
+  // breadth-first level sets from r over the not-yet-ordered cells; returns
+  // the eccentricity and the least-degree (lowest index) cell of the last level
+  std::vector<int32_t> touched;
+  auto bfs_last = [&](int r, int &ecc) -> int {
+    touched.clear();
+    std::vector<int32_t> cur{r}, nxt;
+    level[r] = 0;
+    touched.push_back(r);
+    ecc = 0;
+    std::vector<int32_t> last = cur;
+    while (!cur.empty()) {
+      nxt.clear();
+      for (int c : cur)
+        for (int k = ai[c]; k < ai[c + 1]; ++k) {
+          const int o = aj[k];
+          if (done[o] || level[o] >= 0) continue;
+          level[o] = level[c] + 1;
+          touched.push_back(o);
+          nxt.push_back(o);
+        }
+      if (nxt.empty()) break;
+      ++ecc;
+      last = nxt;
+      cur.swap(nxt);
+    }
+    for (int c : touched) level[c] = -1;
+    int best = last[0];
+    for (int c : last)
+      if (deg[c] < deg[best] || (deg[c] == deg[best] && c < best)) best = c;
+    return best;
+  };
+  for (;;) {
+    int seed = -1;
+    for (int c = 0; c < nc; ++c)
+      if (!done[c] && (seed < 0 || deg[c] < deg[seed])) seed = c;
+    if (seed < 0) break;
+    int ecc = 0;
+    int cand = bfs_last(seed, ecc);
+    for (;;) {
+      int ecc2 = 0;
+      const int cand2 = bfs_last(cand, ecc2);
+      if (ecc2 <= ecc) break;
+      seed = cand;
+      ecc = ecc2;
+      cand = cand2;
+    }
+    // Cuthill-McKee from the pseudo-peripheral cell `seed`
+    size_t head = order.size();
+    order.push_back(seed);
+    done[seed] = 1;
+    while (head < order.size()) {
+      const int c = order[head++];
+      for (int k = ai[c]; k < ai[c + 1]; ++k) {
+        const int o = aj[k];
+        if (done[o]) continue;
+        done[o] = 1;
+        order.push_back(o);
+      }
+    }
+  }
+  perm.assign(order.rbegin(), order.rend());
 }
 
 }  // namespace fcfd

@@ -227,10 +227,13 @@ __global__ void k_precond(int nc, const double *__restrict__ Minv, const T *__re
 
 // r = D^-1 v rounded to the preconditioner's type P, y = Minv r: the start of
 // the Gauss-Seidel preconditioner in one pass
+// (bar: the persistent Gauss-Seidel kernel's barrier counter, zeroed here, or null)
 template <class T, class P>
 __global__ void k_precond_split(int nc, const double *__restrict__ Minv, const T *__restrict__ v,
-                                const RowScale *__restrict__ rs, P *__restrict__ r, P *__restrict__ y) {
+                                const RowScale *__restrict__ rs, P *__restrict__ r, P *__restrict__ y,
+                                unsigned *bar = nullptr) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (bar && c == 0) bar[0] = 0u;
   if (c >= nc) return;
   double xv[5];
 #pragma unroll
@@ -370,6 +373,173 @@ __global__ void __launch_bounds__(160) k_gs_rows(int nc, int deg, int cnt, const
 #pragma unroll
     for (int k = 0; k < 5; ++k) v += MinvP[(size_t)(5 * q + k) * cnt + i] * ts[k][threadIdx.x];
     y[q * nc + c] = v;
+  }
+}
+
+// ---- all colour updates of one preconditioner application in one launch
+//
+// The per-colour launches above leave a 16k-cell colour update latency-bound
+// (a few microseconds of work per launch, most of it the launch ramp and the
+// dependent index -> neighbour loads).  Here one cooperative grid runs every
+// colour update of the symmetric sweeps in turn, with a grid-wide barrier
+// between updates: block b takes the b-th chunk of each colour's cells, so
+// with STAGE its couplings, inverse diagonal blocks, neighbour lists and
+// right-hand side are read from HBM once per application into shared memory
+// (they fit for FP32 couplings up to ~60k cells on 148 SMs) and every update
+// reads them from there; only the neighbours' y crosses the barrier, through
+// L2 (ld.global.cg).  The arithmetic per (cell, row) is k_gs_rows's, in the
+// same order.  The barrier is an arrival counter that the preceding
+// k_precond_split zeroes; a block that waits longer than kGsSpinLimit polls
+// sets the timeout word and every later barrier of the launch stops waiting,
+// so the launch always ends and the host reports FCFD_ERR_TIMEOUT.
+constexpr int kGsZ = 4;                   // 32-cell groups per block (640 threads)
+constexpr int kGsMaxCol = 32;             // colours of the greedy face-neighbour colouring
+constexpr unsigned kGsSpinLimit = 1u << 22;  // polls of ~64 ns: > 0.25 s per barrier
+
+struct GsPersistArgs {
+  int nc, deg, ncol, nphase;
+  const int *sched;   // [nphase] colour of each update
+  const int *cells;   // cells by colour
+  const int *nbr;     // [deg][cells of the colour] per colour
+  unsigned *bar;      // [0] arrivals (zeroed before the launch), [1] timeout flag
+  int cidx[kGsMaxCol + 1];  // colour offsets
+  int soff[kGsMaxCol + 1];  // STAGE: offset of each colour's chunk in the staged arrays (prefix sums of chunk sizes)
+};
+
+__device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned *p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// grid barrier number `k` (1-based) of the launch: every block arrives once.
+// The block's writes are ordered before the arrival by __syncthreads and the
+// release reduction (cumulative); the acquire load that sees every arrival
+// orders the other blocks' writes before this block's later reads.
+__device__ __forceinline__ void gs_grid_barrier(unsigned *bar, unsigned k) {
+  __syncthreads();
+  if (threadIdx.x == 0 && threadIdx.y == 0 && threadIdx.z == 0) {
+    asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(bar), "r"(1u) : "memory");
+    const unsigned target = k * gridDim.x;
+    if (!ld_acquire_gpu(&bar[1])) {
+      unsigned it = 0;
+      while (ld_acquire_gpu(&bar[0]) < target) {
+        if (++it > kGsSpinLimit) {
+          atomicExch(&bar[1], 1u);
+          break;
+        }
+        if (it > 256) __nanosleep(32);
+      }
+    }
+  }
+  __syncthreads();
+}
+
+template <class P, bool STAGE, int DMAX>
+__global__ void __launch_bounds__(32 * 5 * kGsZ, 1) k_gs_persist(GsPersistArgs a, const P *__restrict__ OB,
+                                                                 const P *__restrict__ MinvP, const P *__restrict__ r,
+                                                                 P *y) {
+  extern __shared__ __align__(16) unsigned char gs_smem[];
+  constexpr int NG = 32 * kGsZ;  // cells per pass
+  const int lx = threadIdx.x, q = threadIdx.y, z = threadIdx.z;
+  const int tid = lx + 32 * (q + 5 * z), nthr = 32 * 5 * kGsZ;
+  const int nb = gridDim.x, b = blockIdx.x, nc = a.nc, deg = a.deg;
+  P *ts = reinterpret_cast<P *>(gs_smem);  // [5][NG]
+  // staged arrays (STAGE): per colour, this block's chunk at offset soff[col]
+  // with stride ch = chunk size of the colour
+  const int stot = a.soff[a.ncol];
+  P *sOB = ts + 5 * NG;                       // [stot * deg * 25]
+  P *sMi = sOB + (size_t)stot * deg * 25;     // [stot * 25]
+  P *sR = sMi + (size_t)stot * 25;            // [stot * 5]
+  int *sCell = reinterpret_cast<int *>(sR + (size_t)stot * 5);  // [stot]
+  int *sNbr = sCell + stot;                   // [stot * deg]
+  if constexpr (STAGE) {
+    for (int col = 0; col < a.ncol; ++col) {
+      const int base = a.cidx[col], cnt = a.cidx[col + 1] - base;
+      const int ch = a.soff[col + 1] - a.soff[col];
+      const int lo = b * ch, n = max(0, min(cnt, lo + ch) - lo);
+      const int so = a.soff[col];
+      for (int t = tid; t < n; t += nthr) {
+        const int c = a.cells[base + lo + t];
+        sCell[so + t] = c;
+        for (int v = 0; v < 5; ++v) sR[(size_t)so * 5 + v * ch + t] = r[(size_t)v * nc + c];
+      }
+      for (int t = tid; t < n * deg; t += nthr) {
+        const int sl = t / n, i = t - sl * n;
+        sNbr[(size_t)so * deg + sl * ch + i] = a.nbr[(size_t)base * deg + (size_t)sl * cnt + lo + i];
+      }
+      for (int t = tid; t < n * deg * 25; t += nthr) {
+        const int e = t / n, i = t - e * n;  // e = slot * 25 + entry
+        sOB[(size_t)so * deg * 25 + (size_t)e * ch + i] = OB[(size_t)base * deg * 25 + (size_t)e * cnt + lo + i];
+      }
+      for (int t = tid; t < n * 25; t += nthr) {
+        const int e = t / n, i = t - e * n;
+        sMi[(size_t)so * 25 + (size_t)e * ch + i] = MinvP[(size_t)base * 25 + (size_t)e * cnt + lo + i];
+      }
+    }
+    __syncthreads();
+  }
+  for (int ph = 0; ph < a.nphase; ++ph) {
+    const int col = a.sched[ph];
+    const int base = a.cidx[col], cnt = a.cidx[col + 1] - base;
+    const int ch = STAGE ? a.soff[col + 1] - a.soff[col] : (cnt + nb - 1) / nb;
+    const int lo = b * ch, hi = min(cnt, lo + ch);
+    const int so = STAGE ? a.soff[col] : 0;
+    for (int i0 = lo; i0 < hi; i0 += NG) {
+      const int i = i0 + 32 * z + lx, li = i - lo;
+      const bool act = i < hi;
+      int c = 0;
+      P t = P(0.);
+      if (act) {
+        if constexpr (STAGE) {
+          c = sCell[so + li];
+          t = sR[(size_t)so * 5 + q * ch + li];
+        } else {
+          c = a.cells[base + i];
+          t = r[(size_t)q * nc + c];
+        }
+        int o[DMAX];
+#pragma unroll
+        for (int sl = 0; sl < DMAX; ++sl)
+          o[sl] = sl < deg ? (STAGE ? sNbr[(size_t)so * deg + sl * ch + li] : a.nbr[(size_t)base * deg + (size_t)sl * cnt + i])
+                           : -1;
+        P yv[DMAX][5];
+#pragma unroll
+        for (int sl = 0; sl < DMAX; ++sl)
+#pragma unroll
+          for (int k = 0; k < 5; ++k) yv[sl][k] = o[sl] >= 0 ? __ldcg(y + (size_t)k * nc + o[sl]) : P(0.);
+#pragma unroll
+        for (int sl = 0; sl < DMAX; ++sl) {
+          if (o[sl] < 0) continue;
+          P acc = P(0.);
+          if constexpr (STAGE) {
+            const P *B = sOB + (size_t)so * deg * 25 + (size_t)(sl * 25 + 5 * q) * ch + li;
+#pragma unroll
+            for (int k = 0; k < 5; ++k) acc += B[(size_t)k * ch] * yv[sl][k];
+          } else {
+            const P *B = OB + (size_t)base * deg * 25 + ((size_t)sl * 25 + 5 * q) * cnt + i;
+#pragma unroll
+            for (int k = 0; k < 5; ++k) acc += B[(size_t)k * cnt] * yv[sl][k];
+          }
+          t += acc;
+        }
+      }
+      ts[q * NG + 32 * z + lx] = t;
+      __syncthreads();
+      if (act) {
+        P v = P(0.);
+        if constexpr (STAGE) {
+#pragma unroll
+          for (int k = 0; k < 5; ++k) v += sMi[(size_t)so * 25 + (size_t)(5 * q + k) * ch + li] * ts[k * NG + 32 * z + lx];
+        } else {
+#pragma unroll
+          for (int k = 0; k < 5; ++k) v += MinvP[(size_t)base * 25 + (size_t)(5 * q + k) * cnt + i] * ts[k * NG + 32 * z + lx];
+        }
+        y[(size_t)q * nc + c] = v;
+      }
+      __syncthreads();
+    }
+    if (ph + 1 < a.nphase) gs_grid_barrier(a.bar, (unsigned)(ph + 1));
   }
 }
 
@@ -678,7 +848,130 @@ struct NewtonState {
   int sweeps = 0, cycles = 1;
   IterConsts hic;      // host copy of the iteration scalars
   DBuf<IterConsts> ic; // their device copy
+  // persistent Gauss-Seidel launch (k_gs_persist): on when the options ask
+  // for it and the colouring fits its limits
+  bool gs_persist = false, gs_stage = false;
+  int gs_blocks = 0, gs_dmax = 0;  // gs_dmax: neighbour slots the kernel is compiled for (4 or kGsMaxDeg)
+  size_t gs_smem = 0;
+  GsPersistArgs gs_args{};
+  DBuf<int> gs_sched;
+  DBuf<unsigned> gs_bar;  // [0] barrier arrivals, [1] timeout flag
 };
+
+// Colour of every Gauss-Seidel update of one preconditioner application with
+// `sweeps` symmetric sweeps: colours forward, then backward, skipping a
+// colour that would be updated twice in a row (no change) and empty colours.
+static std::vector<int> gs_schedule(const std::vector<int> &ci, int sweeps) {
+  const int ncol = (int)ci.size() - 1;
+  std::vector<int> out;
+  int last = -1;
+  for (int k = 0; k < sweeps; ++k)
+    for (int pass = 0; pass < 2; ++pass)
+      for (int q = 0; q < ncol; ++q) {
+        const int col = pass == 0 ? q : ncol - 1 - q;
+        if (ci[col + 1] - ci[col] <= 0 || col == last) continue;
+        last = col;
+        out.push_back(col);
+      }
+  return out;
+}
+
+// Grid size, shared memory and staging of k_gs_persist for couplings of type
+// P: one block per SM with the couplings staged when they fit in shared
+// memory, else as many co-resident blocks as the occupancy allows (at least
+// 32 cells of the largest colour per block).
+template <class P>
+static void plan_gs_persist(fcfd_ctx *x, NewtonState &ns) {
+  const std::vector<int> &ci = x->color_index;
+  const int ncol = (int)ci.size() - 1, deg = x->gs_deg;
+  if (ncol < 1 || ncol > kGsMaxCol || deg < 1 || deg > kGsMaxDeg) return;
+  const std::vector<int> sched = gs_schedule(ci, ns.sweeps);
+  if (sched.empty()) return;
+  int nsm = 0, coop = 0, optin = 0;
+  CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, x->device));
+  CK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, x->device));
+  CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, x->device));
+  if (!coop || nsm < 1) return;
+  int maxcnt = 0;
+  for (int col = 0; col < ncol; ++col) maxcnt = std::max(maxcnt, ci[col + 1] - ci[col]);
+  const int need = std::max(1, (maxcnt + 31) / 32);
+  const size_t ts_bytes = sizeof(P) * 5 * 32 * kGsZ;
+  auto chunks = [&](int nb, int *soff) {
+    soff[0] = 0;
+    for (int col = 0; col < ncol; ++col) soff[col + 1] = soff[col] + (ci[col + 1] - ci[col] + nb - 1) / nb;
+    return soff[ncol];
+  };
+  GsPersistArgs &a = ns.gs_args;
+  a.nc = x->dm.nc; a.deg = deg; a.ncol = ncol; a.nphase = (int)sched.size();
+  a.cells = x->color_cells.p; a.nbr = x->gs_nbr.p;
+  for (int col = 0; col <= ncol; ++col) a.cidx[col] = ci[col];
+  const int threads = 32 * 5 * kGsZ;
+  int nb = std::min(nsm, need);
+  const int stot = chunks(nb, a.soff);
+  const size_t stage_bytes = ts_bytes + (size_t)stot * ((size_t)deg * 25 + 30) * sizeof(P) + (size_t)stot * (1 + deg) * sizeof(int);
+  int occ = 0;
+  ns.gs_dmax = deg <= 4 ? 4 : kGsMaxDeg;
+  auto kern = [&](bool stage) -> const void * {
+    if (ns.gs_dmax == 4) return stage ? (const void *)k_gs_persist<P, true, 4> : (const void *)k_gs_persist<P, false, 4>;
+    return stage ? (const void *)k_gs_persist<P, true, kGsMaxDeg> : (const void *)k_gs_persist<P, false, kGsMaxDeg>;
+  };
+  if (stage_bytes <= (size_t)optin) {
+    CK(cudaFuncSetAttribute(kern(true), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stage_bytes));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern(true), threads, stage_bytes));
+    if (occ >= 1) {
+      ns.gs_stage = true;
+      ns.gs_smem = stage_bytes;
+    }
+  }
+  if (!ns.gs_stage) {
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern(false), threads, ts_bytes));
+    if (occ < 1) return;
+    nb = std::min(nsm * occ, need);
+    chunks(nb, a.soff);
+    ns.gs_smem = ts_bytes;
+  }
+  ns.gs_blocks = nb;
+  ns.gs_sched.upload(sched);
+  ns.gs_bar.alloc(2);
+  CK(cudaMemsetAsync(ns.gs_bar.p, 0, 2 * sizeof(unsigned), x->stream));
+  a.sched = ns.gs_sched.p;
+  a.bar = ns.gs_bar.p;
+  ns.gs_persist = true;
+}
+
+template <class P>
+static void launch_gs_persist(fcfd_ctx *x, NewtonState &ns, const P *OB, const P *MinvP, const P *r, P *y) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(ns.gs_blocks);
+  cfg.blockDim = dim3(32, 5, kGsZ);
+  cfg.dynamicSmemBytes = ns.gs_smem;
+  cfg.stream = x->stream;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeCooperative;
+  at[0].val.cooperative = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  if (ns.gs_dmax == 4) {
+    if (ns.gs_stage) CK(cudaLaunchKernelEx(&cfg, k_gs_persist<P, true, 4>, ns.gs_args, OB, MinvP, r, y));
+    else CK(cudaLaunchKernelEx(&cfg, k_gs_persist<P, false, 4>, ns.gs_args, OB, MinvP, r, y));
+  } else {
+    if (ns.gs_stage) CK(cudaLaunchKernelEx(&cfg, k_gs_persist<P, true, kGsMaxDeg>, ns.gs_args, OB, MinvP, r, y));
+    else CK(cudaLaunchKernelEx(&cfg, k_gs_persist<P, false, kGsMaxDeg>, ns.gs_args, OB, MinvP, r, y));
+  }
+}
+
+// FCFD_ERR_TIMEOUT if a grid barrier of the persistent Gauss-Seidel kernel ran
+// out of polls since the last check (the flag is cleared)
+static void check_gs_timeout(fcfd_ctx *x, NewtonState &ns) {
+  if (!ns.gs_persist) return;
+  unsigned h = 0;
+  CK(cudaMemcpyAsync(&h, ns.gs_bar.p + 1, sizeof(unsigned), cudaMemcpyDeviceToHost, x->stream));
+  CK(cudaStreamSynchronize(x->stream));
+  if (h) {
+    CK(cudaMemsetAsync(ns.gs_bar.p + 1, 0, sizeof(unsigned), x->stream));
+    throw Error(FCFD_ERR_TIMEOUT, "a grid barrier of the persistent Gauss-Seidel kernel timed out");
+  }
+}
 template <class T>
 __global__ void k_axpy_to(int n, const double *__restrict__ b, const T *__restrict__ w, T *__restrict__ out) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -768,6 +1061,10 @@ static void apply_prec(fcfd_ctx *x, NewtonState &ns, const T *v, T *z, int sweep
   // each turn is skipped.  FP64 or, with the FP32 preconditioner, FP32
   // couplings, vectors and arithmetic.
   auto sweep = [&](auto *OB, auto *MinvP, auto *r, auto *a) {
+    if (ns.gs_persist) {
+      launch_gs_persist(x, ns, OB, MinvP, r, a);
+      return;
+    }
     const std::vector<int> &ci = x->color_index;
     const int ncol = (int)ci.size() - 1, deg = x->gs_deg;
     int last = -1;
@@ -787,11 +1084,12 @@ static void apply_prec(fcfd_ctx *x, NewtonState &ns, const T *v, T *z, int sweep
   // the sweeps run in place on z itself when it has the preconditioner's type
   auto run = [&](auto *OB, auto *MinvP, auto *r, auto *y) {
     using P = std::remove_pointer_t<decltype(y)>;
+    unsigned *bar = ns.gs_persist ? ns.gs_bar.p : nullptr;
     if constexpr (std::is_same_v<P, T>) {
-      k_precond_split<T, P><<<gc, tb, 0, s>>>(nc, ns.Minv.p, v, rs, r, z);
+      k_precond_split<T, P><<<gc, tb, 0, s>>>(nc, ns.Minv.p, v, rs, r, z, bar);
       sweep(OB, MinvP, r, z);
     } else {
-      k_precond_split<T, P><<<gc, tb, 0, s>>>(nc, ns.Minv.p, v, rs, r, y);
+      k_precond_split<T, P><<<gc, tb, 0, s>>>(nc, ns.Minv.p, v, rs, r, y, bar);
       sweep(OB, MinvP, r, y);
       k_cast<T, P><<<(5 * nc + tb - 1) / tb, tb, 0, s>>>(5 * nc, y, z);
     }
@@ -901,7 +1199,7 @@ static void gmres(fcfd_ctx *x, NewtonState &ns, Krylov<T> &K, int mode, double r
 }
 
 // Buffers of the implicit solve; volumes uploaded.
-static void alloc_state(fcfd_ctx *x, NewtonState &ns, int sweeps, int cycles, bool prec32) {
+static void alloc_state(fcfd_ctx *x, NewtonState &ns, int sweeps, int cycles, bool prec32, int gs_launch = 0) {
   const DevMesh &m = x->dm;
   const int nc = m.nc, n = 5 * nc;
   cudaStream_t s = x->stream;
@@ -918,6 +1216,10 @@ static void alloc_state(fcfd_ctx *x, NewtonState &ns, int sweeps, int cycles, bo
     } else {
       ns.OB.alloc((size_t)nc * x->gs_deg * 25 + 1); ns.MinvP.alloc(25 * (size_t)nc);
     }
+  }
+  if (ns.sweeps > 0 && gs_launch == 1) {
+    if (ns.prec32) plan_gs_persist<float>(x, ns);
+    else plan_gs_persist<double>(x, ns);
   }
   CK(cudaMemsetAsync(ns.JR.p, 0, sizeof(double) * 25 * (size_t)m.nf, s));
   std::vector<double> vol(x->mesh->c_volume.begin(), x->mesh->c_volume.begin() + nc);
@@ -1029,6 +1331,7 @@ static LinearSolve implicit_solve(fcfd_ctx *x, NewtonState &ns, Krylov<double> &
   LinearSolve out;
   if (f32) gmres<float>(x, ns, K32, jmode, krtol, ns.R1.p, out.iters, out.relres, rs, abstol);
   else gmres<double>(x, ns, K64, jmode, krtol, ns.R1.p, out.iters, out.relres, rs, abstol);
+  check_gs_timeout(x, ns);
   return out;
 }
 
@@ -1148,7 +1451,7 @@ int fcfd_newton_solve(fcfd_ctx *x, double *W, const fcfd_newton_opts *o, fcfd_ne
     const int tb = 256, gc = (nc + tb - 1) / tb, gn = (n + tb - 1) / tb;
     std::memset(rep, 0, sizeof(*rep));
     NewtonState ns;
-    alloc_state(x, ns, o->precond_sweeps, o->krylov_cycles, o->fp32_krylov != 0);
+    alloc_state(x, ns, o->precond_sweeps, o->krylov_cycles, o->fp32_krylov != 0, o->gs_launch);
     CK(cudaMemcpyAsync(x->Win.p, W, sizeof(double) * n, cudaMemcpyHostToDevice, s));
     k_aos_to_soa_nc<<<gc, tb, 0, s>>>(x->Win.p, ns.Wn.p, nc);
     const int mdim = o->krylov_dim > 0 ? o->krylov_dim : 30;

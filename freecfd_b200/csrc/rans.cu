@@ -97,6 +97,22 @@ __global__ void k_rans_grad(DevMesh m, const S *__restrict__ K, S *__restrict__ 
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   const int nc = m.nc, nt = m.nt;
   if (c >= nc) return;
+  if (m.st_w) {
+    // stored map weights (curvilinear cases): grad += weight * phi in key order
+    S g[6] = {S(0.), S(0.), S(0.), S(0.), S(0.), S(0.)};
+    for (int j = m.st_index[c]; j < m.st_index[c + 1]; ++j) {
+      const int k = m.st_keys[j];
+      const double w0 = m.st_w[3 * (size_t)j], w1 = m.st_w[3 * (size_t)j + 1], w2 = m.st_w[3 * (size_t)j + 2];
+      for (int v = 0; v < 2; ++v) {
+        const S phi = K[v * nt + k];
+        g[3 * v] = g[3 * v] + w0 * phi;
+        g[3 * v + 1] = g[3 * v + 1] + w1 * phi;
+        g[3 * v + 2] = g[3 * v + 2] + w2 * phi;
+      }
+    }
+    for (int i = 0; i < 6; ++i) GK[i * nc + c] = g[i];
+    return;
+  }
   const double xc0 = m.c_x[c], xc1 = m.c_x[nt + c], xc2 = m.c_x[2 * nt + c];
   const S u0[2] = {K[c], K[nt + c]};
   S acc[6] = {S(0.), S(0.), S(0.), S(0.), S(0.), S(0.)};

@@ -107,6 +107,21 @@ class Mesh:
         check(lib.fcfd_mesh_lsq(self.h, _d(cof), _d(selfw)))
         return cof, selfw
 
+    def grad_weights(self):
+        """Stored gradient-map weights [E][3] in stencil-key order (meshes
+        with curvilinear cells)."""
+        w = np.empty((self.n_grad_entries, 3))
+        check(lib.fcfd_mesh_grad_weights(self.h, _d(w)))
+        return w
+
+    def rcm_order(self):
+        """Reverse Cuthill-McKee order of the interior cells (perm[new] =
+        old) over the face-neighbour graph; `cases.renumber_cells` lists a
+        grid's elements in this order."""
+        perm = np.empty(self.nc, np.int32)
+        check(lib.fcfd_mesh_rcm(self.h, _i(perm)))
+        return perm
+
     def __del__(self):
         if getattr(self, "h", None):
             lib.fcfd_mesh_destroy(self.h)
@@ -137,6 +152,31 @@ class NavierStokes:
             raise ValueError("W and R must both be host arrays or both be device tensors")
         check(lib.fcfd_residual(self.h, pw, pr, fw))
         return out
+
+    def residual_mixed(self, W, shock_ratio: float = 2.0, out=None):
+        """R(W) with the face pass in FP32 except faces whose cell-centre
+        absolute pressures differ by more than the factor shock_ratio (FP64);
+        ghosts, gradients, limiters and the gather in FP64.  Returns (R,
+        number of FP64 faces)."""
+        nc = self.mesh.nc
+        if out is None:
+            out = np.empty((nc, 5)) if isinstance(W, np.ndarray) else W.new_empty((nc, 5))
+        if isinstance(W, np.ndarray):
+            W = np.ascontiguousarray(W, dtype=np.float64)
+        pw, fw = _ptr(W)
+        pr, fr = _ptr(out)
+        if fw != fr:
+            raise ValueError("W and R must both be host arrays or both be device tensors")
+        n64 = ctypes.c_int64(0)
+        check(lib.fcfd_residual_mixed(self.h, pw, pr, float(shock_ratio), fw, ctypes.byref(n64)))
+        return out, int(n64.value)
+
+    def time_residual_mixed(self, reps: int = 20, flush_l2: bool = True, shock_ratio: float = 2.0):
+        """Mean device ms of the mixed-precision chain on the state of the
+        last residual call, and its number of FP64 faces."""
+        out = np.zeros(2)
+        check(lib.fcfd_time_residual_mixed(self.h, int(reps), int(bool(flush_l2)), float(shock_ratio), _d(out)))
+        return float(out[0]), int(out[1])
 
     def set_partition(self, lo: int, hi: int):
         """Evaluate only the part of the residual that owned cells [lo, hi)
@@ -268,17 +308,20 @@ class NavierStokes:
     def newton_solve(self, W, tol=1e-10, max_newton=200, krylov_dim=30, krylov_rtol=1e-2, cfl0=1.0,
                      cfl_growth=1.2, cfl_max=1e6, cfl_mode=1, ser_exponent=1.0, jvp=True, fp32_krylov=False,
                      max_seconds=0.0, raise_on_fail=True, precond_sweeps=0, krylov_cycles=1, exact_jvp=False,
-                     fp32_jvp=False, stop_all_rows=False, fp32_frozen_limiter=False):
+                     fp32_jvp=False, stop_all_rows=False, fp32_frozen_limiter=False, gs_persistent=False):
         """Steady solve R(W) = 0 (pseudo-transient Newton-Krylov on the device).
         stop_all_rows: also wait for the momentum and energy residuals to drop
         by tol.  fp32_frozen_limiter: with fp32_jvp, hold the limiter fixed in
-        the FP32 tangent (jvp_mode 4).  Returns (W_converged, report dict)."""
+        the FP32 tangent (jvp_mode 4).  gs_persistent: run all Gauss-Seidel
+        colour updates of a preconditioner application in one cooperative
+        launch with grid barriers instead of one launch per colour update.
+        Returns (W_converged, report dict)."""
         W = np.array(W, dtype=np.float64, order="C", copy=True)
         o = NewtonOpts(int(max_newton), float(tol), int(krylov_dim), float(krylov_rtol), float(cfl0), float(cfl_growth),
                        float(cfl_max), int(cfl_mode), float(ser_exponent),
                        ((4 if fp32_frozen_limiter else 3) if fp32_jvp else (2 if exact_jvp else 1)) if jvp else 0,
                        int(bool(fp32_krylov)), float(max_seconds), int(precond_sweeps), int(krylov_cycles),
-                       int(bool(stop_all_rows)))
+                       int(bool(stop_all_rows)), int(bool(gs_persistent)))
         r = NewtonReport()
         rc = lib.fcfd_newton_solve(self.h, _d(W), ctypes.byref(o), ctypes.byref(r))
         rep = dict(status=r.status, newton_iterations=r.newton_iterations, krylov_iterations=r.krylov_iterations,

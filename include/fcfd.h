@@ -111,6 +111,25 @@ int fcfd_mesh_geometry(const fcfd_mesh *m, double *face_normal, double *face_are
  * (lsqr_grad_map, src/lsqr_grad_map.cc:74-96). */
 int fcfd_mesh_lsq(const fcfd_mesh *m, double *cofactors, double *self_weight);
 
+/* Stored gradient-map weights, weights[E][3] in the order of the stencil
+ * keys of fcfd_mesh_connectivity (grad_index / grad_keys): built when some
+ * cell takes the curvilinear map (curvilinear_grad_map.cc:28-228, the
+ * reference's default for hexahedra and prisms, read_inputs.cc:47-48); the
+ * least-squares cells of such a mesh store lsqr_grad_map's weights
+ * (lsqr_grad_map.cc:86-96).  FCFD_ERR_UNSUPPORTED for a mesh without
+ * curvilinear cells (its least-squares weights are rebuilt on the device). */
+int fcfd_mesh_grad_weights(const fcfd_mesh *m, double *weights);
+
+/* Reverse Cuthill-McKee order of the interior cells over the face-neighbour
+ * graph: perm[new] = old, nc entries.  The reference takes its cell order
+ * from the grid file's element order, or from ParMETIS when partitioned
+ * (grid_partition.cc:25-141); it has no renumbering for locality.  A caller
+ * with an unordered grid (a face-based Tecplot file, a shuffled export)
+ * lists the elements in this order and builds the mesh again: every face's
+ * gathers then touch nearby cells.  Deterministic (ties to the lower index).
+ * Host only. */
+int fcfd_mesh_rcm(const fcfd_mesh *m, int32_t *perm);
+
 /* Create a device context on CUDA device `device`. */
 int fcfd_ctx_create(const fcfd_mesh *m, const fcfd_case *cs, int device, fcfd_ctx **out);
 void fcfd_ctx_destroy(fcfd_ctx *ctx);
@@ -245,6 +264,10 @@ typedef struct fcfd_newton_opts {
   int32_t krylov_cycles;  /* GMRES(m) restarts per Newton step (default 1) */
   int32_t stop_all_rows;  /* 1: stop only when the momentum (x,y,z together) and energy residual
                              norms have also dropped by tol from their initial values */
+  int32_t gs_launch;      /* Gauss-Seidel sweeps: 0 one launch per colour update (default); 1 all colour
+                             updates of a preconditioner application in one cooperative launch with
+                             grid barriers between them (couplings staged in shared memory where they
+                             fit; a barrier that waits too long ends the solve with FCFD_ERR_TIMEOUT) */
 } fcfd_newton_opts;
 
 typedef struct fcfd_newton_report {
@@ -256,6 +279,26 @@ typedef struct fcfd_newton_report {
   double seconds_history[512]; /* wall time at each history[] entry */
   double kw_final[2];     /* fcfd_rans_newton_solve: final / initial norm of the k and omega residuals */
 } fcfd_newton_report;
+
+/* Mixed-precision residual: fcfd_residual's R(W) with the face pass in FP32
+ * where the flow is smooth and in FP64 at shocks.  Ghost states, gradients,
+ * limiters and the gather stay FP64 (the reference's minmod / Barth-Jespersen
+ * decisions on one-layer meshes follow the sign of the FP64 gradient's
+ * rounding noise); a face whose two cell-centre absolute pressures differ by
+ * more than the factor shock_ratio runs in FP64, so the equation of state
+ * (material.cc:108-153) and the flux's pressure terms across a captured
+ * shock keep FP64; every other face evaluates reconstruction, equation of
+ * state, convective and viscous flux in FP32 and its face difference is
+ * summed in FP64.  shock_ratio < 1 sends every face to the FP64 pass.
+ * *n_fp64_faces (may be null) receives the number of FP64 faces.  No
+ * counterpart in the reference (its residual is FP64 throughout). */
+int fcfd_residual_mixed(fcfd_ctx *ctx, const double *W, double *R, double shock_ratio, int32_t flags,
+                        int64_t *n_fp64_faces);
+
+/* Device time of the mixed-precision chain on the state of the last residual
+ * call: out[0] = mean ms per evaluation over reps (L2 flushed before each
+ * when flush_l2), out[1] = FP64 faces of the last evaluation. */
+int fcfd_time_residual_mixed(fcfd_ctx *ctx, int32_t reps, int32_t flush_l2, double shock_ratio, double *out);
 
 /* Steady solve R(W) = 0 by pseudo-transient matrix-free Newton-Krylov on the
  * device: (V P/dt - dR/dW) dW = R(W), W += dW, with P = cons2prim

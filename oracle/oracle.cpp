@@ -995,12 +995,133 @@ static void lsqr_grad_map(Grid &g, int ci) {
   }
 }
 
+// curvilinear_grad_map.cc:28-228.  The hexahedron branch (lines 58-77)
+// erases the std::set element its loop iterator points at and then
+// increments that iterator (undefined behaviour); restated here is the
+// pairing the loop is written to produce: the faces still unpaired, in
+// ascending order, each paired with the later unpaired face whose outward
+// normal is most opposite (first minimum).
+static void curvilinear_grad_map(Grid &g, int c) {
+  std::set<int> stencil;
+  std::vector<int> face_pairs(6, -1), cell_pairs(6, -1), cell_pairs_temp(6, -1);
+  std::vector<Vec3> Jac(3), Jac_temp(3), Jac_invT(3);
+  double det;
+  int cell_plus, cell_minus;
+  for (int cf = 0; cf < (int)g.cell[c].faces.size(); ++cf) stencil.insert(cf);
+  if (g.cell[c].nodes.size() == 8) {
+    int counter = 0;
+    while (!stencil.empty()) {
+      std::set<int>::iterator sit1 = stencil.begin(), sit2;
+      double min_product = 1.e20;
+      Vec3 my_normal = g.cellFace(c, *sit1).normal;
+      if (g.cellFace(c, *sit1).parent != c) my_normal *= -1.;
+      face_pairs[2 * counter + 1] = *sit1;
+      sit2 = sit1;
+      sit2++;
+      for (; sit2 != stencil.end(); sit2++) {
+        Vec3 other_normal = g.cellFace(c, *sit2).normal;
+        if (g.cellFace(c, *sit2).parent != c) other_normal *= -1.;
+        double product = my_normal.dot(other_normal);
+        if (product < min_product) {
+          min_product = product;
+          face_pairs[2 * counter] = *sit2;
+        }
+      }
+      stencil.erase(face_pairs[2 * counter]);
+      stencil.erase(face_pairs[2 * counter + 1]);
+      counter++;
+      if (counter == 3) break;
+    }
+    for (int i = 0; i < 3; ++i) {
+      cell_plus = g.cellFace(c, face_pairs[2 * i + 1]).neighbor;
+      if (cell_plus == c) cell_plus = g.cellFace(c, face_pairs[2 * i + 1]).parent;
+      cell_pairs[2 * i + 1] = cell_plus;
+      Jac[i] = g.cell[cell_plus].centroid;
+      cell_minus = g.cellFace(c, face_pairs[2 * i]).neighbor;
+      if (cell_minus == c) cell_minus = g.cellFace(c, face_pairs[2 * i]).parent;
+      cell_pairs[2 * i] = cell_minus;
+      Jac[i] -= g.cell[cell_minus].centroid;
+    }
+  } else {
+    double max_det = 0.;
+    stencil.clear();
+    for (int cf = 0; cf < (int)g.cell[c].faces.size(); ++cf) stencil.insert(g.cell[c].faces[cf]);
+    std::set<int>::iterator sit1, sit2, sit3, sit4, sit5, sit6;
+    for (sit1 = stencil.begin(); sit1 != stencil.end(); sit1++) {
+      for (sit2 = sit1; sit2 != stencil.end(); sit2++) {
+        cell_plus = g.face[*sit2].neighbor;
+        if (cell_plus == c) cell_plus = g.face[*sit2].parent;
+        cell_pairs_temp[1] = cell_plus;
+        Jac_temp[0] = g.cell[cell_plus].centroid;
+        cell_minus = g.face[*sit1].neighbor;
+        if (cell_minus == c) cell_minus = g.face[*sit1].parent;
+        cell_pairs_temp[0] = cell_minus;
+        Jac_temp[0] -= g.cell[cell_minus].centroid;
+        for (sit3 = sit1; sit3 != stencil.end(); sit3++) {
+          for (sit4 = sit3; sit4 != stencil.end(); sit4++) {
+            cell_plus = g.face[*sit4].neighbor;
+            if (cell_plus == c) cell_plus = g.face[*sit4].parent;
+            cell_pairs_temp[3] = cell_plus;
+            Jac_temp[1] = g.cell[cell_plus].centroid;
+            cell_minus = g.face[*sit3].neighbor;
+            if (cell_minus == c) cell_minus = g.face[*sit3].parent;
+            cell_pairs_temp[2] = cell_minus;
+            Jac_temp[1] -= g.cell[cell_minus].centroid;
+            for (sit5 = sit2; sit5 != stencil.end(); sit5++) {
+              for (sit6 = sit5; sit6 != stencil.end(); sit6++) {
+                cell_plus = g.face[*sit6].neighbor;
+                if (cell_plus == c) cell_plus = g.face[*sit6].parent;
+                cell_pairs_temp[5] = cell_plus;
+                Jac_temp[2] = g.cell[cell_plus].centroid;
+                cell_minus = g.face[*sit5].neighbor;
+                if (cell_minus == c) cell_minus = g.face[*sit5].parent;
+                cell_pairs_temp[4] = cell_minus;
+                Jac_temp[2] -= g.cell[cell_minus].centroid;
+                det = Jac_temp[0].dot(Jac_temp[1].cross(Jac_temp[2]));
+                if (det > max_det) {
+                  max_det = det;
+                  cell_pairs = cell_pairs_temp;
+                  Jac = Jac_temp;
+                }
+              }
+            }
+          }
+        }
+      }
+    }
+    if (!(max_det > 0.)) throw DeckError("curvilinear gradient: no face pairs with a positive determinant");
+  }
+  det = Jac[0].dot(Jac[1].cross(Jac[2]));
+  Jac_invT[0][0] = (Jac[1][1] * Jac[2][2] - Jac[1][2] * Jac[2][1]) / det;
+  Jac_invT[1][0] = (Jac[0][2] * Jac[2][1] - Jac[0][1] * Jac[2][2]) / det;
+  Jac_invT[2][0] = (Jac[0][1] * Jac[1][2] - Jac[0][2] * Jac[1][1]) / det;
+  Jac_invT[0][1] = (Jac[1][2] * Jac[2][0] - Jac[1][0] * Jac[2][2]) / det;
+  Jac_invT[1][1] = (Jac[0][0] * Jac[2][2] - Jac[0][2] * Jac[2][0]) / det;
+  Jac_invT[2][1] = (Jac[0][2] * Jac[1][0] - Jac[0][0] * Jac[1][2]) / det;
+  Jac_invT[0][2] = (Jac[1][0] * Jac[2][1] - Jac[1][1] * Jac[2][0]) / det;
+  Jac_invT[1][2] = (Jac[0][1] * Jac[2][0] - Jac[0][0] * Jac[2][1]) / det;
+  Jac_invT[2][2] = (Jac[0][0] * Jac[1][1] - Jac[0][1] * Jac[1][0]) / det;
+  std::map<int, Vec3> gradMap;
+  gradMap.insert(std::pair<int, Vec3>(cell_pairs[0], -1. * Jac_invT[0]));
+  if (gradMap.find(cell_pairs[1]) == gradMap.end()) gradMap.insert(std::pair<int, Vec3>(cell_pairs[1], Jac_invT[0]));
+  else gradMap[cell_pairs[1]] += Jac_invT[0];
+  if (gradMap.find(cell_pairs[2]) == gradMap.end()) gradMap.insert(std::pair<int, Vec3>(cell_pairs[2], -1. * Jac_invT[1]));
+  else gradMap[cell_pairs[2]] -= Jac_invT[1];
+  if (gradMap.find(cell_pairs[3]) == gradMap.end()) gradMap.insert(std::pair<int, Vec3>(cell_pairs[3], Jac_invT[1]));
+  else gradMap[cell_pairs[3]] += Jac_invT[1];
+  if (gradMap.find(cell_pairs[4]) == gradMap.end()) gradMap.insert(std::pair<int, Vec3>(cell_pairs[4], -1. * Jac_invT[2]));
+  else gradMap[cell_pairs[4]] -= Jac_invT[2];
+  if (gradMap.find(cell_pairs[5]) == gradMap.end()) gradMap.insert(std::pair<int, Vec3>(cell_pairs[5], Jac_invT[2]));
+  else gradMap[cell_pairs[5]] += Jac_invT[2];
+  g.cell[c].gradMap = gradMap;
+}
+
 // gradient_maps.cc:39-78
 static void gradient_maps(Oracle &O) {
   Grid &g = O.grid;
   for (int c = 0; c < g.cellCount; ++c) {
     int m = (g.cell[c].nodes.size() == 8) ? O.hex_method : (g.cell[c].nodes.size() == 6 ? O.prism_method : O.other_method);
-    if (m == CURVILINEAR) throw DeckError("curvilinear gradients are not restated; set hex/prism method=lsqr");
+    if (m == CURVILINEAR) curvilinear_grad_map(g, c);
     if (m == LSQR) lsqr_grad_map(g, c);
   }
 }

@@ -8,7 +8,7 @@ the residual is smooth along the direction (no limiter switch inside +-h)."""
 import numpy as np
 import pytest
 
-from tests.util import ELEMENTS, SMALL, build_pair, rel_err
+from tests.util import ELEMENTS, SMALL, build_pair, rel_err, res_err
 
 
 def _dirs(shape, seed, n):
@@ -33,7 +33,11 @@ def test_jvp_matches_complex_step(family, flux, limiter, oracle_mod, fb):
         V = V * scale
         R, jv = ns.jvp(case.state, V, with_residual=True)
         cs_ref = o.residual_cstep(case.state, V)
-        assert rel_err(R, ns.residual(case.state)).max() <= 1e-13
+        # the residual riding on the tangent chain against the plain residual
+        # chain (on small meshes a two-warp gradient kernel with a different
+        # summation order): momentum components share one scale, since the
+        # z-momentum of the one-layer meshes is rounding noise
+        assert res_err(R, ns.residual(case.state)).max() <= 1e-13
         cols = [k for k in range(5) if np.abs(cs_ref[:, k]).max() > 1e-12 * np.abs(cs_ref).max()]
         err = rel_err(jv[:, cols], cs_ref[:, cols])
         assert err.max() <= 1e-10, err
