@@ -654,6 +654,24 @@ def profile_newton(args):
     print(json.dumps({"workload": case.workload, "newton": run_newton(fb, cs, mesh, case, 0, None, False)}), flush=True)
 
 
+def profile_mixed(args):
+    """Only residual evaluations of the hypersonic workload with a bow-shock
+    jump: each repeat one FP64 residual, then one mixed-precision residual
+    (a short run for kernel profiles); prints the FP64 face count."""
+    import tempfile
+    import freecfd_b200 as fb
+    case = make_case("hypersonic")
+    cs = fb.Case(case.write_deck(tempfile.mkdtemp(prefix="fcfd_bench_")))
+    mesh = fb.Mesh(case.mesh, cs)
+    ns = fb.NavierStokes(mesh, cs, 0)
+    W = np.ascontiguousarray(load_cases().hypersonic_shock_state(case, mesh.geometry()["cell_centroid"]))
+    n = 0
+    for _ in range(int(args.profile_mixed)):
+        ns.residual(W)
+        _, n = ns.residual_mixed(W, 2.0)
+    print(json.dumps({"workload": case.workload, "state": "bow_shock_jump", "fp64_faces": n}), flush=True)
+
+
 def run_newton(fb, cs, mesh, case, dev, dist, reference_state=True):
     """Steady solve from the seeded state until |R_mass|/|R_mass0| <= 1e-10:
     plain FP64 (finite-difference J.v, FP64 Krylov) against mixed (tangent
@@ -817,9 +835,13 @@ def main():
                     help="also time the domain-decomposed residual (always on under torchrun)")
     ap.add_argument("--profile-newton", type=int, default=0,
                     help="run only the two Newton arms, capped at this many Newton steps")
+    ap.add_argument("--profile-mixed", type=int, default=0,
+                    help="run only this many FP64 + mixed-precision residual pairs of the hypersonic workload")
     args = ap.parse_args()
     if args.profile_newton > 0:
         profile_newton(args)
+    elif args.profile_mixed > 0:
+        profile_mixed(args)
     elif args.impl == "reference":
         run_reference(args)
     else:

@@ -132,6 +132,9 @@ struct fcfd_ctx {
   DBuf<int> face_order;  // faces grouped by kind (DevMesh::face_list of the whole mesh)
   // mixed-precision residual: faces sent to the FP64 pass, and their count
   DBuf<int> mx_list, mx_count;
+  // tiles of the shared-memory gradient kernel (DevMesh::tile_off ...)
+  DBuf<int> tile_off, tile_cells, st_local, cf_local, self_local;
+  int grad_kernel = 0;  // fcfd_ctx_set_gradient_kernel: 0 automatic, 1 per cell, 2 tiles
 };
 
 
@@ -150,6 +153,15 @@ inline void launch_grad_limiter(const DevCase &cs, const DevMesh &m, const S *W,
                                 const int *argx, S *G, S *Lm, cudaStream_t s) {
   const int g = ((PART ? m.n_part_cells : m.nc) + 127) / 128;
   if (g == 0) return;
+  if constexpr (std::is_same<S, double>::value && !PART) {
+    if (cs.tile_grad && m.tile_off) {
+      const int nt_ = (m.nc + kGradTile - 1) / kGradTile;
+      const size_t smem = sizeof(double) * 8 * (size_t)m.tile_slots_max;
+      if (cs.fast_grad) k_grad_limiter_tile<true><<<nt_, kGradTile, smem, s>>>(cs, m, W, ext, G, Lm);
+      else k_grad_limiter_tile<false><<<nt_, kGradTile, smem, s>>>(cs, m, W, ext, G, Lm);
+      return;
+    }
+  }
   if constexpr (std::is_same<S, double>::value) {
     // meshes too small to fill the GPU with one thread per cell (fewer than
     // 148 SMs x 512 cells) take two threads per cell

@@ -296,6 +296,52 @@ int fcfd_ctx_create(const fcfd_mesh *mp, const fcfd_case *csp, int device, fcfd_
       if (m.st_index[cc] == m.st_index[cc + 1]) { x->green_gauss = true; break; }
   }
   d.pair_grad = (x->green_gauss || m.grad_weights) ? 0 : 1;
+  if (!x->green_gauss && !m.grad_weights) {
+    // tiles of kGradTile consecutive cells for the shared-memory gradient
+    // kernel: each tile's staged set (the cells its stencils and faces name,
+    // ascending) and every stencil / face entry as a slot in it
+    const int T = kGradTile, ntile = (nc + T - 1) / T;
+    std::vector<int32_t> toff(ntile + 1, 0), tcells, stl(m.st_keys.size()), cfl_loc(m.cf_list.size()), selfl(nc);
+    std::vector<int32_t> set;
+    int smax = 0;
+    for (int t = 0; t < ntile; ++t) {
+      const int c0 = t * T, c1 = std::min(nc, c0 + T);
+      set.clear();
+      for (int c = c0; c < c1; ++c) {
+        for (int j = m.st_index[c]; j < m.st_index[c + 1]; ++j) set.push_back(m.st_keys[j]);
+        for (int j = m.cf_index[c]; j < m.cf_index[c + 1]; ++j) {
+          const int f = m.cf_list[j];
+          set.push_back(m.f_parent[f] == c ? m.f_neighbor[f] : m.f_parent[f]);
+        }
+        set.push_back(c);
+      }
+      std::sort(set.begin(), set.end());
+      set.erase(std::unique(set.begin(), set.end()), set.end());
+      auto slot = [&](int k) { return (int32_t)(std::lower_bound(set.begin(), set.end(), k) - set.begin()); };
+      for (int c = c0; c < c1; ++c) {
+        selfl[c] = slot(c);
+        for (int j = m.st_index[c]; j < m.st_index[c + 1]; ++j) stl[j] = slot(m.st_keys[j]);
+        for (int j = m.cf_index[c]; j < m.cf_index[c + 1]; ++j) {
+          const int f = m.cf_list[j];
+          cfl_loc[j] = slot(m.f_parent[f] == c ? m.f_neighbor[f] : m.f_parent[f]);
+        }
+      }
+      tcells.insert(tcells.end(), set.begin(), set.end());
+      toff[t + 1] = (int32_t)tcells.size();
+      smax = std::max(smax, (int)set.size());
+    }
+    int optin = 0;
+    CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
+    const size_t smem = sizeof(double) * 8 * (size_t)smax;
+    if (smem <= (size_t)optin) {
+      x->tile_off.upload(toff); x->tile_cells.upload(tcells); x->st_local.upload(stl);
+      x->cf_local.upload(cfl_loc); x->self_local.upload(selfl);
+      x->dm.tile_slots_max = smax;
+      CK(cudaFuncSetAttribute(k_grad_limiter_tile<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      CK(cudaFuncSetAttribute(k_grad_limiter_tile<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    }
+  }
+  d.tile_grad = 0;
   std::vector<int32_t> bface(nb), outl;
   for (int f = 0; f < nf; ++f) {
     if (m.f_bc[f] >= 0) {
@@ -382,6 +428,8 @@ int fcfd_ctx_create(const fcfd_mesh *mp, const fcfd_case *csp, int device, fcfd_
   dm.st_keys = x->st_keys.p; dm.st_cof = x->st_cof.p; dm.st_self = x->st_self.p; dm.bface = x->bface.p;
   dm.st_recip = x->st_recip.p; dm.st_mirror = x->st_mirror.p; dm.c_vol = x->c_vol.p;
   dm.st_w = x->st_w.p;
+  dm.tile_off = x->tile_off.p; dm.tile_cells = x->tile_cells.p; dm.st_local = x->st_local.p;
+  dm.cf_local = x->cf_local.p; dm.self_local = x->self_local.p;
   dm.f_wall = x->f_wall.p; dm.f_diss = x->f_diss.p;
   dm.outlet_faces = x->outlet.p; dm.n_outlet = x->n_outlet;
   dm.face_list = x->face_order.p; dm.n_face_list = nf;
@@ -626,6 +674,19 @@ int fcfd_time_residual(fcfd_ctx *x, int reps, int flush_l2, double *out, int out
     for (int k = 0; k < 5; ++k) { CK(cudaEventElapsedTime(&ms, t.ev[k], t.ev[k + 1])); acc[k + 1] += ms; }
   }
   for (int k = 0; k < 6 && k < out_len; ++k) out[k] = acc[k] / reps;
+  API_END
+}
+
+int fcfd_ctx_set_gradient_kernel(fcfd_ctx *x, int kind) {
+  API_BEGIN
+  if (!x) throw Error(FCFD_ERR_INPUT, "null context");
+  if (kind < 0 || kind > 2) throw Error(FCFD_ERR_INPUT, "gradient kernel kind must be 0, 1 or 2");
+  if (kind == 2 && !x->dm.tile_off) throw Error(FCFD_ERR_UNSUPPORTED, "no gradient tiles for this mesh (Green-Gauss or curvilinear cells, or a tile's cells exceed shared memory)");
+  x->grad_kernel = kind;
+  x->cs.tile_grad = (kind == 2) ? 1 : 0;
+  // the captured chains hold the previous gradient kernel
+  if (x->graph) { CK(cudaGraphExecDestroy(x->graph)); x->graph = nullptr; }
+  if (x->host_graph) { CK(cudaGraphExecDestroy(x->host_graph)); x->host_graph = nullptr; }
   API_END
 }
 

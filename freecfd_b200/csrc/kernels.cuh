@@ -206,6 +206,7 @@ struct DevCase {
   int sutherland, prandtl, flux, limiter, order, viscous, nbc, frozen_limiter;
   int fast_grad;
   int pair_grad;  // every cell has a gradient stencil: the two-threads-per-cell gradient may run
+  int tile_grad;  // the shared-memory tile gradient kernel runs (DevMesh tiles built)
   DevBC bc[kMaxBC];
 };
 
@@ -223,6 +224,13 @@ struct DevMesh {
   const double *c_vol;                     // [nc] cell volumes (Green-Gauss gradients)
   const double *st_mirror;                 // [3][nc] summed symmetry-mirror weights
   const double *st_w = nullptr;            // [E][3] stored map weights (curvilinear cases), else null
+  // tiles of the shared-memory gradient kernel (null: not built): the staged
+  // cells of tile t are tile_cells[tile_off[t], tile_off[t+1]); st_local and
+  // cf_local give a stencil entry's / face entry's cell as a slot in its
+  // cell's tile, self_local the cell's own slot
+  const int *tile_off = nullptr, *tile_cells = nullptr, *st_local = nullptr, *cf_local = nullptr,
+            *self_local = nullptr;
+  int tile_slots_max = 0;
   const int *bface;                        // boundary faces in ghost order [nb]
   const int *outlet_faces;                 // outlet boundary faces [n_outlet]
   const double *f_wall, *f_diss;           // [nf] wall distance, dissipation factor (Steger-Warming only)
@@ -617,25 +625,47 @@ __global__ void k_split_dual(const Dual<T> *__restrict__ R, double *__restrict__
   }
 }
 
-// LSQ gradient (bit-exact restatement of Variable::cell_gradient over the
-// lsqr_grad_map weights) + limiter, one thread per interior cell.
-// The FP64 bit-exact instantiation runs at six blocks per SM (register cap),
-// measured 8 % faster on the prism mesh; the others keep their registers.
-template <class S, bool FAST, bool PART = false>
-__global__ void __launch_bounds__(128, (!FAST && std::is_same<S, double>::value) ? 6 : 1) k_grad_limiter(DevCase cs, DevMesh m, const S *__restrict__ W,
-                                                      const unsigned long long *__restrict__ ext, const int *__restrict__ argx,
-                                                      S *__restrict__ G, S *__restrict__ Lm) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int nc = m.nc, nt = m.nt;
-  // PART: one rank's gradient cells of a domain decomposition
-  int c = i;
-  if constexpr (PART) {
-    if (i >= m.n_part_cells) return;
-    c = m.part_cells[i];
-  } else {
-    if (i >= nc) return;
+// Cell data of the gradient + limiter body: states W and centroids c_x of
+// the cells a stencil entry or a face neighbour names, from global memory
+// (cell ids), or from a tile staged in shared memory (slots).
+template <class S>
+struct CellsGlobal {
+  const S *W;
+  const double *cx;
+  int nt;
+  __device__ __forceinline__ S w(int v, int k) const { return W[v * nt + k]; }
+  __device__ __forceinline__ double x(int i, int k) const { return cx[i * nt + k]; }
+  // stencil entry j's cell, the cell itself, the other cell of face entry j
+  __device__ __forceinline__ int key(const DevMesh &m, int j) const { return m.st_keys[j]; }
+  __device__ __forceinline__ int self(int c) const { return c; }
+  __device__ __forceinline__ int nbr(const DevMesh &m, int j, int e) const {
+    const int f = e >= 0 ? e : ~e;
+    return e >= 0 ? m.f_neighbor[f] : m.f_parent[f];
   }
-  const double xc0 = m.c_x[c], xc1 = m.c_x[nt + c], xc2 = m.c_x[2 * nt + c];
+};
+struct CellsTile {
+  const double *sW, *sX;  // [5][ns], [3][ns] in shared memory
+  int ns, self_slot;
+  const int *st_local, *cf_local;
+  __device__ __forceinline__ double w(int v, int s) const { return sW[v * ns + s]; }
+  __device__ __forceinline__ double x(int i, int s) const { return sX[i * ns + s]; }
+  __device__ __forceinline__ int key(const DevMesh &, int j) const { return st_local[j]; }
+  __device__ __forceinline__ int self(int) const { return self_slot; }
+  __device__ __forceinline__ int nbr(const DevMesh &, int j, int) const { return cf_local[j]; }
+};
+
+// LSQ gradient (bit-exact restatement of Variable::cell_gradient over the
+// lsqr_grad_map weights) + limiter of interior cell c, reading the cells it
+// needs through the accessor A (W itself is read directly only for the VK
+// extrema quirks: cells 0 and nc-1).
+template <class S, bool FAST, class A>
+__device__ __forceinline__ void grad_limiter_cell(const DevCase &cs, const DevMesh &m, const S *__restrict__ W,
+                                                  const unsigned long long *__restrict__ ext,
+                                                  const int *__restrict__ argx, int c, const A &cells,
+                                                  S *__restrict__ G, S *__restrict__ Lm) {
+  const int nc = m.nc, nt = m.nt;
+  const int cself = cells.self(c);
+  const double xc0 = cells.x(0, cself), xc1 = cells.x(1, cself), xc2 = cells.x(2, cself);
   S g[15];
 #pragma unroll
   for (int i = 0; i < 15; ++i) g[i] = S(0.);
@@ -649,19 +679,19 @@ __global__ void __launch_bounds__(128, (!FAST && std::is_same<S, double>::value)
     // with fused multiply-adds (equal to the reference's sum up to rounding).
     S u0[5];
 #pragma unroll
-    for (int v = 0; v < 5; ++v) u0[v] = W[v * nt + c];
+    for (int v = 0; v < 5; ++v) u0[v] = cells.w(v, cself);
     S acc[15];
 #pragma unroll
     for (int i = 0; i < 15; ++i) acc[i] = S(0.);
 #pragma unroll 4
     for (int j = j0; j < j1; ++j) {
-      const int k = m.st_keys[j];
-      if (k == c) continue;
-      const double d0 = m.c_x[k] - xc0, d1 = m.c_x[nt + k] - xc1, d2 = m.c_x[2 * nt + k] - xc2;
+      const int k = cells.key(m, j);
+      if (k == cself) continue;
+      const double d0 = cells.x(0, k) - xc0, d1 = cells.x(1, k) - xc1, d2 = cells.x(2, k) - xc2;
       const double w = d0 * d0 + d1 * d1 + d2 * d2;
 #pragma unroll
       for (int v = 0; v < 5; ++v) {
-        const S a = w * (W[v * nt + k] - u0[v]);
+        const S a = w * (cells.w(v, k) - u0[v]);
         acc[3 * v] = acc[3 * v] + a * d0;
         acc[3 * v + 1] = acc[3 * v + 1] + a * d1;
         acc[3 * v + 2] = acc[3 * v + 2] + a * d2;
@@ -688,11 +718,11 @@ __global__ void __launch_bounds__(128, (!FAST && std::is_same<S, double>::value)
       // stored map weights (curvilinear maps, and the least-squares maps of a
       // mesh that has any): grad += weight * phi in key order
       for (int j = j0; j < j1; ++j) {
-        const int k = m.st_keys[j];
+        const int k = cells.key(m, j);
         const double wt0 = m.st_w[3 * (size_t)j], wt1 = m.st_w[3 * (size_t)j + 1], wt2 = m.st_w[3 * (size_t)j + 2];
 #pragma unroll
         for (int v = 0; v < 5; ++v) {
-          const S phi = W[v * nt + k];
+          const S phi = cells.w(v, k);
           g[3 * v] = add_rn(g[3 * v], mul_rn(S(wt0), phi));
           g[3 * v + 1] = add_rn(g[3 * v + 1], mul_rn(S(wt1), phi));
           g[3 * v + 2] = add_rn(g[3 * v + 2], mul_rn(S(wt2), phi));
@@ -712,12 +742,12 @@ __global__ void __launch_bounds__(128, (!FAST && std::is_same<S, double>::value)
       return __ddiv_rn(x, det);
     };
     for (int j = m.st_w ? j1 : j0; j < j1; ++j) {
-      const int k = m.st_keys[j];
+      const int k = cells.key(m, j);
       double wt0, wt1, wt2;
-      if (k == c) {
+      if (k == cself) {
         wt0 = m.st_self[c]; wt1 = m.st_self[nc + c]; wt2 = m.st_self[2 * nc + c];
       } else {
-        const double d0 = sub_rn(m.c_x[k], xc0), d1 = sub_rn(m.c_x[nt + k], xc1), d2 = sub_rn(m.c_x[2 * nt + k], xc2);
+        const double d0 = sub_rn(cells.x(0, k), xc0), d1 = sub_rn(cells.x(1, k), xc1), d2 = sub_rn(cells.x(2, k), xc2);
         const double w = add_rn(add_rn(mul_rn(d0, d0), mul_rn(d1, d1)), mul_rn(d2, d2));
         wt0 = qdiv(mul_rn(w, add_rn(add_rn(mul_rn(d0, C00), mul_rn(d1, C01)), mul_rn(d2, C02))));
         wt1 = qdiv(mul_rn(w, add_rn(add_rn(mul_rn(d0, C01), mul_rn(d1, C11)), mul_rn(d2, C12))));
@@ -725,7 +755,7 @@ __global__ void __launch_bounds__(128, (!FAST && std::is_same<S, double>::value)
       }
 #pragma unroll
       for (int v = 0; v < 5; ++v) {
-        const S phi = W[v * nt + k];
+        const S phi = cells.w(v, k);
         g[3 * v] = add_rn(g[3 * v], mul_rn(S(wt0), phi));
         g[3 * v + 1] = add_rn(g[3 * v + 1], mul_rn(S(wt1), phi));
         g[3 * v + 2] = add_rn(g[3 * v + 2], mul_rn(S(wt2), phi));
@@ -744,18 +774,18 @@ __global__ void __launch_bounds__(128, (!FAST && std::is_same<S, double>::value)
     const int f0 = m.cf_index[c], f1 = m.cf_index[c + 1];
     S u0[5];
 #pragma unroll
-    for (int v = 0; v < 5; ++v) { u0[v] = W[v * nt + c]; phi[v] = S(1.); }
+    for (int v = 0; v < 5; ++v) { u0[v] = cells.w(v, cself); phi[v] = S(1.); }
     if (cs.limiter == 3) {
       // minmod (ns_limiters.cc:45-92)
       const double small = 1.e-12;
       for (int j = f0; j < f1; ++j) {
         const int e = m.cf_list[j];
         const int f = e >= 0 ? e : ~e;
-        const int nb = e >= 0 ? m.f_neighbor[f] : m.f_parent[f];
+        const int nb = cells.nbr(m, j, e);
         const double cf0 = sub_rn(m.f_x[f], xc0), cf1 = sub_rn(m.f_x[m.nf + f], xc1), cf2 = sub_rn(m.f_x[2 * m.nf + f], xc2);
 #pragma unroll
         for (int v = 0; v < 5; ++v) {
-          S dU = sub_rn(W[v * nt + nb], u0[v]);
+          S dU = sub_rn(cells.w(v, nb), u0[v]);
           S dUg = add_rn(add_rn(mul_rn(g[3 * v], S(cf0)), mul_rn(g[3 * v + 1], S(cf1))), mul_rn(g[3 * v + 2], S(cf2)));
           S mm;
           if (dU * dUg < 0.) mm = S(0.);
@@ -773,11 +803,10 @@ __global__ void __launch_bounds__(128, (!FAST && std::is_same<S, double>::value)
       for (int v = 0; v < 5; ++v) umax[v] = umin[v] = u0[v];
       for (int j = f0; j < f1; ++j) {
         const int e = m.cf_list[j];
-        const int f = e >= 0 ? e : ~e;
-        const int nb = e >= 0 ? m.f_neighbor[f] : m.f_parent[f];
+        const int nb = cells.nbr(m, j, e);
 #pragma unroll
         for (int v = 0; v < 5; ++v) {
-          const S x = W[v * nt + nb];
+          const S x = cells.w(v, nb);
           umax[v] = smax(umax[v], x);
           umin[v] = smin(umin[v], x);
         }
@@ -849,6 +878,53 @@ __global__ void __launch_bounds__(128, (!FAST && std::is_same<S, double>::value)
   }
 #pragma unroll
   for (int v = 0; v < 5; ++v) Lm[v * nc + c] = phi[v];
+}
+
+template <class S, bool FAST, bool PART = false>
+__global__ void __launch_bounds__(128, (!FAST && std::is_same<S, double>::value) ? 6 : 1) k_grad_limiter(DevCase cs, DevMesh m, const S *__restrict__ W,
+                                                      const unsigned long long *__restrict__ ext, const int *__restrict__ argx,
+                                                      S *__restrict__ G, S *__restrict__ Lm) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  // PART: one rank's gradient cells of a domain decomposition
+  int c = i;
+  if constexpr (PART) {
+    if (i >= m.n_part_cells) return;
+    c = m.part_cells[i];
+  } else {
+    if (i >= m.nc) return;
+  }
+  const CellsGlobal<S> cells{W, m.c_x, m.nt};
+  grad_limiter_cell<S, FAST>(cs, m, W, ext, argx, c, cells, G, Lm);
+}
+
+// The same body over tiles of kGradTile consecutive cells, one block per
+// tile: the states and centroids of every cell the tile's stencils and faces
+// name (the tile's staged set, sorted by cell id, so the loads run along
+// ascending addresses) are copied into shared memory once, and the stencil
+// and limiter loops read them from there through precomputed slot indices
+// (st_local, cf_local, self_local) instead of gathering each from L2 by its
+// cell id.  Least-squares meshes without Green-Gauss cells, FP64, whole mesh.
+constexpr int kGradTile = 128;
+template <bool FAST>
+__global__ void __launch_bounds__(kGradTile) k_grad_limiter_tile(DevCase cs, DevMesh m, const double *__restrict__ W,
+                                                                 const unsigned long long *__restrict__ ext,
+                                                                 double *__restrict__ G, double *__restrict__ Lm) {
+  extern __shared__ double tile_smem[];
+  const int t = blockIdx.x, nt = m.nt;
+  const int s0 = m.tile_off[t], ns = m.tile_off[t + 1] - s0;
+  double *sW = tile_smem, *sX = tile_smem + 5 * ns;
+  for (int s = threadIdx.x; s < ns; s += kGradTile) {
+    const int k = m.tile_cells[s0 + s];
+#pragma unroll
+    for (int v = 0; v < 5; ++v) sW[v * ns + s] = W[v * nt + k];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) sX[i * ns + s] = m.c_x[i * nt + k];
+  }
+  __syncthreads();
+  const int c = t * kGradTile + threadIdx.x;
+  if (c >= m.nc) return;
+  const CellsTile cells{sW, sX, ns, m.self_local[c], m.st_local, m.cf_local};
+  grad_limiter_cell<double, FAST>(cs, m, W, ext, nullptr, c, cells, G, Lm);
 }
 
 // LSQ gradient + continuous limiter (VK with K > 0, none, first order), FP64,

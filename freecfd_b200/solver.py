@@ -178,6 +178,10 @@ class NavierStokes:
         check(lib.fcfd_time_residual_mixed(self.h, int(reps), int(bool(flush_l2)), float(shock_ratio), _d(out)))
         return float(out[0]), int(out[1])
 
+    def set_gradient_kernel(self, kind: int):
+        """0 automatic, 1 per cell, 2 shared-memory tiles of 128 cells."""
+        check(lib.fcfd_ctx_set_gradient_kernel(self.h, int(kind)))
+
     def set_partition(self, lo: int, hi: int):
         """Evaluate only the part of the residual that owned cells [lo, hi)
         need (lo = hi = 0: the whole mesh again)."""

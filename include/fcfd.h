@@ -141,6 +141,14 @@ void fcfd_ctx_destroy(fcfd_ctx *ctx);
  * rounding otherwise.  exact=1 forces the bit-exact form for every limiter. */
 int fcfd_ctx_set_exact_gradients(fcfd_ctx *ctx, int exact);
 
+/* Gradient + limiter kernel (calc_cell_grads + calc_limiter, ns.cc:301-336,
+ * ns_limiters.cc): 0 automatic, 1 per cell (one or, on small meshes, two
+ * threads per cell gathering each stencil cell from L2), 2 per tile of 128
+ * consecutive cells with the states and centroids the tile's stencils and
+ * faces name staged in shared memory once (least-squares meshes without
+ * Green-Gauss cells; FCFD_ERR_UNSUPPORTED otherwise).  Same arithmetic. */
+int fcfd_ctx_set_gradient_kernel(fcfd_ctx *ctx, int kind);
+
 /* Spatial residual R(W) = sum over faces of +/-(F_diffusive - F_convective)
  * for the interior-cell state W[nc][5].  Replaces the residual part of
  * NavierStokes::assemble_linear_system (src/navier_stokes/ns_assemble_linear_system.cc:34-140)
