@@ -206,6 +206,82 @@ __global__ void k_block_jacobi(DevCase cs, DevMesh m, const double *__restrict__
   for (int i = 0; i < 25; ++i) Minv[i * nc + c] = I[i];
 }
 
+// Block ILU(0) of the first-order operator A = B + O in the multicolour
+// order (colours ascending, cells of one colour never face neighbours):
+// modified diagonal blocks Dt_i = B_i - sum over face neighbours j of an
+// earlier colour of A_ij Dt_j^-1 A_ji, with A_ij = -JR_f, A_ji = +JL_f when i
+// is face f's parent and A_ij = +JL_f, A_ji = -JR_f when it is its
+// neighbour (the signs of k_jacobi_sweep).  This is the incomplete LU with
+// no fill when no three cells are pairwise face neighbours (hexahedra,
+// prisms: every other product falls outside the sparsity pattern); around
+// tetrahedral edges the fill between two neighbours of j is dropped (the
+// diagonal form of ILU(0)).  One launch per colour, in colour order; writes
+// Dt_i^-1 ([25][nc], by cell) for the cells of colour `col`.
+__global__ void k_ilu_diag(DevCase cs, DevMesh m, const double *__restrict__ Wn, const double *__restrict__ vol,
+                           const double *__restrict__ dt, const double *__restrict__ JL, const double *__restrict__ JR,
+                           int deg, int cnt, int col, const int *__restrict__ cells, const int *__restrict__ nbr,
+                           const int *__restrict__ src, const int *__restrict__ colour, double *__restrict__ MinvT,
+                           int *__restrict__ err) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= cnt) return;
+  const int nc = m.nc, nf = m.nf;
+  const int c = cells[i];
+  double B[25];
+  diag_block(cs, m, Wn, vol, dt, JL, JR, c, B);
+  for (int sl = 0; sl < deg; ++sl) {
+    const int o = nbr[(size_t)sl * cnt + i];
+    if (o < 0 || colour[o] >= col) continue;
+    const int e = src[(size_t)sl * cnt + i];
+    const int f = e >= 0 ? e : ~e;
+    const double *Jij = e >= 0 ? JR : JL, *Jji = e >= 0 ? JL : JR;
+    const double sij = e >= 0 ? -1. : 1., sji = -sij;
+    // T = Dt_o^-1 A_oc (5x5), then B -= A_co T
+    double T[25];
+#pragma unroll
+    for (int r = 0; r < 5; ++r)
+#pragma unroll
+      for (int q = 0; q < 5; ++q) {
+        double a = 0.;
+#pragma unroll
+        for (int k = 0; k < 5; ++k) a += MinvT[(size_t)(5 * r + k) * nc + o] * (sji * Jji[(size_t)(5 * k + q) * nf + f]);
+        T[5 * r + q] = a;
+      }
+#pragma unroll
+    for (int r = 0; r < 5; ++r)
+#pragma unroll
+      for (int q = 0; q < 5; ++q) {
+        double a = 0.;
+#pragma unroll
+        for (int k = 0; k < 5; ++k) a += (sij * Jij[(size_t)(5 * r + k) * nf + f]) * T[5 * k + q];
+        B[5 * r + q] -= a;
+      }
+  }
+  double I[25];
+#pragma unroll
+  for (int q = 0; q < 25; ++q) I[q] = (q % 6 == 0) ? 1. : 0.;
+  for (int cc = 0; cc < 5; ++cc) {
+    int piv = cc;
+    double best = ::fabs(B[5 * cc + cc]);
+    for (int r = cc + 1; r < 5; ++r)
+      if (::fabs(B[5 * r + cc]) > best) { best = ::fabs(B[5 * r + cc]); piv = r; }
+    if (!(best > 0.)) { atomicOr(err, 4); best = 1.; }
+    if (piv != cc)
+      for (int k = 0; k < 5; ++k) {
+        double t = B[5 * cc + k]; B[5 * cc + k] = B[5 * piv + k]; B[5 * piv + k] = t;
+        t = I[5 * cc + k]; I[5 * cc + k] = I[5 * piv + k]; I[5 * piv + k] = t;
+      }
+    const double inv = 1. / B[5 * cc + cc];
+    for (int k = 0; k < 5; ++k) { B[5 * cc + k] *= inv; I[5 * cc + k] *= inv; }
+    for (int r = 0; r < 5; ++r) {
+      if (r == cc) continue;
+      const double fct = B[5 * r + cc];
+      for (int k = 0; k < 5; ++k) { B[5 * r + k] -= fct * B[5 * cc + k]; I[5 * r + k] -= fct * I[5 * cc + k]; }
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < 25; ++q) MinvT[(size_t)q * nc + c] = I[q];
+}
+
 // z = Minv x (per-cell 5x5), vectors [5][nc] of type T
 // z = Minv (D^-1 x): right preconditioner of the row-scaled system D A
 template <class T>
@@ -856,6 +932,12 @@ struct NewtonState {
   GsPersistArgs gs_args{};
   DBuf<int> gs_sched;
   DBuf<unsigned> gs_bar;  // [0] barrier arrivals, [1] timeout flag
+  // block ILU(0) in the multicolour order: the modified diagonal inverses by
+  // cell and every cell's colour; the solve is one symmetric colour sweep
+  // from y = 0 with those inverses
+  bool ilu = false;
+  DBuf<double> MinvT;
+  DBuf<int> colour;
 };
 
 // Colour of every Gauss-Seidel update of one preconditioner application with
@@ -1087,9 +1169,12 @@ static void apply_prec(fcfd_ctx *x, NewtonState &ns, const T *v, T *z, int sweep
     unsigned *bar = ns.gs_persist ? ns.gs_bar.p : nullptr;
     if constexpr (std::is_same_v<P, T>) {
       k_precond_split<T, P><<<gc, tb, 0, s>>>(nc, ns.Minv.p, v, rs, r, z, bar);
+      // ILU(0): the forward colour sweep starts from y = 0
+      if (ns.ilu) CK(cudaMemsetAsync(z, 0, sizeof(P) * 5 * (size_t)nc, s));
       sweep(OB, MinvP, r, z);
     } else {
       k_precond_split<T, P><<<gc, tb, 0, s>>>(nc, ns.Minv.p, v, rs, r, y, bar);
+      if (ns.ilu) CK(cudaMemsetAsync(y, 0, sizeof(P) * 5 * (size_t)nc, s));
       sweep(OB, MinvP, r, y);
       k_cast<T, P><<<(5 * nc + tb - 1) / tb, tb, 0, s>>>(5 * nc, y, z);
     }
@@ -1199,7 +1284,8 @@ static void gmres(fcfd_ctx *x, NewtonState &ns, Krylov<T> &K, int mode, double r
 }
 
 // Buffers of the implicit solve; volumes uploaded.
-static void alloc_state(fcfd_ctx *x, NewtonState &ns, int sweeps, int cycles, bool prec32, int gs_launch = 0) {
+static void alloc_state(fcfd_ctx *x, NewtonState &ns, int sweeps, int cycles, bool prec32, int gs_launch = 0,
+                        bool ilu = false) {
   const DevMesh &m = x->dm;
   const int nc = m.nc, n = 5 * nc;
   cudaStream_t s = x->stream;
@@ -1209,6 +1295,19 @@ static void alloc_state(fcfd_ctx *x, NewtonState &ns, int sweeps, int cycles, bo
   ns.ic.alloc(1);
   ns.sweeps = sweeps; ns.cycles = cycles > 0 ? cycles : 1;
   ns.prec32 = prec32;
+  ns.ilu = ilu && x->gs_deg > 0;
+  if (ns.ilu) {
+    // ILU(0): one forward and one backward colour sweep (the packed couplings
+    // of the Gauss-Seidel path, the modified diagonal inverses)
+    ns.sweeps = 1;
+    ns.MinvT.alloc(25 * (size_t)nc);
+    std::vector<int> colour(nc, 0);
+    const std::vector<int> &ci = x->color_index;
+    const std::vector<int32_t> &cc = x->mesh->color_cells;
+    for (size_t col = 0; col + 1 < ci.size(); ++col)
+      for (int k = ci[col]; k < ci[col + 1]; ++k) colour[cc[k]] = (int)col;
+    ns.colour.upload(colour);
+  }
   if (ns.sweeps > 0) {
     if (ns.prec32) {
       ns.OB32.alloc((size_t)nc * x->gs_deg * 25 + 1); ns.MinvP32.alloc(25 * (size_t)nc);
@@ -1292,6 +1391,17 @@ static LinearSolve implicit_solve(fcfd_ctx *x, NewtonState &ns, Krylov<double> &
   if (ns.sweeps > 0) {
     const std::vector<int> &ci = x->color_index;
     const int deg = x->gs_deg;
+    if (ns.ilu) {
+      for (size_t col = 0; col + 1 < ci.size(); ++col) {
+        const int cnt = ci[col + 1] - ci[col];
+        if (cnt <= 0) continue;
+        const size_t base = (size_t)ci[col];
+        k_ilu_diag<<<(cnt + 127) / 128, 128, 0, s>>>(x->cs, m, ns.Wn.p, ns.vol.p, ns.dt.p, ns.JL.p, ns.JR.p, deg, cnt,
+                                                     (int)col, x->color_cells.p + base, x->gs_nbr.p + base * deg,
+                                                     x->gs_src.p + base * deg, ns.colour.p, ns.MinvT.p, x->err.p);
+      }
+    }
+    const double *Mpack = ns.ilu ? ns.MinvT.p : ns.Minv.p;
     for (size_t col = 0; col + 1 < ci.size(); ++col) {
       const int cnt = ci[col + 1] - ci[col];
       if (cnt <= 0) continue;
@@ -1299,12 +1409,12 @@ static LinearSolve implicit_solve(fcfd_ctx *x, NewtonState &ns, Krylov<double> &
       if (ns.prec32)
         k_pack_gs<float><<<(cnt + 127) / 128, 128, 0, s>>>(nc, m.nf, deg, cnt, x->color_cells.p + base,
                                                            x->gs_nbr.p + base * deg, x->gs_src.p + base * deg, ns.JL.p,
-                                                           ns.JR.p, ns.Minv.p, ns.OB32.p + base * deg * 25,
+                                                           ns.JR.p, Mpack, ns.OB32.p + base * deg * 25,
                                                            ns.MinvP32.p + base * 25);
       else
         k_pack_gs<double><<<(cnt + 127) / 128, 128, 0, s>>>(nc, m.nf, deg, cnt, x->color_cells.p + base,
                                                             x->gs_nbr.p + base * deg, x->gs_src.p + base * deg, ns.JL.p,
-                                                            ns.JR.p, ns.Minv.p, ns.OB.p + base * deg * 25,
+                                                            ns.JR.p, Mpack, ns.OB.p + base * deg * 25,
                                                             ns.MinvP.p + base * 25);
     }
   }
@@ -1451,7 +1561,7 @@ int fcfd_newton_solve(fcfd_ctx *x, double *W, const fcfd_newton_opts *o, fcfd_ne
     const int tb = 256, gc = (nc + tb - 1) / tb, gn = (n + tb - 1) / tb;
     std::memset(rep, 0, sizeof(*rep));
     NewtonState ns;
-    alloc_state(x, ns, o->precond_sweeps, o->krylov_cycles, o->fp32_krylov != 0, o->gs_launch);
+    alloc_state(x, ns, o->precond_sweeps, o->krylov_cycles, o->fp32_krylov != 0, o->gs_launch, o->precond_ilu0 != 0);
     CK(cudaMemcpyAsync(x->Win.p, W, sizeof(double) * n, cudaMemcpyHostToDevice, s));
     k_aos_to_soa_nc<<<gc, tb, 0, s>>>(x->Win.p, ns.Wn.p, nc);
     const int mdim = o->krylov_dim > 0 ? o->krylov_dim : 30;

@@ -276,6 +276,11 @@ typedef struct fcfd_newton_opts {
                              updates of a preconditioner application in one cooperative launch with
                              grid barriers between them (couplings staged in shared memory where they
                              fit; a barrier that waits too long ends the solve with FCFD_ERR_TIMEOUT) */
+  int32_t precond_ilu0;   /* 1: block ILU(0) of the first-order operator in the multicolour order
+                             (modified diagonal blocks, one forward and one backward colour sweep)
+                             instead of block Jacobi / Gauss-Seidel; precond_sweeps is ignored.  The
+                             reference's PETSc default for its FGMRES (ns_petsc_functions.cc:25-83) is
+                             block Jacobi with ILU(0) inside each process's block */
 } fcfd_newton_opts;
 
 typedef struct fcfd_newton_report {
