@@ -162,6 +162,20 @@ __global__ void k_diag_blocks(DevCase cs, DevMesh m, const double *__restrict__ 
   for (int i = 0; i < 25; ++i) out[25 * (size_t)c + i] = B[i];
 }
 
+// Time-term blocks V P/dt per cell ([nc][25], row = equation, column =
+// primitive variable): NavierStokes::time_terms (ns_time_terms.cc:107-186)
+// with cons2prim (26-56).
+__global__ void k_time_blocks(DevCase cs, int nc, const double *__restrict__ Wn, const double *__restrict__ vol,
+                              const double *__restrict__ dt, double *__restrict__ out) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nc) return;
+  double P[25];
+  cons2prim(cs, Wn[c], Wn[nc + c], Wn[2 * nc + c], Wn[3 * nc + c], Wn[4 * nc + c], P);
+  const double sc = vol[c] / dt[c];
+#pragma unroll
+  for (int i = 0; i < 25; ++i) out[25 * (size_t)c + i] = sc * P[i];
+}
+
 // Block assembly + inversion (Gauss-Jordan, partial pivoting): Minv_c = (V P/dt - J_cc)^-1
 __global__ void k_block_jacobi(DevCase cs, DevMesh m, const double *__restrict__ Wn, const double *__restrict__ vol,
                                const double *__restrict__ dt, const double *__restrict__ JL, const double *__restrict__ JR,
@@ -1705,6 +1719,33 @@ int fcfd_newton_solve(fcfd_ctx *x, double *W, const fcfd_newton_opts *o, fcfd_ne
 // 107-186, cons2prim 26-56) and assemble_linear_system's first-order Jacobian
 // (ns_assemble_linear_system.cc:142-190) build.  blocks[nc][5][5] (row =
 // equation, column = primitive variable).
+int fcfd_time_terms(fcfd_ctx *x, const double *W, const double *dt, double *blocks) {
+  try {
+    if (!x || !W || !dt || !blocks) throw Error(FCFD_ERR_INPUT, "null argument");
+    CK(cudaSetDevice(x->device));
+    const DevMesh &m = x->dm;
+    const int nc = m.nc, n = 5 * nc;
+    cudaStream_t s = x->stream;
+    const int tb = 256, gc = (nc + tb - 1) / tb;
+    DBuf<double> Wn, dtd, B;
+    Wn.alloc(n); dtd.alloc(nc); B.alloc(25 * (size_t)nc);
+    CK(cudaMemcpyAsync(dtd.p, dt, sizeof(double) * nc, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(x->Win.p, W, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+    k_aos_to_soa_nc<<<gc, tb, 0, s>>>(x->Win.p, Wn.p, nc);
+    k_time_blocks<<<gc, tb, 0, s>>>(x->cs, nc, Wn.p, m.c_vol, dtd.p, B.p);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(blocks, B.p, sizeof(double) * 25 * (size_t)nc, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+  } catch (const Error &e) {
+    set_last_error(e.what());
+    return e.code;
+  } catch (const std::exception &e) {
+    set_last_error(e.what());
+    return FCFD_ERR_INPUT;
+  }
+  return FCFD_OK;
+}
+
 int fcfd_diag_blocks(fcfd_ctx *x, const double *W, const double *dt, double *blocks) {
   try {
     if (!x || !W || !dt || !blocks) throw Error(FCFD_ERR_INPUT, "null argument");

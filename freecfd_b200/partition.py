@@ -134,3 +134,192 @@ class PartitionedResidual:
             combine_extrema(self.ext)
             self.ns.partition_residual(self.ext, R)
         return R
+
+
+def gmres(matvec, precond, b, allreduce=None, m: int = 30, rtol: float = 1e-2, cycles: int = 1):
+    """Right-preconditioned GMRES(m) on distributed vectors: each rank holds
+    its owned rows (torch tensors, FP64); `matvec` and `precond` act on them
+    (exchanging halos themselves); every dot product is a local sum followed
+    by one all-reduce (SUM) of the column of dots, so all ranks take the
+    same steps.  Classical Gram-Schmidt applied twice, Givens rotations on
+    the host.  Returns (x, iterations, relative residual).  The distributed
+    counterpart of the device GMRES of fcfd_newton_solve."""
+    import torch
+
+    def dots(vs, w):
+        loc = torch.stack([(v * w).sum() for v in vs])
+        if allreduce is not None:
+            allreduce(loc)
+        return loc.cpu().numpy()
+
+    x = torch.zeros_like(b)
+    bnorm = float(np.sqrt(dots([b], b)[0]))
+    if not bnorm > 0.0:
+        return x, 0, 0.0
+    r = b.clone()
+    its, rel = 0, 1.0
+    for cyc in range(max(1, cycles)):
+        beta = float(np.sqrt(dots([r], r)[0]))
+        if not beta > 0.0:
+            break
+        V, Z = [r / beta], []
+        H = np.zeros((m + 1, m))
+        cs, sn, g = np.zeros(m), np.zeros(m), np.zeros(m + 1)
+        g[0] = beta
+        k = 0
+        for j in range(m):
+            z = precond(V[j])
+            Z.append(z)
+            w = matvec(z)
+            h1 = dots(V, w)
+            w = w - sum(float(h1[i]) * V[i] for i in range(j + 1))
+            h2 = dots(V, w)
+            w = w - sum(float(h2[i]) * V[i] for i in range(j + 1))
+            hn = float(np.sqrt(dots([w], w)[0]))
+            H[: j + 1, j] = h1 + h2
+            H[j + 1, j] = hn
+            for i in range(j):
+                a, c = H[i, j], H[i + 1, j]
+                H[i, j], H[i + 1, j] = cs[i] * a + sn[i] * c, -sn[i] * a + cs[i] * c
+            a, c = H[j, j], H[j + 1, j]
+            rr = float(np.hypot(a, c))
+            cs[j], sn[j] = (a / rr, c / rr) if rr > 0.0 else (1.0, 0.0)
+            H[j, j], H[j + 1, j] = rr, 0.0
+            g[j + 1] = -sn[j] * g[j]
+            g[j] = cs[j] * g[j]
+            k = j + 1
+            its += 1
+            rel = abs(g[j + 1]) / bnorm
+            if rel <= rtol or not hn > 0.0:
+                break
+            V.append(w / hn)
+        y = np.zeros(k)
+        for i in range(k - 1, -1, -1):
+            y[i] = (g[i] - H[i, i + 1:k] @ y[i + 1:k]) / H[i, i]
+        x = x + sum(float(y[i]) * Z[i] for i in range(k))
+        if rel <= rtol or cyc + 1 == max(1, cycles):
+            break
+        r = b - matvec(x)
+    return x, its, rel
+
+
+class DecomposedNewton:
+    """Pseudo-transient Newton-Krylov on one rank of a domain decomposition
+    (the implicit step of NavierStokes::solve, ns.cc:104-118, run as the
+    reference's MPI ranks would: every rank owns a cell range, exchanges its
+    halo before each residual and takes part in every reduction).
+
+    Per Newton step: the owned rows of R(W) (PartitionedResidual), the local
+    time step and the owned cells' diagonal blocks V P/dt - J_cc and time
+    terms V P/dt (fcfd_local_dt, fcfd_diag_blocks, fcfd_time_terms on this
+    rank's state copy, whose owned and halo rows are current), then GMRES on
+    (V P/dt - dR/dW) dW = R with J.v an FP64 finite difference of the
+    partitioned residual (the perturbed state's halo exchanged like the
+    state's), block-Jacobi preconditioning, equations weighted by their RMS
+    row magnitudes and every dot product all-reduced (`gmres`).  The step is
+    limited to a 20 % change of p and T (all-reduced maximum) and the CFL
+    follows the mass residual (switched evolution / relaxation).  The block
+    inverses of a rank use the VK extrema of its own state copy (its
+    preconditioner only; the residual's extrema are all-reduced)."""
+
+    def __init__(self, ns, mesh, case, plan: HaloPlan, rank: int, W):
+        import torch
+        self.ns, self.mesh, self.plan, self.rank = ns, mesh, plan, rank
+        self.lo, self.hi = plan.ranges[rank]
+        self.W = W
+        self.Wp = W.clone()
+        self.res = PartitionedResidual(ns, plan, rank, self.W)
+        self.res_p = PartitionedResidual(ns, plan, rank, self.Wp)
+        self.R = torch.zeros_like(W)
+        self.Rp = torch.zeros_like(W)
+        dv = np.zeros(13)
+        iv = np.zeros(64, np.int32)
+        from ._lib import _d
+        check(lib.fcfd_case_summary(case.h, _d(dv), _i(iv), int(iv.size)))
+        self.Pref, self.Tref = float(dv[2]), float(dv[3])
+
+    def _allreduce(self, t, op=None):
+        import torch.distributed as dist
+        if dist.is_available() and dist.is_initialized():
+            dist.all_reduce(t, op=op or dist.ReduceOp.SUM)
+        return t
+
+    def _gnorm(self, x):
+        import torch
+        t = (x * x).sum().reshape(1).clone()
+        self._allreduce(t)
+        return float(torch.sqrt(t).item())
+
+    def residual(self):
+        self.res(self.R)
+        import torch
+        torch.cuda.synchronize(self.W.device)
+        return self.R[self.lo:self.hi]
+
+    def solve(self, tol=1e-10, max_newton=200, cfl0=1.0, cfl_max=1e6, ser_exponent=1.0, krylov_dim=30,
+              krylov_rtol=1e-2, krylov_cycles=1):
+        import torch
+        import torch.distributed as dist
+        lo, hi = self.lo, self.hi
+        W, dev = self.W, self.W.device
+        R0 = self.residual().clone()
+        r0 = self._gnorm(R0[:, 0])
+        rm, cfl = r0, cfl0
+        history = [1.0]
+        krylov = 0
+        eps_mach = float(np.finfo(np.float64).eps)
+        for it in range(max_newton):
+            if rm <= tol * r0:
+                break
+            Wh = W.cpu().numpy()
+            dt = self.ns.local_dt(Wh, cfl)
+            D = torch.as_tensor(self.ns.diag_blocks(Wh, dt)[lo:hi], device=dev)
+            T = torch.as_tensor(self.ns.time_terms(Wh, dt)[lo:hi], device=dev)
+            Minv = torch.linalg.inv(D)
+            # reference magnitudes of p, |V|, T and the RMS row magnitudes of D
+            Wo = W[lo:hi]
+            n_all = torch.tensor([float(hi - lo)], dtype=torch.float64, device=dev)
+            self._allreduce(n_all)
+            sq = (Wo * Wo).sum(dim=0)
+            self._allreduce(sq)
+            rms = torch.sqrt(sq / n_all)
+            U = float(torch.sqrt(rms[1:4].pow(2).sum()).item()) or 1.0
+            wref = torch.tensor([float(rms[0]) + abs(self.Pref), U, U, U, float(rms[4]) + abs(self.Tref)],
+                                dtype=torch.float64, device=dev)
+            rowmag = (D.abs() * wref.view(1, 1, 5)).sum(dim=2)
+            rsq = (rowmag * rowmag).sum(dim=0)
+            self._allreduce(rsq)
+            wrow = 1.0 / torch.sqrt(rsq / n_all)
+            Winv = 1.0 / wref
+            wscale = self._gnorm(Wo * Winv)
+
+            def matvec(z):
+                zn = self._gnorm(z * Winv)
+                eps = np.sqrt(eps_mach) * (1.0 + wscale) / zn if zn > 0.0 else np.sqrt(eps_mach)
+                self.Wp.copy_(W)
+                self.Wp[lo:hi] += eps * z
+                self.res_p(self.Rp)
+                Jz = (self.Rp[lo:hi] - R0) / eps
+                y = torch.einsum("cij,cj->ci", T, z) - Jz
+                return y * wrow
+
+            def precond(v):
+                return torch.einsum("cij,cj->ci", Minv, v / wrow)
+
+            dW, its, rel = gmres(matvec, precond, R0 * wrow, allreduce=lambda t: self._allreduce(t), m=krylov_dim,
+                                 rtol=krylov_rtol, cycles=krylov_cycles)
+            krylov += its
+            ch = torch.maximum((dW[:, 0] / (Wo[:, 0] + self.Pref)).abs().max(),
+                               (dW[:, 4] / (Wo[:, 4] + self.Tref)).abs().max()).reshape(1).clone()
+            self._allreduce(ch, dist.ReduceOp.MAX if dist.is_available() and dist.is_initialized() else None)
+            dmax = float(ch.item())
+            alpha = 0.2 / dmax if dmax > 0.2 else 1.0
+            W[lo:hi] += alpha * dW
+            R0 = self.residual().clone()
+            rm = self._gnorm(R0[:, 0])
+            history.append(rm / r0)
+            if not np.isfinite(rm):
+                break
+            cfl = min(max(cfl0 * (r0 / rm) ** ser_exponent, 1e-3), cfl_max)
+        return dict(newton_iterations=len(history) - 1, krylov_iterations=krylov, res0=r0, res_final=rm,
+                    history=np.array(history), converged=bool(rm <= tol * r0))

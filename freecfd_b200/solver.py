@@ -408,6 +408,16 @@ class NavierStokes:
         check(lib.fcfd_diag_blocks(self.h, _d(W), _d(dt), _d(out)))
         return out
 
+    def time_terms(self, W, dt):
+        """Time-term blocks V P/dt (nc, 5, 5) at state W and local time
+        steps dt (NavierStokes::time_terms, ns_time_terms.cc:107-186)."""
+        nc = self.mesh.nc
+        W = np.ascontiguousarray(W, dtype=np.float64).reshape(nc, 5)
+        dt = np.ascontiguousarray(dt, dtype=np.float64).reshape(nc)
+        out = np.empty((nc, 5, 5))
+        check(lib.fcfd_time_terms(self.h, _d(W), _d(dt), _d(out)))
+        return out
+
     def time_residual(self, reps: int = 50, flush_l2: bool = True):
         out = np.zeros(8)
         check(lib.fcfd_time_residual(self.h, int(reps), int(bool(flush_l2)), _d(out), out.size))

@@ -334,6 +334,13 @@ int fcfd_newton_solve(fcfd_ctx *ctx, double *W, const fcfd_newton_opts *opts, fc
  * equation (mass, momentum x/y/z, energy), column = primitive (p,u,v,w,T). */
 int fcfd_diag_blocks(fcfd_ctx *ctx, const double *W, const double *dt, double *blocks);
 
+/* Time-term blocks V P/dt of the implicit operator at the state W[nc][5] and
+ * local time steps dt[nc] (host): NavierStokes::time_terms
+ * (ns_time_terms.cc:107-186, cons2prim 26-56).  blocks[nc][5][5], the layout
+ * of fcfd_diag_blocks.  A caller that forms (V P/dt - dR/dW) z itself (a
+ * domain-decomposed solver) applies these to z. */
+int fcfd_time_terms(fcfd_ctx *ctx, const double *W, const double *dt, double *blocks);
+
 /* Coupled steady solve of the flow and k-omega residuals (turbulent decks):
  * pseudo-transient Newton-Krylov on X = (p,u,v,w,T,k,omega) per cell, one
  * system where the reference solves NavierStokes::solve and then RANS::solve
