@@ -83,13 +83,24 @@ def alg_bytes(m, s=8):
             + m.n_grad_entries * 4 + m.n_cell_faces * 4)
 
 
-def kernel_bytes(m, name, viscous=True, exact_grad=False, s=8):
+def kernel_bytes(m, name, viscous=True, exact_grad=False, s=8, fold_entries=0):
     """Algorithmic bytes of one launch of a residual kernel: every array it
     must read once and every array it writes (cell/face/stencil counts from
     the mesh).  Gradients and limiters are counted where a kernel reads or
-    writes them."""
+    writes them.  fold_entries > 0: the gradient over folded stencils, which
+    reads per entry a key and two weighted offsets instead of the entry
+    cell's centroid, and the ghosts' states only in the limiter's face loops."""
     nc, nf, nb, nt = m.nc, m.nf, m.nghost, m.nc + m.nghost
     E, ncf = m.n_grad_entries, m.n_cell_faces
+    if name == "grad_limiter" and fold_entries:
+        b = nc * (5 * s + 3 * s)                     # interior states, own centroid
+        b += nc * (7 * s + 4 + 4) + ncf * 4          # cofactors + det, stencil and cell->face CSR
+        b += fold_entries * (4 + 6 * s)              # folded entries: key, w d of the cell and of its mirror ghosts
+        b += nc * 3 * s                              # mirror weights
+        b += nb * 5 * s                              # ghost states (limiter face loops)
+        b += nf * (8 + 3 * s)                        # face parent/neighbour, face centroids
+        b += nc * (15 * s + 5 * s)                   # gradient and limiter writes
+        return b
     if name == "grad_limiter":
         b = nt * (5 * s + 3 * s)                    # states, centroids (stencils reach the ghosts)
         b += nc * (7 * s + 4 + 4) + E * 4 + ncf * 4  # cofactors + det, stencil and cell->face CSR
@@ -341,7 +352,8 @@ def residual_subline(fb, name, dev, steps, warmup, parity):
     top = max(("grad_limiter", "face_flux", "gather", "ghost_minmax"), key=lambda k: kern[k])
     viscous = "viscosity=0." not in case.deck
     exact_grad = "limiter=minmod" in case.deck or "limiter=bj" in case.deck
-    kb = kernel_bytes(mesh, top, viscous, exact_grad)
+    gi = ns.gradient_info()
+    kb = kernel_bytes(mesh, top, viscous, exact_grad, fold_entries=gi["fold_entries"] if gi["kind"] == 3 else 0)
     out = {"workload": case.workload, "cells": mesh.nc, "faces": mesh.nf, "steps": steps,
            "ms_per_step": round(ms, 5), "value": round(mesh.nf / (ms * 1e-3) / 1e6, 3), "unit": UNIT,
            "step_roofline": {"achieved": round(B / (ms * 1e-3) / 1e9, 1), "frac": round(B / (ms * 1e-3) / 1e9 / peak, 4),
@@ -521,6 +533,7 @@ def run_ours(args):
     # dominant kernel: its own algorithmic bytes over its event-timed duration
     viscous = args.workload in ("cylinder", "plate", "plate64", "plate_rans", "plate64_rans")  # viscous materials
     exact_grad = "limiter=minmod" in case.deck or "limiter=bj" in case.deck
+    gi = ns.gradient_info()
     if rans:
         # coupled step: flow arrays plus k, omega (read with ghosts), their
         # residual, the eddy viscosity per cell and face
@@ -530,7 +543,7 @@ def run_ours(args):
         n_kernels = 11
     else:
         top = max(("grad_limiter", "face_flux", "gather", "ghost_minmax"), key=lambda k: kern[k])
-        kb = kernel_bytes(mesh, top, viscous, exact_grad)
+        kb = kernel_bytes(mesh, top, viscous, exact_grad, fold_entries=gi["fold_entries"] if gi["kind"] == 3 else 0)
         k_ms = float(kern[top])
     k_ach = kb / (k_ms * 1e-3) / 1e9
     traffic = NCU_TRAFFIC.get((args.workload, top))
@@ -544,6 +557,7 @@ def run_ours(args):
                     "d2h_bytes_per_step": int(W.nbytes + (K.nbytes if rans else 0))},
             "roofline": {"bound": "hbm", "achieved": round(k_ach, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(k_ach / peak, 4), "traffic": traffic, "peak_kind": kind, "kernel": top,
+                         "gradient_kernel": {1: "per cell", 2: "tiles", 3: "per cell, folded stencils"}[gi["kind"]],
                          "alg_bytes_per_launch": int(kb), "ms_per_launch": round(k_ms, 5)},
             "step_roofline": {"achieved": round(achieved, 1), "frac": round(achieved / peak, 4), "alg_bytes": int(B),
                               "unit_of_work": "one residual evaluation (all kernels)"},

@@ -29,7 +29,7 @@ EXPORTED = [
     "fcfd_run", "fcfd_restart_write", "fcfd_restart_read", "fcfd_mesh_from_tecplot", "fcfd_rans_jvp",
     "fcfd_partition_sets", "fcfd_ctx_set_partition", "fcfd_partition_extrema", "fcfd_partition_residual",
     "fcfd_ctx_stream", "fcfd_diag_blocks", "fcfd_rans_newton_solve", "fcfd_residual_mixed",
-    "fcfd_time_residual_mixed", "fcfd_ctx_set_gradient_kernel", "fcfd_time_terms",
+    "fcfd_time_residual_mixed", "fcfd_ctx_set_gradient_kernel", "fcfd_time_terms", "fcfd_ctx_gradient_info",
 ]
 
 
@@ -114,6 +114,7 @@ def _load():
     L.fcfd_ctx_set_exact_gradients.argtypes = [vp, ctypes.c_int]
     L.fcfd_ctx_set_gradient_kernel.argtypes = [vp, ctypes.c_int]
     L.fcfd_time_terms.argtypes = [vp, dp, dp, dp]
+    L.fcfd_ctx_gradient_info.argtypes = [vp, i64p]
     L.fcfd_residual.argtypes = [vp, vp, vp, ctypes.c_int]
     L.fcfd_last_stages.argtypes = [vp, dp, dp, dp, dp, dp]
     L.fcfd_local_dt.argtypes = [vp, vp, ctypes.c_double, ctypes.c_int, vp, ctypes.c_int]

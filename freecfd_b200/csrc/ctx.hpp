@@ -134,6 +134,9 @@ struct fcfd_ctx {
   DBuf<int> mx_list, mx_count;
   // tiles of the shared-memory gradient kernel (DevMesh::tile_off ...)
   DBuf<int> tile_off, tile_cells, st_local, cf_local, self_local;
+  // folded stencils of the fused gradient (DevMesh::fold_index ...)
+  DBuf<int> fold_index, fold_key;
+  DBuf<double> fold_e;
   int grad_kernel = 0;  // fcfd_ctx_set_gradient_kernel: 0 automatic, 1 per cell, 2 tiles
 };
 

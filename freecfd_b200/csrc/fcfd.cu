@@ -342,6 +342,58 @@ int fcfd_ctx_create(const fcfd_mesh *mp, const fcfd_case *csp, int device, fcfd_
     }
   }
   d.tile_grad = 0;
+  d.fold_grad = 0;
+  if (!x->green_gauss && !m.grad_weights) {
+    // Folded stencils for the fused gradient: a ghost of a symmetry face whose
+    // normal is exactly (0, 0, +-1) holds its parent's state with w negated
+    // (the symmetry branch of apply_bc), so where the parent is in the same
+    // stencil the ghost's term w (phi_g - phi_c) d joins the parent's entry.
+    // Built when folding removes at least a third of the entries (extruded
+    // one-layer meshes: 27 entries become 9).
+    std::vector<int32_t> gh_face(nb, -1);  // ghost nc + g is the neighbour of boundary face gh_face[g]
+    for (int f = 0; f < nf; ++f)
+      if (m.f_bc[f] >= 0) gh_face[m.f_neighbor[f] - nc] = f;
+    auto zsym = [&](int k) {
+      if (k < nc) return -1;
+      const int f = gh_face[k - nc];
+      const BcRegion &br = c.bc[m.f_bc[f]];
+      if (br.type != BC_SYMMETRY) return -1;
+      if (m.f_normal[3 * (size_t)f] != 0. || m.f_normal[3 * (size_t)f + 1] != 0.) return -1;
+      return m.f_parent[f];
+    };
+    std::vector<int32_t> fidx(nc + 1, 0), fkey;
+    std::vector<double> fe;
+    std::vector<int32_t> keys;
+    for (int cc = 0; cc < nc; ++cc) {
+      const double xc0 = m.c_centroid[3 * (size_t)cc], xc1 = m.c_centroid[3 * (size_t)cc + 1], xc2 = m.c_centroid[3 * (size_t)cc + 2];
+      const int j0 = m.st_index[cc], j1 = m.st_index[cc + 1];
+      keys.assign(m.st_keys.begin() + j0, m.st_keys.begin() + j1);
+      const size_t e0 = fkey.size();
+      auto slot = [&](int k) -> size_t {
+        for (size_t q = e0; q < fkey.size(); ++q)
+          if (fkey[q] == k) return q;
+        fkey.push_back(k);
+        for (int t = 0; t < 6; ++t) fe.push_back(0.);
+        return fkey.size() - 1;
+      };
+      for (int k : keys) {
+        const double d0 = m.c_centroid[3 * (size_t)k] - xc0, d1 = m.c_centroid[3 * (size_t)k + 1] - xc1,
+                     d2 = m.c_centroid[3 * (size_t)k + 2] - xc2;
+        const double w = d0 * d0 + d1 * d1 + d2 * d2;
+        const int par = zsym(k);
+        const bool folded = par >= 0 && std::find(keys.begin(), keys.end(), par) != keys.end();
+        if (k == cc) { slot(cc); continue; }  // the self entry contributes nothing
+        const size_t q = slot(folded ? par : k);
+        const int o = folded ? 3 : 0;
+        fe[6 * q + o] += w * d0; fe[6 * q + o + 1] += w * d1; fe[6 * q + o + 2] += w * d2;
+      }
+      fidx[cc + 1] = (int32_t)fkey.size();
+    }
+    if (3 * fkey.size() <= 2 * m.st_keys.size()) {
+      x->fold_index.upload(fidx); x->fold_key.upload(fkey); x->fold_e.upload(fe);
+      d.fold_grad = 1;
+    }
+  }
   std::vector<int32_t> bface(nb), outl;
   for (int f = 0; f < nf; ++f) {
     if (m.f_bc[f] >= 0) {
@@ -430,6 +482,7 @@ int fcfd_ctx_create(const fcfd_mesh *mp, const fcfd_case *csp, int device, fcfd_
   dm.st_w = x->st_w.p;
   dm.tile_off = x->tile_off.p; dm.tile_cells = x->tile_cells.p; dm.st_local = x->st_local.p;
   dm.cf_local = x->cf_local.p; dm.self_local = x->self_local.p;
+  dm.fold_index = x->fold_index.p; dm.fold_key = x->fold_key.p; dm.fold_e = x->fold_e.p;
   dm.f_wall = x->f_wall.p; dm.f_diss = x->f_diss.p;
   dm.outlet_faces = x->outlet.p; dm.n_outlet = x->n_outlet;
   dm.face_list = x->face_order.p; dm.n_face_list = nf;
@@ -680,13 +733,24 @@ int fcfd_time_residual(fcfd_ctx *x, int reps, int flush_l2, double *out, int out
 int fcfd_ctx_set_gradient_kernel(fcfd_ctx *x, int kind) {
   API_BEGIN
   if (!x) throw Error(FCFD_ERR_INPUT, "null context");
-  if (kind < 0 || kind > 2) throw Error(FCFD_ERR_INPUT, "gradient kernel kind must be 0, 1 or 2");
+  if (kind < 0 || kind > 3) throw Error(FCFD_ERR_INPUT, "gradient kernel kind must be 0, 1, 2 or 3");
   if (kind == 2 && !x->dm.tile_off) throw Error(FCFD_ERR_UNSUPPORTED, "no gradient tiles for this mesh (Green-Gauss or curvilinear cells, or a tile's cells exceed shared memory)");
+  if (kind == 3 && !x->dm.fold_index) throw Error(FCFD_ERR_UNSUPPORTED, "no folded stencils for this mesh (fewer than a third of the entries are z-symmetry ghosts of stencil cells)");
   x->grad_kernel = kind;
   x->cs.tile_grad = (kind == 2) ? 1 : 0;
+  x->cs.fold_grad = ((kind == 0 || kind == 3) && x->dm.fold_index) ? 1 : 0;
   // the captured chains hold the previous gradient kernel
   if (x->graph) { CK(cudaGraphExecDestroy(x->graph)); x->graph = nullptr; }
   if (x->host_graph) { CK(cudaGraphExecDestroy(x->host_graph)); x->host_graph = nullptr; }
+  API_END
+}
+
+int fcfd_ctx_gradient_info(const fcfd_ctx *x, int64_t *out) {
+  API_BEGIN
+  if (!x || !out) throw Error(FCFD_ERR_INPUT, "null argument");
+  out[0] = x->cs.tile_grad ? 2 : ((x->cs.fold_grad && x->cs.fast_grad) ? 3 : 1);
+  out[1] = (int64_t)x->fold_key.n;
+  out[2] = x->cs.fast_grad;
   API_END
 }
 

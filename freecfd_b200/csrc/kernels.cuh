@@ -207,6 +207,7 @@ struct DevCase {
   int fast_grad;
   int pair_grad;  // every cell has a gradient stencil: the two-threads-per-cell gradient may run
   int tile_grad;  // the shared-memory tile gradient kernel runs (DevMesh tiles built)
+  int fold_grad;  // the fused gradient sums the folded stencils (DevMesh fold_* built)
   DevBC bc[kMaxBC];
 };
 
@@ -231,6 +232,13 @@ struct DevMesh {
   const int *tile_off = nullptr, *tile_cells = nullptr, *st_local = nullptr, *cf_local = nullptr,
             *self_local = nullptr;
   int tile_slots_max = 0;
+  // least-squares stencils with the symmetry ghosts of z-normal planes folded
+  // into their parents' entries (null: not built): per cell the entries
+  // [fold_index[c], fold_index[c+1]), entry j naming cell fold_key[j] with
+  // the weighted offsets fold_e[6j..6j+2] = w d of the cell itself and
+  // fold_e[6j+3..6j+5] = sum of w d over its mirror ghosts in the stencil
+  const int *fold_index = nullptr, *fold_key = nullptr;
+  const double *fold_e = nullptr;
   const int *bface;                        // boundary faces in ghost order [nb]
   const int *outlet_faces;                 // outlet boundary faces [n_outlet]
   const double *f_wall, *f_diss;           // [nf] wall distance, dissipation factor (Steger-Warming only)
@@ -654,6 +662,40 @@ struct CellsTile {
   __device__ __forceinline__ int nbr(const DevMesh &, int j, int) const { return cf_local[j]; }
 };
 
+// Fused least-squares sums over the folded stencil entries [j0, j1) of cell
+// c: entry j names cell k with E0 = w d of k itself (zero for c) and Eg = the
+// sum of w d over k's mirror ghosts across z-normal symmetry planes in c's
+// stencil; those ghosts hold (p, u, v, -w, T) of k, so
+//   acc_v += (phi_k - phi_c) (E0 + Eg)        for p, u, v, T
+//   acc_w += (w_k - w_c) E0 + (-w_k - w_c) Eg
+// which is the unfolded sum over all the entries, regrouped.
+template <class S>
+__device__ __forceinline__ void fold_sum(const DevMesh &m, const S *__restrict__ W, int nt, int c, const S u0[5],
+                                         S acc[15], int j0, int j1) {
+#pragma unroll 2
+  for (int j = j0; j < j1; ++j) {
+    const int k = m.fold_key[j];
+    const double *E = m.fold_e + 6 * (size_t)j;
+    const double a0 = E[0], a1 = E[1], a2 = E[2], b0 = E[3], b1 = E[4], b2 = E[5];
+    const double s0 = a0 + b0, s1 = a1 + b1, s2 = a2 + b2;
+#pragma unroll
+    for (int v = 0; v < 5; ++v) {
+      const S phi = W[v * nt + k];
+      if (v == 3) {
+        const S q0 = phi - u0[3], qg = -1. * phi - u0[3];
+        acc[9] = acc[9] + q0 * a0 + qg * b0;
+        acc[10] = acc[10] + q0 * a1 + qg * b1;
+        acc[11] = acc[11] + q0 * a2 + qg * b2;
+      } else {
+        const S q = phi - u0[v];
+        acc[3 * v] = acc[3 * v] + q * s0;
+        acc[3 * v + 1] = acc[3 * v + 1] + q * s1;
+        acc[3 * v + 2] = acc[3 * v + 2] + q * s2;
+      }
+    }
+  }
+}
+
 // LSQ gradient (bit-exact restatement of Variable::cell_gradient over the
 // lsqr_grad_map weights) + limiter of interior cell c, reading the cells it
 // needs through the accessor A (W itself is read directly only for the VK
@@ -683,8 +725,15 @@ __device__ __forceinline__ void grad_limiter_cell(const DevCase &cs, const DevMe
     S acc[15];
 #pragma unroll
     for (int i = 0; i < 15; ++i) acc[i] = S(0.);
+    if constexpr (std::is_same<A, CellsGlobal<S>>::value) {
+      if (cs.fold_grad) {
+        // folded stencil: a z-normal symmetry ghost holds its parent's state
+        // with w negated, so its term w (phi_g - phi_c) d joins the parent's
+        fold_sum(m, cells.W, nt, c, u0, acc, m.fold_index[c], m.fold_index[c + 1]);
+      }
+    }
 #pragma unroll 4
-    for (int j = j0; j < j1; ++j) {
+    for (int j = (std::is_same<A, CellsGlobal<S>>::value && cs.fold_grad) ? j1 : j0; j < j1; ++j) {
       const int k = cells.key(m, j);
       if (k == cself) continue;
       const double d0 = cells.x(0, k) - xc0, d1 = cells.x(1, k) - xc1, d2 = cells.x(2, k) - xc2;
@@ -957,8 +1006,12 @@ __global__ void __launch_bounds__(64) k_grad_limiter_pair(DevCase cs, DevMesh m,
     xc0 = m.c_x[c]; xc1 = m.c_x[nt + c]; xc2 = m.c_x[2 * nt + c];
 #pragma unroll
     for (int v = 0; v < 5; ++v) u0[v] = W[v * nt + c];
+    if (cs.fold_grad) {
+      const int f0 = m.fold_index[c], f1 = m.fold_index[c + 1], fm = (f0 + f1) >> 1;
+      fold_sum(m, W, nt, c, u0, acc, h == 0 ? f0 : fm, h == 0 ? fm : f1);
+    }
     const int j0 = m.st_index[c], j1 = m.st_index[c + 1], mid = (j0 + j1) >> 1;
-    const int a = h == 0 ? j0 : mid, b = h == 0 ? mid : j1;
+    const int a = h == 0 ? j0 : mid, b = cs.fold_grad ? a : (h == 0 ? mid : j1);
 #pragma unroll 4
     for (int j = a; j < b; ++j) {
       const int k = m.st_keys[j];

@@ -182,6 +182,13 @@ class NavierStokes:
         """0 automatic, 1 per cell, 2 shared-memory tiles of 128 cells."""
         check(lib.fcfd_ctx_set_gradient_kernel(self.h, int(kind)))
 
+    def gradient_info(self):
+        """dict(kind=1 per cell | 2 tiles | 3 folded stencils, fold_entries,
+        fused) of the gradient kernel the residual runs."""
+        out = (ctypes.c_int64 * 3)()
+        check(lib.fcfd_ctx_gradient_info(self.h, out))
+        return dict(kind=int(out[0]), fold_entries=int(out[1]), fused=bool(out[2]))
+
     def set_partition(self, lo: int, hi: int):
         """Evaluate only the part of the residual that owned cells [lo, hi)
         need (lo = hi = 0: the whole mesh again)."""

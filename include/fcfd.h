@@ -142,12 +142,23 @@ void fcfd_ctx_destroy(fcfd_ctx *ctx);
 int fcfd_ctx_set_exact_gradients(fcfd_ctx *ctx, int exact);
 
 /* Gradient + limiter kernel (calc_cell_grads + calc_limiter, ns.cc:301-336,
- * ns_limiters.cc): 0 automatic, 1 per cell (one or, on small meshes, two
- * threads per cell gathering each stencil cell from L2), 2 per tile of 128
- * consecutive cells with the states and centroids the tile's stencils and
- * faces name staged in shared memory once (least-squares meshes without
- * Green-Gauss cells; FCFD_ERR_UNSUPPORTED otherwise).  Same arithmetic. */
+ * ns_limiters.cc): 0 automatic (3 where built, else 1), 1 per cell (one or,
+ * on small meshes, two threads per cell gathering each stencil cell from
+ * L2), 2 per tile of 128 consecutive cells with the states and centroids the
+ * tile's stencils and faces name staged in shared memory once (same
+ * arithmetic), 3 per cell with the fused least-squares sums over folded
+ * stencils: the ghosts of z-normal symmetry faces (the front and back planes
+ * of one-layer meshes) hold their parents' states with w negated, so their
+ * terms join their parents' entries (27 entries become 9; equal to the
+ * unfolded sum to rounding; continuous limiters only, the bit-exact path is
+ * unchanged).  FCFD_ERR_UNSUPPORTED for a kind the mesh does not have. */
 int fcfd_ctx_set_gradient_kernel(fcfd_ctx *ctx, int kind);
+
+/* The gradient kernel the residual runs: out[0] = 1 per cell, 2 tiles, 3
+ * per cell over folded stencils; out[1] = folded stencil entries (0 if not
+ * built); out[2] = 1 for the fused (continuous-limiter) gradient, 0 for the
+ * bit-exact one. */
+int fcfd_ctx_gradient_info(const fcfd_ctx *ctx, int64_t *out);
 
 /* Spatial residual R(W) = sum over faces of +/-(F_diffusive - F_convective)
  * for the interior-cell state W[nc][5].  Replaces the residual part of

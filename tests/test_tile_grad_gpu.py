@@ -12,7 +12,7 @@ import numpy as np
 import pytest
 
 from freecfd_b200 import cases
-from tests.util import ALL, build_pair, res_err
+from tests.util import ALL, SMALL, build_pair, res_err
 
 
 @pytest.mark.gpu
@@ -56,3 +56,34 @@ def test_tile_gradient_refused_without_lsq(oracle_mod, fb):
         assert e.value.code == 7
         ns.set_gradient_kernel(1)
         ns.set_gradient_kernel(0)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("family", ["cylinder", "wedge", "hypersonic"])
+def test_folded_stencil_gradient(family, oracle_mod, fb):
+    """Folded stencils (kind 3, the default where built): on one-layer meshes
+    the z-symmetry ghosts' terms join their parents' entries.  The residual
+    equals the unfolded one to rounding and keeps the oracle bar, with the
+    fused gradient (VK, K > 0); the tangent chain folds too."""
+    case = SMALL[family](limiter="vk")
+    o, cs, m = build_pair(case, oracle_mod, fb)
+    ns = fb.NavierStokes(m, cs, 0)
+    ns.set_gradient_kernel(3)
+    R3 = ns.residual(case.state)
+    ns.set_gradient_kernel(1)
+    R1 = ns.residual(case.state)
+    ref = o.residual(case.state)
+    assert res_err(R3, ref).max() <= 1e-12
+    assert res_err(R3, R1).max() <= 1e-13
+    ns.set_gradient_kernel(0)
+    assert np.array_equal(ns.residual(case.state), R3)
+
+
+@pytest.mark.gpu
+def test_folded_stencil_not_built_for_layered_plate(oracle_mod, fb):
+    case = cases.plate_case(ni=24, nj=12, nk=6, turbulent=False)
+    o, cs, m = build_pair(case, oracle_mod, fb)
+    ns = fb.NavierStokes(m, cs, 0)
+    with pytest.raises(fb.FcfdError) as e:
+        ns.set_gradient_kernel(3)
+    assert e.value.code == 7
