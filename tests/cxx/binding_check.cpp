@@ -9,6 +9,8 @@
 //             xyz[n_nodes*3] f64, conn_index[n_cells+1], conn[conn_len],
 //             bc_index[n_bc+1], bc_nodes[bc_len] (int32)
 // Prints one line of key=value pairs.
+#include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <fstream>
@@ -59,6 +61,19 @@ int main(int argc, char **argv) {
   fcfd_mesh_sizes(mesh, sz);
   std::printf(" n_cells=%lld n_faces=%lld n_ghosts=%lld", (long long)sz[0], (long long)sz[1], (long long)sz[2]);
 
+  // reverse Cuthill-McKee order: a permutation of the cells
+  {
+    std::vector<int32_t> perm((size_t)sz[0]), seen((size_t)sz[0], 0);
+    const int rcr = fcfd_mesh_rcm(mesh, perm.data());
+    bool ok = rcr == FCFD_OK;
+    for (int32_t p : perm) {
+      if (p < 0 || p >= sz[0] || seen[(size_t)p]) { ok = false; break; }
+      seen[(size_t)p] = 1;
+    }
+    std::printf(" rcm_rc=%d rcm_permutation=%d", rcr, ok ? 1 : 0);
+    std::printf(" grad_weights_rc=%d", fcfd_mesh_grad_weights(mesh, nullptr));
+  }
+
   // error path: a mesh with a cell of 7 nodes is rejected, not aborted
   std::vector<int32_t> cidx7(cidx);
   cidx7[1] = cidx7[0] + 7;
@@ -79,6 +94,17 @@ int main(int argc, char **argv) {
     if (!get(fw, W.data(), W.size())) { std::printf(" state_file=short\n"); return 1; }
     rc = fcfd_residual(ctx, W.data(), R.data(), 0);
     std::printf(" residual_rc=%d", rc);
+    // the mixed-precision residual with every face in FP64 equals it
+    std::vector<double> R2(R.size());
+    int64_t n64 = -1;
+    const int rcm = fcfd_residual_mixed(ctx, W.data(), R2.data(), 0.0, 0, &n64);
+    double dmax = 0., rmax = 0.;
+    for (size_t i = 0; i < R.size(); ++i) {
+      dmax = std::max(dmax, std::fabs(R2[i] - R[i]));
+      rmax = std::max(rmax, std::fabs(R[i]));
+    }
+    std::printf(" mixed_rc=%d mixed_fp64_faces=%lld mixed_rel_diff=%.3e", rcm, (long long)n64, rmax > 0. ? dmax / rmax : dmax);
+    std::printf(" set_kernel_bad_rc=%d", fcfd_ctx_set_gradient_kernel(ctx, 9));
     std::ofstream fr(argv[4], std::ios::binary);
     fr.write(reinterpret_cast<const char *>(R.data()), (std::streamsize)(R.size() * sizeof(double)));
   }

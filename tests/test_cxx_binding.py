@@ -67,6 +67,8 @@ def test_cxx_caller_cpu_paths(oracle_mod):
     o = oracle_mod.Oracle(case, tmp)
     assert (int(kv["n_cells"]), int(kv["n_faces"]), int(kv["n_ghosts"])) == (o.nc, o.nf, o.nghost)
     assert kv["ctx_rc"] == ("0" if torch.cuda.is_available() else "5")
+    assert kv["rcm_rc"] == "0" and kv["rcm_permutation"] == "1"
+    assert kv["grad_weights_rc"] == "1"  # null output pointer: FCFD_ERR_INPUT
 
 
 @pytest.mark.gpu
@@ -78,3 +80,8 @@ def test_cxx_caller_residual(oracle_mod):
     R = np.fromfile(rfile).reshape(-1, 5)
     ref = oracle_mod.Oracle(case, tmp).residual(case.state)
     assert res_err(R, ref).max() <= 1e-12
+    # the mixed-precision residual with every face in FP64 (shock ratio 0)
+    # equals the FP64 residual; a bad gradient-kernel kind is FCFD_ERR_INPUT
+    assert kv["mixed_rc"] == "0" and int(kv["mixed_fp64_faces"]) > 0
+    assert float(kv["mixed_rel_diff"]) <= 1e-14
+    assert kv["set_kernel_bad_rc"] == "1"
