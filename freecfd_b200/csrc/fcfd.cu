@@ -344,7 +344,7 @@ int fcfd_ctx_create(const fcfd_mesh *mp, const fcfd_case *csp, int device, fcfd_
   d.tile_grad = 0;
   d.fold_grad = 0;
   if (!x->green_gauss && !m.grad_weights) {
-    // Folded stencils for the fused gradient: a ghost of a symmetry face whose
+    // Folded stencils for the fused gradient (kind 3): a ghost of a symmetry face whose
     // normal is exactly (0, 0, +-1) holds its parent's state with w negated
     // (the symmetry branch of apply_bc), so where the parent is in the same
     // stencil the ghost's term w (phi_g - phi_c) d joins the parent's entry.
@@ -391,7 +391,6 @@ int fcfd_ctx_create(const fcfd_mesh *mp, const fcfd_case *csp, int device, fcfd_
     }
     if (3 * fkey.size() <= 2 * m.st_keys.size()) {
       x->fold_index.upload(fidx); x->fold_key.upload(fkey); x->fold_e.upload(fe);
-      d.fold_grad = 1;
     }
   }
   std::vector<int32_t> bface(nb), outl;
@@ -738,7 +737,7 @@ int fcfd_ctx_set_gradient_kernel(fcfd_ctx *x, int kind) {
   if (kind == 3 && !x->dm.fold_index) throw Error(FCFD_ERR_UNSUPPORTED, "no folded stencils for this mesh (fewer than a third of the entries are z-symmetry ghosts of stencil cells)");
   x->grad_kernel = kind;
   x->cs.tile_grad = (kind == 2) ? 1 : 0;
-  x->cs.fold_grad = ((kind == 0 || kind == 3) && x->dm.fold_index) ? 1 : 0;
+  x->cs.fold_grad = (kind == 3) ? 1 : 0;
   // the captured chains hold the previous gradient kernel
   if (x->graph) { CK(cudaGraphExecDestroy(x->graph)); x->graph = nullptr; }
   if (x->host_graph) { CK(cudaGraphExecDestroy(x->host_graph)); x->host_graph = nullptr; }

@@ -142,7 +142,7 @@ void fcfd_ctx_destroy(fcfd_ctx *ctx);
 int fcfd_ctx_set_exact_gradients(fcfd_ctx *ctx, int exact);
 
 /* Gradient + limiter kernel (calc_cell_grads + calc_limiter, ns.cc:301-336,
- * ns_limiters.cc): 0 automatic (3 where built, else 1), 1 per cell (one or,
+ * ns_limiters.cc): 0 automatic (1), 1 per cell (one or,
  * on small meshes, two threads per cell gathering each stencil cell from
  * L2), 2 per tile of 128 consecutive cells with the states and centroids the
  * tile's stencils and faces name staged in shared memory once (same
@@ -151,7 +151,9 @@ int fcfd_ctx_set_exact_gradients(fcfd_ctx *ctx, int exact);
  * of one-layer meshes) hold their parents' states with w negated, so their
  * terms join their parents' entries (27 entries become 9; equal to the
  * unfolded sum to rounding; continuous limiters only, the bit-exact path is
- * unchanged).  FCFD_ERR_UNSUPPORTED for a kind the mesh does not have. */
+ * unchanged; measured no faster than 1 on the benchmark cylinder, since the
+ * stencil loop does not set that kernel's time).  FCFD_ERR_UNSUPPORTED for a
+ * kind the mesh does not have. */
 int fcfd_ctx_set_gradient_kernel(fcfd_ctx *ctx, int kind);
 
 /* The gradient kernel the residual runs: out[0] = 1 per cell, 2 tiles, 3

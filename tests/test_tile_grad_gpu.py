@@ -61,10 +61,10 @@ def test_tile_gradient_refused_without_lsq(oracle_mod, fb):
 @pytest.mark.gpu
 @pytest.mark.parametrize("family", ["cylinder", "wedge", "hypersonic"])
 def test_folded_stencil_gradient(family, oracle_mod, fb):
-    """Folded stencils (kind 3, the default where built): on one-layer meshes
-    the z-symmetry ghosts' terms join their parents' entries.  The residual
-    equals the unfolded one to rounding and keeps the oracle bar, with the
-    fused gradient (VK, K > 0); the tangent chain folds too."""
+    """Folded stencils (kind 3): on one-layer meshes the z-symmetry ghosts'
+    terms join their parents' entries.  The residual equals the unfolded one
+    to rounding and keeps the oracle bar, with the fused gradient (VK,
+    K > 0); the automatic choice is the unfolded per-cell kernel."""
     case = SMALL[family](limiter="vk")
     o, cs, m = build_pair(case, oracle_mod, fb)
     ns = fb.NavierStokes(m, cs, 0)
@@ -76,7 +76,7 @@ def test_folded_stencil_gradient(family, oracle_mod, fb):
     assert res_err(R3, ref).max() <= 1e-12
     assert res_err(R3, R1).max() <= 1e-13
     ns.set_gradient_kernel(0)
-    assert np.array_equal(ns.residual(case.state), R3)
+    assert np.array_equal(ns.residual(case.state), R1)
 
 
 @pytest.mark.gpu
