@@ -58,7 +58,7 @@ class _RawMesh(ctypes.Structure):
 class RunOpts(ctypes.Structure):
     _fields_ = [("work_dir", ctypes.c_char_p), ("restart_step", ctypes.c_int32), ("max_steps", ctypes.c_int32),
                 ("jvp_mode", ctypes.c_int32), ("fp32_krylov", ctypes.c_int32), ("precond_sweeps", ctypes.c_int32),
-                ("echo", ctypes.c_int32)]
+                ("echo", ctypes.c_int32), ("K", ctypes.POINTER(ctypes.c_double))]
 
 
 class RunReport(ctypes.Structure):

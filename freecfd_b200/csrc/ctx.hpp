@@ -210,6 +210,14 @@ inline void launch_faces(fcfd_ctx *x, Pipe<S> &P, const S *mu_t, S *mo, S *wo, c
 void ns_block_inverse(fcfd_ctx *x, const double *Wn, const double *vol, const double *dt, const double *mutf,
                       double *JL, double *JR, double *Minv, double *rowmag);
 void adjoint_free(fcfd_ctx *x);
+// rans.cu: the coupled implicit step of the time-marching driver for turbulent
+// decks (an opaque driver state: X = (W, K), its residual, the Krylov solve)
+void *kw_driver_create(fcfd_ctx *x, const double *W, const double *K, int mdim);
+void kw_driver_destroy(void *p);
+void kw_driver_residual(fcfd_ctx *x, void *p);
+int kw_driver_step(fcfd_ctx *x, void *p, const double *dt, int mode, double krtol, double kabstol);
+void kw_driver_update(fcfd_ctx *x, void *p, const double *dt, double *part, int *err);
+void kw_driver_state(fcfd_ctx *x, void *p, double *W, double *K, double *mut);
 // mixed.cu: FP32 face pass + FP64 pass over the shock-flagged faces
 void launch_mixed_faces(fcfd_ctx *x, double shock_ratio, int *list, int *count, cudaStream_t s);
 void rans_setup(fcfd_ctx *x);

@@ -1797,7 +1797,9 @@ int fcfd_run(fcfd_ctx *x, double *W, const fcfd_run_opts *o, fcfd_run_report *re
     CK(cudaSetDevice(x->device));
     std::memset(rep, 0, sizeof(*rep));
     const fcfd_case &cs = *x->case_ptr;
-    if (cs.turbulent) throw Error(FCFD_ERR_UNSUPPORTED, "the time-marching driver runs laminar / Euler cases (no implicit k-omega step)");
+    // turbulent decks: one coupled implicit solve per time step on (W, K)
+    const bool turb = cs.turbulent;
+    if (turb && !o->K) throw Error(FCFD_ERR_INPUT, "a turbulent deck needs opts->K (k and omega per cell, in/out)");
     TimeMarching tm = cs.tm;
     if (tm.ps_steps > 1) throw Error(FCFD_ERR_UNSUPPORTED, "pseudo-time (dual time stepping) iterations are not on the B200 path");
     if ((int)cs.load_bcs.size() > kMaxBC) throw Error(FCFD_ERR_UNSUPPORTED, "more than 16 load BCs");
@@ -1811,10 +1813,11 @@ int fcfd_run(fcfd_ctx *x, double *W, const fcfd_run_opts *o, fcfd_run_report *re
     const int restart_step = o->restart_step > 0 ? o->restart_step : 0;
     double time = 0.;
     double first[3] = {0., 0., 0.};
-    if (restart_step > 0) {
-      double rf[2];
-      restart_read(wd.c_str(), 1, restart_step, nc, &time, first, rf, W, nullptr, nullptr);
-    }
+    double first_rans[2] = {0., 0.};
+    std::vector<double> mut_h(turb ? nc : 0);
+    if (restart_step > 0)
+      restart_read(wd.c_str(), 1, restart_step, nc, &time, first, first_rans, W, turb ? o->K : nullptr,
+                   turb ? mut_h.data() : nullptr);
     // solver state (one GMRES cycle of at most `maximumiterations` vectors)
     NewtonState ns;
     alloc_state(x, ns, o->precond_sweeps, 1, o->fp32_krylov != 0);
@@ -1826,6 +1829,8 @@ int fcfd_run(fcfd_ctx *x, double *W, const fcfd_run_opts *o, fcfd_run_report *re
     x->newton_f32 = o->jvp_mode == 3 || o->jvp_mode == 4;
     const int jmode = o->jvp_mode == 0 ? 0 : 1;
     if (f32) K32.alloc(x, mdim); else K64.alloc(x, mdim);
+    struct KwGuard { void *p = nullptr; ~KwGuard() { if (p) kw_driver_destroy(p); } } kd;
+    if (turb) kd.p = kw_driver_create(x, W, o->K, mdim);
     DBuf<double> part, hh, lpart, hdt;
     part.alloc(kRedBlocks); hh.alloc(1);
     DBuf<unsigned long long> key;
@@ -1835,7 +1840,7 @@ int fcfd_run(fcfd_ctx *x, double *W, const fcfd_run_opts *o, fcfd_run_report *re
     const int nlb = (m.nf + kLoadBlock - 1) / kLoadBlock;
     if (nl > 0) { lbcs.upload(cs.load_bcs); lpart.alloc((size_t)nlb * nl * 6); }
     DBuf<double> upart;
-    upart.alloc((size_t)gc * 3);
+    upart.alloc((size_t)gc * (turb ? 5 : 3));
     CK(cudaMemcpyAsync(x->Win.p, W, sizeof(double) * n, cudaMemcpyHostToDevice, s));
     k_aos_to_soa_nc<<<gc, tb, 0, s>>>(x->Win.p, ns.Wn.p, nc);
     // schedule file (set_time_step_options, time_step.cc:44-58)
@@ -1868,14 +1873,21 @@ int fcfd_run(fcfd_ctx *x, double *W, const fcfd_run_opts *o, fcfd_run_report *re
       std::printf("=============================================================================================================\n");
     }
     if (nl > 0) mkdir((wd + "/volume_output").c_str(), S_IRWXU);
-    std::vector<double> host_W(n), host_dt(nc);
+    std::vector<double> host_W(n), host_dt(nc), host_K(turb ? 2 * (size_t)nc : 0);
     auto save_restart = [&](int step) {
-      k_soa_to_aos_nc<<<gc, tb, 0, s>>>(ns.Wn.p, x->Win.p, nc);
-      CK(cudaMemcpyAsync(host_W.data(), x->Win.p, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+      if (turb) {
+        // the eddy viscosity of the updated state, as RANS::solve leaves it
+        // (update_eddy_viscosity after update_variables, rans.cc:85-98)
+        kw_driver_residual(x, kd.p);
+        kw_driver_state(x, kd.p, host_W.data(), host_K.data(), mut_h.data());
+      } else {
+        k_soa_to_aos_nc<<<gc, tb, 0, s>>>(ns.Wn.p, x->Win.p, nc);
+        CK(cudaMemcpyAsync(host_W.data(), x->Win.p, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+      }
       CK(cudaMemcpyAsync(host_dt.data(), ns.dt.p, sizeof(double) * nc, cudaMemcpyDeviceToHost, s));
       CK(cudaStreamSynchronize(s));
-      restart_write(wd.c_str(), 1, step, time, first, nullptr, nc, (int)(x->mesh->nodes.size() / 3), host_W.data(),
-                    host_dt.data(), nullptr, nullptr);
+      restart_write(wd.c_str(), 1, step, time, first, turb ? first_rans : nullptr, nc, (int)(x->mesh->nodes.size() / 3),
+                    host_W.data(), host_dt.data(), turb ? host_K.data() : nullptr, turb ? mut_h.data() : nullptr);
     };
     auto t0 = std::chrono::steady_clock::now();
     int status = FCFD_OK;
@@ -1896,7 +1908,8 @@ int fcfd_run(fcfd_ctx *x, double *W, const fcfd_run_opts *o, fcfd_run_report *re
       }
       // the state and its residual (the residual also loads W into the
       // gradient / limiter pipeline that the time step reads)
-      eval_residual<double>(x, ns.Wn.p, ns.R0.p, (const double *)nullptr, (const double *)nullptr);
+      if (turb) kw_driver_residual(x, kd.p);
+      else eval_residual<double>(x, ns.Wn.p, ns.R0.p, (const double *)nullptr, (const double *)nullptr);
       double max_cfl = -1.;
       if (tm.type == TS_FIXED) {
         k_fill_value<<<gc, tb, 0, s>>>(nc, ns.dt.p, ts_cur);
@@ -1952,11 +1965,15 @@ int fcfd_run(fcfd_ctx *x, double *W, const fcfd_run_opts *o, fcfd_run_report *re
           for (size_t k = 0; k < loads.size(); ++k) loads[k] += hp[(size_t)bl * nl * 6 + k];
       }
       // ---- implicit step
-      const LinearSolve ls = implicit_solve(x, ns, K64, K32, f32, jmode, cs.lin_rtol, cs.lin_abstol, part, hh);
+      LinearSolve ls;
+      if (turb) ls.iters = kw_driver_step(x, kd.p, ns.dt.p, o->jvp_mode, cs.lin_rtol, cs.lin_abstol);
+      else ls = implicit_solve(x, ns, K64, K32, f32, jmode, cs.lin_rtol, cs.lin_abstol, part, hh);
       rep->krylov_iterations += ls.iters;
       CK(cudaMemsetAsync(x->err.p, 0, sizeof(int), s));
-      k_update_res<<<gc, tb, 0, s>>>(nc, ns.Wn.p, ns.R1.p, ns.dt.p, upart.p, x->err.p);
-      std::vector<double> hu((size_t)gc * 3);
+      const int nsum = turb ? 5 : 3;
+      if (turb) kw_driver_update(x, kd.p, ns.dt.p, upart.p, x->err.p);
+      else k_update_res<<<gc, tb, 0, s>>>(nc, ns.Wn.p, ns.R1.p, ns.dt.p, upart.p, x->err.p);
+      std::vector<double> hu((size_t)gc * nsum);
       int h = 0;
       CK(cudaMemcpyAsync(hu.data(), upart.p, sizeof(double) * hu.size(), cudaMemcpyDeviceToHost, s));
       CK(cudaMemcpyAsync(&h, x->err.p, sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -1968,17 +1985,32 @@ int fcfd_run(fcfd_ctx *x, double *W, const fcfd_run_opts *o, fcfd_run_report *re
         rep->steps = step - restart_step;
         break;
       }
-      double tot[3] = {0., 0., 0.};
+      double tot[5] = {0., 0., 0., 0., 0.};
       for (int bl = 0; bl < gc; ++bl)
-        for (int i = 0; i < 3; ++i) tot[i] += hu[(size_t)bl * 3 + i];
-      if (step == 1)
+        for (int i = 0; i < nsum; ++i) tot[i] += hu[(size_t)bl * nsum + i];
+      if (step == 1) {
         for (int i = 0; i < 3; ++i) first[i] = std::sqrt(tot[i]);
+        if (turb)
+          for (int i = 0; i < 2; ++i) first_rans[i] = std::sqrt(tot[3 + i]);
+      }
       res = 0.;
       for (int i = 0; i < 3; ++i) res += std::sqrt(tot[i]) / first[i] / 3.;
-      // ---- screen and convergence.dat lines (main.cc:351-369)
-      std::fprintf(conv, "%d\t%d\t%.3e\t%.3e\t%d\t%.3e\n", step, 1, time, max_cfl, ls.iters, res);
+      // the k-omega residual of RANS::update_variables (rans.cc:240-250)
+      double rres = 0.;
+      if (turb)
+        for (int i = 0; i < 2; ++i) rres += std::sqrt(tot[3 + i]) / first_rans[i] / 2.;
+      // ---- screen and convergence.dat lines (main.cc:351-369; a turbulent
+      // grid adds the k-omega solve's iterations and residual -- one coupled
+      // solve here, so its iteration count is the flow's)
+      char line[256];
+      if (turb)
+        std::snprintf(line, sizeof(line), "%d\t%d\t%.3e\t%.3e\t%d\t%.3e\t%d\t%.3e\n", step, 1, time, max_cfl, ls.iters, res,
+                      ls.iters, rres);
+      else
+        std::snprintf(line, sizeof(line), "%d\t%d\t%.3e\t%.3e\t%d\t%.3e\n", step, 1, time, max_cfl, ls.iters, res);
+      std::fputs(line, conv);
       std::fflush(conv);
-      if (o->echo) std::printf("%d\t%d\t%.3e\t%.3e\t%d\t%.3e\n", step, 1, time, max_cfl, ls.iters, res);
+      if (o->echo) std::fputs(line, stdout);
       rep->steps = step - restart_step;
       // ---- restart and loads files
       if (step % restart_freq == 0 || last) save_restart(step);
@@ -2012,9 +2044,13 @@ int fcfd_run(fcfd_ctx *x, double *W, const fcfd_run_opts *o, fcfd_run_report *re
     rep->time = time;
     rep->res = res;
     rep->status = status;
-    k_soa_to_aos_nc<<<gc, tb, 0, s>>>(ns.Wn.p, x->Win.p, nc);
-    CK(cudaMemcpyAsync(W, x->Win.p, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
-    CK(cudaStreamSynchronize(s));
+    if (turb) {
+      kw_driver_state(x, kd.p, W, o->K, nullptr);
+    } else {
+      k_soa_to_aos_nc<<<gc, tb, 0, s>>>(ns.Wn.p, x->Win.p, nc);
+      CK(cudaMemcpyAsync(W, x->Win.p, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+      CK(cudaStreamSynchronize(s));
+    }
     if (o->echo) std::printf("[I] Wall time = %g second\n", rep->wall_seconds);
     return status;
   } catch (const Error &e) {

@@ -16,6 +16,8 @@
 #include <cstring>
 #include <vector>
 
+#include <memory>
+
 #include "ctx.hpp"
 
 namespace fcfd {
@@ -762,6 +764,262 @@ static void kw_tangent32(fcfd_ctx *x, const double *X, const double *z, double *
 
 using namespace fcfd::kwn;
 
+// One linearised backward-Euler solve of the coupled system at S.X (its
+// residual in S.F0, local time steps in S.dt): the flow rows' block inverses
+// and the k-omega diagonal at X, then GMRES(mdim), one cycle, on
+// wr (D/dt - J) M^-1 u = wr F0 stopped at |r| <= krtol |wr F0| or kabstol;
+// dX = M^-1 u into S.dX.  mode 0: J.v by an FP64 finite difference of the
+// coupled residual, else the FP32 coupled tangent.  Returns the Krylov
+// iterations.  Shared by the coupled Newton solve and the time-marching
+// driver of turbulent decks.
+static int kw_linear_step(fcfd_ctx *x, KwSolve &S, int mdim, int mode, double krtol, double kabstol, const Wt7 &wr,
+                          const Wt7 &iwr) {
+  const DevMesh &m = x->dm;
+  const int nc = m.nc, n = kNv * nc;
+  cudaStream_t s = x->stream;
+  const int gc = (nc + 255) / 256, gn = (n + 255) / 256;
+  auto norms = [&](const double *F, double out[kNv]) {
+    for (int v = 0; v < kNv; ++v) {
+      double d;
+      kw_dots(x, S, nc, 1, F + (size_t)v * nc, 0, F + (size_t)v * nc, &d);
+      out[v] = std::sqrt(d);
+    }
+  };
+  ns_block_inverse(x, S.X.p, S.vol.p, S.dt.p, x->rans->b.mutf.p, S.JL.p, S.JR.p, S.Minv.p, S.rowmag.p);
+  k_kw_diag<<<gc, 256, 0, s>>>(x->cs, m, S.X.p, S.vol.p, S.dt.p, x->mdot.p, x->rans->b.mutf.p, S.dk.p);
+  // GMRES(m), one cycle, on wr (D - J) M^-1 u = wr F0, dX = M^-1 u
+  // |S^-1 X| for the finite-difference step (S: the equations' scales)
+  double xn = 0.;
+  {
+    double d[kNv];
+    norms(S.X.p, d);
+    const double ref[kNv] = {std::fabs(x->cs.Pref) + d[0] / std::sqrt((double)nc), 0., 0., 0.,
+                             std::fabs(x->cs.Tref) + d[4] / std::sqrt((double)nc), d[5] / std::sqrt((double)nc),
+                             d[6] / std::sqrt((double)nc)};
+    double U = std::sqrt(d[1] * d[1] + d[2] * d[2] + d[3] * d[3]) / std::sqrt((double)nc);
+    for (int v = 0; v < kNv; ++v) {
+      const double r = (v >= 1 && v <= 3) ? U : ref[v];
+      if (r > 0.) xn += (d[v] / r) * (d[v] / r);
+    }
+    xn = std::sqrt(xn);
+  }
+  for (int v = 0; v < kNv; ++v)
+    k_kw_scale<<<gc, 256, 0, s>>>(nc, wr.s[v], S.F0.p + (size_t)v * nc, S.w.p + (size_t)v * nc);
+  double beta;
+  kw_dots(x, S, n, 1, S.w.p, 0, S.w.p, &beta);
+  beta = std::sqrt(beta);
+  int kit = 0;
+  std::vector<double> H((size_t)(mdim + 1) * mdim, 0.), g(mdim + 1, 0.), cs_(mdim), sn(mdim);
+  g[0] = beta;
+  if (beta > 0.) {
+    k_kw_scale<<<gn, 256, 0, s>>>(n, 1. / beta, S.w.p, S.Vb.p);
+    for (int j = 0; j < mdim; ++j) {
+      double *vj = S.Vb.p + (size_t)j * n;
+      // z = M^-1 v_j, then w = wr (D z - J z)
+      k_kw_prec<<<gc, 256, 0, s>>>(nc, S.Minv.p, S.dk.p, iwr, vj, S.z.p);
+      if (mode == 0) {
+        double zn;
+        kw_dots(x, S, n, 1, S.z.p, 0, S.z.p, &zn);
+        zn = std::sqrt(zn);
+        const double eps = zn > 0. ? 1.4901161193847656e-08 * (1. + xn) / zn : 1e-8;
+        kw_residual(x, S.X.p, S.z.p, eps, S.F1.p);
+        k_kw_matvec<<<gc, 256, 0, s>>>(x->cs, nc, S.X.p, S.vol.p, S.dt.p, S.z.p, S.F1.p, S.F0.p, 1. / eps, wr, S.w.p);
+      } else {
+        kw_tangent32(x, S.X.p, S.z.p, S.Jz.p);
+        k_kw_matvec<<<gc, 256, 0, s>>>(x->cs, nc, S.X.p, S.vol.p, S.dt.p, S.z.p, S.Jz.p, nullptr, 0., wr, S.w.p);
+      }
+      // classical Gram-Schmidt, twice
+      std::vector<double> hc(j + 1, 0.), hh(j + 1);
+      for (int pass = 0; pass < 2; ++pass) {
+        kw_dots(x, S, n, j + 1, S.Vb.p, (size_t)n, S.w.p, hh.data());
+        CK(cudaMemcpyAsync(S.h.p, hh.data(), sizeof(double) * (j + 1), cudaMemcpyHostToDevice, s));
+        k_kw_sub<<<gn, 256, 0, s>>>(n, j + 1, S.Vb.p, (size_t)n, S.h.p, S.w.p);
+        for (int i = 0; i <= j; ++i) hc[i] += hh[i];
+      }
+      double hn;
+      kw_dots(x, S, n, 1, S.w.p, 0, S.w.p, &hn);
+      hn = std::sqrt(hn);
+      for (int i = 0; i <= j; ++i) H[(size_t)i * mdim + j] = hc[i];
+      H[(size_t)(j + 1) * mdim + j] = hn;
+      if (hn > 0.) k_kw_scale<<<gn, 256, 0, s>>>(n, 1. / hn, S.w.p, S.Vb.p + (size_t)(j + 1) * n);
+      // Givens rotations of the new column
+      for (int i = 0; i < j; ++i) {
+        const double a = H[(size_t)i * mdim + j], b = H[(size_t)(i + 1) * mdim + j];
+        H[(size_t)i * mdim + j] = cs_[i] * a + sn[i] * b;
+        H[(size_t)(i + 1) * mdim + j] = -sn[i] * a + cs_[i] * b;
+      }
+      const double a = H[(size_t)j * mdim + j], b = H[(size_t)(j + 1) * mdim + j];
+      const double r = std::hypot(a, b);
+      cs_[j] = r > 0. ? a / r : 1.;
+      sn[j] = r > 0. ? b / r : 0.;
+      H[(size_t)j * mdim + j] = r;
+      H[(size_t)(j + 1) * mdim + j] = 0.;
+      g[j + 1] = -sn[j] * g[j];
+      g[j] = cs_[j] * g[j];
+      kit = j + 1;
+      if (std::fabs(g[j + 1]) <= krtol * beta || std::fabs(g[j + 1]) <= kabstol || hn == 0.) break;
+    }
+    // y = H^-1 g, u = V y, dX = M^-1 u
+    std::vector<double> y(kit, 0.);
+    for (int i = kit - 1; i >= 0; --i) {
+      double t = g[i];
+      for (int k = i + 1; k < kit; ++k) t -= H[(size_t)i * mdim + k] * y[k];
+      y[i] = t / H[(size_t)i * mdim + i];
+    }
+    CK(cudaMemcpyAsync(S.h.p, y.data(), sizeof(double) * kit, cudaMemcpyHostToDevice, s));
+    k_kw_combo<<<gn, 256, 0, s>>>(n, kit, S.Vb.p, (size_t)n, S.h.p, S.x.p);
+    k_kw_prec<<<gc, 256, 0, s>>>(nc, S.Minv.p, S.dk.p, iwr, S.x.p, S.dX.p);
+  } else {
+    CK(cudaMemsetAsync(S.dX.p, 0, sizeof(double) * n, s));
+  }
+  return kit;
+}
+
+namespace fcfd {
+
+// ---- the implicit step of the time-marching driver for turbulent decks
+// (fcfd_run): one coupled backward-Euler solve per time step on
+// X = (p,u,v,w,T,k,omega), where the reference solves the flow system and
+// then the k-omega system (ns.cc:104-118, rans.cc:85-98) -- the same steady
+// state, one linear solve instead of two.
+struct KwDriver {
+  KwSolve S;
+  Wt7 wr, iwr;
+  int mdim = 10;
+};
+
+// X += dX with the reference's k-omega update limits (rans.cc:214-220: k
+// kept in [klow, khigh], omega above omegalow), NaN/Inf updates flagged (err
+// bit 8), and per block the sums of dp^2, |dV|^2, dT^2, dk^2, domega^2 over
+// dt^2 (update_variables of both solvers, ns.cc:338-396, rans.cc:193-255)
+__global__ void k_kw_drive_update(int nc, double *__restrict__ X, const double *__restrict__ dX,
+                                  const double *__restrict__ dt, double klow, double khigh, double omlow,
+                                  double *__restrict__ part, int *__restrict__ err) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  double r[5] = {0., 0., 0., 0., 0.};
+  if (c < nc) {
+    double d[kNv];
+    bool bad = false;
+    for (int k = 0; k < kNv; ++k) {
+      d[k] = dX[(size_t)k * nc + c];
+      if (!isfinite(d[k])) bad = true;
+    }
+    if (bad) atomicOr(err, 8);
+    const double kk = X[(size_t)5 * nc + c], om = X[(size_t)6 * nc + c];
+    d[5] = fmax(-1. * (kk - klow), d[5]);
+    d[5] = fmin(khigh - kk, d[5]);
+    d[6] = fmax(-1. * (om - omlow), d[6]);
+    for (int k = 0; k < kNv; ++k) X[(size_t)k * nc + c] += d[k];
+    const double dt2 = dt[c] * dt[c];
+    r[0] = d[0] * d[0] / dt2;
+    r[1] = d[1] * d[1] / dt2 + d[2] * d[2] / dt2 + d[3] * d[3] / dt2;
+    r[2] = d[4] * d[4] / dt2;
+    r[3] = d[5] * d[5] / dt2;
+    r[4] = d[6] * d[6] / dt2;
+  }
+  __shared__ double sh[5][8];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for (int i = 0; i < 5; ++i) {
+    double t = r[i];
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+    if (lane == 0) sh[i][wid] = t;
+  }
+  __syncthreads();
+  if (threadIdx.x < 5) {
+    double t = 0.;
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) t += sh[threadIdx.x][k];
+    part[(size_t)blockIdx.x * 5 + threadIdx.x] = t;
+  }
+}
+
+void *kw_driver_create(fcfd_ctx *x, const double *W, const double *K, int mdim) {
+  if (!x->rans) throw Error(FCFD_ERR_INPUT, "the case has no turbulence model");
+  const DevMesh &m = x->dm;
+  const int nc = m.nc, n = kNv * nc;
+  cudaStream_t s = x->stream;
+  std::unique_ptr<KwDriver> d(new KwDriver());
+  d->mdim = mdim > 0 ? mdim : 10;
+  KwSolve &S = d->S;
+  S.X.alloc(n); S.Xsave.alloc(n); S.F0.alloc(n); S.F1.alloc(n); S.Jz.alloc(n); S.dt.alloc(nc); S.vol.alloc(nc);
+  S.Minv.alloc(25 * (size_t)nc); S.JL.alloc(25 * (size_t)m.nf); S.JR.alloc(25 * (size_t)m.nf);
+  S.rowmag.alloc(5 * (size_t)nc); S.dk.alloc(2 * (size_t)nc);
+  S.Vb.alloc((size_t)(d->mdim + 1) * n); S.w.alloc(n); S.z.alloc(n); S.part.alloc((size_t)kRedBlk * (d->mdim + 1));
+  S.h.alloc(d->mdim + 1); S.x.alloc(n); S.dX.alloc(n); S.key.alloc(2);
+  std::vector<double> hx((size_t)n);
+  for (int c = 0; c < nc; ++c) {
+    for (int v = 0; v < 5; ++v) hx[(size_t)v * nc + c] = W[5 * (size_t)c + v];
+    for (int v = 0; v < 2; ++v) hx[(size_t)(5 + v) * nc + c] = K[2 * (size_t)c + v];
+  }
+  CK(cudaMemcpyAsync(S.X.p, hx.data(), sizeof(double) * n, cudaMemcpyHostToDevice, s));
+  std::vector<double> vol(x->mesh->c_volume.begin(), x->mesh->c_volume.begin() + nc);
+  CK(cudaMemcpyAsync(S.vol.p, vol.data(), sizeof(double) * nc, cudaMemcpyHostToDevice, s));
+  CK(cudaStreamSynchronize(s));
+  return d.release();
+}
+
+void kw_driver_destroy(void *p) { delete static_cast<KwDriver *>(p); }
+
+// F0 = the coupled residual at X; it also loads X's flow state into the
+// residual pipeline (x->p64: the time step and loads read it).  The Krylov
+// equation weights are the inverse norms of this residual (momentum as
+// one), formed anew at every step so that a run continued from restart files
+// takes the same steps as an uninterrupted one.
+void kw_driver_residual(fcfd_ctx *x, void *p) {
+  KwDriver &d = *static_cast<KwDriver *>(p);
+  KwSolve &S = d.S;
+  const int nc = x->dm.nc;
+  kw_residual(x, S.X.p, nullptr, 0., S.F0.p);
+  check_err(x);
+  {
+    double r0[kNv];
+    for (int v = 0; v < kNv; ++v) {
+      double q;
+      kw_dots(x, S, nc, 1, S.F0.p + (size_t)v * nc, 0, S.F0.p + (size_t)v * nc, &q);
+      r0[v] = std::sqrt(q);
+    }
+    const double m0 = std::sqrt(r0[1] * r0[1] + r0[2] * r0[2] + r0[3] * r0[3]);
+    for (int v = 0; v < kNv; ++v) {
+      const double r = (v >= 1 && v <= 3) ? m0 : r0[v];
+      d.wr.s[v] = r > 0. ? 1. / r : 1.;
+      d.iwr.s[v] = 1. / d.wr.s[v];
+    }
+  }
+}
+
+// the implicit solve at X with local time steps dt (device, [nc]); dX in the driver state
+int kw_driver_step(fcfd_ctx *x, void *p, const double *dt, int mode, double krtol, double kabstol) {
+  KwDriver &d = *static_cast<KwDriver *>(p);
+  CK(cudaMemcpyAsync(d.S.dt.p, dt, sizeof(double) * x->dm.nc, cudaMemcpyDeviceToDevice, x->stream));
+  return kw_linear_step(x, d.S, d.mdim, mode, krtol, kabstol, d.wr, d.iwr);
+}
+
+// X += dX (limits as k_kw_drive_update); part: 5 partial sums per 256-cell block
+void kw_driver_update(fcfd_ctx *x, void *p, const double *dt, double *part, int *err) {
+  KwDriver &d = *static_cast<KwDriver *>(p);
+  const fcfd_case &cs = *x->case_ptr;
+  const int nc = x->dm.nc;
+  k_kw_drive_update<<<(nc + 255) / 256, 256, 0, x->stream>>>(nc, d.S.X.p, d.S.dX.p, dt, cs.k_low, cs.k_high, cs.omega_low,
+                                                               part, err);
+  CK(cudaGetLastError());
+}
+
+// host copies of the state: W[nc][5], K[nc][2] and (mut, may be null) the
+// cells' eddy viscosity of the last residual evaluation
+void kw_driver_state(fcfd_ctx *x, void *p, double *W, double *K, double *mut) {
+  KwDriver &d = *static_cast<KwDriver *>(p);
+  const int nc = x->dm.nc, n = kNv * nc;
+  std::vector<double> hx((size_t)n);
+  CK(cudaMemcpyAsync(hx.data(), d.S.X.p, sizeof(double) * n, cudaMemcpyDeviceToHost, x->stream));
+  if (mut) CK(cudaMemcpyAsync(mut, x->rans->b.mut.p, sizeof(double) * nc, cudaMemcpyDeviceToHost, x->stream));
+  CK(cudaStreamSynchronize(x->stream));
+  for (int c = 0; c < nc; ++c) {
+    for (int v = 0; v < 5; ++v) W[5 * (size_t)c + v] = hx[(size_t)v * nc + c];
+    for (int v = 0; v < 2; ++v) K[2 * (size_t)c + v] = hx[(size_t)(5 + v) * nc + c];
+  }
+}
+
+}  // namespace fcfd
+
 extern "C" int fcfd_rans_newton_solve(fcfd_ctx *x, double *W, double *K, const fcfd_newton_opts *o,
                                       fcfd_newton_report *rep) {
   try {
@@ -846,94 +1104,8 @@ extern "C" int fcfd_rans_newton_solve(fcfd_ctx *x, double *W, double *K, const f
       if (o->max_seconds > 0 && seconds() > o->max_seconds) break;
       // time step, preconditioner at X (the chain's state of F0 is current)
       k_local_dt<double><<<gc, 256, 0, s>>>(x->cs, m, x->p64.W.p, S.dt.p, cfl, nullptr);
-      ns_block_inverse(x, S.X.p, S.vol.p, S.dt.p, x->rans->b.mutf.p, S.JL.p, S.JR.p, S.Minv.p, S.rowmag.p);
-      k_kw_diag<<<gc, 256, 0, s>>>(x->cs, m, S.X.p, S.vol.p, S.dt.p, x->mdot.p, x->rans->b.mutf.p, S.dk.p);
       CK(cudaMemcpyAsync(S.Xsave.p, S.X.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
-      // GMRES(m), one cycle, on wr (D - J) M^-1 u = wr F0, dX = M^-1 u
-      // |S^-1 X| for the finite-difference step (S: the equations' scales)
-      double xn = 0.;
-      {
-        double d[kNv];
-        norms(S.X.p, d);
-        const double ref[kNv] = {std::fabs(x->cs.Pref) + d[0] / std::sqrt((double)nc), 0., 0., 0.,
-                                 std::fabs(x->cs.Tref) + d[4] / std::sqrt((double)nc), d[5] / std::sqrt((double)nc),
-                                 d[6] / std::sqrt((double)nc)};
-        double U = std::sqrt(d[1] * d[1] + d[2] * d[2] + d[3] * d[3]) / std::sqrt((double)nc);
-        for (int v = 0; v < kNv; ++v) {
-          const double r = (v >= 1 && v <= 3) ? U : ref[v];
-          if (r > 0.) xn += (d[v] / r) * (d[v] / r);
-        }
-        xn = std::sqrt(xn);
-      }
-      for (int v = 0; v < kNv; ++v)
-        k_kw_scale<<<gc, 256, 0, s>>>(nc, wr.s[v], S.F0.p + (size_t)v * nc, S.w.p + (size_t)v * nc);
-      double beta;
-      kw_dots(x, S, n, 1, S.w.p, 0, S.w.p, &beta);
-      beta = std::sqrt(beta);
-      int kit = 0;
-      std::vector<double> H((size_t)(mdim + 1) * mdim, 0.), g(mdim + 1, 0.), cs_(mdim), sn(mdim);
-      g[0] = beta;
-      if (beta > 0.) {
-        k_kw_scale<<<gn, 256, 0, s>>>(n, 1. / beta, S.w.p, S.Vb.p);
-        for (int j = 0; j < mdim; ++j) {
-          double *vj = S.Vb.p + (size_t)j * n;
-          // z = M^-1 v_j, then w = wr (D z - J z)
-          k_kw_prec<<<gc, 256, 0, s>>>(nc, S.Minv.p, S.dk.p, iwr, vj, S.z.p);
-          if (mode == 0) {
-            double zn;
-            kw_dots(x, S, n, 1, S.z.p, 0, S.z.p, &zn);
-            zn = std::sqrt(zn);
-            const double eps = zn > 0. ? 1.4901161193847656e-08 * (1. + xn) / zn : 1e-8;
-            kw_residual(x, S.X.p, S.z.p, eps, S.F1.p);
-            k_kw_matvec<<<gc, 256, 0, s>>>(x->cs, nc, S.X.p, S.vol.p, S.dt.p, S.z.p, S.F1.p, S.F0.p, 1. / eps, wr, S.w.p);
-          } else {
-            kw_tangent32(x, S.X.p, S.z.p, S.Jz.p);
-            k_kw_matvec<<<gc, 256, 0, s>>>(x->cs, nc, S.X.p, S.vol.p, S.dt.p, S.z.p, S.Jz.p, nullptr, 0., wr, S.w.p);
-          }
-          // classical Gram-Schmidt, twice
-          std::vector<double> hc(j + 1, 0.), hh(j + 1);
-          for (int pass = 0; pass < 2; ++pass) {
-            kw_dots(x, S, n, j + 1, S.Vb.p, (size_t)n, S.w.p, hh.data());
-            CK(cudaMemcpyAsync(S.h.p, hh.data(), sizeof(double) * (j + 1), cudaMemcpyHostToDevice, s));
-            k_kw_sub<<<gn, 256, 0, s>>>(n, j + 1, S.Vb.p, (size_t)n, S.h.p, S.w.p);
-            for (int i = 0; i <= j; ++i) hc[i] += hh[i];
-          }
-          double hn;
-          kw_dots(x, S, n, 1, S.w.p, 0, S.w.p, &hn);
-          hn = std::sqrt(hn);
-          for (int i = 0; i <= j; ++i) H[(size_t)i * mdim + j] = hc[i];
-          H[(size_t)(j + 1) * mdim + j] = hn;
-          if (hn > 0.) k_kw_scale<<<gn, 256, 0, s>>>(n, 1. / hn, S.w.p, S.Vb.p + (size_t)(j + 1) * n);
-          // Givens rotations of the new column
-          for (int i = 0; i < j; ++i) {
-            const double a = H[(size_t)i * mdim + j], b = H[(size_t)(i + 1) * mdim + j];
-            H[(size_t)i * mdim + j] = cs_[i] * a + sn[i] * b;
-            H[(size_t)(i + 1) * mdim + j] = -sn[i] * a + cs_[i] * b;
-          }
-          const double a = H[(size_t)j * mdim + j], b = H[(size_t)(j + 1) * mdim + j];
-          const double r = std::hypot(a, b);
-          cs_[j] = r > 0. ? a / r : 1.;
-          sn[j] = r > 0. ? b / r : 0.;
-          H[(size_t)j * mdim + j] = r;
-          H[(size_t)(j + 1) * mdim + j] = 0.;
-          g[j + 1] = -sn[j] * g[j];
-          g[j] = cs_[j] * g[j];
-          kit = j + 1;
-          if (std::fabs(g[j + 1]) <= krtol * beta || hn == 0.) break;
-        }
-        // y = H^-1 g, u = V y, dX = M^-1 u
-        std::vector<double> y(kit, 0.);
-        for (int i = kit - 1; i >= 0; --i) {
-          double t = g[i];
-          for (int k = i + 1; k < kit; ++k) t -= H[(size_t)i * mdim + k] * y[k];
-          y[i] = t / H[(size_t)i * mdim + i];
-        }
-        CK(cudaMemcpyAsync(S.h.p, y.data(), sizeof(double) * kit, cudaMemcpyHostToDevice, s));
-        k_kw_combo<<<gn, 256, 0, s>>>(n, kit, S.Vb.p, (size_t)n, S.h.p, S.x.p);
-        k_kw_prec<<<gc, 256, 0, s>>>(nc, S.Minv.p, S.dk.p, iwr, S.x.p, S.dX.p);
-      } else {
-        CK(cudaMemsetAsync(S.dX.p, 0, sizeof(double) * n, s));
-      }
+      const int kit = kw_linear_step(x, S, mdim, mode, krtol, 0., wr, iwr);
       rep->krylov_iterations += kit;
       // relaxation: |dp/p|, |dT/T| <= 0.2
       CK(cudaMemsetAsync(S.key.p, 0, 2 * sizeof(unsigned long long), s));

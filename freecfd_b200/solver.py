@@ -370,19 +370,25 @@ class NavierStokes:
         return W, K, rep
 
     def run(self, W, work_dir=".", restart_step=0, max_steps=0, jvp=False, fp32_krylov=False, precond_sweeps=0,
-            echo=False, raise_on_fail=True):
+            echo=False, raise_on_fail=True, K=None):
         """The deck's time loop (the reference's main program): per step the
         CFL schedule, one implicit backward-Euler step, convergence.dat,
         loads and restart files under ``work_dir``.  ``restart_step`` > 0
         starts from the restart files of that step (W is then only the
-        output buffer).  Returns (W_final, report dict)."""
+        output buffer).  Turbulent decks need ``K`` (k and omega per cell,
+        [nc][2]); each step is then one coupled solve on the flow and k-omega
+        variables.  Returns (W_final, report dict), with the final K under
+        ``"K"`` for turbulent decks."""
         W = np.array(W, dtype=np.float64, order="C", copy=True)
+        Kc = None if K is None else np.array(K, dtype=np.float64, order="C", copy=True)
         o = RunOpts(os.fsencode(str(work_dir)), int(restart_step), int(max_steps), 1 if jvp else 0,
-                    int(bool(fp32_krylov)), int(precond_sweeps), int(bool(echo)))
+                    int(bool(fp32_krylov)), int(precond_sweeps), int(bool(echo)), None if Kc is None else _d(Kc))
         r = RunReport()
         rc = lib.fcfd_run(self.h, _d(W), ctypes.byref(o), ctypes.byref(r))
         rep = dict(status=r.status, steps=r.steps, krylov_iterations=r.krylov_iterations, time=r.time, res=r.res,
                    wall_seconds=r.wall_seconds)
+        if Kc is not None:
+            rep["K"] = Kc
         if rc != 0 and raise_on_fail:
             raise FcfdError(rc, lib.fcfd_last_error().decode() + f" after {r.steps} steps")
         return W, rep

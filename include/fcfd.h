@@ -399,6 +399,11 @@ typedef struct fcfd_run_opts {
   int32_t fp32_krylov;    /* as in fcfd_newton_opts */
   int32_t precond_sweeps; /* as in fcfd_newton_opts */
   int32_t echo;           /* 1: also print the reference's screen lines to stdout */
+  double *K;              /* turbulent decks: k and omega per cell [nc][2], in/out (required); the
+                             time step is then one coupled implicit solve on (p,u,v,w,T,k,omega)
+                             where the reference solves the flow and then the k-omega system
+                             (ns.cc:104-118, rans.cc:85-98); convergence.dat adds the k-omega
+                             iterations and residual (main.cc:351-361), restart files k, omega, mu_t */
 } fcfd_run_opts;
 
 typedef struct fcfd_run_report {
