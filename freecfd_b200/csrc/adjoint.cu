@@ -32,11 +32,13 @@
 // gathered per cell in face order, the outlet faces' stale-density adjoints are
 // summed per target face in outlet order, and the global extrema's adjoints go
 // through per-block partial sums added by one block.
+#include <algorithm>
 #include <cmath>
 #include <vector>
 
 #include "ctx.hpp"
 #include "dn.cuh"
+#include "kw.cuh"
 
 namespace fcfd {
 
@@ -47,8 +49,8 @@ namespace {
 constexpr int kLanes = 4;
 typedef DN<kLanes> DA;
 
-// local face inputs
-enum { U_QL = 0, U_CL = 5, U_QR = 10, U_CR = 15, U_STALE = 20, U_GPA = 21, U_GNB = 33, U_N = 45 };
+// local face inputs (U_MUT: the face eddy viscosity of a turbulent case)
+enum { U_QL = 0, U_CL = 5, U_QR = 10, U_CR = 15, U_STALE = 20, U_GPA = 21, U_GNB = 33, U_MUT = 45, U_N = 46 };
 
 // seeded view of a face's local inputs for one pass: input i carries lane l
 // when chunk[l] == i
@@ -69,6 +71,13 @@ struct SeedGrad {
   __device__ __forceinline__ DA at_pa(int i) const { return (*s)(U_GPA + i); }
   __device__ __forceinline__ DA at_nb(int i) const { return (*s)(U_GNB + i); }
 };
+// the face eddy viscosity as face_D reads it (mu_t[f]); off for laminar cases
+struct SeedMut {
+  DA v;
+  bool on;
+  __device__ __forceinline__ DA operator[](int) const { return v; }
+  __device__ __forceinline__ explicit operator bool() const { return on; }
+};
 
 template <class F>
 __device__ __forceinline__ void state_from(const DevCase &cs, FState<DA> &s, const F &in, int q, int cc, const double n[3]) {
@@ -78,11 +87,12 @@ __device__ __forceinline__ void state_from(const DevCase &cs, FState<DA> &s, con
   finish(cs, s, n);
 }
 
-// D_f and the right density of face f from its local inputs (the same
-// sequence as face_states + face_D).
+// D_f, the left weight and the right density of face f from its local
+// inputs (the same sequence as face_states + face_D); turb: the face eddy
+// viscosity is an input.
 template <bool VISCOUS, int FX>
 __device__ void face_from_inputs(const DevCase &cs, const DevMesh &m, int f, const double n[3], double A, int b, int pa,
-                                 int nb, const Seeds &in, DA D[5], DA &rhoR) {
+                                 int nb, bool turb, const Seeds &in, DA D[5], DA &wL, DA &rhoR) {
   FState<DA> L, R;
   state_from(cs, L, in, U_QL, U_CL, n);
   if (b < 0) {
@@ -94,14 +104,14 @@ __device__ void face_from_inputs(const DevCase &cs, const DevMesh &m, int f, con
     finish(cs, R, n);
   }
   rhoR = R.rho;
-  DA wL;
   const SeedGrad gs{&in};
-  face_D<DA, SeedGrad, VISCOUS, FX>(cs, m, f, n, A, b, pa, nb, L, R, gs, (const DA *)nullptr, D, wL);
+  const SeedMut mt{turb ? in(U_MUT) : DA(0.), turb};
+  face_D<DA, SeedGrad, VISCOUS, FX, SeedMut>(cs, m, f, n, A, b, pa, nb, L, R, gs, mt, D, wL);
 }
 
 // Forward values of face f's local inputs.
 __device__ void face_inputs(const DevMesh &m, int f, int b, int pa, int nb, const double *W, const double *G,
-                            const double *Lm, const double *stale, double u[U_N]) {
+                            const double *Lm, const double *stale, const double *mutf, double u[U_N]) {
   const int nt = m.nt, nc = m.nc, nf = m.nf;
   const double xf[3] = {m.f_x[f], m.f_x[nf + f], m.f_x[2 * nf + f]};
   for (int i = 0; i < U_N; ++i) u[i] = 0.;
@@ -120,11 +130,12 @@ __device__ void face_inputs(const DevMesh &m, int f, int b, int pa, int nb, cons
   for (int i = 0; i < 12; ++i) u[U_GPA + i] = G[(3 + i) * nc + pa];
   if (b < 0)
     for (int i = 0; i < 12; ++i) u[U_GNB + i] = G[(3 + i) * nc + nb];
+  if (mutf) u[U_MUT] = mutf[f];
 }
 
 // Inputs that can influence D_f (or the right density) for this face.
 template <bool VISCOUS>
-__device__ int active_inputs(const DevCase &cs, int b, int act[U_N]) {
+__device__ int active_inputs(const DevCase &cs, int b, bool turb, int act[U_N]) {
   int na = 0;
   for (int i = 0; i < 5; ++i) act[na++] = U_QL + i;
   if (b < 0) for (int i = 0; i < 5; ++i) act[na++] = U_QR + i;
@@ -134,6 +145,7 @@ __device__ int active_inputs(const DevCase &cs, int b, int act[U_N]) {
   if (VISCOUS) {
     for (int i = 0; i < 12; ++i) act[na++] = U_GPA + i;
     if (b < 0) for (int i = 0; i < 12; ++i) act[na++] = U_GNB + i;
+    if (turb) act[na++] = U_MUT;
   }
   return na;
 }
@@ -157,41 +169,49 @@ __global__ void k_wlim_gather(DevMesh m, const double *__restrict__ Wface, doubl
   Wlim[(size_t)v * m.nt + c] = acc;
 }
 
-// Face stage: FA[i][f] = sum_v Dbar_v dD_v/du_i.
+// Face stage: FA[i][f] = sum_v Dbar_v dD_v/du_i (+ wLbar dwL/du_i).  A
+// turbulent case adds the face eddy viscosity mutf as an input and seeds,
+// from the k-omega faces, the adjoints of the face's mass flux mdot = -D_0/A
+// (mdotb) and left weight (wlb).
 template <bool VISCOUS, int FX>
 __global__ void __launch_bounds__(128) k_face_adj(DevCase cs, DevMesh m, const double *__restrict__ W,
                                                   const double *__restrict__ G, const double *__restrict__ Lm,
                                                   const double *__restrict__ stale, const double *__restrict__ Rbar,
                                                   unsigned int load_mask, double dir0, double dir1, double dir2,
-                                                  double *__restrict__ FA) {
+                                                  const double *__restrict__ mutf, const double *__restrict__ mdotb,
+                                                  const double *__restrict__ wlb, double *__restrict__ FA) {
   const int f = blockIdx.x * blockDim.x + threadIdx.x;
   const int nf = m.nf, nc = m.nc;
   if (f >= nf) return;
   const int pa = m.f_parent[f], nb = m.f_neighbor[f], b = m.f_bc[f];
+  const double A = m.f_area[f];
   double Db[5] = {0., 0., 0., 0., 0.};
   if (Rbar) {
     for (int v = 0; v < 5; ++v) Db[v] = Rbar[v * nc + pa] - (b < 0 ? Rbar[v * nc + nb] : 0.);
   }
   if (b >= 0 && ((load_mask >> b) & 1u)) { Db[1] -= dir0; Db[2] -= dir1; Db[3] -= dir2; }
+  if (mdotb) Db[0] -= mdotb[f] / A;
+  const double wb = wlb ? wlb[f] : 0.;
+  const bool turb = mutf != nullptr;
   double ub[U_N];
   for (int i = 0; i < U_N; ++i) ub[i] = 0.;
-  if (Db[0] != 0. || Db[1] != 0. || Db[2] != 0. || Db[3] != 0. || Db[4] != 0.) {
+  if (Db[0] != 0. || Db[1] != 0. || Db[2] != 0. || Db[3] != 0. || Db[4] != 0. || wb != 0.) {
     const double n[3] = {m.f_n[f], m.f_n[nf + f], m.f_n[2 * nf + f]};
-    const double A = m.f_area[f];
     double u[U_N];
-    face_inputs(m, f, b, pa, nb, W, G, Lm, stale, u);
+    face_inputs(m, f, b, pa, nb, W, G, Lm, stale, mutf, u);
     int act[U_N];
-    const int na = active_inputs<VISCOUS>(cs, b, act);
+    const int na = active_inputs<VISCOUS>(cs, b, turb, act);
     for (int k0 = 0; k0 < na; k0 += kLanes) {
       Seeds in;
       in.u = u;
       for (int l = 0; l < kLanes; ++l) in.chunk[l] = (k0 + l < na) ? act[k0 + l] : -1;
-      DA D[5], rhoR;
-      face_from_inputs<VISCOUS, FX>(cs, m, f, n, A, b, pa, nb, in, D, rhoR);
+      DA D[5], wL, rhoR;
+      face_from_inputs<VISCOUS, FX>(cs, m, f, n, A, b, pa, nb, turb, in, D, wL, rhoR);
       for (int l = 0; l < kLanes; ++l) {
         if (in.chunk[l] < 0) continue;
         double s = 0.;
         for (int v = 0; v < 5; ++v) s += Db[v] * D[v].d[l];
+        if (wb != 0.) s += wb * wL.d[l];
         ub[in.chunk[l]] = s;
       }
     }
@@ -203,8 +223,8 @@ __global__ void __launch_bounds__(128) k_face_adj(DevCase cs, DevMesh m, const d
 // earlier face (cached_right_rho) hands that adjoint to the earlier face.
 template <bool VISCOUS, int FX>
 __global__ void k_stale_adj(DevCase cs, DevMesh m, const double *__restrict__ W, const double *__restrict__ G,
-                            const double *__restrict__ Lm, const double *__restrict__ stale, const double *__restrict__ FA,
-                            double *__restrict__ SC, int *__restrict__ tgt) {
+                            const double *__restrict__ Lm, const double *__restrict__ stale, const double *__restrict__ mutf,
+                            const double *__restrict__ FA, double *__restrict__ SC, int *__restrict__ tgt) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= m.n_outlet) return;
   const int nf = m.nf;
@@ -230,15 +250,16 @@ __global__ void k_stale_adj(DevCase cs, DevMesh m, const double *__restrict__ W,
     tgt[i] = g;
     if (sb == 0.) return;
     double u[U_N];
-    face_inputs(m, g, b, pa, nb, W, G, Lm, stale, u);
+    face_inputs(m, g, b, pa, nb, W, G, Lm, stale, mutf, u);
     int act[U_N];
-    const int na = active_inputs<VISCOUS>(cs, b, act);
+    // the right density does not depend on the eddy viscosity
+    const int na = active_inputs<VISCOUS>(cs, b, false, act);
     for (int k0 = 0; k0 < na; k0 += kLanes) {
       Seeds in;
       in.u = u;
       for (int l = 0; l < kLanes; ++l) in.chunk[l] = (k0 + l < na) ? act[k0 + l] : -1;
-      DA D[5], rhoR;
-      face_from_inputs<VISCOUS, FX>(cs, m, g, n, A, b, pa, nb, in, D, rhoR);
+      DA D[5], wL, rhoR;
+      face_from_inputs<VISCOUS, FX>(cs, m, g, n, A, b, pa, nb, mutf != nullptr, in, D, wL, rhoR);
       for (int l = 0; l < kLanes; ++l)
         if (in.chunk[l] >= 0) SC[(size_t)in.chunk[l] * m.n_outlet + i] = sb * rhoR.d[l];
     }
@@ -524,13 +545,16 @@ __global__ void k_e2_adj(DevCase cs, DevMesh m, const double *__restrict__ W, co
 }
 
 // Gradient stage: Wgrad_k = sum over cells c whose stencil holds k of
-// w_ck . Gbar_c (transposed stencil, ascending c).
+// w_ck . Gbar_c (transposed stencil, ascending c), for NV variables (the
+// flow's 5, or k and omega).
+template <int NV>
 __global__ void k_grad_adj(DevMesh m, const int *__restrict__ tr_index, const int *__restrict__ tr_cell,
                            const int *__restrict__ tr_entry, const double *__restrict__ Gb, double *__restrict__ Wgrad) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   const int nc = m.nc, nt = m.nt;
   if (k >= nt) return;
-  double acc[5] = {0., 0., 0., 0., 0.};
+  double acc[NV];
+  for (int v = 0; v < NV; ++v) acc[v] = 0.;
   const double xk[3] = {m.c_x[k], m.c_x[nt + k], m.c_x[2 * nt + k]};
   for (int j = tr_index[k]; j < tr_index[k + 1]; ++j) {
     const int c = tr_cell[j];
@@ -550,16 +574,19 @@ __global__ void k_grad_adj(DevMesh m, const int *__restrict__ tr_index, const in
       wt[1] = w * (d0 * C01 + d1 * C11 + d2 * C12);
       wt[2] = w * (d0 * C02 + d1 * C12 + d2 * C22);
     }
-    for (int v = 0; v < 5; ++v)
+    for (int v = 0; v < NV; ++v)
       acc[v] += wt[0] * Gb[(3 * v) * nc + c] + wt[1] * Gb[(3 * v + 1) * nc + c] + wt[2] * Gb[(3 * v + 2) * nc + c];
   }
-  for (int v = 0; v < 5; ++v) Wgrad[(size_t)v * nt + k] = acc[v];
+  for (int v = 0; v < NV; ++v) Wgrad[(size_t)v * nt + k] = acc[v];
 }
 
 // Ghost stage: ghost t (boundary face bface[t]) is the first-order BC state
 // of its parent; GA[.][t] = (d ghost / d W_parent)^T gbar.
+// Wx ([5][nb], may be null): further adjoints of the ghost states (the
+// k-omega terms of a turbulent case).
 __global__ void k_ghost_adj(DevCase cs, DevMesh m, const double *__restrict__ W, const double *__restrict__ FA,
-                            const double *__restrict__ Wgrad, const double *__restrict__ Wlim, double *__restrict__ GA) {
+                            const double *__restrict__ Wgrad, const double *__restrict__ Wlim,
+                            const double *__restrict__ Wx, double *__restrict__ GA) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= m.nb) return;
   const int nt = m.nt, nf = m.nf, nc = m.nc;
@@ -568,6 +595,7 @@ __global__ void k_ghost_adj(DevCase cs, DevMesh m, const double *__restrict__ W,
   bool any = false;
   for (int v = 0; v < 5; ++v) {
     gbar[v] = FA[(size_t)(U_CR + v) * nf + f] + Wgrad[(size_t)v * nt + g] + Wlim[(size_t)v * nt + g];
+    if (Wx) gbar[v] += Wx[(size_t)v * m.nb + t];
     any = any || gbar[v] != 0.;
   }
   double out[5] = {0., 0., 0., 0., 0.};
@@ -648,8 +676,194 @@ __global__ void k_rearm(unsigned long long *ext, int *argx) {
   }
 }
 
+// ---- k-omega stages of a turbulent case (reverse of the k-omega half of
+// the coupled evaluation: eddy viscosity, its face values, the k / omega
+// gradients, face fluxes, gather and sources; kw.cuh).
+
+// local inputs of a k-omega face flux (kw_face_flux)
+enum { KW_TPA = 0, KW_TNB = 1, KW_KL = 2, KW_OL = 3, KW_KR = 4, KW_OR = 5, KW_GPA = 6, KW_GNB = 12, KW_MUTF = 18, KW_MDOT = 19,
+       KW_WL = 20, KW_N = 21 };
+
+// Face stage: RFA[i][f] = sum_v DKbar_v dDK_v/du_i with DKbar from RKbar by
+// the gather's transpose (+ for the parent, - for the neighbour).
+__global__ void __launch_bounds__(128) k_kw_face_adj(DevCase cs, DevMesh m, const double *__restrict__ W,
+                                                     const double *__restrict__ K, const double *__restrict__ GK,
+                                                     const double *__restrict__ mutf, const double *__restrict__ mdot,
+                                                     const double *__restrict__ wl, const double *__restrict__ RKb,
+                                                     double *__restrict__ RFA) {
+  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nf = m.nf, nc = m.nc, nt = m.nt;
+  if (f >= nf) return;
+  const int pa = m.f_parent[f], nb = m.f_neighbor[f], b = m.f_bc[f];
+  const double db0 = RKb[pa] - (b < 0 ? RKb[nb] : 0.), db1 = RKb[nc + pa] - (b < 0 ? RKb[nc + nb] : 0.);
+  double ub[KW_N];
+  for (int i = 0; i < KW_N; ++i) ub[i] = 0.;
+  if (db0 != 0. || db1 != 0.) {
+    double u[KW_N];
+    u[KW_TPA] = W[4 * nt + pa]; u[KW_TNB] = W[4 * nt + nb];
+    u[KW_KL] = K[pa]; u[KW_OL] = K[nt + pa]; u[KW_KR] = K[nb]; u[KW_OR] = K[nt + nb];
+    for (int i = 0; i < 6; ++i) {
+      u[KW_GPA + i] = GK[i * nc + pa];
+      u[KW_GNB + i] = b < 0 ? GK[i * nc + nb] : 0.;
+    }
+    u[KW_MUTF] = mutf[f]; u[KW_MDOT] = mdot[f]; u[KW_WL] = wl[f];
+    int act[KW_N], na = 0;
+    const bool tfix = b >= 0 && cs.bc[b].T_fixed;
+    for (int i = 0; i < KW_N; ++i) {
+      if (tfix && (i == KW_TPA || i == KW_TNB)) continue;
+      if (b >= 0 && i >= KW_GNB && i < KW_GNB + 6) continue;
+      act[na++] = i;
+    }
+    for (int k0 = 0; k0 < na; k0 += kLanes) {
+      Seeds in;
+      in.u = u;
+      for (int l = 0; l < kLanes; ++l) in.chunk[l] = (k0 + l < na) ? act[k0 + l] : -1;
+      DA gpa[6], gnb[6];
+      for (int i = 0; i < 6; ++i) { gpa[i] = in(KW_GPA + i); gnb[i] = in(KW_GNB + i); }
+      DA d0, d1;
+      kw_face_flux<DA>(cs, m, f, b, pa, nb, in(KW_TPA), in(KW_TNB), in(KW_KL), in(KW_OL), in(KW_KR), in(KW_OR), gpa, gnb,
+                       in(KW_MUTF), in(KW_MDOT), in(KW_WL), d0, d1);
+      for (int l = 0; l < kLanes; ++l)
+        if (in.chunk[l] >= 0) ub[in.chunk[l]] = db0 * d0.d[l] + db1 * d1.d[l];
+    }
+  }
+  for (int i = 0; i < KW_N; ++i) RFA[(size_t)i * nf + f] = ub[i];
+}
+
+// (p, T, k, omega) adjoints of mu_t = kw_mut(p, T, k, omega), scaled by mb
+__device__ __forceinline__ void kw_mut_adj(const DevCase &cs, double p, double T, double k, double om, double ratio,
+                                           double mb, double out[4]) {
+  typedef DN<4> D4;
+  D4 a(p), t(T), kk(k), o(om);
+  a.d[0] = 1.; t.d[1] = 1.; kk.d[2] = 1.; o.d[3] = 1.;
+  const D4 r = kw_mut<D4>(cs, a, t, kk, o, ratio);
+  for (int i = 0; i < 4; ++i) out[i] = mb * r.d[i];
+}
+
+// Cell stage: per cell, the k-omega faces' adjoints of its T, k, omega and
+// k / omega gradient (its side of each face, ascending face order), the face
+// eddy viscosities' adjoints (the face value is the weighted average of the
+// two cells' unless the BC fixes it), the sources' adjoints (velocity
+// gradient rows into Gb, p and T into Wcell) and the cell eddy viscosity's
+// (into p, T, k, omega).  Kcell: k, omega adjoints ([2][nc]); GKb: the k /
+// omega gradients' ([6][nc]).
+__global__ void __launch_bounds__(128) k_kw_cell_adj(DevCase cs, DevMesh m, const double *__restrict__ W,
+                                                     const double *__restrict__ K, const double *__restrict__ G,
+                                                     const double *__restrict__ mut, const double *__restrict__ vol,
+                                                     const double *__restrict__ RKb, const double *__restrict__ RFA,
+                                                     const double *__restrict__ FA, double ratio,
+                                                     double *__restrict__ Wcell, double *__restrict__ Gb,
+                                                     double *__restrict__ Kcell, double *__restrict__ GKb) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nc = m.nc, nt = m.nt, nf = m.nf;
+  if (c >= nc) return;
+  double pb = 0., tb = 0., kb[2] = {0., 0.}, gkb[6] = {0., 0., 0., 0., 0., 0.}, mb = 0.;
+  for (int j = m.cf_index[c]; j < m.cf_index[c + 1]; ++j) {
+    const int e = m.cf_list[j];
+    const bool parent = e >= 0;
+    const int f = parent ? e : ~e;
+    tb += RFA[(size_t)(parent ? KW_TPA : KW_TNB) * nf + f];
+    kb[0] += RFA[(size_t)(parent ? KW_KL : KW_KR) * nf + f];
+    kb[1] += RFA[(size_t)(parent ? KW_OL : KW_OR) * nf + f];
+    for (int i = 0; i < 6; ++i) gkb[i] += RFA[(size_t)((parent ? KW_GPA : KW_GNB) + i) * nf + f];
+    const int b = m.f_bc[f];
+    if (!(b >= 0 && cs.bc[b].mut_fixed))
+      mb += (parent ? m.f_w[f] : m.f_w[nf + f]) * (RFA[(size_t)KW_MUTF * nf + f] + FA[(size_t)U_MUT * nf + f]);
+  }
+  // sources: inputs g9 (0..8), p, T, k, omega, mu_t (9..13)
+  const double sb0 = RKb[c] * vol[c], sb1 = RKb[nc + c] * vol[c];
+  double sbar[14];
+  for (int i = 0; i < 14; ++i) sbar[i] = 0.;
+  if (sb0 != 0. || sb1 != 0.) {
+    double u[14];
+    for (int i = 0; i < 9; ++i) u[i] = G[(3 + i) * nc + c];
+    u[9] = W[c]; u[10] = W[4 * nt + c]; u[11] = K[c]; u[12] = K[nt + c]; u[13] = mut[c];
+    for (int k0 = 0; k0 < 14; k0 += kLanes) {
+      Seeds in;
+      in.u = u;
+      for (int l = 0; l < kLanes; ++l) in.chunk[l] = (k0 + l < 14) ? k0 + l : -1;
+      DA g9[9];
+      for (int i = 0; i < 9; ++i) g9[i] = in(i);
+      DA s0, s1;
+      kw_source<DA>(cs, g9, in(9), in(10), in(11), in(12), in(13), s0, s1);
+      for (int l = 0; l < kLanes; ++l)
+        if (in.chunk[l] >= 0) sbar[in.chunk[l]] = sb0 * s0.d[l] + sb1 * s1.d[l];
+    }
+  }
+  pb += sbar[9]; tb += sbar[10]; kb[0] += sbar[11]; kb[1] += sbar[12]; mb += sbar[13];
+  if (mb != 0.) {
+    double a[4];
+    kw_mut_adj(cs, W[c], W[4 * nt + c], K[c], K[nt + c], ratio, mb, a);
+    pb += a[0]; tb += a[1]; kb[0] += a[2]; kb[1] += a[3];
+  }
+  for (int i = 0; i < 9; ++i) Gb[(size_t)(3 + i) * nc + c] += sbar[i];
+  Wcell[c] += pb;
+  Wcell[(size_t)4 * nc + c] += tb;
+  Kcell[c] = kb[0];
+  Kcell[nc + c] = kb[1];
+  for (int i = 0; i < 6; ++i) GKb[(size_t)i * nc + c] = gkb[i];
+}
+
+// Ghost stage: ghost t's T, k, omega adjoints from its boundary face's
+// k-omega flux and the k / omega gradients' stencils (Kgrad), and its eddy
+// viscosity's (the face value's neighbour weight, unless the BC fixes it).
+// Wx: the ghost's p, T adjoints for the flow's ghost stage ([5][nb]); KGA:
+// the ghost's k, omega adjoints for its parent ([2][nb]; zero where the BC
+// fixes k and omega).
+__global__ void k_kw_ghost_adj(DevCase cs, DevMesh m, const double *__restrict__ W, const double *__restrict__ K,
+                               const double *__restrict__ RFA, const double *__restrict__ FA,
+                               const double *__restrict__ Kgrad, double ratio, double *__restrict__ Wx,
+                               double *__restrict__ KGA) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nb = m.nb, nc = m.nc, nt = m.nt, nf = m.nf;
+  if (t >= nb) return;
+  const int f = m.bface[t], b = m.f_bc[f], g = nc + t;
+  double tb = RFA[(size_t)KW_TNB * nf + f], pb = 0.;
+  double kb0 = RFA[(size_t)KW_KR * nf + f] + Kgrad[g], kb1 = RFA[(size_t)KW_OR * nf + f] + Kgrad[nt + g];
+  const double mb = cs.bc[b].mut_fixed ? 0. : m.f_w[nf + f] * (RFA[(size_t)KW_MUTF * nf + f] + FA[(size_t)U_MUT * nf + f]);
+  if (mb != 0.) {
+    double a[4];
+    kw_mut_adj(cs, W[g], W[4 * nt + g], K[g], K[nt + g], ratio, mb, a);
+    pb += a[0]; tb += a[1]; kb0 += a[2]; kb1 += a[3];
+  }
+  for (int v = 0; v < 5; ++v) Wx[(size_t)v * nb + t] = v == 0 ? pb : (v == 4 ? tb : 0.);
+  const bool fixed = cs.bc[b].kw_fixed;
+  KGA[t] = fixed ? 0. : kb0;
+  KGA[nb + t] = fixed ? 0. : kb1;
+}
+
+// Kbar per cell (AoS [nc][2]): its own terms, its k / omega stencil terms
+// and its ghosts' (boundary faces in ascending order).
+__global__ void k_kw_final_adj(DevMesh m, const double *__restrict__ Kcell, const double *__restrict__ Kgrad,
+                               const double *__restrict__ KGA, double *__restrict__ out) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nc = m.nc, nt = m.nt;
+  if (c >= nc) return;
+  double r[2] = {Kcell[c] + Kgrad[c], Kcell[nc + c] + Kgrad[nt + c]};
+  for (int j = m.cf_index[c]; j < m.cf_index[c + 1]; ++j) {
+    const int e = m.cf_list[j];
+    if (e < 0 || m.f_bc[e] < 0) continue;
+    const int t = m.f_neighbor[e] - nc;
+    r[0] += KGA[t];
+    r[1] += KGA[m.nb + t];
+  }
+  out[2 * c] = r[0];
+  out[2 * c + 1] = r[1];
+}
+
+// k-omega staging (SoA [2][nc]) of a turbulent case's RKbar
+__global__ void k_aos2_to_soa(const double *__restrict__ in, double *__restrict__ out, int nc) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nc) return;
+  out[c] = in[2 * c];
+  out[nc + c] = in[2 * c + 1];
+}
+
 struct AdjBufs {
   DBuf<double> FA, Wcell, Gb, Wlim, Wgrad, GA, e2part, Rb, out;
+  // turbulent cases: k-omega face adjoints, cell / gradient / ghost terms, staging
+  DBuf<double> RFA, Kcell, GKb, Kgrad, Wx, KGA, RKb, Kin, Kout;
+  bool kw_ready = false;
   DBuf<double> Wface, SC;  // per-face-side limiter contributions; outlet faces' stale-density adjoints
   DBuf<int> tr_index, tr_cell, tr_entry, tgt;
   bool ready = false;
@@ -704,9 +918,32 @@ static AdjBufs &adj_bufs(fcfd_ctx *x) {
   return a;
 }
 
+static void kw_adj_bufs(fcfd_ctx *x, AdjBufs &a) {
+  if (a.kw_ready) return;
+  const DevMesh &m = x->dm;
+  const int nc = m.nc, nt = m.nt, nb = std::max(m.nb, 1);
+  a.RFA.alloc((size_t)KW_N * m.nf);
+  a.Kcell.alloc(2 * (size_t)nc); a.GKb.alloc(6 * (size_t)nc); a.Kgrad.alloc(2 * (size_t)nt);
+  a.Wx.alloc(5 * (size_t)nb); a.KGA.alloc(2 * (size_t)nb);
+  a.RKb.alloc(2 * (size_t)nc); a.Kin.alloc(2 * (size_t)nc); a.Kout.alloc(2 * (size_t)nc);
+  a.kw_ready = true;
+}
+
+// The k-omega half of a turbulent case's reverse sweep: the forward
+// evaluation's arrays, the seed RKbar (SoA [2][nc]) and the output Kbar (AoS
+// [nc][2], device).
+struct KwAdj {
+  RansFwd fw;
+  const double *RKb;
+  double *Kout;
+};
+
 // Reverse sweep for seed Rbar (SoA [5][nc], may be null) and/or the load
 // seed (mask, dir); the forward state must already be in x->p64.W (interior).
-static void run_adjoint(fcfd_ctx *x, const double *Rbar_soa, unsigned int mask, const double dir[3], double *out, bool aos) {
+// kw: a turbulent case's k-omega seed and output (the forward evaluation of
+// rans_eval_for_adjoint already run), else null.
+static void run_adjoint(fcfd_ctx *x, const double *Rbar_soa, unsigned int mask, const double dir[3], double *out, bool aos,
+                        const KwAdj *kw = nullptr) {
   const DevMesh &m = x->dm;
   cudaStream_t s = x->stream;
   const int tb = 256;
@@ -722,16 +959,25 @@ static void run_adjoint(fcfd_ctx *x, const double *Rbar_soa, unsigned int mask, 
     k_outlet_rho<double><<<(m.n_outlet + 127) / 128, 128, 0, s>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p);
   // reverse
   const int gf = (m.nf + 127) / 128, gc = (m.nc + 127) / 128;
+  const double *mutf = nullptr, *mdotb = nullptr, *wlb = nullptr;
+  if (kw) {
+    // k-omega faces first: their mdot and weightL adjoints seed the flow's faces
+    k_kw_face_adj<<<gf, 128, 0, s>>>(x->cs, m, P.W.p, kw->fw.K, kw->fw.GK, kw->fw.mutf, kw->fw.mdot, kw->fw.wl, kw->RKb,
+                                     a.RFA.p);
+    mutf = kw->fw.mutf;
+    mdotb = a.RFA.p + (size_t)KW_MDOT * m.nf;
+    wlb = a.RFA.p + (size_t)KW_WL * m.nf;
+  }
   if (x->viscous)
-    FCFD_BY_FLUX(x->cs.flux, k_face_adj<true, FX><<<gf, 128, 0, s>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p, Rbar_soa, mask, dir[0], dir[1], dir[2], a.FA.p));
+    FCFD_BY_FLUX(x->cs.flux, k_face_adj<true, FX><<<gf, 128, 0, s>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p, Rbar_soa, mask, dir[0], dir[1], dir[2], mutf, mdotb, wlb, a.FA.p));
   else
-    FCFD_BY_FLUX(x->cs.flux, k_face_adj<false, FX><<<gf, 128, 0, s>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p, Rbar_soa, mask, dir[0], dir[1], dir[2], a.FA.p));
+    FCFD_BY_FLUX(x->cs.flux, k_face_adj<false, FX><<<gf, 128, 0, s>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p, Rbar_soa, mask, dir[0], dir[1], dir[2], mutf, mdotb, wlb, a.FA.p));
   if (m.n_outlet > 0) {
     const int go = (m.n_outlet + 127) / 128;
     CK(cudaMemsetAsync(a.SC.p, 0, sizeof(double) * U_N * (size_t)m.n_outlet, s));
     CK(cudaMemsetAsync(a.tgt.p, 0xFF, sizeof(int) * (size_t)m.n_outlet, s));
-    if (x->viscous) FCFD_BY_FLUX(x->cs.flux, k_stale_adj<true, FX><<<go, 128, 0, s>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p, a.FA.p, a.SC.p, a.tgt.p));
-    else FCFD_BY_FLUX(x->cs.flux, k_stale_adj<false, FX><<<go, 128, 0, s>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p, a.FA.p, a.SC.p, a.tgt.p));
+    if (x->viscous) FCFD_BY_FLUX(x->cs.flux, k_stale_adj<true, FX><<<go, 128, 0, s>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p, mutf, a.FA.p, a.SC.p, a.tgt.p));
+    else FCFD_BY_FLUX(x->cs.flux, k_stale_adj<false, FX><<<go, 128, 0, s>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p, mutf, a.FA.p, a.SC.p, a.tgt.p));
     k_stale_apply<<<go, 128, 0, s>>>(m.n_outlet, m.nf, a.SC.p, a.tgt.p, a.FA.p);
   }
   CK(cudaMemsetAsync(a.Wlim.p, 0, sizeof(double) * 5 * (size_t)m.nt, s));
@@ -740,12 +986,23 @@ static void run_adjoint(fcfd_ctx *x, const double *Rbar_soa, unsigned int mask, 
     k_cell_adj<true><<<gc, 128, 0, s>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, x->ext.p, a.FA.p, a.Wcell.p, a.Gb.p, a.Wface.p, a.e2part.p);
   else
     k_cell_adj<false><<<gc, 128, 0, s>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, x->ext.p, a.FA.p, a.Wcell.p, a.Gb.p, a.Wface.p, a.e2part.p);
+  if (kw)
+    k_kw_cell_adj<<<gc, 128, 0, s>>>(x->cs, m, P.W.p, kw->fw.K, P.G.p, kw->fw.mut, kw->fw.vol, kw->RKb, a.RFA.p, a.FA.p,
+                                     kw->fw.ratio, a.Wcell.p, a.Gb.p, a.Kcell.p, a.GKb.p);
   k_wlim_gather<<<(5 * m.nc + 255) / 256, 256, 0, s>>>(m, a.Wface.p, a.Wlim.p);
   if (need_ext) k_e2_adj<<<1, 32, 0, s>>>(x->cs, m, P.W.p, x->ext.p, x->argx.p, a.e2part.p, gc, a.Wlim.p);
-  k_grad_adj<<<(m.nt + 127) / 128, 128, 0, s>>>(m, a.tr_index.p, a.tr_cell.p, a.tr_entry.p, a.Gb.p, a.Wgrad.p);
-  if (m.nb > 0) k_ghost_adj<<<(m.nb + 127) / 128, 128, 0, s>>>(x->cs, m, P.W.p, a.FA.p, a.Wgrad.p, a.Wlim.p, a.GA.p);
+  k_grad_adj<5><<<(m.nt + 127) / 128, 128, 0, s>>>(m, a.tr_index.p, a.tr_cell.p, a.tr_entry.p, a.Gb.p, a.Wgrad.p);
+  if (kw) {
+    k_grad_adj<2><<<(m.nt + 127) / 128, 128, 0, s>>>(m, a.tr_index.p, a.tr_cell.p, a.tr_entry.p, a.GKb.p, a.Kgrad.p);
+    if (m.nb > 0)
+      k_kw_ghost_adj<<<(m.nb + 127) / 128, 128, 0, s>>>(x->cs, m, P.W.p, kw->fw.K, a.RFA.p, a.FA.p, a.Kgrad.p, kw->fw.ratio,
+                                                        a.Wx.p, a.KGA.p);
+  }
+  if (m.nb > 0)
+    k_ghost_adj<<<(m.nb + 127) / 128, 128, 0, s>>>(x->cs, m, P.W.p, a.FA.p, a.Wgrad.p, a.Wlim.p, kw ? a.Wx.p : nullptr, a.GA.p);
   if (aos) k_final_adj<true><<<(m.nc + tb - 1) / tb, tb, 0, s>>>(m, a.Wcell.p, a.Wgrad.p, a.Wlim.p, a.GA.p, out);
   else k_final_adj<false><<<(m.nc + tb - 1) / tb, tb, 0, s>>>(m, a.Wcell.p, a.Wgrad.p, a.Wlim.p, a.GA.p, out);
+  if (kw) k_kw_final_adj<<<(m.nc + tb - 1) / tb, tb, 0, s>>>(m, a.Kcell.p, a.Kgrad.p, a.KGA.p, kw->Kout);
   k_rearm<<<1, 32, 0, s>>>(x->ext.p, x->argx.p);
   CK(cudaGetLastError());
 }
@@ -780,6 +1037,54 @@ int fcfd_vjp(fcfd_ctx *x, const double *W, const double *Rbar, double *Wbar, int
     double *out = dev ? Wbar : a.out.p;
     run_adjoint(x, a.Rb.p, 0u, dir, out, true);
     if (!dev) CK(cudaMemcpyAsync(Wbar, a.out.p, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    check_err(x);
+  } catch (const Error &e) {
+    set_last_error(e.what());
+    return e.code;
+  } catch (const std::exception &e) {
+    set_last_error(e.what());
+    return FCFD_ERR_INPUT;
+  }
+  return FCFD_OK;
+}
+
+// (Wbar, Kbar) = (d(R, RK)/d(W, K))^T (Rbar, RKbar) for a turbulent case:
+// the flow adjoint above with the k-omega terms reversed as well.
+int fcfd_rans_vjp(fcfd_ctx *x, const double *W, const double *K, const double *Rbar, const double *RKbar, double *Wbar,
+                  double *Kbar, int flags) {
+  try {
+    if (!x || !W || !K || !Rbar || !RKbar || !Wbar || !Kbar) throw Error(FCFD_ERR_INPUT, "null argument");
+    if (!x->rans) throw Error(FCFD_ERR_INPUT, "the case has no turbulence model");
+    CK(cudaSetDevice(x->device));
+    const DevMesh &m = x->dm;
+    cudaStream_t s = x->stream;
+    const bool dev = flags & FCFD_DEVICE_PTRS;
+    const size_t n = 5 * (size_t)m.nc, nk = 2 * (size_t)m.nc;
+    AdjBufs &a = adj_bufs(x);
+    kw_adj_bufs(x, a);
+    const double *w = W, *k = K, *rb = Rbar, *rkb = RKbar;
+    if (!dev) {
+      CK(cudaMemcpyAsync(x->Win.p, W, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+      CK(cudaMemcpyAsync(a.Kin.p, K, sizeof(double) * nk, cudaMemcpyHostToDevice, s));
+      CK(cudaMemcpyAsync(a.out.p, Rbar, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+      CK(cudaMemcpyAsync(a.Kout.p, RKbar, sizeof(double) * nk, cudaMemcpyHostToDevice, s));
+      w = x->Win.p; k = a.Kin.p; rb = a.out.p; rkb = a.Kout.p;
+    }
+    const int tb = 256;
+    KwAdj kw;
+    rans_eval_for_adjoint(x, w, k, kw.fw);
+    k_aos_to_soa<double><<<(m.nc + tb - 1) / tb, tb, 0, s>>>(rb, a.Rb.p, m.nc, m.nc);
+    k_aos2_to_soa<<<(m.nc + tb - 1) / tb, tb, 0, s>>>(rkb, a.RKb.p, m.nc);
+    kw.RKb = a.RKb.p;
+    kw.Kout = dev ? Kbar : a.Kout.p;
+    const double dir[3] = {0., 0., 0.};
+    double *out = dev ? Wbar : a.out.p;
+    run_adjoint(x, a.Rb.p, 0u, dir, out, true, &kw);
+    if (!dev) {
+      CK(cudaMemcpyAsync(Wbar, a.out.p, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+      CK(cudaMemcpyAsync(Kbar, a.Kout.p, sizeof(double) * nk, cudaMemcpyDeviceToHost, s));
+    }
     CK(cudaStreamSynchronize(s));
     check_err(x);
   } catch (const Error &e) {

@@ -218,6 +218,21 @@ void kw_driver_residual(fcfd_ctx *x, void *p);
 int kw_driver_step(fcfd_ctx *x, void *p, const double *dt, int mode, double krtol, double kabstol);
 void kw_driver_update(fcfd_ctx *x, void *p, const double *dt, double *part, int *err);
 void kw_driver_state(fcfd_ctx *x, void *p, double *W, double *K, double *mut);
+
+// The coupled NS + k-omega evaluation at (W, K) (device AoS [nc][5], [nc][2])
+// that the adjoint reverses: leaves W with its ghosts in x->p64.W and these
+// device arrays (SoA) of the same evaluation.
+struct RansFwd {
+  const double *K;     // [2][nt] k, omega with the ghosts' values
+  const double *GK;    // [6][nc] k, omega gradients
+  const double *mut;   // [nt] eddy viscosity
+  const double *mutf;  // [nf] its face values
+  const double *mdot;  // [nf] NS face mass flux
+  const double *wl;    // [nf] NS face left weight
+  const double *vol;   // [nc] cell volumes
+  double ratio;        // eddy viscosity ratio limit
+};
+void rans_eval_for_adjoint(fcfd_ctx *x, const double *W, const double *K, RansFwd &out);
 // mixed.cu: FP32 face pass + FP64 pass over the shock-flagged faces
 void launch_mixed_faces(fcfd_ctx *x, double shock_ratio, int *list, int *count, cudaStream_t s);
 void rans_setup(fcfd_ctx *x);

@@ -1457,10 +1457,14 @@ struct LocalGrad {
 // 5 = Steger-Warming.  Kernels are instantiated per selector (FCFD_BY_FLUX)
 // so the larger SD-SLAU and Steger-Warming bodies add no registers to the
 // other fluxes' kernels.
-template <class S, class GS, bool VISCOUS, int FX>
+//
+// mu_t: the face eddy viscosities, indexed by face (null: laminar); MT is a
+// pointer, or a view whose operator[] gives the face's value (the adjoint's
+// seeded input).
+template <class S, class GS, bool VISCOUS, int FX, class MT = const typename GS::value_type *>
 __device__ __forceinline__ void face_D(const DevCase &cs, const DevMesh &m, int f, const double n[3], double A, int b,
                                        int pa, int nb, const FState<S> &L, const FState<S> &R, const GS &gs,
-                                       const typename GS::value_type *__restrict__ mu_t, S D[5], S &wL) {
+                                       MT mu_t, S D[5], S &wL) {
   const int nf = m.nf, nt = m.nt;
   S F[5];
   if (FX == 4) sdslau(cs, L, R, n, F, wL);

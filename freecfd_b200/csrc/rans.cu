@@ -19,17 +19,13 @@
 #include <memory>
 
 #include "ctx.hpp"
+#include "kw.cuh"
 
 namespace fcfd {
 
 extern template __global__ void k_ghost_minmax<double>(DevCase, DevMesh, double *, unsigned long long *, int *);
 extern template __global__ void k_ghost_minmax<Dual<double>>(DevCase, DevMesh, Dual<double> *, unsigned long long *, int *);
 extern template __global__ void k_ghost_minmax<Dual<float>>(DevCase, DevMesh, Dual<float> *, unsigned long long *, int *);
-
-// rans.cc:43-49, model=k-omega (blending = 1)
-struct KOmega {
-  static constexpr double sigma_k = 0.85, sigma_omega = 0.5, beta = 0.075, beta_star = 0.09, alpha = 5. / 9.;
-};
 
 // Per-state buffers of one coupled evaluation (S = double for the residual,
 // Dual<double> for its tangent).
@@ -76,11 +72,7 @@ __global__ void k_rans_prep(DevCase cs, DevMesh m, const S *__restrict__ W, S *_
     if (bc.kw_fixed) { K[i] = S(bc.k_bc); K[nt + i] = S(bc.omega_bc); }
     else { K[i] = K[pa]; K[nt + i] = K[nt + pa]; }
   }
-  const S p = W[i], T = W[4 * nt + i];
-  const S rho = eos_rho(cs, p, T);
-  const S mu = viscosity(cs, T);
-  const S mt = rho * K[i] / K[nt + i];
-  mut[i] = smin(S(ratio_limit * mu), mt);
+  mut[i] = kw_mut(cs, W[i], W[4 * nt + i], K[i], K[nt + i], ratio_limit);
 }
 
 // mu_t.face (variable.h:134-147): the BC value where fixed, else the average.
@@ -142,8 +134,7 @@ __global__ void k_rans_grad(DevMesh m, const S *__restrict__ K, S *__restrict__ 
   }
 }
 
-// k and omega face fluxes: DK = diffusive - convective (rans_terms.cc:59-112,
-// get_kOmega 277-319).
+// k and omega face fluxes: DK = diffusive - convective (kw_face_flux).
 template <class S>
 __global__ void k_rans_face(DevCase cs, DevMesh m, const S *__restrict__ W, const S *__restrict__ K,
                             const S *__restrict__ GK, const S *__restrict__ mutf,
@@ -152,35 +143,16 @@ __global__ void k_rans_face(DevCase cs, DevMesh m, const S *__restrict__ W, cons
   const int nf = m.nf, nc = m.nc, nt = m.nt;
   if (f >= nf) return;
   const int pa = m.f_parent[f], nb = m.f_neighbor[f], b = m.f_bc[f];
-  const S Tf = (b >= 0 && cs.bc[b].T_fixed) ? S(cs.bc[b].T) : face_avg(m, f, W + 4 * nt);
-  const S lam = viscosity(cs, Tf);
-  const S turb = mutf[f];
-  const S md = mdot[f], wL = wl[f], wR = 1. - wL;
-  const S kL = K[pa], oL = K[nt + pa], kR = K[nb], oR = K[nt + nb];
-  S gk[3], go[3];
-  for (int i = 0; i < 3; ++i) {
-    if (b >= 0) { gk[i] = GK[i * nc + pa]; go[i] = GK[(3 + i) * nc + pa]; }
-    else {
-      gk[i] = m.f_w[f] * GK[i * nc + pa] + m.f_w[nf + f] * GK[i * nc + nb];
-      go[i] = m.f_w[f] * GK[(3 + i) * nc + pa] + m.f_w[nf + f] * GK[(3 + i) * nc + nb];
-    }
+  S gpa[6], gnb[6];
+  for (int i = 0; i < 6; ++i) {
+    gpa[i] = GK[i * nc + pa];
+    gnb[i] = b < 0 ? GK[i * nc + nb] : S(0.);
   }
-  const double l0 = m.c_x[nb] - m.c_x[pa], l1 = m.c_x[nt + nb] - m.c_x[nt + pa], l2 = m.c_x[2 * nt + nb] - m.c_x[2 * nt + pa];
-  const double lm = sqrt(l0 * l0 + l1 * l1 + l2 * l2);
-  const double e[3] = {l0 / lm, l1 / lm, l2 / lm};
-  const S dk = gk[0] * e[0] + gk[1] * e[1] + gk[2] * e[2];
-  const S dw = go[0] * e[0] + go[1] * e[1] + go[2] * e[2];
-  for (int i = 0; i < 3; ++i) {
-    gk[i] = gk[i] - dk * e[i] + (kR - kL) / lm * e[i];
-    go[i] = go[i] - dw * e[i] + (oR - oL) / lm * e[i];
-  }
-  const double n[3] = {m.f_n[f], m.f_n[nf + f], m.f_n[2 * nf + f]};
-  const double A = m.f_area[f];
-  const S conv0 = md * (wL * kL + wR * kR) * A, conv1 = md * (wL * oL + wR * oR) * A;
-  const S diff0 = (lam + turb * KOmega::sigma_k) * (gk[0] * n[0] + gk[1] * n[1] + gk[2] * n[2]) * A;
-  const S diff1 = (lam + turb * KOmega::sigma_omega) * (go[0] * n[0] + go[1] * n[1] + go[2] * n[2]) * A;
-  DK[f] = diff0 - conv0;
-  DK[nf + f] = diff1 - conv1;
+  S d0, d1;
+  kw_face_flux<S>(cs, m, f, b, pa, nb, W[4 * nt + pa], W[4 * nt + nb], K[pa], K[nt + pa], K[nb], K[nt + nb], gpa, gnb,
+                  mutf[f], mdot[f], wl[f], d0, d1);
+  DK[f] = d0;
+  DK[nf + f] = d1;
 }
 
 // Per cell: sum of +-DK in ascending face order, plus sources x volume
@@ -198,19 +170,10 @@ __global__ void k_rans_gather(DevCase cs, DevMesh m, const S *__restrict__ W, co
     if (e >= 0) { r0 = r0 + DK[e]; r1 = r1 + DK[nf + e]; }
     else { r0 = r0 + -1. * DK[~e]; r1 = r1 + -1. * DK[nf + ~e]; }
   }
-  const S dudx = G[3 * nc + c], dudy = G[4 * nc + c], dudz = G[5 * nc + c];
-  const S dvdx = G[6 * nc + c], dvdy = G[7 * nc + c], dvdz = G[8 * nc + c];
-  const S dwdx = G[9 * nc + c], dwdy = G[10 * nc + c], dwdz = G[11 * nc + c];
-  const S divU = dudx + dvdy + dwdz;
-  const S sr = sqrt(2. * (dudx * dudx + dvdy * dvdy + dwdz * dwdz) + (dudy + dvdx) * (dudy + dvdx) +
-                    (dudz + dwdx) * (dudz + dwdx) + (dvdz + dwdy) * (dvdz + dwdy));
-  const S rho = eos_rho(cs, W[c], W[4 * nt + c]);
-  const S k = K[c], om = K[nt + c], mt = mut[c];
-  S Prod = mt * (sr * sr - 2. / 3. * divU * divU) - 2. / 3. * rho * k * divU;
-  const S Dest = KOmega::beta_star * rho * om * k;
-  Prod = smin(Prod, S(10. * Dest));
-  const S s0 = Prod - Dest;
-  const S s1 = KOmega::alpha * rho / mt * Prod - KOmega::beta * rho * om * om;
+  S g9[9];
+  for (int i = 0; i < 9; ++i) g9[i] = G[(3 + i) * nc + c];
+  S s0, s1;
+  kw_source<S>(cs, g9, W[c], W[4 * nt + c], K[c], K[nt + c], mut[c], s0, s1);
   RK[2 * c] = r0 + s0 * vol[c];
   RK[2 * c + 1] = r1 + s1 * vol[c];
 }
@@ -341,6 +304,19 @@ static void rans_chain(fcfd_ctx *x, Pipe<S> &P, RansBuf<S> &s, S *mdot, S *wl, S
   k_rans_gather<S><<<(m.nc + 127) / 128, 128, 0, st>>>(x->cs, m, P.W.p, s.K.p, P.G.p, s.mut.p, x->rans->vol.p, s.DK.p, RK);
   if (ev) CK(cudaEventRecord(ev[2], st));
   CK(cudaGetLastError());
+}
+
+void rans_eval_for_adjoint(fcfd_ctx *x, const double *W, const double *K, RansFwd &out) {
+  const DevMesh &m = x->dm;
+  cudaStream_t s = x->stream;
+  RansBuf<double> &b = x->rans->b;
+  const int tb = 256;
+  k_aos_to_soa<double><<<(m.nc + tb - 1) / tb, tb, 0, s>>>(W, x->p64.W.p, m.nc, m.nt);
+  k_k_to_soa<<<(m.nc + tb - 1) / tb, tb, 0, s>>>(K, b.K.p, m.nc, m.nt);
+  rans_chain<double, false>(x, x->p64, b, x->mdot.p, x->wl.p, x->p64.R.p, b.RK.p);
+  out.K = b.K.p; out.GK = b.GK.p; out.mut = b.mut.p; out.mutf = b.mutf.p;
+  out.mdot = x->mdot.p; out.wl = x->wl.p; out.vol = x->rans->vol.p;
+  out.ratio = x->case_ptr->visc_ratio_limit;
 }
 
 }  // namespace fcfd

@@ -289,6 +289,15 @@ class NavierStokes:
         check(lib.fcfd_rans_jvp(self.h, *[_d(a) for a in arrs], _d(R), _d(RK), _d(JV), _d(JVK), 4 if fp32 else 0))
         return (R, RK, JV, JVK) if with_residual else (JV, JVK)
 
+    def rans_vjp(self, W, K, Rbar, RKbar):
+        """Adjoint of the coupled residual (backward half of rans_jvp):
+        (Wbar[nc][5], Kbar[nc][2]) = (d(R, RK)/d(W, K))^T (Rbar, RKbar)."""
+        nc = self.mesh.nc
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (W, K, Rbar, RKbar)]
+        Wb, Kb = np.empty((nc, 5)), np.empty((nc, 2))
+        check(lib.fcfd_rans_vjp(self.h, *[_d(a) for a in arrs], _d(Wb), _d(Kb), 0))
+        return Wb, Kb
+
     def time_rans(self, reps: int = 50, flush_l2: bool = True):
         """[total, NS part, k-omega part] ms per coupled residual (device events)."""
         out = np.zeros(3)

@@ -215,6 +215,16 @@ int fcfd_time_rans(fcfd_ctx *ctx, int reps, int flush_l2, double *out, int out_l
  * add FCFD_JVP_FP32: the tangent chain in single precision (as fcfd_jvp). */
 int fcfd_rans_jvp(fcfd_ctx *ctx, const double *W, const double *K, const double *V, const double *VK, double *R,
                   double *RK, double *JV, double *JVK, int flags);
+/* Adjoint of the coupled residual, the backward half of the (fcfd_rans_jvp,
+ * fcfd_rans_vjp) pair: (Wbar[nc][5], Kbar[nc][2]) = (d(R, RK)/d(W, K))^T
+ * (Rbar[nc][5], RKbar[nc][2]), exact for the discrete residual (the branches
+ * taken at W, K).  Reverses the eddy viscosity (rans_update_eddy_viscosity.cc
+ * :26-56), its face values, the k-omega gradients, face fluxes and sources
+ * (rans_terms.cc:39-275), their coupling into the NS viscous flux
+ * (ns_diffusive_face_flux.cc:36-39) and the NS residual as fcfd_vjp does.
+ * Deterministic (every accumulation has a fixed order). */
+int fcfd_rans_vjp(fcfd_ctx *ctx, const double *W, const double *K, const double *Rbar, const double *RKbar,
+                  double *Wbar, double *Kbar, int flags);
 /* Domain decomposition: one rank's part of the residual.  Replaces the
  * partition-ghost exchange of the reference's MPI runs
  * (NavierStokes::mpi_update_ghost_primitives / mpi_update_ghost_gradients,

@@ -174,3 +174,97 @@ def test_coupled_komega_newton(fb):
         assert np.isfinite(W).all() and (K > 0).all()
         drag[label] = ns.drag(W, [2], (1.0, 0.0, 0.0), gradient=False)[0][0]
     assert abs(drag["mixed"] - drag["plain"]) <= 1e-3 * abs(drag["plain"])
+
+
+def _rans_jacobian_cs(o, W, K):
+    """Dense d(R, RK)/d(W, K) ([7nc] x [7nc]; rows and columns ordered
+    (W AoS, then K AoS)) from the oracle's complex-step columns."""
+    nc = W.shape[0]
+    n = 7 * nc
+    J = np.empty((n, n))
+    eW, eK = np.zeros((nc, 5)), np.zeros((nc, 2))
+    for k in range(n):
+        e = eW if k < 5 * nc else eK
+        i = k if k < 5 * nc else k - 5 * nc
+        e.flat[i] = 1.0
+        dR, dRK = o.rans_residual_cstep(W, K, eW, eK)
+        J[:, k] = np.concatenate([dR.ravel(), dRK.ravel()])
+        e.flat[i] = 0.0
+    return J
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("limiter,flux", [("vk", "Roe"), ("none", "AUSM+up"), ("minmod", "vanLeer"), ("bj", "SD-SLAU")])
+def test_rans_vjp_matches_jacobian_transpose(limiter, flux, oracle_mod, fb):
+    """Adjoint of the coupled residual entry by entry against the transpose of
+    the Jacobian assembled from the oracle's complex step (8x4x2 plate: inlet
+    with fixed k, omega and mu_t, no-slip wall with mu_t = 0, outlet,
+    symmetry)."""
+    case = _plate(ni=8, nj=4, nk=2, limiter=limiter, flux=flux)
+    o, cs, m = build_pair(case, oracle_mod, fb)
+    ns = fb.NavierStokes(m, cs, 0)
+    W, K = _generic(case), case.kstate
+    J = _rans_jacobian_cs(o, W, K)
+    nc = m.nc
+    rng = np.random.default_rng(31)
+    for _ in range(2):
+        Rb, RKb = rng.standard_normal((nc, 5)), rng.standard_normal((nc, 2))
+        ref = J.T @ np.concatenate([Rb.ravel(), RKb.ravel()])
+        rW, rK = ref[:5 * nc].reshape(nc, 5), ref[5 * nc:].reshape(nc, 2)
+        Wb, Kb = ns.rans_vjp(W, K, Rb, RKb)
+        cols = [k for k in range(5) if np.abs(rW[:, k]).max() > 1e-9 * np.abs(rW).max()]
+        errW = (np.abs(Wb - rW).max(axis=0) / np.maximum(np.abs(rW).max(axis=0), 1e-300))[cols]
+        errK = np.abs(Kb - rK).max(axis=0) / np.abs(rK).max(axis=0)
+        assert errW.max() <= 1e-9 and errK.max() <= 1e-9, (errW, errK)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("size,limiter,flux", [((24, 12, 3), "vk", "Roe"), ((24, 12, 3), "minmod", "AUSM+up"),
+                                               ((24, 12, 3), "vk", "SW")])
+def test_rans_vjp_dot_product(size, limiter, flux, oracle_mod, fb):
+    """<(Rbar, RKbar), J (V, VK)> with J (V, VK) from the oracle's complex
+    step equals <J^T (Rbar, RKbar), (V, VK)> from the device adjoint."""
+    ni, nj, nk = size
+    case = _plate(ni=ni, nj=nj, nk=nk, limiter=limiter, flux=flux)
+    o, cs, m = build_pair(case, oracle_mod, fb)
+    ns = fb.NavierStokes(m, cs, 0)
+    W, K = _generic(case), case.kstate
+    rng = np.random.default_rng(37)
+    for _ in range(3):
+        V = rng.standard_normal(W.shape) * np.abs(W).max(axis=0)
+        VK = rng.standard_normal(K.shape) * np.abs(K).max(axis=0)
+        Rb, RKb = rng.standard_normal(W.shape), rng.standard_normal(K.shape)
+        # scale the k-omega seed so both halves weigh alike in the sums
+        dR, dRK = o.rans_residual_cstep(W, K, V, VK)
+        RKb *= np.abs(dR).max() / np.abs(dRK).max()
+        Wb, Kb = ns.rans_vjp(W, K, Rb, RKb)
+        lhs = float((Rb * dR).sum() + (RKb * dRK).sum())
+        rhs = float((Wb * V).sum() + (Kb * VK).sum())
+        mag = float(np.abs(Rb * dR).sum() + np.abs(RKb * dRK).sum())
+        assert abs(lhs - rhs) <= 1e-11 * mag, (lhs, rhs, mag)
+
+
+@pytest.mark.gpu
+def test_rans_vjp_deterministic_and_pairs_with_jvp(oracle_mod, fb):
+    """Repeated adjoints are the same bits (fixed-order accumulations), and
+    the device pair (fcfd_rans_jvp, fcfd_rans_vjp) satisfies the dot-product
+    identity on its own; the flow-only seed reaches K through the eddy
+    viscosity."""
+    case = _plate(ni=24, nj=12, nk=3)
+    o, cs, m = build_pair(case, oracle_mod, fb)
+    ns = fb.NavierStokes(m, cs, 0)
+    W, K = _generic(case), case.kstate
+    rng = np.random.default_rng(41)
+    Rb, RKb = rng.standard_normal(W.shape), rng.standard_normal(K.shape)
+    Wb, Kb = ns.rans_vjp(W, K, Rb, RKb)
+    for _ in range(3):
+        W2, K2 = ns.rans_vjp(W, K, Rb, RKb)
+        assert np.array_equal(W2, Wb) and np.array_equal(K2, Kb)
+    V = rng.standard_normal(W.shape) * np.abs(W).max(axis=0)
+    VK = rng.standard_normal(K.shape) * np.abs(K).max(axis=0)
+    JV, JVK = ns.rans_jvp(W, K, V, VK)
+    lhs = float((Rb * JV).sum() + (RKb * JVK).sum())
+    rhs = float((Wb * V).sum() + (Kb * VK).sum())
+    assert abs(lhs - rhs) <= 1e-11 * float(np.abs(Rb * JV).sum() + np.abs(RKb * JVK).sum())
+    _, Kf = ns.rans_vjp(W, K, Rb, np.zeros_like(RKb))
+    assert np.abs(Kf).max() > 0.0
