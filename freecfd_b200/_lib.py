@@ -73,7 +73,8 @@ class NewtonOpts(ctypes.Structure):
                 ("cfl_max", ctypes.c_double), ("cfl_mode", ctypes.c_int32), ("ser_exponent", ctypes.c_double),
                 ("jvp_mode", ctypes.c_int32), ("fp32_krylov", ctypes.c_int32), ("max_seconds", ctypes.c_double),
                 ("precond_sweeps", ctypes.c_int32), ("krylov_cycles", ctypes.c_int32),
-                ("stop_all_rows", ctypes.c_int32), ("gs_launch", ctypes.c_int32), ("precond_ilu0", ctypes.c_int32)]
+                ("stop_all_rows", ctypes.c_int32), ("gs_launch", ctypes.c_int32), ("precond_ilu0", ctypes.c_int32),
+                ("local_relax", ctypes.c_int32)]
 
 
 class NewtonReport(ctypes.Structure):

@@ -781,6 +781,22 @@ __global__ void k_max_rel_change(DevCase cs, int nc, const double *__restrict__ 
   for (int o = 16; o > 0; o >>= 1) r = fmax(r, __shfl_xor_sync(0xffffffffu, r, o));
   if ((threadIdx.x & 31) == 0) atomicMax(key, okey(r));
 }
+// W += a_c dW per cell, a_c = min(1, 0.2 / max(|dp|/|p|, |dT|/|T|)) (absolute
+// p, T), with the NaN/Inf check of k_update
+__global__ void k_update_local(DevCase cs, int nc, double *__restrict__ Wn, const double *__restrict__ dW,
+                               int *__restrict__ err) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nc) return;
+  const double pa = Wn[c] + cs.Pref, Ta = Wn[4 * nc + c] + cs.Tref;
+  const double rp = ::fabs(dW[c]) / ::fabs(pa), rT = ::fabs(dW[4 * nc + c]) / ::fabs(Ta);
+  const double r = rp > rT ? rp : rT;
+  if (!isfinite(r)) {
+    atomicOr(err, 8);
+    return;
+  }
+  const double a = r > 0.2 ? 0.2 / r : 1.;
+  for (int v = 0; v < 5; ++v) Wn[(size_t)v * nc + c] += a * dW[(size_t)v * nc + c];
+}
 __global__ void k_aos_to_soa_nc(const double *__restrict__ in, double *__restrict__ out, int nc) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= nc) return;
@@ -1637,20 +1653,25 @@ int fcfd_newton_solve(fcfd_ctx *x, double *W, const fcfd_newton_opts *o, fcfd_ne
       const LinearSolve ls = implicit_solve(x, ns, K64, K32, f32, jmode, krtol, 0., part, hh);
       const int kit = ls.iters;
       rep->krylov_iterations += kit;
-      // relax the update so that p and T change by at most 20 % per step
-      CK(cudaMemsetAsync(key.p, 0, sizeof(unsigned long long), s));
-      k_max_rel_change<<<gc, tb, 0, s>>>(x->cs, nc, ns.Wn.p, ns.R1.p, key.p);
-      unsigned long long kh = 0;
-      CK(cudaMemcpyAsync(&kh, key.p, sizeof(kh), cudaMemcpyDeviceToHost, s));
-      CK(cudaStreamSynchronize(s));
-      double dmax = 0.;
-      {
-        unsigned long long b = (kh >> 63) ? (kh & 0x7fffffffffffffffull) : ~kh;
-        std::memcpy(&dmax, &b, sizeof(dmax));
-      }
-      const double alpha = (dmax > 0.2) ? 0.2 / dmax : 1.;
+      // relax the update so that p and T change by at most 20 % per step:
+      // one factor for the whole update, or per cell (local_relax)
       CK(cudaMemcpyAsync(Wsave.p, ns.Wn.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
-      k_update<double><<<gn, tb, 0, s>>>(n, ns.Wn.p, ns.R1.p, alpha, x->err.p);
+      if (o->local_relax) {
+        k_update_local<<<gc, tb, 0, s>>>(x->cs, nc, ns.Wn.p, ns.R1.p, x->err.p);
+      } else {
+        CK(cudaMemsetAsync(key.p, 0, sizeof(unsigned long long), s));
+        k_max_rel_change<<<gc, tb, 0, s>>>(x->cs, nc, ns.Wn.p, ns.R1.p, key.p);
+        unsigned long long kh = 0;
+        CK(cudaMemcpyAsync(&kh, key.p, sizeof(kh), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        double dmax = 0.;
+        {
+          unsigned long long b = (kh >> 63) ? (kh & 0x7fffffffffffffffull) : ~kh;
+          std::memcpy(&dmax, &b, sizeof(dmax));
+        }
+        const double alpha = (dmax > 0.2) ? 0.2 / dmax : 1.;
+        k_update<double><<<gn, tb, 0, s>>>(n, ns.Wn.p, ns.R1.p, alpha, x->err.p);
+      }
       int h = 0;
       CK(cudaMemcpyAsync(&h, x->err.p, sizeof(int), cudaMemcpyDeviceToHost, s));
       CK(cudaStreamSynchronize(s));

@@ -328,7 +328,8 @@ class NavierStokes:
     def newton_solve(self, W, tol=1e-10, max_newton=200, krylov_dim=30, krylov_rtol=1e-2, cfl0=1.0,
                      cfl_growth=1.2, cfl_max=1e6, cfl_mode=1, ser_exponent=1.0, jvp=True, fp32_krylov=False,
                      max_seconds=0.0, raise_on_fail=True, precond_sweeps=0, krylov_cycles=1, exact_jvp=False,
-                     fp32_jvp=False, stop_all_rows=False, fp32_frozen_limiter=False, gs_persistent=False, ilu0=False):
+                     fp32_jvp=False, stop_all_rows=False, fp32_frozen_limiter=False, gs_persistent=False, ilu0=False,
+                     local_relax=False):
         """Steady solve R(W) = 0 (pseudo-transient Newton-Krylov on the device).
         stop_all_rows: also wait for the momentum and energy residuals to drop
         by tol.  fp32_frozen_limiter: with fp32_jvp, hold the limiter fixed in
@@ -336,14 +337,15 @@ class NavierStokes:
         colour updates of a preconditioner application in one cooperative
         launch with grid barriers instead of one launch per colour update.
         ilu0: block ILU(0) preconditioner in the multicolour order instead
-        of block Jacobi / Gauss-Seidel.  Returns (W_converged, report
-        dict)."""
+        of block Jacobi / Gauss-Seidel.  local_relax: limit each cell's
+        update to a 20 % change of p and T on its own instead of scaling the
+        whole update.  Returns (W_converged, report dict)."""
         W = np.array(W, dtype=np.float64, order="C", copy=True)
         o = NewtonOpts(int(max_newton), float(tol), int(krylov_dim), float(krylov_rtol), float(cfl0), float(cfl_growth),
                        float(cfl_max), int(cfl_mode), float(ser_exponent),
                        ((4 if fp32_frozen_limiter else 3) if fp32_jvp else (2 if exact_jvp else 1)) if jvp else 0,
                        int(bool(fp32_krylov)), float(max_seconds), int(precond_sweeps), int(krylov_cycles),
-                       int(bool(stop_all_rows)), int(bool(gs_persistent)), int(bool(ilu0)))
+                       int(bool(stop_all_rows)), int(bool(gs_persistent)), int(bool(ilu0)), int(bool(local_relax)))
         r = NewtonReport()
         rc = lib.fcfd_newton_solve(self.h, _d(W), ctypes.byref(o), ctypes.byref(r))
         rep = dict(status=r.status, newton_iterations=r.newton_iterations, krylov_iterations=r.krylov_iterations,

@@ -304,6 +304,10 @@ typedef struct fcfd_newton_opts {
                              instead of block Jacobi / Gauss-Seidel; precond_sweeps is ignored.  The
                              reference's PETSc default for its FGMRES (ns_petsc_functions.cc:25-83) is
                              block Jacobi with ILU(0) inside each process's block */
+  int32_t local_relax;    /* 0: the whole update is scaled so that p and T change by at most 20 % in
+                             every cell; 1: each cell's update is scaled on its own to that bound
+                             (local under-relaxation: cells far from a shock or a wake take full
+                             steps), inactive once every cell's change is below the bound */
 } fcfd_newton_opts;
 
 typedef struct fcfd_newton_report {
