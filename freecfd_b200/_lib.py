@@ -26,7 +26,7 @@ EXPORTED = [
     "fcfd_mesh_lsq", "fcfd_mesh_rcm", "fcfd_mesh_grad_weights",
     "fcfd_ctx_create", "fcfd_ctx_destroy", "fcfd_ctx_set_exact_gradients", "fcfd_residual", "fcfd_last_stages", "fcfd_local_dt",
     "fcfd_time_residual", "fcfd_point_flux", "fcfd_jvp", "fcfd_vjp", "fcfd_drag", "fcfd_rans_residual", "fcfd_rans_bcs", "fcfd_time_rans", "fcfd_newton_solve", "fcfd_local_dt_cflmax_noalloc",
-    "fcfd_run", "fcfd_restart_write", "fcfd_restart_read", "fcfd_mesh_from_tecplot", "fcfd_rans_jvp", "fcfd_rans_vjp",
+    "fcfd_run", "fcfd_restart_write", "fcfd_restart_read", "fcfd_mesh_from_tecplot", "fcfd_rans_jvp", "fcfd_rans_vjp", "fcfd_ctx_set_launch_overlap",
     "fcfd_partition_sets", "fcfd_ctx_set_partition", "fcfd_partition_extrema", "fcfd_partition_residual",
     "fcfd_ctx_stream", "fcfd_diag_blocks", "fcfd_rans_newton_solve", "fcfd_residual_mixed",
     "fcfd_time_residual_mixed", "fcfd_ctx_set_gradient_kernel", "fcfd_time_terms", "fcfd_ctx_gradient_info",
@@ -124,6 +124,7 @@ def _load():
     L.fcfd_rans_residual.argtypes = [vp, vp, vp, vp, vp, ctypes.c_int]
     L.fcfd_rans_jvp.argtypes = [vp, dp, dp, dp, dp, dp, dp, dp, dp, ctypes.c_int]
     L.fcfd_rans_vjp.argtypes = [vp, dp, dp, dp, dp, dp, dp, ctypes.c_int]
+    L.fcfd_ctx_set_launch_overlap.argtypes = [vp, ctypes.c_int32]
     L.fcfd_rans_bcs.argtypes = [vp, vp, ctypes.c_int32]
     L.fcfd_time_rans.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp, ctypes.c_int]
     L.fcfd_drag.argtypes = [vp, vp, ctypes.c_uint32, vp, vp, vp, ctypes.c_int]

@@ -138,11 +138,36 @@ struct fcfd_ctx {
   DBuf<int> fold_index, fold_key;
   DBuf<double> fold_e;
   int grad_kernel = 0;  // fcfd_ctx_set_gradient_kernel: 0 automatic, 1 per cell, 2 tiles
+  // the residual chain's gradient and face launches overlap their
+  // predecessor's tail (programmatic dependent launch); fcfd_ctx_set_launch_overlap
+  bool pdl = true;
 };
 
 
 namespace fcfd {
 constexpr int kExtremaBlocks = 296;  // 2 x 148 SMs
+
+// Launches kernel k; with pdl, as a programmatic dependent launch (it may be
+// scheduled before its stream predecessor completes and waits for it in
+// pdl_wait()).
+template <class... KP, class... A>
+inline void launch_k(bool pdl, void (*k)(KP...), int grid, int block, size_t smem, cudaStream_t s, A... args) {
+  if (!pdl) {
+    k<<<grid, block, smem, s>>>(args...);
+    return;
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(block);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  CK(cudaLaunchKernelEx(&cfg, k, args...));
+}
 constexpr int kPairGradCells = 148 * 512;
 template <class S>
 void launch_chain(fcfd_ctx *x, Pipe<S> &P, S *Rout, bool aos_out, S *mo, S *wo, bool frozen_limiter = false);
@@ -153,15 +178,15 @@ int check_err(fcfd_ctx *x);
 // PART: the gradient cells of one rank of a domain decomposition (m = dmp).
 template <class S, bool PART = false>
 inline void launch_grad_limiter(const DevCase &cs, const DevMesh &m, const S *W, const unsigned long long *ext,
-                                const int *argx, S *G, S *Lm, cudaStream_t s) {
+                                const int *argx, S *G, S *Lm, cudaStream_t s, bool pdl = false) {
   const int g = ((PART ? m.n_part_cells : m.nc) + 127) / 128;
   if (g == 0) return;
   if constexpr (std::is_same<S, double>::value && !PART) {
     if (cs.tile_grad && m.tile_off) {
       const int nt_ = (m.nc + kGradTile - 1) / kGradTile;
       const size_t smem = sizeof(double) * 8 * (size_t)m.tile_slots_max;
-      if (cs.fast_grad) k_grad_limiter_tile<true><<<nt_, kGradTile, smem, s>>>(cs, m, W, ext, G, Lm);
-      else k_grad_limiter_tile<false><<<nt_, kGradTile, smem, s>>>(cs, m, W, ext, G, Lm);
+      if (cs.fast_grad) launch_k(pdl, k_grad_limiter_tile<true>, nt_, kGradTile, smem, s, cs, m, W, ext, G, Lm);
+      else launch_k(pdl, k_grad_limiter_tile<false>, nt_, kGradTile, smem, s, cs, m, W, ext, G, Lm);
       return;
     }
   }
@@ -170,14 +195,14 @@ inline void launch_grad_limiter(const DevCase &cs, const DevMesh &m, const S *W,
     // 148 SMs x 512 cells) take two threads per cell
     const int ncell = PART ? m.n_part_cells : m.nc;
     if (cs.fast_grad && cs.pair_grad && ncell < kPairGradCells) {
-      k_grad_limiter_pair<PART><<<(ncell + 31) / 32, 64, 0, s>>>(cs, m, W, ext, G, Lm);
+      launch_k(pdl, k_grad_limiter_pair<PART>, (ncell + 31) / 32, 64, 0, s, cs, m, W, ext, G, Lm);
       return;
     }
   }
   if (cs.fast_grad)
-    k_grad_limiter<S, true, PART><<<g, 128, 0, s>>>(cs, m, W, ext, argx, G, Lm);
+    launch_k(pdl, k_grad_limiter<S, true, PART>, g, 128, 0, s, cs, m, W, ext, argx, G, Lm);
   else
-    k_grad_limiter<S, false, PART><<<g, 128, 0, s>>>(cs, m, W, ext, argx, G, Lm);
+    launch_k(pdl, k_grad_limiter<S, false, PART>, g, 128, 0, s, cs, m, W, ext, argx, G, Lm);
 }
 // Face fluxes of one residual: the main launch over all faces and, when the
 // mesh has outlet faces, the outlet-face launch (stale right densities) on the
@@ -199,10 +224,11 @@ inline void launch_faces(fcfd_ctx *x, Pipe<S> &P, const S *mu_t, S *mo, S *wo, c
     CK(cudaEventRecord(x->ev_join, x->side));
   }
   const int g = (nfl + 127) / 128;
+  const bool pdl = x->pdl;
   if (g > 0 && x->viscous)
-    FCFD_BY_FLUX(x->cs.flux, k_face_flux<S, true, FX, false, PART><<<g, 128, 0, s>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p, mu_t, P.D.p, mo, wo, x->err.p));
+    FCFD_BY_FLUX(x->cs.flux, launch_k(pdl, k_face_flux<S, true, FX, false, PART>, g, 128, 0, s, x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p, mu_t, P.D.p, mo, wo, x->err.p));
   else if (g > 0)
-    FCFD_BY_FLUX(x->cs.flux, k_face_flux<S, false, FX, false, PART><<<g, 128, 0, s>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p, mu_t, P.D.p, mo, wo, x->err.p));
+    FCFD_BY_FLUX(x->cs.flux, launch_k(pdl, k_face_flux<S, false, FX, false, PART>, g, 128, 0, s, x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p, mu_t, P.D.p, mo, wo, x->err.p));
   if (side) CK(cudaStreamWaitEvent(s, x->ev_join, 0));
 }
 // newton.cu: inverse flow-equation blocks of the block-Jacobi preconditioner

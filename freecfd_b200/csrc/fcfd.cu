@@ -44,7 +44,7 @@ void launch_chain(fcfd_ctx *x, Pipe<S> &P, S *Rout, bool aos_out, S *mo, S *wo, 
     k_argext<S><<<(m.nc + tb - 1) / tb, tb, 0, s>>>(m, P.W.p, x->ext.p, x->argx.p);
     argx = x->argx.p;
   }
-  launch_grad_limiter<S>(csl, m, P.W.p, x->ext.p, argx, P.G.p, P.Lm.p, s);
+  launch_grad_limiter<S>(csl, m, P.W.p, x->ext.p, argx, P.G.p, P.Lm.p, s, x->pdl);
   launch_faces<S>(x, P, (const S *)nullptr, mo, wo, s);
   const int gg = (5 * m.nc + tb - 1) / tb;
   if (aos_out)
@@ -683,7 +683,7 @@ int fcfd_time_residual(fcfd_ctx *x, int reps, int flush_l2, double *out, int out
     if (k == 0) {
       if (ng > 0) k_ghost_minmax<double><<<ng, tb, 0, s>>>(x->cs, m, P.W.p, need_ext ? x->ext.p : nullptr, x->err.p);
     } else if (k == 1) {
-      launch_grad_limiter<double>(x->cs, m, P.W.p, x->ext.p, nullptr, P.G.p, P.Lm.p, s);
+      launch_grad_limiter<double>(x->cs, m, P.W.p, x->ext.p, nullptr, P.G.p, P.Lm.p, s, x->pdl);
     } else if (k == 3) {
       launch_faces<double>(x, P, nullptr, nullptr, nullptr, s);
     } else if (k == 4) {
@@ -739,6 +739,15 @@ int fcfd_ctx_set_gradient_kernel(fcfd_ctx *x, int kind) {
   x->cs.tile_grad = (kind == 2) ? 1 : 0;
   x->cs.fold_grad = (kind == 3) ? 1 : 0;
   // the captured chains hold the previous gradient kernel
+  if (x->graph) { CK(cudaGraphExecDestroy(x->graph)); x->graph = nullptr; }
+  if (x->host_graph) { CK(cudaGraphExecDestroy(x->host_graph)); x->host_graph = nullptr; }
+  API_END
+}
+
+int fcfd_ctx_set_launch_overlap(fcfd_ctx *x, int32_t on) {
+  API_BEGIN
+  if (!x) throw Error(FCFD_ERR_INPUT, "null context");
+  x->pdl = on != 0;
   if (x->graph) { CK(cudaGraphExecDestroy(x->graph)); x->graph = nullptr; }
   if (x->host_graph) { CK(cudaGraphExecDestroy(x->host_graph)); x->host_graph = nullptr; }
   API_END

@@ -183,6 +183,16 @@ template <class T> __host__ __device__ __forceinline__ T tan_of(const Dual<T> &x
     }                                                 \
   } while (0)
 
+// Programmatic dependent launch.  A kernel launched with the programmatic
+// stream-serialization attribute may be scheduled while its predecessor in
+// the stream is still running: pdl_wait() blocks until every prerequisite grid
+// has completed and its writes are visible (a no-op for an ordinary launch),
+// so each kernel of the residual chain calls it before touching any array;
+// pdl_trigger() lets the successor be scheduled as this grid's last blocks
+// run, so its launch overlaps this kernel's tail.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 template <class S> __host__ __device__ __forceinline__ S smax(const S &a, const S &b) { return (a < b) ? b : a; }
 template <class S> __host__ __device__ __forceinline__ S smin(const S &a, const S &b) { return (b < a) ? b : a; }
 
@@ -537,6 +547,8 @@ __device__ __forceinline__ double okey_inv(unsigned long long k) {
 // min v, max p over cells < nc-1, min p over cells < nc-1 (ordered keys).
 template <class S>
 __global__ void k_ghost_minmax(DevCase cs, DevMesh m, S *__restrict__ W, unsigned long long *__restrict__ ext, int *err) {
+  pdl_wait();
+  pdl_trigger();
   const int nt = m.nt;
   const int nbl = n_ghost_threads(m);
   const int ghost_blocks = (nbl + blockDim.x - 1) / blockDim.x;
@@ -933,6 +945,8 @@ template <class S, bool FAST, bool PART = false>
 __global__ void __launch_bounds__(128, (!FAST && std::is_same<S, double>::value) ? 6 : 1) k_grad_limiter(DevCase cs, DevMesh m, const S *__restrict__ W,
                                                       const unsigned long long *__restrict__ ext, const int *__restrict__ argx,
                                                       S *__restrict__ G, S *__restrict__ Lm) {
+  pdl_wait();
+  pdl_trigger();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   // PART: one rank's gradient cells of a domain decomposition
   int c = i;
@@ -959,6 +973,8 @@ __global__ void __launch_bounds__(kGradTile) k_grad_limiter_tile(DevCase cs, Dev
                                                                  const unsigned long long *__restrict__ ext,
                                                                  double *__restrict__ G, double *__restrict__ Lm) {
   extern __shared__ double tile_smem[];
+  pdl_wait();
+  pdl_trigger();
   const int t = blockIdx.x, nt = m.nt;
   const int s0 = m.tile_off[t], ns = m.tile_off[t + 1] - s0;
   double *sW = tile_smem, *sX = tile_smem + 5 * ns;
@@ -991,6 +1007,8 @@ __global__ void __launch_bounds__(64) k_grad_limiter_pair(DevCase cs, DevMesh m,
                                                           const unsigned long long *__restrict__ ext,
                                                           double *__restrict__ G, double *__restrict__ Lm) {
   __shared__ double part[2][15][32];
+  pdl_wait();
+  pdl_trigger();
   const int lane = threadIdx.x & 31, h = threadIdx.x >> 5;
   const int nc = m.nc, nt = m.nt;
   const int ncell = PART ? m.n_part_cells : nc;
@@ -1568,6 +1586,8 @@ __global__ void __launch_bounds__(128) k_face_flux(DevCase cs, DevMesh m, const 
                                                    const S *__restrict__ Lm, S *stale,
                                                    const S *__restrict__ mu_t, S *__restrict__ D, S *__restrict__ mdot_out,
                                                    S *__restrict__ wl_out, int *err) {
+  pdl_wait();
+  pdl_trigger();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int nf = m.nf;
   // main launch: face_list when viscous (faces grouped by kind: an interior
@@ -1621,6 +1641,7 @@ __device__ __forceinline__ void reset_extrema(unsigned long long *ext, int *argx
 // next chain (every reader of them has finished by now on this stream).
 template <class S, bool AOS>
 __global__ void k_gather(DevMesh m, const S *__restrict__ D, S *__restrict__ R, unsigned long long *ext, int *argx) {
+  pdl_wait();
   reset_extrema(ext, argx);
   // one thread per (cell, equation): 5 nc threads, equation-major so that a
   // warp covers consecutive cells of one equation

@@ -182,6 +182,11 @@ class NavierStokes:
         """0 automatic, 1 per cell, 2 shared-memory tiles of 128 cells."""
         check(lib.fcfd_ctx_set_gradient_kernel(self.h, int(kind)))
 
+    def set_launch_overlap(self, on: bool):
+        """Programmatic dependent launches for the residual chain's gradient
+        and face kernels (default on); the results are the same bits."""
+        check(lib.fcfd_ctx_set_launch_overlap(self.h, int(bool(on))))
+
     def gradient_info(self):
         """dict(kind=1 per cell | 2 tiles | 3 folded stencils, fold_entries,
         fused) of the gradient kernel the residual runs."""

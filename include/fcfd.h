@@ -156,6 +156,13 @@ int fcfd_ctx_set_exact_gradients(fcfd_ctx *ctx, int exact);
  * kind the mesh does not have. */
 int fcfd_ctx_set_gradient_kernel(fcfd_ctx *ctx, int kind);
 
+/* on = 1 (the default): the residual chain's gradient and face kernels are
+ * programmatic dependent launches, scheduled while their predecessor in the
+ * stream finishes and waiting on the device for its results, so a
+ * kernel boundary costs less than a full drain and launch; 0: ordinary
+ * launches.  The results are the same bits either way. */
+int fcfd_ctx_set_launch_overlap(fcfd_ctx *ctx, int32_t on);
+
 /* The gradient kernel the residual runs: out[0] = 1 per cell, 2 tiles, 3
  * per cell over folded stencils; out[1] = folded stencil entries (0 if not
  * built); out[2] = 1 for the fused (continuous-limiter) gradient, 0 for the

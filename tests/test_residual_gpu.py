@@ -192,6 +192,30 @@ def test_determinism_and_device_pointers(oracle_mod, fb):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("family", ["cylinder", "wedge", "hypersonic", "plate"])
+def test_launch_overlap_same_bits(family, oracle_mod, fb):
+    """Programmatic dependent launches of the gradient and face kernels (the
+    default) and ordinary launches give the same residual bits, through the
+    direct chain and through the pinned-buffer graph."""
+    import torch
+    case = SMALL[family]()
+    o, cs, m, ns = _ctx(case, oracle_mod, fb)
+    Wp = torch.empty((m.nc, 5), dtype=torch.float64, pin_memory=True)
+    Rp = torch.empty((m.nc, 5), dtype=torch.float64, pin_memory=True)
+    Wp.numpy()[:] = case.state
+    out = {}
+    for on in (True, False, True):
+        ns.set_launch_overlap(on)
+        r = ns.residual(case.state)
+        ns.residual(Wp.numpy(), Rp.numpy())
+        assert np.array_equal(Rp.numpy(), r)
+        if on in out:
+            assert np.array_equal(out[on], r)
+        out[on] = r
+    assert np.array_equal(out[True], out[False])
+
+
+@pytest.mark.gpu
 def test_pinned_host_buffers(oracle_mod, fb):
     """Page-locked W and R take the one-graph path (copies, chain and error
     flag replayed as a CUDA graph): same bits as pageable buffers, for a new
