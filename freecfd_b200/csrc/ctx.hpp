@@ -151,14 +151,14 @@ constexpr int kExtremaBlocks = 296;  // 2 x 148 SMs
 // scheduled before its stream predecessor completes and waits for it in
 // pdl_wait()).
 template <class... KP, class... A>
-inline void launch_k(bool pdl, void (*k)(KP...), int grid, int block, size_t smem, cudaStream_t s, A... args) {
+inline void launch_k(bool pdl, void (*k)(KP...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, A... args) {
   if (!pdl) {
     k<<<grid, block, smem, s>>>(args...);
     return;
   }
   cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(grid);
-  cfg.blockDim = dim3(block);
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
   cfg.dynamicSmemBytes = smem;
   cfg.stream = s;
   cudaLaunchAttribute at[1];

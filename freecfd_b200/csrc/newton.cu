@@ -418,6 +418,10 @@ template <class P>
 __global__ void __launch_bounds__(160) k_gs_rows(int nc, int deg, int cnt, const int *__restrict__ cells,
                                                  const int *__restrict__ nbr, const P *__restrict__ OB,
                                                  const P *__restrict__ MinvP, const P *__restrict__ r, P *__restrict__ y) {
+  // consecutive colour updates are programmatic dependent launches: wait for
+  // the previous colour's writes, let the next colour's launch overlap this tail
+  pdl_wait();
+  pdl_trigger();
   const int i = blockIdx.x * 32 + threadIdx.x, q = threadIdx.y;
   __shared__ P ts[5][32];
   const bool act = i < cnt;
@@ -1188,8 +1192,10 @@ static void apply_prec(fcfd_ctx *x, NewtonState &ns, const T *v, T *z, int sweep
           if (cnt <= 0 || col == last) continue;
           last = col;
           const size_t base = (size_t)ci[col];
-          k_gs_rows<<<(cnt + 31) / 32, dim3(32, 5), 0, s>>>(
-              nc, deg, cnt, x->color_cells.p + base, x->gs_nbr.p + base * deg, OB + base * deg * 25, MinvP + base * 25, r, a);
+          launch_k(x->pdl, k_gs_rows<std::remove_const_t<std::remove_pointer_t<decltype(a)>>>, dim3((cnt + 31) / 32),
+                   dim3(32, 5), 0, s, nc, deg, cnt, (const int *)(x->color_cells.p + base),
+                   (const int *)(x->gs_nbr.p + base * deg), (const decltype(+*a) *)(OB + base * deg * 25),
+                   (const decltype(+*a) *)(MinvP + base * 25), (const decltype(+*a) *)r, a);
         }
     }
   };
