@@ -38,7 +38,8 @@ void launch_chain(fcfd_ctx *x, Pipe<S> &P, S *Rout, bool aos_out, S *mo, S *wo, 
   // previous chain's gather)
   const bool need_ext = x->cs.limiter == 1 && x->cs.order != 1;
   const int ng = (m.nb + tb - 1) / tb + (need_ext ? kExtremaBlocks : 0);
-  if (ng > 0) k_ghost_minmax<S><<<ng, tb, 0, s>>>(x->cs, m, P.W.p, need_ext ? x->ext.p : nullptr, x->err.p);
+  if (ng > 0)
+    launch_k(x->pdl, k_ghost_minmax<S>, ng, tb, 0, s, x->cs, m, P.W.p, need_ext ? x->ext.p : nullptr, x->err.p);
   const int *argx = nullptr;
   if (!std::is_same<S, double>::value && x->cs.limiter == 1 && x->cs.order != 1) {
     k_argext<S><<<(m.nc + tb - 1) / tb, tb, 0, s>>>(m, P.W.p, x->ext.p, x->argx.p);

@@ -301,6 +301,8 @@ __global__ void k_ilu_diag(DevCase cs, DevMesh m, const double *__restrict__ Wn,
 template <class T>
 __global__ void k_precond(int nc, const double *__restrict__ Minv, const T *__restrict__ x, T *__restrict__ z,
                           const RowScale *__restrict__ rs) {
+  pdl_wait();
+  pdl_trigger();
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= nc) return;
   double xv[5];
@@ -322,6 +324,8 @@ template <class T, class P>
 __global__ void k_precond_split(int nc, const double *__restrict__ Minv, const T *__restrict__ v,
                                 const RowScale *__restrict__ rs, P *__restrict__ r, P *__restrict__ y,
                                 unsigned *bar = nullptr) {
+  pdl_wait();
+  pdl_trigger();
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (bar && c == 0) bar[0] = 0u;
   if (c >= nc) return;
@@ -649,6 +653,8 @@ __device__ __forceinline__ double fd_eps(const double *eps_p, const double *zz) 
 template <class T>
 __global__ void k_load_state(int nc, int nt, const double *__restrict__ Wn, const T *__restrict__ dir,
                              const double *__restrict__ eps_num, const double *__restrict__ zz, double *__restrict__ W) {
+  pdl_wait();
+  pdl_trigger();
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= nc) return;
   const double eps = dir ? fd_eps(eps_num, zz) : 0.;
@@ -657,6 +663,8 @@ __global__ void k_load_state(int nc, int nt, const double *__restrict__ Wn, cons
 }
 template <class T, class D>
 __global__ void k_load_dual(int nc, int nt, const double *__restrict__ Wn, const T *__restrict__ dir, Dual<D> *__restrict__ W) {
+  pdl_wait();
+  pdl_trigger();
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= nc) return;
 #pragma unroll
@@ -669,6 +677,8 @@ __global__ void k_matvec_finish(DevCase cs, int nc, const double *__restrict__ W
                                 const double *__restrict__ dt, const T *__restrict__ z, const double *__restrict__ R1,
                                 const double *__restrict__ R0, const IterConsts *__restrict__ ic, const double *__restrict__ zz,
                                 const Dual<D> *__restrict__ JV, T *__restrict__ y) {
+  pdl_wait();
+  pdl_trigger();
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= nc) return;
   const double inv_eps = JV ? 0. : 1. / fd_eps(&ic->eps_num, zz);
@@ -695,6 +705,8 @@ __device__ void last_block_sum(int nparts, const double *part, double *__restric
 template <class T>
 __global__ void k_dots(int n, int nv, const T *__restrict__ V, size_t ld, const T *__restrict__ w, double *__restrict__ part,
                        double *__restrict__ out = nullptr, unsigned *__restrict__ count = nullptr) {
+  pdl_wait();
+  pdl_trigger();
   // part[v*gridDim.x + block] = sum over this block's slice of V_v . w; with
   // counters (one per column, blockDim == 256) the column's last block also
   // writes out[v]
@@ -715,6 +727,8 @@ __global__ void k_dots(int n, int nv, const T *__restrict__ V, size_t ld, const 
   (void)nv;
 }
 __global__ void k_sum_parts(int nparts, const double *__restrict__ part, double *__restrict__ out) {
+  pdl_wait();
+  pdl_trigger();
   const int v = blockIdx.x;
   double s = 0.;
   for (int i = threadIdx.x; i < nparts; i += blockDim.x) s += part[v * nparts + i];
@@ -731,6 +745,8 @@ __global__ void k_sum_parts(int nparts, const double *__restrict__ part, double 
 // w -= sum_v h[v] V_v
 template <class T>
 __global__ void k_sub_combo(int n, int nv, const T *__restrict__ V, size_t ld, const double *__restrict__ h, T *__restrict__ w) {
+  pdl_wait();
+  pdl_trigger();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   double s = double(w[i]);
@@ -740,6 +756,8 @@ __global__ void k_sub_combo(int n, int nv, const T *__restrict__ V, size_t ld, c
 // out = sum_v y[v] V_v
 template <class T>
 __global__ void k_combo(int n, int nv, const T *__restrict__ V, size_t ld, const double *__restrict__ y, T *__restrict__ out) {
+  pdl_wait();
+  pdl_trigger();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   double s = 0.;
@@ -748,17 +766,23 @@ __global__ void k_combo(int n, int nv, const T *__restrict__ V, size_t ld, const
 }
 template <class T>
 __global__ void k_scale_copy(int n, const double *__restrict__ a, double alpha, T *__restrict__ b) {
+  pdl_wait();
+  pdl_trigger();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) b[i] = T(alpha * a[i]);
 }
 template <class T>
 __global__ void k_scale(int n, double alpha, T *__restrict__ b) {
+  pdl_wait();
+  pdl_trigger();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) b[i] = T(alpha * double(b[i]));
 }
 // W += alpha dW with a NaN/Inf check (update_variables, ns.cc:338-356)
 template <class T>
 __global__ void k_update(int n, double *__restrict__ Wn, const T *__restrict__ dW, double alpha, int *__restrict__ err) {
+  pdl_wait();
+  pdl_trigger();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const double d = double(dW[i]);
@@ -849,6 +873,8 @@ __device__ void last_block_sum(int nparts, const double *part, double *__restric
 template <class T>
 __global__ void k_wdot(int n, int nc, const T *__restrict__ z, const RowScale *__restrict__ winv, double *__restrict__ part,
                        double *__restrict__ out = nullptr, unsigned *__restrict__ count = nullptr) {
+  pdl_wait();
+  pdl_trigger();
   double s = 0.;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const double q = double(z[i]) * winv->s[i / nc];
@@ -869,6 +895,8 @@ __global__ void k_wdot(int n, int nc, const T *__restrict__ z, const RowScale *_
 
 template <class T>
 __global__ void k_scale_rsqrt(int n, const double *__restrict__ ss, T *__restrict__ b) {
+  pdl_wait();
+  pdl_trigger();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const double q = *ss;
   if (i < n && q > 0.) b[i] = T(double(b[i]) / sqrt(q));
@@ -918,7 +946,8 @@ struct Krylov {
   }
   // out[v] = Vb_v . u for v < nv in one launch (the column's last block adds the partials)
   void dots_fused(int nv, const T *Vb, const T *u, double *out) {
-    k_dots<T><<<dim3(nparts, nv), kFusedThreads, 0, x->stream>>>(n, nv, Vb, (size_t)n, u, part.p, out, count.p);
+    launch_k(x->pdl, k_dots<T>, dim3(nparts, nv), kFusedThreads, 0, x->stream, n, nv, Vb, (size_t)n, u, part.p, out,
+             count.p);
   }
   // bring hd back to the host (the one synchronisation of a GMRES iteration)
   void fetch_async() {
@@ -936,7 +965,7 @@ struct Krylov {
   // |S^-1 u|^2 on the device (S = per-variable reference magnitudes)
   void wnorm2_dev(const T *u, const RowScale *winv, double *out) {
     cudaStream_t s = x->stream;
-    k_wdot<T><<<nparts, kFusedThreads, 0, s>>>(n, nc, u, winv, part.p, out, count.p);
+    launch_k(x->pdl, k_wdot<T>, nparts, kFusedThreads, 0, s, n, nc, u, winv, part.p, out, count.p);
   }
   double norm64(const double *u) {
     cudaStream_t s = x->stream;
@@ -1090,11 +1119,15 @@ static void check_gs_timeout(fcfd_ctx *x, NewtonState &ns) {
 }
 template <class T>
 __global__ void k_axpy_to(int n, const double *__restrict__ b, const T *__restrict__ w, T *__restrict__ out) {
+  pdl_wait();
+  pdl_trigger();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) out[i] = T(b[i] - double(w[i]));
 }
 template <class T, class A = double>
 __global__ void k_cast(int n, const A *__restrict__ a, T *__restrict__ b) {
+  pdl_wait();
+  pdl_trigger();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) b[i] = T(a[i]);
 }
@@ -1104,7 +1137,7 @@ template <class T>
 static void eval_residual(fcfd_ctx *x, const double *Wn, double *R, const T *dir, const double *eps,
                           const double *zz = nullptr) {
   const DevMesh &m = x->dm;
-  k_load_state<T><<<(m.nc + 255) / 256, 256, 0, x->stream>>>(m.nc, m.nt, Wn, dir, eps, zz, x->p64.W.p);
+  launch_k(x->pdl, k_load_state<T>, (m.nc + 255) / 256, 256, 0, x->stream, m.nc, m.nt, Wn, dir, eps, zz, x->p64.W.p);
   launch_chain<double>(x, x->p64, R, false, nullptr, nullptr);
 }
 
@@ -1131,19 +1164,21 @@ static void matvec(fcfd_ctx *x, NewtonState &ns, int mode, const T *z, T *y, con
   prepare_matvec(x, mode);
   if (mode == 0) {
     eval_residual<T>(x, ns.Wn.p, ns.R1.p, z, &ns.ic.p->eps_num, zz);
-    k_matvec_finish<T, double><<<gb, tb, 0, s>>>(x->cs, m.nc, ns.Wn.p, ns.vol.p, ns.dt.p, z, ns.R1.p, ns.R0.p, ns.ic.p, zz,
-                                                 (const Dual<double> *)nullptr, y);
+    launch_k(x->pdl, k_matvec_finish<T, double>, gb, tb, 0, s, x->cs, m.nc, ns.Wn.p, ns.vol.p, ns.dt.p, z, ns.R1.p,
+             ns.R0.p, ns.ic.p, zz, (const Dual<double> *)nullptr, y);
   } else {
     if (x->newton_f32) {
-      k_load_dual<T, float><<<gb, tb, 0, s>>>(m.nc, m.nt, ns.Wn.p, z, x->pjv32.W.p);
+      launch_k(x->pdl, k_load_dual<T, float>, gb, tb, 0, s, m.nc, m.nt, ns.Wn.p, z, x->pjv32.W.p);
       launch_chain<Dual<float>>(x, x->pjv32, x->pjv32.R.p, false, nullptr, nullptr, x->newton_frozen);
-      k_matvec_finish<T, float><<<gb, tb, 0, s>>>(x->cs, m.nc, ns.Wn.p, ns.vol.p, ns.dt.p, z, nullptr, nullptr, ns.ic.p,
-                                                  nullptr, x->pjv32.R.p, y);
+      launch_k(x->pdl, k_matvec_finish<T, float>, gb, tb, 0, s, x->cs, m.nc, ns.Wn.p, ns.vol.p, ns.dt.p, z,
+               (const double *)nullptr, (const double *)nullptr, ns.ic.p, (const double *)nullptr,
+               (const Dual<float> *)x->pjv32.R.p, y);
     } else {
-      k_load_dual<T, double><<<gb, tb, 0, s>>>(m.nc, m.nt, ns.Wn.p, z, x->pjv.W.p);
+      launch_k(x->pdl, k_load_dual<T, double>, gb, tb, 0, s, m.nc, m.nt, ns.Wn.p, z, x->pjv.W.p);
       launch_chain<Dual<double>>(x, x->pjv, x->pjv.R.p, false, nullptr, nullptr, x->newton_frozen);
-      k_matvec_finish<T, double><<<gb, tb, 0, s>>>(x->cs, m.nc, ns.Wn.p, ns.vol.p, ns.dt.p, z, nullptr, nullptr, ns.ic.p,
-                                                   nullptr, x->pjv.R.p, y);
+      launch_k(x->pdl, k_matvec_finish<T, double>, gb, tb, 0, s, x->cs, m.nc, ns.Wn.p, ns.vol.p, ns.dt.p, z,
+               (const double *)nullptr, (const double *)nullptr, ns.ic.p, (const double *)nullptr,
+               (const Dual<double> *)x->pjv.R.p, y);
     }
   }
   CK(cudaGetLastError());
@@ -1168,7 +1203,7 @@ static void apply_prec(fcfd_ctx *x, NewtonState &ns, const T *v, T *z, int sweep
   cudaStream_t s = x->stream;
   const RowScale *rs = &ns.ic.p->rs;
   if (sweeps <= 0) {
-    k_precond<T><<<gc, tb, 0, s>>>(nc, ns.Minv.p, v, z, rs);
+    launch_k(x->pdl, k_precond<T>, gc, tb, 0, s, nc, (const double *)ns.Minv.p, v, z, rs);
     return;
   }
   // r = D^-1 v, y0 = Binv r; then symmetric multicolour block Gauss-Seidel:
@@ -1204,15 +1239,15 @@ static void apply_prec(fcfd_ctx *x, NewtonState &ns, const T *v, T *z, int sweep
     using P = std::remove_pointer_t<decltype(y)>;
     unsigned *bar = ns.gs_persist ? ns.gs_bar.p : nullptr;
     if constexpr (std::is_same_v<P, T>) {
-      k_precond_split<T, P><<<gc, tb, 0, s>>>(nc, ns.Minv.p, v, rs, r, z, bar);
+      launch_k(x->pdl, k_precond_split<T, P>, gc, tb, 0, s, nc, (const double *)ns.Minv.p, v, rs, r, z, bar);
       // ILU(0): the forward colour sweep starts from y = 0
       if (ns.ilu) CK(cudaMemsetAsync(z, 0, sizeof(P) * 5 * (size_t)nc, s));
       sweep(OB, MinvP, r, z);
     } else {
-      k_precond_split<T, P><<<gc, tb, 0, s>>>(nc, ns.Minv.p, v, rs, r, y, bar);
+      launch_k(x->pdl, k_precond_split<T, P>, gc, tb, 0, s, nc, (const double *)ns.Minv.p, v, rs, r, y, bar);
       if (ns.ilu) CK(cudaMemsetAsync(y, 0, sizeof(P) * 5 * (size_t)nc, s));
       sweep(OB, MinvP, r, y);
-      k_cast<T, P><<<(5 * nc + tb - 1) / tb, tb, 0, s>>>(5 * nc, y, z);
+      launch_k(x->pdl, k_cast<T, P>, (5 * nc + tb - 1) / tb, tb, 0, s, 5 * nc, (const P *)y, z);
     }
   };
   if (ns.prec32)
@@ -1269,11 +1304,11 @@ static void gmres(fcfd_ctx *x, NewtonState &ns, Krylov<T> &K, int mode, double r
         matvec<T>(x, ns, mode, K.tmpT.p, w, K.zz());
         // classical Gram-Schmidt twice, coefficients kept on the device
         K.dots_fused(j + 1, K.V.p, w, K.h1());
-        k_sub_combo<T><<<gn, tb, 0, s>>>(n, j + 1, K.V.p, (size_t)n, K.h1(), w);
+        launch_k(x->pdl, k_sub_combo<T>, gn, tb, 0, s, n, j + 1, (const T *)K.V.p, (size_t)n, (const double *)K.h1(), w);
         K.dots_fused(j + 1, K.V.p, w, K.h2());
-        k_sub_combo<T><<<gn, tb, 0, s>>>(n, j + 1, K.V.p, (size_t)n, K.h2(), w);
+        launch_k(x->pdl, k_sub_combo<T>, gn, tb, 0, s, n, j + 1, (const T *)K.V.p, (size_t)n, (const double *)K.h2(), w);
         K.dots_fused(1, w, w, K.ww());
-        k_scale_rsqrt<T><<<gn, tb, 0, s>>>(n, K.ww(), w);
+        launch_k(x->pdl, k_scale_rsqrt<T>, gn, tb, 0, s, n, (const double *)K.ww(), w);
         K.fetch_async();
         CK(cudaStreamEndCapture(s, &gr));
         CK(cudaGraphInstantiate(&K.graphs[j], gr, 0));

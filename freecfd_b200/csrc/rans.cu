@@ -63,6 +63,8 @@ __device__ __forceinline__ S face_avg(const DevMesh &m, int f, const S *x) {
 template <class S>
 __global__ void k_rans_prep(DevCase cs, DevMesh m, const S *__restrict__ W, S *__restrict__ K,
                             S *__restrict__ mut, double ratio_limit) {
+  pdl_wait();
+  pdl_trigger();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int nc = m.nc, nt = m.nt;
   if (i >= nt) return;
@@ -78,6 +80,8 @@ __global__ void k_rans_prep(DevCase cs, DevMesh m, const S *__restrict__ W, S *_
 // mu_t.face (variable.h:134-147): the BC value where fixed, else the average.
 template <class S>
 __global__ void k_rans_mutf(DevCase cs, DevMesh m, const S *__restrict__ mut, S *__restrict__ mutf) {
+  pdl_wait();
+  pdl_trigger();
   const int f = blockIdx.x * blockDim.x + threadIdx.x;
   if (f >= m.nf) return;
   const int b = m.f_bc[f];
@@ -88,6 +92,8 @@ __global__ void k_rans_mutf(DevCase cs, DevMesh m, const S *__restrict__ mut, S 
 // the same weights as the flow gradients in their fused form.
 template <class S>
 __global__ void k_rans_grad(DevMesh m, const S *__restrict__ K, S *__restrict__ GK) {
+  pdl_wait();
+  pdl_trigger();
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   const int nc = m.nc, nt = m.nt;
   if (c >= nc) return;
@@ -139,6 +145,8 @@ template <class S>
 __global__ void k_rans_face(DevCase cs, DevMesh m, const S *__restrict__ W, const S *__restrict__ K,
                             const S *__restrict__ GK, const S *__restrict__ mutf,
                             const S *__restrict__ mdot, const S *__restrict__ wl, S *__restrict__ DK) {
+  pdl_wait();
+  pdl_trigger();
   const int f = blockIdx.x * blockDim.x + threadIdx.x;
   const int nf = m.nf, nc = m.nc, nt = m.nt;
   if (f >= nf) return;
@@ -161,6 +169,8 @@ template <class S>
 __global__ void k_rans_gather(DevCase cs, DevMesh m, const S *__restrict__ W, const S *__restrict__ K,
                               const S *__restrict__ G, const S *__restrict__ mut,
                               const double *__restrict__ vol, const S *__restrict__ DK, S *__restrict__ RK) {
+  pdl_wait();
+  pdl_trigger();
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   const int nc = m.nc, nt = m.nt, nf = m.nf;
   if (c >= nc) return;
@@ -293,15 +303,19 @@ static void rans_chain(fcfd_ctx *x, Pipe<S> &P, RansBuf<S> &s, S *mdot, S *wl, S
     k_argext<S><<<(m.nc + tb - 1) / tb, tb, 0, st>>>(m, P.W.p, x->ext.p, x->argx.p);
     argx = x->argx.p;
   }
-  k_rans_prep<S><<<(m.nt + 127) / 128, 128, 0, st>>>(x->cs, m, P.W.p, s.K.p, s.mut.p, x->case_ptr->visc_ratio_limit);
-  k_rans_mutf<S><<<(m.nf + 127) / 128, 128, 0, st>>>(x->cs, m, s.mut.p, s.mutf.p);
-  launch_grad_limiter<S>(x->cs, m, P.W.p, x->ext.p, argx, P.G.p, P.Lm.p, st);
+  const bool pdl = x->pdl;
+  launch_k(pdl, k_rans_prep<S>, (m.nt + 127) / 128, 128, 0, st, x->cs, m, (const S *)P.W.p, s.K.p, s.mut.p,
+           x->case_ptr->visc_ratio_limit);
+  launch_k(pdl, k_rans_mutf<S>, (m.nf + 127) / 128, 128, 0, st, x->cs, m, (const S *)s.mut.p, s.mutf.p);
+  launch_grad_limiter<S>(x->cs, m, P.W.p, x->ext.p, argx, P.G.p, P.Lm.p, st, pdl);
   launch_faces<S>(x, P, s.mutf.p, mdot, wl, st);
   k_gather<S, AOS><<<(5 * m.nc + tb - 1) / tb, tb, 0, st>>>(m, P.D.p, R, x->ext.p, x->argx.p);
   if (ev) CK(cudaEventRecord(ev[1], st));
-  k_rans_grad<S><<<(m.nc + 127) / 128, 128, 0, st>>>(m, s.K.p, s.GK.p);
-  k_rans_face<S><<<(m.nf + 127) / 128, 128, 0, st>>>(x->cs, m, P.W.p, s.K.p, s.GK.p, s.mutf.p, mdot, wl, s.DK.p);
-  k_rans_gather<S><<<(m.nc + 127) / 128, 128, 0, st>>>(x->cs, m, P.W.p, s.K.p, P.G.p, s.mut.p, x->rans->vol.p, s.DK.p, RK);
+  launch_k(pdl, k_rans_grad<S>, (m.nc + 127) / 128, 128, 0, st, m, (const S *)s.K.p, s.GK.p);
+  launch_k(pdl, k_rans_face<S>, (m.nf + 127) / 128, 128, 0, st, x->cs, m, (const S *)P.W.p, (const S *)s.K.p,
+           (const S *)s.GK.p, (const S *)s.mutf.p, (const S *)mdot, (const S *)wl, s.DK.p);
+  launch_k(pdl, k_rans_gather<S>, (m.nc + 127) / 128, 128, 0, st, x->cs, m, (const S *)P.W.p, (const S *)s.K.p,
+           (const S *)P.G.p, (const S *)s.mut.p, (const double *)x->rans->vol.p, (const S *)s.DK.p, RK);
   if (ev) CK(cudaEventRecord(ev[2], st));
   CK(cudaGetLastError());
 }
