@@ -513,10 +513,18 @@ constexpr int kNv = 7;
 constexpr int kRedBlk = 592;  // 4 x 148 blocks for the reductions
 
 // X (SoA [7][nc]) + eps z -> the chain's W [5][nt] and K [2][nt] (interiors)
+// finite-difference step of the Krylov matvec, eps_num / |z| with |z|^2 read
+// from the device (1e-8 where |z| = 0)
+__device__ __forceinline__ double kw_fd_eps(double eps_num, const double *zz) {
+  const double q = *zz;
+  return q > 0. ? eps_num / sqrt(q) : 1e-8;
+}
 __global__ void k_x_load(int nc, int nt, const double *__restrict__ X, const double *__restrict__ z, double eps,
-                         double *__restrict__ W, double *__restrict__ K) {
+                         double *__restrict__ W, double *__restrict__ K, double eps_num = 0.,
+                         const double *__restrict__ zz = nullptr) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= nc) return;
+  if (zz) eps = kw_fd_eps(eps_num, zz);
 #pragma unroll
   for (int v = 0; v < 5; ++v) W[v * nt + c] = X[v * nc + c] + (z ? eps * z[v * nc + c] : 0.);
 #pragma unroll
@@ -560,9 +568,11 @@ struct Wt7 {
 };
 __global__ void k_kw_matvec(DevCase cs, int nc, const double *__restrict__ X, const double *__restrict__ vol,
                             const double *__restrict__ dt, const double *__restrict__ z, const double *__restrict__ F1,
-                            const double *__restrict__ F0, double inv_eps, Wt7 wr, double *__restrict__ y) {
+                            const double *__restrict__ F0, double inv_eps, Wt7 wr, double *__restrict__ y,
+                            double eps_num = 0., const double *__restrict__ zz = nullptr) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= nc) return;
+  if (zz) inv_eps = 1. / kw_fd_eps(eps_num, zz);
   const double p = X[c], u = X[nc + c], v = X[2 * nc + c], w = X[3 * nc + c], T = X[4 * nc + c];
   const double pressure = p + cs.Pref, temperature = T + cs.Tref;
   const double rho = pressure / (cs.R * temperature);
@@ -640,8 +650,35 @@ __global__ void k_kw_prec(int nc, const double *__restrict__ Minv, const double 
 }
 
 // part[j * gridDim.x + b] = block b's share of V_j . w (j < nv)
+// The column's last block adds its partials (in block order, strided over
+// the block's threads) and re-arms the column's counter.
+__device__ void kw_last_block_sum(int nparts, const double *part, double *__restrict__ out, unsigned *__restrict__ count) {
+  __shared__ unsigned ticket;
+  __shared__ double shs[8];
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) ticket = atomicAdd(count, 1u);
+  __syncthreads();
+  if (ticket != (unsigned)nparts - 1u) return;
+  __threadfence();
+  double s = 0.;
+  for (int i = threadIdx.x; i < nparts; i += blockDim.x) s += __ldcg(part + i);
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) shs[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.;
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) t += shs[k];
+    *out = t;
+    *count = 0u;
+  }
+}
+// part[j][block] = this block's share of V_j . w; with out and count (one
+// counter per column, 256-thread blocks) the column's last block also writes
+// out[j], so the sums stay on the device
 __global__ void k_kw_dots(int n, int nv, const double *__restrict__ V, size_t ld, const double *__restrict__ w,
-                          double *__restrict__ part) {
+                          double *__restrict__ part, double *__restrict__ out = nullptr,
+                          unsigned *__restrict__ count = nullptr) {
   const int j = blockIdx.y;
   const double *a = V + (size_t)j * ld;
   double s = 0.;
@@ -655,6 +692,13 @@ __global__ void k_kw_dots(int n, int nv, const double *__restrict__ V, size_t ld
     for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
     if (threadIdx.x == 0) part[(size_t)j * gridDim.x + blockIdx.x] = t;
   }
+  if (count) kw_last_block_sum(gridDim.x, part + (size_t)j * gridDim.x, out + j, count + j);
+}
+// y = x / sqrt(*ss) where *ss > 0
+__global__ void k_kw_scale_rsqrt(int n, const double *__restrict__ ss, const double *__restrict__ x, double *__restrict__ y) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const double q = *ss;
+  if (i < n && q > 0.) y[i] = x[i] / sqrt(q);
 }
 
 // w -= sum_j h[j] V_j (h in device memory), then optionally out = w * scale
@@ -707,6 +751,17 @@ struct KwSolve {
   DBuf<double> X, Xsave, F0, F1, Jz, dt, vol, Minv, JL, JR, rowmag, dk, Vb, w, z, part, h, x, dX;
   DBuf<unsigned long long> key;
   std::vector<double> hpart;
+  // device-side Gram-Schmidt: coefficients h1[mdim+1], h2[mdim+1], |w|^2,
+  // |z|^2; one counter per dot-product column
+  DBuf<double> hd;
+  DBuf<unsigned> cnt;
+  std::vector<double> hh;
+  void alloc_gs(int mdim, cudaStream_t s) {
+    hd.alloc(2 * (size_t)(mdim + 1) + 2);
+    cnt.alloc((size_t)mdim + 1);
+    CK(cudaMemsetAsync(cnt.p, 0, sizeof(unsigned) * (mdim + 1), s));
+    hh.resize(hd.n);
+  }
 };
 
 // sum of the per-block partials of nv dot products, in block order (host)
@@ -807,31 +862,34 @@ static int kw_linear_step(fcfd_ctx *x, KwSolve &S, int mdim, int mode, double kr
       double *vj = S.Vb.p + (size_t)j * n;
       // z = M^-1 v_j, then w = wr (D z - J z)
       k_kw_prec<<<gc, 256, 0, s>>>(nc, S.Minv.p, S.dk.p, iwr, vj, S.z.p);
+      // the Gram-Schmidt coefficients, |w|^2 and |z|^2 stay on the device
+      // (fused dot products); one copy back and one synchronisation per step
+      double *h1 = S.hd.p, *h2 = S.hd.p + (mdim + 1), *hw = S.hd.p + 2 * (mdim + 1), *zz = hw + 1;
       if (mode == 0) {
-        double zn;
-        kw_dots(x, S, n, 1, S.z.p, 0, S.z.p, &zn);
-        zn = std::sqrt(zn);
-        const double eps = zn > 0. ? 1.4901161193847656e-08 * (1. + xn) / zn : 1e-8;
-        kw_residual(x, S.X.p, S.z.p, eps, S.F1.p);
-        k_kw_matvec<<<gc, 256, 0, s>>>(x->cs, nc, S.X.p, S.vol.p, S.dt.p, S.z.p, S.F1.p, S.F0.p, 1. / eps, wr, S.w.p);
+        // eps = sqrt(eps_mach) (1 + |S^-1 X|) / |z|, |z| read on the device
+        const double eps_num = 1.4901161193847656e-08 * (1. + xn);
+        k_kw_dots<<<dim3(kRedBlk, 1), 256, 0, s>>>(n, 1, S.z.p, 0, S.z.p, S.part.p, zz, S.cnt.p);
+        k_x_load<<<gc, 256, 0, s>>>(m.nc, m.nt, S.X.p, S.z.p, 0., x->p64.W.p, x->rans->b.K.p, eps_num, zz);
+        rans_chain<double, false>(x, x->p64, x->rans->b, x->mdot.p, x->wl.p, S.F1.p, x->rans->b.RK.p);
+        k_rk_planes<<<gc, 256, 0, s>>>(m.nc, x->rans->b.RK.p, S.F1.p);
+        k_kw_matvec<<<gc, 256, 0, s>>>(x->cs, nc, S.X.p, S.vol.p, S.dt.p, S.z.p, S.F1.p, S.F0.p, 0., wr, S.w.p, eps_num,
+                                        zz);
       } else {
         kw_tangent32(x, S.X.p, S.z.p, S.Jz.p);
         k_kw_matvec<<<gc, 256, 0, s>>>(x->cs, nc, S.X.p, S.vol.p, S.dt.p, S.z.p, S.Jz.p, nullptr, 0., wr, S.w.p);
       }
       // classical Gram-Schmidt, twice
-      std::vector<double> hc(j + 1, 0.), hh(j + 1);
-      for (int pass = 0; pass < 2; ++pass) {
-        kw_dots(x, S, n, j + 1, S.Vb.p, (size_t)n, S.w.p, hh.data());
-        CK(cudaMemcpyAsync(S.h.p, hh.data(), sizeof(double) * (j + 1), cudaMemcpyHostToDevice, s));
-        k_kw_sub<<<gn, 256, 0, s>>>(n, j + 1, S.Vb.p, (size_t)n, S.h.p, S.w.p);
-        for (int i = 0; i <= j; ++i) hc[i] += hh[i];
-      }
-      double hn;
-      kw_dots(x, S, n, 1, S.w.p, 0, S.w.p, &hn);
-      hn = std::sqrt(hn);
-      for (int i = 0; i <= j; ++i) H[(size_t)i * mdim + j] = hc[i];
+      k_kw_dots<<<dim3(kRedBlk, j + 1), 256, 0, s>>>(n, j + 1, S.Vb.p, (size_t)n, S.w.p, S.part.p, h1, S.cnt.p);
+      k_kw_sub<<<gn, 256, 0, s>>>(n, j + 1, S.Vb.p, (size_t)n, h1, S.w.p);
+      k_kw_dots<<<dim3(kRedBlk, j + 1), 256, 0, s>>>(n, j + 1, S.Vb.p, (size_t)n, S.w.p, S.part.p, h2, S.cnt.p);
+      k_kw_sub<<<gn, 256, 0, s>>>(n, j + 1, S.Vb.p, (size_t)n, h2, S.w.p);
+      k_kw_dots<<<dim3(kRedBlk, 1), 256, 0, s>>>(n, 1, S.w.p, 0, S.w.p, S.part.p, hw, S.cnt.p);
+      k_kw_scale_rsqrt<<<gn, 256, 0, s>>>(n, hw, S.w.p, S.Vb.p + (size_t)(j + 1) * n);
+      CK(cudaMemcpyAsync(S.hh.data(), S.hd.p, sizeof(double) * S.hd.n, cudaMemcpyDeviceToHost, s));
+      CK(cudaStreamSynchronize(s));
+      const double hn = std::sqrt(S.hh[2 * (mdim + 1)]);
+      for (int i = 0; i <= j; ++i) H[(size_t)i * mdim + j] = S.hh[i] + S.hh[mdim + 1 + i];
       H[(size_t)(j + 1) * mdim + j] = hn;
-      if (hn > 0.) k_kw_scale<<<gn, 256, 0, s>>>(n, 1. / hn, S.w.p, S.Vb.p + (size_t)(j + 1) * n);
       // Givens rotations of the new column
       for (int i = 0; i < j; ++i) {
         const double a = H[(size_t)i * mdim + j], b = H[(size_t)(i + 1) * mdim + j];
@@ -935,6 +993,7 @@ void *kw_driver_create(fcfd_ctx *x, const double *W, const double *K, int mdim) 
   S.rowmag.alloc(5 * (size_t)nc); S.dk.alloc(2 * (size_t)nc);
   S.Vb.alloc((size_t)(d->mdim + 1) * n); S.w.alloc(n); S.z.alloc(n); S.part.alloc((size_t)kRedBlk * (d->mdim + 1));
   S.h.alloc(d->mdim + 1); S.x.alloc(n); S.dX.alloc(n); S.key.alloc(2);
+  S.alloc_gs(d->mdim, s);
   std::vector<double> hx((size_t)n);
   for (int c = 0; c < nc; ++c) {
     for (int v = 0; v < 5; ++v) hx[(size_t)v * nc + c] = W[5 * (size_t)c + v];
@@ -1030,6 +1089,7 @@ extern "C" int fcfd_rans_newton_solve(fcfd_ctx *x, double *W, double *K, const f
     S.rowmag.alloc(5 * (size_t)nc); S.dk.alloc(2 * (size_t)nc);
     S.Vb.alloc((size_t)(mdim + 1) * n); S.w.alloc(n); S.z.alloc(n); S.part.alloc((size_t)kRedBlk * (mdim + 1));
     S.h.alloc(mdim + 1); S.x.alloc(n); S.dX.alloc(n); S.key.alloc(2);
+    S.alloc_gs(mdim, s);
     // X from the host's AoS W[nc][5], K[nc][2]
     {
       std::vector<double> hx((size_t)n);
