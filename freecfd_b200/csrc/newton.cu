@@ -1256,6 +1256,14 @@ static void apply_prec(fcfd_ctx *x, NewtonState &ns, const T *v, T *z, int sweep
     run(ns.OB.p, ns.MinvP.p, ns.Pr.p, ns.Py0.p);
 }
 
+// dW = NaN: the update of a step whose right-hand side is not finite, so
+// that the NaN check of the update reports the divergence (the reference's
+// linear solve propagates the NaN into its update, ns.cc:349-355)
+__global__ void k_fill_nan(int n, double *__restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = __longlong_as_double(0x7ff8000000000000ll);
+}
+
 // Right-preconditioned GMRES(m) with up to `cycles` restarts.
 template <class T>
 static void gmres(fcfd_ctx *x, NewtonState &ns, Krylov<T> &K, int mode, double rtol, double *dW, int &iters, double &relres,
@@ -1270,6 +1278,11 @@ static void gmres(fcfd_ctx *x, NewtonState &ns, Krylov<T> &K, int mode, double r
   k_rowscale_copy<<<gc, tb, 0, s>>>(nc, ns.R0.p, rs, 1., dW);
   const double bnorm = K.norm64(dW);
   CK(cudaMemsetAsync(ns.Xs.p, 0, sizeof(double) * n, s));
+  if (!std::isfinite(bnorm)) {
+    k_fill_nan<<<gn, tb, 0, s>>>(n, dW);
+    relres = bnorm;
+    return;
+  }
   if (!(bnorm > 0.)) { CK(cudaMemsetAsync(dW, 0, sizeof(double) * n, s)); relres = 0.; return; }
   std::vector<double> H((size_t)(m + 1) * m, 0.), cs(m), sn(m), g(m + 1, 0.);
   for (int cyc = 0; cyc < ns.cycles; ++cyc) {

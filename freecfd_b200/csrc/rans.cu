@@ -16,6 +16,7 @@
 #include <cstring>
 #include <vector>
 
+#include <limits>
 #include <memory>
 
 #include "ctx.hpp"
@@ -917,6 +918,10 @@ static int kw_linear_step(fcfd_ctx *x, KwSolve &S, int mdim, int mode, double kr
     CK(cudaMemcpyAsync(S.h.p, y.data(), sizeof(double) * kit, cudaMemcpyHostToDevice, s));
     k_kw_combo<<<gn, 256, 0, s>>>(n, kit, S.Vb.p, (size_t)n, S.h.p, S.x.p);
     k_kw_prec<<<gc, 256, 0, s>>>(nc, S.Minv.p, S.dk.p, iwr, S.x.p, S.dX.p);
+  } else if (!std::isfinite(beta)) {
+    // a non-finite right-hand side: a NaN update, which the update's NaN
+    // check reports as divergence (as the reference's NaN check would)
+    k_kw_scale<<<gn, 256, 0, s>>>(n, std::numeric_limits<double>::quiet_NaN(), S.w.p, S.dX.p);
   } else {
     CK(cudaMemsetAsync(S.dX.p, 0, sizeof(double) * n, s));
   }

@@ -307,3 +307,23 @@ def test_run_turbulent_plate_converges(oracle_mod, fb, tmp_path):
     print("oracle residual reduction per equation:", red)
     assert (red[:3] < 0.1).all() and red[4] < 2e-2, red
     assert rows[-1][4] < 1e-2 and rows[-1][6] < 0.5, rows[-1]
+
+
+@pytest.mark.gpu
+def test_run_reports_nonphysical_state_as_divergence(oracle_mod, fb, tmp_path):
+    """The impulsively started M = 8 cylinder at first order and CFL 0.5
+    leaves negative pressures after its first implicit step; the next
+    residual is then not finite, and the run ends with FCFD_ERR_DIVERGED
+    (the reference's NaN check, ns.cc:349-355) instead of marching on with
+    zero updates."""
+    case = cases.hypersonic_case(128, 64, ns_extra=" order=first;")
+    case.deck = case.deck.replace("time marching { CFLmax=1.e3; number of steps=500; ramp (initial=0.1; growth=1.1;); }",
+                                  "time marching { CFLmax=0.5; number of steps=20; }")
+    o, cs, m = build_pair(case, oracle_mod, fb)
+    ns = fb.NavierStokes(m, cs, 0)
+    W, rep = ns.run(case.state, work_dir=tmp_path, raise_on_fail=False)
+    assert rep["status"] == 3, rep
+    assert 1 <= rep["steps"] < 20
+    with pytest.raises(fb.FcfdError) as e:
+        ns.run(case.state, work_dir=tmp_path / "b" if (tmp_path / "b").mkdir() is None else tmp_path)
+    assert e.value.code == 3
