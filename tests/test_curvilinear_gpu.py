@@ -84,6 +84,32 @@ def test_curvilinear_rans_residual(oracle_mod, fb):
 
 
 @pytest.mark.gpu
+def test_curvilinear_rans_vjp_dot_product(oracle_mod, fb):
+    """Adjoint of the coupled k-omega residual on curvilinear maps (the flow
+    and the k, omega gradients' transposed maps use the stored weights):
+    <(Rbar, RKbar), J (V, VK)> with J (V, VK) from the oracle's complex step
+    equals <J^T (Rbar, RKbar), (V, VK)>."""
+    case = cases.plate_case(ni=24, nj=12, nk=3, turbulent=True, grad="curvilinear")
+    o, cs, m = build_pair(case, oracle_mod, fb)
+    ns = fb.NavierStokes(m, cs, 0)
+    W = case.state.copy()
+    rng = np.random.default_rng(43)
+    W[:, 2] = 0.02 * W[:, 1] * rng.uniform(-1.0, 1.0, W.shape[0])
+    K = case.kstate
+    for _ in range(2):
+        V = rng.standard_normal(W.shape) * np.abs(W).max(axis=0)
+        VK = rng.standard_normal(K.shape) * np.abs(K).max(axis=0)
+        dR, dRK = o.rans_residual_cstep(W, K, V, VK)
+        Rb = rng.standard_normal(W.shape)
+        RKb = rng.standard_normal(K.shape) * np.abs(dR).max() / np.abs(dRK).max()
+        Wb, Kb = ns.rans_vjp(W, K, Rb, RKb)
+        lhs = float((Rb * dR).sum() + (RKb * dRK).sum())
+        rhs = float((Wb * V).sum() + (Kb * VK).sum())
+        mag = float(np.abs(Rb * dR).sum() + np.abs(RKb * dRK).sum())
+        assert abs(lhs - rhs) <= 1e-11 * mag, (lhs, rhs, mag)
+
+
+@pytest.mark.gpu
 def test_curvilinear_newton_converges(oracle_mod, fb):
     """Laminar cylinder 64x32 with the default (curvilinear) hexahedron
     gradients, unlimited: the plain FP64 and mixed Newton arms reach a 1e-10

@@ -268,3 +268,27 @@ def test_rans_vjp_deterministic_and_pairs_with_jvp(oracle_mod, fb):
     assert abs(lhs - rhs) <= 1e-11 * float(np.abs(Rb * JV).sum() + np.abs(RKb * JVK).sum())
     _, Kf = ns.rans_vjp(W, K, Rb, np.zeros_like(RKb))
     assert np.abs(Kf).max() > 0.0
+
+
+@pytest.mark.gpu
+def test_rans_vjp_full_plate(fb):
+    """At the full 384x192x4 plate the adjoint and the FP64 tangent of the
+    coupled residual satisfy the dot-product identity along seeded
+    directions, and repeated adjoints are the same bits."""
+    case = cases.plate_case()
+    cs = fb.Case.from_case(case)
+    m = fb.Mesh(case.mesh, cs)
+    ns = fb.NavierStokes(m, cs, 0)
+    W, K = _generic(case), case.kstate
+    rng = np.random.default_rng(47)
+    Rb, RKb = rng.standard_normal(W.shape), rng.standard_normal(K.shape)
+    Wb, Kb = ns.rans_vjp(W, K, Rb, RKb)
+    W2, K2 = ns.rans_vjp(W, K, Rb, RKb)
+    assert np.array_equal(W2, Wb) and np.array_equal(K2, Kb)
+    for _ in range(2):
+        V = rng.standard_normal(W.shape) * np.abs(W).max(axis=0)
+        VK = rng.standard_normal(K.shape) * np.abs(K).max(axis=0)
+        JV, JVK = ns.rans_jvp(W, K, V, VK)
+        lhs = float((Rb * JV).sum() + (RKb * JVK).sum())
+        rhs = float((Wb * V).sum() + (Kb * VK).sum())
+        assert abs(lhs - rhs) <= 1e-11 * float(np.abs(Rb * JV).sum() + np.abs(RKb * JVK).sum())
