@@ -141,16 +141,6 @@ struct fcfd_ctx {
   // the residual chain's gradient and face launches overlap their
   // predecessor's tail (programmatic dependent launch); fcfd_ctx_set_launch_overlap
   bool pdl = true;
-  // residual from page-locked host buffers, pipelined: the faces ordered by
-  // their parent's cell chunk (pipe_order); the rows of chunk i
-  // [pipe_cells[i], pipe_cells[i+1]) are complete once the face-list prefix
-  // [0, pipe_faces[i+1]) is done, and are copied out on `copy` while the
-  // next chunk's faces run.  One chunk: no pipeline.
-  DBuf<int> pipe_order;
-  std::vector<int> pipe_cells, pipe_faces;
-  cudaStream_t copy = nullptr;
-  std::vector<cudaEvent_t> ev_pipe;
-  cudaEvent_t ev_copy = nullptr;
 };
 
 

@@ -55,64 +55,6 @@ void launch_chain(fcfd_ctx *x, Pipe<S> &P, S *Rout, bool aos_out, S *mo, S *wo, 
   CK(cudaGetLastError());
 }
 
-// The FP64 chain on x->p64 (state already in P.W) with the copy of R out to
-// the host pipelined behind it: ghosts and extrema, gradients and limiters,
-// the stale-density outlet faces on the side stream, then per cell chunk i
-// the faces of the pipelined order up to pipe_faces[i+1], the chunk's rows
-// of R ([nc][5], into Rdev), and their device-to-host copy on the copy
-// stream, which overlaps the next chunk's faces.  The same face values and
-// the same ascending-face sums as launch_chain, so the same bits.
-static void launch_chain_pipelined(fcfd_ctx *x, double *Rdev, double *Rhost) {
-  const DevMesh &m = x->dm;
-  Pipe<double> &P = x->p64;
-  cudaStream_t s = x->stream;
-  const int tb = 256;
-  const bool need_ext = x->cs.limiter == 1 && x->cs.order != 1;
-  const int ng = (m.nb + tb - 1) / tb + (need_ext ? kExtremaBlocks : 0);
-  if (ng > 0)
-    launch_k(x->pdl, k_ghost_minmax<double>, ng, tb, 0, s, x->cs, m, P.W.p, need_ext ? x->ext.p : nullptr, x->err.p);
-  launch_grad_limiter<double>(x->cs, m, P.W.p, x->ext.p, nullptr, P.G.p, P.Lm.p, s, x->pdl);
-  const bool side = m.n_outlet > 0;
-  if (side) {
-    CK(cudaEventRecord(x->ev_fork, s));
-    CK(cudaStreamWaitEvent(x->side, x->ev_fork, 0));
-    const int g = (m.n_outlet + 127) / 128;
-    if (x->viscous)
-      FCFD_BY_FLUX(x->cs.flux, k_face_flux<double, true, FX, true><<<g, 128, 0, x->side>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p, nullptr, P.D.p, x->mdot.p, x->wl.p, x->err.p));
-    else
-      FCFD_BY_FLUX(x->cs.flux, k_face_flux<double, false, FX, true><<<g, 128, 0, x->side>>>(x->cs, m, P.W.p, P.G.p, P.Lm.p, P.stale.p, nullptr, P.D.p, x->mdot.p, x->wl.p, x->err.p));
-    CK(cudaEventRecord(x->ev_join, x->side));
-  }
-  const int nchunk = (int)x->pipe_cells.size() - 1;
-  for (int i = 0; i < nchunk; ++i) {
-    // faces [pipe_faces[i], pipe_faces[i+1]) of the pipelined order
-    DevMesh mc = m;
-    mc.face_list = x->pipe_order.p + x->pipe_faces[i];
-    mc.n_face_list = x->pipe_faces[i + 1] - x->pipe_faces[i];
-    const int gf = (mc.n_face_list + 127) / 128;
-    if (gf > 0) {
-      if (x->viscous)
-        FCFD_BY_FLUX(x->cs.flux, launch_k(x->pdl, k_face_flux<double, true, FX, false, true>, gf, 128, 0, s, x->cs, mc, (const double *)P.W.p, (const double *)P.G.p, (const double *)P.Lm.p, P.stale.p, (const double *)nullptr, P.D.p, x->mdot.p, x->wl.p, x->err.p));
-      else
-        FCFD_BY_FLUX(x->cs.flux, launch_k(x->pdl, k_face_flux<double, false, FX, false, true>, gf, 128, 0, s, x->cs, mc, (const double *)P.W.p, (const double *)P.G.p, (const double *)P.Lm.p, P.stale.p, (const double *)nullptr, P.D.p, x->mdot.p, x->wl.p, x->err.p));
-    }
-    // the outlet faces' differences before the first rows are summed (an
-    // ordinary launch after the join)
-    const bool join = side && i == 0;
-    if (join) CK(cudaStreamWaitEvent(s, x->ev_join, 0));
-    const int lo = x->pipe_cells[i], no = x->pipe_cells[i + 1] - lo;
-    launch_k(x->pdl && !join, k_gather_rows<double, true>, (5 * no + tb - 1) / tb, tb, 0, s, m, (const double *)P.D.p, Rdev,
-             x->ext.p, x->argx.p, lo, no);
-    CK(cudaEventRecord(x->ev_pipe[i], s));
-    CK(cudaStreamWaitEvent(x->copy, x->ev_pipe[i], 0));
-    CK(cudaMemcpyAsync(Rhost + 5 * (size_t)lo, Rdev + 5 * (size_t)lo, sizeof(double) * 5 * (size_t)no,
-                       cudaMemcpyDeviceToHost, x->copy));
-  }
-  CK(cudaEventRecord(x->ev_copy, x->copy));
-  CK(cudaStreamWaitEvent(s, x->ev_copy, 0));
-  CK(cudaGetLastError());
-}
-
 // Mixed-precision residual chain on x->p64 (state already in P.W): FP64
 // ghosts, extrema, gradients and limiters; the stale-density outlet faces in
 // FP64 on the side stream; the FP32 face pass with the shock-flagged faces
@@ -477,42 +419,6 @@ int fcfd_ctx_create(const fcfd_mesh *mp, const fcfd_case *csp, int device, fcfd_
     });
     x->face_order.upload(order);
   }
-  {
-    // pipelined host-buffer residual: four cell chunks on meshes of at least
-    // 16,384 cells; faces ordered by their parent's chunk, interior faces
-    // first within a chunk; chunk i's rows need the face-list prefix that
-    // holds every face of its cells (and of the chunks before it)
-    const int nchunk = nc >= 16384 ? 4 : 1;
-    x->pipe_cells.assign(nchunk + 1, 0);
-    for (int i = 0; i <= nchunk; ++i) x->pipe_cells[i] = (int)((int64_t)nc * i / nchunk);
-    std::vector<int32_t> order(nf), pos(nf), chunk_of(nc);
-    for (int i = 0; i < nchunk; ++i)
-      for (int cc = x->pipe_cells[i]; cc < x->pipe_cells[i + 1]; ++cc) chunk_of[cc] = i;
-    for (int f = 0; f < nf; ++f) order[f] = f;
-    std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
-      const int ca = chunk_of[m.f_parent[a]], cb = chunk_of[m.f_parent[b]];
-      return ca != cb ? ca < cb : m.f_bc[a] < m.f_bc[b];
-    });
-    for (int k = 0; k < nf; ++k) pos[order[k]] = k;
-    x->pipe_faces.assign(nchunk + 1, 0);
-    int reach = 0;
-    for (int i = 0; i < nchunk; ++i) {
-      for (int cc = x->pipe_cells[i]; cc < x->pipe_cells[i + 1]; ++cc)
-        for (int j = m.cf_index[cc]; j < m.cf_index[cc + 1]; ++j) {
-          const int e = m.cf_list[j];
-          reach = std::max(reach, pos[e >= 0 ? e : ~e] + 1);
-        }
-      x->pipe_faces[i + 1] = reach;
-    }
-    x->pipe_faces[nchunk] = nf;
-    x->pipe_order.upload(order);
-    if (nchunk > 1) {
-      CK(cudaStreamCreateWithFlags(&x->copy, cudaStreamNonBlocking));
-      x->ev_pipe.assign(nchunk, nullptr);
-      for (auto &e : x->ev_pipe) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-      CK(cudaEventCreateWithFlags(&x->ev_copy, cudaEventDisableTiming));
-    }
-  }
   x->color_cells.upload(m.color_cells);
   x->color_index = m.color_index;
   {
@@ -594,10 +500,6 @@ void fcfd_ctx_destroy(fcfd_ctx *x) {
   if (x->err_pinned) cudaFreeHost(x->err_pinned);
   adjoint_free(x);
   rans_free(x);
-  for (cudaEvent_t e : x->ev_pipe)
-    if (e) cudaEventDestroy(e);
-  if (x->ev_copy) cudaEventDestroy(x->ev_copy);
-  if (x->copy) cudaStreamDestroy(x->copy);
   if (x->ev_fork) cudaEventDestroy(x->ev_fork);
   if (x->ev_join) cudaEventDestroy(x->ev_join);
   if (x->side) cudaStreamDestroy(x->side);
@@ -632,12 +534,8 @@ int fcfd_residual(fcfd_ctx *x, const double *W, double *R, int flags) {
       CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
       CK(cudaMemcpyAsync(x->Win.p, W, sizeof(double) * 5 * m.nc, cudaMemcpyHostToDevice, s));
       k_aos_to_soa<double><<<(m.nc + 255) / 256, 256, 0, s>>>(x->Win.p, x->p64.W.p, m.nc, m.nt);
-      if (x->pipe_cells.size() > 2) {
-        launch_chain_pipelined(x, x->Rtmp.p, R);
-      } else {
-        launch_chain<double>(x, x->p64, x->Rtmp.p, true, x->mdot.p, x->wl.p);
-        CK(cudaMemcpyAsync(R, x->Rtmp.p, sizeof(double) * 5 * m.nc, cudaMemcpyDeviceToHost, s));
-      }
+      launch_chain<double>(x, x->p64, x->Rtmp.p, true, x->mdot.p, x->wl.p);
+      CK(cudaMemcpyAsync(R, x->Rtmp.p, sizeof(double) * 5 * m.nc, cudaMemcpyDeviceToHost, s));
       CK(cudaMemcpyAsync(x->err_pinned, x->err.p, sizeof(int), cudaMemcpyDeviceToHost, s));
       CK(cudaStreamEndCapture(s, &g));
       CK(cudaGraphInstantiate(&x->host_graph, g, 0));

@@ -1639,12 +1639,15 @@ __device__ __forceinline__ void reset_extrema(unsigned long long *ext, int *argx
 // of (+D) for the parent side and (-D) for the neighbour side.  The last
 // kernel of a residual chain, so it also re-arms the extrema slots for the
 // next chain (every reader of them has finished by now on this stream).
-// Row t of the rows [lo, lo + no): one thread per (cell, equation),
-// equation-major so that a warp covers consecutive cells of one equation.
 template <class S, bool AOS>
-__device__ __forceinline__ void gather_one(const DevMesh &m, const S *__restrict__ D, S *__restrict__ R, int t, int no,
-                                           int lo) {
-  const int nc = m.nc;
+__global__ void k_gather(DevMesh m, const S *__restrict__ D, S *__restrict__ R, unsigned long long *ext, int *argx) {
+  pdl_wait();
+  reset_extrema(ext, argx);
+  // one thread per (cell, equation): 5 nc threads, equation-major so that a
+  // warp covers consecutive cells of one equation
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nc = m.nc, no = n_owned(m), lo = m.part_cells ? m.own_lo : 0;
+  if (t >= 5 * no) return;
   const int v = t / no, c = lo + (t - v * no);
   const S *Dv = D + (size_t)v * m.nf;
   const int j0 = m.cf_index[c], j1 = m.cf_index[c + 1];
@@ -1669,26 +1672,6 @@ __device__ __forceinline__ void gather_one(const DevMesh &m, const S *__restrict
   }
   if (AOS) R[5 * c + v] = r;
   else R[(size_t)v * nc + c] = r;
-}
-template <class S, bool AOS>
-__global__ void k_gather(DevMesh m, const S *__restrict__ D, S *__restrict__ R, unsigned long long *ext, int *argx) {
-  pdl_wait();
-  reset_extrema(ext, argx);
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  const int no = n_owned(m), lo = m.part_cells ? m.own_lo : 0;
-  if (t >= 5 * no) return;
-  gather_one<S, AOS>(m, D, R, t, no, lo);
-}
-// The same over the cells [lo, lo + no) only: one chunk of the pipelined
-// residual, whose rows are copied out while the next chunk is computed.
-template <class S, bool AOS>
-__global__ void k_gather_rows(DevMesh m, const S *__restrict__ D, S *__restrict__ R, unsigned long long *ext, int *argx,
-                              int lo, int no) {
-  pdl_wait();
-  reset_extrema(ext, argx);
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= 5 * no) return;
-  gather_one<S, AOS>(m, D, R, t, no, lo);
 }
 
 // Local time step (time_step.cc:143-224).

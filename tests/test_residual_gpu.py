@@ -216,32 +216,6 @@ def test_launch_overlap_same_bits(family, oracle_mod, fb):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("family", ["cylinder", "hypersonic", "plate"])
-def test_pipelined_copy_out_same_bits(family, fb):
-    """Meshes of 16,384 cells or more take the pipelined page-locked path
-    (faces in cell-chunk order, each chunk's rows copied out while the next
-    chunk computes): the same bits as the pageable path, for two states in
-    the same buffers, with the launch overlap on and off."""
-    import torch
-    case = {"cylinder": lambda: cases.cylinder_case(), "hypersonic": lambda: cases.hypersonic_case(),
-            "plate": lambda: cases.plate_case(turbulent=False)}[family]()
-    cs = fb.Case.from_case(case)
-    m = fb.Mesh(case.mesh, cs)
-    ns = fb.NavierStokes(m, cs, 0)
-    W2 = case.state * (1 + 1e-3 * np.random.default_rng(9).uniform(-1, 1, case.state.shape))
-    Wp = torch.empty((m.nc, 5), dtype=torch.float64, pin_memory=True)
-    Rp = torch.empty((m.nc, 5), dtype=torch.float64, pin_memory=True)
-    for on in (True, False):
-        ns.set_launch_overlap(on)
-        for W in (case.state, W2, case.state):
-            ref = ns.residual(np.ascontiguousarray(W))
-            Wp.numpy()[:] = W
-            Rp.numpy()[:] = np.nan
-            ns.residual(Wp.numpy(), Rp.numpy())
-            assert np.array_equal(Rp.numpy(), ref)
-
-
-@pytest.mark.gpu
 def test_pinned_host_buffers(oracle_mod, fb):
     """Page-locked W and R take the one-graph path (copies, chain and error
     flag replayed as a CUDA graph): same bits as pageable buffers, for a new
