@@ -514,6 +514,15 @@ constexpr int kNv = 7;
 constexpr int kRedBlk = 592;  // 4 x 148 blocks for the reductions
 
 // X (SoA [7][nc]) + eps z -> the chain's W [5][nt] and K [2][nt] (interiors)
+struct Wt7 {
+  double s[kNv];
+};
+// per linear step constants the captured Arnoldi steps read from the device:
+// equation weights, their inverses, the finite-difference numerator
+struct KwIter {
+  Wt7 wr, iwr;
+  double eps_num;
+};
 // finite-difference step of the Krylov matvec, eps_num / |z| with |z|^2 read
 // from the device (1e-8 where |z| = 0)
 __device__ __forceinline__ double kw_fd_eps(double eps_num, const double *zz) {
@@ -521,11 +530,11 @@ __device__ __forceinline__ double kw_fd_eps(double eps_num, const double *zz) {
   return q > 0. ? eps_num / sqrt(q) : 1e-8;
 }
 __global__ void k_x_load(int nc, int nt, const double *__restrict__ X, const double *__restrict__ z, double eps,
-                         double *__restrict__ W, double *__restrict__ K, double eps_num = 0.,
+                         double *__restrict__ W, double *__restrict__ K, const KwIter *__restrict__ it = nullptr,
                          const double *__restrict__ zz = nullptr) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= nc) return;
-  if (zz) eps = kw_fd_eps(eps_num, zz);
+  if (zz) eps = kw_fd_eps(it->eps_num, zz);
 #pragma unroll
   for (int v = 0; v < 5; ++v) W[v * nt + c] = X[v * nc + c] + (z ? eps * z[v * nc + c] : 0.);
 #pragma unroll
@@ -564,16 +573,14 @@ __global__ void k_dual_planes(int nc, const Dual<float> *__restrict__ R, const D
 
 // y = wr * (D z - Jz): D the time terms; Jz = (F1 - F0) * inv_eps, or the
 // tangent (F0 null).  wr: per-equation weights.
-struct Wt7 {
-  double s[kNv];
-};
 __global__ void k_kw_matvec(DevCase cs, int nc, const double *__restrict__ X, const double *__restrict__ vol,
                             const double *__restrict__ dt, const double *__restrict__ z, const double *__restrict__ F1,
-                            const double *__restrict__ F0, double inv_eps, Wt7 wr, double *__restrict__ y,
-                            double eps_num = 0., const double *__restrict__ zz = nullptr) {
+                            const double *__restrict__ F0, double inv_eps, const KwIter *__restrict__ it,
+                            double *__restrict__ y, const double *__restrict__ zz = nullptr) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= nc) return;
-  if (zz) inv_eps = 1. / kw_fd_eps(eps_num, zz);
+  if (zz) inv_eps = 1. / kw_fd_eps(it->eps_num, zz);
+  const Wt7 &wr = it->wr;
   const double p = X[c], u = X[nc + c], v = X[2 * nc + c], w = X[3 * nc + c], T = X[4 * nc + c];
   const double pressure = p + cs.Pref, temperature = T + cs.Tref;
   const double rho = pressure / (cs.R * temperature);
@@ -632,10 +639,11 @@ __global__ void k_kw_diag(DevCase cs, DevMesh m, const double *__restrict__ X, c
 
 // z = M^-1 v: flow rows through the inverse blocks, k and omega rows by the
 // diagonal; v carries the equation weights wr (removed first).
-__global__ void k_kw_prec(int nc, const double *__restrict__ Minv, const double *__restrict__ dk, Wt7 iwr,
-                          const double *__restrict__ v, double *__restrict__ z) {
+__global__ void k_kw_prec(int nc, const double *__restrict__ Minv, const double *__restrict__ dk,
+                          const KwIter *__restrict__ it, const double *__restrict__ v, double *__restrict__ z) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= nc) return;
+  const Wt7 &iwr = it->iwr;
   double b[5];
 #pragma unroll
   for (int k = 0; k < 5; ++k) b[k] = iwr.s[k] * v[k * nc + c];
@@ -756,12 +764,22 @@ struct KwSolve {
   // |z|^2; one counter per dot-product column
   DBuf<double> hd;
   DBuf<unsigned> cnt;
-  std::vector<double> hh;
+  double *hh = nullptr;  // page-locked copy of hd
+  DBuf<KwIter> it;
+  // one captured Arnoldi step per basis index, for the J.v mode graph_mode
+  std::vector<cudaGraphExec_t> graphs;
+  int graph_mode = -1;
   void alloc_gs(int mdim, cudaStream_t s) {
     hd.alloc(2 * (size_t)(mdim + 1) + 2);
     cnt.alloc((size_t)mdim + 1);
+    it.alloc(1);
     CK(cudaMemsetAsync(cnt.p, 0, sizeof(unsigned) * (mdim + 1), s));
-    hh.resize(hd.n);
+    CK(cudaMallocHost((void **)&hh, sizeof(double) * hd.n));
+  }
+  ~KwSolve() {
+    for (cudaGraphExec_t g : graphs)
+      if (g) cudaGraphExecDestroy(g);
+    if (hh) cudaFreeHost(hh);
   }
 };
 
@@ -859,34 +877,58 @@ static int kw_linear_step(fcfd_ctx *x, KwSolve &S, int mdim, int mode, double kr
   g[0] = beta;
   if (beta > 0.) {
     k_kw_scale<<<gn, 256, 0, s>>>(n, 1. / beta, S.w.p, S.Vb.p);
+    // per linear step constants on the device (the captured steps read them)
+    KwIter hit;
+    hit.wr = wr;
+    hit.iwr = iwr;
+    hit.eps_num = 1.4901161193847656e-08 * (1. + xn);
+    CK(cudaMemcpyAsync(S.it.p, &hit, sizeof(KwIter), cudaMemcpyHostToDevice, s));
+    if (mode != 0) {
+      // tangent buffers before any capture
+      if (!x->pjv32.ready) x->pjv32.alloc(m.nc, m.nf, m.nb);
+      if (!x->rans->f.ready) x->rans->f.alloc(m.nc, m.nt, m.nf);
+    }
+    if (S.graph_mode != mode) {
+      for (cudaGraphExec_t &g : S.graphs)
+        if (g) { CK(cudaGraphExecDestroy(g)); g = nullptr; }
+      S.graphs.assign(mdim, nullptr);
+      S.graph_mode = mode;
+    }
+    // the Gram-Schmidt coefficients, |w|^2 and |z|^2 stay on the device
+    // (fused dot products); one Arnoldi step is one captured graph, replayed
+    // with one copy back and one synchronisation
+    double *h1 = S.hd.p, *h2 = S.hd.p + (mdim + 1), *hw = S.hd.p + 2 * (mdim + 1), *zz = hw + 1;
     for (int j = 0; j < mdim; ++j) {
-      double *vj = S.Vb.p + (size_t)j * n;
-      // z = M^-1 v_j, then w = wr (D z - J z)
-      k_kw_prec<<<gc, 256, 0, s>>>(nc, S.Minv.p, S.dk.p, iwr, vj, S.z.p);
-      // the Gram-Schmidt coefficients, |w|^2 and |z|^2 stay on the device
-      // (fused dot products); one copy back and one synchronisation per step
-      double *h1 = S.hd.p, *h2 = S.hd.p + (mdim + 1), *hw = S.hd.p + 2 * (mdim + 1), *zz = hw + 1;
-      if (mode == 0) {
-        // eps = sqrt(eps_mach) (1 + |S^-1 X|) / |z|, |z| read on the device
-        const double eps_num = 1.4901161193847656e-08 * (1. + xn);
-        k_kw_dots<<<dim3(kRedBlk, 1), 256, 0, s>>>(n, 1, S.z.p, 0, S.z.p, S.part.p, zz, S.cnt.p);
-        k_x_load<<<gc, 256, 0, s>>>(m.nc, m.nt, S.X.p, S.z.p, 0., x->p64.W.p, x->rans->b.K.p, eps_num, zz);
-        rans_chain<double, false>(x, x->p64, x->rans->b, x->mdot.p, x->wl.p, S.F1.p, x->rans->b.RK.p);
-        k_rk_planes<<<gc, 256, 0, s>>>(m.nc, x->rans->b.RK.p, S.F1.p);
-        k_kw_matvec<<<gc, 256, 0, s>>>(x->cs, nc, S.X.p, S.vol.p, S.dt.p, S.z.p, S.F1.p, S.F0.p, 0., wr, S.w.p, eps_num,
-                                        zz);
-      } else {
-        kw_tangent32(x, S.X.p, S.z.p, S.Jz.p);
-        k_kw_matvec<<<gc, 256, 0, s>>>(x->cs, nc, S.X.p, S.vol.p, S.dt.p, S.z.p, S.Jz.p, nullptr, 0., wr, S.w.p);
+      if (!S.graphs[j]) {
+        double *vj = S.Vb.p + (size_t)j * n;
+        cudaGraph_t gr = nullptr;
+        CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        // z = M^-1 v_j, then w = wr (D z - J z)
+        k_kw_prec<<<gc, 256, 0, s>>>(nc, S.Minv.p, S.dk.p, S.it.p, vj, S.z.p);
+        if (mode == 0) {
+          // eps = sqrt(eps_mach) (1 + |S^-1 X|) / |z|, |z| read on the device
+          k_kw_dots<<<dim3(kRedBlk, 1), 256, 0, s>>>(n, 1, S.z.p, 0, S.z.p, S.part.p, zz, S.cnt.p);
+          k_x_load<<<gc, 256, 0, s>>>(m.nc, m.nt, S.X.p, S.z.p, 0., x->p64.W.p, x->rans->b.K.p, S.it.p, zz);
+          rans_chain<double, false>(x, x->p64, x->rans->b, x->mdot.p, x->wl.p, S.F1.p, x->rans->b.RK.p);
+          k_rk_planes<<<gc, 256, 0, s>>>(m.nc, x->rans->b.RK.p, S.F1.p);
+          k_kw_matvec<<<gc, 256, 0, s>>>(x->cs, nc, S.X.p, S.vol.p, S.dt.p, S.z.p, S.F1.p, S.F0.p, 0., S.it.p, S.w.p, zz);
+        } else {
+          kw_tangent32(x, S.X.p, S.z.p, S.Jz.p);
+          k_kw_matvec<<<gc, 256, 0, s>>>(x->cs, nc, S.X.p, S.vol.p, S.dt.p, S.z.p, S.Jz.p, nullptr, 0., S.it.p, S.w.p);
+        }
+        // classical Gram-Schmidt, twice
+        k_kw_dots<<<dim3(kRedBlk, j + 1), 256, 0, s>>>(n, j + 1, S.Vb.p, (size_t)n, S.w.p, S.part.p, h1, S.cnt.p);
+        k_kw_sub<<<gn, 256, 0, s>>>(n, j + 1, S.Vb.p, (size_t)n, h1, S.w.p);
+        k_kw_dots<<<dim3(kRedBlk, j + 1), 256, 0, s>>>(n, j + 1, S.Vb.p, (size_t)n, S.w.p, S.part.p, h2, S.cnt.p);
+        k_kw_sub<<<gn, 256, 0, s>>>(n, j + 1, S.Vb.p, (size_t)n, h2, S.w.p);
+        k_kw_dots<<<dim3(kRedBlk, 1), 256, 0, s>>>(n, 1, S.w.p, 0, S.w.p, S.part.p, hw, S.cnt.p);
+        k_kw_scale_rsqrt<<<gn, 256, 0, s>>>(n, hw, S.w.p, S.Vb.p + (size_t)(j + 1) * n);
+        CK(cudaMemcpyAsync(S.hh, S.hd.p, sizeof(double) * S.hd.n, cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamEndCapture(s, &gr));
+        CK(cudaGraphInstantiate(&S.graphs[j], gr, 0));
+        CK(cudaGraphDestroy(gr));
       }
-      // classical Gram-Schmidt, twice
-      k_kw_dots<<<dim3(kRedBlk, j + 1), 256, 0, s>>>(n, j + 1, S.Vb.p, (size_t)n, S.w.p, S.part.p, h1, S.cnt.p);
-      k_kw_sub<<<gn, 256, 0, s>>>(n, j + 1, S.Vb.p, (size_t)n, h1, S.w.p);
-      k_kw_dots<<<dim3(kRedBlk, j + 1), 256, 0, s>>>(n, j + 1, S.Vb.p, (size_t)n, S.w.p, S.part.p, h2, S.cnt.p);
-      k_kw_sub<<<gn, 256, 0, s>>>(n, j + 1, S.Vb.p, (size_t)n, h2, S.w.p);
-      k_kw_dots<<<dim3(kRedBlk, 1), 256, 0, s>>>(n, 1, S.w.p, 0, S.w.p, S.part.p, hw, S.cnt.p);
-      k_kw_scale_rsqrt<<<gn, 256, 0, s>>>(n, hw, S.w.p, S.Vb.p + (size_t)(j + 1) * n);
-      CK(cudaMemcpyAsync(S.hh.data(), S.hd.p, sizeof(double) * S.hd.n, cudaMemcpyDeviceToHost, s));
+      CK(cudaGraphLaunch(S.graphs[j], s));
       CK(cudaStreamSynchronize(s));
       const double hn = std::sqrt(S.hh[2 * (mdim + 1)]);
       for (int i = 0; i <= j; ++i) H[(size_t)i * mdim + j] = S.hh[i] + S.hh[mdim + 1 + i];
@@ -917,7 +959,7 @@ static int kw_linear_step(fcfd_ctx *x, KwSolve &S, int mdim, int mode, double kr
     }
     CK(cudaMemcpyAsync(S.h.p, y.data(), sizeof(double) * kit, cudaMemcpyHostToDevice, s));
     k_kw_combo<<<gn, 256, 0, s>>>(n, kit, S.Vb.p, (size_t)n, S.h.p, S.x.p);
-    k_kw_prec<<<gc, 256, 0, s>>>(nc, S.Minv.p, S.dk.p, iwr, S.x.p, S.dX.p);
+    k_kw_prec<<<gc, 256, 0, s>>>(nc, S.Minv.p, S.dk.p, S.it.p, S.x.p, S.dX.p);
   } else if (!std::isfinite(beta)) {
     // a non-finite right-hand side: a NaN update, which the update's NaN
     // check reports as divergence (as the reference's NaN check would)
