@@ -17,6 +17,7 @@ LIB_PATH = os.path.join(_HERE, "_build", "libfcfd_b200.so")
 
 FCFD_OK = 0
 FCFD_DEVICE_PTRS = 1
+FCFD_NO_SYNC = 8
 STATUS = {0: "OK", 1: "ERR_INPUT", 2: "ERR_MESH", 3: "ERR_DIVERGED", 4: "ERR_NOT_CONVERGED", 5: "ERR_CUDA",
           6: "ERR_TIMEOUT", 7: "ERR_UNSUPPORTED", 8: "ERR_BC"}
 
@@ -27,7 +28,7 @@ EXPORTED = [
     "fcfd_ctx_create", "fcfd_ctx_destroy", "fcfd_ctx_set_exact_gradients", "fcfd_residual", "fcfd_last_stages", "fcfd_local_dt",
     "fcfd_time_residual", "fcfd_point_flux", "fcfd_jvp", "fcfd_vjp", "fcfd_drag", "fcfd_rans_residual", "fcfd_rans_bcs", "fcfd_time_rans", "fcfd_newton_solve", "fcfd_local_dt_cflmax_noalloc",
     "fcfd_run", "fcfd_restart_write", "fcfd_restart_read", "fcfd_mesh_from_tecplot", "fcfd_rans_jvp", "fcfd_rans_vjp", "fcfd_ctx_set_launch_overlap",
-    "fcfd_partition_sets", "fcfd_ctx_set_partition", "fcfd_partition_extrema", "fcfd_partition_residual",
+    "fcfd_partition_sets", "fcfd_ctx_set_partition", "fcfd_partition_extrema", "fcfd_partition_residual", "fcfd_ctx_check",
     "fcfd_ctx_stream", "fcfd_diag_blocks", "fcfd_rans_newton_solve", "fcfd_residual_mixed",
     "fcfd_time_residual_mixed", "fcfd_ctx_set_gradient_kernel", "fcfd_time_terms", "fcfd_ctx_gradient_info",
 ]
@@ -145,6 +146,7 @@ def _load():
     L.fcfd_ctx_set_partition.argtypes = [vp, ctypes.c_int, ctypes.c_int]
     L.fcfd_partition_extrema.argtypes = [vp, vp, vp, ctypes.c_int]
     L.fcfd_partition_residual.argtypes = [vp, vp, vp, ctypes.c_int]
+    L.fcfd_ctx_check.argtypes = [vp]
     L.fcfd_ctx_stream.argtypes = [vp, ctypes.POINTER(vp)]
     L.fcfd_diag_blocks.argtypes = [vp, dp, dp, dp]
     L.fcfd_rans_newton_solve.argtypes = [vp, dp, dp, ctypes.POINTER(NewtonOpts), ctypes.POINTER(NewtonReport)]

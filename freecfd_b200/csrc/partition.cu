@@ -196,6 +196,14 @@ extern "C" int fcfd_ctx_set_partition(fcfd_ctx *x, int lo, int hi) {
 
 // The stream a context's work runs on, for callers that enqueue their own
 // work around it (a halo exchange, the extrema all-reduce).
+extern "C" int fcfd_ctx_check(fcfd_ctx *x) {
+  return api([&] {
+    if (!x) throw Error(FCFD_ERR_INPUT, "null context");
+    CK(cudaSetDevice(x->device));
+    check_err(x);
+  });
+}
+
 extern "C" int fcfd_ctx_stream(const fcfd_ctx *x, void **stream) {
   return api([&] {
     if (!x || !stream) throw Error(FCFD_ERR_INPUT, "null argument");
@@ -272,6 +280,8 @@ extern "C" int fcfd_partition_residual(fcfd_ctx *x, const double ext[8], double 
     if (!dev)
       CK(cudaMemcpyAsync(R + 5 * (size_t)m.own_lo, x->Rtmp.p + 5 * (size_t)m.own_lo,
                          sizeof(double) * 5 * (size_t)n_owned(m), cudaMemcpyDeviceToHost, s));
+    // enqueue only: the error flag stays on the device for fcfd_ctx_check
+    if (dev && (flags & FCFD_NO_SYNC)) return;
     CK(cudaStreamSynchronize(s));
     check_err(x);
   });

@@ -124,7 +124,9 @@ class PartitionedResidual:
         self.ext = W.new_empty(8)
         self.stream = torch.cuda.ExternalStream(ns.stream_handle(), device=W.device)
 
-    def __call__(self, R):
+    def __call__(self, R, sync: bool = True):
+        """sync=False: enqueue the step only (no host synchronisation); a BC
+        error is then reported by check()."""
         import torch
         # W may have been written on torch's stream (a state update)
         self.stream.wait_stream(torch.cuda.current_stream(self.W.device))
@@ -132,8 +134,11 @@ class PartitionedResidual:
             self.ex.exchange()
             self.ns.partition_extrema(self.W, out=self.ext)
             combine_extrema(self.ext)
-            self.ns.partition_residual(self.ext, R)
+            self.ns.partition_residual(self.ext, R, sync=sync)
         return R
+
+    def check(self):
+        self.ns.check()
 
 
 def gmres(matvec, precond, b, allreduce=None, m: int = 30, rtol: float = 1e-2, cycles: int = 1):

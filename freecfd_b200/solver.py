@@ -16,7 +16,8 @@ import tempfile
 
 import numpy as np
 
-from ._lib import NewtonOpts, NewtonReport, RunOpts, RunReport, _RawMesh, _d, _i, _ptr, check, lib, FcfdError
+from ._lib import (FCFD_DEVICE_PTRS, FCFD_NO_SYNC, NewtonOpts, NewtonReport, RunOpts, RunReport, _RawMesh, _d, _i, _ptr,
+                   check, lib, FcfdError)
 
 
 class Case:
@@ -217,9 +218,10 @@ class NavierStokes:
         check(lib.fcfd_partition_extrema(self.h, pw, pe, fw))
         return ext
 
-    def partition_residual(self, ext, out):
+    def partition_residual(self, ext, out, sync: bool = True):
         """Phase 2: rows [lo, hi) of R (numpy [nc][5] or CUDA tensor) from the
-        extrema combined over all ranks (a CUDA tensor with a CUDA R)."""
+        extrema combined over all ranks (a CUDA tensor with a CUDA R).
+        sync=False (CUDA R): enqueue only; check() reports a BC error."""
         if isinstance(out, np.ndarray):
             ext = np.ascontiguousarray(np.asarray(ext, dtype=np.float64))
         elif isinstance(ext, np.ndarray):
@@ -227,8 +229,15 @@ class NavierStokes:
             ext = torch.as_tensor(ext, device=out.device)
         pe, _ = _ptr(ext)
         pr, fr = _ptr(out)
+        if not sync and fr & FCFD_DEVICE_PTRS:
+            fr |= FCFD_NO_SYNC
         check(lib.fcfd_partition_residual(self.h, pe, pr, fr))
         return out
+
+    def check(self):
+        """Wait for the context's stream; raise for a BC error flagged by
+        work enqueued without synchronisation."""
+        check(lib.fcfd_ctx_check(self.h))
 
     def stream_handle(self) -> int:
         """The cudaStream_t this context enqueues its work on (as an int)."""

@@ -39,7 +39,10 @@ enum fcfd_status {
 
 enum fcfd_flags {
   FCFD_DEVICE_PTRS = 1, /* input/output pointers are device pointers on the context's device */
-  FCFD_JVP_FP32 = 4     /* fcfd_jvp: evaluate the tangent chain in FP32 (value and derivative) */
+  FCFD_JVP_FP32 = 4,    /* fcfd_jvp: evaluate the tangent chain in FP32 (value and derivative) */
+  FCFD_NO_SYNC = 8      /* fcfd_partition_residual with device pointers: enqueue only, no host
+                           synchronisation; a BC error stays flagged on the device until
+                           fcfd_ctx_check (or the next synchronising call) reports it */
 };
 
 enum fcfd_precision { FCFD_FP64 = 0, FCFD_FP32 = 1 };
@@ -263,6 +266,10 @@ int fcfd_partition_extrema(fcfd_ctx *ctx, const double *W, double ext[8], int fl
 int fcfd_partition_residual(fcfd_ctx *ctx, const double ext[8], double *R, int flags);
 /* The CUDA stream (cudaStream_t) the context's work is enqueued on. */
 int fcfd_ctx_stream(const fcfd_ctx *ctx, void **stream);
+/* Waits for the context's stream and reports (and clears) a boundary-condition
+ * error flagged by work enqueued without synchronisation (FCFD_NO_SYNC):
+ * FCFD_ERR_BC, or FCFD_OK. */
+int fcfd_ctx_check(fcfd_ctx *ctx);
 
 /* Fixed BC values of the RANS variables, per BC region: kw_fixed, k, omega,
  * mut_fixed, mu_t (5 doubles each; out_len >= 5 * number of regions). */

@@ -132,6 +132,41 @@ def test_partitioned_residual_one_stream(fb):
 
 
 @pytest.mark.gpu
+def test_partitioned_residual_without_sync(fb):
+    """Steps enqueued without a host synchronisation (FCFD_NO_SYNC) give the
+    same rows as synchronised ones; a boundary-condition error raised inside
+    such a step stays flagged until check() reports it (FCFD_ERR_BC), and the
+    flag is cleared afterwards."""
+    import torch
+    from freecfd_b200.partition import PartitionedResidual
+    case = SMALL["cylinder"]()
+    cs, m = _setup(fb, case)
+    ns0 = fb.NavierStokes(m, cs, 0)
+    W = torch.as_tensor(case.state, device="cuda")
+    R = torch.full_like(W, float("nan"))
+    res = PartitionedResidual(fb.NavierStokes(m, cs, 0), HaloPlan(m, cs, 1), 0, W)
+    for k in range(3):
+        Wk = case.state * (1 + 1e-3 * k)
+        W.copy_(torch.as_tensor(Wk))
+        res(R, sync=False)
+        res.check()
+        assert np.array_equal(R.cpu().numpy(), ns0.residual(Wk))
+    # supersonic flow into the inlet, whose deck gives rho and V only
+    Wbad = case.state.copy()
+    Wbad[:, 1] = 1500.0
+    W.copy_(torch.as_tensor(Wbad))
+    res(R, sync=False)
+    with pytest.raises(fb.FcfdError) as e:
+        res.check()
+    assert e.value.code == 8
+    res.check()
+    W.copy_(torch.as_tensor(case.state))
+    res(R, sync=False)
+    res.check()
+    assert np.array_equal(R.cpu().numpy(), ns0.residual(case.state))
+
+
+@pytest.mark.gpu
 def test_partitioned_residual_nccl_process_group(fb):
     """The same step inside an NCCL process group (one rank): the extrema
     all-reduce runs on the library's stream through NCCL; the halo exchange
