@@ -85,6 +85,14 @@ int main(int argc, char **argv) {
   std::printf(" bad_mesh_rc=%d", rc7);
   if (m7) fcfd_mesh_destroy(m7);
 
+  // error path: the context-level entry points reject a null context with a
+  // status instead of dereferencing it
+  {
+    double z[8] = {0.};
+    std::printf(" null_ctx_rc=%d,%d,%d,%d", fcfd_ctx_check(nullptr), fcfd_ctx_set_launch_overlap(nullptr, 1),
+                fcfd_rans_vjp(nullptr, z, z, z, z, z, z, 0), fcfd_vjp(nullptr, z, z, z, 0));
+  }
+
   fcfd_ctx *ctx = nullptr;
   rc = fcfd_ctx_create(mesh, cs, 0, &ctx);
   std::printf(" ctx_rc=%d", rc);
@@ -105,6 +113,17 @@ int main(int argc, char **argv) {
     }
     std::printf(" mixed_rc=%d mixed_fp64_faces=%lld mixed_rel_diff=%.3e", rcm, (long long)n64, rmax > 0. ? dmax / rmax : dmax);
     std::printf(" set_kernel_bad_rc=%d", fcfd_ctx_set_gradient_kernel(ctx, 9));
+    // ordinary launches give the same residual bits; no flagged error
+    std::vector<double> R3(R.size());
+    const int rco = fcfd_ctx_set_launch_overlap(ctx, 0);
+    const int rc3 = fcfd_residual(ctx, W.data(), R3.data(), 0);
+    fcfd_ctx_set_launch_overlap(ctx, 1);
+    std::printf(" overlap_off_rc=%d,%d overlap_same_bits=%d check_rc=%d", rco, rc3,
+                std::memcmp(R3.data(), R.data(), sizeof(double) * R.size()) == 0 ? 1 : 0, fcfd_ctx_check(ctx));
+    // a laminar case has no k-omega adjoint: an input error, not a fault
+    std::vector<double> K(2 * (size_t)n_cells, 1.), Wb(W.size()), Kb(K.size());
+    std::printf(" rans_vjp_laminar_rc=%d",
+                fcfd_rans_vjp(ctx, W.data(), K.data(), R.data(), K.data(), Wb.data(), Kb.data(), 0));
     std::ofstream fr(argv[4], std::ios::binary);
     fr.write(reinterpret_cast<const char *>(R.data()), (std::streamsize)(R.size() * sizeof(double)));
   }

@@ -69,6 +69,8 @@ def test_cxx_caller_cpu_paths(oracle_mod):
     assert kv["ctx_rc"] == ("0" if torch.cuda.is_available() else "5")
     assert kv["rcm_rc"] == "0" and kv["rcm_permutation"] == "1"
     assert kv["grad_weights_rc"] == "1"  # null output pointer: FCFD_ERR_INPUT
+    # a null context: FCFD_ERR_INPUT from every context-level entry point
+    assert kv["null_ctx_rc"] == "1,1,1,1"
 
 
 @pytest.mark.gpu
@@ -85,3 +87,7 @@ def test_cxx_caller_residual(oracle_mod):
     assert kv["mixed_rc"] == "0" and int(kv["mixed_fp64_faces"]) > 0
     assert float(kv["mixed_rel_diff"]) <= 1e-14
     assert kv["set_kernel_bad_rc"] == "1"
+    # ordinary launches: the same bits, no flagged error; no k-omega adjoint
+    # on a laminar case (FCFD_ERR_INPUT)
+    assert kv["overlap_off_rc"] == "0,0" and kv["overlap_same_bits"] == "1" and kv["check_rc"] == "0"
+    assert kv["rans_vjp_laminar_rc"] == "1"
