@@ -75,7 +75,7 @@ class NewtonOpts(ctypes.Structure):
                 ("jvp_mode", ctypes.c_int32), ("fp32_krylov", ctypes.c_int32), ("max_seconds", ctypes.c_double),
                 ("precond_sweeps", ctypes.c_int32), ("krylov_cycles", ctypes.c_int32),
                 ("stop_all_rows", ctypes.c_int32), ("gs_launch", ctypes.c_int32), ("precond_ilu0", ctypes.c_int32),
-                ("local_relax", ctypes.c_int32)]
+                ("local_relax", ctypes.c_int32), ("startup_steps", ctypes.c_int32), ("startup_drop", ctypes.c_double)]
 
 
 class NewtonReport(ctypes.Structure):
@@ -84,7 +84,7 @@ class NewtonReport(ctypes.Structure):
                 ("res_final", ctypes.c_double), ("wall_seconds", ctypes.c_double), ("last_cfl", ctypes.c_double),
                 ("history", ctypes.c_double * 512), ("rows_final", ctypes.c_double * 3),
                 ("seconds_to_tol", ctypes.c_double), ("seconds_history", ctypes.c_double * 512),
-                ("kw_final", ctypes.c_double * 2)]
+                ("kw_final", ctypes.c_double * 2), ("startup_steps", ctypes.c_int32), ("pad2", ctypes.c_int32)]
 
 
 def _load():

@@ -672,6 +672,20 @@ def bandwidth(face_parent, face_neighbor, face_bc) -> int:
     return int(np.abs(fp[m] - fn[m]).max()) if m.any() else 0
 
 
+def hypersonic_smooth_state(case: Case, centroids, width: float = 2.0) -> np.ndarray:
+    """A start for the hypersonic cylinder without the impulsive start's
+    vacuum: the seeded freestream pressure and temperature, the velocity
+    blended (smoothstep) from zero at the wall (r = 0.5) to the freestream
+    over `width` in radius.  The impulsive start's lee-side wall faces pull
+    the M = 8 flow away faster than 2a/(gamma-1) and open a vacuum."""
+    W = case.state.copy()
+    x = np.asarray(centroids)[: W.shape[0]]
+    s = np.clip((np.hypot(x[:, 0], x[:, 1]) - 0.5) / width, 0.0, 1.0)
+    s = s * s * (3.0 - 2.0 * s)
+    W[:, 1:4] *= s[:, None]
+    return W
+
+
 def hypersonic_shock_state(case: Case, centroids, radius: float = 1.2, seed: int = 7, mach: float = 8.0,
                            gamma: float = 1.4) -> np.ndarray:
     """A state with a captured bow-shock jump for the hypersonic cylinder:

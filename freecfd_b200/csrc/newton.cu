@@ -809,6 +809,51 @@ __global__ void k_max_rel_change(DevCase cs, int nc, const double *__restrict__ 
   for (int o = 16; o > 0; o >>= 1) r = fmax(r, __shfl_xor_sync(0xffffffffu, r, o));
   if ((threadIdx.x & 31) == 0) atomicMax(key, okey(r));
 }
+// Explicit start-up step per cell: (V P / dt) dW = R (the time-term block of
+// the implicit operator alone: forward Euler in the primitive variables with
+// the local time step), W += dW, a non-finite dW flagged (err bit 8).  The
+// 5x5 system is solved by Gaussian elimination with partial pivoting.
+__global__ void k_explicit_update(DevCase cs, int nc, double *__restrict__ Wn, const double *__restrict__ R,
+                                  const double *__restrict__ vol, const double *__restrict__ dt, int *__restrict__ err) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nc) return;
+  double A[25], b[5];
+  cons2prim(cs, Wn[c], Wn[nc + c], Wn[2 * nc + c], Wn[3 * nc + c], Wn[4 * nc + c], A);
+  const double s = vol[c] / dt[c];
+#pragma unroll
+  for (int i = 0; i < 25; ++i) A[i] *= s;
+#pragma unroll
+  for (int i = 0; i < 5; ++i) b[i] = R[(size_t)i * nc + c];
+  for (int k = 0; k < 5; ++k) {
+    int piv = k;
+    for (int i = k + 1; i < 5; ++i)
+      if (::fabs(A[5 * i + k]) > ::fabs(A[5 * piv + k])) piv = i;
+    if (piv != k) {
+      for (int j = 0; j < 5; ++j) { const double t = A[5 * k + j]; A[5 * k + j] = A[5 * piv + j]; A[5 * piv + j] = t; }
+      const double t = b[k]; b[k] = b[piv]; b[piv] = t;
+    }
+    for (int i = k + 1; i < 5; ++i) {
+      const double f = A[5 * i + k] / A[5 * k + k];
+      for (int j = k; j < 5; ++j) A[5 * i + j] -= f * A[5 * k + j];
+      b[i] -= f * b[k];
+    }
+  }
+  double d[5];
+  for (int i = 4; i >= 0; --i) {
+    double t = b[i];
+    for (int j = i + 1; j < 5; ++j) t -= A[5 * i + j] * d[j];
+    d[i] = t / A[5 * i + i];
+  }
+  bool bad = false;
+#pragma unroll
+  for (int i = 0; i < 5; ++i) bad = bad || !isfinite(d[i]);
+  if (bad) {
+    atomicOr(err, 8);
+    return;
+  }
+#pragma unroll
+  for (int i = 0; i < 5; ++i) Wn[(size_t)i * nc + c] += d[i];
+}
 // W += a_c dW per cell, a_c = min(1, 0.2 / max(|dp|/|p|, |dT|/|T|)) (absolute
 // p, T), with the NaN/Inf check of k_update
 __global__ void k_update_local(DevCase cs, int nc, double *__restrict__ Wn, const double *__restrict__ dW,
@@ -1684,9 +1729,36 @@ int fcfd_newton_solve(fcfd_ctx *x, double *W, const fcfd_newton_opts *o, fcfd_ne
     double cfl = cfl0, cfl_prev = cfl0;
     int status = FCFD_ERR_NOT_CONVERGED;
     const int maxit = o->max_newton > 0 ? o->max_newton : 200;
+    // explicit start-up through the initial transient (local time steps at
+    // cfl0) until the mass residual has dropped by startup_drop
+    bool startup_failed = false;
+    if (o->startup_steps > 0) {
+      const double drop = o->startup_drop > 0. ? o->startup_drop : 1e-3;
+      int k = 0;
+      for (; k < o->startup_steps && rm > drop * r0; ++k) {
+        k_local_dt<double><<<gc, tb, 0, s>>>(x->cs, m, x->p64.W.p, ns.dt.p, cfl0, nullptr);
+        k_explicit_update<<<gc, tb, 0, s>>>(x->cs, nc, ns.Wn.p, ns.R0.p, ns.vol.p, ns.dt.p, x->err.p);
+        int h = 0;
+        CK(cudaMemcpyAsync(&h, x->err.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        if (h & 8) {
+          CK(cudaMemsetAsync(x->err.p, 0, sizeof(int), s));
+          startup_failed = true;
+          break;
+        }
+        eval_residual<double>(x, ns.Wn.p, ns.R0.p, (const double *)nullptr, (const double *)nullptr);
+        check_err(x);
+        rm = dnorm(x, part, hh, ns.R0.p, nc);
+        if (!std::isfinite(rm)) { startup_failed = true; break; }
+      }
+      rep->startup_steps = k;
+      row_norms(rows);
+      rmom = mom(rows);
+      ren = rows[4];
+    }
     const int hist = (int)(sizeof(rep->history) / sizeof(rep->history[0]));
     int rejects = 0;
-    for (int it = 0; it < maxit; ++it) {
+    for (int it = 0; it < maxit && !startup_failed; ++it) {
       if (it < hist) {
         rep->history[it] = rm / r0;
         rep->seconds_history[it] = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
@@ -1762,6 +1834,7 @@ int fcfd_newton_solve(fcfd_ctx *x, double *W, const fcfd_newton_opts *o, fcfd_ne
       cfl_prev = cfl;
       cfl = std::min(std::max(next, 1e-3), cflmax);
     }
+    if (startup_failed) status = FCFD_ERR_DIVERGED;
     CK(cudaStreamSynchronize(s));
     rep->wall_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     rep->res_final = rm;

@@ -343,7 +343,7 @@ class NavierStokes:
                      cfl_growth=1.2, cfl_max=1e6, cfl_mode=1, ser_exponent=1.0, jvp=True, fp32_krylov=False,
                      max_seconds=0.0, raise_on_fail=True, precond_sweeps=0, krylov_cycles=1, exact_jvp=False,
                      fp32_jvp=False, stop_all_rows=False, fp32_frozen_limiter=False, gs_persistent=False, ilu0=False,
-                     local_relax=False):
+                     local_relax=False, startup_steps=0, startup_drop=1e-3):
         """Steady solve R(W) = 0 (pseudo-transient Newton-Krylov on the device).
         stop_all_rows: also wait for the momentum and energy residuals to drop
         by tol.  fp32_frozen_limiter: with fp32_jvp, hold the limiter fixed in
@@ -353,19 +353,22 @@ class NavierStokes:
         ilu0: block ILU(0) preconditioner in the multicolour order instead
         of block Jacobi / Gauss-Seidel.  local_relax: limit each cell's
         update to a 20 % change of p and T on its own instead of scaling the
-        whole update.  Returns (W_converged, report dict)."""
+        whole update.  startup_steps > 0: first up to that many explicit
+        local-time-step steps at cfl0 until the mass residual has dropped by
+        startup_drop.  Returns (W_converged, report dict)."""
         W = np.array(W, dtype=np.float64, order="C", copy=True)
         o = NewtonOpts(int(max_newton), float(tol), int(krylov_dim), float(krylov_rtol), float(cfl0), float(cfl_growth),
                        float(cfl_max), int(cfl_mode), float(ser_exponent),
                        ((4 if fp32_frozen_limiter else 3) if fp32_jvp else (2 if exact_jvp else 1)) if jvp else 0,
                        int(bool(fp32_krylov)), float(max_seconds), int(precond_sweeps), int(krylov_cycles),
-                       int(bool(stop_all_rows)), int(bool(gs_persistent)), int(bool(ilu0)), int(bool(local_relax)))
+                       int(bool(stop_all_rows)), int(bool(gs_persistent)), int(bool(ilu0)), int(bool(local_relax)),
+                       int(startup_steps), float(startup_drop))
         r = NewtonReport()
         rc = lib.fcfd_newton_solve(self.h, _d(W), ctypes.byref(o), ctypes.byref(r))
         rep = dict(status=r.status, newton_iterations=r.newton_iterations, krylov_iterations=r.krylov_iterations,
                    res0=r.res0, res_final=r.res_final, wall_seconds=r.wall_seconds, last_cfl=r.last_cfl,
                    history=np.array(r.history[:r.newton_iterations + 1]), rows_final=list(r.rows_final),
-                   seconds_to_tol=r.seconds_to_tol,
+                   seconds_to_tol=r.seconds_to_tol, startup_steps=r.startup_steps,
                    seconds_history=np.array(r.seconds_history[:r.newton_iterations + 1]))
         if rc != 0 and raise_on_fail:
             raise FcfdError(rc, lib.fcfd_last_error().decode() + f" after {r.newton_iterations} steps")

@@ -322,6 +322,12 @@ typedef struct fcfd_newton_opts {
                              every cell; 1: each cell's update is scaled on its own to that bound
                              (local under-relaxation: cells far from a shock or a wake take full
                              steps), inactive once every cell's change is below the bound */
+  int32_t startup_steps;  /* > 0: before the Newton steps, up to this many explicit steps (forward
+                             Euler in the primitive variables with local time steps at cfl0,
+                             (V P/dt) dW = R per cell) until the mass residual has dropped by
+                             startup_drop; for start-up transients that a linearised implicit step
+                             does not keep physical (an impulsively started hypersonic flow) */
+  double startup_drop;    /* explicit start-up target drop (default 1e-3) */
 } fcfd_newton_opts;
 
 typedef struct fcfd_newton_report {
@@ -332,6 +338,8 @@ typedef struct fcfd_newton_report {
   double seconds_to_tol;  /* wall time when |R_mass| first dropped by tol */
   double seconds_history[512]; /* wall time at each history[] entry */
   double kw_final[2];     /* fcfd_rans_newton_solve: final / initial norm of the k and omega residuals */
+  int32_t startup_steps;  /* explicit start-up steps taken (fcfd_newton_opts.startup_steps) */
+  int32_t pad2;
 } fcfd_newton_report;
 
 /* Mixed-precision residual: fcfd_residual's R(W) with the face pass in FP32
