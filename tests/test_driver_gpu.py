@@ -324,6 +324,8 @@ def test_run_reports_nonphysical_state_as_divergence(oracle_mod, fb, tmp_path):
     W, rep = ns.run(case.state, work_dir=tmp_path, raise_on_fail=False)
     assert rep["status"] == 3, rep
     assert 1 <= rep["steps"] < 20
+    b = tmp_path / "b"
+    b.mkdir()
     with pytest.raises(fb.FcfdError) as e:
-        ns.run(case.state, work_dir=tmp_path / "b" if (tmp_path / "b").mkdir() is None else tmp_path)
+        ns.run(case.state, work_dir=b)
     assert e.value.code == 3
